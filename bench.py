@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark of the HELIOS-K opacity hot path on B200.
+
+One step = one pass of the path over one batch: the Voigt line sum of every
+state onto the grid (hk_opacity, persistent kernel) followed by the per-bin
+sort + Chebyshev k-distribution fit (hk_kdist).  Inputs are resident in HBM
+(line list >> L2, so no L2 flush is needed between steps).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload hitemp|small|table] [--precision mixed|plain]
+
+Metric: Voigt evaluations per second (algorithmic (line, grid point) pairs
+inside the cutoff windows, counted exactly from the index windows), plus the
+seconds per state/table.  Multi-GPU: every rank computes its own copy of the
+workload's states (states are independent; no collective on the data path),
+time = max over ranks, value = pairs of all ranks / that time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "helios-k_b200"))
+
+# algorithmic FP32 flops per pair by region (committed constants; the C-region
+# figure grows with the Algorithm 916 series length n_iter) + 2 for the
+# strength multiply-add into the sum
+F_A, F_B, F_C0, F_C_ITER, F_ACC = 6, 20, 30, 12, 2
+SIZEOF_STATE = 592  # bytes of hkb::StateDev copied per state per call
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="hitemp", choices=["hitemp", "small", "table"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "plain"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP64 comparison leg")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def workload(name):
+    from hkb import synth
+    if name == "table":
+        W = dict(synth.WORKLOADS["hitemp"])
+        T, P = synth.table_states()
+        W["T"], W["P"] = list(T), list(P)
+        W["label"] = "tp-table-1e7-lines-600-states"
+    else:
+        W = dict(synth.WORKLOADS[name])
+        W["label"] = {"hitemp": "hitemp-1e7-lines-single-state",
+                      "small": "small-1e5-lines-single-state"}[name]
+    return W
+
+
+def make_lines(W):
+    from hkb import synth
+    return synth.hitran_lines(W["n"], seed=W["seed"], logS=W["logS"])
+
+
+def open_ctx(W, L, device):
+    import hkb
+    from hkb import synth
+    ctx = hkb.Context(device)
+    ctx.set_species(hkb.HITRAN, [synth.MASS], [1.0])
+    Tq, Qq = synth.q_table()
+    ctx.set_partition(0, Tq, Qq)
+    ctx.set_options(qalphaL=1.0)
+    ctx.load_lines_hitran(L)
+    ctx.set_grid(W["numin"], W["numax"], W["dnu"], W["nbins"], 0, W["cut"])
+    return ctx
+
+
+def count_pairs(ctx, T, P):
+    """Exact (A, B, C) pair counts of one state from the device index windows."""
+    _, _, _, vy, win = ctx.state_lines(T, P)
+    i0, b0, c0, c1, b1, i1 = (win[:, k] for k in range(6))
+    pa = int(np.sum(b0 - i0) + np.sum(i1 - b1))
+    pb = int(np.sum(c0 - b0) + np.sum(b1 - c1))
+    pc = int(np.sum(c1 - c0))
+    return pa, pb, pc, win, vy
+
+
+def c_series_iterations(ctx, T, P, win, vy, sample=1000, seed=0):
+    """Mean Algorithm-916 series length of the FP32 form over region-C pairs,
+    replaying its stopping rule (|delta s| < TOLF for s1, s2, s3) in numpy."""
+    rng = np.random.default_rng(seed)
+    nu, S, iad, _, _ = ctx.state_lines(T, P)
+    has = np.nonzero(win[:, 3] > win[:, 2])[0]
+    if len(has) == 0:
+        return 0.0
+    ls = rng.choice(has, size=min(sample, len(has)))
+    a = np.float32(0.5999962687492371)
+    tol = np.float32(2.48e-12)
+    its = []
+    for l in ls:
+        i = rng.integers(win[l, 2], win[l, 3])
+        x = np.float32(abs((ctx._numin + i * ctx._dnu - nu[l]) * iad[l]))
+        y = np.float32(vy[l])
+        if x == 0 or y == 0:
+            its.append(0)
+            continue
+        n0 = int(np.ceil(x / a))
+        s = np.zeros(3, np.float32)
+        old = np.zeros(3, np.float32)
+        stop = [False] * 3
+        n_it = 0
+        for n in range(1, 100):
+            n_it = n
+            an, ap, am = a * n, a * (n0 + n - 1), a * (n0 - n)
+            yy = y * y
+            s[0] += np.float32(1) / (an * an + yy) * np.exp(-(an * an + x * x))
+            s[1] += np.float32(1) / (an * an + yy) * np.exp(-(an + x) * (an + x))
+            s[2] += np.float32(1) / (ap * ap + yy) * np.exp(-(ap - x) * (ap - x))
+            if n0 - n >= 1:
+                s[2] += np.float32(1) / (am * am + yy) * np.exp(-(am - x) * (am - x))
+            for k in range(3):
+                if abs(s[k] - old[k]) < tol:
+                    stop[k] = True
+            if all(stop):
+                break
+            old[:] = s
+        its.append(n_it)
+    return float(np.mean(its))
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip() == "Active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    lrank = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(lrank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, lrank
+
+
+def barrier_max(ws, value):
+    if ws == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(W, L, T, P, seconds, tile=2048, seed=0):
+    """The FP64 oracle (OpenMP, all host threads) on a bounded sample of grid
+    tiles of the same workload; returns pairs/s and what was sampled."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from hkb import synth
+    Tq, Qq = synth.q_table()
+    Q = oracle.partition(Tq, Qq, T)
+    nu, S, iad, vy = oracle.prep_hitran(L, [synth.MASS], [1.0], [Q], T, P, qalphaL=1.0)
+    nx = oracle.grid_nx(W["numin"], W["numax"], W["dnu"])
+    win = oracle.windows(nu, S, iad, vy, W["numin"], W["dnu"], nx, 0, W["cut"])
+    rng = np.random.default_rng(seed)
+    ntiles = (nx + tile - 1) // tile
+    order = rng.permutation(ntiles)
+    pairs, tsum, used = 0, 0.0, 0
+    for t in order:
+        ib, ie = int(t * tile), int(min(nx, (t + 1) * tile))
+        t0 = time.perf_counter()
+        _, pr = oracle.opacity(nu, S, iad, vy, win, W["numin"], W["dnu"], nx, irange=(ib, ie))
+        tsum += time.perf_counter() - t0
+        pairs += sum(pr)
+        used += 1
+        if tsum >= seconds:
+            break
+    cores = os.cpu_count() or 1
+    return {"value": pairs / tsum, "unit": "Voigt evals/s", "cores": cores, "kind": "port",
+            "sample": f"{used} random {tile}-point grid tiles of {ntiles} "
+                      f"({pairs:.3e} pairs, {tsum:.1f} s), FP64 oracle, OpenMP {cores} threads"}
+
+
+def run_reference(args):
+    """--impl reference: the reference has no CPU path of its own, so the
+    reference arm is the FP64 CPU restatement (oracle) on the box's host
+    cores, each step a bounded sample of the same workload."""
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    W = workload(args.workload)
+    L = make_lines(W)
+    T, P = W["T"][0], W["P"][0]
+    per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
+    vals = []
+    cb = None
+    for k in range(args.warmup + args.steps):
+        cb = cpu_baseline(W, L, T, P, per_step, seed=k)
+        if k >= args.warmup:
+            vals.append(cb["value"])
+    v = float(np.mean(vals))
+    cb["value"] = v
+    out = {"impl": "reference", "metric": "Voigt evals/s", "value": v, "unit": "Voigt evals/s",
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic (seeded; BASELINE config distributions)",
+           "config": {"workload": W["label"], "lines": W["n"], "states": 1, "T": T, "P": P,
+                      "cut": W["cut"], "sample": "bounded grid-tile sample per step"},
+           "cpu_baseline": cb,
+           "e2e": {"value": v, "unit": "Voigt evals/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    ws, rank, lrank = dist_setup(args)
+    import torch
+    import hkb
+    torch.cuda.set_device(lrank)
+    W = workload(args.workload)
+    L = make_lines(W)
+    ctx = open_ctx(W, L, lrank)
+    ctx._numin, ctx._dnu = W["numin"], W["dnu"]
+    T = np.array(W["T"], np.float64)
+    P = np.array(W["P"], np.float64)
+    ns, nx, nb, nC = len(T), ctx.nx, W["nbins"], W["nC"]
+    prec = hkb.MIXED if args.precision == "mixed" else hkb.PLAIN_FP64
+
+    # exact algorithmic work (outside the timed region)
+    per_state = []
+    probe = range(ns) if ns <= 8 else np.linspace(0, ns - 1, 8).astype(int)
+    for s in probe:
+        pa, pb, pc, win, vy = count_pairs(ctx, float(T[s]), float(P[s]))
+        per_state.append((pa, pb, pc))
+    pa, pb, pc = (float(np.mean([p[k] for p in per_state])) for k in range(3))
+    pairs_step = (pa + pb + pc) * ns  # cutMode 0, no shift: same window per state
+    n_iter = c_series_iterations(ctx, float(T[0]), float(P[0]), win, vy) if pc > 0 else 0.0
+    flops_step = ns * (pa * (F_A + F_ACC) + pb * (F_B + F_ACC) + pc * (F_C0 + F_C_ITER * n_iter + F_ACC))
+
+    stream = torch.cuda.current_stream()
+    K = torch.empty((ns, nx), dtype=torch.float64, device="cuda")
+
+    def step(precision):
+        ctx.opacity(T, P, precision, out=K, stream=stream)
+        ctx.kdist(K, nC=nC, stream=stream)
+
+    for _ in range(args.warmup):
+        step(prec)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    clk = Clocks(lrank)
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(prec)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    clocks = clk.stop()
+    ms = barrier_max(ws, ms)
+    launches_per_step = 4  # state prepass (2) + voigt sum + kdist
+
+    # dominant kernel: per-launch device time with CUDA events on the stream
+    vms, kms = [], []
+    for _ in range(max(3, min(args.steps, 10))):
+        step(prec)
+        v, k = ctx.last_timing()
+        vms.append(v)
+        kms.append(k)
+    voigt_ms = float(np.mean(vms))
+    kdist_ms = float(np.mean(kms))
+    fp32_peak = ctx.fp32_peak_tflops()
+
+    # end to end through the public API with host buffers: states in, K and
+    # the fit out to pinned host memory
+    K_host = torch.empty((ns, nx), dtype=torch.float64, pin_memory=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.opacity(T, P, prec, out=K, stream=stream)
+        r = ctx.kdist(K, nC=nC, stream=stream, outputs_on_device=False)
+        K_host.copy_(K, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    e2e_s = barrier_max(ws, e2e_s)
+
+    plain = None
+    if not args.no_plain and args.precision == "mixed":
+        for _ in range(1):
+            step(hkb.PLAIN_FP64)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        nplain = max(1, min(3, args.steps))
+        for _ in range(nplain):
+            step(hkb.PLAIN_FP64)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pms = barrier_max(ws, e0.elapsed_time(e1) / nplain)
+        plain = {"ms_per_step": pms, "value": pairs_step * ws / (pms * 1e-3),
+                 "speedup_mixed_vs_plain": pms / ms}
+
+    value = pairs_step * ws / (ms * 1e-3)
+    out = {
+        "metric": "Voigt evals/s", "value": value, "unit": "Voigt evals/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 profile, f64 offsets/strengths/sum/fit" if prec == hkb.MIXED else "f64",
+        "data": "synthetic (seeded; BASELINE config distributions)",
+        "config": {"workload": W["label"], "lines": W["n"], "grid_points": nx, "states": ns,
+                   "T": W["T"][0] if ns == 1 else "100-3000 K x 20",
+                   "P": W["P"][0] if ns == 1 else "1e-8-1e3 atm x 30",
+                   "cut_cm-1": W["cut"], "nbins": nb, "nC": nC,
+                   "precision": args.precision, "parallelism": f"states x{ws} ranks",
+                   "l2": "inputs larger than L2 (line list ~480 MB resident), no flush"},
+        "s_per_state": ms * 1e-3 / ns,
+        "pairs_per_state": {"A": pa, "B": pb, "C": pc, "C_series_iters": n_iter},
+        "roofline": {"bound": "fp32", "kernel": "voigt_sum_kernel",
+                     "achieved": flops_step / (voigt_ms * 1e-3) / 1e12,
+                     "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": flops_step / (voigt_ms * 1e-3) / 1e12 / fp32_peak,
+                     "traffic": None, "voigt_ms": voigt_ms, "kdist_ms": kdist_ms,
+                     "peak_source": "in-run FP32 FMA probe (hk_fp32_peak); "
+                                    "MEASURED_PEAKS.json has no FP32 SIMT figure"},
+        "e2e": {"value": pairs_step * ws / e2e_s, "unit": "Voigt evals/s",
+                "h2d_bytes_per_step": SIZEOF_STATE * ns,
+                "d2h_bytes_per_step": ns * nx * 8 + ns * nb * (nC * 8 + 4)},
+        "clocks": clocks,
+        "gpu_launches": launches_per_step * args.steps,
+        "plain_fp64": plain,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(W, L, float(T[0]), float(P[0]), args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,250 @@
+// heliosk_main.cpp -- drop-in replacement for the reference executable on the
+// opacity path.  Same inputs (param.dat + "-flag value" overrides,
+// <path><species>.param, partition files, binary line lists) and the same
+// outputs (Info_<name>.dat, Out_<name>.dat/.bin, Out_<name>_cbin*.dat,
+// Out_<name>_bin*.dat) as heliosk.cu:main, computed through libhkb's C ABI.
+//
+// Options outside this path (CIA, species mixtures, bins/edges files, unequal
+// spacing, sub-Lorentzian, plinth removal, profiles 2-4, transmission and
+// means) are rejected with a message instead of being silently ignored.
+// Unlike the reference (heliosk.cu:365-367) a failed run exits with status 1.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "hkb.h"
+#include "hkb_formats.h"
+#include "hkb_types.h"
+
+using namespace hkb;
+
+static int die(const std::string &m) {
+  printf("%s\n", m.c_str());
+  return 1;
+}
+
+int main(int argc, char **argv) {
+  Params p;
+  std::string msg;
+  if (read_param_file("param.dat", argc, argv, p, msg) != 0) return die(msg);
+  if (p.ciaSystem != "-") return die("Error: ciaSystem is outside this build's opacity path");
+  if (p.SpeciesFilename != "-") return die("Error: species mixtures (SpeciesFile) are outside this build's path");
+  if (p.bins != "-" || p.edges != "-") return die("Error: binsFile / OutputEdgesFile are outside this build's path");
+  if (p.Nxb != 0) return die("Error: 'Nnu per bin' (unequal spacing) is outside this build's path");
+  if (p.subLorentzian != "-") return die("Error: sub-Lorentzian profiles are outside this build's path");
+  if (p.removePlinth != 0) return die("Error: removePlinth is outside this build's path");
+  if (p.profile != 1) return die("Error: only profile = 1 (Voigt) is on this build's path");
+  if (p.doTransmission != 0 || p.doMean != 0)
+    return die("Error: transmission / Planck-Rosseland means are outside this build's path");
+  if (p.nbins < 1) return die("Error: nbins must be >= 1");
+
+  const char *mode = p.replaceFiles == 0 ? "a" : "w";
+  const std::string infoName = "Info_" + p.name + ".dat";
+  FILE *info = fopen(infoName.c_str(), mode);
+  if (!info) return die("Error: cannot open " + infoName);
+
+  hk_status st;
+  hk_ctx *c = hk_create(p.dev, &st);
+  if (!c) return die("Error: Device Number is not allowed (hk_create status " + std::to_string(st) + ")");
+  auto chk = [&](hk_status s) {
+    if (s != HK_OK) {
+      printf("Error: %s\n", hk_last_error(c));
+      fprintf(info, "Error: %s\n", hk_last_error(c));
+      fclose(info);
+      hk_destroy(c);
+      exit(1);
+    }
+  };
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  auto seconds = [&]() {
+    float ms = 0.f;
+    cudaEventSynchronize(t1);
+    cudaEventElapsedTime(&ms, t0, t1);
+    return ms * 1e-3;
+  };
+
+  for (FILE *f : {info, stdout}) {
+    fprintf(f, "name = %s\nT = %g\nP = %g\npathToData = %s\nnumin = %g\nnumax = %g\ndnu = %g\n",
+            p.name.c_str(), p.T, p.P, p.path.c_str(), p.numin, p.numax, p.dnu);
+    fprintf(f, "cutMode = %d\ncut = %g\ndoResampling = %d\nnC = %d\ndoStoreFullK = %d\ndoStoreSK = %d\n",
+            p.cutMode, p.cut, p.doResampling, p.nC, p.doStoreFullK, p.doStoreK);
+    fprintf(f, "nbins = %d\nkmin = %g\nqalphaL = %g\ngammaF = %g\nUnits = %d\nReplace files = %d\nprofile = %d\n",
+            p.nbins, p.kmin, p.qalphaL, p.gammaF, p.units, p.replaceFiles, p.profile);
+    fprintf(f, "Species Name = %s\nengine = %s\n\n", p.speciesName.c_str(), hk_version());
+  }
+
+  chk(hk_set_options(c, p.qalphaL, p.gammaF, p.units, 1.0));
+  SpeciesInfo sp;
+  int rc = read_species_param(p.path, p.speciesName, sp, msg);
+  if (rc != 0) return die(msg);
+  double meanMass = 0.0;  // heliosk.cu:665-686
+  for (auto &iso : sp.iso) meanMass += iso.ab * iso.mass * 1.0;
+  double unitScale = 1.0;
+  double kmin = p.kmin;
+  if (p.units == 1) {  // heliosk.cu:692-701
+    unitScale = 1.0 / HK_NA * meanMass;
+    kmin /= unitScale;
+  }
+
+  const bool compute = p.doStoreFullK >= 0;
+  cudaEventRecord(t0);
+  if (compute) chk(hk_load_species_file(c, p.path.c_str(), p.speciesName.c_str(), p.numin, p.numax, p.cutMode, p.cut));
+  cudaEventRecord(t1);
+  const double t_input = compute ? seconds() : 0.0;
+  chk(hk_set_grid(c, p.numin, p.numax, p.dnu, p.nbins, p.cutMode, p.cut, kmin));
+  const int64_t nx = hk_grid_points(c);
+  const int nP = p.nP;
+  std::vector<double> K((size_t)nP * nx), x(nx);
+  for (int64_t i = 0; i < nx; ++i) x[i] = std::fma((double)i, p.dnu, p.numin);  // voigt.h:759
+  std::vector<double> Ts(nP, p.T);
+
+  double t_K = 0.0;
+  if (compute) {
+    printf("Number of lines: %lld\n", (long long)hk_num_lines(c));
+    fprintf(info, "Number of lines: %lld\n", (long long)hk_num_lines(c));
+    cudaEventRecord(t0);
+    chk(hk_opacity(c, nP, Ts.data(), p.Plist.data(), HK_PRECISION_MIXED, K.data(), 0, nullptr));
+    cudaEventRecord(t1);
+    t_K = seconds();
+  } else {
+    // doStoreFullK = -1 / -2: read K back (heliosk.cu:1860-1935)
+    const std::string fn = p.pathK + "Out_" + p.name + (p.doStoreFullK == -1 ? ".dat" : ".bin");
+    FILE *f = fopen(fn.c_str(), p.doStoreFullK == -1 ? "r" : "rb");
+    if (!f) return die("Error: Input file not found " + fn);
+    for (int iP = 0; iP < nP; ++iP) {
+      for (int64_t j = 0; j < nx; ++j) {
+        if (p.doStoreFullK == -1) {
+          double xv, kv, tv, pv;
+          int n = (nP == 1) ? fscanf(f, "%lf %lf", &xv, &kv) : fscanf(f, "%lf %lf %lf %lf", &xv, &kv, &tv, &pv);
+          if (n < 2) return die("Error: truncated " + fn);
+          K[(size_t)iP * nx + j] = kv / unitScale;
+        } else {
+          float kf;
+          if (fread(&kf, sizeof kf, 1, f) != 1) return die("Error: truncated " + fn);
+          K[(size_t)iP * nx + j] = (double)kf / unitScale;
+        }
+      }
+    }
+    fclose(f);
+  }
+
+  // full K output, heliosk.cu:1840-1935
+  if (p.doStoreFullK == 1) {
+    FILE *f = fopen(("Out_" + p.name + ".dat").c_str(), mode);
+    for (int iP = 0; iP < nP; ++iP) {
+      const double *Kp = K.data() + (size_t)iP * nx;
+      for (int64_t j = 0; j < nx; ++j) {
+        if (nP == 1) fprintf(f, "%.20g %.20g\n", x[j], Kp[j] * unitScale);
+        else fprintf(f, "%.20g %.20g %.20g %.20g\n", x[j], Kp[j] * unitScale, p.T, p.Plist[iP]);
+      }
+      fprintf(f, "\n\n");
+    }
+    fclose(f);
+  } else if (p.doStoreFullK == 2) {
+    FILE *f = fopen(("Out_" + p.name + ".bin").c_str(), p.replaceFiles == 0 ? "ab" : "wb");
+    for (int64_t j = 0; j < (int64_t)nP * nx; ++j) {
+      const float kf = (float)(K[j] * unitScale);
+      fwrite(&kf, sizeof kf, 1, f);
+    }
+    fclose(f);
+  }
+
+  // sort + resampling, heliosk.cu:2046-2193
+  const int nxb = (int)(nx / p.nbins);
+  const bool fit = p.doResampling > 0;
+  std::vector<double> coeff, sorted, recon;
+  std::vector<int32_t> nxmin;
+  double t_fit = 0.0;
+  if (fit || p.doStoreK > 0) {
+    if (fit) {
+      coeff.resize((size_t)nP * p.nbins * p.nC);
+      nxmin.resize((size_t)nP * p.nbins);
+    }
+    if (p.doStoreK > 0) (fit ? recon : sorted).resize((size_t)nP * nx);
+    cudaEventRecord(t0);
+    chk(hk_kdist(c, nP, K.data(), 0, p.nC, unitScale, fit ? coeff.data() : nullptr,
+                 fit ? nxmin.data() : nullptr, (!fit && p.doStoreK > 0) ? sorted.data() : nullptr,
+                 (fit && p.doStoreK > 0) ? recon.data() : nullptr, 0, nullptr));
+    cudaEventRecord(t1);
+    t_fit = seconds();
+  }
+  if (fit) {
+    FILE *f = nullptr;
+    if (p.doResampling == 1) f = fopen(("Out_" + p.name + "_cbin.dat").c_str(), mode);
+    char fn[512];
+    if (p.doResampling == 2 && p.replaceFiles == 1)
+      for (int i = 0; i < p.nbins; ++i) {
+        snprintf(fn, sizeof fn, "Out_%s_cbin%.4d.dat", p.name.c_str(), i);
+        fclose(fopen(fn, "w"));
+      }
+    for (int iP = 0; iP < nP; ++iP) {
+      for (int i = 0; i < p.nbins; ++i) {
+        if (p.doResampling == 2) {
+          snprintf(fn, sizeof fn, "Out_%s_cbin%.4d.dat", p.name.c_str(), i);
+          f = fopen(fn, "a");
+        }
+        const int nm = nxmin[(size_t)iP * p.nbins + i];
+        fprintf(f, "%.20g %.20g ", p.kmin, std::fmin(nm / ((double)(nxb - 1)), 1.0));
+        for (int ic = 0; ic < p.nC; ++ic) {
+          if (nm != nxb) fprintf(f, "%.20g ", coeff[((size_t)iP * p.nbins + i) * p.nC + ic]);
+          else fprintf(f, "0.0 ");
+        }
+        if (nP > 1) fprintf(f, "%.20g %.20g ", p.T, p.Plist[iP]);
+        if (p.doResampling == 1) fprintf(f, "\n\n");
+        if (p.doResampling == 2) {
+          if (i < p.nbins - 1) fprintf(f, "\n");
+          fclose(f);
+          f = nullptr;
+        }
+      }
+    }
+    if (f) fclose(f);
+  }
+  // per-bin sorted (or reconstructed) K, heliosk.cu:2219-2290
+  if (p.doStoreK > 0) {
+    const std::vector<double> &Kb = fit ? recon : sorted;
+    char fn[512];
+    FILE *f = nullptr;
+    if (p.doStoreK == 1) f = fopen(("Out_" + p.name + "_bin.dat").c_str(), mode);
+    if (p.doStoreK == 2 && p.replaceFiles == 1)
+      for (int i = 0; i < p.nbins; ++i) {
+        snprintf(fn, sizeof fn, "Out_%s_bin%.4d.dat", p.name.c_str(), i);
+        fclose(fopen(fn, "w"));
+      }
+    for (int iP = 0; iP < nP; ++iP) {
+      for (int i = 0; i < p.nbins; ++i) {
+        if (p.doStoreK == 2) {
+          snprintf(fn, sizeof fn, "Out_%s_bin%.4d.dat", p.name.c_str(), i);
+          f = fopen(fn, "a");
+        }
+        const double *Kp = Kb.data() + (size_t)iP * nx + (size_t)i * nxb;
+        for (int j = 0; j < nxb; ++j) {
+          const double y = j / ((double)(nxb - 1));
+          if (nP == 1) fprintf(f, "%g %.20g\n", y, Kp[j] * unitScale);
+          else fprintf(f, "%g %.20g %g %g %d\n", y, Kp[j] * unitScale, p.T, p.Plist[iP], j);
+        }
+        if (p.doStoreK == 1) fprintf(f, "\n\n");
+        if (p.doStoreK == 2) {
+          fclose(f);
+          f = nullptr;
+        }
+      }
+    }
+    if (f) fclose(f);
+  }
+
+  for (FILE *f : {info, stdout}) {
+    fprintf(f, "Time for input:        %g seconds\n", t_input);
+    fprintf(f, "Time for K(x):         %g seconds\n", t_K);
+    fprintf(f, "Time for sort and Resampling:   %g seconds\n", t_fit);
+  }
+  fclose(info);
+  hk_destroy(c);
+  return 0;
+}

@@ -1,0 +1,645 @@
+// hkb_api.cu -- the C ABI of libhkb (declared in include/hkb.h).
+//
+// Host runtime: context, resident line list, grid, per-state constants and
+// the launch sequence.  All arithmetic on lines and grid points runs on the
+// GPU; the host only forms per-state scalars (partition-function
+// interpolation, Doppler factors) exactly as the reference's host code does.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hkb.h"
+#include "hkb_formats.h"
+#include "hkb_kernels.h"
+#include "hkb_types.h"
+
+using namespace hkb;
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&p, b ? b : 16);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+struct hk_ctx {
+  int device = 0;
+  std::string err;
+  // species
+  int database = HK_DB_HITRAN;
+  std::vector<double> iso_mass, iso_ab;
+  double defaultL = 0.0, defaultn = 0.0;
+  std::vector<std::vector<double>> qT, qQ;
+  double qalphaL = 0.5, gammaF = 1.0, Sscale = 1.0;
+  int units = 0;
+  // lines (device, nu-sorted)
+  int64_t nlines = 0;
+  DevBuf nu0, Sfile, EL, gam, nexp, delta, Aterm, iso, order;
+  LinesDev L{};
+  double max_abs_delta = 0.0;
+  // grid
+  bool grid_set = false;
+  GridDev g{};
+  double numax = 0.0;
+  int nbins = 0, nxb = 0;
+  double kmin = 0.0;
+  // workspace
+  DevBuf states, ticket, maxexp, wbits, Kwork, outwork, scratch;
+  DevBuf qrV, qrC, qrD;
+  int qr_nxb = -1, qr_nc = -1;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool have_voigt_t = false, have_kdist_t = false;
+};
+
+static hk_status fail(hk_ctx *c, hk_status s, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return s;
+}
+
+#define CUDA_TRY(ctx, expr)                                                   \
+  do {                                                                        \
+    cudaError_t e_ = (expr);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return fail(ctx, (e_ == cudaErrorMemoryAllocation) ? HK_ERR_NOMEM       \
+                                                         : HK_ERR_CUDA,       \
+                  "%s: %s", #expr, cudaGetErrorString(e_));                   \
+  } while (0)
+
+static void ok(hk_ctx *c) { c->err.clear(); }
+
+extern "C" {
+
+const char *hk_version(void) { return "hkb 0.1 (sm_100a)"; }
+
+hk_ctx *hk_create(int device, hk_status *status) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    if (status) *status = HK_ERR_CUDA;
+    return nullptr;
+  }
+  if (device < 0 || device >= n) {
+    if (status) *status = HK_ERR_ARG;
+    return nullptr;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    if (status) *status = HK_ERR_CUDA;
+    return nullptr;
+  }
+  hk_ctx *c = new hk_ctx();
+  c->device = device;
+  for (auto &e : c->ev) cudaEventCreate(&e);
+  if (c->ticket.ensure(sizeof(unsigned)) != cudaSuccess) {
+    delete c;
+    if (status) *status = HK_ERR_NOMEM;
+    return nullptr;
+  }
+  if (status) *status = HK_OK;
+  return c;
+}
+
+void hk_destroy(hk_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  for (DevBuf *b : {&c->nu0, &c->Sfile, &c->EL, &c->gam, &c->nexp, &c->delta,
+                    &c->Aterm, &c->iso, &c->order, &c->states, &c->ticket,
+                    &c->maxexp, &c->wbits, &c->Kwork, &c->outwork, &c->scratch,
+                    &c->qrV, &c->qrC, &c->qrD})
+    b->release();
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+  delete c;
+}
+
+const char *hk_last_error(const hk_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+int hk_tile_points(void) { return voigt_tile_points(); }
+
+// ------------------------------------------------------------- species
+hk_status hk_set_species(hk_ctx *c, int database, int niso, const double *mass,
+                         const double *ab, double defaultL, double defaultn) {
+  if (!c) return HK_ERR_ARG;
+  if (database != HK_DATABASE_HITRAN && database != HK_DATABASE_EXOMOL)
+    return fail(c, HK_ERR_UNSUPPORTED, "database %d: only 0 (HITRAN) and 2 (ExoMol) are on this path", database);
+  if (niso < 1 || niso > HK_MAX_ISO || !mass || !ab)
+    return fail(c, HK_ERR_ARG, "niso must be 1..%d with mass and abundance arrays", HK_MAX_ISO);
+  for (int i = 0; i < niso; ++i)
+    if (!(mass[i] > 0.0)) return fail(c, HK_ERR_ARG, "isotopologue %d: mass must be > 0", i);
+  c->database = database;
+  c->iso_mass.assign(mass, mass + niso);
+  c->iso_ab.assign(ab, ab + niso);
+  c->defaultL = defaultL;
+  c->defaultn = defaultn;
+  c->qT.assign(niso, {});
+  c->qQ.assign(niso, {});
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_set_partition(hk_ctx *c, int iso, int n, const double *T, const double *Q) {
+  if (!c) return HK_ERR_ARG;
+  if (iso < 0 || iso >= (int)c->qT.size()) return fail(c, HK_ERR_STATE, "hk_set_species must come first (iso %d)", iso);
+  if (n < 1 || !T || !Q) return fail(c, HK_ERR_ARG, "empty partition table");
+  c->qT[iso].assign(T, T + n);
+  c->qQ[iso].assign(Q, Q + n);
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_set_options(hk_ctx *c, double qalphaL, double gammaF, int units, double Sscale) {
+  if (!c) return HK_ERR_ARG;
+  if (units != 0 && units != 1) return fail(c, HK_ERR_ARG, "units must be 0 or 1");
+  c->qalphaL = qalphaL;
+  c->gammaF = gammaF;
+  c->units = units;
+  c->Sscale = Sscale;
+  ok(c);
+  return HK_OK;
+}
+
+// --------------------------------------------------------------- lines
+static bool uniform(const double *a, int64_t n) {
+  for (int64_t i = 1; i < n; ++i)
+    if (a[i] != a[0]) return false;
+  return true;
+}
+
+// Upload one column; a uniform column becomes a scalar (null pointer).
+static hk_status upload_col(hk_ctx *c, DevBuf &buf, const std::vector<double> &h,
+                            bool allow_uniform, const double **dptr, double *cval) {
+  const int64_t n = (int64_t)h.size();
+  *cval = n ? h[0] : 0.0;
+  if (allow_uniform && uniform(h.data(), n)) {
+    buf.release();
+    *dptr = nullptr;
+    return HK_OK;
+  }
+  DevBuf tmp;
+  CUDA_TRY(c, tmp.ensure(n * sizeof(double)));
+  CUDA_TRY(c, cudaMemcpy(tmp.p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(c, buf.ensure(n * sizeof(double)));
+  CUDA_TRY(c, launch_gather_lines(n, c->order.as<int64_t>(), tmp.as<double>(), buf.as<double>(), 0));
+  CUDA_TRY(c, cudaDeviceSynchronize());
+  tmp.release();
+  *dptr = buf.as<double>();
+  return HK_OK;
+}
+
+static hk_status load_common(hk_ctx *c, int64_t n, const double *nu,
+                             const std::vector<double> &Sv, const std::vector<double> &ELv,
+                             const std::vector<double> &gamv, const std::vector<double> &nexpv,
+                             const std::vector<double> &deltav, const std::vector<double> &Atv,
+                             const std::vector<uint8_t> &isov) {
+  cudaSetDevice(c->device);
+  c->nlines = 0;
+  c->L = LinesDev{};
+  c->L.database = c->database;
+  if (n == 0) {
+    ok(c);
+    return HK_OK;
+  }
+  // sort by centre on the GPU (once per load)
+  CUDA_TRY(c, c->nu0.ensure(n * sizeof(double)));
+  CUDA_TRY(c, c->order.ensure(n * sizeof(int64_t)));
+  CUDA_TRY(c, cudaMemcpy(c->nu0.p, nu, n * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(c, sort_lines_by_nu(n, c->nu0.as<double>(), c->order.as<int64_t>(), 0));
+  CUDA_TRY(c, cudaDeviceSynchronize());
+  hk_status st;
+  const double *p;
+  double cv;
+  if ((st = upload_col(c, c->Sfile, Sv, false, &p, &cv)) != HK_OK) return st;
+  c->L.Sfile = p;
+  if ((st = upload_col(c, c->EL, ELv, true, &p, &cv)) != HK_OK) return st;
+  c->L.EL = p;
+  c->L.EL_c = cv;
+  if ((st = upload_col(c, c->gam, gamv, true, &p, &cv)) != HK_OK) return st;
+  c->L.gam = p;
+  c->L.gam_c = cv;
+  if ((st = upload_col(c, c->nexp, nexpv, true, &p, &cv)) != HK_OK) return st;
+  c->L.nexp = p;
+  c->L.nexp_c = cv;
+  if ((st = upload_col(c, c->delta, deltav, true, &p, &cv)) != HK_OK) return st;
+  c->L.delta = p;
+  c->L.delta_c = cv;
+  if ((st = upload_col(c, c->Aterm, Atv, true, &p, &cv)) != HK_OK) return st;
+  c->L.Aterm = p;
+  c->L.Aterm_c = cv;
+  bool iso_uniform = true;
+  for (int64_t i = 1; i < n; ++i)
+    if (isov[i] != isov[0]) { iso_uniform = false; break; }
+  if (iso_uniform && isov[0] == 0) {
+    c->iso.release();
+    c->L.iso = nullptr;
+  } else {
+    // gather on the host side of the permutation: pull the order back
+    std::vector<int64_t> ord(n);
+    CUDA_TRY(c, cudaMemcpy(ord.data(), c->order.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    std::vector<uint8_t> sorted(n);
+    for (int64_t k = 0; k < n; ++k) sorted[k] = isov[ord[k]];
+    CUDA_TRY(c, c->iso.ensure(n));
+    CUDA_TRY(c, cudaMemcpy(c->iso.p, sorted.data(), n, cudaMemcpyHostToDevice));
+    c->L.iso = c->iso.as<uint8_t>();
+  }
+  double md = 0.0;
+  for (double d : deltav) md = std::max(md, std::fabs(d));
+  c->max_abs_delta = md;
+  c->L.nu0 = c->nu0.as<double>();
+  c->L.n = n;
+  c->nlines = n;
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_load_lines_hitran(hk_ctx *c, int64_t n, const double *nu, const double *S,
+                               const double *EL, const double *A, const double *delta,
+                               const double *gair, const double *gself, const double *nexp,
+                               const int32_t *iso) {
+  if (!c) return HK_ERR_ARG;
+  if (c->iso_mass.empty()) return fail(c, HK_ERR_STATE, "hk_set_species must come before loading lines");
+  if (c->database != HK_DB_HITRAN) return fail(c, HK_ERR_STATE, "species database is not HITRAN");
+  if (n < 0 || (n > 0 && (!nu || !S || !EL || !A || !delta || !gair || !gself || !nexp)))
+    return fail(c, HK_ERR_ARG, "null line array");
+  const int niso = (int)c->iso_mass.size();
+  std::vector<double> Sv(S, S + n), ELv(EL, EL + n), gamv(n), nexpv(nexp, nexp + n),
+      deltav(delta, delta + n), Atv(n);
+  std::vector<uint8_t> isov(n, 0);
+  for (int64_t i = 0; i < n; ++i) {
+    if (iso) {
+      if (iso[i] < 0 || iso[i] >= niso)
+        return fail(c, HK_ERR_FORMAT, "line %lld: isotopologue index %d not in the species table", (long long)i, iso[i]);
+      isov[i] = (uint8_t)iso[i];
+    }
+    // host.h:640-641
+    double vy = (1.0 - c->qalphaL) * gair[i] + c->qalphaL * gself[i];
+    vy *= c->gammaF;
+    gamv[i] = vy;
+    // voigt.h:349
+    Atv[i] = A[i] / (4.0 * M_PI * HK_C);
+  }
+  return load_common(c, n, nu, Sv, ELv, gamv, nexpv, deltav, Atv, isov);
+}
+
+hk_status hk_load_lines_exomol(hk_ctx *c, int64_t n, const double *nu, const double *S,
+                               const double *EL, const double *A) {
+  if (!c) return HK_ERR_ARG;
+  if (c->iso_mass.empty()) return fail(c, HK_ERR_STATE, "hk_set_species must come before loading lines");
+  if (c->database != HK_DB_EXOMOL) return fail(c, HK_ERR_STATE, "species database is not ExoMol");
+  if (n < 0 || (n > 0 && (!nu || !S || !EL || !A))) return fail(c, HK_ERR_ARG, "null line array");
+  std::vector<double> Sv(S, S + n), ELv(EL, EL + n), gamv(n), nexpv(n, c->defaultn),
+      deltav(n, 0.0), Atv(n);
+  std::vector<uint8_t> isov(n, 0);
+  for (int64_t i = 0; i < n; ++i) {
+    gamv[i] = c->defaultL * c->gammaF;          // voigt.h:497
+    Atv[i] = A[i] / (4.0 * M_PI * HK_C);        // voigt.h:496
+  }
+  return load_common(c, n, nu, Sv, ELv, gamv, nexpv, deltav, Atv, isov);
+}
+
+int64_t hk_num_lines(const hk_ctx *c) { return c ? c->nlines : 0; }
+
+hk_status hk_line_order(hk_ctx *c, int64_t *order) {
+  if (!c || !order) return HK_ERR_ARG;
+  if (c->nlines == 0) return HK_OK;
+  cudaSetDevice(c->device);
+  CUDA_TRY(c, cudaMemcpy(order, c->order.p, c->nlines * sizeof(int64_t), cudaMemcpyDeviceToHost));
+  ok(c);
+  return HK_OK;
+}
+
+// ---------------------------------------------------------------- grid
+hk_status hk_set_grid(hk_ctx *c, double numin, double numax, double dnu, int nbins,
+                      int cutMode, double cut, double kmin) {
+  if (!c) return HK_ERR_ARG;
+  if (!(dnu > 0.0) || !(numax > numin)) return fail(c, HK_ERR_ARG, "need numax > numin and dnu > 0");
+  if (nbins < 1) return fail(c, HK_ERR_ARG, "nbins must be >= 1");
+  if (cutMode < 0 || cutMode > 2) return fail(c, HK_ERR_ARG, "cutMode must be 0, 1 or 2");
+  if (cut < 0.0) return fail(c, HK_ERR_ARG, "cut must be >= 0");
+  // heliosk.cu:448-461
+  const double nxd = (numax - numin) / dnu + 0.5;
+  if (nxd >= 2147483647.0) return fail(c, HK_ERR_RANGE, "Nx too large, integer overflow. %g", nxd);
+  const int nx = (int)nxd;
+  if (nx % nbins != 0)
+    return fail(c, HK_ERR_RANGE, "range cannot be divided evenly in bins. %d %d %g", nx, nbins, nx / (double)nbins);
+  c->g.numin = numin;
+  c->g.dnu = dnu;
+  c->g.nx = nx;
+  c->g.cutMode = cutMode;
+  c->g.cut = (cut == 0.0) ? 1.0e30 : cut;  // heliosk.cu:947
+  c->numax = numax;
+  c->nbins = nbins;
+  c->nxb = nx / nbins;
+  c->kmin = kmin;
+  c->grid_set = true;
+  ok(c);
+  return HK_OK;
+}
+
+int64_t hk_grid_points(const hk_ctx *c) { return (c && c->grid_set) ? c->g.nx : 0; }
+
+// --------------------------------------------------------------- states
+static hk_status build_states(hk_ctx *c, int nstates, const double *T, const double *P,
+                              std::vector<StateDev> &out) {
+  const int niso = (int)c->iso_mass.size();
+  double meanMass = 0.0;  // heliosk.cu:672-686
+  for (int i = 0; i < niso; ++i) meanMass += c->iso_ab[i] * c->iso_mass[i] * c->Sscale;
+  out.assign(nstates, StateDev{});
+  for (int s = 0; s < nstates; ++s) {
+    StateDev &st = out[s];
+    const double Ts = T[s], Ps = P[s];
+    if (!(Ts > 0.0)) return fail(c, HK_ERR_ARG, "state %d: T must be > 0", s);
+    if (!(Ps >= 0.0)) return fail(c, HK_ERR_ARG, "state %d: P must be >= 0", s);
+    st.T = Ts;
+    st.P = Ps;
+    st.PoverP0 = (c->database == HK_DB_HITRAN) ? Ps / HK_PO_ATM : Ps / HK_PO_BAR;
+    st.powbase = HK_T0 / Ts;
+    st.c1 = HK_H * HK_C / (HK_KB * Ts);
+    st.scale = 1.0;
+    st.inv_scale = 1.0;
+    st.wmax = c->g.cut;
+    st.shift = c->max_abs_delta * Ps;
+    st.kmin = c->kmin;
+    for (int j = 0; j < niso; ++j) {
+      double Q;
+      if (c->qT[j].empty()) return fail(c, HK_ERR_STATE, "no partition table for isotopologue %d", j);
+      if (!partition_interp(c->qT[j].data(), c->qQ[j].data(), (int)c->qT[j].size(), Ts, &Q))
+        return fail(c, HK_ERR_RANGE, "partition function not valid for given temperature. T: %g (isotopologue %d)", Ts, j);
+      const double mass = c->iso_mass[j] / HK_NA;
+      st.iad0[j] = HK_C * std::sqrt(mass / (2.0 * HK_KB * Ts));
+      st.Q[j] = Q;
+      double Abundance = c->iso_ab[j];
+      double Ss = c->Sscale;
+      if (c->units == 0) {
+        Abundance *= c->iso_mass[j] / meanMass;
+        Ss *= c->iso_mass[j] / meanMass;
+      }
+      st.ab[j] = Abundance;
+      st.ss[j] = Ss;
+    }
+  }
+  return HK_OK;
+}
+
+static hk_status check_ready(hk_ctx *c) {
+  if (!c->grid_set) return fail(c, HK_ERR_STATE, "hk_set_grid must come first");
+  if (c->iso_mass.empty()) return fail(c, HK_ERR_STATE, "hk_set_species must come first");
+  return HK_OK;
+}
+
+hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, int precision,
+                     double *K_out, int K_on_device, void *stream) {
+  if (!c) return HK_ERR_ARG;
+  hk_status st;
+  if ((st = check_ready(c)) != HK_OK) return st;
+  if (nstates < 1 || !T || !P || !K_out) return fail(c, HK_ERR_ARG, "need nstates >= 1, T, P and K_out");
+  if (precision != HK_PRECISION_PLAIN_FP64 && precision != HK_PRECISION_MIXED)
+    return fail(c, HK_ERR_ARG, "precision must be 0 (plain FP64) or 1 (mixed)");
+  if (nstates > 65535) return fail(c, HK_ERR_RANGE, "at most 65535 states per call");
+  cudaSetDevice(c->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<StateDev> hs;
+  if ((st = build_states(c, nstates, T, P, hs)) != HK_OK) return st;
+  CUDA_TRY(c, c->states.ensure(nstates * sizeof(StateDev)));
+  CUDA_TRY(c, c->maxexp.ensure(nstates * sizeof(int)));
+  CUDA_TRY(c, c->wbits.ensure(nstates * sizeof(unsigned long long)));
+  CUDA_TRY(c, cudaMemcpyAsync(c->states.p, hs.data(), nstates * sizeof(StateDev), cudaMemcpyHostToDevice, s));
+  const int64_t nx = c->g.nx;
+  double *Kd = K_out;
+  if (!K_on_device) {
+    CUDA_TRY(c, c->Kwork.ensure((size_t)nstates * nx * sizeof(double)));
+    Kd = c->Kwork.as<double>();
+  }
+  CUDA_TRY(c, launch_state_prepass(c->L, c->g, c->states.as<StateDev>(), nstates,
+                                   c->maxexp.as<int>(), c->wbits.as<unsigned long long>(), s));
+  if (precision == HK_PRECISION_PLAIN_FP64) {
+    // the plain form computes in FP64 with unit scale
+    // (prepass also sets wmax, which the plain form needs too)
+  }
+  CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
+  CUDA_TRY(c, launch_voigt_sum(precision == HK_PRECISION_MIXED, c->L, c->g,
+                               c->states.as<StateDev>(), nstates, c->ticket.as<unsigned>(),
+                               Kd, nx, 0, s));
+  CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
+  c->have_voigt_t = true;
+  if (!K_on_device) {
+    CUDA_TRY(c, cudaMemcpyAsync(K_out, Kd, (size_t)nstates * nx * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(c, cudaStreamSynchronize(s));
+  }
+  ok(c);
+  return HK_OK;
+}
+
+// -------------------------------------------------------------- kdist
+static hk_status ensure_qr(hk_ctx *c, int nc, cudaStream_t s) {
+  if (c->qr_nxb == c->nxb && c->qr_nc == nc) return HK_OK;
+  CUDA_TRY(c, c->qrV.ensure((size_t)c->nxb * nc * sizeof(double)));
+  CUDA_TRY(c, c->qrC.ensure(nc * sizeof(double)));
+  CUDA_TRY(c, c->qrD.ensure(nc * sizeof(double)));
+  CUDA_TRY(c, launch_qr(c->nxb, nc, c->qrV.as<double>(), c->qrC.as<double>(), c->qrD.as<double>(), s));
+  c->qr_nxb = c->nxb;
+  c->qr_nc = nc;
+  return HK_OK;
+}
+
+hk_status hk_kdist(hk_ctx *c, int nstates, const double *K, int K_on_device, int nC,
+                   double unitScale, double *coeff_out, int32_t *nxmin_out,
+                   double *sortedK_out, double *recon_out, int outputs_on_device, void *stream) {
+  if (!c) return HK_ERR_ARG;
+  if (!c->grid_set) return fail(c, HK_ERR_STATE, "hk_set_grid must come first");
+  if (nstates < 1 || !K) return fail(c, HK_ERR_ARG, "need nstates >= 1 and K");
+  if (nstates > 65535) return fail(c, HK_ERR_RANGE, "at most 65535 states per call");
+  const bool fit = coeff_out || nxmin_out || recon_out;
+  if (fit) {
+    if (nC < 1 || nC > 100) return fail(c, HK_ERR_RANGE, "nC must be 1..100 (def_NmaxSample)");
+    if (c->nxb < 4 || nC > c->nxb) return fail(c, HK_ERR_RANGE, "need Nxb >= 4 and nC <= Nxb for the fit");
+  }
+  cudaSetDevice(c->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t nx = c->g.nx;
+  const size_t nK = (size_t)nstates * nx;
+  const double *Kd = K;
+  if (!K_on_device) {
+    CUDA_TRY(c, c->Kwork.ensure(nK * sizeof(double)));
+    CUDA_TRY(c, cudaMemcpyAsync(c->Kwork.p, K, nK * sizeof(double), cudaMemcpyHostToDevice, s));
+    Kd = c->Kwork.as<double>();
+  }
+  hk_status st;
+  if (fit && (st = ensure_qr(c, nC, s)) != HK_OK) return st;
+  // device outputs: caller's or the workspace
+  const size_t ncoef = (size_t)nstates * c->nbins * (fit ? nC : 0);
+  const size_t nnx = (size_t)nstates * c->nbins;
+  double *coef_d = nullptr, *sorted_d = nullptr, *recon_d = nullptr;
+  int *nxmin_d = nullptr;
+  if (outputs_on_device) {
+    coef_d = coeff_out;
+    nxmin_d = nxmin_out;
+    sorted_d = sortedK_out;
+    recon_d = recon_out;
+  } else {
+    size_t bytes = ncoef * 8 + nnx * 4 + 64 + (sortedK_out ? nK * 8 : 0) + (recon_out ? nK * 8 : 0);
+    CUDA_TRY(c, c->outwork.ensure(bytes));
+    char *base = (char *)c->outwork.p;
+    size_t off = 0;
+    if (fit) { coef_d = (double *)(base + off); off += ncoef * 8; }
+    if (sortedK_out) { sorted_d = (double *)(base + off); off += nK * 8; }
+    if (recon_out) { recon_d = (double *)(base + off); off += nK * 8; }
+    if (fit) { nxmin_d = (int *)(base + off); off += nnx * 4; }
+  }
+  // the fit chain needs Nxmin even if the caller does not ask for it
+  DevBuf nxtmp;
+  if (fit && !nxmin_d) {
+    CUDA_TRY(c, nxtmp.ensure(nnx * sizeof(int)));
+    nxmin_d = nxtmp.as<int>();
+  }
+  double *scr = nullptr;
+  const size_t nscr = kdist_scratch_doubles(c->nxb, c->nbins, nstates);
+  if (nscr) {
+    CUDA_TRY(c, c->scratch.ensure(nscr * sizeof(double)));
+    scr = c->scratch.as<double>();
+  }
+  CUDA_TRY(c, cudaEventRecord(c->ev[2], s));
+  CUDA_TRY(c, launch_kdist(Kd, nx, nstates, c->nxb, c->nbins, fit ? nC : 0, c->kmin, unitScale,
+                           c->qrV.as<double>(), c->qrC.as<double>(), c->qrD.as<double>(),
+                           fit ? coef_d : nullptr, nxmin_d, sorted_d, recon_d, scr, s));
+  CUDA_TRY(c, cudaEventRecord(c->ev[3], s));
+  c->have_kdist_t = true;
+  if (!outputs_on_device) {
+    if (coeff_out) CUDA_TRY(c, cudaMemcpyAsync(coeff_out, coef_d, ncoef * 8, cudaMemcpyDeviceToHost, s));
+    if (nxmin_out) CUDA_TRY(c, cudaMemcpyAsync(nxmin_out, nxmin_d, nnx * 4, cudaMemcpyDeviceToHost, s));
+    if (sortedK_out) CUDA_TRY(c, cudaMemcpyAsync(sortedK_out, sorted_d, nK * 8, cudaMemcpyDeviceToHost, s));
+    if (recon_out) CUDA_TRY(c, cudaMemcpyAsync(recon_out, recon_d, nK * 8, cudaMemcpyDeviceToHost, s));
+  }
+  if (!outputs_on_device || nxtmp.p) CUDA_TRY(c, cudaStreamSynchronize(s));
+  nxtmp.release();
+  ok(c);
+  return HK_OK;
+}
+
+// --------------------------------------------------------- diagnostics
+hk_status hk_state_lines(hk_ctx *c, double T, double P, double *nu, double *S, double *iad,
+                         double *vy, int64_t *win6) {
+  if (!c) return HK_ERR_ARG;
+  hk_status st;
+  if ((st = check_ready(c)) != HK_OK) return st;
+  cudaSetDevice(c->device);
+  std::vector<StateDev> hs;
+  if ((st = build_states(c, 1, &T, &P, hs)) != HK_OK) return st;
+  const int64_t n = c->nlines;
+  if (n == 0) return HK_OK;
+  DevBuf o4, w6;
+  CUDA_TRY(c, o4.ensure(n * 4 * sizeof(double)));
+  CUDA_TRY(c, w6.ensure(n * 6 * sizeof(long long)));
+  CUDA_TRY(c, launch_prep_dump(c->L, c->g, hs[0], o4.as<double>(), w6.as<long long>(), 0));
+  CUDA_TRY(c, cudaDeviceSynchronize());
+  std::vector<double> h4(n * 4);
+  CUDA_TRY(c, cudaMemcpy(h4.data(), o4.p, n * 4 * sizeof(double), cudaMemcpyDeviceToHost));
+  if (win6) CUDA_TRY(c, cudaMemcpy(win6, w6.p, n * 6 * sizeof(long long), cudaMemcpyDeviceToHost));
+  for (int64_t l = 0; l < n; ++l) {
+    if (nu) nu[l] = h4[4 * l + 0];
+    if (S) S[l] = h4[4 * l + 1];
+    if (iad) iad[l] = h4[4 * l + 2];
+    if (vy) vy[l] = h4[4 * l + 3];
+  }
+  o4.release();
+  w6.release();
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_profile_eval(hk_ctx *c, int64_t n, const double *x, const double *y, int precision,
+                          double *out) {
+  if (!c || n < 0 || (n > 0 && (!x || !y || !out))) return HK_ERR_ARG;
+  if (n == 0) return HK_OK;
+  cudaSetDevice(c->device);
+  DevBuf b;
+  CUDA_TRY(c, b.ensure(n * 3 * sizeof(double)));
+  double *xd = b.as<double>(), *yd = xd + n, *od = yd + n;
+  CUDA_TRY(c, cudaMemcpy(xd, x, n * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(yd, y, n * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, launch_profile_eval(n, xd, yd, precision == HK_PRECISION_MIXED, od, 0));
+  CUDA_TRY(c, cudaMemcpy(out, od, n * 8, cudaMemcpyDeviceToHost));
+  b.release();
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_last_timing(const hk_ctx *c, double *voigt_ms, double *kdist_ms) {
+  if (!c) return HK_ERR_ARG;
+  float ms = 0.f;
+  if (voigt_ms) {
+    *voigt_ms = -1.0;
+    if (c->have_voigt_t && cudaEventSynchronize(c->ev[1]) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]) == cudaSuccess)
+      *voigt_ms = ms;
+  }
+  if (kdist_ms) {
+    *kdist_ms = -1.0;
+    if (c->have_kdist_t && cudaEventSynchronize(c->ev[3]) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]) == cudaSuccess)
+      *kdist_ms = ms;
+  }
+  return HK_OK;
+}
+
+hk_status hk_fp32_peak(hk_ctx *c, double *tflops) {
+  if (!c || !tflops) return HK_ERR_ARG;
+  cudaSetDevice(c->device);
+  CUDA_TRY(c, measure_fp32_peak(tflops, 0));
+  ok(c);
+  return HK_OK;
+}
+
+// ---------------------------------------------------------- file loader
+hk_status hk_load_species_file(hk_ctx *c, const char *path, const char *species, double numin,
+                               double numax, int cutMode, double cut) {
+  if (!c || !species) return HK_ERR_ARG;
+  SpeciesInfo sp;
+  std::string msg;
+  int rc = read_species_param(path ? path : "", species, sp, msg);
+  if (rc != 0) return fail(c, rc, "%s", msg.c_str());
+  std::vector<double> mass, ab;
+  for (auto &iso : sp.iso) {
+    mass.push_back(iso.mass);
+    ab.push_back(iso.ab);
+  }
+  hk_status st = hk_set_species(c, sp.database, (int)mass.size(), mass.data(), ab.data(),
+                                sp.defaultL, sp.defaultn);
+  if (st != HK_OK) return st;
+  for (size_t j = 0; j < sp.iso.size(); ++j) {
+    std::vector<double> T, Q;
+    rc = read_q_file(sp.iso[j].qfile, sp.npfcol, T, Q, msg);
+    if (rc != 0) return fail(c, rc, "%s", msg.c_str());
+    if ((st = hk_set_partition(c, (int)j, (int)T.size(), T.data(), Q.data())) != HK_OK) return st;
+  }
+  LineColumns cols;
+  rc = read_line_files(sp, numin, numax, cutMode, cut, cols, msg);
+  if (rc != 0) return fail(c, rc, "%s", msg.c_str());
+  const int64_t n = (int64_t)cols.nu.size();
+  if (sp.database == HK_DB_HITRAN)
+    return hk_load_lines_hitran(c, n, cols.nu.data(), cols.S.data(), cols.EL.data(), cols.A.data(),
+                                cols.delta.data(), cols.gair.data(), cols.gself.data(),
+                                cols.nexp.data(), cols.iso.data());
+  return hk_load_lines_exomol(c, n, cols.nu.data(), cols.S.data(), cols.EL.data(), cols.A.data());
+}
+
+}  // extern "C"

@@ -1,0 +1,321 @@
+// hkb_device.cuh -- device-side math of the opacity path (sm_100a).
+//
+// Line scaling to a (T, P) state, the exact FP64 index-window rule, and the
+// piecewise Voigt profile in FP64 (plain form) and FP32 (mixed form).
+// Reference citations are file:line in the HELIOS-K source tree.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "hkb_types.h"
+
+namespace hkb {
+
+// ----------------------------------------------------------------- grid
+// voigt.h:751-768 (setX_kernel): x_d[id] = numin + id * dnu, contracted to
+// one FMA by nvcc; reproduced exactly with __fma_rn.
+__device__ __forceinline__ double grid_x(const GridDev &g, int64_t i) {
+  return __fma_rn((double)i, g.dnu, g.numin);
+}
+
+// ------------------------------------------------------------ line prep
+struct LineState {
+  double nu;   // line centre after the pressure shift
+  double S;    // integrated strength scaled to (T, P), times 1/alphaD
+  double iad;  // 1 / alphaD
+  double vy;   // gammaL / alphaD
+};
+
+// HITRAN: host.h:598-649 (readFile) + voigt.h:331-363 (S2_kernel).
+// ExoMol: voigt.h:484-504 (L_kernelExomol) + voigt.h:365-397 (Sf_kernel).
+// The state-independent parts (combined width gam, A/(4 pi c)) were formed
+// on the host at load time with the reference's expressions.
+__device__ __forceinline__ LineState prep_line(const LinesDev &L,
+                                               const StateDev &st,
+                                               int64_t l) {
+  LineState o;
+  const int j = L.iso ? (int)L.iso[l] : 0;
+  const double nu0 = L.nu0[l];
+  const double Sf = L.Sfile[l];
+  const double el = L.EL ? L.EL[l] : L.EL_c;
+  const double gam = L.gam ? L.gam[l] : L.gam_c;
+  const double ne = L.nexp ? L.nexp[l] : L.nexp_c;
+  const double At = L.Aterm ? L.Aterm[l] : L.Aterm_c;
+  double nu, S, iad;
+  if (L.database == HK_DB_HITRAN) {
+    const double de = L.delta ? L.delta[l] : L.delta_c;
+    const double c = HK_H * HK_C / HK_KB;
+    nu = __fma_rn(de, st.P, nu0);
+    iad = __ddiv_rn(st.iad0[j], nu);
+    S = __dmul_rn(__dmul_rn(__ddiv_rn(Sf, st.Q[j]), st.ab[j]), st.ss[j]);
+    const double earg = __dadd_rn(__ddiv_rn(__dmul_rn(-el, c), st.T),
+                                  __ddiv_rn(__dmul_rn(el, c), HK_T0));
+    const double e1 = exp(__ddiv_rn(__dmul_rn(-c, nu), st.T));
+    const double e0 = exp(__ddiv_rn(__dmul_rn(-c, nu), HK_T0));
+    const double f = __dmul_rn(
+        __ddiv_rn(__dmul_rn(exp(earg), __dsub_rn(1.0, e1)), __dsub_rn(1.0, e0)),
+        iad);
+    S = __dmul_rn(S, f);
+  } else {
+    // ExoMol: no pressure shift; S = S_file * Ab * Sscale / Q first
+    nu = nu0;
+    iad = __ddiv_rn(st.iad0[j], nu);
+    S = __ddiv_rn(__dmul_rn(__dmul_rn(Sf, st.ab[j]), st.ss[j]), st.Q[j]);
+    const double e1 = exp(__dmul_rn(-st.c1, el));
+    const double e2 = exp(__dmul_rn(-st.c1, nu));
+    S = __dmul_rn(S, __dmul_rn(__dmul_rn(e1, __dsub_rn(1.0, e2)), iad));
+  }
+  double aL = __dmul_rn(gam, __dmul_rn(st.PoverP0, pow(st.powbase, ne)));
+  aL = __dadd_rn(aL, At);
+  double vy = __dmul_rn(aL, iad);
+  if (nu == 0.0) {
+    S = 0.0;
+    iad = 0.0;
+    vy = 0.0;
+  }
+  o.nu = nu;
+  o.S = S;
+  o.iad = iad;
+  o.vy = vy;
+  return o;
+}
+
+// -------------------------------------------------------- index windows
+// The region classes of nuLimits_kernel (voigt.h:2205-2341) and the
+// per-pair tests of Line6fA/B/C (voigt.h:1223, 1481, 1662), as exact FP64
+// index ranges (same predicates as the oracle, evaluated with explicit
+// IEEE-rounded intrinsics so no FMA contraction changes a bit):
+//   cut window [i0, i1): |x_i - nu| < w ;  B or C [b0, b1): r2 < 1e6 ;
+//   C [c0, c1): r2 < 100 ;  r2 = (dnu_i * iad)^2 + vy^2.
+struct WinCtx {
+  double numin, dnu, nu, iad, vy2, w;
+};
+
+enum { HK_P_LEFT_CUT = 0, HK_P_RIGHT_CUT, HK_P_CENTER, HK_P_LEFT_R, HK_P_RIGHT_R };
+
+__device__ __forceinline__ double win_d(const WinCtx &c, int64_t i) {
+  return __dsub_rn(__fma_rn((double)i, c.dnu, c.numin), c.nu);
+}
+
+__device__ __forceinline__ bool win_pred(const WinCtx &c, int kind, int64_t i,
+                                         double R) {
+  const double d = win_d(c, i);
+  switch (kind) {
+  case HK_P_LEFT_CUT: return d > -c.w;
+  case HK_P_RIGHT_CUT: return d >= c.w;
+  case HK_P_CENTER: return d >= 0.0;
+  default: {
+    const double x = __dmul_rn(d, c.iad);
+    const double r2 = __dadd_rn(__dmul_rn(x, x), c.vy2);
+    return (kind == HK_P_LEFT_R) ? (r2 < R) : (r2 >= R);
+  }
+  }
+}
+
+// First index in [lo, hi) where the monotone predicate holds (hi if none).
+// The answer does not depend on the estimate e (galloping + bisection).
+static __device__ __noinline__ int64_t first_true(const WinCtx &c, int kind, double R,
+                                           int64_t lo, int64_t hi, int64_t e) {
+  if (lo >= hi) return lo;
+  if (e < lo) e = lo;
+  if (e > hi) e = hi;
+  int64_t a, b;
+  if (e >= hi || win_pred(c, kind, e, R)) {
+    b = e;
+    int64_t step = 1;
+    while (true) {
+      const int64_t t = b - step;
+      if (t < lo) { a = lo; break; }
+      if (!win_pred(c, kind, t, R)) { a = t + 1; break; }
+      b = t;
+      step *= 2;
+    }
+  } else {
+    a = e + 1;
+    int64_t step = 1;
+    while (true) {
+      const int64_t t = a - 1 + step;
+      if (t >= hi) { b = hi; break; }
+      if (win_pred(c, kind, t, R)) { b = t; break; }
+      a = t + 1;
+      step *= 2;
+    }
+  }
+  while (a < b) {
+    const int64_t m = a + (b - a) / 2;
+    if (win_pred(c, kind, m, R)) b = m;
+    else a = m + 1;
+  }
+  return a;
+}
+
+__device__ __forceinline__ int64_t est_index(double edge, const GridDev &g,
+                                             int64_t hi) {
+  const double e = ceil((edge - g.numin) / g.dnu);
+  if (!(e > -1.0)) return 0;
+  if (e > (double)hi) return hi;
+  return (int64_t)e;
+}
+
+// Window boundaries of one line restricted to grid indices [g0, g1):
+// out[0..5] = i0, b0, c0, c1, b1, i1 (absolute indices, each clipped to
+// [g0, g1]).  Equals clip(oracle window) because every predicate is
+// monotone on the range it is searched over.
+__device__ __forceinline__ void line_windows(const GridDev &g, const StateDev &st,
+                                             const LineState &ls, int64_t g0,
+                                             int64_t g1, int64_t out[6]) {
+  if (ls.S == 0.0 || !(ls.iad > 0.0)) {
+    for (int k = 0; k < 6; ++k) out[k] = g0;
+    return;
+  }
+  WinCtx c;
+  c.numin = g.numin;
+  c.dnu = g.dnu;
+  c.nu = ls.nu;
+  c.iad = ls.iad;
+  c.vy2 = __dmul_rn(ls.vy, ls.vy);
+  double w;
+  if (g.cutMode == 1) w = __ddiv_rn(__dmul_rn(g.cut, ls.vy), ls.iad);
+  else if (g.cutMode == 2) w = __ddiv_rn(g.cut, ls.iad);
+  else w = g.cut;
+  c.w = w;
+  const int64_t i0 = first_true(c, HK_P_LEFT_CUT, 0.0, g0, g1, est_index(ls.nu - w, g, g1));
+  const int64_t i1 = first_true(c, HK_P_RIGHT_CUT, 0.0, i0, g1, est_index(ls.nu + w, g, g1));
+  if (i1 <= i0) {
+    for (int k = 0; k < 6; ++k) out[k] = i0;
+    return;
+  }
+  const int64_t ic = first_true(c, HK_P_CENTER, 0.0, i0, i1, est_index(ls.nu, g, g1));
+  const double Rs[2] = {1.0e6, 100.0};
+  int64_t lohi[2][2];
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const double R = Rs[r];
+    const double h2 = R - c.vy2;
+    if (h2 > 0.0) {
+      const double h = sqrt(h2) / c.iad;
+      lohi[r][0] = first_true(c, HK_P_LEFT_R, R, i0, ic, est_index(ls.nu - h, g, g1));
+      lohi[r][1] = first_true(c, HK_P_RIGHT_R, R, ic, i1, est_index(ls.nu + h, g, g1));
+    } else {
+      lohi[r][0] = ic;
+      lohi[r][1] = ic;
+    }
+  }
+  out[0] = i0;
+  out[1] = lohi[0][0];
+  out[2] = lohi[1][0];
+  out[3] = lohi[1][1];
+  out[4] = lohi[0][1];
+  out[5] = i1;
+}
+
+// -------------------------------------------------------------- profile
+// Region B rational (voigt.h:1481-1490), rewritten with u = r2, s = x^2:
+//   t4 = [(u+1.5)(u+1) - (4/pi) s] / [u ((u+1.5)^2 - (6/pi) s)]
+// which is the reference's (t3(2t2+r2) - 2t1) / (3 r2 (t3 t2 - t1)) with
+// numerator and denominator divided by 3 pi.
+__device__ __forceinline__ double gh2_d(double x, double y2) {
+  const double s = x * x;
+  const double u = s + y2;
+  const double a1 = u + 1.5;
+  const double num = a1 * (u + 1.0) - (4.0 / CUDART_PI) * s;
+  const double den = u * (a1 * a1 - (6.0 / CUDART_PI) * s);
+  return num / den;
+}
+
+// Zaghloul & Ali, Algorithm 916 in FP64: restates voigt.h:165-216 (Sigmab)
+// and voigt.h:278-300 (voigt_916) with def_TOL; ey = erfcx(y) per line.
+static __device__ __noinline__ double voigt916_d(double x, double y, double ey) {
+  const double a = HK_A916_D;
+  double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  const double ax = fabs(x);
+  const double ex2 = exp(-ax * ax);
+  if (ax != 0.0 && y != 0.0) {
+    double o1 = 0.0, o2 = 0.0, o3 = 0.0;
+    const double yy = y * y;
+    const int n0 = (int)ceil(ax / a);
+    bool st1 = false, st2 = false, st3 = false;
+    for (int n = 1; n < 100; ++n) {
+      const int n3p = n0 + n - 1, n3n = n0 - n;
+      const double an = a * n, an3p = a * n3p, an3n = a * n3n;
+      const double f = 1.0 / (an * an + yy);
+      const double f3p = 1.0 / (an3p * an3p + yy);
+      const double f3n = 1.0 / (an3n * an3n + yy);
+      s1 += f * exp(-(an * an + ax * ax));
+      s2 += f * exp(-(an + ax) * (an + ax));
+      s3 += f3p * exp(-(an3p - ax) * (an3p - ax));
+      if (n3n >= 1) s3 += f3n * exp(-(an3n - ax) * (an3n - ax));
+      if (fabs(s1 - o1) < HK_TOL) st1 = true;
+      if (fabs(s2 - o2) < HK_TOL) st2 = true;
+      if (fabs(s3 - o3) < HK_TOL) st3 = true;
+      if (st1 && st2 && st3) break;
+      o1 = s1;
+      o2 = s2;
+      o3 = s3;
+    }
+  }
+  const double xy = ax * y;
+  const double cos2xy = cos(2.0 * xy);
+  const double sinxy = sin(xy);
+  double t1 = ex2 * ey * cos2xy;
+  if (ax != 0.0 && y != 0.0) {
+    const double a2ipi = 2.0 * a / CUDART_PI;
+    t1 += a2ipi * sinxy * ex2 * sinxy / y;
+    t1 += a2ipi * y * (-cos2xy * s1 + 0.5 * (s2 + s3));
+  }
+  if (ax == 0.0) t1 = ey;
+  if (y == 0.0) t1 = ex2;
+  return t1;
+}
+
+// Algorithm 916 in FP32 with def_TOLF (the series of voigt.h:217-268,
+// Sigmabf, and the region-C formula of voigt.h:1662-1682).  Differences
+// from the reference's FP32 kernel: the argument x arrives with FP32
+// relative accuracy (the offset is formed from a double-float split, not
+// from (numin - nu)/alphaD rounded to float), and erfcx(y) is a per-line
+// constant computed in FP64.
+static __device__ __noinline__ float voigt916_f(float x, float y, float ey) {
+  const float a = HK_A916_F;
+  const float cc = HK_C916_F;  // 2a/pi
+  float s1 = 0.f, s2 = 0.f, s3 = 0.f;
+  x = fabsf(x);
+  const float ex2 = expf(-x * x);
+  if (x != 0.f && y != 0.f) {
+    float o1 = 0.f, o2 = 0.f, o3 = 0.f;
+    const float yy = y * y;
+    const int n0 = (int)ceilf(x / a);
+    bool st1 = false, st2 = false, st3 = false;
+    for (int n = 1; n < 100; ++n) {
+      const int n3p = n0 + n - 1, n3n = n0 - n;
+      const float an = a * n, an3p = a * n3p, an3n = a * n3n;
+      const float f = 1.0f / (an * an + yy);
+      const float f3p = 1.0f / (an3p * an3p + yy);
+      const float f3n = 1.0f / (an3n * an3n + yy);
+      s1 += f * expf(-(an * an + x * x));
+      s2 += f * expf(-(an + x) * (an + x));
+      s3 += f3p * expf(-(an3p - x) * (an3p - x));
+      if (n3n >= 1) s3 += f3n * expf(-(an3n - x) * (an3n - x));
+      if (fabsf(s1 - o1) < HK_TOLF) st1 = true;
+      if (fabsf(s2 - o2) < HK_TOLF) st2 = true;
+      if (fabsf(s3 - o3) < HK_TOLF) st3 = true;
+      if (st1 && st2 && st3) break;
+      o1 = s1;
+      o2 = s2;
+      o3 = s3;
+    }
+  }
+  const float xy = x * y;
+  const float cos2xy = cosf(2.0f * xy);
+  const float sinxy = sinf(xy);
+  float t1 = ex2 * ey * cos2xy;
+  const float t2 = sinxy * ex2 * sinxy / y;
+  const float t3 = y * (-cos2xy * s1 + 0.5f * (s2 + s3));
+  t1 += cc * (t2 + t3);
+  if (x == 0.f) t1 = ey;
+  if (y == 0.f) t1 = ex2;
+  return t1;
+}
+
+}  // namespace hkb

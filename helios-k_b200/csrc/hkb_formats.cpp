@@ -1,0 +1,388 @@
+// hkb_formats.cpp -- readers for the reference's input files (host C++).
+// Compiled with -ffp-contract=off: the partition interpolation must be the
+// same IEEE sequence as the reference's host code.
+#include "hkb_formats.h"
+
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+#include "hkb.h"
+
+namespace hkb {
+
+// host.h:9-73 (readPartition): walk the (T, Q) table, stop at the first row
+// with T1 >= T, interpolate linearly from the previous row.  Returns 1 on
+// success, 0 on the reference's error conditions.
+int partition_interp(const double *Tq, const double *q, int n, double T, double *out) {
+  double T0, T1 = -1.0, q0, q1 = 1.0;
+  for (int j = 0; j < 100000; ++j) {
+    T0 = T1;
+    q0 = q1;
+    if (j >= n) return 0;
+    T1 = Tq[j];
+    q1 = q[j];
+    if (T0 == T1 && T0 < T && j > 0) return 0;
+    if (T1 > T && j == 0) return 0;
+    if (T0 < T && T1 >= T) {
+      double tt = (T - T0) / (T1 - T0);
+      double qv = (q1 - q0) * tt + q0;
+      if (j == 0) qv = q1;
+      *out = qv;
+      return 1;
+    }
+  }
+  return 0;
+}
+
+int read_q_file(const std::string &fname, int ncol, std::vector<double> &T,
+                std::vector<double> &Q, std::string &msg) {
+  FILE *f = fopen(fname.c_str(), "r");
+  if (!f) {
+    msg = "Error: partition file not found " + fname;
+    return HK_ERR_IO;
+  }
+  if (ncol != 2 && ncol != 3) {
+    fclose(f);
+    msg = "Error: partition file not specified";
+    return HK_ERR_FORMAT;
+  }
+  T.clear();
+  Q.clear();
+  double a, b, skip;
+  while (true) {
+    if (fscanf(f, "%lf", &a) != 1) break;
+    if (fscanf(f, "%lf", &b) != 1) break;
+    if (ncol == 3 && fscanf(f, "%lf", &skip) != 1) break;
+    T.push_back(a);
+    Q.push_back(b);
+  }
+  fclose(f);
+  if (T.empty()) {
+    msg = "Error: partition function can not be read: " + fname;
+    return HK_ERR_FORMAT;
+  }
+  return 0;
+}
+
+// read one "<key> = value" line; returns false if the key does not match
+static bool key_line(std::istream &in, const char *key, std::string &rest) {
+  std::string line;
+  while (std::getline(in, line)) {
+    if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
+    break;
+  }
+  size_t k = line.find(key);
+  if (k != 0) return false;
+  rest = line.substr(strlen(key));
+  return true;
+}
+
+// ISO.h:16-219 (Init)
+int read_species_param(const std::string &path, const std::string &species,
+                       SpeciesInfo &sp, std::string &msg) {
+  const std::string fname = path + species + ".param";
+  std::ifstream in(fname);
+  if (!in) {
+    msg = "Error, no molecule.param file " + fname;
+    return HK_ERR_IO;
+  }
+  std::string rest;
+  auto bad = [&](const char *what) {
+    msg = std::string("Error in molecule.param file, ") + what + " (" + fname + ")";
+    return HK_ERR_FORMAT;
+  };
+  if (!key_line(in, "Database =", rest)) return bad("Database");
+  sp.database = atoi(rest.c_str());
+  if (!key_line(in, "Molecule number =", rest)) return bad("Molecule number");
+  sp.id = atoi(rest.c_str());
+  if (!key_line(in, "Name =", rest)) return bad("Name");
+  {
+    std::istringstream ss(rest);
+    ss >> sp.name;
+  }
+  std::string line;
+  std::getline(in, line);
+  size_t eq = line.find('=');
+  if (eq == std::string::npos) return bad("Number of Isotopes");
+  std::string k = line.substr(0, eq);
+  if (k != "Number of Isotopes " && k != "Number of Isotopologues ") return bad("Number of Isotopes");
+  int niso = atoi(line.c_str() + eq + 1);
+  if (niso < 1 || niso > 16) return bad("Number of Isotopes (1..16)");
+  std::getline(in, line);  // header
+  sp.iso.clear();
+  for (int i = 0; i < niso; ++i) {
+    IsoInfo iso;
+    std::string cid, qf;
+    if (!(in >> cid >> iso.ab >> iso.Q296 >> iso.g >> iso.mass >> qf)) return bad("isotopologue row");
+    char buf[16];
+    snprintf(buf, sizeof buf, "%3s", cid.c_str());
+    iso.cid = std::string(buf).substr(0, 3);
+    iso.qfile = path + qf;
+    sp.iso.push_back(iso);
+  }
+  std::getline(in, line);  // rest of the last row
+  if (!key_line(in, "Number of columns in partition File =", rest)) return bad("Number of columns in partition File");
+  sp.npfcol = atoi(rest.c_str());
+  if (!key_line(in, "Number of line/transition files =", rest)) return bad("Number of line/transition files");
+  sp.nFiles = atoi(rest.c_str());
+  if (sp.nFiles < 0 || sp.nFiles > 500) return bad("Number of line/transition files (0..500)");
+  std::getline(in, line);  // "Number of lines per file :"
+  sp.NL.assign(sp.nFiles, 0);
+  for (int i = 0; i < sp.nFiles; ++i)
+    if (!(in >> sp.NL[i])) return bad("Number of lines per file");
+  std::getline(in, line);
+  std::getline(in, line);  // "Line file limits :"
+  sp.fileLimit.assign(sp.nFiles + 1, 0);
+  for (int i = 0; i < sp.nFiles + 1; ++i)
+    if (!(in >> sp.fileLimit[i])) return bad("Line file limits");
+  std::getline(in, line);
+  char buf[1024];
+  sp.dataFilename.assign(sp.nFiles, "");
+  for (int i = 0; i < sp.nFiles; ++i) {
+    const char *p = path.c_str();
+    const char *n = sp.name.c_str();
+    if (sp.database == 0 || sp.database == 1) {
+      if (sp.nFiles > 1) snprintf(buf, sizeof buf, "%s%s_%05d-%05d.", p, n, sp.fileLimit[i], sp.fileLimit[i + 1]);
+      else snprintf(buf, sizeof buf, "%s%s.", p, n);
+    } else if (sp.database == 2) {
+      if (sp.nFiles > 1) snprintf(buf, sizeof buf, "%s%s__%05d-%05d.", p, n, sp.fileLimit[i], sp.fileLimit[i + 1]);
+      else snprintf(buf, sizeof buf, "%s%s.", p, n);
+    } else {
+      msg = "Error: database " + std::to_string(sp.database) +
+            " (superlines, Kurucz, NIST, VALD, CDSD) is outside this build's path";
+      return HK_ERR_UNSUPPORTED;
+    }
+    sp.dataFilename[i] = buf;
+  }
+  std::getline(in, line);  // "#ExoMol :"
+  if (!key_line(in, "Number of states =", rest)) return bad("Number of states");
+  sp.nStates = atoi(rest.c_str());
+  if (!key_line(in, "Number of columns in transition files =", rest)) return bad("Number of columns in transition files");
+  sp.ntcol = atoi(rest.c_str());
+  if (!key_line(in, "Default value of Lorentzian half-width for all lines =", rest)) return bad("Default value of Lorentzian half-width for all lines");
+  sp.defaultL = atof(rest.c_str());
+  if (!key_line(in, "Default value of temperature exponent for all lines =", rest)) return bad("Default value of temperature exponent for all lines");
+  sp.defaultn = atof(rest.c_str());
+  if (!key_line(in, "Version =", rest)) return bad("Version");
+  sp.version = atoi(rest.c_str());
+  if (sp.database == 1) sp.database = 0;  // HITEMP uses the HITRAN record
+  return 0;
+}
+
+// heliosk.cu:943-956 file pruning, then the records of host.h:607-615
+// (HITRAN) or prepareExomol.cpp:222-225 (ExoMol).
+int read_line_files(const SpeciesInfo &sp, double numin, double numax, int cutMode,
+                    double cut, LineColumns &cols, std::string &msg) {
+  if (cut == 0.0) cut = 1.0e30;
+  int fi0 = sp.nFiles, fi1 = 0;
+  if (cutMode == 0) {
+    for (int fi = 0; fi < sp.nFiles; ++fi) {
+      if (sp.fileLimit[fi] - cut <= numax) fi1 = fi + 1;
+      else break;
+    }
+    for (int fi = sp.nFiles - 1; fi >= 0; --fi) {
+      if (sp.fileLimit[fi + 1] + cut >= numin) fi0 = fi;
+      else break;
+    }
+  } else {
+    fi0 = 0;
+    fi1 = sp.nFiles;
+  }
+  cols = LineColumns{};
+  for (int fi = fi0; fi < fi1; ++fi) {
+    const std::string fname = sp.dataFilename[fi] + "bin";
+    FILE *f = fopen(fname.c_str(), "rb");
+    if (!f) {
+      msg = "Error: line list file not found: " + fname;
+      return HK_ERR_IO;
+    }
+    const long long nl = sp.NL[fi];
+    const size_t rec = (sp.database == 0) ? 68 : 32;
+    std::vector<unsigned char> buf((size_t)nl * rec);
+    size_t got = nl ? fread(buf.data(), rec, (size_t)nl, f) : 0;
+    fclose(f);
+    if ((long long)got != nl) {
+      msg = "Error: line list file " + fname + " is truncated (" + std::to_string(got) +
+            " of " + std::to_string(nl) + " records)";
+      return HK_ERR_FORMAT;
+    }
+    const size_t base = cols.nu.size();
+    for (auto *v : {&cols.nu, &cols.S, &cols.EL, &cols.A, &cols.delta, &cols.gair, &cols.gself, &cols.nexp})
+      v->resize(base + nl);
+    cols.iso.resize(base + nl);
+    for (long long i = 0; i < nl; ++i) {
+      const unsigned char *r = buf.data() + (size_t)i * rec;
+      double v[8];
+      if (sp.database == 0) {
+        char cid[4];
+        memcpy(cid, r, 4);
+        memcpy(v, r + 4, 64);
+        int j = -1;
+        for (size_t k = 0; k < sp.iso.size(); ++k)
+          if (strncmp(cid, sp.iso[k].cid.c_str(), 4) == 0) j = (int)k;
+        if (j < 0) {
+          char b[160];
+          snprintf(b, sizeof b, "Error: partition function not found. %lld |%.3s|%s|", i, cid, sp.iso[0].cid.c_str());
+          msg = b;
+          return HK_ERR_FORMAT;
+        }
+        cols.nu[base + i] = v[0];
+        cols.S[base + i] = v[1];
+        cols.EL[base + i] = v[2];
+        cols.A[base + i] = v[3];
+        cols.delta[base + i] = v[4];
+        cols.gair[base + i] = v[5];
+        cols.gself[base + i] = v[6];
+        cols.nexp[base + i] = v[7];
+        cols.iso[base + i] = j;
+      } else {
+        memcpy(v, r, 32);
+        cols.nu[base + i] = v[0];
+        cols.S[base + i] = v[1];
+        cols.EL[base + i] = v[2];
+        cols.A[base + i] = v[3];
+        cols.delta[base + i] = 0.0;
+        cols.gair[base + i] = 0.0;
+        cols.gself[base + i] = 0.0;
+        cols.nexp[base + i] = sp.defaultn;
+        cols.iso[base + i] = 0;
+      }
+    }
+  }
+  return 0;
+}
+
+// host.h:75-525 (read_parameters): "key = value" lines, an unknown key is an
+// error; then "-flag value" command-line overrides.
+int read_param_file(const std::string &fname, int argc, char **argv, Params &p,
+                    std::string &msg) {
+  FILE *f = fopen(fname.c_str(), "r");
+  if (!f) {
+    msg = "Error: parameter file not found: " + fname;
+    return HK_ERR_IO;
+  }
+  char line[1024];
+  int lineno = 0;
+  while (fgets(line, sizeof line, f)) {
+    std::string s(line);
+    if (s.find_first_not_of(" \t\r\n") == std::string::npos) continue;
+    size_t e = s.find_first_of("=:");
+    if (e == std::string::npos) {
+      msg = "Undefined line in param.dat file: line " + std::to_string(lineno);
+      fclose(f);
+      return HK_ERR_FORMAT;
+    }
+    std::string key = s.substr(0, e);
+    while (!key.empty() && (key.back() == ' ' || key.back() == '\t')) key.pop_back();
+    std::string val = s.substr(e + 1);
+    std::istringstream vs(val);
+    std::string tok;
+    vs >> tok;
+    auto D = [&](double &d) { d = atof(tok.c_str()); };
+    auto I = [&](int &i) { i = atoi(tok.c_str()); };
+    if (key == "name") p.name = tok;
+    else if (key == "T") D(p.T);
+    else if (key == "P") D(p.P);
+    else if (key == "PFile") p.PFilename = tok;
+    else if (key == "Species Name") p.speciesName = tok;
+    else if (key == "SpeciesFile") p.SpeciesFilename = tok;
+    else if (key == "ciaSystem") p.ciaSystem = tok;
+    else if (key == "pathToData") p.path = tok;
+    else if (key == "numin") D(p.numin);
+    else if (key == "numax") D(p.numax);
+    else if (key == "dnu") D(p.dnu);
+    else if (key == "Nnu per bin") I(p.Nxb);
+    else if (key == "cutMode") I(p.cutMode);
+    else if (key == "cut") D(p.cut);
+    else if (key == "doResampling") I(p.doResampling);
+    else if (key == "nC") { I(p.nC); if (p.nC > 100) p.nC = 100; }
+    else if (key == "doTransmission") I(p.doTransmission);
+    else if (key == "nTr") I(p.nTr);
+    else if (key == "dTr") D(p.dTr);
+    else if (key == "doStoreFullK") I(p.doStoreFullK);
+    else if (key == "pathToK") p.pathK = tok;
+    else if (key == "doStoreSK") I(p.doStoreK);
+    else if (key == "nbins") I(p.nbins);
+    else if (key == "binsFile") p.bins = tok;
+    else if (key == "OutputEdgesFile") p.edges = tok;
+    else if (key == "kmin") D(p.kmin);
+    else if (key == "qalphaL") D(p.qalphaL);
+    else if (key == "gammaF") D(p.gammaF);
+    else if (key == "doMean") I(p.doMean);
+    else if (key == "Units") I(p.units);
+    else if (key == "ReplaceFiles") I(p.replaceFiles);
+    else if (key == "RLOW") { /* not used anymore, host.h:266-271 */ }
+    else if (key == "profile") I(p.profile);
+    else if (key == "doTuning") I(p.doTuning);
+    else if (key == "removePlinth") I(p.removePlinth);
+    else if (key == "subLorentzianfile") p.subLorentzian = tok;
+    else {
+      msg = "Undefined line in param.dat file: line " + std::to_string(lineno) + " (" + key + ")";
+      fclose(f);
+      return HK_ERR_FORMAT;
+    }
+    ++lineno;
+  }
+  fclose(f);
+  // "pathToK =" with an empty value leaves pathK empty (tok == "")
+  for (int i = 1; i < argc; i += 2) {
+    if (i + 1 >= argc) {
+      msg = "Error: Console arguments not valid!";
+      return HK_ERR_ARG;
+    }
+    std::string a = argv[i];
+    const char *v = argv[i + 1];
+    if (a == "-name") p.name = v;
+    else if (a == "-T") p.T = atof(v);
+    else if (a == "-P") p.P = atof(v);
+    else if (a == "-M") p.speciesName = v;
+    else if (a == "-path") p.path = v;
+    else if (a == "-pathK") p.pathK = v;
+    else if (a == "-numin") p.numin = atof(v);
+    else if (a == "-numax") p.numax = atof(v);
+    else if (a == "-dnu") p.dnu = atof(v);
+    else if (a == "-cutM") p.cutMode = atoi(v);
+    else if (a == "-cut") p.cut = atof(v);
+    else if (a == "-dR") p.doResampling = atoi(v);
+    else if (a == "-nC") p.nC = atoi(v);
+    else if (a == "-dT") p.doTransmission = atoi(v);
+    else if (a == "-nTr") p.nTr = atoi(v);
+    else if (a == "-dTr") p.dTr = atof(v);
+    else if (a == "-dSF") p.doStoreFullK = atoi(v);
+    else if (a == "-dSS") p.doStoreK = atoi(v);
+    else if (a == "-nbins") p.nbins = atoi(v);
+    else if (a == "-kmin") p.kmin = atof(v);
+    else if (a == "-q") p.qalphaL = atof(v);
+    else if (a == "-gammaF") p.gammaF = atof(v);
+    else if (a == "-dev") p.dev = atoi(v);
+    else if (a == "-Mean") p.doMean = atoi(v);
+    else if (a == "-tuning") p.doTuning = atoi(v);
+    else {
+      msg = "Error: Console arguments not valid!";
+      return HK_ERR_ARG;
+    }
+  }
+  if (p.PFilename != "-") {
+    FILE *pf = fopen(p.PFilename.c_str(), "r");
+    if (!pf) {
+      msg = "Error: Pressure file not found: " + p.PFilename;
+      return HK_ERR_IO;
+    }
+    double b;
+    p.Plist.clear();
+    while (fscanf(pf, "%lf", &b) == 1) p.Plist.push_back(b);
+    fclose(pf);
+    p.nP = (int)p.Plist.size();
+  } else {
+    p.Plist.assign(1, p.P);
+    p.nP = 1;
+  }
+  return 0;
+}
+
+}  // namespace hkb

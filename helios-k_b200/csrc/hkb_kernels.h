@@ -1,0 +1,57 @@
+// hkb_kernels.h -- host-side launchers of the sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "hkb_types.h"
+
+namespace hkb {
+
+// dynamic shared memory budget of one kdist CTA (sm_100: 227 KB per block,
+// minus the kernel's static shared arrays)
+constexpr int KD_SMEM_LIMIT = 225 * 1024;
+
+int voigt_tile_points();
+cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream);
+
+cudaError_t launch_state_prepass(const LinesDev &L, const GridDev &g,
+                                 StateDev *states_d, int nstates,
+                                 int *maxexp_d, unsigned long long *wbits_d,
+                                 cudaStream_t stream);
+
+cudaError_t launch_voigt_sum(bool mixed, const LinesDev &L, const GridDev &g,
+                             const StateDev *states_d, int nstates,
+                             unsigned *ticket_d, double *K_d, int64_t k_stride,
+                             int grid_ctas, cudaStream_t stream);
+
+cudaError_t launch_prep_dump(const LinesDev &L, const GridDev &g,
+                             const StateDev &st, double *out4_d,
+                             long long *win6_d, cudaStream_t stream);
+
+cudaError_t launch_profile_eval(int64_t n, const double *x_d, const double *y_d,
+                                int mixed, double *out_d, cudaStream_t stream);
+
+size_t kdist_smem_bytes(int nxb);
+size_t kdist_scratch_doubles(int nxb, int nbins, int nstates);
+
+cudaError_t launch_qr(int nxb, int nc, double *V_d, double *C_d, double *D_d,
+                      cudaStream_t stream);
+
+cudaError_t launch_kdist(const double *K_d, int64_t k_stride, int nstates,
+                         int nxb, int nbins, int nc, double kmin,
+                         double unitScale, const double *V_d, const double *C_d,
+                         const double *D_d, double *coeff_d, int *nxmin_d,
+                         double *sorted_d, double *recon_d, double *scratch_d,
+                         cudaStream_t stream);
+
+cudaError_t launch_gather_lines(int64_t n, const int64_t *order_d,
+                                const double *src_d, double *dst_d,
+                                cudaStream_t stream);
+
+cudaError_t sort_lines_by_nu(int64_t n, double *nu_d, int64_t *order_d,
+                             cudaStream_t stream);
+
+}  // namespace hkb

@@ -1,0 +1,68 @@
+// hkb_types.h -- plain-data types shared by the host runtime and kernels.
+#pragma once
+
+#include <cstdint>
+
+namespace hkb {
+
+// physical constants, define.h:36-45
+constexpr double HK_T0 = 296.0;
+constexpr double HK_PO_BAR = 0.986923;
+constexpr double HK_PO_ATM = 1.0;
+constexpr double HK_KB = 1.3806489e-16;
+constexpr double HK_H = 6.62606957e-27;
+constexpr double HK_C = 2.99792458e10;
+constexpr double HK_NA = 6.0221412927e23;
+// Voigt series tolerances, define.h:47-48
+constexpr double HK_TOL = 1.43e-17;
+constexpr float HK_TOLF = 2.48e-12f;
+// Algorithm 916 step a = pi * sqrt(-1 / ln(TOL / 2)) (voigt.h:601, and
+// heliosk.cu:1656-1658 for the FP32 constants a and c = 2a/pi)
+constexpr double HK_A916_D = 0.4999936567001175;
+constexpr float HK_A916_F = 0.5999962687492371f;
+constexpr float HK_C916_F = 0.38196948170661926f;
+
+constexpr int HK_DB_HITRAN = 0;
+constexpr int HK_DB_EXOMOL = 2;
+constexpr int HK_MAX_ISO = 16;
+
+// Sorted line list resident in HBM (SoA, FP64).  A null array means the
+// column is uniform and its *_c scalar is used instead.
+struct LinesDev {
+  int64_t n;
+  int database;
+  const double *nu0;    // line centre, ascending
+  const double *Sfile;  // strength as stored in the line file
+  const double *EL;     // lower-state energy
+  const double *gam;    // ((1-q) gamma_air + q gamma_self) * gammaF  (host.h:640-641)
+  const double *nexp;   // temperature exponent
+  const double *delta;  // pressure shift (HITRAN)
+  const double *Aterm;  // A / (4 pi c)
+  const uint8_t *iso;   // isotopologue index (null: 0)
+  double EL_c, gam_c, nexp_c, delta_c, Aterm_c;
+};
+
+struct GridDev {
+  double numin, dnu;
+  int64_t nx;
+  int cutMode;
+  double cut;  // 1e30 when the parameter file says 0 (heliosk.cu:947)
+};
+
+// Per-(T, P) constants formed on the host.
+struct StateDev {
+  double T, P;
+  double PoverP0;  // P / 1 atm (HITRAN) or P / 1 bar in atm (ExoMol)
+  double powbase;  // T0 / T
+  double c1;       // h c / (kB T)   (ExoMol strength)
+  double scale, inv_scale;  // power of two applied to FP32 strengths
+  double wmax;     // upper bound of the cutoff half-width over lines (cm^-1)
+  double shift;    // upper bound of |delta| * P
+  double kmin;
+  double iad0[HK_MAX_ISO];  // c sqrt(m / (2 kB T))
+  double Q[HK_MAX_ISO];     // partition function at T
+  double ab[HK_MAX_ISO];    // abundance * (m / meanMass) when units == 0
+  double ss[HK_MAX_ISO];    // species scale * (m / meanMass) when units == 0
+};
+
+}  // namespace hkb

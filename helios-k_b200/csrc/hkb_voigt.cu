@@ -1,0 +1,427 @@
+// hkb_voigt.cu -- the Voigt line sum onto the wavenumber grid (sm_100a).
+//
+// One persistent kernel walks (state, grid tile) tickets.  A CTA owns a tile
+// of HK_G consecutive grid points, so every output point has exactly one
+// writer: there are no atomics on K and no partial-row reduction (the
+// reference's 32 KS_d rows + AddKStreams_kernel, voigt.h:728-742, are gone).
+// For its tile the CTA
+//   1. finds the ν-sorted line range whose cutoff windows can reach the tile
+//      (warp-parallel lower_bound),
+//   2. stages the lines in chunks of HK_CH through shared memory: each thread
+//      scales one line to the state in FP64 (prep_line) and computes the
+//      exact window/region index boundaries clipped to the tile,
+//   3. lets each warp sweep its 256-point slice against every staged line:
+//      lane-interleaved points (coalesced stores), register accumulators.
+// Two precisions share the structure:
+//   MIXED: FP32 profile + Kahan-compensated FP32 sums; the offset x is formed
+//          from a double-float split of the FP64 line-centre offset.
+//   PLAIN: FP64 everywhere (the "plain FP64 form" used as the GPU baseline).
+// Reference: Line6fA/B/C kernels voigt.h:1177-1816 and their launchers
+// Line6A_Call/Line6B_Call/Line6C_Call voigt.h:1820-2036.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "hkb_device.cuh"
+#include "hkb_kernels.h"
+
+namespace hkb {
+
+constexpr int HK_WARPS = 8;
+constexpr int HK_THREADS = HK_WARPS * 32;
+constexpr int HK_PPL = 8;                    // points per lane
+constexpr int HK_SLICE = 32 * HK_PPL;        // points per warp
+constexpr int HK_G = HK_WARPS * HK_SLICE;    // points per tile (2048)
+constexpr int HK_CH = HK_THREADS;            // lines per staged chunk
+static_assert(HK_G <= 2048, "k * vb_hi must stay exact in FP32 (11 bits)");
+
+struct __align__(16) RecF {
+  float dh, dl, vbh, vbl;  // x at the tile start (hi, lo), x step (hi, lo)
+  double S1, Sc;           // S*y/pi (regions A, B), S/sqrt(pi) (region C)
+  float y2, y, ey;         // y^2, y, erfcx(y)
+  int i0;                  // tile-local window boundaries
+  int b0, c0, c1, b1;
+  int i1, p0, p1, p2;
+};
+
+struct __align__(16) RecD {
+  double nu, iad, y2, y, S1, Sc, ey, pad;
+  int i0, b0, c0, c1, b1, i1, p0, p1;
+};
+
+__device__ __forceinline__ float rcp_approx(float v) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
+
+// Exact widening of a positive normal float to double with integer ops
+// (keeps the conversion off the XU pipe that rcp.approx already uses).
+__device__ __forceinline__ double widen_pos(float f) {
+  const unsigned u = __float_as_uint(f);
+  const unsigned lo = u << 29;
+  const unsigned hi = (u >> 3) + (896u << 20);
+  return __hiloint2double((int)hi, (int)lo);
+}
+
+// first index in [0, n) with a[idx] >= v (n if none); all 32 lanes call it
+__device__ int64_t lower_bound_warp(const double *__restrict__ a, int64_t n,
+                                    double v) {
+  const int lane = threadIdx.x & 31;
+  int64_t lo = 0, hi = n;
+  while (hi - lo > 32) {
+    const int64_t span = hi - lo;
+    const int64_t pos = lo + ((int64_t)(lane + 1) * span) / 33;
+    const bool ge = a[pos] >= v;
+    const unsigned m = __ballot_sync(0xffffffffu, ge);
+    if (m == 0u) {
+      lo = lo + (32 * span) / 33 + 1;
+    } else {
+      const int f = __ffs(m) - 1;
+      const int64_t nh = lo + ((int64_t)(f + 1) * span) / 33;
+      const int64_t nl = (f == 0) ? lo : lo + ((int64_t)f * span) / 33 + 1;
+      lo = nl;
+      hi = nh;
+    }
+  }
+  const int64_t pos = lo + lane;
+  const bool lt = (pos < hi) && (a[pos] < v);
+  const unsigned m = __ballot_sync(0xffffffffu, lt);
+  return lo + __popc(m);
+}
+
+// Scale line l to the state, compute its tile-local windows and fill the
+// staged record.  Returns nothing; an empty window is i0 == i1 == 0.
+template <bool MIXED>
+__device__ __forceinline__ void stage_line(const LinesDev &L, const GridDev &g,
+                                           const StateDev &st, int64_t l,
+                                           int64_t g0, int64_t g1, void *recp) {
+  const LineState ls = prep_line(L, st, l);
+  int64_t w[6];
+  line_windows(g, st, ls, g0, g1, w);
+  int li[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) li[k] = (int)(w[k] - g0);
+  const bool nonempty = li[5] > li[0];
+  const bool hasC = li[3] > li[2];
+  const double ey = hasC ? erfcx(ls.vy) : 1.0;
+  if (MIXED) {
+    RecF r;
+    const double D0 = __dmul_rn(__dsub_rn(grid_x(g, g0), ls.nu), ls.iad);
+    const double vb = __dmul_rn(g.dnu, ls.iad);
+    r.dh = (float)D0;
+    r.dl = (float)(D0 - (double)r.dh);
+    const float vbf = (float)vb;
+    r.vbh = __uint_as_float(__float_as_uint(vbf) & 0xFFFFF800u);  // 13 bits
+    r.vbl = (float)(vb - (double)r.vbh);
+    r.y = (float)ls.vy;
+    r.y2 = (float)(ls.vy * ls.vy);
+    r.S1 = ls.S * ls.vy / CUDART_PI;
+    r.Sc = ls.S * (1.0 / 1.7724538509055160273);
+    r.ey = (float)ey;
+    r.i0 = nonempty ? li[0] : 0;
+    r.b0 = li[1];
+    r.c0 = li[2];
+    r.c1 = li[3];
+    r.b1 = li[4];
+    r.i1 = nonempty ? li[5] : 0;
+    r.p0 = r.p1 = r.p2 = 0;
+    *reinterpret_cast<RecF *>(recp) = r;
+  } else {
+    RecD r;
+    r.nu = ls.nu;
+    r.iad = ls.iad;
+    r.y = ls.vy;
+    r.y2 = ls.vy * ls.vy;
+    r.S1 = ls.S * ls.vy / CUDART_PI;
+    r.Sc = ls.S * (1.0 / 1.7724538509055160273);
+    r.ey = ey;
+    r.pad = 0.0;
+    r.i0 = nonempty ? li[0] : 0;
+    r.b0 = li[1];
+    r.c0 = li[2];
+    r.c1 = li[3];
+    r.b1 = li[4];
+    r.i1 = nonempty ? li[5] : 0;
+    r.p0 = r.p1 = 0;
+    *reinterpret_cast<RecD *>(recp) = r;
+  }
+}
+
+// ------------------------------------------------------------ FP32 sweep
+__device__ __forceinline__ float gh2_f(float s, float u) {
+  const float a1 = u + 1.5f;
+  const float num = fmaf(-1.2732395447351628f, s, fmaf(a1, u, a1));   // 4/pi
+  const float q = fmaf(-1.9098593171027440f, s, a1 * a1);            // 6/pi
+  return num * rcp_approx(u * q);
+}
+
+// The profile shape (x, region formula) is FP32; the strength multiply and
+// the grid sum are one FP64 FMA, so one state's opacity may span the full
+// FP64 range (the strongest lines of a list can exceed the typical opacity
+// by more than the FP32 exponent range).
+__device__ __forceinline__ void sweep_mixed(const RecF &r, int wb, int lane,
+                                            const float (&kf)[HK_PPL],
+                                            double (&acc)[HK_PPL]) {
+  const int we = wb + HK_SLICE;
+  if (r.i1 <= wb || r.i0 >= we) return;
+  const bool full = r.i0 <= wb && r.i1 >= we;
+  if (full && ((r.b0 <= wb && r.c0 >= we) || (r.c1 <= wb && r.b1 >= we))) {
+    // region B only
+#pragma unroll
+    for (int p = 0; p < HK_PPL; ++p) {
+      const float x = fmaf(kf[p], r.vbh, r.dh) + fmaf(kf[p], r.vbl, r.dl);
+      const float s = x * x;
+      const float u = s + r.y2;
+      acc[p] = fma(r.S1, widen_pos(gh2_f(s, u)), acc[p]);
+    }
+  } else if (full && (r.b0 >= we || r.b1 <= wb)) {
+    // region A only
+#pragma unroll
+    for (int p = 0; p < HK_PPL; ++p) {
+      const float x = fmaf(kf[p], r.vbh, r.dh) + fmaf(kf[p], r.vbl, r.dl);
+      acc[p] = fma(r.S1, widen_pos(rcp_approx(fmaf(x, x, r.y2))), acc[p]);
+    }
+  } else {
+#pragma unroll
+    for (int p = 0; p < HK_PPL; ++p) {
+      const int k = wb + lane + 32 * p;
+      if (k >= r.i0 && k < r.i1) {
+        const float x = fmaf(kf[p], r.vbh, r.dh) + fmaf(kf[p], r.vbl, r.dl);
+        if (k >= r.c0 && k < r.c1) {
+          acc[p] = fma(r.Sc, (double)voigt916_f(x, r.y, r.ey), acc[p]);
+        } else {
+          const float s = x * x;
+          const float u = s + r.y2;
+          const float t = (k >= r.b0 && k < r.b1) ? gh2_f(s, u) : rcp_approx(u);
+          acc[p] = fma(r.S1, widen_pos(t), acc[p]);
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ FP64 sweep
+__device__ __forceinline__ void sweep_plain(const RecD &r, int wb, int lane,
+                                            const double (&xg)[HK_PPL],
+                                            double (&acc)[HK_PPL]) {
+  const int we = wb + HK_SLICE;
+  if (r.i1 <= wb || r.i0 >= we) return;
+  const bool full = r.i0 <= wb && r.i1 >= we;
+  if (full && ((r.b0 <= wb && r.c0 >= we) || (r.c1 <= wb && r.b1 >= we))) {
+#pragma unroll
+    for (int p = 0; p < HK_PPL; ++p) {
+      const double x = (xg[p] - r.nu) * r.iad;
+      acc[p] += r.S1 * gh2_d(x, r.y2);
+    }
+  } else if (full && (r.b0 >= we || r.b1 <= wb)) {
+#pragma unroll
+    for (int p = 0; p < HK_PPL; ++p) {
+      const double x = (xg[p] - r.nu) * r.iad;
+      acc[p] += r.S1 / (x * x + r.y2);
+    }
+  } else {
+#pragma unroll
+    for (int p = 0; p < HK_PPL; ++p) {
+      const int k = wb + lane + 32 * p;
+      if (k >= r.i0 && k < r.i1) {
+        const double x = (xg[p] - r.nu) * r.iad;
+        double v;
+        if (k >= r.c0 && k < r.c1) v = r.Sc * voigt916_d(x, r.y, r.ey);
+        else if (k >= r.b0 && k < r.b1) v = r.S1 * gh2_d(x, r.y2);
+        else v = r.S1 / (x * x + r.y2);
+        acc[p] += v;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------- persistent kernel
+template <bool MIXED>
+__global__ void __launch_bounds__(HK_THREADS, 2)
+voigt_sum_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
+                 int tiles_per_state, int total_tickets,
+                 unsigned *__restrict__ ticket, double *__restrict__ K,
+                 int64_t k_stride) {
+  using Rec = typename std::conditional<MIXED, RecF, RecD>::type;
+  __shared__ Rec rec[HK_CH];
+  __shared__ int s_ticket;
+  __shared__ long long s_L0, s_L1;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int wb = warp * HK_SLICE;
+
+  for (;;) {
+    if (tid == 0) s_ticket = (int)atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int t = s_ticket;
+    if (t >= total_tickets) break;
+    const int s = t / tiles_per_state;
+    const int tile = t - s * tiles_per_state;
+    const StateDev &st = states[s];
+    const int64_t g0 = (int64_t)tile * HK_G;
+    const int64_t g1 = min(g0 + (int64_t)HK_G, g.nx);
+    if (warp == 0) {
+      const double W = st.wmax + st.shift + 2.0 * g.dnu;
+      const double xlo = grid_x(g, g0) - W;
+      const double xhi = grid_x(g, g1 - 1) + W;
+      const double pad = 1e-12 * (fabs(xlo) + fabs(xhi)) + 1e-300;
+      const int64_t L0 = lower_bound_warp(L.nu0, L.n, xlo - pad);
+      const int64_t L1 = lower_bound_warp(L.nu0, L.n, xhi + pad);
+      if (lane == 0) {
+        s_L0 = L0;
+        s_L1 = L1;
+      }
+    }
+    __syncthreads();
+    const int64_t L0 = s_L0, L1 = s_L1;
+
+    float kf[HK_PPL];
+    double acc[HK_PPL], xg[HK_PPL];
+#pragma unroll
+    for (int p = 0; p < HK_PPL; ++p) {
+      const int k = wb + lane + 32 * p;
+      acc[p] = 0.0;
+      if (MIXED) kf[p] = (float)k;
+      else xg[p] = grid_x(g, g0 + k);
+    }
+
+    for (int64_t c0 = L0; c0 < L1; c0 += HK_CH) {
+      const int cnt = (int)min((int64_t)HK_CH, L1 - c0);
+      if (tid < cnt) stage_line<MIXED>(L, g, st, c0 + tid, g0, g1, &rec[tid]);
+      __syncthreads();
+      for (int j = 0; j < cnt; ++j) {
+        if (MIXED) sweep_mixed(reinterpret_cast<const RecF &>(rec[j]), wb, lane, kf, acc);
+        else sweep_plain(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc);
+      }
+      __syncthreads();
+    }
+
+    double *Ks = K + (int64_t)s * k_stride;
+#pragma unroll
+    for (int p = 0; p < HK_PPL; ++p) {
+      const int64_t gi = g0 + wb + lane + 32 * p;
+      if (gi < g1) Ks[gi] = st.kmin + acc[p];
+    }
+  }
+}
+
+// ------------------------------------------------------ diagnostics kernels
+__global__ void prep_dump_kernel(LinesDev L, GridDev g, StateDev st,
+                                 double *__restrict__ out4,
+                                 long long *__restrict__ win6) {
+  const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= L.n) return;
+  const LineState ls = prep_line(L, st, l);
+  out4[4 * l + 0] = ls.nu;
+  out4[4 * l + 1] = ls.S;
+  out4[4 * l + 2] = ls.iad;
+  out4[4 * l + 3] = ls.vy;
+  int64_t w[6];
+  line_windows(g, st, ls, 0, g.nx, w);
+  for (int k = 0; k < 6; ++k) win6[6 * l + k] = w[k];
+}
+
+__global__ void profile_eval_kernel(int64_t n, const double *__restrict__ x,
+                                    const double *__restrict__ y, int mixed,
+                                    double *__restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double ey = erfcx(y[i]);
+  if (mixed) out[i] = (double)voigt916_f((float)x[i], (float)y[i], (float)ey);
+  else out[i] = voigt916_d(x[i], y[i], ey);
+}
+
+// FP32 FMA throughput probe: 8 independent FMA chains per thread, every SM
+// busy.  Gives the FP32 SIMT peak under the clocks of the current run (the
+// roofline denominator of the Voigt sum).
+__global__ void fma_peak_kernel(int iters, float seed, float *__restrict__ sink) {
+  float a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = seed + threadIdx.x * 1e-7f + k;
+  const float m = 0.9999999f, c = 1e-7f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = fmaf(a[k], m, c);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += a[k];
+  if (s == 123.456f) sink[blockIdx.x] = s;  // keeps the chains alive
+}
+
+cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream) {
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = nsm * 8, threads = 256, iters = 1 << 16;
+  float *sink = nullptr;
+  cudaError_t e = cudaMallocAsync((void **)&sink, blocks * sizeof(float), stream);
+  if (e != cudaSuccess) return e;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  fma_peak_kernel<<<blocks, threads, 0, stream>>>(iters / 8, 1.0f, sink);  // warm-up
+  cudaEventRecord(a, stream);
+  fma_peak_kernel<<<blocks, threads, 0, stream>>>(iters, 1.0f, sink);
+  cudaEventRecord(b, stream);
+  e = cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFreeAsync(sink, stream);
+  const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
+  *tflops = (ms > 0.f) ? flops / (ms * 1e-3) / 1e12 : 0.0;
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+// ------------------------------------------------------------- launchers
+int voigt_tile_points() { return HK_G; }
+
+cudaError_t launch_voigt_sum(bool mixed, const LinesDev &L, const GridDev &g,
+                             const StateDev *states_d, int nstates,
+                             unsigned *ticket_d, double *K_d, int64_t k_stride,
+                             int grid_ctas, cudaStream_t stream) {
+  const int tps = (int)((g.nx + HK_G - 1) / HK_G);
+  const int total = tps * nstates;
+  cudaError_t e = cudaMemsetAsync(ticket_d, 0, sizeof(unsigned), stream);
+  if (e != cudaSuccess) return e;
+  if (total <= 0) return cudaSuccess;
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (mixed)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, voigt_sum_kernel<true>, HK_THREADS, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, voigt_sum_kernel<false>, HK_THREADS, 0);
+  if (per_sm < 1) per_sm = 1;
+  int ctas = grid_ctas > 0 ? grid_ctas : nsm * per_sm;
+  if (ctas > total) ctas = total;
+  if (mixed)
+    voigt_sum_kernel<true><<<ctas, HK_THREADS, 0, stream>>>(L, g, states_d, tps, total, ticket_d, K_d, k_stride);
+  else
+    voigt_sum_kernel<false><<<ctas, HK_THREADS, 0, stream>>>(L, g, states_d, tps, total, ticket_d, K_d, k_stride);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prep_dump(const LinesDev &L, const GridDev &g,
+                             const StateDev &st, double *out4_d,
+                             long long *win6_d, cudaStream_t stream) {
+  if (L.n == 0) return cudaSuccess;
+  const int b = 128;
+  const int64_t nb = (L.n + b - 1) / b;
+  prep_dump_kernel<<<(unsigned)nb, b, 0, stream>>>(L, g, st, out4_d, win6_d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_profile_eval(int64_t n, const double *x_d, const double *y_d,
+                                int mixed, double *out_d, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  const int b = 128;
+  profile_eval_kernel<<<(unsigned)((n + b - 1) / b), b, 0, stream>>>(n, x_d, y_d, mixed, out_d);
+  return cudaGetLastError();
+}
+
+}  // namespace hkb

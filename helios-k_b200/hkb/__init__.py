@@ -1,0 +1,277 @@
+"""hkb -- Python binding of libhkb, the B200 (sm_100a) HELIOS-K opacity engine.
+
+A thin ctypes layer over the C ABI in include/hkb.h.  Host arrays are numpy;
+device buffers are torch CUDA tensors (plumbing only: torch supplies device
+memory and streams, every computation runs in libhkb's own kernels).
+
+There is no CPU fallback: importing works anywhere, but creating a Context
+needs a CUDA device and the built library (helios-k_b200/lib/libhkb.so);
+both missing conditions raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_PKG), "lib", "libhkb.so")
+HEADER_PATH = os.path.join(os.path.dirname(os.path.dirname(_PKG)), "include", "hkb.h")
+
+HK_OK = 0
+STATUS_NAMES = {0: "HK_OK", -1: "HK_ERR_ARG", -2: "HK_ERR_IO", -3: "HK_ERR_FORMAT",
+                -4: "HK_ERR_RANGE", -5: "HK_ERR_CUDA", -6: "HK_ERR_STATE",
+                -7: "HK_ERR_NOMEM", -8: "HK_ERR_UNSUPPORTED"}
+PLAIN_FP64 = 0
+MIXED = 1
+HITRAN = 0
+EXOMOL = 2
+
+_lib = None
+_p = C.c_void_p
+_d = C.c_double
+_i = C.c_int
+_i64 = C.c_int64
+
+
+class HkError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def lib():
+    """Load libhkb.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"libhkb.so not built: {LIB_PATH} (run __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        sig = {
+            "hk_create": (_p, [_i, C.POINTER(_i)]),
+            "hk_destroy": (None, [_p]),
+            "hk_last_error": (C.c_char_p, [_p]),
+            "hk_version": (C.c_char_p, []),
+            "hk_set_species": (_i, [_p, _i, _i, _p, _p, _d, _d]),
+            "hk_set_partition": (_i, [_p, _i, _i, _p, _p]),
+            "hk_set_options": (_i, [_p, _d, _d, _i, _d]),
+            "hk_load_lines_hitran": (_i, [_p, _i64] + [_p] * 9),
+            "hk_load_lines_exomol": (_i, [_p, _i64] + [_p] * 4),
+            "hk_load_species_file": (_i, [_p, C.c_char_p, C.c_char_p, _d, _d, _i, _d]),
+            "hk_num_lines": (_i64, [_p]),
+            "hk_set_grid": (_i, [_p, _d, _d, _d, _i, _i, _d, _d]),
+            "hk_grid_points": (_i64, [_p]),
+            "hk_opacity": (_i, [_p, _i, _p, _p, _i, _p, _i, _p]),
+            "hk_kdist": (_i, [_p, _i, _p, _i, _i, _d, _p, _p, _p, _p, _i, _p]),
+            "hk_state_lines": (_i, [_p, _d, _d, _p, _p, _p, _p, _p]),
+            "hk_line_order": (_i, [_p, _p]),
+            "hk_profile_eval": (_i, [_p, _i64, _p, _p, _i, _p]),
+            "hk_last_timing": (_i, [_p, _p, _p]),
+            "hk_tile_points": (_i, []),
+            "hk_fp32_peak": (_i, [_p, _p]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def header_functions(path: str = HEADER_PATH):
+    """Names of the functions declared in include/hkb.h."""
+    import re
+    txt = open(path).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(hk_[a-z_0-9]+)\s*\(", txt)))
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _is_dev(t):
+    return hasattr(t, "is_cuda") and t.is_cuda
+
+
+class Context:
+    """One libhkb context bound to one GPU (hk_create / hk_destroy)."""
+
+    def __init__(self, device: int = 0):
+        st = C.c_int(0)
+        self._h = lib().hk_create(device, C.byref(st))
+        if not self._h:
+            raise HkError(st.value, f"hk_create(device={device}) failed (no CUDA device?)")
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().hk_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _chk(self, st):
+        if st != HK_OK:
+            raise HkError(st, lib().hk_last_error(self._h).decode())
+
+    # ---------------------------------------------------------- setup
+    def set_species(self, database, mass, abundance, defaultL=0.0, defaultn=0.0):
+        m = _f64(np.atleast_1d(mass))
+        a = _f64(np.atleast_1d(abundance))
+        self._chk(lib().hk_set_species(self._h, database, len(m), _ptr(m), _ptr(a),
+                                       defaultL, defaultn))
+
+    def set_partition(self, iso, T, Q):
+        T = _f64(T)
+        Q = _f64(Q)
+        self._chk(lib().hk_set_partition(self._h, iso, len(T), _ptr(T), _ptr(Q)))
+
+    def set_options(self, qalphaL=0.5, gammaF=1.0, units=0, Sscale=1.0):
+        self._chk(lib().hk_set_options(self._h, qalphaL, gammaF, units, Sscale))
+
+    def load_lines_hitran(self, lines: dict):
+        n = len(lines["nu"])
+        cols = [_f64(lines[k]) for k in ("nu", "S", "EL", "A", "delta", "gair", "gself", "n")]
+        iso = lines.get("iso")
+        iso = None if iso is None else np.ascontiguousarray(iso, dtype=np.int32)
+        self._chk(lib().hk_load_lines_hitran(self._h, n, *[_ptr(c) for c in cols], _ptr(iso)))
+
+    def load_lines_exomol(self, lines: dict):
+        n = len(lines["nu"])
+        cols = [_f64(lines[k]) for k in ("nu", "S", "EL", "A")]
+        self._chk(lib().hk_load_lines_exomol(self._h, n, *[_ptr(c) for c in cols]))
+
+    def load_species_file(self, path, species, numin, numax, cutMode, cut):
+        self._chk(lib().hk_load_species_file(self._h, path.encode(), species.encode(),
+                                             numin, numax, cutMode, cut))
+
+    @property
+    def num_lines(self):
+        return int(lib().hk_num_lines(self._h))
+
+    def set_grid(self, numin, numax, dnu, nbins, cutMode=0, cut=25.0, kmin=0.0):
+        self._chk(lib().hk_set_grid(self._h, numin, numax, dnu, nbins, cutMode, cut, kmin))
+        self._nbins = nbins
+
+    @property
+    def nx(self):
+        return int(lib().hk_grid_points(self._h))
+
+    # -------------------------------------------------------- compute
+    def opacity(self, T, P, precision=MIXED, out=None, stream=None):
+        """K for every state (T[s], P[s]): array (nstates, Nx), FP64.
+
+        out: optional numpy array or torch CUDA tensor (nstates * Nx float64).
+        With a CUDA tensor the call is asynchronous on `stream` (a torch
+        stream or raw handle; default: torch's current stream).
+        """
+        T = _f64(np.atleast_1d(T))
+        P = _f64(np.atleast_1d(P))
+        ns = len(T)
+        if out is None:
+            out = np.empty((ns, self.nx), np.float64)
+        dev = _is_dev(out)
+        sh = _stream_handle(stream, dev)
+        self._chk(lib().hk_opacity(self._h, ns, _ptr(T), _ptr(P), precision, _ptr(out),
+                                   int(dev), sh))
+        return out
+
+    def kdist(self, K, nC=20, unitScale=1.0, coeff=True, nxmin=True, sorted_K=False,
+              recon=False, stream=None, outputs_on_device=None):
+        """Per-bin sort + Chebyshev fit of K (nstates, Nx).
+
+        Returns dict with 'coeff' (nstates, nbins, nC), 'nxmin' (nstates, nbins)
+        and optionally 'sorted' / 'recon' (nstates, Nx).
+        """
+        dev_in = _is_dev(K)
+        if not dev_in:
+            K = _f64(K)
+        ns = K.shape[0] if K.ndim == 2 else 1
+        nx = self.nx
+        nb = self._nbins
+        if outputs_on_device is None:
+            outputs_on_device = dev_in
+        if outputs_on_device:
+            import torch
+            mk = lambda shape, dt: torch.empty(shape, dtype=dt, device=K.device)
+            f64, i32 = torch.float64, torch.int32
+        else:
+            mk = lambda shape, dt: np.empty(shape, dt)
+            f64, i32 = np.float64, np.int32
+        res = {}
+        res["coeff"] = mk((ns, nb, nC), f64) if coeff else None
+        res["nxmin"] = mk((ns, nb), i32) if nxmin else None
+        res["sorted"] = mk((ns, nx), f64) if sorted_K else None
+        res["recon"] = mk((ns, nx), f64) if recon else None
+        sh = _stream_handle(stream, dev_in or outputs_on_device)
+        self._chk(lib().hk_kdist(self._h, ns, _ptr(K), int(dev_in), nC, unitScale,
+                                 _ptr(res["coeff"]), _ptr(res["nxmin"]), _ptr(res["sorted"]),
+                                 _ptr(res["recon"]), int(outputs_on_device), sh))
+        return res
+
+    # ---------------------------------------------------- diagnostics
+    def state_lines(self, T, P):
+        n = self.num_lines
+        outs = [np.empty(n, np.float64) for _ in range(4)]
+        win = np.empty((n, 6), np.int64)
+        self._chk(lib().hk_state_lines(self._h, T, P, *[_ptr(o) for o in outs], _ptr(win)))
+        return (*outs, win)
+
+    def line_order(self):
+        o = np.empty(self.num_lines, np.int64)
+        self._chk(lib().hk_line_order(self._h, _ptr(o)))
+        return o
+
+    def profile_eval(self, x, y, precision=MIXED):
+        x = _f64(x)
+        y = _f64(y)
+        out = np.empty(len(x), np.float64)
+        self._chk(lib().hk_profile_eval(self._h, len(x), _ptr(x), _ptr(y), precision, _ptr(out)))
+        return out
+
+    def last_timing(self):
+        a = C.c_double(-1)
+        b = C.c_double(-1)
+        self._chk(lib().hk_last_timing(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def fp32_peak_tflops(self):
+        t = C.c_double(0)
+        self._chk(lib().hk_fp32_peak(self._h, C.byref(t)))
+        return t.value
+
+
+def _stream_handle(stream, device_io):
+    if stream is None:
+        if not device_io:
+            return None
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if hasattr(stream, "cuda_stream"):
+        return C.c_void_p(stream.cuda_stream)
+    return C.c_void_p(int(stream))
+
+
+def tile_points() -> int:
+    return int(lib().hk_tile_points())
+

@@ -1,0 +1,175 @@
+/*
+ * hkb.h -- C ABI of libhkb, the B200 (sm_100a) opacity engine.
+ *
+ * The reference (HELIOS-K) is a single executable with no library API; its
+ * internal seam for this path is the kernel-launch helpers
+ * Line6A_Call/Line6B_Call/Line6C_Call (voigt.h:1820, 1968, 2004) fed by the
+ * host readers (host.h, ISO.h) and followed by the post-processing chain of
+ * heliosk.cu:2046-2195.  Each entry point below names what it replaces.
+ * The heliosk drop-in executable (helios-k_b200/bin/heliosk) is built on
+ * these calls and keeps the reference's param.dat / <species>.param inputs
+ * and Out_* / Info_* outputs.
+ *
+ * Conventions
+ *  - Every call returns hk_status: 0 = HK_OK, negative = error class; the
+ *    message is available from hk_last_error(ctx).  Nothing is printed.
+ *  - Pointers are plain host pointers unless a *_on_device flag says the
+ *    buffer is device memory of the context's GPU.  Callers own their
+ *    buffers; the library owns its device workspace.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = the legacy default
+ *    stream).  Calls with host outputs synchronise that stream before
+ *    returning; calls with device outputs are asynchronous on it.
+ *  - One context per host thread at a time.
+ */
+#ifndef HKB_H
+#define HKB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hk_ctx hk_ctx;
+typedef int hk_status;
+
+enum {
+  HK_OK = 0,
+  HK_ERR_ARG = -1,         /* invalid argument                          */
+  HK_ERR_IO = -2,          /* file missing or unreadable                */
+  HK_ERR_FORMAT = -3,      /* malformed parameter / species / line file */
+  HK_ERR_RANGE = -4,       /* value outside what the path supports      */
+  HK_ERR_CUDA = -5,        /* CUDA runtime error                        */
+  HK_ERR_STATE = -6,       /* call order (e.g. no grid set)             */
+  HK_ERR_NOMEM = -7,       /* device or host allocation failed          */
+  HK_ERR_UNSUPPORTED = -8  /* option outside this build's scope        */
+};
+
+enum { HK_PRECISION_PLAIN_FP64 = 0, HK_PRECISION_MIXED = 1 };
+enum { HK_DATABASE_HITRAN = 0, HK_DATABASE_EXOMOL = 2 };
+
+/* ------------------------------------------------------------ context */
+
+/* Bind a GPU and create the workspace.
+ * Replaces cudaSetDevice(param.dev) (heliosk.cu:392) and the K/x/bin
+ * allocations of heliosk.cu:712-725. */
+hk_ctx *hk_create(int device, hk_status *status);
+void hk_destroy(hk_ctx *ctx);
+/* Message of the last failed call on this context ("" if none). */
+const char *hk_last_error(const hk_ctx *ctx);
+const char *hk_version(void);
+
+/* ------------------------------------------------------------ species */
+
+/* Isotopologue table of one species: molar masses (g/mol) and abundances.
+ * Replaces Init (ISO.h:16-219) for callers that do not read a .param file.
+ * defaultL / defaultn are the ExoMol width defaults (ISO.h:192-206). */
+hk_status hk_set_species(hk_ctx *ctx, int database, int niso,
+                         const double *mass_g_mol, const double *abundance,
+                         double defaultL, double defaultn);
+
+/* Partition-function table (T, Q) of isotopologue `iso`, interpolated per
+ * state exactly as readPartition (host.h:9-73). */
+hk_status hk_set_partition(hk_ctx *ctx, int iso, int n, const double *T,
+                           const double *Q);
+
+/* param.dat keys qalphaL, gammaF, Units (host.h:75-300) and the species
+ * abundance scale of a mixture entry (heliosk.cu:787-789).  Defaults:
+ * qalphaL = 0.5 (define.h:66), gammaF = 1, units = 0, Sscale = 1. */
+hk_status hk_set_options(hk_ctx *ctx, double qalphaL, double gammaF, int units,
+                         double Sscale);
+
+/* -------------------------------------------------------------- lines */
+
+/* HITRAN/HITEMP line list as host SoA (copied to HBM, sorted by nu).
+ * Fields as in the 68-byte record (host.h:607-615): nu, S, E'', A, delta,
+ * gamma_air, gamma_self, n; iso = isotopologue index per line (NULL: 0).
+ * Replaces readFile (host.h:598-649) + Copy_Line (host.h:958-967). */
+hk_status hk_load_lines_hitran(hk_ctx *ctx, int64_t n, const double *nu,
+                               const double *S, const double *EL,
+                               const double *A, const double *delta,
+                               const double *gair, const double *gself,
+                               const double *nexp, const int32_t *iso);
+
+/* ExoMol line list (nu, S, E'', A), widths from hk_set_species defaults.
+ * Replaces readFileExomol (host.h:656-668) + L_kernelExomol
+ * (voigt.h:484-504). */
+hk_status hk_load_lines_exomol(hk_ctx *ctx, int64_t n, const double *nu,
+                               const double *S, const double *EL,
+                               const double *A);
+
+/* Read <path><species>.param, its partition files and every binary line
+ * file whose range can reach [numin - cut, numax + cut] (heliosk.cu:943-956),
+ * then load them.  Replaces Init + readPartition + the file loop of
+ * heliosk.cu:943-1043.  cut == 0 means no cutoff. */
+hk_status hk_load_species_file(hk_ctx *ctx, const char *path,
+                               const char *species, double numin, double numax,
+                               int cutMode, double cut);
+
+int64_t hk_num_lines(const hk_ctx *ctx);
+
+/* --------------------------------------------------------------- grid */
+
+/* Wavenumber grid x_i = numin + i dnu, Nx = (int)((numax-numin)/dnu + 0.5)
+ * points in nbins equal bins; cutoff mode/width; K floor kmin.
+ * Replaces heliosk.cu:417-476 and InitialK/setX/binKey/binIndex
+ * (voigt.h:713-832).  Nx must divide evenly into nbins (heliosk.cu:456). */
+hk_status hk_set_grid(hk_ctx *ctx, double numin, double numax, double dnu,
+                      int nbins, int cutMode, double cut, double kmin);
+int64_t hk_grid_points(const hk_ctx *ctx);
+
+/* ------------------------------------------------------------ compute */
+
+/* Opacity K(nu) of every state (T[s], P[s]) onto the grid:
+ * K_out[s * Nx + i], FP64.  precision selects the FP64 plain form or the
+ * mixed FP32/FP64 form.  All states run in one persistent launch.
+ * Replaces the per-part / per-pressure loop of heliosk.cu:1051-1776:
+ * S2_kernel, the nu sort, S3_kernel, nuLimits/iiLimits, Line6A/B/C_Call and
+ * AddKStreams_kernel. */
+hk_status hk_opacity(hk_ctx *ctx, int nstates, const double *T, const double *P,
+                     int precision, double *K_out, int K_on_device,
+                     void *stream);
+
+/* Per-bin sort and Chebyshev k-distribution fit of K (nstates x Nx):
+ * coeff_out[(s * nbins + b) * nC + j], nxmin_out[s * nbins + b] (the
+ * reference's Nxmin; ystart = min(Nxmin / (Nxb - 1), 1)), optional
+ * per-bin sorted K and optional reconstruction (expfx + inverse rescale).
+ * Any output pointer may be NULL.  Replaces heliosk.cu:2046-2193
+ * (thrust sorts, Vandermonde/QR/findCut/rescale/copyK2/lnK/leastSquare/
+ * expfx kernels of resample.h:14-524). */
+hk_status hk_kdist(hk_ctx *ctx, int nstates, const double *K, int K_on_device,
+                   int nC, double unitScale, double *coeff_out,
+                   int32_t *nxmin_out, double *sortedK_out, double *recon_out,
+                   int outputs_on_device, void *stream);
+
+/* ------------------------------------------------------- diagnostics */
+
+/* Per-line state (nu, S, 1/alphaD, gammaL/alphaD) and the six window
+ * indices i0, b0, c0, c1, b1, i1 of every loaded line (in load order is NOT
+ * kept: lines are in the library's nu-sorted order, see hk_line_order) for
+ * one state, computed by the same device code the sum uses.  Any output may
+ * be NULL. */
+hk_status hk_state_lines(hk_ctx *ctx, double T, double P, double *nu,
+                         double *S, double *iad, double *vy, int64_t *win6);
+
+/* Permutation applied at load: sorted position k holds input line order[k]. */
+hk_status hk_line_order(hk_ctx *ctx, int64_t *order);
+
+/* Voigt function V(x, y) (region-C formula, Algorithm 916) evaluated by the
+ * device code of the given precision. */
+hk_status hk_profile_eval(hk_ctx *ctx, int64_t n, const double *x,
+                          const double *y, int precision, double *out);
+
+/* Device time of the last hk_opacity / hk_kdist kernels (CUDA events on
+ * the launching stream), in milliseconds; and the grid tile size. */
+hk_status hk_last_timing(const hk_ctx *ctx, double *voigt_ms, double *kdist_ms);
+int hk_tile_points(void);
+
+/* FP32 FMA throughput of this GPU at the current clocks (TFLOP/s), from a
+ * short all-SM FMA probe; the roofline denominator of the Voigt sum. */
+hk_status hk_fp32_peak(hk_ctx *ctx, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HKB_H */

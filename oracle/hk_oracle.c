@@ -1,0 +1,708 @@
+/*
+ * hk_oracle.c -- FP64 CPU restatement of the HELIOS-K opacity hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the parity checker for the CUDA path and the
+ * timed CPU baseline.  The product never links or calls this file.
+ *
+ * Built with -O2 -ffp-contract=off -fopenmp (see oracle/Makefile) so that
+ * every FP64 predicate below is the plain IEEE sequence written here.
+ * Where the reference's CUDA code is contracted to an FMA by nvcc
+ * (a*b + c in one expression), the restatement calls fma() explicitly.
+ */
+#include "hk_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------ grid */
+
+/* voigt.h:751-768 (setX_kernel): x_d[id] = numin + id * dnu, contracted. */
+double hko_grid_x(double numin, double dnu, int64_t i) {
+  return fma((double)i, dnu, numin);
+}
+
+/* heliosk.cu:448-455: Nx = (int)((numax - numin) / dnu + 0.5) */
+int hko_grid_nx(double numin, double numax, double dnu) {
+  return (int)((numax - numin) / dnu + 0.5);
+}
+
+void hko_grid_fill(double numin, double dnu, int64_t nx, double *x) {
+  for (int64_t i = 0; i < nx; ++i) x[i] = hko_grid_x(numin, dnu, i);
+}
+
+/* Bin boundaries heliosk.cu:436-441, binKey_kernel voigt.h:779-805,
+ * binIndex_kernel voigt.h:815-832. */
+void hko_bin_keys(double numin, double numax, double dnu, int64_t nx, int nbins,
+                  int32_t *key, int32_t *bin_index) {
+  double *bb = (double *)malloc((size_t)(nbins + 1) * sizeof(double));
+  for (int i = 0; i < nbins; ++i)
+    bb[i] = numin + i * (numax - numin) / ((double)nbins);
+  bb[nbins] = numax;
+  for (int64_t id = 0; id < nx; ++id) {
+    double nu = hko_grid_x(numin, dnu, id);
+    int32_t k = 0;
+    /* first bin with bb[i] <= nu < bb[i+1]; the intervals are disjoint so a
+     * binary search finds the same bin the reference's linear scan finds */
+    int lo = 0, hi = nbins - 1, found = -1;
+    while (lo <= hi) {
+      int mid = (lo + hi) / 2;
+      if (nu < bb[mid]) hi = mid - 1;
+      else if (nu >= bb[mid + 1]) lo = mid + 1;
+      else { found = mid; break; }
+    }
+    if (found >= 0) k = found;
+    if (nu >= numax) k = nbins;
+    key[id] = k;
+  }
+  if (bin_index) {
+    for (int i = 0; i < nbins + 2; ++i) bin_index[i] = 0;
+    for (int64_t id = 0; id + 1 < nx; ++id) {
+      int32_t b0 = key[id], b1 = key[id + 1];
+      if (b1 > b0) bin_index[b1] = (int32_t)(id + 1);
+    }
+    bin_index[0] = 0;
+    bin_index[nbins] = (int32_t)nx;
+    bin_index[nbins + 1] = (int32_t)nx;
+  }
+  free(bb);
+}
+
+/* ------------------------------------------------------- partition Q(T) */
+
+/* host.h:9-73 readPartition: walk the table, first row with T1 >= T,
+ * linear interpolation between the previous row and that row.
+ * Returns 1 on success, 0 on the reference's error conditions. */
+int hko_partition_interp(const double *Tq, const double *q, int nq, double T,
+                         double *Q_out) {
+  double T0, T1 = -1.0, q0, q1 = 1.0, qv = 1.0;
+  for (int j = 0; j < 100000; ++j) {
+    T0 = T1;
+    q0 = q1;
+    if (j >= nq) return 0; /* fscanf returned EOF */
+    T1 = Tq[j];
+    q1 = q[j];
+    if (T0 == T1 && T0 < T && j > 0) return 0;
+    if (T1 > T && j == 0) return 0;
+    if (T0 < T && T1 >= T) {
+      double tt = (T - T0) / (T1 - T0);
+      qv = (q1 - q0) * tt + q0;
+      if (j == 0) qv = q1;
+      *Q_out = qv;
+      return 1;
+    }
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------ line prep */
+
+/* host.h:598-649 (readFile) followed by voigt.h:331-363 (S2_kernel). */
+void hko_prep_hitran(int64_t n, const double *nu, const double *S_file,
+                     const double *EL, const double *A, const double *delta,
+                     const double *gair, const double *gself,
+                     const double *nexp, const int32_t *iso, int niso,
+                     const double *iso_mass, const double *iso_ab,
+                     const double *iso_Q, double T, double P, double qalphaL,
+                     double gammaF, int units, double meanMass, double Sscale,
+                     double *out_nu, double *out_S, double *out_iad,
+                     double *out_vy) {
+  const double c = HKO_H * HKO_C / HKO_KB;
+  (void)niso;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    int j = iso[i];
+    double mass = iso_mass[j] / HKO_NA;
+    double Abundance = iso_ab[j];
+    double Sscale1 = Sscale;
+    if (units == 0) {
+      Abundance *= iso_mass[j] / meanMass;
+      Sscale1 *= iso_mass[j] / meanMass;
+    }
+    double Q = iso_Q[j];
+    double vy = (1.0 - qalphaL) * gair[i] + qalphaL * gself[i];
+    vy *= gammaF;
+    double iad0 = HKO_C * sqrt(mass / (2.0 * HKO_KB * T));
+    double S = S_file[i] / Q * Abundance * Sscale1;
+    /* S2_kernel */
+    double nuv = fma(delta[i], P, nu[i]);
+    double iad = iad0 / nuv;
+    double el = EL[i];
+    S *= exp(-el * c / T + el * c / HKO_T0) * (1.0 - exp(-c * nuv / T)) /
+         (1.0 - exp(-c * nuv / HKO_T0)) * iad;
+    double aL = vy * ((P / HKO_PO_ATM) * pow(HKO_T0 / T, nexp[i]));
+    aL = aL + A[i] / (4.0 * M_PI * HKO_C);
+    double vyv = aL * iad;
+    if (nuv == 0.0) {
+      S = 0.0;
+      iad = 0.0;
+      vyv = 0.0;
+    }
+    out_nu[i] = nuv;
+    out_S[i] = S;
+    out_iad[i] = iad;
+    out_vy[i] = vyv;
+  }
+}
+
+/* voigt.h:484-504 (L_kernelExomol) followed by voigt.h:365-397 (Sf_kernel),
+ * with the caller-side scalings of heliosk.cu:1064-1070. */
+void hko_prep_exomol(int64_t n, const double *nu, const double *S_file,
+                     const double *EL, const double *A, double mass_g_mol,
+                     double ab, double Q, double defaultL, double defaultn,
+                     double T, double P, double gammaF, int units,
+                     double meanMass, double Sscale, double *out_nu,
+                     double *out_S, double *out_iad, double *out_vy) {
+  double mass = mass_g_mol / HKO_NA;
+  double Abundance = ab;
+  if (units == 0) {
+    Abundance *= mass_g_mol / meanMass;
+    Sscale *= mass_g_mol / meanMass;
+  }
+  const double c1 = HKO_H * HKO_C / (HKO_KB * T);
+  const double T1 = HKO_T0 / T;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    double nuv = nu[i];
+    double iad0 = HKO_C * sqrt(mass / (2.0 * HKO_KB * T));
+    double Ad = A[i] / (4.0 * M_PI * HKO_C);
+    double vy = defaultL * gammaF;
+    double S = S_file[i] * Abundance * Sscale / Q;
+    double iad = iad0 / nuv;
+    S *= exp(-c1 * EL[i]) * (1.0 - exp(-c1 * nuv)) * iad;
+    double aL = vy * ((P / HKO_PO_BAR) * pow(T1, defaultn));
+    aL = aL + Ad;
+    double vyv = aL * iad;
+    if (nuv == 0.0) {
+      S = 0.0;
+      iad = 0.0;
+      vyv = 0.0;
+    }
+    out_nu[i] = nuv;
+    out_S[i] = S;
+    out_iad[i] = iad;
+    out_vy[i] = vyv;
+  }
+}
+
+/* -------------------------------------------------------------- windows */
+
+typedef struct {
+  double numin, dnu, nu, iad, vy2, w;
+} wctx;
+
+static inline double w_d(const wctx *c, int64_t i) {
+  return hko_grid_x(c->numin, c->dnu, i) - c->nu;
+}
+static inline double w_r2(const wctx *c, int64_t i) {
+  double x = w_d(c, i) * c->iad;
+  return x * x + c->vy2;
+}
+/* predicate kinds: all monotone false..true over the searched range */
+enum { P_LEFT_CUT, P_RIGHT_CUT, P_CENTER, P_LEFT_R, P_RIGHT_R };
+static inline int w_pred(const wctx *c, int kind, int64_t i, double R) {
+  switch (kind) {
+  case P_LEFT_CUT: return w_d(c, i) > -c->w;  /* inside from the left  */
+  case P_RIGHT_CUT: return w_d(c, i) >= c->w; /* outside on the right   */
+  case P_CENTER: return w_d(c, i) >= 0.0;
+  case P_LEFT_R: return w_r2(c, i) < R;       /* i < centre            */
+  default: return w_r2(c, i) >= R;            /* i >= centre           */
+  }
+}
+
+/* First index in [lo, hi) where the monotone predicate is true, hi if none.
+ * The result does not depend on the estimate e. */
+static int64_t first_true(const wctx *c, int kind, double R, int64_t lo,
+                          int64_t hi, int64_t e) {
+  if (lo >= hi) return lo;
+  if (e < lo) e = lo;
+  if (e > hi) e = hi;
+  /* bracket [a, b]: every index below a is false (or a == lo), b is true
+   * (index hi counts as true); gallop outwards from the estimate e */
+  int64_t a, b;
+  if (e >= hi || w_pred(c, kind, e, R)) {
+    b = e;
+    int64_t step = 1;
+    while (1) {
+      int64_t t = b - step;
+      if (t < lo) { a = lo; break; }
+      if (!w_pred(c, kind, t, R)) { a = t + 1; break; }
+      b = t;
+      step *= 2;
+    }
+  } else {
+    a = e + 1;
+    int64_t step = 1;
+    while (1) {
+      int64_t t = a - 1 + step;
+      if (t >= hi) { b = hi; break; }
+      if (w_pred(c, kind, t, R)) { b = t; break; }
+      a = t + 1;
+      step *= 2;
+    }
+  }
+  /* binary search in [a, b]: pred false before a, true at b (or b == hi) */
+  while (a < b) {
+    int64_t m = a + (b - a) / 2;
+    if (w_pred(c, kind, m, R)) b = m;
+    else a = m + 1;
+  }
+  return a;
+}
+
+static int64_t est_index(double nu_edge, double numin, double dnu, int64_t nx) {
+  double e = ceil((nu_edge - numin) / dnu);
+  if (!(e > -1.0)) return 0;        /* also catches NaN */
+  if (e > (double)nx) return nx;
+  return (int64_t)e;
+}
+
+/* Per-line index windows.  Restates the region classes of nuLimits_kernel
+ * (voigt.h:2205-2341) and the per-pair predicates of Line6fA/B/C
+ * (voigt.h:1223, 1481, 1662) as exact FP64 index ranges:
+ *   cut window  [i0, i1)     : |x_i - nu| < w
+ *   B or C      [b0, b1)     : r2 < 1e6   (inside the cut window)
+ *   C           [c0, c1)     : r2 < 100   (inside the cut window)
+ * win[6*l + 0..5] = i0, b0, c0, c1, b1, i1.
+ * Lines with S == 0 or ialphaD == 0 contribute exactly zero in the
+ * reference (S2_kernel zeroes them, voigt.h:355-359) and get empty windows. */
+void hko_windows(int64_t n, const double *nu, const double *S,
+                 const double *iad, const double *vy, double numin, double dnu,
+                 int64_t nx, int cutMode, double cut, int64_t *win) {
+  if (cut == 0.0) cut = 1.0e30; /* heliosk.cu:947 */
+#pragma omp parallel for schedule(static)
+  for (int64_t l = 0; l < n; ++l) {
+    int64_t *o = win + 6 * l;
+    if (S[l] == 0.0 || iad[l] == 0.0 || !(iad[l] > 0.0)) {
+      for (int k = 0; k < 6; ++k) o[k] = 0;
+      continue;
+    }
+    wctx c;
+    c.numin = numin;
+    c.dnu = dnu;
+    c.nu = nu[l];
+    c.iad = iad[l];
+    c.vy2 = vy[l] * vy[l];
+    double w;
+    if (cutMode == 1) w = cut * vy[l] / iad[l];
+    else if (cutMode == 2) w = cut / iad[l];
+    else w = cut;
+    c.w = w;
+    int64_t i0 = first_true(&c, P_LEFT_CUT, 0, 0, nx,
+                            est_index(c.nu - w, numin, dnu, nx));
+    int64_t i1 = first_true(&c, P_RIGHT_CUT, 0, i0, nx,
+                            est_index(c.nu + w, numin, dnu, nx));
+    if (i1 <= i0) {
+      for (int k = 0; k < 6; ++k) o[k] = i0;
+      continue;
+    }
+    int64_t ic = first_true(&c, P_CENTER, 0, i0, i1,
+                            est_index(c.nu, numin, dnu, nx));
+    int64_t bc[2][2];
+    const double Rs[2] = {1.0e6, 100.0};
+    for (int r = 0; r < 2; ++r) {
+      double R = Rs[r];
+      double h2 = R - c.vy2;
+      int64_t lo, hi;
+      if (h2 > 0.0) {
+        double h = sqrt(h2) / c.iad;
+        lo = first_true(&c, P_LEFT_R, R, i0, ic,
+                        est_index(c.nu - h, numin, dnu, nx));
+        hi = first_true(&c, P_RIGHT_R, R, ic, i1,
+                        est_index(c.nu + h, numin, dnu, nx));
+      } else {
+        lo = ic;
+        hi = ic;
+      }
+      bc[r][0] = lo;
+      bc[r][1] = hi;
+    }
+    o[0] = i0;
+    o[1] = bc[0][0];
+    o[2] = bc[1][0];
+    o[3] = bc[1][1];
+    o[4] = bc[0][1];
+    o[5] = i1;
+  }
+}
+
+/* --------------------------------------------------------------- profile */
+
+/* Scaled complementary error function erfcx(y) = exp(y^2) erfc(y), y >= 0.
+ * Own implementation from classical expansions (test oracle only):
+ *   y < 0.5      : erfc = 1 - erf, erf from its Maclaurin series
+ *                  erf(y) = 2/sqrt(pi) sum (-1)^k y^(2k+1) / (k! (2k+1));
+ *   0.5 <= y < 2 : erf(y) = 2/sqrt(pi) exp(-y^2) sum 2^k y^(2k+1)/(2k+1)!!
+ *                  (all terms positive), erfcx = exp(y^2) - that sum;
+ *   y >= 2       : Laplace continued fraction
+ *                  sqrt(pi) erfcx(y) = 1/(y + (1/2)/(y + 1/(y + (3/2)/(y + ...))))
+ *                  evaluated bottom-up at fixed depth.
+ * Checked against scipy.special.erfcx in tests/test_oracle_profile.py. */
+double hko_erfcx(double y) {
+  const double isqpi = 0.56418958354775628695; /* 1/sqrt(pi) */
+  if (y < 0.0) return 2.0 * exp(y * y) - hko_erfcx(-y);
+  if (y < 0.5) {
+    double y2 = y * y, term = y, sum = y;
+    for (int k = 1; k < 60; ++k) {
+      term *= -y2 / (double)k;
+      double add = term / (double)(2 * k + 1);
+      sum += add;
+      if (fabs(add) < 1e-18 * fabs(sum)) break;
+    }
+    return exp(y2) * (1.0 - 2.0 * isqpi * sum);
+  }
+  if (y < 2.0) {
+    double y2 = y * y, term = y, sum = y;
+    for (int k = 1; k < 400; ++k) {
+      term *= 2.0 * y2 / (double)(2 * k + 1);
+      sum += term;
+      if (term < 1e-18 * sum) break;
+    }
+    return exp(y2) - 2.0 * isqpi * sum;
+  }
+  double f = y;
+  for (int k = 400; k >= 1; --k) f = y + (0.5 * k) / f;
+  return isqpi / f;
+}
+
+/* Zaghloul & Ali, Algorithm 916, as restated in voigt.h:165-216 (Sigmab)
+ * and voigt.h:278-300 (voigt_916), FP64 with def_TOL, a = pi/sqrt(-ln(TOL/2)).
+ * ey = erfcx(y) (per-line constant). */
+static double voigt916_ey(double x, double y, double ey) {
+  static double a = 0.0;
+  if (a == 0.0) a = M_PI * sqrt(-1.0 / log(HKO_TOL * 0.5));
+  double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  double ex2 = exp(-x * x);
+  double ax = fabs(x);
+  if (x != 0.0 && y != 0.0) {
+    double sold1 = 0.0, sold2 = 0.0, sold3 = 0.0;
+    double yy = y * y;
+    int n0 = (int)ceil(ax / a);
+    int stop1 = 0, stop2 = 0, stop3 = 0;
+    for (int n = 1; n < 100; ++n) {
+      int n3p = n0 + n - 1;
+      int n3n = n0 - n;
+      double an = a * n, an3p = a * n3p, an3n = a * n3n;
+      double f = 1.0 / (an * an + yy);
+      double f3p = 1.0 / (an3p * an3p + yy);
+      double f3n = 1.0 / (an3n * an3n + yy);
+      s1 += f * exp(-(an * an + ax * ax));
+      s2 += f * exp(-(an + ax) * (an + ax));
+      s3 += f3p * exp(-(an3p - ax) * (an3p - ax));
+      if (n3n >= 1) s3 += f3n * exp(-(an3n - ax) * (an3n - ax));
+      if (fabs(s1 - sold1) < HKO_TOL) stop1 = 1;
+      if (fabs(s2 - sold2) < HKO_TOL) stop2 = 1;
+      if (fabs(s3 - sold3) < HKO_TOL) stop3 = 1;
+      if (stop1 && stop2 && stop3) break;
+      sold1 = s1;
+      sold2 = s2;
+      sold3 = s3;
+    }
+  }
+  double xy = ax * y;
+  double a2ipi = 2.0 * a / M_PI;
+  double cos2xy = cos(2.0 * xy);
+  double sinxy = sin(xy);
+  double t1 = ex2 * ey * cos2xy;
+  if (x != 0.0 && y != 0.0) {
+    t1 += a2ipi * ax * sinxy * ex2 * sinxy / xy;
+    t1 += a2ipi * y * (-cos2xy * s1 + 0.5 * (s2 + s3));
+  }
+  if (x == 0.0) t1 = ey;
+  if (y == 0.0) t1 = ex2;
+  return t1;
+}
+
+double hko_voigt916(double x, double y) {
+  return voigt916_ey(x, y, hko_erfcx(y));
+}
+
+/* region B, 2nd-order Gauss-Hermite, voigt.h:1481-1490; returns t4 such
+ * that the contribution is S1 * t4 with S1 = S * y / pi */
+double hko_gh2(double x, double y) {
+  double t1 = x * x;
+  double r2 = t1 + y * y;
+  t1 *= 6.0;
+  double t2 = r2 + 1.5;
+  double t3 = M_PI * t2;
+  return (t3 * (2.0 * t2 + r2) - 2.0 * t1) / (3.0 * r2 * (t3 * t2 - t1));
+}
+
+/* --------------------------------------------------------------- opacity */
+
+typedef struct {
+  int64_t i0;
+  int64_t l;
+} lkey;
+
+static int cmp_lkey(const void *a, const void *b) {
+  const lkey *x = (const lkey *)a, *y = (const lkey *)b;
+  if (x->i0 < y->i0) return -1;
+  if (x->i0 > y->i0) return 1;
+  return (x->l < y->l) ? -1 : (x->l > y->l);
+}
+
+/* Sum of the Voigt contributions of all lines onto the grid:
+ *   C: S * V(x, y) / sqrt(pi)         (voigt.h:1662-1682, b = 1/sqrt(pi))
+ *   B: S1 * t4,   S1 = S * y / pi     (voigt.h:1481-1490; S3_kernel 454)
+ *   A: S1 / r2                        (voigt.h:1223-1227)
+ * then K = kmin + sum (InitialK_kernel + AddKStreams_kernel, voigt.h:713-742).
+ * OpenMP over grid tiles; each tile owns its points, so no atomics. */
+void hko_opacity(int64_t n, const double *nu, const double *S,
+                 const double *iad, const double *vy, const int64_t *win,
+                 double numin, double dnu, int64_t ib, int64_t ie, double kmin,
+                 double *K, int nthreads, int64_t pairs_out[3]) {
+  lkey *ord = (lkey *)malloc((size_t)(n > 0 ? n : 1) * sizeof(lkey));
+  double *ey = (double *)malloc((size_t)(n > 0 ? n : 1) * sizeof(double));
+  int64_t m = 0, wmax = 0;
+  for (int64_t l = 0; l < n; ++l) {
+    const int64_t *o = win + 6 * l;
+    if (o[5] > o[0]) {
+      ord[m].i0 = o[0];
+      ord[m].l = l;
+      ++m;
+      if (o[5] - o[0] > wmax) wmax = o[5] - o[0];
+    }
+  }
+  qsort(ord, (size_t)m, sizeof(lkey), cmp_lkey);
+#pragma omp parallel for schedule(static)
+  for (int64_t l = 0; l < n; ++l) ey[l] = hko_erfcx(vy[l]);
+
+  const int64_t TILE = 4096;
+  int64_t ntile = (ie - ib + TILE - 1) / TILE;
+  int64_t pa = 0, pb = 0, pc = 0;
+  const double isqpi = 1.0 / sqrt(M_PI);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : pa, pb, pc)
+  for (int64_t t = 0; t < ntile; ++t) {
+    int64_t t0 = ib + t * TILE, t1 = t0 + TILE;
+    if (t1 > ie) t1 = ie;
+    double acc[4096];
+    for (int64_t i = 0; i < t1 - t0; ++i) acc[i] = 0.0;
+    /* candidate lines: i0 in (t0 - wmax, t1) */
+    int64_t lo = 0, hi = m;
+    int64_t key = t0 - wmax;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) / 2;
+      if (ord[mid].i0 <= key) lo = mid + 1;
+      else hi = mid;
+    }
+    for (int64_t q = lo; q < m && ord[q].i0 < t1; ++q) {
+      int64_t l = ord[q].l;
+      const int64_t *o = win + 6 * l;
+      int64_t a0 = o[0] > t0 ? o[0] : t0;
+      int64_t a1 = o[5] < t1 ? o[5] : t1;
+      if (a0 >= a1) continue;
+      double nul = nu[l], il = iad[l], y = vy[l], Sl = S[l];
+      double S1 = Sl * y / M_PI;
+      double y2 = y * y;
+      for (int64_t i = a0; i < a1; ++i) {
+        double d = hko_grid_x(numin, dnu, i) - nul;
+        double x = d * il;
+        double v;
+        if (i >= o[2] && i < o[3]) {
+          v = Sl * voigt916_ey(x, y, ey[l]) * isqpi;
+          ++pc;
+        } else if (i >= o[1] && i < o[4]) {
+          double t1x = x * x;
+          double r2 = t1x + y2;
+          t1x *= 6.0;
+          double t2 = r2 + 1.5;
+          double t3 = M_PI * t2;
+          double t4 =
+              (t3 * (2.0 * t2 + r2) - 2.0 * t1x) / (3.0 * r2 * (t3 * t2 - t1x));
+          v = S1 * t4;
+          ++pb;
+        } else {
+          double r2 = x * x + y2;
+          v = S1 / r2;
+          ++pa;
+        }
+        acc[i - t0] += v;
+      }
+    }
+    for (int64_t i = t0; i < t1; ++i) K[i - ib] = kmin + acc[i - t0];
+  }
+  if (pairs_out) {
+    pairs_out[0] = pa;
+    pairs_out[1] = pb;
+    pairs_out[2] = pc;
+  }
+  free(ord);
+  free(ey);
+}
+
+/* ------------------------------------------------------- k-distribution */
+
+/* resample.h:14-37 (Vandermonde_kernel), column-major V[id + nxb*i]. */
+void hko_vandermonde(int nxb, int nc, double *V) {
+  for (int id = 0; id < nxb; ++id) {
+    double x = id * 2.0 / ((double)nxb - 1.0) - 1.0;
+    V[id] = 1.0;
+    if (nc > 1) V[id + (int64_t)nxb] = x;
+    double t = x, t0 = 1.0;
+    for (int i = 2; i < nc; ++i) {
+      double tt = t;
+      t = fma(2.0 * x, t, -t0);
+      t0 = tt;
+      V[id + (int64_t)nxb * i] = t;
+    }
+  }
+}
+
+/* resample.h:73-227 (QR_kernel): scaled Householder QR of the nxb x nc
+ * matrix in place; C[i] = sigma (v_ii + sigma), D[i] = -scale sigma. */
+void hko_qr(int nxb, int nc, double *V, double *C, double *D) {
+  for (int i = 0; i < nc; ++i) {
+    double *vi = V + (int64_t)nxb * i;
+    double scale = 0.0;
+    for (int k = i; k < nxb; ++k) scale = fmax(scale, fabs(vi[k]));
+    double ss = 0.0;
+    for (int k = i; k < nxb; ++k) {
+      double v = vi[k] / scale;
+      vi[k] = v;
+      ss = fma(v, v, ss);
+    }
+    double s = sqrt(ss);
+    double v0 = vi[i];
+    double sigma = (v0 < 0.0) ? -s : s;
+    vi[i] += sigma;
+    C[i] = sigma * (v0 + sigma);
+    D[i] = -scale * sigma;
+    for (int j = i + 1; j < nc; ++j) {
+      double *vj = V + (int64_t)nxb * j;
+      double dot = 0.0;
+      for (int k = i; k < nxb; ++k) dot = fma(vi[k], vj[k], dot);
+      double t = dot / C[i];
+      for (int k = i; k < nxb; ++k) vj[k] = fma(-t, vi[k], vj[k]);
+    }
+  }
+}
+
+static int cmp_double(const void *a, const void *b) {
+  double x = *(const double *)a, y = *(const double *)b;
+  return (x < y) ? -1 : (x > y);
+}
+
+/* heliosk.cu:2046-2051: sort_by_key(K, binKey) then
+ * stable_sort_by_key(binKey, K) == ascending K inside each bin segment. */
+void hko_sort_bins(int64_t nx, const int32_t *bin_index, int nbins, double *K) {
+  (void)nx;
+  for (int b = 0; b <= nbins; ++b) {
+    int64_t s = bin_index[b], e = bin_index[b + 1];
+    if (e > s) qsort(K + s, (size_t)(e - s), sizeof(double), cmp_double);
+  }
+}
+
+/* resample.h:362-388 (findCut_kernel), one pass over the state in index
+ * order.  Where the kernel's threads could race on one bin (the id == NL-3
+ * rule against a later transition), the later index wins here. */
+void hko_find_cut(const double *K, int64_t nx, int nxb, double kmin,
+                  int nbins, int32_t *nxmin) {
+  for (int b = 0; b < nbins; ++b) nxmin[b] = 0;
+  for (int64_t id = 0; id < nx - 1; ++id) {
+    int64_t ib = id / nxb;
+    if (ib >= nbins) break;
+    double k = K[id], k1 = K[id + 1];
+    if (k <= kmin && k1 > kmin) nxmin[ib] = (int32_t)(id - ib * nxb + 1);
+    if (k <= kmin && id % nxb == nxb - 1) nxmin[ib] = nxb;
+    if (k <= kmin && id == nx - 3) nxmin[ib] = nxb;
+  }
+}
+
+/* rescale_kernel f = +1 (resample.h:405-417) for one bin */
+static void rescale_fwd(const double *Kb, double *out, int nxb, int nxmin) {
+  for (int j = 0; j < nxb; ++j) {
+    double ii = fma(1.0 - nxmin / ((double)(nxb - 1)), (double)j, (double)nxmin);
+    if (ii >= nxb - 1) ii = 0.999999 * (nxb - 1);
+    int il = (int)(ii / ((double)nxb) * nxb);
+    double Kl = Kb[il], Kr = Kb[il + 1];
+    out[j] = fma(Kr - Kl, ii - il, Kl);
+  }
+}
+
+/* rescale_kernel f = -1 (resample.h:418-431) for one bin */
+static void rescale_inv(const double *Kb, double *out, int nxb, int nxmin,
+                        double kmin) {
+  for (int j = 0; j < nxb; ++j) {
+    double Ki = kmin;
+    if (j >= nxmin) {
+      double ii = (j - nxmin) / ((double)(nxb - nxmin - 1)) * (nxb - 1);
+      if (ii >= nxb - 1) ii = 0.999999 * (nxb - 1);
+      int il = (int)(ii / ((double)nxb) * nxb);
+      double Kl = Kb[il], Kr = Kb[il + 1];
+      Ki = fma(Kr - Kl, ii - il, Kl);
+    }
+    out[j] = Ki;
+  }
+}
+
+/* The post-sort chain of heliosk.cu:2139-2193 for one state:
+ * findCut -> rescale(+1) -> copyK2 -> lnK -> leastSquare -> coefficients,
+ * then (recon != NULL) expfx -> rescale(-1) -> copyK2.
+ * K is the per-bin sorted state (nx values) and is overwritten with ln K.
+ * leastSquare_kernel (resample.h:243-353) applies only the first nc-1
+ * Householder reflections and its back-substitution reduction keeps only
+ * the first 64 partial sums; both are restated. */
+void hko_kdist(double *K, int64_t nx, int nxb, int nbins, int nc, double kmin,
+               double unitScale, const double *V, const double *C,
+               const double *D, int32_t *nxmin, double *coeff, double *recon) {
+  hko_find_cut(K, nx, nxb, kmin, nbins, nxmin);
+  double *tmp = (double *)malloc((size_t)nxb * sizeof(double));
+  for (int b = 0; b < nbins; ++b) {
+    double *Kb = K + (int64_t)b * nxb;
+    if (nxmin[b] > 0) {
+      rescale_fwd(Kb, tmp, nxb, nxmin[b]);
+      memcpy(Kb, tmp, (size_t)nxb * sizeof(double));
+    }
+  }
+  for (int64_t i = 0; i < nx; ++i) K[i] = log(K[i] * unitScale);
+  int lim = nc < 64 ? nc : 64;
+  for (int b = 0; b < nbins; ++b) {
+    double *bb = K + (int64_t)b * nxb;
+    for (int j = 0; j < nc - 1; ++j) {
+      const double *vj = V + (int64_t)nxb * j;
+      double dot = 0.0;
+      for (int k = j; k < nxb; ++k) dot = fma(vj[k], bb[k], dot);
+      double t = dot / C[j];
+      for (int k = j; k < nxb; ++k) bb[k] = fma(-t, vj[k], bb[k]);
+    }
+    bb[nc - 1] /= D[nc - 1];
+    for (int i = nc - 2; i >= 0; --i) {
+      double s = 0.0;
+      for (int j = i + 1; j < lim; ++j) s = fma(V[i + (int64_t)nxb * j], bb[j], s);
+      bb[i] = (bb[i] - s) / D[i];
+    }
+    for (int i = 0; i < nc; ++i) coeff[(int64_t)b * nc + i] = bb[i];
+  }
+  if (recon) {
+    for (int b = 0; b < nbins; ++b) {
+      const double *cb = coeff + (int64_t)b * nc;
+      double *rb = recon + (int64_t)b * nxb;
+      /* expfx_kernel, resample.h:497-524 (x uses /Nxb, not /(Nxb-1)) */
+      for (int j = 0; j < nxb; ++j) {
+        double x = -1.0 + j * 2.0 / ((double)nxb);
+        double d1 = 0.0, d2 = 0.0;
+        for (int i = nc - 1; i >= 1; --i) {
+          double t = d1;
+          d1 = fma(2.0 * x, d1, -d2) + cb[i];
+          d2 = t;
+        }
+        double f = fma(x, d1, -d2) + 0.5 * cb[0] + 0.5 * cb[0];
+        rb[j] = exp(f) / unitScale;
+      }
+      if (nxmin[b] > 0) {
+        rescale_inv(rb, tmp, nxb, nxmin[b], kmin);
+        memcpy(rb, tmp, (size_t)nxb * sizeof(double));
+      }
+    }
+  }
+  free(tmp);
+}

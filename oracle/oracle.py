@@ -1,0 +1,246 @@
+"""ctypes wrapper of the FP64 CPU oracle (oracle/hk_oracle.c).
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py import this module, and only as the
+checker or as the timed CPU baseline.  The product path (libhkb, hkb) never
+imports it.
+
+Each wrapper names the reference file:line of the algorithm it restates; see
+oracle/hk_oracle.c for the restatement itself.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "build", "libhkoracle.so")
+_lib = None
+
+_d = C.c_double
+_i = C.c_int
+_i64 = C.c_int64
+_p = C.c_void_p
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (gcc, OpenMP, -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.hko_grid_x.restype = _d
+        L.hko_grid_x.argtypes = [_d, _d, _i64]
+        L.hko_grid_nx.restype = _i
+        L.hko_grid_nx.argtypes = [_d, _d, _d]
+        L.hko_grid_fill.argtypes = [_d, _d, _i64, _p]
+        L.hko_bin_keys.argtypes = [_d, _d, _d, _i64, _i, _p, _p]
+        L.hko_partition_interp.restype = _i
+        L.hko_partition_interp.argtypes = [_p, _p, _i, _d, _p]
+        L.hko_prep_hitran.argtypes = [_i64] + [_p] * 9 + [_i, _p, _p, _p] + [
+            _d, _d, _d, _d, _i, _d, _d] + [_p] * 4
+        L.hko_prep_exomol.argtypes = [_i64, _p, _p, _p, _p, _d, _d, _d, _d, _d,
+                                      _d, _d, _d, _i, _d, _d, _p, _p, _p, _p]
+        L.hko_windows.argtypes = [_i64, _p, _p, _p, _p, _d, _d, _i64, _i, _d, _p]
+        L.hko_erfcx.restype = _d
+        L.hko_erfcx.argtypes = [_d]
+        L.hko_voigt916.restype = _d
+        L.hko_voigt916.argtypes = [_d, _d]
+        L.hko_gh2.restype = _d
+        L.hko_gh2.argtypes = [_d, _d]
+        L.hko_opacity.argtypes = [_i64, _p, _p, _p, _p, _p, _d, _d, _i64, _i64,
+                                  _d, _p, _i, _p]
+        L.hko_vandermonde.argtypes = [_i, _i, _p]
+        L.hko_qr.argtypes = [_i, _i, _p, _p, _p]
+        L.hko_sort_bins.argtypes = [_i64, _p, _i, _p]
+        L.hko_find_cut.argtypes = [_p, _i64, _i, _d, _i, _p]
+        L.hko_kdist.argtypes = [_p, _i64, _i, _i, _i, _d, _d, _p, _p, _p, _p,
+                                _p, _p]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+# ------------------------------------------------------------------ grid
+
+def grid_nx(numin, numax, dnu) -> int:
+    """heliosk.cu:448-455."""
+    return int(lib().hko_grid_nx(numin, numax, dnu))
+
+
+def grid_x(numin, dnu, nx) -> np.ndarray:
+    """voigt.h:751-768 setX_kernel (x_i = fma(i, dnu, numin))."""
+    x = np.empty(nx, np.float64)
+    lib().hko_grid_fill(numin, dnu, nx, _ptr(x))
+    return x
+
+
+def bin_keys(numin, numax, dnu, nx, nbins):
+    """voigt.h:779-832 binKey_kernel + binIndex_kernel."""
+    key = np.empty(nx, np.int32)
+    idx = np.empty(nbins + 2, np.int32)
+    lib().hko_bin_keys(numin, numax, dnu, nx, nbins, _ptr(key), _ptr(idx))
+    return key, idx
+
+
+def partition(Tq, q, T) -> float:
+    """host.h:9-73 readPartition interpolation; raises on its error cases."""
+    Tq = _f64(Tq)
+    q = _f64(q)
+    out = np.zeros(1)
+    ok = lib().hko_partition_interp(_ptr(Tq), _ptr(q), len(Tq), T, _ptr(out))
+    if not ok:
+        raise ValueError(f"partition function not valid for T={T}")
+    return float(out[0])
+
+
+# ------------------------------------------------------------- line prep
+
+def prep_hitran(lines: dict, iso_mass, iso_ab, iso_Q, T, P, qalphaL=1.0,
+                gammaF=1.0, units=0, meanMass=None, Sscale=1.0):
+    """host.h:598-649 readFile + voigt.h:331-363 S2_kernel.
+
+    lines: dict of float64 arrays nu, S, EL, A, delta, gair, gself, n and an
+    int32 array iso (isotopologue index).  Returns (nu, S, ialphaD, vy).
+    """
+    n = len(lines["nu"])
+    iso_mass = _f64(iso_mass)
+    iso_ab = _f64(iso_ab)
+    iso_Q = _f64(iso_Q)
+    if meanMass is None:
+        meanMass = float(np.sum(iso_ab * iso_mass) * Sscale)
+    cols = [_f64(lines[k]) for k in ("nu", "S", "EL", "A", "delta", "gair",
+                                     "gself", "n")]
+    iso = np.ascontiguousarray(lines.get("iso", np.zeros(n, np.int32)),
+                               dtype=np.int32)
+    outs = [np.empty(n, np.float64) for _ in range(4)]
+    lib().hko_prep_hitran(n, *[_ptr(c) for c in cols], _ptr(iso), len(iso_mass),
+                          _ptr(iso_mass), _ptr(iso_ab), _ptr(iso_Q), T, P,
+                          qalphaL, gammaF, units, meanMass, Sscale,
+                          *[_ptr(o) for o in outs])
+    return tuple(outs)
+
+
+def prep_exomol(lines: dict, mass, ab, Q, defaultL, defaultn, T, P,
+                gammaF=1.0, units=0, meanMass=None, Sscale=1.0):
+    """voigt.h:484-504 L_kernelExomol + voigt.h:365-397 Sf_kernel."""
+    n = len(lines["nu"])
+    if meanMass is None:
+        meanMass = ab * mass * Sscale
+    cols = [_f64(lines[k]) for k in ("nu", "S", "EL", "A")]
+    outs = [np.empty(n, np.float64) for _ in range(4)]
+    lib().hko_prep_exomol(n, *[_ptr(c) for c in cols], mass, ab, Q, defaultL,
+                          defaultn, T, P, gammaF, units, meanMass, Sscale,
+                          *[_ptr(o) for o in outs])
+    return tuple(outs)
+
+
+def windows(nu, S, iad, vy, numin, dnu, nx, cutMode, cut) -> np.ndarray:
+    """Per-line index windows (n, 6): i0, b0, c0, c1, b1, i1.
+
+    Restates the region classes of voigt.h:2205-2341 and the per-pair
+    predicates of voigt.h:1223, 1481, 1662 as exact FP64 index ranges.
+    """
+    nu, S, iad, vy = map(_f64, (nu, S, iad, vy))
+    n = len(nu)
+    win = np.empty((n, 6), np.int64)
+    lib().hko_windows(n, _ptr(nu), _ptr(S), _ptr(iad), _ptr(vy), numin, dnu,
+                      nx, cutMode, cut, _ptr(win))
+    return win
+
+
+def erfcx(y: float) -> float:
+    return float(lib().hko_erfcx(y))
+
+
+def voigt916(x: float, y: float) -> float:
+    """voigt.h:278-300 voigt_916 (FP64, def_TOL)."""
+    return float(lib().hko_voigt916(x, y))
+
+
+def gh2(x: float, y: float) -> float:
+    """voigt.h:1481-1490 region-B rational (t4)."""
+    return float(lib().hko_gh2(x, y))
+
+
+def opacity(nu, S, iad, vy, win, numin, dnu, nx, kmin=0.0, nthreads=0,
+            irange=None):
+    """Line6fA/B/C + AddKStreams restated: K = kmin + sum of contributions.
+
+    irange=(ib, ie) evaluates only grid indices ib <= i < ie of the nx-point
+    grid.  Returns (K, pairs) with pairs = (A, B, C) pair counts.
+    """
+    nu, S, iad, vy = map(_f64, (nu, S, iad, vy))
+    win = np.ascontiguousarray(win, dtype=np.int64)
+    ib, ie = irange if irange is not None else (0, nx)
+    K = np.empty(ie - ib, np.float64)
+    pairs = np.zeros(3, np.int64)
+    lib().hko_opacity(len(nu), _ptr(nu), _ptr(S), _ptr(iad), _ptr(vy),
+                      _ptr(win), numin, dnu, ib, ie, kmin, _ptr(K), nthreads,
+                      _ptr(pairs))
+    return K, tuple(int(p) for p in pairs)
+
+
+# ---------------------------------------------------------- k-distribution
+
+def qr(nxb: int, nc: int):
+    """resample.h:14-37 Vandermonde + resample.h:73-227 QR_kernel."""
+    V = np.empty(nxb * nc, np.float64)
+    Cv = np.empty(nc, np.float64)
+    D = np.empty(nc, np.float64)
+    lib().hko_vandermonde(nxb, nc, _ptr(V))
+    lib().hko_qr(nxb, nc, _ptr(V), _ptr(Cv), _ptr(D))
+    return V, Cv, D
+
+
+def sort_bins(K, bin_index, nbins):
+    """heliosk.cu:2046-2051 per-bin ascending sort (returns a copy)."""
+    K = _f64(K).copy()
+    bi = np.ascontiguousarray(bin_index, dtype=np.int32)
+    lib().hko_sort_bins(len(K), _ptr(bi), nbins, _ptr(K))
+    return K
+
+
+def kdist(K_sorted, nxb, nbins, nc, kmin=0.0, unitScale=1.0, recon=False,
+          qr_mats=None):
+    """heliosk.cu:2139-2193 chain (findCut, rescale, lnK, leastSquare[, expfx]).
+
+    Returns (coeff[nbins, nc], nxmin[nbins], recon or None).
+    """
+    K = _f64(K_sorted).copy()
+    nx = len(K)
+    V, Cv, D = qr_mats if qr_mats is not None else qr(nxb, nc)
+    coeff = np.empty(nbins * nc, np.float64)
+    nxmin = np.empty(nbins, np.int32)
+    rec = np.empty(nx, np.float64) if recon else None
+    lib().hko_kdist(_ptr(K), nx, nxb, nbins, nc, kmin, unitScale, _ptr(V),
+                    _ptr(Cv), _ptr(D), _ptr(nxmin), _ptr(coeff), _ptr(rec))
+    return coeff.reshape(nbins, nc), nxmin, rec
+
+
+def state_opacity(lines, iso_mass, iso_ab, iso_Q, T, P, numin, numax, dnu,
+                  cutMode=0, cut=25.0, kmin=0.0, qalphaL=1.0, gammaF=1.0,
+                  nthreads=0):
+    """Whole forward path for one HITRAN-format state: prep, windows, sum."""
+    nx = grid_nx(numin, numax, dnu)
+    nu, S, iad, vy = prep_hitran(lines, iso_mass, iso_ab, iso_Q, T, P,
+                                 qalphaL=qalphaL, gammaF=gammaF)
+    win = windows(nu, S, iad, vy, numin, dnu, nx, cutMode, cut)
+    K, pairs = opacity(nu, S, iad, vy, win, numin, dnu, nx, kmin, nthreads)
+    return K, pairs, (nu, S, iad, vy, win)
