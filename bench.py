@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hitemp", choices=["hitemp", "small", "table"])
+    ap.add_argument("--workload", default="hitemp", choices=["hitemp", "small", "table", "hitemp_slice"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -61,13 +61,15 @@ def workload(name):
     else:
         W = dict(synth.WORKLOADS[name])
         W["label"] = {"hitemp": "hitemp-1e7-lines-single-state",
-                      "small": "small-1e5-lines-single-state"}[name]
+                      "small": "small-1e5-lines-single-state",
+                      "hitemp_slice": "hitemp-density-1e6-lines-3000cm-1-band"}[name]
     return W
 
 
 def make_lines(W):
     from hkb import synth
-    return synth.hitran_lines(W["n"], seed=W["seed"], logS=W["logS"])
+    return synth.hitran_lines(W["n"], seed=W["seed"], logS=W["logS"],
+                              nu_min=W.get("nu_min", 0.0), nu_max=W.get("nu_max", 30000.0))
 
 
 def open_ctx(W, L, device):

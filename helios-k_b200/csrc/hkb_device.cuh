@@ -270,51 +270,106 @@ static __device__ __noinline__ double voigt916_d(double x, double y, double ey) 
   return t1;
 }
 
-// Algorithm 916 in FP32 with def_TOLF (the series of voigt.h:217-268,
-// Sigmabf, and the region-C formula of voigt.h:1662-1682).  Differences
-// from the reference's FP32 kernel: the argument x arrives with FP32
-// relative accuracy (the offset is formed from a double-float split, not
-// from (numin - nu)/alphaD rounded to float), and erfcx(y) is a per-line
-// constant computed in FP64.
-static __device__ __noinline__ float voigt916_f(float x, float y, float ey) {
+// ------------------------------------------- region C, recurrence form
+// Algorithm 916 in FP32 (the series of voigt.h:217-268, Sigmabf, and the
+// region-C formula of voigt.h:1662-1682, with a from def_TOLF).  Unlike the
+// reference's FP32 kernel, x arrives with FP32 relative accuracy (formed
+// from a double-float split of the FP64 offset, not from (numin - nu)/alphaD
+// rounded to float) and erfcx(y) is a per-line FP64 constant.  The series
+// are rearranged for FP32 throughput:
+//   s1 = sum_m R_m exp(-(a^2 m^2 + x^2)) = exp(-x^2) * Sig1(y),
+//        Sig1(y) = sum_m exp(-a^2 m^2) R_m  -- a per-line constant;
+//   s3 = sum_{m>=1} R_m exp(-(a m - x)^2),  s2 = sum_{m>=1} R_m exp(-(a m + x)^2),
+//        R_m = 1 / (a^2 m^2 + y^2).
+// The Gaussians of s3 are generated from the centre m_c = rint(x/a) outwards
+// with the exact ratio exp(-(a(m+1)-x)^2) / exp(-(a m - x)^2)
+//   = exp(-a^2 (2m+1) + 2 a x), itself advanced by the constant exp(-2 a^2):
+// three exps instead of one per term.  HK_C916_K terms each side reach
+// |a m - x| >= 4.8, where the Gaussian is below 1e-10 of the centre term,
+// so the trip counts are fixed (no data-dependent convergence loop).
+constexpr int HK_C916_K = 8;
+
+// rcp.approx.ftz.f32: maximum error 1 ulp (PTX ISA), one XU instruction
+__device__ __forceinline__ float rcp_fast(float v) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
+
+// per-line constant Sig1(y), FP64 at staging
+__device__ __forceinline__ double c916_sig1(double y) {
+  const double a = (double)HK_A916_F;
+  const double y2 = y * y;
+  double s = 0.0;
+  for (int m = 1; m <= 12; ++m) {
+    const double am2 = a * a * m * m;
+    s += exp(-am2) / (am2 + y2);
+  }
+  return s;
+}
+
+static __device__ __noinline__ float voigt916_rf(float x, float y, float y2, float ey,
+                                                 float sig1) {
   const float a = HK_A916_F;
-  const float cc = HK_C916_F;  // 2a/pi
-  float s1 = 0.f, s2 = 0.f, s3 = 0.f;
+  const float a2 = a * a;
+  const float G = 0.48675662279129028f;  // exp(-2 a^2)
   x = fabsf(x);
   const float ex2 = expf(-x * x);
-  if (x != 0.f && y != 0.f) {
-    float o1 = 0.f, o2 = 0.f, o3 = 0.f;
-    const float yy = y * y;
-    const int n0 = (int)ceilf(x / a);
-    bool st1 = false, st2 = false, st3 = false;
-    for (int n = 1; n < 100; ++n) {
-      const int n3p = n0 + n - 1, n3n = n0 - n;
-      const float an = a * n, an3p = a * n3p, an3n = a * n3n;
-      const float f = 1.0f / (an * an + yy);
-      const float f3p = 1.0f / (an3p * an3p + yy);
-      const float f3n = 1.0f / (an3n * an3n + yy);
-      s1 += f * expf(-(an * an + x * x));
-      s2 += f * expf(-(an + x) * (an + x));
-      s3 += f3p * expf(-(an3p - x) * (an3p - x));
-      if (n3n >= 1) s3 += f3n * expf(-(an3n - x) * (an3n - x));
-      if (fabsf(s1 - o1) < HK_TOLF) st1 = true;
-      if (fabsf(s2 - o2) < HK_TOLF) st2 = true;
-      if (fabsf(s3 - o3) < HK_TOLF) st3 = true;
-      if (st1 && st2 && st3) break;
-      o1 = s1;
-      o2 = s2;
-      o3 = s3;
+  float t1;
+  if (x == 0.f) {
+    t1 = ey;
+  } else if (y == 0.f) {
+    t1 = ex2;
+  } else {
+    // s3: centre term and the two geometric ratios
+    const float mcf = fmaxf(1.0f, rintf(x * (1.0f / a)));
+    const float d = fmaf(a, mcf, -x);
+    const float Tc = expf(-d * d);
+    const float up0 = expf(fmaf(-a2, fmaf(2.0f, mcf, 1.0f), 2.0f * a * x));   // ratio m_c -> m_c+1
+    const float dn0 = expf(fmaf(a2, fmaf(2.0f, mcf, -1.0f), -2.0f * a * x));  // ratio m_c -> m_c-1
+    float s3 = Tc * rcp_fast(fmaf(a2 * mcf, mcf, y2));
+    float T = Tc, q = up0, m = mcf;
+#pragma unroll
+    for (int k = 0; k < HK_C916_K; ++k) {
+      T *= q;
+      q *= G;
+      m += 1.0f;
+      s3 = fmaf(T, rcp_fast(fmaf(a2 * m, m, y2)), s3);
     }
+    T = Tc;
+    q = dn0;
+    m = mcf;
+#pragma unroll
+    for (int k = 0; k < HK_C916_K; ++k) {
+      T *= q;
+      q *= G;
+      m -= 1.0f;
+      if (m >= 1.0f) s3 = fmaf(T, rcp_fast(fmaf(a2 * m, m, y2)), s3);
+    }
+    // s2: only within ~4.8 of the origin does exp(-(a m + x)^2) matter
+    float s2 = 0.f;
+    if (x < 4.8f) {
+      float T2 = expf(-(a + x) * (a + x));
+      float q2 = expf(fmaf(-3.0f, a2, -2.0f * a * x));
+      float m2 = 1.0f;
+#pragma unroll
+      for (int k = 0; k < HK_C916_K; ++k) {
+        s2 = fmaf(T2, rcp_fast(fmaf(a2 * m2, m2, y2)), s2);
+        T2 *= q2;
+        q2 *= G;
+        m2 += 1.0f;
+      }
+    }
+    const float s1 = ex2 * sig1;
+    const float xy = x * y;
+    float sinxy, cosxy;
+    sincosf(xy, &sinxy, &cosxy);
+    const float cos2xy = fmaf(-2.0f * sinxy, sinxy, 1.0f);
+    t1 = ex2 * ey * cos2xy;
+    const float t2 = sinxy * ex2 * sinxy / y;
+    const float t3 = y * (-cos2xy * s1 + 0.5f * (s2 + s3));
+    t1 += HK_C916_F * (t2 + t3);
   }
-  const float xy = x * y;
-  const float cos2xy = cosf(2.0f * xy);
-  const float sinxy = sinf(xy);
-  float t1 = ex2 * ey * cos2xy;
-  const float t2 = sinxy * ex2 * sinxy / y;
-  const float t3 = y * (-cos2xy * s1 + 0.5f * (s2 + s3));
-  t1 += cc * (t2 + t3);
-  if (x == 0.f) t1 = ey;
-  if (y == 0.f) t1 = ex2;
   return t1;
 }
 

@@ -13,8 +13,9 @@
 //   3. lets each warp sweep its 256-point slice against every staged line:
 //      lane-interleaved points (coalesced stores), register accumulators.
 // Two precisions share the structure:
-//   MIXED: FP32 profile + Kahan-compensated FP32 sums; the offset x is formed
-//          from a double-float split of the FP64 line-centre offset.
+//   MIXED: FP32 profile (the offset x from a double-float split of the FP64
+//          line-centre offset; region formulas in FP32), strength multiply
+//          and grid sum as one FP64 FMA per pair.
 //   PLAIN: FP64 everywhere (the "plain FP64 form" used as the GPU baseline).
 // Reference: Line6fA/B/C kernels voigt.h:1177-1816 and their launchers
 // Line6A_Call/Line6B_Call/Line6C_Call voigt.h:1820-2036.
@@ -41,7 +42,9 @@ struct __align__(16) RecF {
   float y2, y, ey;         // y^2, y, erfcx(y)
   int i0;                  // tile-local window boundaries
   int b0, c0, c1, b1;
-  int i1, p0, p1, p2;
+  int i1;
+  float sig1;              // region-C series constant Sig1(y)
+  int p1, p2;
 };
 
 struct __align__(16) RecD {
@@ -125,7 +128,8 @@ __device__ __forceinline__ void stage_line(const LinesDev &L, const GridDev &g,
     r.c1 = li[3];
     r.b1 = li[4];
     r.i1 = nonempty ? li[5] : 0;
-    r.p0 = r.p1 = r.p2 = 0;
+    r.sig1 = hasC ? (float)c916_sig1(ls.vy) : 0.f;
+    r.p1 = r.p2 = 0;
     *reinterpret_cast<RecF *>(recp) = r;
   } else {
     RecD r;
@@ -189,7 +193,7 @@ __device__ __forceinline__ void sweep_mixed(const RecF &r, int wb, int lane,
       if (k >= r.i0 && k < r.i1) {
         const float x = fmaf(kf[p], r.vbh, r.dh) + fmaf(kf[p], r.vbl, r.dl);
         if (k >= r.c0 && k < r.c1) {
-          acc[p] = fma(r.Sc, (double)voigt916_f(x, r.y, r.ey), acc[p]);
+          acc[p] = fma(r.Sc, (double)voigt916_rf(x, r.y, r.y2, r.ey, r.sig1), acc[p]);
         } else {
           const float s = x * x;
           const float u = s + r.y2;
@@ -287,9 +291,16 @@ voigt_sum_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
       else xg[p] = grid_x(g, g0 + k);
     }
 
-    for (int64_t c0 = L0; c0 < L1; c0 += HK_CH) {
-      const int cnt = (int)min((int64_t)HK_CH, L1 - c0);
-      if (tid < cnt) stage_line<MIXED>(L, g, st, c0 + tid, g0, g1, &rec[tid]);
+    // Chunk c holds the lines L0 + c + q*nch (q < HK_CH): every chunk spans
+    // the tile's whole line range, so the costly region-C points of its
+    // lines fall into all warp slices instead of one or two (consecutive
+    // nu-sorted lines would put a chunk's line cores into a single slice
+    // and leave the other warps idle at the barrier).
+    const int64_t nL = L1 - L0;
+    const int64_t nch = (nL + HK_CH - 1) / HK_CH;
+    for (int64_t c = 0; c < nch; ++c) {
+      const int cnt = (int)((nL - c + nch - 1) / nch);
+      if (tid < cnt) stage_line<MIXED>(L, g, st, L0 + c + (int64_t)tid * nch, g0, g1, &rec[tid]);
       __syncthreads();
       for (int j = 0; j < cnt; ++j) {
         if (MIXED) sweep_mixed(reinterpret_cast<const RecF &>(rec[j]), wb, lane, kf, acc);
@@ -329,7 +340,9 @@ __global__ void profile_eval_kernel(int64_t n, const double *__restrict__ x,
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double ey = erfcx(y[i]);
-  if (mixed) out[i] = (double)voigt916_f((float)x[i], (float)y[i], (float)ey);
+  if (mixed)
+    out[i] = (double)voigt916_rf((float)x[i], (float)y[i], (float)(y[i] * y[i]), (float)ey,
+                                 (float)c916_sig1(y[i]));
   else out[i] = voigt916_d(x[i], y[i], ey);
 }
 

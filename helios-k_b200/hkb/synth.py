@@ -39,10 +39,11 @@ def q_table():
     return T, q_of_T(T)
 
 
-def hitran_lines(n, seed=0, logS=(-30.0, -18.0), nu_max=30000.0, E_mean=3000.0):
+def hitran_lines(n, seed=0, logS=(-30.0, -18.0), nu_max=30000.0, E_mean=3000.0,
+                 nu_min=0.0):
     """Line dict (nu, S_file, EL, A, delta, gair, gself, n, iso) in file units."""
     rng = np.random.default_rng(seed)
-    nu = rng.uniform(0.0, nu_max, n)
+    nu = rng.uniform(nu_min, nu_max, n)
     S296 = 10.0 ** rng.uniform(logS[0], logS[1], n)
     EL = rng.exponential(E_mean, n)
     gair = rng.uniform(0.01, 0.1, n)
@@ -71,6 +72,11 @@ WORKLOADS = {
                    numin=0.0, numax=30000.0, dnu=0.01, cut=25.0, nbins=300, nC=20),
     "adjoint": dict(n=1_000_000, seed=3, logS=(-30.0, -18.0), T=[800.0], P=[1.0],
                     numin=1000.0, numax=10000.0, dnu=0.01, cut=100.0, nbins=300, nC=20),
+    # a 3000 cm^-1 band of the hitemp list at the same line density (used
+    # for profiler captures: same per-pair mix, 1/10 of the work)
+    "hitemp_slice": dict(n=1_000_000, seed=1, logS=(-32.0, -18.0), T=[1500.0], P=[0.1],
+                         numin=15000.0, numax=18000.0, dnu=0.01, cut=25.0, nbins=30, nC=20,
+                         nu_min=15000.0, nu_max=18000.0),
 }
 
 
