@@ -61,7 +61,9 @@ struct hk_ctx {
   int nbins = 0, nxb = 0;
   double kmin = 0.0;
   // workspace
-  DevBuf states, ticket, maxexp, wbits, Kwork, outwork, scratch;
+  DevBuf states, ticket, wbits, Kwork, outwork, scratch, prep;
+  size_t prep_budget = (size_t)24 << 30;  // bytes of per-(state, line) records per batch
+  double voigt_ms_acc = 0.0;
   DevBuf qrV, qrC, qrD;
   int qr_nxb = -1, qr_nc = -1;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -124,7 +126,7 @@ void hk_destroy(hk_ctx *c) {
   cudaSetDevice(c->device);
   for (DevBuf *b : {&c->nu0, &c->Sfile, &c->EL, &c->gam, &c->nexp, &c->delta,
                     &c->Aterm, &c->iso, &c->order, &c->states, &c->ticket,
-                    &c->maxexp, &c->wbits, &c->Kwork, &c->outwork, &c->scratch,
+                    &c->prep, &c->wbits, &c->Kwork, &c->outwork, &c->scratch,
                     &c->qrV, &c->qrC, &c->qrD})
     b->release();
   for (auto &e : c->ev)
@@ -374,8 +376,6 @@ static hk_status build_states(hk_ctx *c, int nstates, const double *T, const dou
     st.PoverP0 = (c->database == HK_DB_HITRAN) ? Ps / HK_PO_ATM : Ps / HK_PO_BAR;
     st.powbase = HK_T0 / Ts;
     st.c1 = HK_H * HK_C / (HK_KB * Ts);
-    st.scale = 1.0;
-    st.inv_scale = 1.0;
     st.wmax = c->g.cut;
     st.shift = c->max_abs_delta * Ps;
     st.kmin = c->kmin;
@@ -420,7 +420,6 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   std::vector<StateDev> hs;
   if ((st = build_states(c, nstates, T, P, hs)) != HK_OK) return st;
   CUDA_TRY(c, c->states.ensure(nstates * sizeof(StateDev)));
-  CUDA_TRY(c, c->maxexp.ensure(nstates * sizeof(int)));
   CUDA_TRY(c, c->wbits.ensure(nstates * sizeof(unsigned long long)));
   CUDA_TRY(c, cudaMemcpyAsync(c->states.p, hs.data(), nstates * sizeof(StateDev), cudaMemcpyHostToDevice, s));
   const int64_t nx = c->g.nx;
@@ -429,18 +428,34 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
     CUDA_TRY(c, c->Kwork.ensure((size_t)nstates * nx * sizeof(double)));
     Kd = c->Kwork.as<double>();
   }
-  CUDA_TRY(c, launch_state_prepass(c->L, c->g, c->states.as<StateDev>(), nstates,
-                                   c->maxexp.as<int>(), c->wbits.as<unsigned long long>(), s));
-  if (precision == HK_PRECISION_PLAIN_FP64) {
-    // the plain form computes in FP64 with unit scale
-    // (prepass also sets wmax, which the plain form needs too)
+  // States run in batches whose per-(state, line) records fit the prep
+  // budget; each batch is one prep launch and one persistent Voigt launch.
+  const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * sizeof(LinePrep);
+  int batch = (int)std::max<size_t>(1, c->prep_budget / per_state);
+  batch = std::min(batch, nstates);
+  CUDA_TRY(c, c->prep.ensure((size_t)batch * per_state));
+  StateDev *sd = c->states.as<StateDev>();
+  unsigned long long *wb = c->wbits.as<unsigned long long>();
+  c->voigt_ms_acc = 0.0;
+  c->have_voigt_t = false;
+  for (int b0 = 0; b0 < nstates; b0 += batch) {
+    const int nb = std::min(batch, nstates - b0);
+    CUDA_TRY(c, launch_line_prep(c->L, c->g, sd + b0, nb, c->prep.as<LinePrep>(), wb + b0, s));
+    CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
+    CUDA_TRY(c, launch_voigt_sum(precision == HK_PRECISION_MIXED, c->prep.as<LinePrep>(),
+                                 c->L.nu0, c->nlines, c->g, sd + b0, nb, c->ticket.as<unsigned>(),
+                                 Kd + (size_t)b0 * nx, nx, 0, s));
+    CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
+    c->have_voigt_t = true;
+    if (b0 + nb < nstates) {
+      // accumulate the Voigt time of earlier batches (the last one is read
+      // lazily by hk_last_timing)
+      float ms = 0.f;
+      CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
+      CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+      c->voigt_ms_acc += ms;
+    }
   }
-  CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
-  CUDA_TRY(c, launch_voigt_sum(precision == HK_PRECISION_MIXED, c->L, c->g,
-                               c->states.as<StateDev>(), nstates, c->ticket.as<unsigned>(),
-                               Kd, nx, 0, s));
-  CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
-  c->have_voigt_t = true;
   if (!K_on_device) {
     CUDA_TRY(c, cudaMemcpyAsync(K_out, Kd, (size_t)nstates * nx * sizeof(double), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(c, cudaStreamSynchronize(s));
@@ -590,7 +605,7 @@ hk_status hk_last_timing(const hk_ctx *c, double *voigt_ms, double *kdist_ms) {
     *voigt_ms = -1.0;
     if (c->have_voigt_t && cudaEventSynchronize(c->ev[1]) == cudaSuccess &&
         cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]) == cudaSuccess)
-      *voigt_ms = ms;
+      *voigt_ms = c->voigt_ms_acc + ms;
   }
   if (kdist_ms) {
     *kdist_ms = -1.0;

@@ -17,14 +17,13 @@ constexpr int KD_SMEM_LIMIT = 225 * 1024;
 int voigt_tile_points();
 cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream);
 
-cudaError_t launch_state_prepass(const LinesDev &L, const GridDev &g,
-                                 StateDev *states_d, int nstates,
-                                 int *maxexp_d, unsigned long long *wbits_d,
-                                 cudaStream_t stream);
+cudaError_t launch_line_prep(const LinesDev &L, const GridDev &g, StateDev *states_d,
+                             int nstates, LinePrep *prep_d, unsigned long long *wbits_d,
+                             cudaStream_t stream);
 
-cudaError_t launch_voigt_sum(bool mixed, const LinesDev &L, const GridDev &g,
-                             const StateDev *states_d, int nstates,
-                             unsigned *ticket_d, double *K_d, int64_t k_stride,
+cudaError_t launch_voigt_sum(bool mixed, const LinePrep *prep_d, const double *nu0_d,
+                             int64_t nlines, const GridDev &g, const StateDev *states_d,
+                             int nstates, unsigned *ticket_d, double *K_d, int64_t k_stride,
                              int grid_ctas, cudaStream_t stream);
 
 cudaError_t launch_prep_dump(const LinesDev &L, const GridDev &g,

@@ -1,10 +1,13 @@
-// hkb_lines.cu -- line-list residency and per-state pre-pass (sm_100a).
+// hkb_lines.cu -- line-list residency and the per-state line prep (sm_100a).
 //
 // The reference sorts every 2^20-line part by nu for every pressure
-// (heliosk.cu:1147-1171: thrust::sort_by_key + six gather kernels).  Here the
-// list is sorted once at load (CUB radix sort on the FP64 centres, one gather
-// per column) and stays resident in HBM; the per-state pressure shift is
-// absorbed by widening each tile's line search by max|delta| P.
+// (heliosk.cu:1147-1171: thrust::sort_by_key + six gather kernels) and
+// rescales it with S2_kernel/S3_kernel (voigt.h:331-482).  Here the list is
+// sorted once at load (CUB radix sort on the FP64 centres, one gather per
+// column) and stays resident in HBM; line_prep_kernel then scales every line
+// to every state of a batch in FP64 and computes its exact index windows,
+// one thread per (line, state).  The per-state pressure shift is absorbed by
+// widening each tile's line search by max|delta| P.
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
@@ -65,46 +68,56 @@ cudaError_t sort_lines_by_nu(int64_t n, double *nu_d, int64_t *order_d,
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
-// Per state: the exponent of the largest scaled strength (sets the power of
-// two that keeps the FP32 strengths in range) and, for cutMode 1/2, the
-// largest cutoff half-width in cm^-1 (bounds each tile's line search).
-__global__ void state_prepass_kernel(LinesDev L, GridDev g,
-                                     const StateDev *__restrict__ states,
-                                     int *__restrict__ maxexp,
-                                     unsigned long long *__restrict__ wbits) {
+// One thread per (line, state): FP64 scaling (prep_line), the global index
+// windows (line_windows over [0, Nx)), and the region-C per-line constants
+// erfcx(y) and Sig1(y) for lines that have a region-C window.  For cutMode
+// 1/2 it also bounds the state's largest cutoff half-width (cm^-1), which
+// sizes each tile's line search.
+__global__ void __launch_bounds__(256)
+line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
+                 LinePrep *__restrict__ out, unsigned long long *__restrict__ wbits) {
   const int s = blockIdx.y;
   const StateDev &st = states[s];
-  int e_loc = INT_MIN;
+  LinePrep *O = out + (int64_t)s * L.n;
   double w_loc = 0.0;
   for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < L.n;
        l += (int64_t)gridDim.x * blockDim.x) {
     const LineState ls = prep_line(L, st, l);
-    if (ls.S > 0.0 && ls.iad > 0.0) {
-      e_loc = max(e_loc, ilogb(ls.S));
+    int64_t w[6];
+    line_windows(g, st, ls, 0, g.nx, w);
+    LinePrep r;
+    r.nu = ls.nu;
+    r.iad = ls.iad;
+    r.vy = ls.vy;
+    r.S1 = ls.S * ls.vy / CUDART_PI;
+    r.Sc = ls.S * (1.0 / 1.7724538509055160273);
+    const bool hasC = w[3] > w[2];
+    r.ey = hasC ? erfcx(ls.vy) : 1.0;
+    r.sig1 = hasC ? (float)c916_sig1(ls.vy) : 0.f;
+    r.i0 = (int)w[0];
+    r.b0 = (int)w[1];
+    r.c0 = (int)w[2];
+    r.c1 = (int)w[3];
+    r.b1 = (int)w[4];
+    r.i1 = (int)w[5];
+    r.pad = 0;
+    O[l] = r;
+    if (ls.S != 0.0 && ls.iad > 0.0) {
       if (g.cutMode == 1) w_loc = fmax(w_loc, g.cut * ls.vy / ls.iad);
       else if (g.cutMode == 2) w_loc = fmax(w_loc, g.cut / ls.iad);
     }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    e_loc = max(e_loc, __shfl_xor_sync(0xffffffffu, e_loc, o));
-    w_loc = fmax(w_loc, __shfl_xor_sync(0xffffffffu, w_loc, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomicMax(&maxexp[s], e_loc);
-    atomicMax(&wbits[s], (unsigned long long)__double_as_longlong(w_loc));
+  if (g.cutMode != 0) {
+    for (int o = 16; o > 0; o >>= 1) w_loc = fmax(w_loc, __shfl_xor_sync(0xffffffffu, w_loc, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&wbits[s], (unsigned long long)__double_as_longlong(w_loc));
   }
 }
 
 __global__ void state_finalize_kernel(GridDev g, StateDev *__restrict__ states,
-                                      int nstates, const int *__restrict__ maxexp,
+                                      int nstates,
                                       const unsigned long long *__restrict__ wbits) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nstates) return;
-  int e = maxexp[s];
-  if (e < -900) e = 0;  // no line with S > 0
-  if (e > 900) e = 900;
-  states[s].scale = ldexp(1.0, -e);
-  states[s].inv_scale = ldexp(1.0, e);
   if (g.cutMode == 0) {
     states[s].wmax = g.cut;
   } else {
@@ -113,23 +126,46 @@ __global__ void state_finalize_kernel(GridDev g, StateDev *__restrict__ states,
   }
 }
 
-cudaError_t launch_state_prepass(const LinesDev &L, const GridDev &g,
-                                 StateDev *states_d, int nstates,
-                                 int *maxexp_d, unsigned long long *wbits_d,
-                                 cudaStream_t stream) {
-  cudaError_t e = cudaMemsetAsync(maxexp_d, 0x80, nstates * sizeof(int), stream);
-  if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(wbits_d, 0, nstates * sizeof(unsigned long long), stream);
+cudaError_t launch_line_prep(const LinesDev &L, const GridDev &g, StateDev *states_d,
+                             int nstates, LinePrep *prep_d, unsigned long long *wbits_d,
+                             cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(wbits_d, 0, nstates * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return e;
   if (L.n > 0) {
     const int64_t nb = (L.n + 255) / 256;
-    const int bx = (int)(nb < 1184 ? nb : 1184);
+    const int bx = (int)(nb < 2368 ? nb : 2368);
     dim3 grid(bx, nstates);
-    state_prepass_kernel<<<grid, 256, 0, stream>>>(L, g, states_d, maxexp_d, wbits_d);
+    line_prep_kernel<<<grid, 256, 0, stream>>>(L, g, states_d, prep_d, wbits_d);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  state_finalize_kernel<<<(nstates + 127) / 128, 128, 0, stream>>>(g, states_d, nstates, maxexp_d, wbits_d);
+  state_finalize_kernel<<<(nstates + 127) / 128, 128, 0, stream>>>(g, states_d, nstates, wbits_d);
+  return cudaGetLastError();
+}
+
+// Diagnostics: per-line state and global windows with the exact FP64 S.
+__global__ void prep_dump_kernel(LinesDev L, GridDev g, StateDev st,
+                                 double *__restrict__ out4,
+                                 long long *__restrict__ win6) {
+  const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= L.n) return;
+  const LineState ls = prep_line(L, st, l);
+  out4[4 * l + 0] = ls.nu;
+  out4[4 * l + 1] = ls.S;
+  out4[4 * l + 2] = ls.iad;
+  out4[4 * l + 3] = ls.vy;
+  int64_t w[6];
+  line_windows(g, st, ls, 0, g.nx, w);
+  for (int k = 0; k < 6; ++k) win6[6 * l + k] = w[k];
+}
+
+cudaError_t launch_prep_dump(const LinesDev &L, const GridDev &g,
+                             const StateDev &st, double *out4_d,
+                             long long *win6_d, cudaStream_t stream) {
+  if (L.n == 0) return cudaSuccess;
+  const int b = 128;
+  const int64_t nb = (L.n + b - 1) / b;
+  prep_dump_kernel<<<(unsigned)nb, b, 0, stream>>>(L, g, st, out4_d, win6_d);
   return cudaGetLastError();
 }
 

@@ -49,13 +49,26 @@ struct GridDev {
   double cut;  // 1e30 when the parameter file says 0 (heliosk.cu:947)
 };
 
+// One line scaled to one state, as written by line_prep_kernel and read by
+// the Voigt sum (80 bytes; FP64 parameters, global index windows).
+struct __align__(16) LinePrep {
+  double nu;    // centre after the pressure shift
+  double iad;   // 1 / alphaD
+  double vy;    // gammaL / alphaD
+  double S1;    // S * vy / pi      (regions A, B)
+  double Sc;    // S / sqrt(pi)     (region C)
+  double ey;    // erfcx(vy)        (lines with a region-C window)
+  int i0, b0, c0, c1, b1, i1;  // [i0,b0) A [b0,c0) B [c0,c1) C [c1,b1) B [b1,i1) A
+  float sig1;   // region-C series constant Sig1(vy)
+  int pad;
+};
+
 // Per-(T, P) constants formed on the host.
 struct StateDev {
   double T, P;
   double PoverP0;  // P / 1 atm (HITRAN) or P / 1 bar in atm (ExoMol)
   double powbase;  // T0 / T
   double c1;       // h c / (kB T)   (ExoMol strength)
-  double scale, inv_scale;  // power of two applied to FP32 strengths
   double wmax;     // upper bound of the cutoff half-width over lines (cm^-1)
   double shift;    // upper bound of |delta| * P
   double kmin;

@@ -5,11 +5,12 @@
 // writer: there are no atomics on K and no partial-row reduction (the
 // reference's 32 KS_d rows + AddKStreams_kernel, voigt.h:728-742, are gone).
 // For its tile the CTA
-//   1. finds the ν-sorted line range whose cutoff windows can reach the tile
+//   1. finds the nu-sorted line range whose cutoff windows can reach the tile
 //      (warp-parallel lower_bound),
 //   2. stages the lines in chunks of HK_CH through shared memory: each thread
-//      scales one line to the state in FP64 (prep_line) and computes the
-//      exact window/region index boundaries clipped to the tile,
+//      loads one line's state record (FP64 parameters and global index
+//      windows, written by line_prep_kernel), clips the windows to the tile
+//      and forms the line-centre offset at the tile start,
 //   3. lets each warp sweep its 256-point slice against every staged line:
 //      lane-interleaved points (coalesced stores), register accumulators.
 // Two precisions share the structure:
@@ -22,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <type_traits>
 
 #include "hkb_device.cuh"
 #include "hkb_kernels.h"
@@ -39,24 +41,15 @@ static_assert(HK_G <= 2048, "k * vb_hi must stay exact in FP32 (11 bits)");
 struct __align__(16) RecF {
   float dh, dl, vbh, vbl;  // x at the tile start (hi, lo), x step (hi, lo)
   double S1, Sc;           // S*y/pi (regions A, B), S/sqrt(pi) (region C)
-  float y2, y, ey;         // y^2, y, erfcx(y)
-  int i0;                  // tile-local window boundaries
-  int b0, c0, c1, b1;
-  int i1;
-  float sig1;              // region-C series constant Sig1(y)
-  int p1, p2;
+  float y2, y, ey, sig1;   // y^2, y, erfcx(y), region-C series constant
+  int i0, b0, c0, c1;      // tile-local window boundaries
+  int b1, i1, p0, p1;
 };
 
 struct __align__(16) RecD {
   double nu, iad, y2, y, S1, Sc, ey, pad;
   int i0, b0, c0, c1, b1, i1, p0, p1;
 };
-
-__device__ __forceinline__ float rcp_approx(float v) {
-  float r;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
-  return r;
-}
 
 // Exact widening of a positive normal float to double with integer ops
 // (keeps the conversion off the XU pipe that rcp.approx already uses).
@@ -93,53 +86,55 @@ __device__ int64_t lower_bound_warp(const double *__restrict__ a, int64_t n,
   return lo + __popc(m);
 }
 
-// Scale line l to the state, compute its tile-local windows and fill the
-// staged record.  Returns nothing; an empty window is i0 == i1 == 0.
+__device__ __forceinline__ int clip_local(int w, int64_t g0, int64_t g1) {
+  const int64_t v = (int64_t)w < g0 ? g0 : ((int64_t)w > g1 ? g1 : (int64_t)w);
+  return (int)(v - g0);
+}
+
+// Clip one line's global windows to the tile [g0, g1) and fill the staged
+// record.  Clipping the oracle's global boundaries equals searching the
+// clipped range, because every window predicate is monotone on its range.
 template <bool MIXED>
-__device__ __forceinline__ void stage_line(const LinesDev &L, const GridDev &g,
-                                           const StateDev &st, int64_t l,
+__device__ __forceinline__ void stage_line(const LinePrep *__restrict__ P,
+                                           const GridDev &g, int64_t l,
                                            int64_t g0, int64_t g1, void *recp) {
-  const LineState ls = prep_line(L, st, l);
-  int64_t w[6];
-  line_windows(g, st, ls, g0, g1, w);
-  int li[6];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) li[k] = (int)(w[k] - g0);
+  const LinePrep lp = P[l];
+  int li[6] = {clip_local(lp.i0, g0, g1), clip_local(lp.b0, g0, g1),
+               clip_local(lp.c0, g0, g1), clip_local(lp.c1, g0, g1),
+               clip_local(lp.b1, g0, g1), clip_local(lp.i1, g0, g1)};
   const bool nonempty = li[5] > li[0];
-  const bool hasC = li[3] > li[2];
-  const double ey = hasC ? erfcx(ls.vy) : 1.0;
   if (MIXED) {
     RecF r;
-    const double D0 = __dmul_rn(__dsub_rn(grid_x(g, g0), ls.nu), ls.iad);
-    const double vb = __dmul_rn(g.dnu, ls.iad);
+    const double D0 = __dmul_rn(__dsub_rn(grid_x(g, g0), lp.nu), lp.iad);
+    const double vb = __dmul_rn(g.dnu, lp.iad);
     r.dh = (float)D0;
     r.dl = (float)(D0 - (double)r.dh);
     const float vbf = (float)vb;
     r.vbh = __uint_as_float(__float_as_uint(vbf) & 0xFFFFF800u);  // 13 bits
     r.vbl = (float)(vb - (double)r.vbh);
-    r.y = (float)ls.vy;
-    r.y2 = (float)(ls.vy * ls.vy);
-    r.S1 = ls.S * ls.vy / CUDART_PI;
-    r.Sc = ls.S * (1.0 / 1.7724538509055160273);
-    r.ey = (float)ey;
+    r.y = (float)lp.vy;
+    r.y2 = (float)(lp.vy * lp.vy);
+    r.S1 = lp.S1;
+    r.Sc = lp.Sc;
+    r.ey = (float)lp.ey;
+    r.sig1 = lp.sig1;
     r.i0 = nonempty ? li[0] : 0;
     r.b0 = li[1];
     r.c0 = li[2];
     r.c1 = li[3];
     r.b1 = li[4];
     r.i1 = nonempty ? li[5] : 0;
-    r.sig1 = hasC ? (float)c916_sig1(ls.vy) : 0.f;
-    r.p1 = r.p2 = 0;
+    r.p0 = r.p1 = 0;
     *reinterpret_cast<RecF *>(recp) = r;
   } else {
     RecD r;
-    r.nu = ls.nu;
-    r.iad = ls.iad;
-    r.y = ls.vy;
-    r.y2 = ls.vy * ls.vy;
-    r.S1 = ls.S * ls.vy / CUDART_PI;
-    r.Sc = ls.S * (1.0 / 1.7724538509055160273);
-    r.ey = ey;
+    r.nu = lp.nu;
+    r.iad = lp.iad;
+    r.y = lp.vy;
+    r.y2 = lp.vy * lp.vy;
+    r.S1 = lp.S1;
+    r.Sc = lp.Sc;
+    r.ey = lp.ey;
     r.pad = 0.0;
     r.i0 = nonempty ? li[0] : 0;
     r.b0 = li[1];
@@ -157,7 +152,7 @@ __device__ __forceinline__ float gh2_f(float s, float u) {
   const float a1 = u + 1.5f;
   const float num = fmaf(-1.2732395447351628f, s, fmaf(a1, u, a1));   // 4/pi
   const float q = fmaf(-1.9098593171027440f, s, a1 * a1);            // 6/pi
-  return num * rcp_approx(u * q);
+  return num * rcp_fast(u * q);
 }
 
 // The profile shape (x, region formula) is FP32; the strength multiply and
@@ -184,7 +179,7 @@ __device__ __forceinline__ void sweep_mixed(const RecF &r, int wb, int lane,
 #pragma unroll
     for (int p = 0; p < HK_PPL; ++p) {
       const float x = fmaf(kf[p], r.vbh, r.dh) + fmaf(kf[p], r.vbl, r.dl);
-      acc[p] = fma(r.S1, widen_pos(rcp_approx(fmaf(x, x, r.y2))), acc[p]);
+      acc[p] = fma(r.S1, widen_pos(rcp_fast(fmaf(x, x, r.y2))), acc[p]);
     }
   } else {
 #pragma unroll
@@ -197,7 +192,7 @@ __device__ __forceinline__ void sweep_mixed(const RecF &r, int wb, int lane,
         } else {
           const float s = x * x;
           const float u = s + r.y2;
-          const float t = (k >= r.b0 && k < r.b1) ? gh2_f(s, u) : rcp_approx(u);
+          const float t = (k >= r.b0 && k < r.b1) ? gh2_f(s, u) : rcp_fast(u);
           acc[p] = fma(r.S1, widen_pos(t), acc[p]);
         }
       }
@@ -241,12 +236,13 @@ __device__ __forceinline__ void sweep_plain(const RecD &r, int wb, int lane,
 }
 
 // ------------------------------------------------------- persistent kernel
+// mixed form: 3 CTAs (24 warps) per SM fit in 80 registers without spills
 template <bool MIXED>
-__global__ void __launch_bounds__(HK_THREADS, 2)
-voigt_sum_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
-                 int tiles_per_state, int total_tickets,
-                 unsigned *__restrict__ ticket, double *__restrict__ K,
-                 int64_t k_stride) {
+__global__ void __launch_bounds__(HK_THREADS, MIXED ? 3 : 2)
+voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ nu0,
+                 int64_t nlines, GridDev g, const StateDev *__restrict__ states,
+                 int tiles_per_state, int total_tickets, unsigned *__restrict__ ticket,
+                 double *__restrict__ K, int64_t k_stride) {
   using Rec = typename std::conditional<MIXED, RecF, RecD>::type;
   __shared__ Rec rec[HK_CH];
   __shared__ int s_ticket;
@@ -264,6 +260,7 @@ voigt_sum_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
     const int s = t / tiles_per_state;
     const int tile = t - s * tiles_per_state;
     const StateDev &st = states[s];
+    const LinePrep *P = prep + (int64_t)s * nlines;
     const int64_t g0 = (int64_t)tile * HK_G;
     const int64_t g1 = min(g0 + (int64_t)HK_G, g.nx);
     if (warp == 0) {
@@ -271,8 +268,8 @@ voigt_sum_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
       const double xlo = grid_x(g, g0) - W;
       const double xhi = grid_x(g, g1 - 1) + W;
       const double pad = 1e-12 * (fabs(xlo) + fabs(xhi)) + 1e-300;
-      const int64_t L0 = lower_bound_warp(L.nu0, L.n, xlo - pad);
-      const int64_t L1 = lower_bound_warp(L.nu0, L.n, xhi + pad);
+      const int64_t L0 = lower_bound_warp(nu0, nlines, xlo - pad);
+      const int64_t L1 = lower_bound_warp(nu0, nlines, xhi + pad);
       if (lane == 0) {
         s_L0 = L0;
         s_L1 = L1;
@@ -300,7 +297,7 @@ voigt_sum_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
     const int64_t nch = (nL + HK_CH - 1) / HK_CH;
     for (int64_t c = 0; c < nch; ++c) {
       const int cnt = (int)((nL - c + nch - 1) / nch);
-      if (tid < cnt) stage_line<MIXED>(L, g, st, L0 + c + (int64_t)tid * nch, g0, g1, &rec[tid]);
+      if (tid < cnt) stage_line<MIXED>(P, g, L0 + c + (int64_t)tid * nch, g0, g1, &rec[tid]);
       __syncthreads();
       for (int j = 0; j < cnt; ++j) {
         if (MIXED) sweep_mixed(reinterpret_cast<const RecF &>(rec[j]), wb, lane, kf, acc);
@@ -319,21 +316,6 @@ voigt_sum_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
 }
 
 // ------------------------------------------------------ diagnostics kernels
-__global__ void prep_dump_kernel(LinesDev L, GridDev g, StateDev st,
-                                 double *__restrict__ out4,
-                                 long long *__restrict__ win6) {
-  const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= L.n) return;
-  const LineState ls = prep_line(L, st, l);
-  out4[4 * l + 0] = ls.nu;
-  out4[4 * l + 1] = ls.S;
-  out4[4 * l + 2] = ls.iad;
-  out4[4 * l + 3] = ls.vy;
-  int64_t w[6];
-  line_windows(g, st, ls, 0, g.nx, w);
-  for (int k = 0; k < 6; ++k) win6[6 * l + k] = w[k];
-}
-
 __global__ void profile_eval_kernel(int64_t n, const double *__restrict__ x,
                                     const double *__restrict__ y, int mixed,
                                     double *__restrict__ out) {
@@ -343,7 +325,8 @@ __global__ void profile_eval_kernel(int64_t n, const double *__restrict__ x,
   if (mixed)
     out[i] = (double)voigt916_rf((float)x[i], (float)y[i], (float)(y[i] * y[i]), (float)ey,
                                  (float)c916_sig1(y[i]));
-  else out[i] = voigt916_d(x[i], y[i], ey);
+  else
+    out[i] = voigt916_d(x[i], y[i], ey);
 }
 
 // FP32 FMA throughput probe: 8 independent FMA chains per thread, every SM
@@ -393,9 +376,9 @@ cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream) {
 // ------------------------------------------------------------- launchers
 int voigt_tile_points() { return HK_G; }
 
-cudaError_t launch_voigt_sum(bool mixed, const LinesDev &L, const GridDev &g,
-                             const StateDev *states_d, int nstates,
-                             unsigned *ticket_d, double *K_d, int64_t k_stride,
+cudaError_t launch_voigt_sum(bool mixed, const LinePrep *prep_d, const double *nu0_d,
+                             int64_t nlines, const GridDev &g, const StateDev *states_d,
+                             int nstates, unsigned *ticket_d, double *K_d, int64_t k_stride,
                              int grid_ctas, cudaStream_t stream) {
   const int tps = (int)((g.nx + HK_G - 1) / HK_G);
   const int total = tps * nstates;
@@ -413,19 +396,11 @@ cudaError_t launch_voigt_sum(bool mixed, const LinesDev &L, const GridDev &g,
   int ctas = grid_ctas > 0 ? grid_ctas : nsm * per_sm;
   if (ctas > total) ctas = total;
   if (mixed)
-    voigt_sum_kernel<true><<<ctas, HK_THREADS, 0, stream>>>(L, g, states_d, tps, total, ticket_d, K_d, k_stride);
+    voigt_sum_kernel<true><<<ctas, HK_THREADS, 0, stream>>>(prep_d, nu0_d, nlines, g, states_d, tps,
+                                                            total, ticket_d, K_d, k_stride);
   else
-    voigt_sum_kernel<false><<<ctas, HK_THREADS, 0, stream>>>(L, g, states_d, tps, total, ticket_d, K_d, k_stride);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_prep_dump(const LinesDev &L, const GridDev &g,
-                             const StateDev &st, double *out4_d,
-                             long long *win6_d, cudaStream_t stream) {
-  if (L.n == 0) return cudaSuccess;
-  const int b = 128;
-  const int64_t nb = (L.n + b - 1) / b;
-  prep_dump_kernel<<<(unsigned)nb, b, 0, stream>>>(L, g, st, out4_d, win6_d);
+    voigt_sum_kernel<false><<<ctas, HK_THREADS, 0, stream>>>(prep_d, nu0_d, nlines, g, states_d, tps,
+                                                             total, ticket_d, K_d, k_stride);
   return cudaGetLastError();
 }
 
