@@ -308,69 +308,70 @@ __device__ __forceinline__ double c916_sig1(double y) {
   return s;
 }
 
-static __device__ __noinline__ float voigt916_rf(float x, float y, float y2, float ey,
-                                                 float sig1) {
+// R[m-1] = 1 / (a^2 m^2 + y^2), m = 1..HK_C916_MR, is a per-line table built
+// once per (line, tile) in shared memory; the recurrence seeds use ex2.approx
+// (their arguments are bounded by ~2a^2, so it keeps ~1e-7 relative
+// accuracy).
+constexpr int HK_C916_MR = 26;  // x < 10 -> m_c <= 17, plus HK_C916_K
+
+__device__ __forceinline__ float ex2_fast(float v) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
+
+__device__ __forceinline__ float voigt916_tab(float x, float y, float ey, float sig1,
+                                              const float *__restrict__ R) {
   const float a = HK_A916_F;
   const float a2 = a * a;
-  const float G = 0.48675662279129028f;  // exp(-2 a^2)
+  const float L2E = 1.4426950408889634f;  // log2(e)
+  const float G = 0.48675662279129028f;   // exp(-2 a^2)
   x = fabsf(x);
   const float ex2 = expf(-x * x);
-  float t1;
-  if (x == 0.f) {
-    t1 = ey;
-  } else if (y == 0.f) {
-    t1 = ex2;
-  } else {
-    // s3: centre term and the two geometric ratios
-    const float mcf = fmaxf(1.0f, rintf(x * (1.0f / a)));
-    const float d = fmaf(a, mcf, -x);
-    const float Tc = expf(-d * d);
-    const float up0 = expf(fmaf(-a2, fmaf(2.0f, mcf, 1.0f), 2.0f * a * x));   // ratio m_c -> m_c+1
-    const float dn0 = expf(fmaf(a2, fmaf(2.0f, mcf, -1.0f), -2.0f * a * x));  // ratio m_c -> m_c-1
-    float s3 = Tc * rcp_fast(fmaf(a2 * mcf, mcf, y2));
-    float T = Tc, q = up0, m = mcf;
+  if (x == 0.f) return ey;
+  if (y == 0.f) return ex2;
+  const int mc = min(17, max(1, __float2int_rn(x * (1.0f / a))));
+  const float mcf = (float)mc;
+  const float d = fmaf(a, mcf, -x);
+  const float Tc = ex2_fast(-L2E * d * d);
+  const float up0 = ex2_fast(L2E * fmaf(-a2, fmaf(2.0f, mcf, 1.0f), 2.0f * a * x));
+  const float dn0 = ex2_fast(L2E * fmaf(a2, fmaf(2.0f, mcf, -1.0f), -2.0f * a * x));
+  const float *Rc = R + (mc - 1);
+  float s3 = Tc * Rc[0];
+  float T = Tc, q = up0;
 #pragma unroll
-    for (int k = 0; k < HK_C916_K; ++k) {
-      T *= q;
-      q *= G;
-      m += 1.0f;
-      s3 = fmaf(T, rcp_fast(fmaf(a2 * m, m, y2)), s3);
-    }
-    T = Tc;
-    q = dn0;
-    m = mcf;
-#pragma unroll
-    for (int k = 0; k < HK_C916_K; ++k) {
-      T *= q;
-      q *= G;
-      m -= 1.0f;
-      if (m >= 1.0f) s3 = fmaf(T, rcp_fast(fmaf(a2 * m, m, y2)), s3);
-    }
-    // s2: only within ~4.8 of the origin does exp(-(a m + x)^2) matter
-    float s2 = 0.f;
-    if (x < 4.8f) {
-      float T2 = expf(-(a + x) * (a + x));
-      float q2 = expf(fmaf(-3.0f, a2, -2.0f * a * x));
-      float m2 = 1.0f;
-#pragma unroll
-      for (int k = 0; k < HK_C916_K; ++k) {
-        s2 = fmaf(T2, rcp_fast(fmaf(a2 * m2, m2, y2)), s2);
-        T2 *= q2;
-        q2 *= G;
-        m2 += 1.0f;
-      }
-    }
-    const float s1 = ex2 * sig1;
-    const float xy = x * y;
-    float sinxy, cosxy;
-    sincosf(xy, &sinxy, &cosxy);
-    const float cos2xy = fmaf(-2.0f * sinxy, sinxy, 1.0f);
-    t1 = ex2 * ey * cos2xy;
-    const float t2 = sinxy * ex2 * sinxy / y;
-    const float t3 = y * (-cos2xy * s1 + 0.5f * (s2 + s3));
-    t1 += HK_C916_F * (t2 + t3);
+  for (int k = 1; k <= HK_C916_K; ++k) {
+    T *= q;
+    q *= G;
+    s3 = fmaf(T, Rc[k], s3);
   }
-  return t1;
+  T = Tc;
+  q = dn0;
+#pragma unroll
+  for (int k = 1; k <= HK_C916_K; ++k) {
+    T *= q;
+    q *= G;
+    if (mc - k >= 1) s3 = fmaf(T, Rc[-k], s3);
+  }
+  float s2 = 0.f;
+  if (x < 4.8f) {
+    float T2 = expf(-(a + x) * (a + x));
+    float q2 = ex2_fast(L2E * fmaf(-3.0f, a2, -2.0f * a * x));
+#pragma unroll
+    for (int k = 0; k < HK_C916_K; ++k) {
+      s2 = fmaf(T2, R[k], s2);
+      T2 *= q2;
+      q2 *= G;
+    }
+  }
+  const float s1 = ex2 * sig1;
+  const float xy = x * y;
+  float sinxy, cosxy;
+  sincosf(xy, &sinxy, &cosxy);
+  const float cos2xy = fmaf(-2.0f * sinxy, sinxy, 1.0f);
+  const float t2 = sinxy * ex2 * sinxy / y;
+  const float t3 = y * (-cos2xy * s1 + 0.5f * (s2 + s3));
+  return fmaf(ex2 * ey, cos2xy, HK_C916_F * (t2 + t3));
 }
 
 }  // namespace hkb

@@ -38,13 +38,30 @@ constexpr int HK_G = HK_WARPS * HK_SLICE;    // points per tile (2048)
 constexpr int HK_CH = HK_THREADS;            // lines per staged chunk
 static_assert(HK_G <= 2048, "k * vb_hi must stay exact in FP32 (11 bits)");
 
+// Staged line record of the mixed form.  The FP32 line constants are stored
+// twice ({v, v}) so the packed f32x2 sweep (two grid points per
+// instruction) reads them as ready-made float2 operands.
 struct __align__(16) RecF {
-  float dh, dl, vbh, vbl;  // x at the tile start (hi, lo), x step (hi, lo)
+  float2 dh, dl;           // x at the tile start (hi, lo)
+  float2 vbh, vbl;         // x step per grid point (hi, lo)
+  float2 Y, A1;            // Y = y^2 and the region-B Horner coefficients
+  float2 B1, A2;
+  float2 B2;
   double S1, Sc;           // S*y/pi (regions A, B), S/sqrt(pi) (region C)
-  float y2, y, ey, sig1;   // y^2, y, erfcx(y), region-C series constant
-  int i0, b0, c0, c1;      // tile-local window boundaries
-  int b1, i1, p0, p1;
+  float y, ey, sig1;       // y, erfcx(y), region-C series constant
+  int i0, b0, c0, c1, b1;  // tile-local window boundaries
+  int i1;
 };
+static_assert(sizeof(RecF) == 128, "RecF layout");
+
+// Shared memory of one mixed-form CTA: staged records, the per-line
+// region-C denominator tables (8 leading pad floats keep R[m-1-k] of the
+// first line in bounds for predicated reads), and a per-point FP64
+// accumulator for the region-C contributions.
+constexpr int HK_RPAD = 8;
+constexpr size_t HK_SMEM_MIXED = sizeof(RecF) * HK_CH +
+                                 sizeof(float) * (HK_RPAD + HK_CH * HK_C916_MR) +
+                                 sizeof(double) * HK_G;
 
 struct __align__(16) RecD {
   double nu, iad, y2, y, S1, Sc, ey, pad;
@@ -97,7 +114,8 @@ __device__ __forceinline__ int clip_local(int w, int64_t g0, int64_t g1) {
 template <bool MIXED>
 __device__ __forceinline__ void stage_line(const LinePrep *__restrict__ P,
                                            const GridDev &g, int64_t l,
-                                           int64_t g0, int64_t g1, void *recp) {
+                                           int64_t g0, int64_t g1, void *recp,
+                                           float *__restrict__ Rtab) {
   const LinePrep lp = P[l];
   int li[6] = {clip_local(lp.i0, g0, g1), clip_local(lp.b0, g0, g1),
                clip_local(lp.c0, g0, g1), clip_local(lp.c1, g0, g1),
@@ -107,24 +125,42 @@ __device__ __forceinline__ void stage_line(const LinePrep *__restrict__ P,
     RecF r;
     const double D0 = __dmul_rn(__dsub_rn(grid_x(g, g0), lp.nu), lp.iad);
     const double vb = __dmul_rn(g.dnu, lp.iad);
-    r.dh = (float)D0;
-    r.dl = (float)(D0 - (double)r.dh);
-    const float vbf = (float)vb;
-    r.vbh = __uint_as_float(__float_as_uint(vbf) & 0xFFFFF800u);  // 13 bits
-    r.vbl = (float)(vb - (double)r.vbh);
+    const float dh = (float)D0;
+    const float dl = (float)(D0 - (double)dh);
+    const float vbh = __uint_as_float(__float_as_uint((float)vb) & 0xFFFFF800u);  // 13 bits
+    const float vbl = (float)(vb - (double)vbh);
+    const double Y = lp.vy * lp.vy;
+    const float Yf = (float)Y;
+    const float A1 = (float)(2.0 * Y + 2.5 - 4.0 / CUDART_PI);
+    const float B1 = (float)((Y + 1.5) * (Y + 1.0));
+    const float A2 = (float)(2.0 * Y + 3.0 - 6.0 / CUDART_PI);
+    const float B2 = (float)((Y + 1.5) * (Y + 1.5));
+    r.dh = make_float2(dh, dh);
+    r.dl = make_float2(dl, dl);
+    r.vbh = make_float2(vbh, vbh);
+    r.vbl = make_float2(vbl, vbl);
+    r.Y = make_float2(Yf, Yf);
+    r.A1 = make_float2(A1, A1);
+    r.B1 = make_float2(B1, B1);
+    r.A2 = make_float2(A2, A2);
+    r.B2 = make_float2(B2, B2);
     r.y = (float)lp.vy;
-    r.y2 = (float)(lp.vy * lp.vy);
     r.S1 = lp.S1;
     r.Sc = lp.Sc;
     r.ey = (float)lp.ey;
     r.sig1 = lp.sig1;
+    if (li[3] > li[2]) {
+      // region C inside this tile: denominators of the Algorithm-916 series
+      const float a2 = HK_A916_F * HK_A916_F;
+#pragma unroll 2
+      for (int m = 1; m <= HK_C916_MR; ++m) Rtab[m - 1] = rcp_fast(fmaf(a2 * m, (float)m, Yf));
+    }
     r.i0 = nonempty ? li[0] : 0;
     r.b0 = li[1];
     r.c0 = li[2];
     r.c1 = li[3];
     r.b1 = li[4];
     r.i1 = nonempty ? li[5] : 0;
-    r.p0 = r.p1 = 0;
     *reinterpret_cast<RecF *>(recp) = r;
   } else {
     RecD r;
@@ -148,52 +184,124 @@ __device__ __forceinline__ void stage_line(const LinePrep *__restrict__ P,
 }
 
 // ------------------------------------------------------------ FP32 sweep
-__device__ __forceinline__ float gh2_f(float s, float u) {
-  const float a1 = u + 1.5f;
-  const float num = fmaf(-1.2732395447351628f, s, fmaf(a1, u, a1));   // 4/pi
-  const float q = fmaf(-1.9098593171027440f, s, a1 * a1);            // 6/pi
-  return num * rcp_fast(u * q);
+// Region B rational in Horner form with per-line coefficients:
+//   t4 = (s (s + A1) + B1) / ((s + Y) (s (s + A2) + B2)),  s = x^2,
+//   A1 = 2Y + 2.5 - 4/pi, B1 = (Y+1.5)(Y+1), A2 = 2Y + 3 - 6/pi, B2 = (Y+1.5)^2;
+// all terms positive, so no cancellation.
+__device__ __forceinline__ float gh2_h(float s, const RecF &r) {
+  const float num = fmaf(s, s + r.A1.x, r.B1.x);
+  const float q = fmaf(s, s + r.A2.x, r.B2.x);
+  return num * rcp_fast((s + r.Y.x) * q);
+}
+
+// x at two grid points (kf2 = {k, k + 32}) from the double-float split
+__device__ __forceinline__ float2 x_pair(float2 kf2, const RecF &r) {
+  return __fadd2_rn(__ffma2_rn(kf2, r.vbh, r.dh), __ffma2_rn(kf2, r.vbl, r.dl));
+}
+
+// region-B t4 at two grid points, packed f32x2 (same Horner form as gh2_h)
+__device__ __forceinline__ float2 gh2_pair(float2 x, const RecF &r) {
+  const float2 s = __fmul2_rn(x, x);
+  const float2 num = __ffma2_rn(s, __fadd2_rn(s, r.A1), r.B1);
+  const float2 q = __ffma2_rn(s, __fadd2_rn(s, r.A2), r.B2);
+  const float2 den = __fmul2_rn(__fadd2_rn(s, r.Y), q);
+  return __fmul2_rn(num, make_float2(rcp_fast(den.x), rcp_fast(den.y)));
 }
 
 // The profile shape (x, region formula) is FP32; the strength multiply and
 // the grid sum are one FP64 FMA, so one state's opacity may span the full
 // FP64 range (the strongest lines of a list can exceed the typical opacity
 // by more than the FP32 exponent range).
-__device__ __forceinline__ void sweep_mixed(const RecF &r, int wb, int lane,
-                                            const float (&kf)[HK_PPL],
-                                            double (&acc)[HK_PPL]) {
+//
+// Each warp classifies the staged lines against its 256-point slice, 32
+// lines per instruction (one lane per line), and sweeps them by class:
+//   HK_CLS_B  slice inside the cut window and inside one region-B part,
+//   HK_CLS_A  slice inside the cut window and inside one region-A part,
+//   HK_CLS_G  anything else that intersects the slice (window edges,
+//             region boundaries, region C),
+// so the specialised loops carry no per-pair tests and non-intersecting
+// lines cost nothing.  Region-C points are evaluated in a rolled loop and
+// summed into the per-point shared accumulator cacc (each point has one
+// owning lane: deterministic).
+enum { HK_CLS_SKIP = 0, HK_CLS_B = 1, HK_CLS_A = 2, HK_CLS_G = 3 };
+
+__device__ __forceinline__ int classify(const RecF &r, int wb) {
   const int we = wb + HK_SLICE;
-  if (r.i1 <= wb || r.i0 >= we) return;
+  if (r.i1 <= wb || r.i0 >= we) return HK_CLS_SKIP;
   const bool full = r.i0 <= wb && r.i1 >= we;
-  if (full && ((r.b0 <= wb && r.c0 >= we) || (r.c1 <= wb && r.b1 >= we))) {
-    // region B only
+  if (full && ((r.b0 <= wb && r.c0 >= we) || (r.c1 <= wb && r.b1 >= we))) return HK_CLS_B;
+  if (full && (r.b0 >= we || r.b1 <= wb)) return HK_CLS_A;
+  return HK_CLS_G;
+}
+
+// region B only, two points per packed instruction; the record's first 80
+// bytes are read as five 16-byte words
+__device__ __forceinline__ void sweep_B(const RecF &rr, const float2 (&kf)[HK_PPL / 2],
+                                        double (&acc)[HK_PPL]) {
+  const float4 *w = reinterpret_cast<const float4 *>(&rr);
+  const float4 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
+  const double S1 = rr.S1;
+  const float2 dh = make_float2(w0.x, w0.y), dl = make_float2(w0.z, w0.w);
+  const float2 vbh = make_float2(w1.x, w1.y), vbl = make_float2(w1.z, w1.w);
+  const float2 Y = make_float2(w2.x, w2.y), A1 = make_float2(w2.z, w2.w);
+  const float2 B1 = make_float2(w3.x, w3.y), A2 = make_float2(w3.z, w3.w);
+  const float2 B2 = rr.B2;
 #pragma unroll
-    for (int p = 0; p < HK_PPL; ++p) {
-      const float x = fmaf(kf[p], r.vbh, r.dh) + fmaf(kf[p], r.vbl, r.dl);
-      const float s = x * x;
-      const float u = s + r.y2;
-      acc[p] = fma(r.S1, widen_pos(gh2_f(s, u)), acc[p]);
-    }
-  } else if (full && (r.b0 >= we || r.b1 <= wb)) {
-    // region A only
+  for (int q = 0; q < HK_PPL / 2; ++q) {
+    const float2 x = __fadd2_rn(__ffma2_rn(kf[q], vbh, dh), __ffma2_rn(kf[q], vbl, dl));
+    const float2 s = __fmul2_rn(x, x);
+    const float2 num = __ffma2_rn(s, __fadd2_rn(s, A1), B1);
+    const float2 qq = __ffma2_rn(s, __fadd2_rn(s, A2), B2);
+    const float2 den = __fmul2_rn(__fadd2_rn(s, Y), qq);
+    const float2 t = __fmul2_rn(num, make_float2(rcp_fast(den.x), rcp_fast(den.y)));
+    acc[2 * q] = fma(S1, widen_pos(t.x), acc[2 * q]);
+    acc[2 * q + 1] = fma(S1, widen_pos(t.y), acc[2 * q + 1]);
+  }
+}
+
+// region A only
+__device__ __forceinline__ void sweep_A(const RecF &rr, const float2 (&kf)[HK_PPL / 2],
+                                        double (&acc)[HK_PPL]) {
+  const float4 *w = reinterpret_cast<const float4 *>(&rr);
+  const float4 w0 = w[0], w1 = w[1];
+  const float2 Y = rr.Y;
+  const double S1 = rr.S1;
+  const float2 dh = make_float2(w0.x, w0.y), dl = make_float2(w0.z, w0.w);
+  const float2 vbh = make_float2(w1.x, w1.y), vbl = make_float2(w1.z, w1.w);
 #pragma unroll
-    for (int p = 0; p < HK_PPL; ++p) {
-      const float x = fmaf(kf[p], r.vbh, r.dh) + fmaf(kf[p], r.vbl, r.dl);
-      acc[p] = fma(r.S1, widen_pos(rcp_fast(fmaf(x, x, r.y2))), acc[p]);
-    }
-  } else {
+  for (int q = 0; q < HK_PPL / 2; ++q) {
+    const float2 x = __fadd2_rn(__ffma2_rn(kf[q], vbh, dh), __ffma2_rn(kf[q], vbl, dl));
+    const float2 u = __ffma2_rn(x, x, Y);
+    acc[2 * q] = fma(S1, widen_pos(rcp_fast(u.x)), acc[2 * q]);
+    acc[2 * q + 1] = fma(S1, widen_pos(rcp_fast(u.y)), acc[2 * q + 1]);
+  }
+}
+
+// everything else: per-point window/region tests, region C deferred
+__device__ __forceinline__ void sweep_G(const RecF &r, const float *__restrict__ Rj,
+                                     double *__restrict__ cacc, int wb, int lane,
+                                     const float2 (&kf)[HK_PPL / 2], double (&acc)[HK_PPL]) {
+  const int we = wb + HK_SLICE;
+  {
 #pragma unroll
     for (int p = 0; p < HK_PPL; ++p) {
       const int k = wb + lane + 32 * p;
-      if (k >= r.i0 && k < r.i1) {
-        const float x = fmaf(kf[p], r.vbh, r.dh) + fmaf(kf[p], r.vbl, r.dl);
-        if (k >= r.c0 && k < r.c1) {
-          acc[p] = fma(r.Sc, (double)voigt916_rf(x, r.y, r.y2, r.ey, r.sig1), acc[p]);
-        } else {
-          const float s = x * x;
-          const float u = s + r.y2;
-          const float t = (k >= r.b0 && k < r.b1) ? gh2_f(s, u) : rcp_fast(u);
-          acc[p] = fma(r.S1, widen_pos(t), acc[p]);
+      if (k >= r.i0 && k < r.i1 && !(k >= r.c0 && k < r.c1)) {
+        const float kk = (p & 1) ? kf[p >> 1].y : kf[p >> 1].x;
+        const float x = fmaf(kk, r.vbh.x, r.dh.x) + fmaf(kk, r.vbl.x, r.dl.x);
+        const float s = x * x;
+        const float t = (k >= r.b0 && k < r.b1) ? gh2_h(s, r) : rcp_fast(s + r.Y.x);
+        acc[p] = fma(r.S1, widen_pos(t), acc[p]);
+      }
+    }
+    const int lo = max(r.c0, wb), hi = min(r.c1, we);
+    if (lo < hi) {
+      for (int pp = (lo - wb) >> 5; pp <= (hi - 1 - wb) >> 5; ++pp) {
+        const int k = wb + lane + 32 * pp;
+        if (k >= lo && k < hi) {
+          const float kk = (float)k;
+          const float x = fmaf(kk, r.vbh.x, r.dh.x) + fmaf(kk, r.vbl.x, r.dl.x);
+          cacc[k] = fma(r.Sc, (double)voigt916_tab(x, r.y, r.ey, r.sig1, Rj), cacc[k]);
         }
       }
     }
@@ -244,7 +352,11 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
                  int tiles_per_state, int total_tickets, unsigned *__restrict__ ticket,
                  double *__restrict__ K, int64_t k_stride) {
   using Rec = typename std::conditional<MIXED, RecF, RecD>::type;
-  __shared__ Rec rec[HK_CH];
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  Rec *rec = reinterpret_cast<Rec *>(smem_dyn);
+  float *Rtab = reinterpret_cast<float *>(smem_dyn + sizeof(Rec) * HK_CH) + HK_RPAD;
+  double *cacc = reinterpret_cast<double *>(smem_dyn + sizeof(Rec) * HK_CH +
+                                            sizeof(float) * (HK_RPAD + HK_CH * HK_C916_MR));
   __shared__ int s_ticket;
   __shared__ long long s_L0, s_L1;
   const int tid = threadIdx.x;
@@ -278,14 +390,19 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
     __syncthreads();
     const int64_t L0 = s_L0, L1 = s_L1;
 
-    float kf[HK_PPL];
+    float2 kf[HK_PPL / 2];  // lane-local point indices, paired {p, p+1}
     double acc[HK_PPL], xg[HK_PPL];
 #pragma unroll
     for (int p = 0; p < HK_PPL; ++p) {
       const int k = wb + lane + 32 * p;
       acc[p] = 0.0;
-      if (MIXED) kf[p] = (float)k;
-      else xg[p] = grid_x(g, g0 + k);
+      if (MIXED) {
+        if (p & 1) kf[p >> 1].y = (float)k;
+        else kf[p >> 1].x = (float)k;
+        cacc[k] = 0.0;  // owned by this lane only: no barrier needed
+      } else {
+        xg[p] = grid_x(g, g0 + k);
+      }
     }
 
     // Chunk c holds the lines L0 + c + q*nch (q < HK_CH): every chunk spans
@@ -297,11 +414,37 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
     const int64_t nch = (nL + HK_CH - 1) / HK_CH;
     for (int64_t c = 0; c < nch; ++c) {
       const int cnt = (int)((nL - c + nch - 1) / nch);
-      if (tid < cnt) stage_line<MIXED>(P, g, L0 + c + (int64_t)tid * nch, g0, g1, &rec[tid]);
+      if (tid < cnt)
+        stage_line<MIXED>(P, g, L0 + c + (int64_t)tid * nch, g0, g1, &rec[tid],
+                          Rtab + tid * HK_C916_MR);
       __syncthreads();
-      for (int j = 0; j < cnt; ++j) {
-        if (MIXED) sweep_mixed(reinterpret_cast<const RecF &>(rec[j]), wb, lane, kf, acc);
-        else sweep_plain(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc);
+      if (MIXED) {
+        const RecF *rf = reinterpret_cast<const RecF *>(rec);
+        for (int g32 = 0; g32 < cnt; g32 += 32) {
+          const int j = g32 + lane;
+          const int cls = (j < cnt) ? classify(rf[j], wb) : HK_CLS_SKIP;
+          unsigned mB = __ballot_sync(0xffffffffu, cls == HK_CLS_B);
+          unsigned mA = __ballot_sync(0xffffffffu, cls == HK_CLS_A);
+          unsigned mG = __ballot_sync(0xffffffffu, cls == HK_CLS_G);
+          while (mB) {
+            const int b = __ffs(mB) - 1;
+            mB &= mB - 1;
+            sweep_B(rf[g32 + b], kf, acc);
+          }
+          while (mA) {
+            const int b = __ffs(mA) - 1;
+            mA &= mA - 1;
+            sweep_A(rf[g32 + b], kf, acc);
+          }
+          while (mG) {
+            const int b = __ffs(mG) - 1;
+            mG &= mG - 1;
+            sweep_G(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, kf, acc);
+          }
+        }
+      } else {
+        for (int j = 0; j < cnt; ++j)
+          sweep_plain(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc);
       }
       __syncthreads();
     }
@@ -309,7 +452,9 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
     double *Ks = K + (int64_t)s * k_stride;
 #pragma unroll
     for (int p = 0; p < HK_PPL; ++p) {
-      const int64_t gi = g0 + wb + lane + 32 * p;
+      const int k = wb + lane + 32 * p;
+      const int64_t gi = g0 + k;
+      if (MIXED) acc[p] += cacc[k];
       if (gi < g1) Ks[gi] = st.kmin + acc[p];
     }
   }
@@ -322,11 +467,18 @@ __global__ void profile_eval_kernel(int64_t n, const double *__restrict__ x,
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double ey = erfcx(y[i]);
-  if (mixed)
-    out[i] = (double)voigt916_rf((float)x[i], (float)y[i], (float)(y[i] * y[i]), (float)ey,
-                                 (float)c916_sig1(y[i]));
-  else
+  if (mixed) {
+    // same table the Voigt kernel stages per line (padded like Rtab)
+    float R[HK_RPAD + HK_C916_MR];
+    const float Y = (float)(y[i] * y[i]);
+    const float a2 = HK_A916_F * HK_A916_F;
+    for (int m = 0; m < HK_RPAD; ++m) R[m] = 0.f;
+    for (int m = 1; m <= HK_C916_MR; ++m) R[HK_RPAD + m - 1] = rcp_fast(fmaf(a2 * m, (float)m, Y));
+    out[i] = (double)voigt916_tab((float)x[i], (float)y[i], (float)ey, (float)c916_sig1(y[i]),
+                                  R + HK_RPAD);
+  } else {
     out[i] = voigt916_d(x[i], y[i], ey);
+  }
 }
 
 // FP32 FMA throughput probe: 8 independent FMA chains per thread, every SM
@@ -388,19 +540,23 @@ cudaError_t launch_voigt_sum(bool mixed, const LinePrep *prep_d, const double *n
   int dev = 0, nsm = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  if (mixed)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, voigt_sum_kernel<true>, HK_THREADS, 0);
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, voigt_sum_kernel<false>, HK_THREADS, 0);
+  const size_t smem = mixed ? HK_SMEM_MIXED : sizeof(RecD) * HK_CH;
+  if (mixed) {
+    e = cudaFuncSetAttribute(voigt_sum_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, voigt_sum_kernel<true>, HK_THREADS, smem);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, voigt_sum_kernel<false>, HK_THREADS, smem);
+  }
   if (per_sm < 1) per_sm = 1;
   int ctas = grid_ctas > 0 ? grid_ctas : nsm * per_sm;
   if (ctas > total) ctas = total;
   if (mixed)
-    voigt_sum_kernel<true><<<ctas, HK_THREADS, 0, stream>>>(prep_d, nu0_d, nlines, g, states_d, tps,
-                                                            total, ticket_d, K_d, k_stride);
+    voigt_sum_kernel<true><<<ctas, HK_THREADS, smem, stream>>>(prep_d, nu0_d, nlines, g, states_d,
+                                                               tps, total, ticket_d, K_d, k_stride);
   else
-    voigt_sum_kernel<false><<<ctas, HK_THREADS, 0, stream>>>(prep_d, nu0_d, nlines, g, states_d, tps,
-                                                             total, ticket_d, K_d, k_stride);
+    voigt_sum_kernel<false><<<ctas, HK_THREADS, smem, stream>>>(prep_d, nu0_d, nlines, g, states_d,
+                                                                tps, total, ticket_d, K_d, k_stride);
   return cudaGetLastError();
 }
 

@@ -16,7 +16,8 @@ import os
 import numpy as np
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_PKG), "lib", "libhkb.so")
+# HKB_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("HKB_LIB", os.path.join(os.path.dirname(_PKG), "lib", "libhkb.so"))
 HEADER_PATH = os.path.join(os.path.dirname(os.path.dirname(_PKG)), "include", "hkb.h")
 
 HK_OK = 0
