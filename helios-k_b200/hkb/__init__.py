@@ -71,6 +71,8 @@ def lib():
             "hk_last_timing": (_i, [_p, _p, _p]),
             "hk_tile_points": (_i, []),
             "hk_fp32_peak": (_i, [_p, _p]),
+            "hk_kdist_noalloc": (_i, [_p, _i, _i64, _i, _i, _d, _d, _p, _p, _p, _p,
+                                      C.c_char_p, _i]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

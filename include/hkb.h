@@ -142,6 +142,28 @@ hk_status hk_kdist(hk_ctx *ctx, int nstates, const double *K, int K_on_device,
                    int32_t *nxmin_out, double *sortedK_out, double *recon_out,
                    int outputs_on_device, void *stream);
 
+/* The same per-bin sort and Chebyshev fit as hk_kdist, for callers that
+ * cannot allocate device memory: host programs that give every byte of the
+ * GPU to their own memory pool or run under a fixed budget, or that must not
+ * make calls which may synchronise the device or fail for lack of memory in
+ * the middle of a run.  No counterpart in the reference (its fit allocates
+ * with cudaMalloc, heliosk.cu:2090-2106).
+ *  - No context, no allocation: it runs on the CURRENT device; K (nstates x
+ *    nx), coeff (nstates x nbins x nC), nxmin (nstates x nbins) and the
+ *    optional sortedK (nstates x nx) are device pointers owned by the caller.
+ *  - Its only scratch is a fixed 2 MiB array in the library (2^18 doubles,
+ *    held on every GPU that loads the library until exit): requires
+ *    (nx / nbins) * nC + 2 nC <= 262144, and a bin small enough for the
+ *    shared-memory sort; larger sizes return HK_ERR_RANGE with a message.
+ *  - The first call on a device looks up that array's device address; make
+ *    that first call before any stream capture.
+ *  - All calls share the array: calls that overlap on the GPU (different
+ *    streams, or different host threads) race.  Serialise them.
+ *  - Asynchronous on `stream`; on failure a message is written to errbuf. */
+hk_status hk_kdist_noalloc(const double *K, int nstates, int64_t nx, int nbins, int nC,
+                           double kmin, double unitScale, double *coeff, int32_t *nxmin,
+                           double *sortedK, void *stream, char *errbuf, int errbuf_len);
+
 /* ------------------------------------------------------- diagnostics */
 
 /* Per-line state (nu, S, 1/alphaD, gammaL/alphaD) and the six window
