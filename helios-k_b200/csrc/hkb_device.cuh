@@ -312,12 +312,48 @@ __device__ __forceinline__ double c916_sig1(double y) {
 // once per (line, tile) in shared memory; the recurrence seeds use ex2.approx
 // (their arguments are bounded by ~2a^2, so it keeps ~1e-7 relative
 // accuracy).
-constexpr int HK_C916_MR = 26;  // x < 10 -> m_c <= 17, plus HK_C916_K
+constexpr int HK_C916_MR = 18;  // x < 6 -> m_c <= 10, plus HK_C916_K
 
 __device__ __forceinline__ float ex2_fast(float v) {
   float r;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
   return r;
+}
+
+// Region C with r = |x + iy| >= 6: the asymptotic (Laplace continued
+// fraction's) series of the Faddeeva function,
+//   w(z) ~ i / (sqrt(pi) z) * sum_{k>=0} c_k u^k,  u = 1/z^2,
+//   c_k = (2k-1)!! / 2^k,
+// so K(x, y) = Re w = (y Re S - x Im S) / (sqrt(pi) r^2).  HK_ASY_K = 8 terms
+// leave c_8 / r^16 < 3e-9 at r = 6 (the series' smallest term is near
+// k = r^2, far beyond).  The expansion omits Re exp(-z^2) =
+// exp(y^2 - x^2) cos(2xy) (the Stokes term that gives w(x) = exp(-x^2) on
+// the real axis); it is added for y < 1 -- for y >= 1 and r >= 6 it is below
+// 1e-13 of K.  Against the FP64 Algorithm 916 the FP32 evaluation keeps
+// 3e-7 relative error over 6 <= r < 10.
+constexpr float HK_ASY_R2 = 36.0f;
+constexpr int HK_ASY_K = 8;
+
+__device__ __forceinline__ float voigt_asy(float x, float y) {
+  const float x2 = x * x, y2 = y * y;
+  const float r2 = x2 + y2;
+  const float ir2 = rcp_fast(r2);
+  const float ir4 = ir2 * ir2;
+  const float ur = (x2 - y2) * ir4;
+  const float ui = -2.0f * x * y * ir4;
+  // c_k, k = 0..8
+  const float c[HK_ASY_K + 1] = {1.0f, 0.5f, 0.75f, 1.875f, 6.5625f, 29.53125f,
+                                 162.421875f, 1055.7421875f, 7918.06640625f};
+  float sr = c[HK_ASY_K], si = 0.0f;
+#pragma unroll
+  for (int k = HK_ASY_K - 1; k >= 0; --k) {
+    const float nr = fmaf(sr, ur, fmaf(-si, ui, c[k]));
+    si = fmaf(sr, ui, si * ur);
+    sr = nr;
+  }
+  float v = fmaf(y, sr, -x * si) * (0.56418958354775628f * ir2);  // 1/sqrt(pi)
+  if (y < 1.0f) v = fmaf(ex2_fast(1.4426950408889634f * (y2 - x2)), __cosf(2.0f * x * y), v);
+  return v;
 }
 
 __device__ __forceinline__ float voigt916_tab(float x, float y, float ey, float sig1,
@@ -327,10 +363,11 @@ __device__ __forceinline__ float voigt916_tab(float x, float y, float ey, float 
   const float L2E = 1.4426950408889634f;  // log2(e)
   const float G = 0.48675662279129028f;   // exp(-2 a^2)
   x = fabsf(x);
+  if (fmaf(x, x, y * y) >= HK_ASY_R2) return voigt_asy(x, y);
   const float ex2 = expf(-x * x);
   if (x == 0.f) return ey;
   if (y == 0.f) return ex2;
-  const int mc = min(17, max(1, __float2int_rn(x * (1.0f / a))));
+  const int mc = min(HK_C916_MR - HK_C916_K, max(1, __float2int_rn(x * (1.0f / a))));
   const float mcf = (float)mc;
   const float d = fmaf(a, mcf, -x);
   const float Tc = ex2_fast(-L2E * d * d);

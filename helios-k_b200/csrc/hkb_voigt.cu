@@ -35,7 +35,7 @@ constexpr int HK_THREADS = HK_WARPS * 32;
 constexpr int HK_PPL = 8;                    // points per lane
 constexpr int HK_SLICE = 32 * HK_PPL;        // points per warp
 constexpr int HK_G = HK_WARPS * HK_SLICE;    // points per tile (2048)
-constexpr int HK_CH = HK_THREADS;            // lines per staged chunk
+constexpr int HK_CH = 128;                   // lines per staged chunk
 static_assert(HK_G <= 2048, "k * vb_hi must stay exact in FP32 (11 bits)");
 
 // Staged line record of the mixed form.  The FP32 line constants are stored
@@ -271,7 +271,7 @@ __device__ __forceinline__ void sweep_A(const RecF &rr, const float2 (&kf)[HK_PP
 #pragma unroll
   for (int q = 0; q < HK_PPL / 2; ++q) {
     const float2 x = __fadd2_rn(__ffma2_rn(kf[q], vbh, dh), __ffma2_rn(kf[q], vbl, dl));
-    const float2 u = __ffma2_rn(x, x, Y);
+    const float2 u = __ffma2_rn(x, x, Y);  // unbounded: separate reciprocals
     acc[2 * q] = fma(S1, widen_pos(rcp_fast(u.x)), acc[2 * q]);
     acc[2 * q + 1] = fma(S1, widen_pos(rcp_fast(u.y)), acc[2 * q + 1]);
   }
@@ -344,9 +344,9 @@ __device__ __forceinline__ void sweep_plain(const RecD &r, int wb, int lane,
 }
 
 // ------------------------------------------------------- persistent kernel
-// mixed form: 3 CTAs (24 warps) per SM fit in 80 registers without spills
+// mixed form: 4 CTAs (32 warps) per SM fit in 64 registers without spills
 template <bool MIXED>
-__global__ void __launch_bounds__(HK_THREADS, MIXED ? 3 : 2)
+__global__ void __launch_bounds__(HK_THREADS, MIXED ? 4 : 2)
 voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ nu0,
                  int64_t nlines, GridDev g, const StateDev *__restrict__ states,
                  int tiles_per_state, int total_tickets, unsigned *__restrict__ ticket,

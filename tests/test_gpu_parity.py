@@ -59,6 +59,13 @@ def test_profile_fp64_and_fp32(small):
     x, y = r * np.cos(th), r * np.sin(th)
     y[:5000] = 10 ** rng.uniform(-9, 0, 5000)
     x[5000:6000] = 0.0
+    # the FP32 form switches from Algorithm 916 to the asymptotic series at
+    # r = 6: both sides of the switch, and tiny y where the exp(-x^2) term
+    # of the real axis dominates
+    r6 = rng.uniform(5.9, 6.1, 2000)
+    x[6000:8000], y[6000:8000] = r6 * np.cos(th[6000:8000]), r6 * np.sin(th[6000:8000])
+    x[8000:9000] = rng.uniform(5.9, 10.0, 1000)
+    y[8000:9000] = 10 ** rng.uniform(-12, 0, 1000)
     keep = x * x + y * y < 100
     x, y = x[keep], y[keep]
     ref = np.array([oracle.voigt916(a, b) for a, b in zip(x, y)])
