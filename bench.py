@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hitemp", choices=["hitemp", "small", "table", "hitemp_slice"])
+    ap.add_argument("--workload", default="hitemp", choices=["hitemp", "small", "table", "hitemp_sparse"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -62,7 +62,7 @@ def workload(name):
         W = dict(synth.WORKLOADS[name])
         W["label"] = {"hitemp": "hitemp-1e7-lines-single-state",
                       "small": "small-1e5-lines-single-state",
-                      "hitemp_slice": "hitemp-density-1e6-lines-3000cm-1-band"}[name]
+                      "hitemp_sparse": "hitemp-distribution-1e6-lines-single-state"}[name]
     return W
 
 

@@ -62,7 +62,9 @@ struct hk_ctx {
   double kmin = 0.0;
   // workspace
   DevBuf states, ticket, wbits, Kwork, outwork, scratch, prep;
+  DevBuf vpart, vcnt;  // split-tile partial sums and per-tile counters
   size_t prep_budget = (size_t)24 << 30;  // bytes of per-(state, line) records per batch
+  size_t part_budget = (size_t)4 << 30;   // bytes of split-tile partial sums per batch
   double voigt_ms_acc = 0.0;
   DevBuf qrV, qrC, qrD;
   int qr_nxb = -1, qr_nc = -1;
@@ -127,7 +129,7 @@ void hk_destroy(hk_ctx *c) {
   for (DevBuf *b : {&c->nu0, &c->Sfile, &c->EL, &c->gam, &c->nexp, &c->delta,
                     &c->Aterm, &c->iso, &c->order, &c->states, &c->ticket,
                     &c->prep, &c->wbits, &c->Kwork, &c->outwork, &c->scratch,
-                    &c->qrV, &c->qrC, &c->qrD})
+                    &c->qrV, &c->qrC, &c->qrD, &c->vpart, &c->vcnt})
     b->release();
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -420,7 +422,7 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   std::vector<StateDev> hs;
   if ((st = build_states(c, nstates, T, P, hs)) != HK_OK) return st;
   CUDA_TRY(c, c->states.ensure(nstates * sizeof(StateDev)));
-  CUDA_TRY(c, c->wbits.ensure(nstates * sizeof(unsigned long long)));
+  CUDA_TRY(c, c->wbits.ensure(2 * nstates * sizeof(unsigned long long)));
   CUDA_TRY(c, cudaMemcpyAsync(c->states.p, hs.data(), nstates * sizeof(StateDev), cudaMemcpyHostToDevice, s));
   const int64_t nx = c->g.nx;
   double *Kd = K_out;
@@ -432,19 +434,32 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   // budget; each batch is one prep launch and one persistent Voigt launch.
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * sizeof(LinePrep);
   int batch = (int)std::max<size_t>(1, c->prep_budget / per_state);
+  const int nsplit = voigt_nsplit(nx);
+  if (nsplit > 1) {
+    // split tiles keep one partial row per part: bound that scratch too
+    const size_t part_per_state = (size_t)((nx + voigt_tile_points() - 1) / voigt_tile_points()) *
+                                  nsplit * voigt_tile_points() * sizeof(double);
+    batch = std::min(batch, (int)std::max<size_t>(1, c->part_budget / part_per_state));
+  }
   batch = std::min(batch, nstates);
   CUDA_TRY(c, c->prep.ensure((size_t)batch * per_state));
   StateDev *sd = c->states.as<StateDev>();
   unsigned long long *wb = c->wbits.as<unsigned long long>();
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
+  const bool mixed = precision == HK_PRECISION_MIXED;
   for (int b0 = 0; b0 < nstates; b0 += batch) {
     const int nb = std::min(batch, nstates - b0);
-    CUDA_TRY(c, launch_line_prep(c->L, c->g, sd + b0, nb, c->prep.as<LinePrep>(), wb + b0, s));
+    const VoigtPlan plan = plan_voigt_sum(mixed, nx, nb, 0);
+    if (plan.nsplit > 1) {
+      CUDA_TRY(c, c->vpart.ensure(plan.partial_doubles * sizeof(double)));
+      CUDA_TRY(c, c->vcnt.ensure(plan.counters * sizeof(unsigned)));
+    }
+    CUDA_TRY(c, launch_line_prep(c->L, c->g, sd + b0, nb, c->prep.as<LinePrep>(), wb + 2 * b0, s));
     CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
-    CUDA_TRY(c, launch_voigt_sum(precision == HK_PRECISION_MIXED, c->prep.as<LinePrep>(),
-                                 c->L.nu0, c->nlines, c->g, sd + b0, nb, c->ticket.as<unsigned>(),
-                                 Kd + (size_t)b0 * nx, nx, 0, s));
+    CUDA_TRY(c, launch_voigt_sum(mixed, plan, c->prep.as<LinePrep>(), c->L.nu0, c->nlines, c->g,
+                                 sd + b0, c->ticket.as<unsigned>(), c->vpart.as<double>(),
+                                 c->vcnt.as<unsigned>(), Kd + (size_t)b0 * nx, nx, s));
     CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
     c->have_voigt_t = true;
     if (b0 + nb < nstates) {

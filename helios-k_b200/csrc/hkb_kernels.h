@@ -21,10 +21,25 @@ cudaError_t launch_line_prep(const LinesDev &L, const GridDev &g, StateDev *stat
                              int nstates, LinePrep *prep_d, unsigned long long *wbits_d,
                              cudaStream_t stream);
 
-cudaError_t launch_voigt_sum(bool mixed, const LinePrep *prep_d, const double *nu0_d,
-                             int64_t nlines, const GridDev &g, const StateDev *states_d,
-                             int nstates, unsigned *ticket_d, double *K_d, int64_t k_stride,
-                             int grid_ctas, cudaStream_t stream);
+// Work plan of one Voigt launch: (state, tile) tickets, each tile's line
+// range split into nsplit parts when there are too few tiles to fill the GPU
+// (parts are combined in part order through partial_doubles of scratch and
+// one counter per tile).
+struct VoigtPlan {
+  int tiles_per_state = 0;
+  int64_t tiles = 0;
+  int ctas = 0;
+  int nsplit = 1;
+  size_t partial_doubles = 0;
+  size_t counters = 0;
+};
+VoigtPlan plan_voigt_sum(bool mixed, int64_t nx, int nstates, int grid_ctas);
+int voigt_nsplit(int64_t nx);  // line-range parts per tile for a grid of nx points
+cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &plan, const LinePrep *prep_d,
+                             const double *nu0_d, int64_t nlines, const GridDev &g,
+                             const StateDev *states_d, unsigned *ticket_d, double *partial_d,
+                             unsigned *tile_cnt_d, double *K_d, int64_t k_stride,
+                             cudaStream_t stream);
 
 cudaError_t launch_prep_dump(const LinesDev &L, const GridDev &g,
                              const StateDev &st, double *out4_d,

@@ -72,14 +72,17 @@ cudaError_t sort_lines_by_nu(int64_t n, double *nu_d, int64_t *order_d,
 // windows (line_windows over [0, Nx)), and the region-C per-line constants
 // erfcx(y) and Sig1(y) for lines that have a region-C window.  For cutMode
 // 1/2 it also bounds the state's largest cutoff half-width (cm^-1), which
-// sizes each tile's line search.
+// sizes each tile's line search; and it takes the state's largest region-A/B
+// term, which sets the power-of-two scale of the mixed form's FP32 sums.
+// wbits holds two words per state: {half-width bits, term bits} (both
+// non-negative doubles, so their bit patterns order like the values).
 __global__ void __launch_bounds__(256)
 line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
                  LinePrep *__restrict__ out, unsigned long long *__restrict__ wbits) {
   const int s = blockIdx.y;
   const StateDev &st = states[s];
   LinePrep *O = out + (int64_t)s * L.n;
-  double w_loc = 0.0;
+  double w_loc = 0.0, s1_loc = 0.0;
   for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < L.n;
        l += (int64_t)gridDim.x * blockDim.x) {
     const LineState ls = prep_line(L, st, l);
@@ -102,14 +105,20 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
     r.i1 = (int)w[5];
     r.pad = 0;
     O[l] = r;
+    // largest region-A/B term of the line: S1 / r^2 with r^2 >= max(100, y^2)
+    if (w[5] > w[0]) s1_loc = fmax(s1_loc, r.S1 / fmax(100.0, ls.vy * ls.vy));
     if (ls.S != 0.0 && ls.iad > 0.0) {
       if (g.cutMode == 1) w_loc = fmax(w_loc, g.cut * ls.vy / ls.iad);
       else if (g.cutMode == 2) w_loc = fmax(w_loc, g.cut / ls.iad);
     }
   }
-  if (g.cutMode != 0) {
-    for (int o = 16; o > 0; o >>= 1) w_loc = fmax(w_loc, __shfl_xor_sync(0xffffffffu, w_loc, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(&wbits[s], (unsigned long long)__double_as_longlong(w_loc));
+  for (int o = 16; o > 0; o >>= 1) {
+    w_loc = fmax(w_loc, __shfl_xor_sync(0xffffffffu, w_loc, o));
+    s1_loc = fmax(s1_loc, __shfl_xor_sync(0xffffffffu, s1_loc, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (g.cutMode != 0) atomicMax(&wbits[2 * s], (unsigned long long)__double_as_longlong(w_loc));
+    atomicMax(&wbits[2 * s + 1], (unsigned long long)__double_as_longlong(s1_loc));
   }
 }
 
@@ -121,15 +130,23 @@ __global__ void state_finalize_kernel(GridDev g, StateDev *__restrict__ states,
   if (g.cutMode == 0) {
     states[s].wmax = g.cut;
   } else {
-    const double w = __longlong_as_double((long long)wbits[s]);
+    const double w = __longlong_as_double((long long)wbits[2 * s]);
     states[s].wmax = w * (1.0 + 1e-9) + 1e-300;
   }
+  const double tmax = __longlong_as_double((long long)wbits[2 * s + 1]);
+  int e = 0;
+  if (tmax > 0.0 && isfinite(tmax)) {
+    frexp(tmax, &e);  // tmax in [2^(e-1), 2^e)
+    e = 40 - e;
+  }
+  states[s].s1scale = ldexp(1.0, e);
+  states[s].s1unscale = ldexp(1.0, -e);
 }
 
 cudaError_t launch_line_prep(const LinesDev &L, const GridDev &g, StateDev *states_d,
                              int nstates, LinePrep *prep_d, unsigned long long *wbits_d,
                              cudaStream_t stream) {
-  cudaError_t e = cudaMemsetAsync(wbits_d, 0, nstates * sizeof(unsigned long long), stream);
+  cudaError_t e = cudaMemsetAsync(wbits_d, 0, 2 * nstates * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return e;
   if (L.n > 0) {
     const int64_t nb = (L.n + 255) / 256;

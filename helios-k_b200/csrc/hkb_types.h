@@ -72,6 +72,8 @@ struct StateDev {
   double wmax;     // upper bound of the cutoff half-width over lines (cm^-1)
   double shift;    // upper bound of |delta| * P
   double kmin;
+  double s1scale;    // 2^e, largest region-A/B term S1/max(100, y^2) * 2^e in [2^39, 2^40)
+  double s1unscale;  // 2^-e
   double iad0[HK_MAX_ISO];  // c sqrt(m / (2 kB T))
   double Q[HK_MAX_ISO];     // partition function at T
   double ab[HK_MAX_ISO];    // abundance * (m / meanMass) when units == 0

@@ -22,6 +22,7 @@
 // Line6A_Call/Line6B_Call/Line6C_Call voigt.h:1820-2036.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <type_traits>
 
@@ -40,24 +41,54 @@ static_assert(HK_G <= 2048, "k * vb_hi must stay exact in FP32 (11 bits)");
 
 // Staged line record of the mixed form.  The FP32 line constants are stored
 // twice ({v, v}) so the packed f32x2 sweep (two grid points per
-// instruction) reads them as ready-made float2 operands.
+// instruction) reads them as ready-made float2 operands.  Regions A and B
+// are summed in FP32 (flushed into the FP64 per-point sums after every
+// chunk of lines) with the line strength folded into the coefficients:
+//   A:  S1f / (s + Y),
+//   B:  S1f t4 = (s (S1f s + C1) + C0) / (((s + D2) s + D1) s + D0),
+// s = x^2, Y = y^2, S1f = S1 * s1scale (a power of two per state),
+// C1 = S1f A1, C0 = S1f B1, and the GH2 denominator (s + Y)(s (s + A2) + B2)
+// expanded: D2 = A2 + Y, D1 = B2 + A2 Y, D0 = B2 Y, with A1 = 2Y + 2.5 - 4/pi,
+// B1 = (Y+1.5)(Y+1), A2 = 2Y + 3 - 6/pi, B2 = (Y+1.5)^2.  Every coefficient
+// is positive, so neither form cancels.
 struct __align__(16) RecF {
   float2 dh, dl;           // x at the tile start (hi, lo)
   float2 vbh, vbl;         // x step per grid point (hi, lo)
-  float2 Y, A1;            // Y = y^2 and the region-B Horner coefficients
-  float2 B1, A2;
-  float2 B2;
-  double S1, Sc;           // S*y/pi (regions A, B), S/sqrt(pi) (region C)
+  float2 S1f, C1;
+  float2 C0, D2;
+  float2 D1, D0;
+  double Sc;               // S/sqrt(pi) (region C, FP64 sum)
   float y, ey, sig1;       // y, erfcx(y), region-C series constant
   int i0, b0, c0, c1, b1;  // tile-local window boundaries
-  int i1;
+  int i1, flags;
 };
 static_assert(sizeof(RecF) == 128, "RecF layout");
 
+// flags: HK_F_WEAK -- the line's smallest FP32 term in this tile,
+// S1f / (x_max^2 + Y), would fall below HK_TERM_MIN (near the FP32 normal
+// range), or S1f itself is above 2^100 (y^2 beyond ~2^60): the line is
+// summed in FP64 with S1f = 1 (unscaled coefficients);
+// HK_F_WIDE -- x_max^2 + Y >= 1e18, so two region-A denominators may not be
+// multiplied in FP32 (paired reciprocals are off).
+// Strength levels: S1f = S1 * s1scale * 2^(HK_LEVEL_BITS * lev) puts every
+// line's largest term near 2^40 whatever its strength; a warp sums the lines
+// of one level at a time in FP32 and flushes (exactly unscaled) into the FP64
+// sums when the level changes, so FP32 never holds terms of lines more than
+// 2^96 apart.  Levels above HK_MAX_LEVEL (2^768 below the strongest line)
+// take the FP64 path.  The level sits in flags bits 8-11.
+constexpr int HK_F_WEAK = 1, HK_F_WIDE = 2;
+constexpr double HK_TERM_MIN = 0x1p-120;
+constexpr int HK_LEVEL_BITS = 96;
+constexpr int HK_MAX_LEVEL = 7;
+
+// 2^e as a double, exact for -1022 <= e <= 1023
+__device__ __forceinline__ double pow2_d(int e) {
+  return __longlong_as_double((long long)(1023 + e) << 52);
+}
+
 // Shared memory of one mixed-form CTA: staged records, the per-line
 // region-C denominator tables (8 leading pad floats keep R[m-1-k] of the
-// first line in bounds for predicated reads), and a per-point FP64
-// accumulator for the region-C contributions.
+// first line in bounds for predicated reads), and the per-point FP64 sums.
 constexpr int HK_RPAD = 8;
 constexpr size_t HK_SMEM_MIXED = sizeof(RecF) * HK_CH +
                                  sizeof(float) * (HK_RPAD + HK_CH * HK_C916_MR) +
@@ -67,15 +98,6 @@ struct __align__(16) RecD {
   double nu, iad, y2, y, S1, Sc, ey, pad;
   int i0, b0, c0, c1, b1, i1, p0, p1;
 };
-
-// Exact widening of a positive normal float to double with integer ops
-// (keeps the conversion off the XU pipe that rcp.approx already uses).
-__device__ __forceinline__ double widen_pos(float f) {
-  const unsigned u = __float_as_uint(f);
-  const unsigned lo = u << 29;
-  const unsigned hi = (u >> 3) + (896u << 20);
-  return __hiloint2double((int)hi, (int)lo);
-}
 
 // first index in [0, n) with a[idx] >= v (n if none); all 32 lanes call it
 __device__ int64_t lower_bound_warp(const double *__restrict__ a, int64_t n,
@@ -108,19 +130,25 @@ __device__ __forceinline__ int clip_local(int w, int64_t g0, int64_t g1) {
   return (int)(v - g0);
 }
 
+__device__ __forceinline__ float2 f2(double v) {
+  const float f = (float)v;
+  return make_float2(f, f);
+}
+
 // Clip one line's global windows to the tile [g0, g1) and fill the staged
 // record.  Clipping the oracle's global boundaries equals searching the
 // clipped range, because every window predicate is monotone on its range.
+// Lines with S = 0 contribute nothing and are staged empty.
 template <bool MIXED>
 __device__ __forceinline__ void stage_line(const LinePrep *__restrict__ P,
                                            const GridDev &g, int64_t l,
-                                           int64_t g0, int64_t g1, void *recp,
-                                           float *__restrict__ Rtab) {
+                                           int64_t g0, int64_t g1, double s1scale,
+                                           void *recp, float *__restrict__ Rtab) {
   const LinePrep lp = P[l];
   int li[6] = {clip_local(lp.i0, g0, g1), clip_local(lp.b0, g0, g1),
                clip_local(lp.c0, g0, g1), clip_local(lp.c1, g0, g1),
                clip_local(lp.b1, g0, g1), clip_local(lp.i1, g0, g1)};
-  const bool nonempty = li[5] > li[0];
+  const bool nonempty = li[5] > li[0] && lp.Sc != 0.0;
   if (MIXED) {
     RecF r;
     const double D0 = __dmul_rn(__dsub_rn(grid_x(g, g0), lp.nu), lp.iad);
@@ -130,28 +158,46 @@ __device__ __forceinline__ void stage_line(const LinePrep *__restrict__ P,
     const float vbh = __uint_as_float(__float_as_uint((float)vb) & 0xFFFFF800u);  // 13 bits
     const float vbl = (float)(vb - (double)vbh);
     const double Y = lp.vy * lp.vy;
-    const float Yf = (float)Y;
-    const float A1 = (float)(2.0 * Y + 2.5 - 4.0 / CUDART_PI);
-    const float B1 = (float)((Y + 1.5) * (Y + 1.0));
-    const float A2 = (float)(2.0 * Y + 3.0 - 6.0 / CUDART_PI);
-    const float B2 = (float)((Y + 1.5) * (Y + 1.5));
+    const double A1 = 2.0 * Y + 2.5 - 4.0 / CUDART_PI, B1 = (Y + 1.5) * (Y + 1.0);
+    const double A2 = 2.0 * Y + 3.0 - 6.0 / CUDART_PI, B2 = (Y + 1.5) * (Y + 1.5);
+    const double xe = D0 + (double)(g1 - g0 - 1) * vb;  // x at the tile's last point
+    const double xm = fmax(fabs(D0), fabs(xe));
+    const double umax = xm * xm + Y;
+    // strength level: the line's largest region-A/B term S1/max(100, Y),
+    // scaled by the state, lies in (2^(40-96(lev+1)), 2^(40-96 lev)]
+    int lev = 0;
+    const double term = lp.S1 / fmax(100.0, Y) * s1scale;
+    if (term > 0.0) {
+      int ex = 0;
+      frexp(term, &ex);  // term in [2^(ex-1), 2^ex), ex <= 40
+      lev = (40 - ex) / HK_LEVEL_BITS;
+    }
+    double S1f = lp.S1 * s1scale * pow2_d(HK_LEVEL_BITS * min(lev, HK_MAX_LEVEL));
+    int flags = umax >= 1e18 ? HK_F_WIDE : 0;
+    if (lev > HK_MAX_LEVEL || S1f < HK_TERM_MIN * umax || S1f > 0x1p100) {
+      flags |= HK_F_WEAK;
+      S1f = 1.0;
+      lev = 0;
+    }
+    flags |= lev << 8;
     r.dh = make_float2(dh, dh);
     r.dl = make_float2(dl, dl);
     r.vbh = make_float2(vbh, vbh);
     r.vbl = make_float2(vbl, vbl);
-    r.Y = make_float2(Yf, Yf);
-    r.A1 = make_float2(A1, A1);
-    r.B1 = make_float2(B1, B1);
-    r.A2 = make_float2(A2, A2);
-    r.B2 = make_float2(B2, B2);
-    r.y = (float)lp.vy;
-    r.S1 = lp.S1;
+    r.S1f = f2(S1f);
+    r.C1 = f2(S1f * A1);
+    r.C0 = f2(S1f * B1);
+    r.D2 = f2(A2 + Y);
+    r.D1 = f2(B2 + A2 * Y);
+    r.D0 = f2(B2 * Y);
     r.Sc = lp.Sc;
+    r.y = (float)lp.vy;
     r.ey = (float)lp.ey;
     r.sig1 = lp.sig1;
-    if (li[3] > li[2]) {
+    if (nonempty && li[3] > li[2]) {
       // region C inside this tile: denominators of the Algorithm-916 series
       const float a2 = HK_A916_F * HK_A916_F;
+      const float Yf = (float)Y;
 #pragma unroll 2
       for (int m = 1; m <= HK_C916_MR; ++m) Rtab[m - 1] = rcp_fast(fmaf(a2 * m, (float)m, Yf));
     }
@@ -161,6 +207,7 @@ __device__ __forceinline__ void stage_line(const LinePrep *__restrict__ P,
     r.c1 = li[3];
     r.b1 = li[4];
     r.i1 = nonempty ? li[5] : 0;
+    r.flags = flags;
     *reinterpret_cast<RecF *>(recp) = r;
   } else {
     RecD r;
@@ -184,125 +231,136 @@ __device__ __forceinline__ void stage_line(const LinePrep *__restrict__ P,
 }
 
 // ------------------------------------------------------------ FP32 sweep
-// Region B rational in Horner form with per-line coefficients:
-//   t4 = (s (s + A1) + B1) / ((s + Y) (s (s + A2) + B2)),  s = x^2,
-//   A1 = 2Y + 2.5 - 4/pi, B1 = (Y+1.5)(Y+1), A2 = 2Y + 3 - 6/pi, B2 = (Y+1.5)^2;
-// all terms positive, so no cancellation.
-__device__ __forceinline__ float gh2_h(float s, const RecF &r) {
-  const float num = fmaf(s, s + r.A1.x, r.B1.x);
-  const float q = fmaf(s, s + r.A2.x, r.B2.x);
-  return num * rcp_fast((s + r.Y.x) * q);
-}
-
-// x at two grid points (kf2 = {k, k + 32}) from the double-float split
-__device__ __forceinline__ float2 x_pair(float2 kf2, const RecF &r) {
-  return __fadd2_rn(__ffma2_rn(kf2, r.vbh, r.dh), __ffma2_rn(kf2, r.vbl, r.dl));
-}
-
-// region-B t4 at two grid points, packed f32x2 (same Horner form as gh2_h)
-__device__ __forceinline__ float2 gh2_pair(float2 x, const RecF &r) {
-  const float2 s = __fmul2_rn(x, x);
-  const float2 num = __ffma2_rn(s, __fadd2_rn(s, r.A1), r.B1);
-  const float2 q = __ffma2_rn(s, __fadd2_rn(s, r.A2), r.B2);
-  const float2 den = __fmul2_rn(__fadd2_rn(s, r.Y), q);
-  return __fmul2_rn(num, make_float2(rcp_fast(den.x), rcp_fast(den.y)));
-}
-
-// The profile shape (x, region formula) is FP32; the strength multiply and
-// the grid sum are one FP64 FMA, so one state's opacity may span the full
-// FP64 range (the strongest lines of a list can exceed the typical opacity
-// by more than the FP32 exponent range).
-//
 // Each warp classifies the staged lines against its 256-point slice, 32
 // lines per instruction (one lane per line), and sweeps them by class:
 //   HK_CLS_B  slice inside the cut window and inside one region-B part,
 //   HK_CLS_A  slice inside the cut window and inside one region-A part,
 //   HK_CLS_G  anything else that intersects the slice (window edges,
 //             region boundaries, region C),
+//   HK_CLS_W  a HK_F_WEAK line that intersects the slice,
 // so the specialised loops carry no per-pair tests and non-intersecting
 // lines cost nothing.  Region-C points are evaluated in a rolled loop and
-// summed into the per-point shared accumulator cacc (each point has one
+// summed in FP64 into the per-point shared sums cacc (each point has one
 // owning lane: deterministic).
-enum { HK_CLS_SKIP = 0, HK_CLS_B = 1, HK_CLS_A = 2, HK_CLS_G = 3 };
+enum { HK_CLS_SKIP = 0, HK_CLS_B = 1, HK_CLS_A = 2, HK_CLS_G = 3, HK_CLS_W = 4 };
 
 __device__ __forceinline__ int classify(const RecF &r, int wb) {
   const int we = wb + HK_SLICE;
   if (r.i1 <= wb || r.i0 >= we) return HK_CLS_SKIP;
+  if (r.flags & HK_F_WEAK) return HK_CLS_W;
   const bool full = r.i0 <= wb && r.i1 >= we;
   if (full && ((r.b0 <= wb && r.c0 >= we) || (r.c1 <= wb && r.b1 >= we))) return HK_CLS_B;
   if (full && (r.b0 >= we || r.b1 <= wb)) return HK_CLS_A;
   return HK_CLS_G;
 }
 
+// 1/d0 and 1/d1 from one reciprocal: R = 1/(d0 d1), then (d1 R, d0 R).
+// Callers guarantee d0 d1 < 2^128 (region B: d < r^6 < 1e18).
+__device__ __forceinline__ float2 rcp_pair(float2 d) {
+  const float R = rcp_fast(d.x * d.y);
+  return __fmul2_rn(make_float2(d.y, d.x), make_float2(R, R));
+}
+
 // region B only, two points per packed instruction; the record's first 80
 // bytes are read as five 16-byte words
 __device__ __forceinline__ void sweep_B(const RecF &rr, const float2 (&kf)[HK_PPL / 2],
-                                        double (&acc)[HK_PPL]) {
+                                        float2 (&a32)[HK_PPL / 2]) {
   const float4 *w = reinterpret_cast<const float4 *>(&rr);
-  const float4 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
-  const double S1 = rr.S1;
+  const float4 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3], w4 = w[4];
   const float2 dh = make_float2(w0.x, w0.y), dl = make_float2(w0.z, w0.w);
   const float2 vbh = make_float2(w1.x, w1.y), vbl = make_float2(w1.z, w1.w);
-  const float2 Y = make_float2(w2.x, w2.y), A1 = make_float2(w2.z, w2.w);
-  const float2 B1 = make_float2(w3.x, w3.y), A2 = make_float2(w3.z, w3.w);
-  const float2 B2 = rr.B2;
+  const float2 S1f = make_float2(w2.x, w2.y), C1 = make_float2(w2.z, w2.w);
+  const float2 C0 = make_float2(w3.x, w3.y), D2 = make_float2(w3.z, w3.w);
+  const float2 D1 = make_float2(w4.x, w4.y), D0 = make_float2(w4.z, w4.w);
 #pragma unroll
   for (int q = 0; q < HK_PPL / 2; ++q) {
     const float2 x = __fadd2_rn(__ffma2_rn(kf[q], vbh, dh), __ffma2_rn(kf[q], vbl, dl));
     const float2 s = __fmul2_rn(x, x);
-    const float2 num = __ffma2_rn(s, __fadd2_rn(s, A1), B1);
-    const float2 qq = __ffma2_rn(s, __fadd2_rn(s, A2), B2);
-    const float2 den = __fmul2_rn(__fadd2_rn(s, Y), qq);
-    const float2 t = __fmul2_rn(num, make_float2(rcp_fast(den.x), rcp_fast(den.y)));
-    acc[2 * q] = fma(S1, widen_pos(t.x), acc[2 * q]);
-    acc[2 * q + 1] = fma(S1, widen_pos(t.y), acc[2 * q + 1]);
+    const float2 num = __ffma2_rn(s, __ffma2_rn(S1f, s, C1), C0);
+    const float2 den = __ffma2_rn(__ffma2_rn(__fadd2_rn(s, D2), s, D1), s, D0);
+    a32[q] = __ffma2_rn(num, rcp_pair(den), a32[q]);
   }
 }
 
 // region A only
 __device__ __forceinline__ void sweep_A(const RecF &rr, const float2 (&kf)[HK_PPL / 2],
-                                        double (&acc)[HK_PPL]) {
+                                        float2 (&a32)[HK_PPL / 2]) {
   const float4 *w = reinterpret_cast<const float4 *>(&rr);
   const float4 w0 = w[0], w1 = w[1];
-  const float2 Y = rr.Y;
-  const double S1 = rr.S1;
+  const float2 S1f = rr.S1f;
+  const float Yf = rr.y * rr.y;
+  const float2 Y = make_float2(Yf, Yf);
   const float2 dh = make_float2(w0.x, w0.y), dl = make_float2(w0.z, w0.w);
   const float2 vbh = make_float2(w1.x, w1.y), vbl = make_float2(w1.z, w1.w);
+  if (!(rr.flags & HK_F_WIDE)) {
 #pragma unroll
-  for (int q = 0; q < HK_PPL / 2; ++q) {
-    const float2 x = __fadd2_rn(__ffma2_rn(kf[q], vbh, dh), __ffma2_rn(kf[q], vbl, dl));
-    const float2 u = __ffma2_rn(x, x, Y);  // unbounded: separate reciprocals
-    acc[2 * q] = fma(S1, widen_pos(rcp_fast(u.x)), acc[2 * q]);
-    acc[2 * q + 1] = fma(S1, widen_pos(rcp_fast(u.y)), acc[2 * q + 1]);
+    for (int q = 0; q < HK_PPL / 2; ++q) {
+      const float2 x = __fadd2_rn(__ffma2_rn(kf[q], vbh, dh), __ffma2_rn(kf[q], vbl, dl));
+      a32[q] = __ffma2_rn(S1f, rcp_pair(__ffma2_rn(x, x, Y)), a32[q]);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < HK_PPL / 2; ++q) {
+      const float2 x = __fadd2_rn(__ffma2_rn(kf[q], vbh, dh), __ffma2_rn(kf[q], vbl, dl));
+      const float2 u = __ffma2_rn(x, x, Y);
+      a32[q] = __ffma2_rn(S1f, make_float2(rcp_fast(u.x), rcp_fast(u.y)), a32[q]);
+    }
   }
 }
 
-// everything else: per-point window/region tests, region C deferred
+// everything else: per-point window/region tests, region C deferred.
+// WEAK lines (S1f = 1) add S1 t in FP64 to cacc; the others add S1f t to
+// the FP32 sums.
+template <bool WEAK>
 __device__ __forceinline__ void sweep_G(const RecF &r, const float *__restrict__ Rj,
-                                     double *__restrict__ cacc, int wb, int lane,
-                                     const float2 (&kf)[HK_PPL / 2], double (&acc)[HK_PPL]) {
+                                        double *__restrict__ cacc, int wb, int lane,
+                                        const float2 (&kf)[HK_PPL / 2],
+                                        float2 (&a32)[HK_PPL / 2]) {
+  // the record lives in shared memory like cacc: read it once into registers
+  const int i0 = r.i0, i1 = r.i1, b0 = r.b0, b1 = r.b1, c0 = r.c0, c1 = r.c1;
+  const float dh = r.dh.x, dl = r.dl.x, vbh = r.vbh.x, vbl = r.vbl.x;
+  const float y = r.y;
+  const float Yf = y * y;
+  const double Sc = r.Sc;
   const int we = wb + HK_SLICE;
-  {
+  if (i0 < we && i1 > wb && !(c0 <= max(i0, wb) && c1 >= min(i1, we))) {
+    const float S1f = r.S1f.x, C1 = r.C1.x, C0 = r.C0.x;
+    const float D2 = r.D2.x, D1 = r.D1.x, D0 = r.D0.x;
+    const double S1w = WEAK ? Sc * (double)y * 0.56418958354775628 : 0.0;  // S y / pi
 #pragma unroll
     for (int p = 0; p < HK_PPL; ++p) {
       const int k = wb + lane + 32 * p;
-      if (k >= r.i0 && k < r.i1 && !(k >= r.c0 && k < r.c1)) {
+      if (k >= i0 && k < i1 && !(k >= c0 && k < c1)) {
         const float kk = (p & 1) ? kf[p >> 1].y : kf[p >> 1].x;
-        const float x = fmaf(kk, r.vbh.x, r.dh.x) + fmaf(kk, r.vbl.x, r.dl.x);
+        const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
         const float s = x * x;
-        const float t = (k >= r.b0 && k < r.b1) ? gh2_h(s, r) : rcp_fast(s + r.Y.x);
-        acc[p] = fma(r.S1, widen_pos(t), acc[p]);
+        float t;
+        if (k >= b0 && k < b1) {
+          const float num = fmaf(s, fmaf(S1f, s, C1), C0);
+          const float den = fmaf(fmaf(s + D2, s, D1), s, D0);
+          t = num * rcp_fast(den);
+        } else {
+          t = S1f * rcp_fast(s + Yf);
+        }
+        if (WEAK) {
+          cacc[k] = fma(S1w, (double)t, cacc[k]);
+        } else if (p & 1) {
+          a32[p >> 1].y += t;
+        } else {
+          a32[p >> 1].x += t;
+        }
       }
     }
-    const int lo = max(r.c0, wb), hi = min(r.c1, we);
-    if (lo < hi) {
-      for (int pp = (lo - wb) >> 5; pp <= (hi - 1 - wb) >> 5; ++pp) {
-        const int k = wb + lane + 32 * pp;
-        if (k >= lo && k < hi) {
-          const float kk = (float)k;
-          const float x = fmaf(kk, r.vbh.x, r.dh.x) + fmaf(kk, r.vbl.x, r.dl.x);
-          cacc[k] = fma(r.Sc, (double)voigt916_tab(x, r.y, r.ey, r.sig1, Rj), cacc[k]);
-        }
+  }
+  const int lo = max(c0, wb), hi = min(c1, we);
+  if (lo < hi) {
+    const float ey = r.ey, sig1 = r.sig1;
+    for (int pp = (lo - wb) >> 5; pp <= (hi - 1 - wb) >> 5; ++pp) {
+      const int k = wb + lane + 32 * pp;
+      if (k >= lo && k < hi) {
+        const float kk = (float)k;
+        const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
+        cacc[k] = fma(Sc, (double)voigt916_tab(x, y, ey, sig1, Rj), cacc[k]);
       }
     }
   }
@@ -343,21 +401,37 @@ __device__ __forceinline__ void sweep_plain(const RecD &r, int wb, int lane,
   }
 }
 
+// add the FP32 sums of level lev into the FP64 sums (exact unscale) and
+// clear them
+__device__ __forceinline__ void flush_sums(float2 (&a32)[HK_PPL / 2], double *__restrict__ cacc,
+                                           int wb, int lane, double s1unscale, int lev) {
+  const double u = s1unscale * pow2_d(-HK_LEVEL_BITS * lev);
+#pragma unroll
+  for (int p = 0; p < HK_PPL; ++p) {
+    const int k = wb + lane + 32 * p;
+    const float v = (p & 1) ? a32[p >> 1].y : a32[p >> 1].x;
+    cacc[k] = fma((double)v, u, cacc[k]);
+  }
+#pragma unroll
+  for (int q = 0; q < HK_PPL / 2; ++q) a32[q] = make_float2(0.f, 0.f);
+}
+
 // ------------------------------------------------------- persistent kernel
-// mixed form: 4 CTAs (32 warps) per SM fit in 64 registers without spills
+// mixed form: 4 CTAs (32 warps) per SM, 64 registers
 template <bool MIXED>
 __global__ void __launch_bounds__(HK_THREADS, MIXED ? 4 : 2)
 voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ nu0,
                  int64_t nlines, GridDev g, const StateDev *__restrict__ states,
-                 int tiles_per_state, int total_tickets, unsigned *__restrict__ ticket,
-                 double *__restrict__ K, int64_t k_stride) {
+                 int tiles_per_state, int nsplit, int total_tickets,
+                 unsigned *__restrict__ ticket, double *__restrict__ partial,
+                 unsigned *__restrict__ tile_cnt, double *__restrict__ K, int64_t k_stride) {
   using Rec = typename std::conditional<MIXED, RecF, RecD>::type;
   extern __shared__ __align__(16) unsigned char smem_dyn[];
   Rec *rec = reinterpret_cast<Rec *>(smem_dyn);
   float *Rtab = reinterpret_cast<float *>(smem_dyn + sizeof(Rec) * HK_CH) + HK_RPAD;
   double *cacc = reinterpret_cast<double *>(smem_dyn + sizeof(Rec) * HK_CH +
                                             sizeof(float) * (HK_RPAD + HK_CH * HK_C916_MR));
-  __shared__ int s_ticket;
+  __shared__ int s_ticket, s_last;
   __shared__ long long s_L0, s_L1;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -369,8 +443,11 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
     __syncthreads();
     const int t = s_ticket;
     if (t >= total_tickets) break;
-    const int s = t / tiles_per_state;
-    const int tile = t - s * tiles_per_state;
+    // ticket -> (tile of a state, part of that tile's line range)
+    const int tt = t / nsplit;
+    const int part = t - tt * nsplit;
+    const int s = tt / tiles_per_state;
+    const int tile = tt - s * tiles_per_state;
     const StateDev &st = states[s];
     const LinePrep *P = prep + (int64_t)s * nlines;
     const int64_t g0 = (int64_t)tile * HK_G;
@@ -390,15 +467,21 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
     __syncthreads();
     const int64_t L0 = s_L0, L1 = s_L1;
 
-    float2 kf[HK_PPL / 2];  // lane-local point indices, paired {p, p+1}
+    float2 kf[HK_PPL / 2];   // lane-local point indices, paired {p, p+1}
+    float2 a32[HK_PPL / 2];  // mixed: FP32 sums of the current chunk (scaled)
     double acc[HK_PPL], xg[HK_PPL];
 #pragma unroll
     for (int p = 0; p < HK_PPL; ++p) {
       const int k = wb + lane + 32 * p;
       acc[p] = 0.0;
       if (MIXED) {
-        if (p & 1) kf[p >> 1].y = (float)k;
-        else kf[p >> 1].x = (float)k;
+        if (p & 1) {
+          kf[p >> 1].y = (float)k;
+          a32[p >> 1].y = 0.f;
+        } else {
+          kf[p >> 1].x = (float)k;
+          a32[p >> 1].x = 0.f;
+        }
         cacc[k] = 0.0;  // owned by this lane only: no barrier needed
       } else {
         xg[p] = grid_x(g, g0 + k);
@@ -412,10 +495,12 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
     // and leave the other warps idle at the barrier).
     const int64_t nL = L1 - L0;
     const int64_t nch = (nL + HK_CH - 1) / HK_CH;
-    for (int64_t c = 0; c < nch; ++c) {
+    const int64_t c_begin = nch * part / nsplit, c_end = nch * (part + 1) / nsplit;
+    int lcur = 0;  // strength level held in a32 (warp-uniform)
+    for (int64_t c = c_begin; c < c_end; ++c) {
       const int cnt = (int)((nL - c + nch - 1) / nch);
       if (tid < cnt)
-        stage_line<MIXED>(P, g, L0 + c + (int64_t)tid * nch, g0, g1, &rec[tid],
+        stage_line<MIXED>(P, g, L0 + c + (int64_t)tid * nch, g0, g1, st.s1scale, &rec[tid],
                           Rtab + tid * HK_C916_MR);
       __syncthreads();
       if (MIXED) {
@@ -423,25 +508,47 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
         for (int g32 = 0; g32 < cnt; g32 += 32) {
           const int j = g32 + lane;
           const int cls = (j < cnt) ? classify(rf[j], wb) : HK_CLS_SKIP;
-          unsigned mB = __ballot_sync(0xffffffffu, cls == HK_CLS_B);
-          unsigned mA = __ballot_sync(0xffffffffu, cls == HK_CLS_A);
-          unsigned mG = __ballot_sync(0xffffffffu, cls == HK_CLS_G);
-          while (mB) {
-            const int b = __ffs(mB) - 1;
-            mB &= mB - 1;
-            sweep_B(rf[g32 + b], kf, acc);
+          const int lev = (j < cnt) ? (rf[j].flags >> 8) : 0;
+          const unsigned bB = __ballot_sync(0xffffffffu, cls == HK_CLS_B);
+          const unsigned bA = __ballot_sync(0xffffffffu, cls == HK_CLS_A);
+          const unsigned bG = __ballot_sync(0xffffffffu, cls == HK_CLS_G);
+          unsigned mW = __ballot_sync(0xffffffffu, cls == HK_CLS_W);
+          unsigned live = bB | bA | bG;
+          while (live) {
+            // the lines of the current level first; switch level (flushing
+            // the FP32 sums) only when none of them is left
+            unsigned m = __ballot_sync(0xffffffffu, lev == lcur) & live;
+            if (m == 0u) {
+              flush_sums(a32, cacc, wb, lane, st.s1unscale, lcur);
+              lcur = __shfl_sync(0xffffffffu, lev, __ffs(live) - 1);
+              m = __ballot_sync(0xffffffffu, lev == lcur) & live;
+            }
+            live &= ~m;
+            unsigned mB = m & bB, mA = m & bA, mG = m & bG;
+            while (mB) {
+              const int b = __ffs(mB) - 1;
+              mB &= mB - 1;
+              sweep_B(rf[g32 + b], kf, a32);
+            }
+            while (mA) {
+              const int b = __ffs(mA) - 1;
+              mA &= mA - 1;
+              sweep_A(rf[g32 + b], kf, a32);
+            }
+            while (mG) {
+              const int b = __ffs(mG) - 1;
+              mG &= mG - 1;
+              sweep_G<false>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, kf, a32);
+            }
           }
-          while (mA) {
-            const int b = __ffs(mA) - 1;
-            mA &= mA - 1;
-            sweep_A(rf[g32 + b], kf, acc);
-          }
-          while (mG) {
-            const int b = __ffs(mG) - 1;
-            mG &= mG - 1;
-            sweep_G(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, kf, acc);
+          while (mW) {
+            const int b = __ffs(mW) - 1;
+            mW &= mW - 1;
+            sweep_G<true>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, kf, a32);
           }
         }
+        // at most one chunk of lines per FP32 sum
+        flush_sums(a32, cacc, wb, lane, st.s1unscale, lcur);
       } else {
         for (int j = 0; j < cnt; ++j)
           sweep_plain(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc);
@@ -450,12 +557,41 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
     }
 
     double *Ks = K + (int64_t)s * k_stride;
+    if (nsplit == 1) {
 #pragma unroll
-    for (int p = 0; p < HK_PPL; ++p) {
-      const int k = wb + lane + 32 * p;
-      const int64_t gi = g0 + k;
-      if (MIXED) acc[p] += cacc[k];
-      if (gi < g1) Ks[gi] = st.kmin + acc[p];
+      for (int p = 0; p < HK_PPL; ++p) {
+        const int k = wb + lane + 32 * p;
+        const int64_t gi = g0 + k;
+        if (MIXED) acc[p] = cacc[k];
+        if (gi < g1) Ks[gi] = st.kmin + acc[p];
+      }
+    } else {
+      // Split tile: publish this part's sums; the CTA that completes the
+      // tile's count adds the parts in part order (the result does not
+      // depend on which CTA ran which part or when).
+      double *pt = partial + ((int64_t)tt * nsplit + part) * HK_G;
+#pragma unroll
+      for (int p = 0; p < HK_PPL; ++p) {
+        const int k = wb + lane + 32 * p;
+        if (MIXED) acc[p] = cacc[k];
+        pt[k] = acc[p];
+      }
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) s_last = (atomicAdd(&tile_cnt[tt], 1u) == (unsigned)(nsplit - 1));
+      __syncthreads();
+      if (s_last) {
+        __threadfence();
+        const double *p0 = partial + (int64_t)tt * nsplit * HK_G;
+#pragma unroll
+        for (int p = 0; p < HK_PPL; ++p) {
+          const int k = wb + lane + 32 * p;
+          double sum = 0.0;
+          for (int j = 0; j < nsplit; ++j) sum += __ldcg(p0 + (int64_t)j * HK_G + k);
+          const int64_t gi = g0 + k;
+          if (gi < g1) Ks[gi] = st.kmin + sum;
+        }
+      }
     }
   }
 }
@@ -528,35 +664,73 @@ cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream) {
 // ------------------------------------------------------------- launchers
 int voigt_tile_points() { return HK_G; }
 
-cudaError_t launch_voigt_sum(bool mixed, const LinePrep *prep_d, const double *nu0_d,
-                             int64_t nlines, const GridDev &g, const StateDev *states_d,
-                             int nstates, unsigned *ticket_d, double *K_d, int64_t k_stride,
-                             int grid_ctas, cudaStream_t stream) {
-  const int tps = (int)((g.nx + HK_G - 1) / HK_G);
-  const int total = tps * nstates;
-  cudaError_t e = cudaMemsetAsync(ticket_d, 0, sizeof(unsigned), stream);
-  if (e != cudaSuccess) return e;
-  if (total <= 0) return cudaSuccess;
+static int voigt_ctas(bool mixed) {
   int dev = 0, nsm = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const size_t smem = mixed ? HK_SMEM_MIXED : sizeof(RecD) * HK_CH;
   if (mixed) {
-    e = cudaFuncSetAttribute(voigt_sum_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    cudaFuncSetAttribute(voigt_sum_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, voigt_sum_kernel<true>, HK_THREADS, smem);
   } else {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, voigt_sum_kernel<false>, HK_THREADS, smem);
   }
-  if (per_sm < 1) per_sm = 1;
-  int ctas = grid_ctas > 0 ? grid_ctas : nsm * per_sm;
-  if (ctas > total) ctas = total;
+  return nsm * (per_sm < 1 ? 1 : per_sm);
+}
+
+// Tiles are split along their line range when a state has few tiles: one
+// tile's sweep lasts ~1/3 of a 1e7-line state, so an unsplit 1465-tile grid
+// ends in a last wave that leaves most of the GPU idle for that long.  The
+// split depends on the grid only (HK_TICKETS_PER_STATE, about 8 tickets per
+// resident CTA of a 148-SM B200 at 4 CTAs/SM), never on the batch or the
+// device, so one state's K is bit-identical however it is batched.
+constexpr int HK_TICKETS_PER_STATE = 4736;
+constexpr int HK_MAX_SPLIT = 8;
+
+int voigt_nsplit(int64_t nx) {
+  const int64_t tps = (nx + HK_G - 1) / HK_G;
+  if (tps <= 0) return 1;
+  return (int)std::min<int64_t>(HK_MAX_SPLIT,
+                                std::max<int64_t>(1, (HK_TICKETS_PER_STATE + tps - 1) / tps));
+}
+
+VoigtPlan plan_voigt_sum(bool mixed, int64_t nx, int nstates, int grid_ctas) {
+  VoigtPlan pl;
+  pl.tiles_per_state = (int)((nx + HK_G - 1) / HK_G);
+  pl.tiles = (int64_t)pl.tiles_per_state * nstates;
+  pl.ctas = grid_ctas > 0 ? grid_ctas : voigt_ctas(mixed);
+  pl.nsplit = voigt_nsplit(nx);
+  pl.partial_doubles = pl.nsplit > 1 ? (size_t)pl.tiles * pl.nsplit * HK_G : 0;
+  pl.counters = pl.nsplit > 1 ? (size_t)pl.tiles : 0;
+  return pl;
+}
+
+cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const LinePrep *prep_d,
+                             const double *nu0_d, int64_t nlines, const GridDev &g,
+                             const StateDev *states_d, unsigned *ticket_d, double *partial_d,
+                             unsigned *tile_cnt_d, double *K_d, int64_t k_stride,
+                             cudaStream_t stream) {
+  const int64_t total64 = pl.tiles * pl.nsplit;
+  if (total64 > 0x7fffffff) return cudaErrorInvalidValue;
+  const int total = (int)total64;
+  cudaError_t e = cudaMemsetAsync(ticket_d, 0, sizeof(unsigned), stream);
+  if (e != cudaSuccess) return e;
+  if (total <= 0) return cudaSuccess;
+  if (pl.nsplit > 1) {
+    if (!partial_d || !tile_cnt_d) return cudaErrorInvalidValue;
+    e = cudaMemsetAsync(tile_cnt_d, 0, sizeof(unsigned) * pl.counters, stream);
+    if (e != cudaSuccess) return e;
+  }
+  const size_t smem = mixed ? HK_SMEM_MIXED : sizeof(RecD) * HK_CH;
+  const int ctas = (int)std::min<int64_t>(pl.ctas, total);
   if (mixed)
-    voigt_sum_kernel<true><<<ctas, HK_THREADS, smem, stream>>>(prep_d, nu0_d, nlines, g, states_d,
-                                                               tps, total, ticket_d, K_d, k_stride);
+    voigt_sum_kernel<true><<<ctas, HK_THREADS, smem, stream>>>(
+        prep_d, nu0_d, nlines, g, states_d, pl.tiles_per_state, pl.nsplit, total, ticket_d,
+        partial_d, tile_cnt_d, K_d, k_stride);
   else
-    voigt_sum_kernel<false><<<ctas, HK_THREADS, smem, stream>>>(prep_d, nu0_d, nlines, g, states_d,
-                                                                tps, total, ticket_d, K_d, k_stride);
+    voigt_sum_kernel<false><<<ctas, HK_THREADS, smem, stream>>>(
+        prep_d, nu0_d, nlines, g, states_d, pl.tiles_per_state, pl.nsplit, total, ticket_d,
+        partial_d, tile_cnt_d, K_d, k_stride);
   return cudaGetLastError();
 }
 

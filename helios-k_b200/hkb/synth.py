@@ -72,11 +72,11 @@ WORKLOADS = {
                    numin=0.0, numax=30000.0, dnu=0.01, cut=25.0, nbins=300, nC=20),
     "adjoint": dict(n=1_000_000, seed=3, logS=(-30.0, -18.0), T=[800.0], P=[1.0],
                     numin=1000.0, numax=10000.0, dnu=0.01, cut=100.0, nbins=300, nC=20),
-    # a 3000 cm^-1 band of the hitemp list at the same line density (used
-    # for profiler captures: same per-pair mix, 1/10 of the work)
-    "hitemp_slice": dict(n=1_000_000, seed=1, logS=(-32.0, -18.0), T=[1500.0], P=[0.1],
-                         numin=15000.0, numax=18000.0, dnu=0.01, cut=25.0, nbins=30, nC=20,
-                         nu_min=15000.0, nu_max=18000.0),
+    # the hitemp line distribution at 1/10 of the line density over the same
+    # grid (used for profiler captures: same tiles and per-pair mix, 1/10 of
+    # the work, ~150 MB on the device)
+    "hitemp_sparse": dict(n=1_000_000, seed=1, logS=(-32.0, -18.0), T=[1500.0], P=[0.1],
+                          numin=0.0, numax=30000.0, dnu=0.01, cut=25.0, nbins=300, nC=20),
 }
 
 

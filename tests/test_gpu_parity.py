@@ -127,6 +127,66 @@ def test_opacity_cut_modes(small, mode, cut):
     assert masked_relerr(Km, Kref, NBINS)[0] < 1e-5
 
 
+def test_opacity_fine_grid_unsplit_tiles(small):
+    """A grid of >= 4736 tiles runs every tile as one ticket; the 300000-point
+    grid of the other tests splits each tile's line range into 8 parts whose
+    sums are combined in part order.  Both must match the oracle."""
+    ctx = small["ctx"]
+    numin, numax, dnu, nbins = 0.0, 1000.0, 1e-4, 10
+    ctx.set_grid(numin, numax, dnu, nbins, 0, 25.0)
+    nx = ctx.nx
+    assert nx == oracle.grid_nx(numin, numax, dnu)
+    assert -(-nx // hkb.tile_points()) >= 4736
+    T, P = 1500.0, 0.1
+    Km = ctx.opacity([T], [P], hkb.MIXED)[0]
+    Kp = ctx.opacity([T], [P], hkb.PLAIN_FP64)[0]
+    Q = oracle.partition(small["Tq"], small["Qq"], T)
+    nu, S, iad, vy = oracle.prep_hitran(small["L"], [synth.MASS], [1.0], [Q], T, P, qalphaL=1.0)
+    win = oracle.windows(nu, S, iad, vy, numin, dnu, nx, 0, 25.0)
+    for ib in (0, 4_000_000 + 777, nx - 20000):
+        Kr, _ = oracle.opacity(nu, S, iad, vy, win, numin, dnu, nx, irange=(ib, ib + 20000))
+        sl = slice(ib, ib + 20000)
+        mask = Kr > 1e-6 * Kr.max()
+        ep = np.max(np.abs(Kp[sl] - Kr)[mask] / Kr[mask])
+        em = np.max(np.abs(Km[sl] - Kr)[mask] / Kr[mask])
+        print(f"fine grid [{ib}, +20000): plain {ep:.2e} mixed {em:.2e}")
+        assert ep < 1e-12
+        assert em < 1e-5
+
+
+def test_opacity_extreme_strength_range():
+    """Strengths over 270 decades: the mixed form sums each 2^96 band of line
+    strengths ('level') in FP32 with its own power-of-two scale, and lines
+    more than 2^768 below the strongest in FP64; lines near nu = 0 (tiny
+    Doppler width, huge x) also take the FP64 path.  All must match the
+    oracle."""
+    L = synth.hitran_lines(6000, seed=21, logS=(-290.0, -18.0), nu_max=3000.0)
+    L["nu"][:3] = [1e-3, 0.05, 2.0]
+    Tq, Qq = synth.q_table()
+    T, P = 900.0, 0.3
+    with hkb.Context(0) as ctx:
+        ctx.set_species(hkb.HITRAN, [synth.MASS], [1.0])
+        ctx.set_partition(0, Tq, Qq)
+        ctx.set_options(qalphaL=1.0)
+        ctx.load_lines_hitran(L)
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+        Km = ctx.opacity([T], [P], hkb.MIXED)[0]
+    Q = oracle.partition(Tq, Qq, T)
+    nu, S, iad, vy = oracle.prep_hitran(L, [synth.MASS], [1.0], [Q], T, P, qalphaL=1.0)
+    nx = oracle.grid_nx(NUMIN, NUMAX, DNU)
+    win = oracle.windows(nu, S, iad, vy, NUMIN, DNU, nx, 0, 25.0)
+    Kr, _ = oracle.opacity(nu, S, iad, vy, win, NUMIN, DNU, nx)
+    term = S * vy / np.pi / np.maximum(100.0, vy * vy)
+    print("decades of line terms:", np.log10(term.max() / term[term > 0].min()))
+    em, n = masked_relerr(Km, Kr, NBINS)
+    # every point, not only those above 1e-6 of their bin maximum
+    pos = Kr > 1e-280  # clear of FP64 subnormals
+    eall = np.max(np.abs(Km[pos] - Kr[pos]) / Kr[pos])
+    print(f"extreme range: mixed {em:.2e} over {n} pts, all points {eall:.2e}")
+    assert em < 1e-5
+    assert eall < 1e-5
+
+
 def test_batched_states_equal_single_states(small):
     ctx = small["ctx"]
     ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
