@@ -34,7 +34,7 @@ sys.path.insert(0, os.path.join(ROOT, "helios-k_b200"))
 # figure grows with the Algorithm 916 series length n_iter) + 2 for the
 # strength multiply-add into the sum
 F_A, F_B, F_C0, F_C_ITER, F_ACC = 6, 20, 30, 12, 2
-SIZEOF_STATE = 576  # bytes of hkb::StateDev copied per state per call
+SIZEOF_STATE = 600  # bytes of hkb::StateDev copied per state per call
 
 
 def parse():

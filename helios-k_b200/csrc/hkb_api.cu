@@ -432,7 +432,8 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   }
   // States run in batches whose per-(state, line) records fit the prep
   // budget; each batch is one prep launch and one persistent Voigt launch.
-  const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * sizeof(LinePrep);
+  const bool mixed = precision == HK_PRECISION_MIXED;
+  const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
   int batch = (int)std::max<size_t>(1, c->prep_budget / per_state);
   const int nsplit = voigt_nsplit(nx);
   if (nsplit > 1) {
@@ -447,7 +448,6 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   unsigned long long *wb = c->wbits.as<unsigned long long>();
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
-  const bool mixed = precision == HK_PRECISION_MIXED;
   for (int b0 = 0; b0 < nstates; b0 += batch) {
     const int nb = std::min(batch, nstates - b0);
     const VoigtPlan plan = plan_voigt_sum(mixed, nx, nb, 0);
@@ -455,9 +455,9 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
       CUDA_TRY(c, c->vpart.ensure(plan.partial_doubles * sizeof(double)));
       CUDA_TRY(c, c->vcnt.ensure(plan.counters * sizeof(unsigned)));
     }
-    CUDA_TRY(c, launch_line_prep(c->L, c->g, sd + b0, nb, c->prep.as<LinePrep>(), wb + 2 * b0, s));
+    CUDA_TRY(c, launch_line_prep(mixed, c->L, c->g, sd + b0, nb, c->prep.p, wb + 2 * b0, s));
     CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
-    CUDA_TRY(c, launch_voigt_sum(mixed, plan, c->prep.as<LinePrep>(), c->L.nu0, c->nlines, c->g,
+    CUDA_TRY(c, launch_voigt_sum(mixed, plan, c->prep.p, c->L.nu0, c->nlines, c->g,
                                  sd + b0, c->ticket.as<unsigned>(), c->vpart.as<double>(),
                                  c->vcnt.as<unsigned>(), Kd + (size_t)b0 * nx, nx, s));
     CUDA_TRY(c, cudaEventRecord(c->ev[1], s));

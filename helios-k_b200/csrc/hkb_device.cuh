@@ -335,6 +335,7 @@ constexpr float HK_ASY_R2 = 36.0f;
 constexpr int HK_ASY_K = 8;
 
 __device__ __forceinline__ float voigt_asy(float x, float y) {
+  x = fabsf(x);
   const float x2 = x * x, y2 = y * y;
   const float r2 = x2 + y2;
   const float ir2 = rcp_fast(r2);
@@ -356,14 +357,14 @@ __device__ __forceinline__ float voigt_asy(float x, float y) {
   return v;
 }
 
-__device__ __forceinline__ float voigt916_tab(float x, float y, float ey, float sig1,
-                                              const float *__restrict__ R) {
+// Algorithm 916 with the per-line table R, valid for |x| < 6.3 (m_c <= 10)
+__device__ __forceinline__ float voigt916_core(float x, float y, float ey, float sig1,
+                                               const float *__restrict__ R) {
   const float a = HK_A916_F;
   const float a2 = a * a;
   const float L2E = 1.4426950408889634f;  // log2(e)
   const float G = 0.48675662279129028f;   // exp(-2 a^2)
   x = fabsf(x);
-  if (fmaf(x, x, y * y) >= HK_ASY_R2) return voigt_asy(x, y);
   const float ex2 = expf(-x * x);
   if (x == 0.f) return ey;
   if (y == 0.f) return ex2;
@@ -409,6 +410,14 @@ __device__ __forceinline__ float voigt916_tab(float x, float y, float ey, float 
   const float t2 = sinxy * ex2 * sinxy / y;
   const float t3 = y * (-cos2xy * s1 + 0.5f * (s2 + s3));
   return fmaf(ex2 * ey, cos2xy, HK_C916_F * (t2 + t3));
+}
+
+// region C in FP32: the asymptotic series for r >= 6, Algorithm 916 below
+__device__ __forceinline__ float voigt916_tab(float x, float y, float ey, float sig1,
+                                              const float *__restrict__ R) {
+  x = fabsf(x);
+  if (fmaf(x, x, y * y) >= HK_ASY_R2) return voigt_asy(x, y);
+  return voigt916_core(x, y, ey, sig1, R);
 }
 
 }  // namespace hkb

@@ -17,9 +17,11 @@ constexpr int KD_SMEM_LIMIT = 225 * 1024;
 int voigt_tile_points();
 cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream);
 
-cudaError_t launch_line_prep(const LinesDev &L, const GridDev &g, StateDev *states_d,
-                             int nstates, LinePrep *prep_d, unsigned long long *wbits_d,
+// per-(line, state) records: LinePrepF (mixed) or LinePrep (plain FP64)
+cudaError_t launch_line_prep(bool mixed, const LinesDev &L, const GridDev &g, StateDev *states_d,
+                             int nstates, void *prep_d, unsigned long long *wbits_d,
                              cudaStream_t stream);
+inline size_t line_prep_bytes(bool mixed) { return mixed ? sizeof(LinePrepF) : sizeof(LinePrep); }
 
 // Work plan of one Voigt launch: (state, tile) tickets, each tile's line
 // range split into nsplit parts when there are too few tiles to fill the GPU
@@ -35,7 +37,7 @@ struct VoigtPlan {
 };
 VoigtPlan plan_voigt_sum(bool mixed, int64_t nx, int nstates, int grid_ctas);
 int voigt_nsplit(int64_t nx);  // line-range parts per tile for a grid of nx points
-cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &plan, const LinePrep *prep_d,
+cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &plan, const void *prep_d,
                              const double *nu0_d, int64_t nlines, const GridDev &g,
                              const StateDev *states_d, unsigned *ticket_d, double *partial_d,
                              unsigned *tile_cnt_d, double *K_d, int64_t k_stride,

@@ -76,37 +76,80 @@ cudaError_t sort_lines_by_nu(int64_t n, double *nu_d, int64_t *order_d,
 // term, which sets the power-of-two scale of the mixed form's FP32 sums.
 // wbits holds two words per state: {half-width bits, term bits} (both
 // non-negative doubles, so their bit patterns order like the values).
+template <bool MIXED>
 __global__ void __launch_bounds__(256)
 line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
-                 LinePrep *__restrict__ out, unsigned long long *__restrict__ wbits) {
+                 void *__restrict__ out, unsigned long long *__restrict__ wbits) {
   const int s = blockIdx.y;
   const StateDev &st = states[s];
-  LinePrep *O = out + (int64_t)s * L.n;
   double w_loc = 0.0, s1_loc = 0.0;
   for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < L.n;
        l += (int64_t)gridDim.x * blockDim.x) {
     const LineState ls = prep_line(L, st, l);
     int64_t w[6];
     line_windows(g, st, ls, 0, g.nx, w);
-    LinePrep r;
-    r.nu = ls.nu;
-    r.iad = ls.iad;
-    r.vy = ls.vy;
-    r.S1 = ls.S * ls.vy / CUDART_PI;
-    r.Sc = ls.S * (1.0 / 1.7724538509055160273);
+    const double S1 = ls.S * ls.vy / CUDART_PI;
+    const double Sc = ls.S * (1.0 / 1.7724538509055160273);
     const bool hasC = w[3] > w[2];
-    r.ey = hasC ? erfcx(ls.vy) : 1.0;
-    r.sig1 = hasC ? (float)c916_sig1(ls.vy) : 0.f;
-    r.i0 = (int)w[0];
-    r.b0 = (int)w[1];
-    r.c0 = (int)w[2];
-    r.c1 = (int)w[3];
-    r.b1 = (int)w[4];
-    r.i1 = (int)w[5];
-    r.pad = 0;
-    O[l] = r;
+    const double ey = hasC ? erfcx(ls.vy) : 1.0;
+    const float sig1 = hasC ? (float)c916_sig1(ls.vy) : 0.f;
     // largest region-A/B term of the line: S1 / r^2 with r^2 >= max(100, y^2)
-    if (w[5] > w[0]) s1_loc = fmax(s1_loc, r.S1 / fmax(100.0, ls.vy * ls.vy));
+    const double Y = ls.vy * ls.vy;
+    const double term = S1 / fmax(100.0, Y);
+    if (MIXED) {
+      LinePrepF r;
+      r.nu = ls.nu;
+      r.iad = ls.iad;
+      r.S1 = S1;
+      r.Sc = Sc;
+      r.y = (float)ls.vy;
+      r.ey = (float)ey;
+      r.sig1 = sig1;
+      const double A2 = 2.0 * Y + 3.0 - 6.0 / CUDART_PI, B2 = (Y + 1.5) * (Y + 1.5);
+      r.A1 = (float)(2.0 * Y + 2.5 - 4.0 / CUDART_PI);
+      r.B1 = (float)((Y + 1.5) * (Y + 1.0));
+      r.D2 = (float)(A2 + Y);
+      r.D1 = (float)(B2 + A2 * Y);
+      r.D0 = (float)(B2 * Y);
+      int ex = -100000;
+      if (term > 0.0) frexp(term, &ex);
+      r.ex = ex;
+      int flags = 0;
+      if (w[5] > w[0]) {
+        // the largest |x| inside the cut window (at its first or last point)
+        const double xa = fabs((grid_x(g, w[0]) - ls.nu) * ls.iad);
+        const double xb = fabs((grid_x(g, w[5] - 1) - ls.nu) * ls.iad);
+        const double umax = fmax(xa, xb) * fmax(xa, xb) + Y;
+        if (umax >= 1e18) flags |= HK_PF_WIDE;
+        if (fmax(100.0, Y) < 0x1p-64 * umax || Y > 0x1p60) flags |= HK_PF_RANGE;
+      }
+      r.flags = flags;
+      r.i0 = (int)w[0];
+      r.b0 = (int)w[1];
+      r.c0 = (int)w[2];
+      r.c1 = (int)w[3];
+      r.b1 = (int)w[4];
+      r.i1 = (int)w[5];
+      reinterpret_cast<LinePrepF *>(out)[(int64_t)s * L.n + l] = r;
+    } else {
+      LinePrep r;
+      r.nu = ls.nu;
+      r.iad = ls.iad;
+      r.vy = ls.vy;
+      r.S1 = S1;
+      r.Sc = Sc;
+      r.ey = ey;
+      r.sig1 = sig1;
+      r.i0 = (int)w[0];
+      r.b0 = (int)w[1];
+      r.c0 = (int)w[2];
+      r.c1 = (int)w[3];
+      r.b1 = (int)w[4];
+      r.i1 = (int)w[5];
+      r.pad = 0;
+      reinterpret_cast<LinePrep *>(out)[(int64_t)s * L.n + l] = r;
+    }
+    if (w[5] > w[0]) s1_loc = fmax(s1_loc, term);
     if (ls.S != 0.0 && ls.iad > 0.0) {
       if (g.cutMode == 1) w_loc = fmax(w_loc, g.cut * ls.vy / ls.iad);
       else if (g.cutMode == 2) w_loc = fmax(w_loc, g.cut / ls.iad);
@@ -141,10 +184,11 @@ __global__ void state_finalize_kernel(GridDev g, StateDev *__restrict__ states,
   }
   states[s].s1scale = ldexp(1.0, e);
   states[s].s1unscale = ldexp(1.0, -e);
+  states[s].s1exp = e;
 }
 
-cudaError_t launch_line_prep(const LinesDev &L, const GridDev &g, StateDev *states_d,
-                             int nstates, LinePrep *prep_d, unsigned long long *wbits_d,
+cudaError_t launch_line_prep(bool mixed, const LinesDev &L, const GridDev &g, StateDev *states_d,
+                             int nstates, void *prep_d, unsigned long long *wbits_d,
                              cudaStream_t stream) {
   cudaError_t e = cudaMemsetAsync(wbits_d, 0, 2 * nstates * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return e;
@@ -152,7 +196,10 @@ cudaError_t launch_line_prep(const LinesDev &L, const GridDev &g, StateDev *stat
     const int64_t nb = (L.n + 255) / 256;
     const int bx = (int)(nb < 2368 ? nb : 2368);
     dim3 grid(bx, nstates);
-    line_prep_kernel<<<grid, 256, 0, stream>>>(L, g, states_d, prep_d, wbits_d);
+    if (mixed)
+      line_prep_kernel<true><<<grid, 256, 0, stream>>>(L, g, states_d, prep_d, wbits_d);
+    else
+      line_prep_kernel<false><<<grid, 256, 0, stream>>>(L, g, states_d, prep_d, wbits_d);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

@@ -63,6 +63,28 @@ struct __align__(16) LinePrep {
   int pad;
 };
 
+// The same line and state for the mixed form (96 bytes): everything that
+// depends on the line and the state only, so staging a line into a tile adds
+// just the tile's offsets and the strength level.
+//   A1 = 2Y + 2.5 - 4/pi, B1 = (Y+1.5)(Y+1)      (GH2 numerator, Y = vy^2)
+//   D2 = A2 + Y, D1 = B2 + A2 Y, D0 = B2 Y         (GH2 denominator expanded,
+//   A2 = 2Y + 3 - 6/pi, B2 = (Y+1.5)^2)
+//   ex: frexp exponent of the line's largest region-A/B term S1 / max(100, Y)
+//   flags: HK_PF_WIDE  -- some x^2 + Y in the cut window reaches 1e18;
+//          HK_PF_RANGE -- the window's terms span more than 2^64, or Y > 2^60:
+//                         FP32 sums cannot hold the line (FP64 instead).
+constexpr int HK_PF_WIDE = 2, HK_PF_RANGE = 1;
+struct __align__(16) LinePrepF {
+  double nu, iad;
+  double S1, Sc;
+  float y, ey, sig1;
+  float A1, B1;
+  float D2, D1, D0;
+  int ex, flags;
+  int i0, b0, c0, c1, b1, i1;
+};
+static_assert(sizeof(LinePrepF) == 96, "LinePrepF layout");
+
 // Per-(T, P) constants formed on the host.
 struct StateDev {
   double T, P;
@@ -74,10 +96,12 @@ struct StateDev {
   double kmin;
   double s1scale;    // 2^e, largest region-A/B term S1/max(100, y^2) * 2^e in [2^39, 2^40)
   double s1unscale;  // 2^-e
+  int s1exp, pad0;   // e
   double iad0[HK_MAX_ISO];  // c sqrt(m / (2 kB T))
   double Q[HK_MAX_ISO];     // partition function at T
   double ab[HK_MAX_ISO];    // abundance * (m / meanMass) when units == 0
   double ss[HK_MAX_ISO];    // species scale * (m / meanMass) when units == 0
 };
+static_assert(sizeof(StateDev) == 600, "StateDev layout (the host copies it per state)");
 
 }  // namespace hkb

@@ -39,52 +39,48 @@ constexpr int HK_G = HK_WARPS * HK_SLICE;    // points per tile (2048)
 constexpr int HK_CH = 128;                   // lines per staged chunk
 static_assert(HK_G <= 2048, "k * vb_hi must stay exact in FP32 (11 bits)");
 
-// Staged line record of the mixed form.  The FP32 line constants are stored
-// twice ({v, v}) so the packed f32x2 sweep (two grid points per
-// instruction) reads them as ready-made float2 operands.  Regions A and B
-// are summed in FP32 (flushed into the FP64 per-point sums after every
-// chunk of lines) with the line strength folded into the coefficients:
+// Staged line record of the mixed form.  Regions A and B are summed in FP32
+// (flushed into the FP64 per-point sums at least once per chunk of lines)
+// with the line strength folded into the coefficients:
 //   A:  S1f / (s + Y),
 //   B:  S1f t4 = (s (S1f s + C1) + C0) / (((s + D2) s + D1) s + D0),
-// s = x^2, Y = y^2, S1f = S1 * s1scale (a power of two per state),
-// C1 = S1f A1, C0 = S1f B1, and the GH2 denominator (s + Y)(s (s + A2) + B2)
-// expanded: D2 = A2 + Y, D1 = B2 + A2 Y, D0 = B2 Y, with A1 = 2Y + 2.5 - 4/pi,
+// s = x^2, Y = y^2, S1f = S1 * 2^(s1exp + 96 lev) (below), C1 = S1f A1,
+// C0 = S1f B1, and the GH2 denominator (s + Y)(s (s + A2) + B2) expanded:
+// D2 = A2 + Y, D1 = B2 + A2 Y, D0 = B2 Y, with A1 = 2Y + 2.5 - 4/pi,
 // B1 = (Y+1.5)(Y+1), A2 = 2Y + 3 - 6/pi, B2 = (Y+1.5)^2.  Every coefficient
 // is positive, so neither form cancels.
+// x at tile point k, regions A and B: x = (k - kc) vb + fr, kc the point
+// nearest the line centre (|fr| <= vb/2): the subtraction is exact, so x
+// carries ~2 roundings relative to itself.  Region C, where x crosses zero,
+// uses the double-float split x = (dh + k vbh) + (dl + k vbl) instead.
 struct __align__(16) RecF {
-  float2 dh, dl;           // x at the tile start (hi, lo)
-  float2 vbh, vbl;         // x step per grid point (hi, lo)
-  float2 S1f, C1;
-  float2 C0, D2;
-  float2 D1, D0;
+  float S1f, C1, C0, D2;
+  float D1, D0, nkc, vb;   // nkc = -kc
+  float fr, y, ey, sig1;   // y, erfcx(y), region-C series constant
+  float dh, dl, vbh, vbl;  // region C: x at the tile start, step (hi, lo)
   double Sc;               // S/sqrt(pi) (region C, FP64 sum)
-  float y, ey, sig1;       // y, erfcx(y), region-C series constant
-  int i0, b0, c0, c1, b1;  // tile-local window boundaries
-  int i1, flags;
+  int i0, b0, c0, c1;      // tile-local window boundaries
+  int b1, i1, flags, pad;
 };
-static_assert(sizeof(RecF) == 128, "RecF layout");
+static_assert(sizeof(RecF) == 112, "RecF layout");
 
-// flags: HK_F_WEAK -- the line's smallest FP32 term in this tile,
-// S1f / (x_max^2 + Y), would fall below HK_TERM_MIN (near the FP32 normal
-// range), or S1f itself is above 2^100 (y^2 beyond ~2^60): the line is
-// summed in FP64 with S1f = 1 (unscaled coefficients);
-// HK_F_WIDE -- x_max^2 + Y >= 1e18, so two region-A denominators may not be
-// multiplied in FP32 (paired reciprocals are off).
-// Strength levels: S1f = S1 * s1scale * 2^(HK_LEVEL_BITS * lev) puts every
-// line's largest term near 2^40 whatever its strength; a warp sums the lines
-// of one level at a time in FP32 and flushes (exactly unscaled) into the FP64
-// sums when the level changes, so FP32 never holds terms of lines more than
-// 2^96 apart.  Levels above HK_MAX_LEVEL (2^768 below the strongest line)
-// take the FP64 path.  The level sits in flags bits 8-11.
+// Strength levels: with 2^(40 - s1exp) the state's largest region-A/B term
+// S1 / max(100, Y), a line of level lev = (40 - ex - s1exp) / 96 (ex: the
+// exponent of its own largest term) gets S1f = S1 * 2^(s1exp + 96 lev), which
+// puts its largest term in (2^-56, 2^40] whatever its strength.  A warp sums
+// the lines of one level at a time in FP32 and flushes (exactly unscaled)
+// into the FP64 sums when the level changes, so FP32 never holds terms of
+// lines more than 2^96 apart, and a line's smallest term (at most 2^64 below
+// its largest, else HK_PF_RANGE) stays a normal float.  With those bounds
+// S1f s^2 < 2^100 and d0 d1 < 2^120 in region B.
+// flags: HK_F_WEAK -- level above HK_MAX_LEVEL (2^768 below the strongest
+// line) or HK_PF_RANGE: the line is summed in FP64 with S1f = 1;
+// HK_F_WIDE -- some x^2 + Y in the window reaches 1e18, so two region-A
+// denominators may not be multiplied in FP32 (paired reciprocals are off).
+// The level sits in flags bits 8-11.
 constexpr int HK_F_WEAK = 1, HK_F_WIDE = 2;
-constexpr double HK_TERM_MIN = 0x1p-120;
 constexpr int HK_LEVEL_BITS = 96;
 constexpr int HK_MAX_LEVEL = 7;
-
-// 2^e as a double, exact for -1022 <= e <= 1023
-__device__ __forceinline__ double pow2_d(int e) {
-  return __longlong_as_double((long long)(1023 + e) << 52);
-}
 
 // Shared memory of one mixed-form CTA: staged records, the per-line
 // region-C denominator tables (8 leading pad floats keep R[m-1-k] of the
@@ -138,119 +134,131 @@ __device__ __forceinline__ float2 f2(double v) {
 // Clip one line's global windows to the tile [g0, g1) and fill the staged
 // record.  Clipping the oracle's global boundaries equals searching the
 // clipped range, because every window predicate is monotone on its range.
-// Lines with S = 0 contribute nothing and are staged empty.
-template <bool MIXED>
-__device__ __forceinline__ void stage_line(const LinePrep *__restrict__ P,
-                                           const GridDev &g, int64_t l,
-                                           int64_t g0, int64_t g1, double s1scale,
-                                           void *recp, float *__restrict__ Rtab) {
+// Lines with S = 0 have empty windows and are staged empty.
+//
+// Mixed form, in two steps: line_key gives the line's sort key within the
+// chunk -- its strength level (0..HK_MAX_LEVEL), HK_MAX_LEVEL + 1 for lines
+// summed in FP64 (weak), HK_MAX_LEVEL + 2 for lines without points in the
+// tile -- and stage_mixed builds the record for that key.
+constexpr int HK_NKEY = HK_MAX_LEVEL + 3;
+constexpr int HK_KEY_WEAK = HK_MAX_LEVEL + 1, HK_KEY_EMPTY = HK_MAX_LEVEL + 2;
+
+__device__ __forceinline__ int line_key(const LinePrepF *__restrict__ P, int64_t l,
+                                        int64_t g0, int64_t g1, int s1exp) {
+  const LinePrepF &lp = P[l];
+  const int i0 = clip_local(lp.i0, g0, g1), i1 = clip_local(lp.i1, g0, g1);
+  if (i1 <= i0) return HK_KEY_EMPTY;
+  // the state's largest term has exponent 40 - s1exp, so 40 - (ex + s1exp) >= 0
+  const int lev = (40 - (lp.ex + s1exp)) / HK_LEVEL_BITS;
+  if ((lp.flags & HK_PF_RANGE) || lev > HK_MAX_LEVEL) return HK_KEY_WEAK;
+  return lev;
+}
+
+__device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, const GridDev &g,
+                                            int64_t l, int64_t g0, int64_t g1, int s1exp,
+                                            int key, RecF &r) {
+  const LinePrepF lp = P[l];
+  const bool nonempty = key != HK_KEY_EMPTY;
+  const bool weak = key == HK_KEY_WEAK;
+  const int lev = (weak || !nonempty) ? 0 : key;
+  const double D0 = __dmul_rn(__dsub_rn(grid_x(g, g0), lp.nu), lp.iad);
+  const double vb = __dmul_rn(g.dnu, lp.iad);
+  const float dh = (float)D0;
+  const float dl = (float)(D0 - (double)dh);
+  const float vbh = __uint_as_float(__float_as_uint((float)vb) & 0xFFFFF800u);  // 13 bits
+  const float vbl = (float)(vb - (double)vbh);
+  // the tile point nearest the centre (|kc| <= 2^23 keeps k - kc exact)
+  const double kc = fmin(fmax(rint(-D0 / vb), -8388608.0), 8388608.0);
+  // S1f = S1 * 2^(s1exp + 96 lev): the line's largest term near 2^40
+  const double S1f = weak ? 1.0 : ldexp(lp.S1, s1exp + HK_LEVEL_BITS * lev);
+  r.S1f = (float)S1f;
+  r.C1 = (float)(S1f * (double)lp.A1);
+  r.C0 = (float)(S1f * (double)lp.B1);
+  r.D2 = lp.D2;
+  r.D1 = lp.D1;
+  r.D0 = lp.D0;
+  r.nkc = (float)(-kc);
+  r.vb = (float)vb;
+  r.fr = (float)(D0 + kc * vb);
+  r.dh = dh;
+  r.dl = dl;
+  r.vbh = vbh;
+  r.vbl = vbl;
+  r.Sc = lp.Sc;
+  r.y = lp.y;
+  r.ey = lp.ey;
+  r.sig1 = lp.sig1;
+  r.i0 = nonempty ? clip_local(lp.i0, g0, g1) : 0;
+  r.b0 = clip_local(lp.b0, g0, g1);
+  r.c0 = clip_local(lp.c0, g0, g1);
+  r.c1 = clip_local(lp.c1, g0, g1);
+  r.b1 = clip_local(lp.b1, g0, g1);
+  r.i1 = nonempty ? clip_local(lp.i1, g0, g1) : 0;
+  r.flags = ((lp.flags & HK_PF_WIDE) ? HK_F_WIDE : 0) | (weak ? HK_F_WEAK : 0) | (lev << 8);
+  r.pad = 0;
+}
+
+// region C inside the tile: denominators of the Algorithm-916 series
+__device__ __forceinline__ void stage_rtab(float y, float *__restrict__ Rtab) {
+  const float a2 = HK_A916_F * HK_A916_F;
+  const float Yf = y * y;
+#pragma unroll 2
+  for (int m = 1; m <= HK_C916_MR; ++m) Rtab[m - 1] = rcp_fast(fmaf(a2 * m, (float)m, Yf));
+}
+
+__device__ __forceinline__ void stage_plain(const LinePrep *__restrict__ P, int64_t l,
+                                            int64_t g0, int64_t g1, RecD *recp) {
   const LinePrep lp = P[l];
   int li[6] = {clip_local(lp.i0, g0, g1), clip_local(lp.b0, g0, g1),
                clip_local(lp.c0, g0, g1), clip_local(lp.c1, g0, g1),
                clip_local(lp.b1, g0, g1), clip_local(lp.i1, g0, g1)};
   const bool nonempty = li[5] > li[0] && lp.Sc != 0.0;
-  if (MIXED) {
-    RecF r;
-    const double D0 = __dmul_rn(__dsub_rn(grid_x(g, g0), lp.nu), lp.iad);
-    const double vb = __dmul_rn(g.dnu, lp.iad);
-    const float dh = (float)D0;
-    const float dl = (float)(D0 - (double)dh);
-    const float vbh = __uint_as_float(__float_as_uint((float)vb) & 0xFFFFF800u);  // 13 bits
-    const float vbl = (float)(vb - (double)vbh);
-    const double Y = lp.vy * lp.vy;
-    const double A1 = 2.0 * Y + 2.5 - 4.0 / CUDART_PI, B1 = (Y + 1.5) * (Y + 1.0);
-    const double A2 = 2.0 * Y + 3.0 - 6.0 / CUDART_PI, B2 = (Y + 1.5) * (Y + 1.5);
-    const double xe = D0 + (double)(g1 - g0 - 1) * vb;  // x at the tile's last point
-    const double xm = fmax(fabs(D0), fabs(xe));
-    const double umax = xm * xm + Y;
-    // strength level: the line's largest region-A/B term S1/max(100, Y),
-    // scaled by the state, lies in (2^(40-96(lev+1)), 2^(40-96 lev)]
-    int lev = 0;
-    const double term = lp.S1 / fmax(100.0, Y) * s1scale;
-    if (term > 0.0) {
-      int ex = 0;
-      frexp(term, &ex);  // term in [2^(ex-1), 2^ex), ex <= 40
-      lev = (40 - ex) / HK_LEVEL_BITS;
-    }
-    double S1f = lp.S1 * s1scale * pow2_d(HK_LEVEL_BITS * min(lev, HK_MAX_LEVEL));
-    int flags = umax >= 1e18 ? HK_F_WIDE : 0;
-    if (lev > HK_MAX_LEVEL || S1f < HK_TERM_MIN * umax || S1f > 0x1p100) {
-      flags |= HK_F_WEAK;
-      S1f = 1.0;
-      lev = 0;
-    }
-    flags |= lev << 8;
-    r.dh = make_float2(dh, dh);
-    r.dl = make_float2(dl, dl);
-    r.vbh = make_float2(vbh, vbh);
-    r.vbl = make_float2(vbl, vbl);
-    r.S1f = f2(S1f);
-    r.C1 = f2(S1f * A1);
-    r.C0 = f2(S1f * B1);
-    r.D2 = f2(A2 + Y);
-    r.D1 = f2(B2 + A2 * Y);
-    r.D0 = f2(B2 * Y);
-    r.Sc = lp.Sc;
-    r.y = (float)lp.vy;
-    r.ey = (float)lp.ey;
-    r.sig1 = lp.sig1;
-    if (nonempty && li[3] > li[2]) {
-      // region C inside this tile: denominators of the Algorithm-916 series
-      const float a2 = HK_A916_F * HK_A916_F;
-      const float Yf = (float)Y;
-#pragma unroll 2
-      for (int m = 1; m <= HK_C916_MR; ++m) Rtab[m - 1] = rcp_fast(fmaf(a2 * m, (float)m, Yf));
-    }
-    r.i0 = nonempty ? li[0] : 0;
-    r.b0 = li[1];
-    r.c0 = li[2];
-    r.c1 = li[3];
-    r.b1 = li[4];
-    r.i1 = nonempty ? li[5] : 0;
-    r.flags = flags;
-    *reinterpret_cast<RecF *>(recp) = r;
-  } else {
-    RecD r;
-    r.nu = lp.nu;
-    r.iad = lp.iad;
-    r.y = lp.vy;
-    r.y2 = lp.vy * lp.vy;
-    r.S1 = lp.S1;
-    r.Sc = lp.Sc;
-    r.ey = lp.ey;
-    r.pad = 0.0;
-    r.i0 = nonempty ? li[0] : 0;
-    r.b0 = li[1];
-    r.c0 = li[2];
-    r.c1 = li[3];
-    r.b1 = li[4];
-    r.i1 = nonempty ? li[5] : 0;
-    r.p0 = r.p1 = 0;
-    *reinterpret_cast<RecD *>(recp) = r;
-  }
+  RecD r;
+  r.nu = lp.nu;
+  r.iad = lp.iad;
+  r.y = lp.vy;
+  r.y2 = lp.vy * lp.vy;
+  r.S1 = lp.S1;
+  r.Sc = lp.Sc;
+  r.ey = lp.ey;
+  r.pad = 0.0;
+  r.i0 = nonempty ? li[0] : 0;
+  r.b0 = li[1];
+  r.c0 = li[2];
+  r.c1 = li[3];
+  r.b1 = li[4];
+  r.i1 = nonempty ? li[5] : 0;
+  r.p0 = r.p1 = 0;
+  *recp = r;
 }
 
 // ------------------------------------------------------------ FP32 sweep
 // Each warp classifies the staged lines against its 256-point slice, 32
-// lines per instruction (one lane per line), and sweeps them by class:
-//   HK_CLS_B  slice inside the cut window and inside one region-B part,
-//   HK_CLS_A  slice inside the cut window and inside one region-A part,
-//   HK_CLS_G  anything else that intersects the slice (window edges,
-//             region boundaries, region C),
-//   HK_CLS_W  a HK_F_WEAK line that intersects the slice,
-// so the specialised loops carry no per-pair tests and non-intersecting
-// lines cost nothing.  Region-C points are evaluated in a rolled loop and
-// summed in FP64 into the per-point shared sums cacc (each point has one
-// owning lane: deterministic).
-enum { HK_CLS_SKIP = 0, HK_CLS_B = 1, HK_CLS_A = 2, HK_CLS_G = 3, HK_CLS_W = 4 };
+// lines per instruction (one lane per line).  With [lo, hi) the line's cut
+// window inside the slice:
+//   HK_CLS_B   [lo, hi) is the whole slice, inside one region-B part;
+//   HK_CLS_A   [lo, hi) is the whole slice, inside region A;
+//   HK_CLS_BM  [lo, hi) lies in region B or C (window edge in the slice, or
+//              region C in it);
+//   HK_CLS_AM  [lo, hi) lies in region A (window edge in the slice);
+//   HK_CLS_G   [lo, hi) holds an A/B region boundary;
+//   HK_CLS_W   an HK_F_WEAK line (FP64 sums);
+// non-intersecting lines cost nothing.  B and A run the packed f32x2 loop
+// with no tests; BM and AM run it per 64-point block of pairs, skipping
+// blocks without points of their region and masking only the blocks a
+// boundary cuts; G tests every point.  Region-C points go to sweep_C and
+// are summed in FP64 into the per-point shared sums cacc.
+enum { HK_CLS_SKIP = 0, HK_CLS_B, HK_CLS_A, HK_CLS_BM, HK_CLS_AM, HK_CLS_G, HK_CLS_W };
 
 __device__ __forceinline__ int classify(const RecF &r, int wb) {
   const int we = wb + HK_SLICE;
-  if (r.i1 <= wb || r.i0 >= we) return HK_CLS_SKIP;
+  const int lo = max(r.i0, wb), hi = min(r.i1, we);
+  if (hi <= lo) return HK_CLS_SKIP;
   if (r.flags & HK_F_WEAK) return HK_CLS_W;
-  const bool full = r.i0 <= wb && r.i1 >= we;
-  if (full && ((r.b0 <= wb && r.c0 >= we) || (r.c1 <= wb && r.b1 >= we))) return HK_CLS_B;
-  if (full && (r.b0 >= we || r.b1 <= wb)) return HK_CLS_A;
+  const bool full = lo == wb && hi == we;
+  const bool noC = r.c0 >= r.c1 || r.c1 <= lo || r.c0 >= hi;
+  if (r.b0 <= lo && r.b1 >= hi) return (full && noC) ? HK_CLS_B : HK_CLS_BM;
+  if (r.b0 >= r.b1 || r.b1 <= lo || r.b0 >= hi) return full ? HK_CLS_A : HK_CLS_AM;
   return HK_CLS_G;
 }
 
@@ -261,106 +269,202 @@ __device__ __forceinline__ float2 rcp_pair(float2 d) {
   return __fmul2_rn(make_float2(d.y, d.x), make_float2(R, R));
 }
 
-// region B only, two points per packed instruction; the record's first 80
-// bytes are read as five 16-byte words
-__device__ __forceinline__ void sweep_B(const RecF &rr, const float2 (&kf)[HK_PPL / 2],
-                                        float2 (&a32)[HK_PPL / 2]) {
-  const float4 *w = reinterpret_cast<const float4 *>(&rr);
-  const float4 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3], w4 = w[4];
-  const float2 dh = make_float2(w0.x, w0.y), dl = make_float2(w0.z, w0.w);
-  const float2 vbh = make_float2(w1.x, w1.y), vbl = make_float2(w1.z, w1.w);
-  const float2 S1f = make_float2(w2.x, w2.y), C1 = make_float2(w2.z, w2.w);
-  const float2 C0 = make_float2(w3.x, w3.y), D2 = make_float2(w3.z, w3.w);
-  const float2 D1 = make_float2(w4.x, w4.y), D0 = make_float2(w4.z, w4.w);
-#pragma unroll
-  for (int q = 0; q < HK_PPL / 2; ++q) {
-    const float2 x = __fadd2_rn(__ffma2_rn(kf[q], vbh, dh), __ffma2_rn(kf[q], vbl, dl));
-    const float2 s = __fmul2_rn(x, x);
-    const float2 num = __ffma2_rn(s, __ffma2_rn(S1f, s, C1), C0);
-    const float2 den = __ffma2_rn(__ffma2_rn(__fadd2_rn(s, D2), s, D1), s, D0);
-    a32[q] = __ffma2_rn(num, rcp_pair(den), a32[q]);
-  }
-}
+// the FP32 constants of regions A and B, read as three 16-byte words and
+// duplicated into the pair operands of the packed f32x2 instructions
+struct CoefB {
+  float2 S1f, C1, C0, D2, D1, D0, nkc, vb, fr;
+};
 
-// region A only
-__device__ __forceinline__ void sweep_A(const RecF &rr, const float2 (&kf)[HK_PPL / 2],
-                                        float2 (&a32)[HK_PPL / 2]) {
+__device__ __forceinline__ float2 dup(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ CoefB load_coef(const RecF &rr) {
   const float4 *w = reinterpret_cast<const float4 *>(&rr);
   const float4 w0 = w[0], w1 = w[1];
-  const float2 S1f = rr.S1f;
-  const float Yf = rr.y * rr.y;
-  const float2 Y = make_float2(Yf, Yf);
-  const float2 dh = make_float2(w0.x, w0.y), dl = make_float2(w0.z, w0.w);
-  const float2 vbh = make_float2(w1.x, w1.y), vbl = make_float2(w1.z, w1.w);
-  if (!(rr.flags & HK_F_WIDE)) {
+  CoefB c;
+  c.S1f = dup(w0.x);
+  c.C1 = dup(w0.y);
+  c.C0 = dup(w0.z);
+  c.D2 = dup(w0.w);
+  c.D1 = dup(w1.x);
+  c.D0 = dup(w1.y);
+  c.nkc = dup(w1.z);
+  c.vb = dup(w1.w);
+  c.fr = dup(rr.fr);
+  return c;
+}
+
+__device__ __forceinline__ float2 x_pair(const CoefB &c, float2 kf) {
+  return __ffma2_rn(__fadd2_rn(kf, c.nkc), c.vb, c.fr);
+}
+
+// S1f t4 at two points as (numerator, 1/denominator); the reciprocals run
+// on the MUFU pipe, beside the FMA pipe that bounds this loop
+__device__ __forceinline__ void gh2_pair(const CoefB &c, float2 s, float2 &num, float2 &inv) {
+  num = __ffma2_rn(s, __ffma2_rn(c.S1f, s, c.C1), c.C0);
+  const float2 den = __ffma2_rn(__ffma2_rn(__fadd2_rn(s, c.D2), s, c.D1), s, c.D0);
+  inv = make_float2(rcp_fast(den.x), rcp_fast(den.y));
+}
+
+// the pair mask of a cut block: point in [lo, hi) and outside [c0, c1)
+__device__ __forceinline__ bool in_run(int k, int lo, int hi, int c0, int c1) {
+  return k >= lo && k < hi && !(k >= c0 && k < c1);
+}
+
+// region B only, whole slice
+__device__ __forceinline__ void sweep_B(const RecF &rr, const float2 (&kf)[HK_PPL / 2],
+                                        float2 (&a32)[HK_PPL / 2]) {
+  const CoefB c = load_coef(rr);
 #pragma unroll
-    for (int q = 0; q < HK_PPL / 2; ++q) {
-      const float2 x = __fadd2_rn(__ffma2_rn(kf[q], vbh, dh), __ffma2_rn(kf[q], vbl, dl));
-      a32[q] = __ffma2_rn(S1f, rcp_pair(__ffma2_rn(x, x, Y)), a32[q]);
-    }
-  } else {
-#pragma unroll
-    for (int q = 0; q < HK_PPL / 2; ++q) {
-      const float2 x = __fadd2_rn(__ffma2_rn(kf[q], vbh, dh), __ffma2_rn(kf[q], vbl, dl));
-      const float2 u = __ffma2_rn(x, x, Y);
-      a32[q] = __ffma2_rn(S1f, make_float2(rcp_fast(u.x), rcp_fast(u.y)), a32[q]);
-    }
+  for (int q = 0; q < HK_PPL / 2; ++q) {
+    const float2 x = x_pair(c, kf[q]);
+    float2 num, inv;
+    gh2_pair(c, __fmul2_rn(x, x), num, inv);
+    a32[q] = __ffma2_rn(num, inv, a32[q]);
   }
 }
 
-// everything else: per-point window/region tests, region C deferred.
-// WEAK lines (S1f = 1) add S1 t in FP64 to cacc; the others add S1f t to
-// the FP32 sums.
-template <bool WEAK>
-__device__ __forceinline__ void sweep_G(const RecF &r, const float *__restrict__ Rj,
-                                        double *__restrict__ cacc, int wb, int lane,
+// region B points of [lo, hi) minus region C, by 64-point blocks
+__device__ __forceinline__ void sweep_BM(const RecF &rr, int wb, int lane,
+                                         const float2 (&kf)[HK_PPL / 2],
+                                         float2 (&a32)[HK_PPL / 2]) {
+  const CoefB c = load_coef(rr);
+  const int lo = max(rr.i0, wb), hi = min(rr.i1, wb + HK_SLICE);
+  const int c0 = rr.c0, c1 = rr.c1;
+#pragma unroll
+  for (int q = 0; q < HK_PPL / 2; ++q) {
+    const int blo = wb + 64 * q, bhi = blo + 64;
+    const int l2 = max(lo, blo), h2 = min(hi, bhi);
+    if (l2 >= h2 || (c0 <= l2 && c1 >= h2)) continue;  // no region-B point
+    const float2 x = x_pair(c, kf[q]);
+    float2 s = __fmul2_rn(x, x);
+    float2 num, inv;
+    if (l2 == blo && h2 == bhi && (c1 <= blo || c0 >= bhi)) {
+      gh2_pair(c, s, num, inv);
+    } else {
+      // masked points take s = 1000 (a finite region-B value) and add 0
+      const bool m0 = in_run(blo + lane, lo, hi, c0, c1);
+      const bool m1 = in_run(blo + lane + 32, lo, hi, c0, c1);
+      s.x = m0 ? s.x : 1000.f;
+      s.y = m1 ? s.y : 1000.f;
+      gh2_pair(c, s, num, inv);
+      num.x = m0 ? num.x : 0.f;
+      num.y = m1 ? num.y : 0.f;
+    }
+    a32[q] = __ffma2_rn(num, inv, a32[q]);
+  }
+}
+
+// region A, whole slice (AM = false) or the points of [lo, hi) (AM = true)
+template <bool AM>
+__device__ __forceinline__ void sweep_A(const RecF &rr, int wb, int lane,
                                         const float2 (&kf)[HK_PPL / 2],
                                         float2 (&a32)[HK_PPL / 2]) {
+  const CoefB c = load_coef(rr);
+  const float Yf = rr.y * rr.y;
+  const float2 Y = make_float2(Yf, Yf);
+  const bool wide = rr.flags & HK_F_WIDE;
+  const int lo = max(rr.i0, wb), hi = min(rr.i1, wb + HK_SLICE);
+#pragma unroll
+  for (int q = 0; q < HK_PPL / 2; ++q) {
+    const int blo = wb + 64 * q, bhi = blo + 64;
+    bool m0 = true, m1 = true;
+    if (AM) {
+      if (max(lo, blo) >= min(hi, bhi)) continue;
+      m0 = blo + lane >= lo && blo + lane < hi;
+      m1 = blo + lane + 32 >= lo && blo + lane + 32 < hi;
+    }
+    const float2 x = x_pair(c, kf[q]);
+    float2 u = __ffma2_rn(x, x, Y);
+    if (AM) {
+      // masked points take u = 1e6 (finite, pairable) and add 0
+      u.x = m0 ? u.x : 1e6f;
+      u.y = m1 ? u.y : 1e6f;
+    }
+    float2 inv = wide ? make_float2(rcp_fast(u.x), rcp_fast(u.y)) : rcp_pair(u);
+    if (AM) {
+      inv.x = m0 ? inv.x : 0.f;
+      inv.y = m1 ? inv.y : 0.f;
+    }
+    a32[q] = __ffma2_rn(c.S1f, inv, a32[q]);
+  }
+}
+
+// Region C points of the slice, summed in FP64 into cacc, lanes packed by
+// evaluator so a warp never runs both: [t0, t1) holds |x| < sqrt(36 - y^2)
+// (Algorithm 916), the rest of [lo, hi) has r >= 6 (asymptotic series).  The
+// split comes from the FP64 offsets; a point within rounding of r = 6 may
+// take either evaluator (both hold there).  Points leave their owning lane
+// here, so the warp syncs before cacc is touched again.
+__device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__ Rj,
+                                        double *__restrict__ cacc, int wb, int lane) {
+  const int lo = max(r.c0, wb), hi = min(r.c1, wb + HK_SLICE);
+  if (lo >= hi) return;
+  const float dh = r.dh, dl = r.dl, vbh = r.vbh, vbl = r.vbl;
+  const float y = r.y, ey = r.ey, sig1 = r.sig1;
+  const double Sc = r.Sc;
+  int t0 = hi, t1 = hi;
+  if (y < 6.0f) {
+    const double xt = sqrt(36.0 - (double)y * (double)y);
+    const double D0 = (double)dh + (double)dl, vb = (double)vbh + (double)vbl;
+    const double k0 = floor((-xt - D0) / vb) + 1.0, k1 = floor((xt - D0) / vb) + 1.0;
+    t0 = (int)fmin(fmax(k0, (double)lo), (double)hi);
+    t1 = (int)fmin(fmax(k1, (double)t0), (double)hi);
+  }
+  __syncwarp();
+  for (int k = t0 + lane; k < t1; k += 32) {
+    const float kk = (float)k;
+    const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
+    cacc[k] = fma(Sc, (double)voigt916_core(x, y, ey, sig1, Rj), cacc[k]);
+  }
+  const int n1 = t0 - lo, ns = n1 + (hi - t1);
+  for (int i = lane; i < ns; i += 32) {
+    const int k = i < n1 ? lo + i : t1 + (i - n1);
+    const float kk = (float)k;
+    const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
+    cacc[k] = fma(Sc, (double)voigt_asy(x, y), cacc[k]);
+  }
+  __syncwarp();
+}
+
+// A/B boundaries in the slice, and weak lines: per-point window/region
+// tests.  WEAK lines (S1f = 1) add S1 t in FP64 to cacc; the others add
+// S1f t to the FP32 sums.
+template <bool WEAK>
+__device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
+                                        const float2 (&kf)[HK_PPL / 2],
+                                        float2 (&a32)[HK_PPL / 2],
+                                        double *__restrict__ cacc) {
   // the record lives in shared memory like cacc: read it once into registers
   const int i0 = r.i0, i1 = r.i1, b0 = r.b0, b1 = r.b1, c0 = r.c0, c1 = r.c1;
-  const float dh = r.dh.x, dl = r.dl.x, vbh = r.vbh.x, vbl = r.vbl.x;
+  const float nkc = r.nkc, vb = r.vb, fr = r.fr;
   const float y = r.y;
   const float Yf = y * y;
-  const double Sc = r.Sc;
   const int we = wb + HK_SLICE;
-  if (i0 < we && i1 > wb && !(c0 <= max(i0, wb) && c1 >= min(i1, we))) {
-    const float S1f = r.S1f.x, C1 = r.C1.x, C0 = r.C0.x;
-    const float D2 = r.D2.x, D1 = r.D1.x, D0 = r.D0.x;
-    const double S1w = WEAK ? Sc * (double)y * 0.56418958354775628 : 0.0;  // S y / pi
+  if (c0 <= max(i0, wb) && c1 >= min(i1, we)) return;  // region C only
+  const float S1f = r.S1f, C1 = r.C1, C0 = r.C0;
+  const float D2 = r.D2, D1 = r.D1, D0 = r.D0;
+  const double S1w = WEAK ? r.Sc * (double)y * 0.56418958354775628 : 0.0;  // S y / pi
 #pragma unroll
-    for (int p = 0; p < HK_PPL; ++p) {
-      const int k = wb + lane + 32 * p;
-      if (k >= i0 && k < i1 && !(k >= c0 && k < c1)) {
-        const float kk = (p & 1) ? kf[p >> 1].y : kf[p >> 1].x;
-        const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
-        const float s = x * x;
-        float t;
-        if (k >= b0 && k < b1) {
-          const float num = fmaf(s, fmaf(S1f, s, C1), C0);
-          const float den = fmaf(fmaf(s + D2, s, D1), s, D0);
-          t = num * rcp_fast(den);
-        } else {
-          t = S1f * rcp_fast(s + Yf);
-        }
-        if (WEAK) {
-          cacc[k] = fma(S1w, (double)t, cacc[k]);
-        } else if (p & 1) {
-          a32[p >> 1].y += t;
-        } else {
-          a32[p >> 1].x += t;
-        }
+  for (int p = 0; p < HK_PPL; ++p) {
+    const int k = wb + lane + 32 * p;
+    if (k >= i0 && k < i1 && !(k >= c0 && k < c1)) {
+      const float kk = (p & 1) ? kf[p >> 1].y : kf[p >> 1].x;
+      const float x = fmaf(kk + nkc, vb, fr);
+      const float s = x * x;
+      float t;
+      if (k >= b0 && k < b1) {
+        const float num = fmaf(s, fmaf(S1f, s, C1), C0);
+        const float den = fmaf(fmaf(s + D2, s, D1), s, D0);
+        t = num * rcp_fast(den);
+      } else {
+        t = S1f * rcp_fast(s + Yf);
       }
-    }
-  }
-  const int lo = max(c0, wb), hi = min(c1, we);
-  if (lo < hi) {
-    const float ey = r.ey, sig1 = r.sig1;
-    for (int pp = (lo - wb) >> 5; pp <= (hi - 1 - wb) >> 5; ++pp) {
-      const int k = wb + lane + 32 * pp;
-      if (k >= lo && k < hi) {
-        const float kk = (float)k;
-        const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
-        cacc[k] = fma(Sc, (double)voigt916_tab(x, y, ey, sig1, Rj), cacc[k]);
+      if (WEAK) {
+        cacc[k] = fma(S1w, (double)t, cacc[k]);
+      } else if (p & 1) {
+        a32[p >> 1].y += t;
+      } else {
+        a32[p >> 1].x += t;
       }
     }
   }
@@ -404,8 +508,8 @@ __device__ __forceinline__ void sweep_plain(const RecD &r, int wb, int lane,
 // add the FP32 sums of level lev into the FP64 sums (exact unscale) and
 // clear them
 __device__ __forceinline__ void flush_sums(float2 (&a32)[HK_PPL / 2], double *__restrict__ cacc,
-                                           int wb, int lane, double s1unscale, int lev) {
-  const double u = s1unscale * pow2_d(-HK_LEVEL_BITS * lev);
+                                           int wb, int lane, int s1exp, int lev) {
+  const double u = ldexp(1.0, -(s1exp + HK_LEVEL_BITS * lev));
 #pragma unroll
   for (int p = 0; p < HK_PPL; ++p) {
     const int k = wb + lane + 32 * p;
@@ -420,7 +524,7 @@ __device__ __forceinline__ void flush_sums(float2 (&a32)[HK_PPL / 2], double *__
 // mixed form: 4 CTAs (32 warps) per SM, 64 registers
 template <bool MIXED>
 __global__ void __launch_bounds__(HK_THREADS, MIXED ? 4 : 2)
-voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ nu0,
+voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
                  int64_t nlines, GridDev g, const StateDev *__restrict__ states,
                  int tiles_per_state, int nsplit, int total_tickets,
                  unsigned *__restrict__ ticket, double *__restrict__ partial,
@@ -432,6 +536,7 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
   double *cacc = reinterpret_cast<double *>(smem_dyn + sizeof(Rec) * HK_CH +
                                             sizeof(float) * (HK_RPAD + HK_CH * HK_C916_MR));
   __shared__ int s_ticket, s_last;
+  __shared__ int s_kcnt[HK_CH / 32][HK_NKEY];  // staged lines per (staging warp, key)
   __shared__ long long s_L0, s_L1;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -449,7 +554,8 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
     const int s = tt / tiles_per_state;
     const int tile = tt - s * tiles_per_state;
     const StateDev &st = states[s];
-    const LinePrep *P = prep + (int64_t)s * nlines;
+    const LinePrep *P = reinterpret_cast<const LinePrep *>(prep) + (int64_t)s * nlines;
+    const LinePrepF *PF = reinterpret_cast<const LinePrepF *>(prep) + (int64_t)s * nlines;
     const int64_t g0 = (int64_t)tile * HK_G;
     const int64_t g1 = min(g0 + (int64_t)HK_G, g.nx);
     if (warp == 0) {
@@ -499,9 +605,39 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
     int lcur = 0;  // strength level held in a32 (warp-uniform)
     for (int64_t c = c_begin; c < c_end; ++c) {
       const int cnt = (int)((nL - c + nch - 1) / nch);
-      if (tid < cnt)
-        stage_line<MIXED>(P, g, L0 + c + (int64_t)tid * nch, g0, g1, st.s1scale, &rec[tid],
-                          Rtab + tid * HK_C916_MR);
+      if (MIXED) {
+        // build the records, then place them sorted by key (stable counting
+        // sort over the HK_CH / 32 staging warps), so a warp's 32-line
+        // groups mostly hold one strength level
+        // (the key pass keeps no record: the record is rebuilt after the
+        // scan rather than held in registers across the barrier)
+        int key = HK_NKEY, rank = 0;
+        const int64_t l = L0 + c + (int64_t)tid * nch;
+        if (tid < cnt) key = line_key(PF, l, g0, g1, st.s1exp);
+        if (tid < HK_CH) {
+          const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+          for (int v = 0; v < HK_NKEY; ++v) {
+            const unsigned m = __ballot_sync(0xffffffffu, key == v);
+            if (key == v) rank = __popc(m & lt);
+            if (lane == 0) s_kcnt[warp][v] = __popc(m);
+          }
+        }
+        __syncthreads();
+        if (tid < cnt) {
+          int pos = rank;
+          for (int v = 0; v < key; ++v)
+#pragma unroll
+            for (int w = 0; w < HK_CH / 32; ++w) pos += s_kcnt[w][v];
+          for (int w = 0; w < warp; ++w) pos += s_kcnt[w][key];
+          RecF r;
+          stage_mixed(PF, g, l, g0, g1, st.s1exp, key, r);
+          reinterpret_cast<RecF *>(rec)[pos] = r;
+          if (r.c1 > r.c0 && r.i1 > r.i0) stage_rtab(r.y, Rtab + pos * HK_C916_MR);
+        }
+      } else if (tid < cnt) {
+        stage_plain(P, L0 + c + (int64_t)tid * nch, g0, g1, reinterpret_cast<RecD *>(rec) + tid);
+      }
       __syncthreads();
       if (MIXED) {
         const RecF *rf = reinterpret_cast<const RecF *>(rec);
@@ -511,20 +647,22 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
           const int lev = (j < cnt) ? (rf[j].flags >> 8) : 0;
           const unsigned bB = __ballot_sync(0xffffffffu, cls == HK_CLS_B);
           const unsigned bA = __ballot_sync(0xffffffffu, cls == HK_CLS_A);
+          const unsigned bBM = __ballot_sync(0xffffffffu, cls == HK_CLS_BM);
+          const unsigned bAM = __ballot_sync(0xffffffffu, cls == HK_CLS_AM);
           const unsigned bG = __ballot_sync(0xffffffffu, cls == HK_CLS_G);
           unsigned mW = __ballot_sync(0xffffffffu, cls == HK_CLS_W);
-          unsigned live = bB | bA | bG;
+          unsigned live = bB | bA | bBM | bAM | bG;
           while (live) {
             // the lines of the current level first; switch level (flushing
             // the FP32 sums) only when none of them is left
             unsigned m = __ballot_sync(0xffffffffu, lev == lcur) & live;
             if (m == 0u) {
-              flush_sums(a32, cacc, wb, lane, st.s1unscale, lcur);
+              flush_sums(a32, cacc, wb, lane, st.s1exp, lcur);
               lcur = __shfl_sync(0xffffffffu, lev, __ffs(live) - 1);
               m = __ballot_sync(0xffffffffu, lev == lcur) & live;
             }
             live &= ~m;
-            unsigned mB = m & bB, mA = m & bA, mG = m & bG;
+            unsigned mB = m & bB, mA = m & bA, mBM = m & bBM, mAM = m & bAM, mG = m & bG;
             while (mB) {
               const int b = __ffs(mB) - 1;
               mB &= mB - 1;
@@ -533,22 +671,35 @@ voigt_sum_kernel(const LinePrep *__restrict__ prep, const double *__restrict__ n
             while (mA) {
               const int b = __ffs(mA) - 1;
               mA &= mA - 1;
-              sweep_A(rf[g32 + b], kf, a32);
+              sweep_A<false>(rf[g32 + b], wb, lane, kf, a32);
+            }
+            while (mBM) {
+              const int b = __ffs(mBM) - 1;
+              mBM &= mBM - 1;
+              sweep_BM(rf[g32 + b], wb, lane, kf, a32);
+              sweep_C(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
+            }
+            while (mAM) {
+              const int b = __ffs(mAM) - 1;
+              mAM &= mAM - 1;
+              sweep_A<true>(rf[g32 + b], wb, lane, kf, a32);
             }
             while (mG) {
               const int b = __ffs(mG) - 1;
               mG &= mG - 1;
-              sweep_G<false>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, kf, a32);
+              sweep_G<false>(rf[g32 + b], wb, lane, kf, a32, cacc);
+              sweep_C(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
             }
           }
           while (mW) {
             const int b = __ffs(mW) - 1;
             mW &= mW - 1;
-            sweep_G<true>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, kf, a32);
+            sweep_G<true>(rf[g32 + b], wb, lane, kf, a32, cacc);
+            sweep_C(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
           }
         }
         // at most one chunk of lines per FP32 sum
-        flush_sums(a32, cacc, wb, lane, st.s1unscale, lcur);
+        flush_sums(a32, cacc, wb, lane, st.s1exp, lcur);
       } else {
         for (int j = 0; j < cnt; ++j)
           sweep_plain(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc);
@@ -705,7 +856,7 @@ VoigtPlan plan_voigt_sum(bool mixed, int64_t nx, int nstates, int grid_ctas) {
   return pl;
 }
 
-cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const LinePrep *prep_d,
+cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d,
                              const double *nu0_d, int64_t nlines, const GridDev &g,
                              const StateDev *states_d, unsigned *ticket_d, double *partial_d,
                              unsigned *tile_cnt_d, double *K_d, int64_t k_stride,
