@@ -357,8 +357,30 @@ __device__ __forceinline__ float voigt_asy(float x, float y) {
   return v;
 }
 
-// Algorithm 916 with the per-line table R, valid for |x| < 6.3 (m_c <= 10)
-__device__ __forceinline__ float voigt916_core(float x, float y, float ey, float sig1,
+// sin(z)^2 for 0 <= z <= 64: z = n pi + r with |r| <= pi/2 (Cody-Waite
+// reduction, pi split into its nearest float and the remainder), then
+// sin(r) from its Taylor series to r^13 (remainder < (pi/2)^15/15! = 9e-10).
+// Near a zero of sin the reduced r keeps its own relative accuracy.
+__device__ __forceinline__ float sin_sq(float z) {
+  const float n = rintf(z * 0.318309886183790672f);   // 1/pi
+  float r = fmaf(-n, 3.14159274101257324f, z);          // float(pi)
+  r = fmaf(-n, -8.74227766e-8f, r);                     // pi - float(pi)
+  const float r2 = r * r;
+  float p = 1.60590438368216146e-10f;                   // 1/13!
+  p = fmaf(p, r2, -2.50521083854417188e-8f);            // -1/11!
+  p = fmaf(p, r2, 2.75573192239858907e-6f);             // 1/9!
+  p = fmaf(p, r2, -1.98412698412698413e-4f);            // -1/7!
+  p = fmaf(p, r2, 8.33333333333333333e-3f);             // 1/5!
+  p = fmaf(p, r2, -0.166666666666666667f);              // -1/3!
+  const float sr = fmaf(p * r2, r, r);
+  return sr * sr;
+}
+
+// Algorithm 916 with the per-line table R, valid for |x| < 6.3 (m_c <= 10);
+// iy = 1/y.  The s2 series stops at the first term below e^-25 of the
+// largest (a m + x >= 5.1), so its length falls from 8 at x = 0 to none at
+// x >= 4.5.
+__device__ __forceinline__ float voigt916_core(float x, float y, float iy, float ey, float sig1,
                                                const float *__restrict__ R) {
   const float a = HK_A916_F;
   const float a2 = a * a;
@@ -392,32 +414,31 @@ __device__ __forceinline__ float voigt916_core(float x, float y, float ey, float
     if (mc - k >= 1) s3 = fmaf(T, Rc[-k], s3);
   }
   float s2 = 0.f;
-  if (x < 4.8f) {
-    float T2 = expf(-(a + x) * (a + x));
+  const int n2 = min(HK_C916_K, __float2int_ru((5.1f - x) * (1.0f / a)));
+  if (n2 > 0) {
+    // exp(-(a + x)^2) = exp(-x^2) exp(-a^2 - 2 a x)
+    float T2 = ex2 * ex2_fast(-L2E * fmaf(2.0f * a, x, a2));
     float q2 = ex2_fast(L2E * fmaf(-3.0f, a2, -2.0f * a * x));
-#pragma unroll
-    for (int k = 0; k < HK_C916_K; ++k) {
+    for (int k = 0; k < n2; ++k) {
       s2 = fmaf(T2, R[k], s2);
       T2 *= q2;
       q2 *= G;
     }
   }
   const float s1 = ex2 * sig1;
-  const float xy = x * y;
-  float sinxy, cosxy;
-  sincosf(xy, &sinxy, &cosxy);
-  const float cos2xy = fmaf(-2.0f * sinxy, sinxy, 1.0f);
-  const float t2 = sinxy * ex2 * sinxy / y;
+  const float sin2 = sin_sq(x * y);
+  const float cos2xy = fmaf(-2.0f, sin2, 1.0f);
+  const float t2 = sin2 * ex2 * iy;
   const float t3 = y * (-cos2xy * s1 + 0.5f * (s2 + s3));
   return fmaf(ex2 * ey, cos2xy, HK_C916_F * (t2 + t3));
 }
 
 // region C in FP32: the asymptotic series for r >= 6, Algorithm 916 below
-__device__ __forceinline__ float voigt916_tab(float x, float y, float ey, float sig1,
+__device__ __forceinline__ float voigt916_tab(float x, float y, float iy, float ey, float sig1,
                                               const float *__restrict__ R) {
   x = fabsf(x);
   if (fmaf(x, x, y * y) >= HK_ASY_R2) return voigt_asy(x, y);
-  return voigt916_core(x, y, ey, sig1, R);
+  return voigt916_core(x, y, iy, ey, sig1, R);
 }
 
 }  // namespace hkb

@@ -60,7 +60,8 @@ struct __align__(16) RecF {
   float dh, dl, vbh, vbl;  // region C: x at the tile start, step (hi, lo)
   double Sc;               // S/sqrt(pi) (region C, FP64 sum)
   int i0, b0, c0, c1;      // tile-local window boundaries
-  int b1, i1, flags, pad;
+  int b1, i1, flags;
+  float iy;                // 1/y (region C)
 };
 static_assert(sizeof(RecF) == 112, "RecF layout");
 
@@ -195,7 +196,7 @@ __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, con
   r.b1 = clip_local(lp.b1, g0, g1);
   r.i1 = nonempty ? clip_local(lp.i1, g0, g1) : 0;
   r.flags = ((lp.flags & HK_PF_WIDE) ? HK_F_WIDE : 0) | (weak ? HK_F_WEAK : 0) | (lev << 8);
-  r.pad = 0;
+  r.iy = lp.y > 0.f ? (float)(1.0 / (double)lp.y) : 0.f;
 }
 
 // region C inside the tile: denominators of the Algorithm-916 series
@@ -400,7 +401,7 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
   const int lo = max(r.c0, wb), hi = min(r.c1, wb + HK_SLICE);
   if (lo >= hi) return;
   const float dh = r.dh, dl = r.dl, vbh = r.vbh, vbl = r.vbl;
-  const float y = r.y, ey = r.ey, sig1 = r.sig1;
+  const float y = r.y, iy = r.iy, ey = r.ey, sig1 = r.sig1;
   const double Sc = r.Sc;
   int t0 = hi, t1 = hi;
   if (y < 6.0f) {
@@ -414,7 +415,7 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
   for (int k = t0 + lane; k < t1; k += 32) {
     const float kk = (float)k;
     const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
-    cacc[k] = fma(Sc, (double)voigt916_core(x, y, ey, sig1, Rj), cacc[k]);
+    cacc[k] = fma(Sc, (double)voigt916_core(x, y, iy, ey, sig1, Rj), cacc[k]);
   }
   const int n1 = t0 - lo, ns = n1 + (hi - t1);
   for (int i = lane; i < ns; i += 32) {
@@ -761,7 +762,9 @@ __global__ void profile_eval_kernel(int64_t n, const double *__restrict__ x,
     const float a2 = HK_A916_F * HK_A916_F;
     for (int m = 0; m < HK_RPAD; ++m) R[m] = 0.f;
     for (int m = 1; m <= HK_C916_MR; ++m) R[HK_RPAD + m - 1] = rcp_fast(fmaf(a2 * m, (float)m, Y));
-    out[i] = (double)voigt916_tab((float)x[i], (float)y[i], (float)ey, (float)c916_sig1(y[i]),
+    const float yf = (float)y[i];
+    const float iy = yf > 0.f ? (float)(1.0 / (double)yf) : 0.f;
+    out[i] = (double)voigt916_tab((float)x[i], yf, iy, (float)ey, (float)c916_sig1(y[i]),
                                   R + HK_RPAD);
   } else {
     out[i] = voigt916_d(x[i], y[i], ey);
