@@ -124,6 +124,19 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
         if (fmax(100.0, Y) < 0x1p-64 * umax || Y > 0x1p60) flags |= HK_PF_RANGE;
       }
       r.flags = flags;
+      // region C's Algorithm-916 part: |x| < sqrt(36 - y^2), from the FP64
+      // offsets (a point within rounding of r = 6 may fall on either side;
+      // both evaluators hold there)
+      int64_t t0 = w[3], t1 = w[3];
+      if (w[3] > w[2] && Y < 36.0) {
+        const double xt = sqrt(36.0 - Y);
+        const double x0 = (g.numin - ls.nu) * ls.iad, vb = g.dnu * ls.iad;
+        const double k0 = floor((-xt - x0) / vb) + 1.0, k1 = floor((xt - x0) / vb) + 1.0;
+        t0 = (int64_t)fmin(fmax(k0, (double)w[2]), (double)w[3]);
+        t1 = (int64_t)fmin(fmax(k1, (double)t0), (double)w[3]);
+      }
+      r.t0 = (int)t0;
+      r.t1 = (int)t1;
       r.i0 = (int)w[0];
       r.b0 = (int)w[1];
       r.c0 = (int)w[2];

@@ -63,7 +63,7 @@ struct __align__(16) LinePrep {
   int pad;
 };
 
-// The same line and state for the mixed form (96 bytes): everything that
+// The same line and state for the mixed form (112 bytes): everything that
 // depends on the line and the state only, so staging a line into a tile adds
 // just the tile's offsets and the strength level.
 //   A1 = 2Y + 2.5 - 4/pi, B1 = (Y+1.5)(Y+1)      (GH2 numerator, Y = vy^2)
@@ -74,6 +74,8 @@ struct __align__(16) LinePrep {
 //          HK_PF_RANGE -- the window's terms span more than 2^64, or Y > 2^60:
 //                         FP32 sums cannot hold the line (FP64 instead).
 constexpr int HK_PF_WIDE = 2, HK_PF_RANGE = 1;
+//   [t0, t1): the part of region C with |x| < sqrt(36 - y^2) (Algorithm 916
+//   in FP32; the rest of region C takes the asymptotic series)
 struct __align__(16) LinePrepF {
   double nu, iad;
   double S1, Sc;
@@ -82,8 +84,9 @@ struct __align__(16) LinePrepF {
   float D2, D1, D0;
   int ex, flags;
   int i0, b0, c0, c1, b1, i1;
+  int t0, t1;
 };
-static_assert(sizeof(LinePrepF) == 96, "LinePrepF layout");
+static_assert(sizeof(LinePrepF) == 112, "LinePrepF layout");
 
 // Per-(T, P) constants formed on the host.
 struct StateDev {

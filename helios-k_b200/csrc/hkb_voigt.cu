@@ -62,6 +62,7 @@ struct __align__(16) RecF {
   int i0, b0, c0, c1;      // tile-local window boundaries
   int b1, i1, flags;
   float iy;                // 1/y (region C)
+  int t0, t1;              // region C: the Algorithm-916 part (tile-local)
 };
 static_assert(sizeof(RecF) == 112, "RecF layout");
 
@@ -195,6 +196,8 @@ __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, con
   r.c1 = clip_local(lp.c1, g0, g1);
   r.b1 = clip_local(lp.b1, g0, g1);
   r.i1 = nonempty ? clip_local(lp.i1, g0, g1) : 0;
+  r.t0 = clip_local(lp.t0, g0, g1);
+  r.t1 = clip_local(lp.t1, g0, g1);
   r.flags = ((lp.flags & HK_PF_WIDE) ? HK_F_WIDE : 0) | (weak ? HK_F_WEAK : 0) | (lev << 8);
   r.iy = lp.y > 0.f ? (float)(1.0 / (double)lp.y) : 0.f;
 }
@@ -393,9 +396,10 @@ __device__ __forceinline__ void sweep_A(const RecF &rr, int wb, int lane,
 // Region C points of the slice, summed in FP64 into cacc, lanes packed by
 // evaluator so a warp never runs both: [t0, t1) holds |x| < sqrt(36 - y^2)
 // (Algorithm 916), the rest of [lo, hi) has r >= 6 (asymptotic series).  The
-// split comes from the FP64 offsets; a point within rounding of r = 6 may
-// take either evaluator (both hold there).  Points leave their owning lane
-// here, so the warp syncs before cacc is touched again.
+// split is the line's own (LinePrepF t0, t1, from the FP64 offsets); a point
+// within rounding of r = 6 may take either evaluator (both hold there).
+// Points leave their owning lane here, so the warp syncs before cacc is
+// touched again.
 __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__ Rj,
                                         double *__restrict__ cacc, int wb, int lane) {
   const int lo = max(r.c0, wb), hi = min(r.c1, wb + HK_SLICE);
@@ -403,14 +407,7 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
   const float dh = r.dh, dl = r.dl, vbh = r.vbh, vbl = r.vbl;
   const float y = r.y, iy = r.iy, ey = r.ey, sig1 = r.sig1;
   const double Sc = r.Sc;
-  int t0 = hi, t1 = hi;
-  if (y < 6.0f) {
-    const double xt = sqrt(36.0 - (double)y * (double)y);
-    const double D0 = (double)dh + (double)dl, vb = (double)vbh + (double)vbl;
-    const double k0 = floor((-xt - D0) / vb) + 1.0, k1 = floor((xt - D0) / vb) + 1.0;
-    t0 = (int)fmin(fmax(k0, (double)lo), (double)hi);
-    t1 = (int)fmin(fmax(k1, (double)t0), (double)hi);
-  }
+  const int t0 = min(max(r.t0, lo), hi), t1 = min(max(r.t1, t0), hi);
   __syncwarp();
   for (int k = t0 + lane; k < t1; k += 32) {
     const float kk = (float)k;
