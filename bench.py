@@ -34,6 +34,10 @@ sys.path.insert(0, os.path.join(ROOT, "helios-k_b200"))
 # figure grows with the Algorithm 916 series length n_iter) + 2 for the
 # strength multiply-add into the sum
 F_A, F_B, F_C0, F_C_ITER, F_ACC = 6, 20, 30, 12, 2
+# DRAM bytes (read + write) of one voigt_sum_kernel<1> launch, from one ncu
+# capture of this workload (profiles/dram_traffic_hitemp.txt); other
+# workloads have no capture and report null
+VOIGT_DRAM_BYTES = {"hitemp-1e7-lines-single-state": 1967831296 + 111279616}
 SIZEOF_STATE = 600  # bytes of hkb::StateDev copied per state per call
 
 
@@ -380,7 +384,8 @@ def main():
                      "achieved": flops_step / (voigt_ms * 1e-3) / 1e12,
                      "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": flops_step / (voigt_ms * 1e-3) / 1e12 / fp32_peak,
-                     "traffic": None, "voigt_ms": voigt_ms, "kdist_ms": kdist_ms,
+                     "traffic": VOIGT_DRAM_BYTES.get(W["label"]) if prec == hkb.MIXED else None,
+                     "voigt_ms": voigt_ms, "kdist_ms": kdist_ms,
                      "peak_source": "in-run FP32 FMA probe (hk_fp32_peak); "
                                     "MEASURED_PEAKS.json has no FP32 SIMT figure"},
         "e2e": {"value": pairs_step * ws / e2e_s, "unit": "Voigt evals/s",
