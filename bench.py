@@ -301,13 +301,19 @@ def main():
 
     stream = torch.cuda.current_stream()
     K = torch.empty((ns, nx), dtype=torch.float64, device="cuda")
+    coeff = torch.empty((ns, nb, nC), dtype=torch.float64, device="cuda")
+    nxmin = torch.empty((ns, nb), dtype=torch.int32, device="cuda")
 
     def step(precision):
         ctx.opacity(T, P, precision, out=K, stream=stream)
         ctx.kdist(K, nC=nC, stream=stream)
 
+    # one step = the whole batch of states (line prep, Voigt sums, fits)
+    # replayed as one CUDA graph (hk_table_build / hk_table_run)
+    ctx.table_build(T, P, K, coeff, nxmin, nC=nC, precision=prec)
+    launches_per_step = ctx.table_kernels
     for _ in range(args.warmup):
-        step(prec)
+        ctx.table_run(stream)
     torch.cuda.synchronize()
     if ws > 1:
         torch.distributed.barrier()
@@ -318,13 +324,13 @@ def main():
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.steps):
-        step(prec)
+        ctx.table_run(stream)
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     clocks = clk.stop()
     ms = barrier_max(ws, ms)
-    launches_per_step = 4  # state prepass (2) + voigt sum + kdist
+    ctx.table_free()
 
     # dominant kernel: per-launch device time with CUDA events on the stream
     vms, kms = [], []
@@ -337,21 +343,24 @@ def main():
     kdist_ms = float(np.mean(kms))
     fp32_peak = ctx.fp32_peak_tflops()
 
-    # end to end through the public API with host buffers: states in, K and
-    # the fit out to pinned host memory
-    K_host = torch.empty((ns, nx), dtype=torch.float64, pin_memory=True)
+    # end to end through the public API with host buffers: states in, the
+    # k-distribution fit out to host memory, and for a single state K too
+    # (a T-P table's product is its fit: its K stays on the device)
+    K_host = torch.empty((ns, nx), dtype=torch.float64, pin_memory=True) if ns == 1 else None
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         ctx.opacity(T, P, prec, out=K, stream=stream)
         r = ctx.kdist(K, nC=nC, stream=stream, outputs_on_device=False)
-        K_host.copy_(K, non_blocking=True)
+        if K_host is not None:
+            K_host.copy_(K, non_blocking=True)
         torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / args.steps
     e2e_s = barrier_max(ws, e2e_s)
+    d2h = ns * nb * (nC * 8 + 4) + (ns * nx * 8 if ns == 1 else 0)
 
     plain = None
-    if not args.no_plain and args.precision == "mixed":
+    if not args.no_plain and args.precision == "mixed" and ns == 1:
         for _ in range(1):
             step(hkb.PLAIN_FP64)
         torch.cuda.synchronize()
@@ -364,6 +373,27 @@ def main():
         pms = barrier_max(ws, e0.elapsed_time(e1) / nplain)
         plain = {"ms_per_step": pms, "value": pairs_step * ws / (pms * 1e-3),
                  "speedup_mixed_vs_plain": pms / ms}
+    elif not args.no_plain and args.precision == "mixed":
+        # a table's plain FP64 run takes minutes: both forms on the same 20
+        # states spread over the table (opacity + fit), 1 untimed + 1 timed
+        sub = np.linspace(0, ns - 1, min(ns, 20)).astype(int)
+        Ks = K[:len(sub)]
+
+        def sub_ms(pr):
+            ctx.opacity(T[sub], P[sub], pr, out=Ks, stream=stream)
+            ctx.kdist(Ks, nC=nC, stream=stream)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            ctx.opacity(T[sub], P[sub], pr, out=Ks, stream=stream)
+            ctx.kdist(Ks, nC=nC, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return barrier_max(ws, e0.elapsed_time(e1))
+
+        mms, pms = sub_ms(hkb.MIXED), sub_ms(hkb.PLAIN_FP64)
+        plain = {"subset_states": len(sub), "mixed_ms": mms, "plain_ms": pms,
+                 "speedup_mixed_vs_plain": pms / mms,
+                 "plain_s_per_table_est": pms * 1e-3 * ns / len(sub)}
 
     value = pairs_step * ws / (ms * 1e-3)
     out = {
@@ -379,6 +409,7 @@ def main():
                    "precision": args.precision, "parallelism": f"states x{ws} ranks",
                    "l2": "inputs larger than L2 (line list ~480 MB resident), no flush"},
         "s_per_state": ms * 1e-3 / ns,
+        "s_per_table": ms * 1e-3 if ns > 1 else None,
         "pairs_per_state": {"A": pa, "B": pb, "C": pc, "C_series_iters": n_iter},
         "roofline": {"bound": "fp32", "kernel": "voigt_sum_kernel",
                      "achieved": flops_step / (voigt_ms * 1e-3) / 1e12,
@@ -390,7 +421,7 @@ def main():
                                     "MEASURED_PEAKS.json has no FP32 SIMT figure"},
         "e2e": {"value": pairs_step * ws / e2e_s, "unit": "Voigt evals/s",
                 "h2d_bytes_per_step": SIZEOF_STATE * ns,
-                "d2h_bytes_per_step": ns * nx * 8 + ns * nb * (nC * 8 + 4)},
+                "d2h_bytes_per_step": d2h},
         "clocks": clocks,
         "gpu_launches": launches_per_step * args.steps,
         "plain_fp64": plain,

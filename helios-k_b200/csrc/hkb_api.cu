@@ -70,6 +70,11 @@ struct hk_ctx {
   int qr_nxb = -1, qr_nc = -1;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   bool have_voigt_t = false, have_kdist_t = false;
+  int64_t launches = 0;  // kernels launched since the last hk_opacity began
+  // T-P table recorded as one CUDA graph (hk_table_build / hk_table_run)
+  cudaGraph_t table_graph = nullptr;
+  cudaGraphExec_t table_exec = nullptr;
+  int64_t table_kernels = 0;
 };
 
 static hk_status fail(hk_ctx *c, hk_status s, const char *fmt, ...) {
@@ -123,9 +128,18 @@ hk_ctx *hk_create(int device, hk_status *status) {
   return c;
 }
 
+static void table_release(hk_ctx *c) {
+  if (c->table_exec) cudaGraphExecDestroy(c->table_exec);
+  if (c->table_graph) cudaGraphDestroy(c->table_graph);
+  c->table_exec = nullptr;
+  c->table_graph = nullptr;
+  c->table_kernels = 0;
+}
+
 void hk_destroy(hk_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
+  table_release(c);
   for (DevBuf *b : {&c->nu0, &c->Sfile, &c->EL, &c->gam, &c->nexp, &c->delta,
                     &c->Aterm, &c->iso, &c->order, &c->states, &c->ticket,
                     &c->prep, &c->wbits, &c->Kwork, &c->outwork, &c->scratch,
@@ -448,9 +462,11 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   unsigned long long *wb = c->wbits.as<unsigned long long>();
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
+  c->launches = 0;
   for (int b0 = 0; b0 < nstates; b0 += batch) {
     const int nb = std::min(batch, nstates - b0);
     const VoigtPlan plan = plan_voigt_sum(mixed, nx, nb, 0);
+    c->launches += 3;  // line prep, state finalize, Voigt sum
     if (plan.nsplit > 1) {
       CUDA_TRY(c, c->vpart.ensure(plan.partial_doubles * sizeof(double)));
       CUDA_TRY(c, c->vcnt.ensure(plan.counters * sizeof(unsigned)));
@@ -548,6 +564,7 @@ hk_status hk_kdist(hk_ctx *c, int nstates, const double *K, int K_on_device, int
     scr = c->scratch.as<double>();
   }
   CUDA_TRY(c, cudaEventRecord(c->ev[2], s));
+  c->launches += 1;
   CUDA_TRY(c, launch_kdist(Kd, nx, nstates, c->nxb, c->nbins, fit ? nC : 0, c->kmin, unitScale,
                            c->qrV.as<double>(), c->qrC.as<double>(), c->qrD.as<double>(),
                            fit ? coef_d : nullptr, nxmin_d, sorted_d, recon_d, scr, s));
@@ -612,6 +629,114 @@ hk_status hk_profile_eval(hk_ctx *c, int64_t n, const double *x, const double *y
   ok(c);
   return HK_OK;
 }
+
+// ---------------------------------------------------------------- tables
+hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *P,
+                         int precision, double *K, int nC, double unitScale, double *coeff,
+                         int32_t *nxmin) {
+  if (!c) return HK_ERR_ARG;
+  hk_status st;
+  if ((st = check_ready(c)) != HK_OK) return st;
+  if (nstates < 1 || !T || !P || !K || !coeff || !nxmin)
+    return fail(c, HK_ERR_ARG, "need nstates >= 1, T, P and device K, coeff, nxmin");
+  if (precision != HK_PRECISION_PLAIN_FP64 && precision != HK_PRECISION_MIXED)
+    return fail(c, HK_ERR_ARG, "precision must be 0 (plain FP64) or 1 (mixed)");
+  if (nstates > 65535) return fail(c, HK_ERR_RANGE, "at most 65535 states per table");
+  if (nC < 1 || nC > 100) return fail(c, HK_ERR_RANGE, "nC must be 1..100 (def_NmaxSample)");
+  if (c->nxb < 4 || nC > c->nxb) return fail(c, HK_ERR_RANGE, "need Nxb >= 4 and nC <= Nxb for the fit");
+  cudaSetDevice(c->device);
+  table_release(c);
+  // everything the graph touches is allocated and uploaded first: capture
+  // records only asynchronous copies, memsets and kernels
+  std::vector<StateDev> hs;
+  if ((st = build_states(c, nstates, T, P, hs)) != HK_OK) return st;
+  CUDA_TRY(c, c->states.ensure(nstates * sizeof(StateDev)));
+  CUDA_TRY(c, c->wbits.ensure(2 * nstates * sizeof(unsigned long long)));
+  CUDA_TRY(c, cudaMemcpy(c->states.p, hs.data(), nstates * sizeof(StateDev), cudaMemcpyHostToDevice));
+  const int64_t nx = c->g.nx;
+  const bool mixed = precision == HK_PRECISION_MIXED;
+  const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
+  int batch = (int)std::max<size_t>(1, c->prep_budget / per_state);
+  const int nsplit = voigt_nsplit(nx);
+  if (nsplit > 1) {
+    const size_t part_per_state = (size_t)((nx + voigt_tile_points() - 1) / voigt_tile_points()) *
+                                  nsplit * voigt_tile_points() * sizeof(double);
+    batch = std::min(batch, (int)std::max<size_t>(1, c->part_budget / part_per_state));
+  }
+  batch = std::min(batch, nstates);
+  CUDA_TRY(c, c->prep.ensure((size_t)batch * per_state));
+  const VoigtPlan plan0 = plan_voigt_sum(mixed, nx, batch, 0);
+  if (plan0.nsplit > 1) {
+    CUDA_TRY(c, c->vpart.ensure(plan0.partial_doubles * sizeof(double)));
+    CUDA_TRY(c, c->vcnt.ensure(plan0.counters * sizeof(unsigned)));
+  }
+  if ((st = ensure_qr(c, nC, 0)) != HK_OK) return st;
+  const size_t nscr = kdist_scratch_doubles(c->nxb, c->nbins, nstates);
+  if (nscr) CUDA_TRY(c, c->scratch.ensure(nscr * sizeof(double)));
+  CUDA_TRY(c, cudaDeviceSynchronize());
+
+  cudaStream_t cs = nullptr;
+  CUDA_TRY(c, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+  StateDev *sd = c->states.as<StateDev>();
+  unsigned long long *wb = c->wbits.as<unsigned long long>();
+  int64_t kernels = 0;
+  for (int b0 = 0; e == cudaSuccess && b0 < nstates; b0 += batch) {
+    const int nb = std::min(batch, nstates - b0);
+    const VoigtPlan plan = plan_voigt_sum(mixed, nx, nb, plan0.ctas);
+    e = launch_line_prep(mixed, c->L, c->g, sd + b0, nb, c->prep.p, wb + 2 * b0, cs);
+    if (e == cudaSuccess)
+      e = launch_voigt_sum(mixed, plan, c->prep.p, c->L.nu0, c->nlines, c->g, sd + b0,
+                           c->ticket.as<unsigned>(), c->vpart.as<double>(), c->vcnt.as<unsigned>(),
+                           K + (size_t)b0 * nx, nx, cs);
+    kernels += 3;
+  }
+  if (e == cudaSuccess) {
+    e = launch_kdist(K, nx, nstates, c->nxb, c->nbins, nC, c->kmin, unitScale, c->qrV.as<double>(),
+                     c->qrC.as<double>(), c->qrD.as<double>(), coeff, nxmin, nullptr, nullptr,
+                     nscr ? c->scratch.as<double>() : nullptr, cs);
+    kernels += 1;
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+  cudaStreamDestroy(cs);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return fail(c, HK_ERR_CUDA, "recording the table graph: %s",
+                cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  cudaGraphExec_t x = nullptr;
+  e = cudaGraphInstantiate(&x, g, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(c, HK_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+  }
+  c->table_graph = g;
+  c->table_exec = x;
+  c->table_kernels = kernels;
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_table_run(hk_ctx *c, void *stream) {
+  if (!c) return HK_ERR_ARG;
+  if (!c->table_exec) return fail(c, HK_ERR_STATE, "hk_table_build must come first");
+  cudaSetDevice(c->device);
+  CUDA_TRY(c, cudaGraphLaunch(c->table_exec, (cudaStream_t)stream));
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_table_free(hk_ctx *c) {
+  if (!c) return HK_ERR_ARG;
+  cudaSetDevice(c->device);
+  table_release(c);
+  return HK_OK;
+}
+
+int64_t hk_table_kernels(const hk_ctx *c) { return c ? c->table_kernels : 0; }
+
+int64_t hk_last_launches(const hk_ctx *c) { return c ? c->launches : 0; }
 
 hk_status hk_last_timing(const hk_ctx *c, double *voigt_ms, double *kdist_ms) {
   if (!c) return HK_ERR_ARG;

@@ -73,6 +73,11 @@ def lib():
             "hk_fp32_peak": (_i, [_p, _p]),
             "hk_kdist_noalloc": (_i, [_p, _i, _i64, _i, _i, _d, _d, _p, _p, _p, _p,
                                       C.c_char_p, _i]),
+            "hk_table_build": (_i, [_p, _i, _p, _p, _i, _p, _i, _d, _p, _p]),
+            "hk_table_run": (_i, [_p, _p]),
+            "hk_table_free": (_i, [_p]),
+            "hk_table_kernels": (_i64, [_p]),
+            "hk_last_launches": (_i64, [_p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -231,6 +236,38 @@ class Context:
                                  _ptr(res["coeff"]), _ptr(res["nxmin"]), _ptr(res["sorted"]),
                                  _ptr(res["recon"]), int(outputs_on_device), sh))
         return res
+
+    # ---------------------------------------------------------- tables
+    def table_build(self, T, P, K, coeff, nxmin, nC=20, unitScale=1.0, precision=MIXED):
+        """Record the T-P table (states T[s], P[s]) as one CUDA graph.
+
+        K (nstates, Nx) float64, coeff (nstates, nbins, nC) float64 and nxmin
+        (nstates, nbins) int32 are torch CUDA tensors that must outlive the
+        table."""
+        T = _f64(np.atleast_1d(T))
+        P = _f64(np.atleast_1d(P))
+        for t in (K, coeff, nxmin):
+            if not _is_dev(t):
+                raise ValueError("table buffers must be CUDA tensors")
+        self._table_bufs = (K, coeff, nxmin)
+        self._chk(lib().hk_table_build(self._h, len(T), _ptr(T), _ptr(P), precision, _ptr(K),
+                                       nC, unitScale, _ptr(coeff), _ptr(nxmin)))
+
+    def table_run(self, stream=None):
+        """Replay the recorded table (one graph launch, asynchronous)."""
+        self._chk(lib().hk_table_run(self._h, _stream_handle(stream, True)))
+
+    def table_free(self):
+        self._chk(lib().hk_table_free(self._h))
+        self._table_bufs = None
+
+    @property
+    def table_kernels(self):
+        return int(lib().hk_table_kernels(self._h))
+
+    @property
+    def last_launches(self):
+        return int(lib().hk_last_launches(self._h))
 
     # ---------------------------------------------------- diagnostics
     def state_lines(self, T, P):

@@ -122,7 +122,9 @@ int64_t hk_grid_points(const hk_ctx *ctx);
 
 /* Opacity K(nu) of every state (T[s], P[s]) onto the grid:
  * K_out[s * Nx + i], FP64.  precision selects the FP64 plain form or the
- * mixed FP32/FP64 form.  All states run in one persistent launch.
+ * mixed FP32/FP64 form.  States run in batches sized to the workspace
+ * budget (per-line records of all states of a batch); each batch is one
+ * persistent Voigt launch.
  * Replaces the per-part / per-pressure loop of heliosk.cu:1051-1776:
  * S2_kernel, the nu sort, S3_kernel, nuLimits/iiLimits, Line6A/B/C_Call and
  * AddKStreams_kernel. */
@@ -164,7 +166,34 @@ hk_status hk_kdist_noalloc(const double *K, int nstates, int64_t nx, int nbins, 
                            double kmin, double unitScale, double *coeff, int32_t *nxmin,
                            double *sortedK, void *stream, char *errbuf, int errbuf_len);
 
+/* ------------------------------------------------------------ tables */
+
+/* A whole T-P table as one CUDA graph: the line scaling, Voigt sums and
+ * k-distribution fits of all nstates states (in batches sized to the
+ * context's workspace budget, each batch one persistent Voigt launch),
+ * recorded once by hk_table_build and replayed by hk_table_run as a single
+ * graph launch.  K (nstates x Nx), coeff (nstates x nbins x nC) and nxmin
+ * (nstates x nbins) are DEVICE buffers owned by the caller that must stay
+ * valid while the table exists; hk_table_build allocates all workspace and
+ * synchronises the device; hk_table_run is asynchronous on `stream`.  The
+ * results equal those of hk_opacity + hk_kdist on the same states.  A new
+ * hk_table_build, hk_table_free or hk_destroy drops the graph; other calls on
+ * the same context between runs reuse its workspace, so rebuild after them.
+ * Replaces the reference's one-state-per-run loop (heliosk.cu:1051-2193 run
+ * once per pressure of the PFile). */
+hk_status hk_table_build(hk_ctx *ctx, int nstates, const double *T, const double *P,
+                         int precision, double *K, int nC, double unitScale,
+                         double *coeff, int32_t *nxmin);
+hk_status hk_table_run(hk_ctx *ctx, void *stream);
+hk_status hk_table_free(hk_ctx *ctx);
+/* kernels recorded in the table graph */
+int64_t hk_table_kernels(const hk_ctx *ctx);
+
 /* ------------------------------------------------------- diagnostics */
+
+/* kernels launched by the last hk_opacity and the hk_kdist calls after it */
+int64_t hk_last_launches(const hk_ctx *ctx);
+
 
 /* Per-line state (nu, S, 1/alphaD, gammaL/alphaD) and the six window
  * indices i0, b0, c0, c1, b1, i1 of every loaded line (in load order is NOT

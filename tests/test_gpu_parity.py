@@ -266,3 +266,37 @@ def test_errors_are_reported(small):
             c2.set_species(hkb.HITRAN, [18.0], [1.0])
             c2.opacity([1000.0], [1.0])
         assert e.value.status == -6
+
+
+def test_table_graph_equals_opacity_and_kdist(small):
+    """hk_table_build/hk_table_run (one CUDA graph for the whole T-P table)
+    give the same bits as hk_opacity + hk_kdist on the same states, on every
+    replay."""
+    import torch
+    ctx = small["ctx"]
+    ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+    Ts = np.array([300.0, 1000.0, 2500.0, 700.0, 1500.0, 120.0])
+    Ps = np.array([1e-6, 1.0, 100.0, 1e-3, 0.1, 10.0])
+    ns, nx, nC = len(Ts), ctx.nx, 20
+    dev = torch.device("cuda")
+    K = torch.empty((ns, nx), dtype=torch.float64, device=dev)
+    coeff = torch.empty((ns, NBINS, nC), dtype=torch.float64, device=dev)
+    nxmin = torch.empty((ns, NBINS), dtype=torch.int32, device=dev)
+    ctx.table_build(Ts, Ps, K, coeff, nxmin, nC=nC)
+    assert ctx.table_kernels >= 4
+    ctx.table_run()
+    torch.cuda.synchronize()
+    K1, c1, n1 = K.cpu().numpy(), coeff.cpu().numpy(), nxmin.cpu().numpy()
+    K.zero_()
+    coeff.zero_()
+    ctx.table_run()
+    torch.cuda.synchronize()
+    assert np.array_equal(K.cpu().numpy(), K1)
+    assert np.array_equal(coeff.cpu().numpy(), c1)
+    ctx.table_free()
+    Kr = ctx.opacity(Ts, Ps, hkb.MIXED)
+    fit = ctx.kdist(Kr, nC=nC)
+    assert ctx.last_launches >= 4
+    assert np.array_equal(K1, Kr)
+    assert np.array_equal(c1, fit["coeff"])
+    assert np.array_equal(n1, fit["nxmin"])
