@@ -63,6 +63,7 @@ struct hk_ctx {
   // workspace
   DevBuf states, ticket, wbits, Kwork, outwork, scratch, prep;
   DevBuf vpart, vcnt;  // split-tile partial sums and per-tile counters
+  DevBuf sscale, gscale, adjwork;  // per-line scales (adjoint parameters), VJP workspace
   size_t prep_budget = (size_t)24 << 30;  // bytes of per-(state, line) records per batch
   size_t part_budget = (size_t)4 << 30;   // bytes of split-tile partial sums per batch
   double voigt_ms_acc = 0.0;
@@ -143,7 +144,7 @@ void hk_destroy(hk_ctx *c) {
   for (DevBuf *b : {&c->nu0, &c->Sfile, &c->EL, &c->gam, &c->nexp, &c->delta,
                     &c->Aterm, &c->iso, &c->order, &c->states, &c->ticket,
                     &c->prep, &c->wbits, &c->Kwork, &c->outwork, &c->scratch,
-                    &c->qrV, &c->qrC, &c->qrD, &c->vpart, &c->vcnt})
+                    &c->qrV, &c->qrC, &c->qrD, &c->vpart, &c->vcnt, &c->sscale, &c->gscale, &c->adjwork})
     b->release();
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -403,6 +404,9 @@ static hk_status build_states(hk_ctx *c, int nstates, const double *T, const dou
       const double mass = c->iso_mass[j] / HK_NA;
       st.iad0[j] = HK_C * std::sqrt(mass / (2.0 * HK_KB * Ts));
       st.Q[j] = Q;
+      double dl = 0.0;
+      partition_dlnq(c->qT[j].data(), c->qQ[j].data(), (int)c->qT[j].size(), Ts, &dl);
+      st.dlnQ[j] = dl;
       double Abundance = c->iso_ab[j];
       double Ss = c->Sscale;
       if (c->units == 0) {
@@ -626,6 +630,96 @@ hk_status hk_profile_eval(hk_ctx *c, int64_t n, const double *x, const double *y
   CUDA_TRY(c, launch_profile_eval(n, xd, yd, precision == HK_PRECISION_MIXED, od, 0));
   CUDA_TRY(c, cudaMemcpy(out, od, n * 8, cudaMemcpyDeviceToHost));
   b.release();
+  ok(c);
+  return HK_OK;
+}
+
+// --------------------------------------------------------------- adjoint
+hk_status hk_set_line_scales(hk_ctx *c, const double *s_scale, const double *g_scale) {
+  if (!c) return HK_ERR_ARG;
+  if (c->nlines == 0 && (s_scale || g_scale)) return fail(c, HK_ERR_STATE, "no lines loaded");
+  cudaSetDevice(c->device);
+  const int64_t n = c->nlines;
+  // host arrays are in load order; the device keeps the nu-sorted order
+  std::vector<int64_t> ord(n);
+  if (n) CUDA_TRY(c, cudaMemcpy(ord.data(), c->order.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
+  std::vector<double> tmp(n);
+  const double *src[2] = {s_scale, g_scale};
+  DevBuf *dst[2] = {&c->sscale, &c->gscale};
+  const double **field[2] = {&c->L.sscale, &c->L.gscale};
+  for (int q = 0; q < 2; ++q) {
+    if (!src[q]) {
+      dst[q]->release();
+      *field[q] = nullptr;
+      continue;
+    }
+    for (int64_t k = 0; k < n; ++k) {
+      const double v = src[q][ord[k]];
+      if (!(v > 0.0) || !std::isfinite(v)) return fail(c, HK_ERR_ARG, "line scale %lld must be finite and > 0", (long long)ord[k]);
+      tmp[k] = v;
+    }
+    CUDA_TRY(c, dst[q]->ensure(n * sizeof(double)));
+    CUDA_TRY(c, cudaMemcpy(dst[q]->p, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    *field[q] = dst[q]->as<double>();
+  }
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_opacity_vjp(hk_ctx *c, double T, double P, int precision, const double *u,
+                         int u_on_device, double *dT, double *dP, double *dlogS, double *dgammaL,
+                         int outputs_on_device, void *stream) {
+  if (!c) return HK_ERR_ARG;
+  hk_status st;
+  if ((st = check_ready(c)) != HK_OK) return st;
+  if (!u) return fail(c, HK_ERR_ARG, "need the seed u (Nx values)");
+  if (precision != HK_PRECISION_PLAIN_FP64 && precision != HK_PRECISION_MIXED)
+    return fail(c, HK_ERR_ARG, "precision must be 0 (plain FP64) or 1 (mixed)");
+  cudaSetDevice(c->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<StateDev> hs;
+  if ((st = build_states(c, 1, &T, &P, hs)) != HK_OK) return st;
+  const int64_t n = c->nlines, nx = c->g.nx;
+  CUDA_TRY(c, c->states.ensure(sizeof(StateDev)));
+  CUDA_TRY(c, c->wbits.ensure(2 * sizeof(unsigned long long)));
+  CUDA_TRY(c, cudaMemcpyAsync(c->states.p, hs.data(), sizeof(StateDev), cudaMemcpyHostToDevice, s));
+  CUDA_TRY(c, c->prep.ensure((size_t)std::max<int64_t>(n, 1) * sizeof(LinePrep)));
+  // the plain per-line records (FP64 windows and constants) of this state
+  CUDA_TRY(c, launch_line_prep(false, c->L, c->g, c->states.as<StateDev>(), 1, c->prep.p,
+                               c->wbits.as<unsigned long long>(), s));
+  // the device copy of the state (wmax finalised) drives both passes
+  CUDA_TRY(c, cudaMemcpyAsync(hs.data(), c->states.p, sizeof(StateDev), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  const double *ud = u;
+  size_t need = 4 * (size_t)std::max<int64_t>(n, 1) + 2;
+  if (!u_on_device) need += (size_t)nx;
+  if (!outputs_on_device) need += 2 * (size_t)n;
+  CUDA_TRY(c, c->adjwork.ensure(need * sizeof(double)));
+  double *G = c->adjwork.as<double>();
+  double *dTP = G + 4 * std::max<int64_t>(n, 1);
+  double *next = dTP + 2;
+  if (!u_on_device) {
+    CUDA_TRY(c, cudaMemcpyAsync(next, u, nx * sizeof(double), cudaMemcpyHostToDevice, s));
+    ud = next;
+    next += nx;
+  }
+  double *dlS = dlogS, *dgm = dgammaL;
+  if (!outputs_on_device) {
+    dlS = dlogS ? next : nullptr;
+    dgm = dgammaL ? next + n : nullptr;
+  }
+  CUDA_TRY(c, launch_opacity_vjp(precision == HK_PRECISION_MIXED, c->L, c->g, c->states.as<StateDev>(),
+                                 hs[0], c->prep.as<LinePrep>(), ud, c->ticket.as<unsigned>(), G,
+                                 c->order.as<int64_t>(), dlS, dgm, dTP, s));
+  double tp[2] = {0.0, 0.0};
+  CUDA_TRY(c, cudaMemcpyAsync(tp, dTP, sizeof tp, cudaMemcpyDeviceToHost, s));
+  if (!outputs_on_device) {
+    if (dlogS) CUDA_TRY(c, cudaMemcpyAsync(dlogS, dlS, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (dgammaL) CUDA_TRY(c, cudaMemcpyAsync(dgammaL, dgm, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  if (dT) *dT = tp[0];
+  if (dP) *dP = tp[1];
   ok(c);
   return HK_OK;
 }

@@ -69,6 +69,8 @@ __device__ __forceinline__ LineState prep_line(const LinesDev &L,
   }
   double aL = __dmul_rn(gam, __dmul_rn(st.PoverP0, pow(st.powbase, ne)));
   aL = __dadd_rn(aL, At);
+  if (L.sscale) S = __dmul_rn(S, L.sscale[l]);
+  if (L.gscale) aL = __dmul_rn(aL, L.gscale[l]);
   double vy = __dmul_rn(aL, iad);
   if (nu == 0.0) {
     S = 0.0;
@@ -439,6 +441,110 @@ __device__ __forceinline__ float voigt916_tab(float x, float y, float iy, float 
   x = fabsf(x);
   if (fmaf(x, x, y * y) >= HK_ASY_R2) return voigt_asy(x, y);
   return voigt916_core(x, y, iy, ey, sig1, R);
+}
+
+// ------------------------------------------------- derivatives (adjoint)
+// Value and partial derivatives in x and y of the line shapes of the three
+// regions, for the vector-Jacobian product of the opacity.
+struct VDer {
+  double v, vx, vy;
+};
+
+// Algorithm 916 in FP64 with forward-mode derivatives: the series of
+// voigt916_d (same terms, same stopping rule, so v equals voigt916_d) with
+// each term differentiated.  With k = 2a/pi, q = sin(xy)^2 / y:
+//   V  = e^{-x^2} erfcx(y) cos 2xy + k e^{-x^2} q + k y (-cos 2xy s1 + (s2 + s3)/2)
+// and d erfcx/dy = 2y erfcx(y) - 2/sqrt(pi).  V is even in x.
+static __device__ __noinline__ VDer voigt916_dd(double x, double y, double ey) {
+  const double a = HK_A916_D;
+  const double ax = fabs(x), sx = x < 0.0 ? -1.0 : 1.0;
+  const double ex2 = exp(-ax * ax);
+  const double isp = 0.56418958354775628695;  // 1/sqrt(pi)
+  VDer o;
+  if (ax == 0.0) {
+    o.v = ey;
+    o.vx = 0.0;
+    o.vy = 2.0 * y * ey - 2.0 * isp;
+    return o;
+  }
+  double s1 = 0.0, s2 = 0.0, s3 = 0.0, s1y = 0.0, s2x = 0.0, s2y = 0.0, s3x = 0.0, s3y = 0.0;
+  {
+    double o1 = 0.0, o2 = 0.0, o3 = 0.0;
+    const double yy = y * y;
+    const int n0 = (int)ceil(ax / a);
+    bool st1 = false, st2 = false, st3 = false;
+    for (int n = 1; n < 100; ++n) {
+      const int n3p = n0 + n - 1, n3n = n0 - n;
+      const double an = a * n, an3p = a * n3p, an3n = a * n3n;
+      const double f = 1.0 / (an * an + yy);
+      const double f3p = 1.0 / (an3p * an3p + yy);
+      const double f3n = 1.0 / (an3n * an3n + yy);
+      const double e1 = exp(-(an * an + ax * ax));
+      const double e2 = exp(-(an + ax) * (an + ax));
+      const double e3p = exp(-(an3p - ax) * (an3p - ax));
+      s1 += f * e1;
+      s1y += -2.0 * y * f * f * e1;
+      s2 += f * e2;
+      s2x += -2.0 * (an + ax) * f * e2;
+      s2y += -2.0 * y * f * f * e2;
+      s3 += f3p * e3p;
+      s3x += 2.0 * (an3p - ax) * f3p * e3p;
+      s3y += -2.0 * y * f3p * f3p * e3p;
+      if (n3n >= 1) {
+        const double e3n = exp(-(an3n - ax) * (an3n - ax));
+        s3 += f3n * e3n;
+        s3x += 2.0 * (an3n - ax) * f3n * e3n;
+        s3y += -2.0 * y * f3n * f3n * e3n;
+      }
+      if (fabs(s1 - o1) < HK_TOL) st1 = true;
+      if (fabs(s2 - o2) < HK_TOL) st2 = true;
+      if (fabs(s3 - o3) < HK_TOL) st3 = true;
+      if (st1 && st2 && st3) break;
+      o1 = s1;
+      o2 = s2;
+      o3 = s3;
+    }
+  }
+  const double s1x = -2.0 * ax * s1;
+  const double xy = ax * y;
+  const double c2 = cos(2.0 * xy), sn2 = sin(2.0 * xy), sn = sin(xy);
+  const double k = 2.0 * a / CUDART_PI;
+  double q, qy;
+  if (y != 0.0) {
+    q = sn * sn / y;
+    qy = ax * sn2 / y - q / y;
+  } else {
+    q = 0.0;
+    qy = ax * ax;
+  }
+  const double br = -c2 * s1 + 0.5 * (s2 + s3);
+  o.v = ex2 * ey * c2 + k * ex2 * q + k * y * br;
+  const double vx = ey * (-2.0 * ax * ex2 * c2 - 2.0 * y * ex2 * sn2) +
+                    k * (-2.0 * ax * ex2 * q + ex2 * sn2) +
+                    k * y * (2.0 * y * sn2 * s1 - c2 * s1x + 0.5 * (s2x + s3x));
+  o.vy = ex2 * ((2.0 * y * ey - 2.0 * isp) * c2 - 2.0 * ax * ey * sn2) + k * ex2 * qy + k * br +
+         k * y * (2.0 * ax * sn2 * s1 - c2 * s1y + 0.5 * (s2y + s3y));
+  o.vx = sx * vx;
+  if (y == 0.0) o.v = ex2;
+  return o;
+}
+
+// GH2 rational of region B (gh2_d) and its partials in s = x^2 and Y = y^2:
+// t = num / den, num = a1 (u + 1) - (4/pi) s, den = u (a1^2 - (6/pi) s),
+// u = s + Y, a1 = u + 1.5.
+template <class F>
+__device__ __forceinline__ void gh2_grad(F s, F Y, F &t, F &ts, F &tY) {
+  const F u = s + Y;
+  const F a1 = u + F(1.5);
+  const F c4 = F(4.0 / CUDART_PI), c6 = F(6.0 / CUDART_PI);
+  const F num = a1 * (u + F(1)) - c4 * s;
+  const F q = a1 * a1 - c6 * s;
+  const F den = u * q;
+  t = num / den;
+  const F num_s = (u + F(1)) + a1 - c4, num_Y = (u + F(1)) + a1;
+  const F den_s = q + u * (F(2) * a1 - c6), den_Y = q + u * F(2) * a1;
+  ts = (num_s - t * den_s) / den;
+  tY = (num_Y - t * den_Y) / den;
 }
 
 }  // namespace hkb

@@ -39,6 +39,25 @@ int partition_interp(const double *Tq, const double *q, int n, double T, double 
   return 0;
 }
 
+// d ln Q / dT of the interpolant partition_interp evaluates: the slope of the
+// segment holding T over Q(T); at a table node, the mean of the slopes of the
+// two segments meeting there (what a central difference sees).
+int partition_dlnq(const double *Tq, const double *q, int n, double T, double *out) {
+  double Q;
+  if (!partition_interp(Tq, q, n, T, &Q) || !(Q > 0.0)) return 0;
+  int j = 1;
+  while (j < n - 1 && Tq[j] < T) ++j;  // Tq[j-1] < T <= Tq[j] (or the ends)
+  if (n < 2) {
+    *out = 0.0;
+    return 1;
+  }
+  if (j >= n) j = n - 1;
+  double slope = (q[j] - q[j - 1]) / (Tq[j] - Tq[j - 1]);
+  if (T == Tq[j] && j + 1 < n) slope = 0.5 * (slope + (q[j + 1] - q[j]) / (Tq[j + 1] - Tq[j]));
+  *out = slope / Q;
+  return 1;
+}
+
 int read_q_file(const std::string &fname, int ncol, std::vector<double> &T,
                 std::vector<double> &Q, std::string &msg) {
   FILE *f = fopen(fname.c_str(), "r");

@@ -58,6 +58,7 @@ struct Params {
 
 // Returns 0 or a negative hk_status; msg explains.
 int partition_interp(const double *T, const double *Q, int n, double Tq, double *out);
+int partition_dlnq(const double *Tq, const double *q, int n, double T, double *out);
 int read_q_file(const std::string &fname, int ncol, std::vector<double> &T,
                 std::vector<double> &Q, std::string &msg);
 int read_species_param(const std::string &path, const std::string &species,

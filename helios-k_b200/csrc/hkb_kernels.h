@@ -17,6 +17,15 @@ constexpr int KD_SMEM_LIMIT = 225 * 1024;
 int voigt_tile_points();
 cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream);
 
+// Vector-Jacobian product of one state's opacity (hkb_adjoint.cu): G_d holds
+// 4 x nlines FP64 sums, dTP_d the two scalars; dlogS_d / dgam_d (load order
+// through order_d, may be null) the per-line results.
+cudaError_t launch_opacity_vjp(bool mixed, const LinesDev &L, const GridDev &g,
+                               const StateDev *state_d, const StateDev &state_h,
+                               const LinePrep *prep_d, const double *u_d, unsigned *ticket_d,
+                               double *G_d, const int64_t *order_d, double *dlogS_d,
+                               double *dgam_d, double *dTP_d, cudaStream_t stream);
+
 // per-(line, state) records: LinePrepF (mixed) or LinePrep (plain FP64)
 cudaError_t launch_line_prep(bool mixed, const LinesDev &L, const GridDev &g, StateDev *states_d,
                              int nstates, void *prep_d, unsigned long long *wbits_d,

@@ -40,6 +40,9 @@ struct LinesDev {
   const double *Aterm;  // A / (4 pi c)
   const uint8_t *iso;   // isotopologue index (null: 0)
   double EL_c, gam_c, nexp_c, delta_c, Aterm_c;
+  // optional per-line multipliers of the scaled strength and of the Lorentz
+  // half-width (null: 1), the differentiable line parameters of the adjoint
+  const double *sscale, *gscale;
 };
 
 struct GridDev {
@@ -104,7 +107,8 @@ struct StateDev {
   double Q[HK_MAX_ISO];     // partition function at T
   double ab[HK_MAX_ISO];    // abundance * (m / meanMass) when units == 0
   double ss[HK_MAX_ISO];    // species scale * (m / meanMass) when units == 0
+  double dlnQ[HK_MAX_ISO];  // d ln Q / dT of the interpolated partition function
 };
-static_assert(sizeof(StateDev) == 600, "StateDev layout (the host copies it per state)");
+static_assert(sizeof(StateDev) == 728, "StateDev layout (the host copies it per state)");
 
 }  // namespace hkb

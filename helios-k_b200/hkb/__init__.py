@@ -73,6 +73,8 @@ def lib():
             "hk_fp32_peak": (_i, [_p, _p]),
             "hk_kdist_noalloc": (_i, [_p, _i, _i64, _i, _i, _d, _d, _p, _p, _p, _p,
                                       C.c_char_p, _i]),
+            "hk_set_line_scales": (_i, [_p, _p, _p]),
+            "hk_opacity_vjp": (_i, [_p, _d, _d, _i, _p, _i, _p, _p, _p, _p, _i, _p]),
             "hk_table_build": (_i, [_p, _i, _p, _p, _i, _p, _i, _d, _p, _p]),
             "hk_table_run": (_i, [_p, _p]),
             "hk_table_free": (_i, [_p]),
@@ -236,6 +238,28 @@ class Context:
                                  _ptr(res["coeff"]), _ptr(res["nxmin"]), _ptr(res["sorted"]),
                                  _ptr(res["recon"]), int(outputs_on_device), sh))
         return res
+
+    # --------------------------------------------------------- adjoint
+    def set_line_scales(self, s_scale=None, g_scale=None):
+        """Per-line multipliers of strength and Lorentz width (load order)."""
+        s = None if s_scale is None else _f64(s_scale)
+        g = None if g_scale is None else _f64(g_scale)
+        self._chk(lib().hk_set_line_scales(self._h, _ptr(s), _ptr(g)))
+
+    def opacity_vjp(self, T, P, u, precision=MIXED, per_line=True, stream=None):
+        """dLoss/dT, dLoss/dP and (per_line) dLoss/dlog S, dLoss/dgammaL for
+        the seed u = dLoss/dK (Nx values; numpy or CUDA tensor)."""
+        dev = _is_dev(u)
+        if not dev:
+            u = _f64(u)
+        n = self.num_lines
+        dT, dP = C.c_double(0), C.c_double(0)
+        dS = np.empty(n, np.float64) if per_line else None
+        dG = np.empty(n, np.float64) if per_line else None
+        sh = _stream_handle(stream, dev)
+        self._chk(lib().hk_opacity_vjp(self._h, float(T), float(P), precision, _ptr(u), int(dev),
+                                       C.byref(dT), C.byref(dP), _ptr(dS), _ptr(dG), 0, sh))
+        return dT.value, dP.value, dS, dG
 
     # ---------------------------------------------------------- tables
     def table_build(self, T, P, K, coeff, nxmin, nC=20, unitScale=1.0, precision=MIXED):

@@ -166,6 +166,30 @@ hk_status hk_kdist_noalloc(const double *K, int nstates, int64_t nx, int nbins, 
                            double kmin, double unitScale, double *coeff, int32_t *nxmin,
                            double *sortedK, void *stream, char *errbuf, int errbuf_len);
 
+/* ----------------------------------------------------------- adjoint */
+
+/* Optional per-line multipliers, in load order (host arrays of
+ * hk_num_lines values, each finite and > 0; NULL restores 1): the scaled
+ * strength of line l is multiplied by s_scale[l] and its Lorentz half-width
+ * gammaL (collisional + natural) by g_scale[l].  They make log S and
+ * gammaL per-line parameters of the forward, for gradient-based fitting.
+ * Loading a new line list clears them.  No counterpart in the reference. */
+hk_status hk_set_line_scales(hk_ctx *ctx, const double *s_scale, const double *g_scale);
+
+/* Vector-Jacobian product of the opacity of one state: with the seed
+ * u[i] = dLoss/dK_i (Nx values, e.g. w_i / K_i for Loss = sum_i w_i log K_i),
+ * returns dLoss/dT (K), dLoss/dP (atm for HITRAN, bar for ExoMol), and per
+ * line (load order) dLoss/dlog S_l and dLoss/dgammaL_l (cm).  The forward is
+ * recomputed per grid tile (nothing of it is stored); regions A and B are
+ * differentiated in the working precision (FP32 in the mixed form, x from
+ * the FP64 offset), region C through the FP64 Algorithm-916 series, and the
+ * per-line sums are FP64 (accumulated with atomics: the last bits may vary
+ * between runs).  Any of dT, dP, dlogS, dgammaL may be NULL.  Synchronous.
+ * No counterpart in the reference (it computes no derivatives). */
+hk_status hk_opacity_vjp(hk_ctx *ctx, double T, double P, int precision, const double *u,
+                         int u_on_device, double *dT, double *dP, double *dlogS,
+                         double *dgammaL, int outputs_on_device, void *stream);
+
 /* ------------------------------------------------------------ tables */
 
 /* A whole T-P table as one CUDA graph: the line scaling, Voigt sums and

@@ -706,3 +706,139 @@ void hko_kdist(double *K, int64_t nx, int nxb, int nbins, int nc, double kmin,
   }
   free(tmp);
 }
+
+/* ---------------------------------------------------- reference gradient */
+
+/* Algorithm 916 (voigt916_ey) with forward-mode derivatives in x and y:
+ * every series term differentiated, same stopping rule.  With k = 2a/pi and
+ * q = sin(xy)^2 / y:
+ *   V = e^{-x^2} erfcx(y) cos 2xy + k e^{-x^2} q + k y (-cos 2xy s1 + (s2+s3)/2),
+ *   d erfcx/dy = 2y erfcx(y) - 2/sqrt(pi).  Test oracle for the adjoint. */
+static void voigt916_grad(double x, double y, double ey, double *v, double *vx, double *vyo) {
+  static double a = 0.0;
+  if (a == 0.0) a = M_PI * sqrt(-1.0 / log(HKO_TOL * 0.5));
+  const double ax = fabs(x), sx = x < 0.0 ? -1.0 : 1.0;
+  const double ex2 = exp(-ax * ax), isp = 1.0 / sqrt(M_PI);
+  if (ax == 0.0) {
+    *v = ey;
+    *vx = 0.0;
+    *vyo = 2.0 * y * ey - 2.0 * isp;
+    return;
+  }
+  double s1 = 0, s2 = 0, s3 = 0, s1y = 0, s2x = 0, s2y = 0, s3x = 0, s3y = 0;
+  double o1 = 0, o2 = 0, o3 = 0;
+  const double yy = y * y;
+  const int n0 = (int)ceil(ax / a);
+  int st1 = 0, st2 = 0, st3 = 0;
+  for (int n = 1; n < 100; ++n) {
+    const int n3p = n0 + n - 1, n3n = n0 - n;
+    const double an = a * n, ap = a * n3p, am = a * n3n;
+    const double f = 1.0 / (an * an + yy), fp = 1.0 / (ap * ap + yy), fm = 1.0 / (am * am + yy);
+    const double e1 = exp(-(an * an + ax * ax)), e2 = exp(-(an + ax) * (an + ax));
+    const double ep = exp(-(ap - ax) * (ap - ax));
+    s1 += f * e1;
+    s1y -= 2.0 * y * f * f * e1;
+    s2 += f * e2;
+    s2x -= 2.0 * (an + ax) * f * e2;
+    s2y -= 2.0 * y * f * f * e2;
+    s3 += fp * ep;
+    s3x += 2.0 * (ap - ax) * fp * ep;
+    s3y -= 2.0 * y * fp * fp * ep;
+    if (n3n >= 1) {
+      const double em = exp(-(am - ax) * (am - ax));
+      s3 += fm * em;
+      s3x += 2.0 * (am - ax) * fm * em;
+      s3y -= 2.0 * y * fm * fm * em;
+    }
+    if (fabs(s1 - o1) < HKO_TOL) st1 = 1;
+    if (fabs(s2 - o2) < HKO_TOL) st2 = 1;
+    if (fabs(s3 - o3) < HKO_TOL) st3 = 1;
+    if (st1 && st2 && st3) break;
+    o1 = s1;
+    o2 = s2;
+    o3 = s3;
+  }
+  const double s1x = -2.0 * ax * s1;
+  const double xy = ax * y, c2 = cos(2.0 * xy), sn2 = sin(2.0 * xy), sn = sin(xy);
+  const double k = 2.0 * a / M_PI;
+  double q, qy;
+  if (y != 0.0) {
+    q = sn * sn / y;
+    qy = ax * sn2 / y - q / y;
+  } else {
+    q = 0.0;
+    qy = ax * ax;
+  }
+  const double br = -c2 * s1 + 0.5 * (s2 + s3);
+  *v = (y == 0.0) ? ex2 : ex2 * ey * c2 + k * ex2 * q + k * y * br;
+  *vx = sx * (ey * (-2.0 * ax * ex2 * c2 - 2.0 * y * ex2 * sn2) + k * (-2.0 * ax * ex2 * q + ex2 * sn2) +
+              k * y * (2.0 * y * sn2 * s1 - c2 * s1x + 0.5 * (s2x + s3x)));
+  *vyo = ex2 * ((2.0 * y * ey - 2.0 * isp) * c2 - 2.0 * ax * ey * sn2) + k * ex2 * qy + k * br +
+         k * y * (2.0 * ax * sn2 * s1 - c2 * s1y + 0.5 * (s2y + s3y));
+}
+
+/* region B's GH2 t4 (hko_gh2, voigt.h:1481-1490) in the algebraically equal
+ * form num/den, num = a1 (u+1) - (4/pi) s, den = u (a1^2 - (6/pi) s),
+ * u = s + Y, a1 = u + 1.5 (s = x^2, Y = y^2), and its partials in s and Y */
+static void gh2_grad(double s, double Y, double *t, double *ts, double *tY) {
+  const double u = s + Y, a1 = u + 1.5, c4 = 4.0 / M_PI, c6 = 6.0 / M_PI;
+  const double num = a1 * (u + 1.0) - c4 * s, q = a1 * a1 - c6 * s, den = u * q;
+  *t = num / den;
+  *ts = (((u + 1.0) + a1 - c4) - *t * (q + u * (2.0 * a1 - c6))) / den;
+  *tY = (((u + 1.0) + a1) - *t * (q + u * 2.0 * a1)) / den;
+}
+
+/* Per-line sums of the vector-Jacobian product of K (test oracle of the
+ * adjoint): with c_li the contribution of line l to K_i (hko_opacity's
+ * regions), G[l] = sum_i u_i c_li, G[n+l] = sum_i u_i dc/dy,
+ * G[2n+l] = sum_i u_i dc/dx x_li, G[3n+l] = sum_i u_i dc/dx, i over the line's
+ * window inside [0, nx).  OpenMP over lines. */
+void hko_vjp_sums(int64_t n, const double *nu, const double *S, const double *iad,
+                  const double *vy, const int64_t *win, double numin, double dnu, int64_t nx,
+                  const double *u, double *G, int nthreads) {
+  const double isp = 1.0 / sqrt(M_PI);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t l = 0; l < n; ++l) {
+    const int64_t *o = win + 6 * l;
+    double gS = 0, gy = 0, gx = 0, gn = 0;
+    const double y = vy[l], Sl = S[l], ey = hko_erfcx(vy[l]);
+    const double Sp = Sl / M_PI;
+    const int64_t a0 = o[0] > 0 ? o[0] : 0, a1 = o[5] < nx ? o[5] : nx;
+    for (int64_t i = a0; i < a1 && Sl != 0.0; ++i) {
+      const double x = (hko_grid_x(numin, dnu, i) - nu[l]) * iad[l];
+      double c, cx, cy;
+      if (i >= o[2] && i < o[3]) {
+        double v, vx, vyy;
+        voigt916_grad(x, y, ey, &v, &vx, &vyy);
+        c = Sl * isp * v;
+        cx = Sl * isp * vx;
+        cy = Sl * isp * vyy;
+      } else {
+        double t, ts, tY;
+        if (i >= o[1] && i < o[4]) {
+          gh2_grad(x * x, y * y, &t, &ts, &tY);
+        } else {
+          t = 1.0 / (x * x + y * y);
+          ts = -t * t;
+          tY = ts;
+        }
+        c = Sp * y * t;
+        cx = Sp * y * ts * 2.0 * x;
+        cy = Sp * (t + 2.0 * y * y * tY);
+      }
+      gS += u[i] * c;
+      gy += u[i] * cy;
+      gx += u[i] * cx * x;
+      gn += u[i] * cx;
+    }
+    G[l] = gS;
+    G[n + l] = gy;
+    G[2 * n + l] = gx;
+    G[3 * n + l] = gn;
+  }
+}

@@ -86,6 +86,12 @@ void hko_opacity(int64_t n, const double *nu, const double *S,
                  double numin, double dnu, int64_t ib, int64_t ie, double kmin,
                  double *K, int nthreads, int64_t pairs_out[3]);
 
+/* per-line sums of the vector-Jacobian product of K (G: 4 x n), test
+ * oracle of the adjoint */
+void hko_vjp_sums(int64_t n, const double *nu, const double *S, const double *iad,
+                  const double *vy, const int64_t *win, double numin, double dnu, int64_t nx,
+                  const double *u, double *G, int nthreads);
+
 /* k-distribution fit, resample.h */
 void hko_vandermonde(int nxb, int nc, double *V);
 void hko_qr(int nxb, int nc, double *V, double *C, double *D);

@@ -59,6 +59,7 @@ def lib():
         L.hko_gh2.argtypes = [_d, _d]
         L.hko_opacity.argtypes = [_i64, _p, _p, _p, _p, _p, _d, _d, _i64, _i64,
                                   _d, _p, _i, _p]
+        L.hko_vjp_sums.argtypes = [_i64, _p, _p, _p, _p, _p, _d, _d, _i64, _p, _p, _i]
         L.hko_vandermonde.argtypes = [_i, _i, _p]
         L.hko_qr.argtypes = [_i, _i, _p, _p, _p]
         L.hko_sort_bins.argtypes = [_i64, _p, _i, _p]
@@ -244,3 +245,76 @@ def state_opacity(lines, iso_mass, iso_ab, iso_Q, T, P, numin, numax, dnu,
     win = windows(nu, S, iad, vy, numin, dnu, nx, cutMode, cut)
     K, pairs = opacity(nu, S, iad, vy, win, numin, dnu, nx, kmin, nthreads)
     return K, pairs, (nu, S, iad, vy, win)
+
+
+# ------------------------------------------------------ reference gradient
+
+_H, _C, _KB, _T0 = 6.62606957e-27, 2.99792458e10, 1.3806489e-16, 296.0
+
+
+def vjp_sums(nu, S, iad, vy, win, numin, dnu, nx, u, nthreads=0):
+    """hko_vjp_sums: (4, n) per-line sums of the vector-Jacobian product of
+    K (G_S, G_y, G_x, G_n), FP64."""
+    n = len(nu)
+    nu, S, iad, vy, u = map(_f64, (nu, S, iad, vy, u))
+    win = np.ascontiguousarray(win, dtype=np.int64)
+    G = np.zeros(4 * n, np.float64)
+    lib().hko_vjp_sums(n, _ptr(nu), _ptr(S), _ptr(iad), _ptr(vy), _ptr(win), numin, dnu, nx,
+                       _ptr(u), _ptr(G), nthreads)
+    return G.reshape(4, n)
+
+
+def partition_dlnq(Tq, q, T):
+    """d ln Q / dT of the linear interpolant of host.h:9-73: the slope of the
+    segment holding T (the mean of the two slopes at a table node) over Q."""
+    Tq, q = _f64(Tq), _f64(q)
+    Q = partition(Tq, q, T)
+    j = int(np.searchsorted(Tq, T, side="left"))
+    j = min(max(j, 1), len(Tq) - 1)
+    slope = (q[j] - q[j - 1]) / (Tq[j] - Tq[j - 1])
+    if T == Tq[j] and j + 1 < len(Tq):
+        slope = 0.5 * (slope + (q[j + 1] - q[j]) / (Tq[j + 1] - Tq[j]))
+    return slope / Q
+
+
+def vjp_hitran(lines, mass, Tq, Qq, T, P, u, numin, dnu, nx, cut=25.0, qalphaL=1.0,
+               s_scale=None, g_scale=None):
+    """FP64 reference gradient of a loss with seed u = dLoss/dK (one HITRAN
+    isotopologue, cutMode 0): returns (dT, dP, dlogS per line, dgammaL per
+    line), by the chain rule of the line scaling of prep_hitran applied to
+    the per-line sums of vjp_sums.  Optional per-line multipliers of the
+    strength and of the Lorentz width, as the library's hk_set_line_scales."""
+    Q = partition(Tq, Qq, T)
+    nu, S, iad, vy = prep_hitran(lines, [mass], [1.0], [Q], T, P, qalphaL=qalphaL)
+    if s_scale is not None:
+        S = S * s_scale
+    if g_scale is not None:
+        vy = vy * g_scale
+    win = windows(nu, S, iad, vy, numin, dnu, nx, 0, cut)
+    gS, gy, gx, gn = vjp_sums(nu, S, iad, vy, win, numin, dnu, nx, u)
+    c = _H * _C / _KB
+    el = _f64(lines["EL"])
+    delta = _f64(lines["delta"])
+    ne = _f64(lines["n"])
+    At = _f64(lines["A"]) / (4.0 * np.pi * _C)
+    gs = np.ones_like(nu) if g_scale is None else _f64(g_scale)
+    dlnQ = partition_dlnq(Tq, Qq, T)
+    e1, e0 = np.exp(-c * nu / T), np.exp(-c * nu / _T0)
+    dlS_dT = -dlnQ + c * el / T**2 - (c * nu / T**2) * e1 / (1 - e1) - 0.5 / T
+    dlS_dnu = (c / T) * e1 / (1 - e1) - (c / _T0) * e0 / (1 - e0) - 1.0 / nu
+    gam = (1.0 - qalphaL) * _f64(lines["gair"]) + qalphaL * _f64(lines["gself"])
+    pb = (_T0 / T) ** ne
+    aLc = gs * gam * P * pb
+    aL = gs * (gam * P * pb + At)
+    daL_dT = -ne * aLc / T
+    daL_dP = gs * gam * pb
+    diad_dT = -0.5 * iad / T
+    diad_dP = -iad * delta / nu
+    dy_dT = daL_dT * iad + aL * diad_dT
+    dy_dP = daL_dP * iad + aL * diad_dP
+    ok = (S != 0) & (iad > 0)
+    gI = np.where(ok, gx / np.where(ok, iad, 1.0), 0.0)
+    gN = -gn * iad
+    dT = float(np.sum(np.where(ok, gS * dlS_dT + gy * dy_dT + gI * diad_dT, 0.0)))
+    dP = float(np.sum(np.where(ok, gS * dlS_dnu * delta + gy * dy_dP + gI * diad_dP + gN * delta, 0.0)))
+    return dT, dP, gS, gy * iad

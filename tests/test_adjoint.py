@@ -1,0 +1,122 @@
+"""GPU: the opacity adjoint (hk_opacity_vjp) against the FP64 oracle gradient
+and central finite differences; the torch.autograd bridge.
+
+Tolerances (written here): plain FP64 adjoint vs oracle 1e-9 relative;
+mixed adjoint (regions A/B in FP32) vs oracle 1e-4 relative on dLoss/dT and
+dLoss/dP and 1e-5 of the largest per-line value; finite differences (h = 1e-3
+relative, central) vs the oracle gradient 1e-4 relative.
+"""
+import numpy as np
+import pytest
+
+import hkb
+import oracle
+from hkb import synth
+
+pytestmark = pytest.mark.gpu
+
+NUMIN, NUMAX, DNU, NBINS = 1000.0, 1300.0, 0.01, 10
+T0, P0 = 800.3, 1.0
+
+
+@pytest.fixture(scope="module")
+def adj():
+    L = synth.hitran_lines(800, seed=5, nu_max=NUMAX, nu_min=NUMIN)
+    Tq, Qq = synth.q_table()
+    ctx = hkb.Context(0)
+    ctx.set_species(hkb.HITRAN, [synth.MASS], [1.0])
+    ctx.set_partition(0, Tq, Qq)
+    ctx.set_options(qalphaL=1.0)
+    ctx.load_lines_hitran(L)
+    ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+    w = np.random.default_rng(0).standard_normal(ctx.nx)
+    yield dict(ctx=ctx, L=L, Tq=Tq, Qq=Qq, w=w)
+    ctx.close()
+
+
+def loss(d, T, P, precision=hkb.PLAIN_FP64):
+    K = d["ctx"].opacity([T], [P], precision)[0]
+    return float(np.sum(d["w"] * np.log(K))), K
+
+
+def reference(d, T=T0, P=P0, u=None):
+    nx = d["ctx"].nx
+    if u is None:
+        u = d["w"] / loss(d, T, P)[1]
+    return oracle.vjp_hitran(d["L"], synth.MASS, d["Tq"], d["Qq"], T, P, u, NUMIN, DNU, nx)
+
+
+def test_vjp_plain_and_mixed_vs_oracle(adj):
+    ctx = adj["ctx"]
+    _, K = loss(adj, T0, P0)
+    u = adj["w"] / K
+    rT, rP, rS, rG = reference(adj, u=u)
+    for prec, tol, tol_line in ((hkb.PLAIN_FP64, 1e-9, 1e-9), (hkb.MIXED, 1e-4, 1e-5)):
+        dT, dP, dS, dG = ctx.opacity_vjp(T0, P0, u, prec)
+        eT, eP = abs(dT - rT) / abs(rT), abs(dP - rP) / abs(rP)
+        eS = np.max(np.abs(dS - rS)) / np.max(np.abs(rS))
+        eG = np.max(np.abs(dG - rG)) / np.max(np.abs(rG))
+        print(f"precision {prec}: dT {eT:.2e} dP {eP:.2e} dlogS {eS:.2e} dgammaL {eG:.2e}")
+        assert eT < tol and eP < tol
+        assert eS < tol_line and eG < tol_line
+
+
+def test_vjp_vs_central_differences(adj):
+    ctx = adj["ctx"]
+    rT, rP, rS, rG = reference(adj)
+    hT, hP = 1e-3 * T0, 1e-3 * P0
+    fT = (loss(adj, T0 + hT, P0)[0] - loss(adj, T0 - hT, P0)[0]) / (2 * hT)
+    fP = (loss(adj, T0, P0 + hP)[0] - loss(adj, T0, P0 - hP)[0]) / (2 * hP)
+    print(f"dT {rT:.6g} fd {fT:.6g}; dP {rP:.6g} fd {fP:.6g}")
+    assert abs(fT - rT) / abs(rT) < 1e-4
+    assert abs(fP - rP) / abs(rP) < 1e-4
+    # per line: strength and width multipliers of the two lines with the
+    # largest gradients, through hk_set_line_scales
+    n = ctx.num_lines
+    _, _, iad, vy, _ = ctx.state_lines(T0, P0)
+    aL = np.empty(n)
+    aL[ctx.line_order()] = vy / iad
+    e = 1e-3
+    for l in np.argsort(-np.abs(rS))[:2]:
+        s = np.ones(n)
+        s[l] = np.exp(e)
+        ctx.set_line_scales(s, None)
+        lp = loss(adj, T0, P0)[0]
+        s[l] = np.exp(-e)
+        ctx.set_line_scales(s, None)
+        lm = loss(adj, T0, P0)[0]
+        assert abs((lp - lm) / (2 * e) - rS[l]) < 1e-4 * abs(rS[l])
+    for l in np.argsort(-np.abs(rG * aL))[:2]:
+        gsc = np.ones(n)
+        gsc[l] = np.exp(e)
+        ctx.set_line_scales(None, gsc)
+        lp = loss(adj, T0, P0)[0]
+        gsc[l] = np.exp(-e)
+        ctx.set_line_scales(None, gsc)
+        lm = loss(adj, T0, P0)[0]
+        assert abs((lp - lm) / (2 * e) - rG[l] * aL[l]) < 1e-4 * abs(rG[l] * aL[l])
+    ctx.set_line_scales(None, None)
+
+
+def test_autograd_function(adj):
+    import torch
+    from hkb.autograd import Opacity
+    ctx = adj["ctx"]
+    n = ctx.num_lines
+    T = torch.tensor(T0, dtype=torch.float64, requires_grad=True)
+    P = torch.tensor(P0, dtype=torch.float64, requires_grad=True)
+    log_s = torch.zeros(n, dtype=torch.float64, requires_grad=True)
+    log_g = torch.zeros(n, dtype=torch.float64, requires_grad=True)
+    w = torch.as_tensor(adj["w"], device="cuda")
+    K = Opacity.apply(ctx, T, P, log_s, log_g, hkb.PLAIN_FP64)
+    L = torch.sum(w * torch.log(K))
+    L.backward()
+    rT, rP, rS, rG = reference(adj)
+    _, _, iad, vy, _ = ctx.state_lines(T0, P0)
+    aL = np.empty(n)
+    aL[ctx.line_order()] = vy / iad
+    assert abs(T.grad.item() - rT) < 1e-9 * abs(rT)
+    assert abs(P.grad.item() - rP) < 1e-9 * abs(rP)
+    assert np.max(np.abs(log_s.grad.numpy() - rS)) < 1e-9 * np.max(np.abs(rS))
+    assert np.max(np.abs(log_g.grad.numpy() - rG * aL)) < 1e-9 * np.max(np.abs(rG * aL))
+    ctx.set_line_scales(None, None)
