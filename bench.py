@@ -47,10 +47,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hitemp", choices=["hitemp", "small", "table", "hitemp_sparse"])
+    ap.add_argument("--workload", default="hitemp",
+                    choices=["hitemp", "small", "table", "hitemp_sparse", "adjoint"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip timing the reference's own CUDA build beside ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -66,6 +69,7 @@ def workload(name):
         W = dict(synth.WORKLOADS[name])
         W["label"] = {"hitemp": "hitemp-1e7-lines-single-state",
                       "small": "small-1e5-lines-single-state",
+                      "adjoint": "adjoint-1e6-lines-1000-10000cm-1",
                       "hitemp_sparse": "hitemp-distribution-1e6-lines-single-state"}[name]
     return W
 
@@ -270,10 +274,104 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def run_adjoint(args):
+    """Adjoint workload: one step = forward K(T, P), the seed u = w / K of
+    Loss = sum_i w_i log K_i, and the vector-Jacobian product (dLoss/dT,
+    dLoss/dP, per-line dLoss/dlog S and dLoss/dgammaL).  1 GPU."""
+    import torch
+    import hkb
+    W = workload("adjoint")
+    L = make_lines(W)
+    ctx = open_ctx(W, L, 0)
+    ctx._numin, ctx._dnu = W["numin"], W["dnu"]
+    T, P = W["T"][0], W["P"][0]
+    prec = hkb.MIXED if args.precision == "mixed" else hkb.PLAIN_FP64
+    nx, n = ctx.nx, ctx.num_lines
+    pa, pb, pc, _, _ = count_pairs(ctx, T, P)
+    pairs = pa + pb + pc
+    w = torch.as_tensor(np.random.default_rng(7).standard_normal(nx), device="cuda")
+    K = torch.empty((1, nx), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        ctx.opacity([T], [P], prec, out=K, stream=stream)
+        u = w / K[0]
+        return ctx.opacity_vjp(T, P, u, prec)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clk = Clocks(0)
+    clk.start()
+    t0 = time.perf_counter()
+    fwd = []
+    for _ in range(args.steps):
+        ctx.opacity([T], [P], prec, out=K, stream=stream)
+        torch.cuda.synchronize()
+        fwd.append(ctx.last_timing()[0])
+        ctx.opacity_vjp(T, P, w / K[0], prec)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    clocks = clk.stop()
+    fwd_ms = float(np.mean(fwd))
+    out = {"metric": "Voigt evals/s (forward + adjoint)", "value": 2 * pairs / (ms * 1e-3),
+           "unit": "Voigt evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32 A/B (f64 offsets), f64 region C and sums" if prec == hkb.MIXED else "f64",
+           "data": "synthetic (seeded; BASELINE config distributions)",
+           "config": {"workload": W["label"], "lines": W["n"], "grid_points": nx, "T": T, "P": P,
+                      "cut_cm-1": W["cut"], "precision": args.precision,
+                      "loss": "sum_i w_i log K_i, w ~ N(0,1)",
+                      "timing": "wall clock around synchronous steps"},
+           "pairs": {"A": pa, "B": pb, "C": pc}, "forward_voigt_ms": fwd_ms,
+           "adjoint_ms": ms - fwd_ms, "clocks": clocks,
+           "gpu_launches": args.steps * 7}  # prep 2 + voigt, then prep 2 + 2 adjoint
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
+def reference_cuda(W, L, T, P):
+    """The reference's own CUDA build (oracle/_ref/heliosk: the reference
+    sources compiled for sm_100a by oracle/Makefile) beside this library's
+    drop-in executable, on one run directory of this workload: K(x) seconds
+    as each writes it to Info_<name>.dat (the reference's includes its kernel
+    self-tuning when doTuning = 1, so both settings are run)."""
+    import shutil
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_run as R
+    if not os.path.exists(R.REF_EXE):
+        return {"unavailable": "oracle/_ref/heliosk not built (needs the reference sources)"}
+    base = tempfile.mkdtemp(prefix="hk_ref_")
+    out = {"lines": W["n"], "T": T, "P": P, "note": "K(x) of one state: line sum onto the grid"}
+    try:
+        data = os.path.join(base, "data")
+        R.write_data(data, L)
+        for tag, exe, tune in (("reference_tuned", R.REF_EXE, 1), ("reference_untuned", R.REF_EXE, 0),
+                               ("dropin", R.OUR_EXE, 1)):
+            d = os.path.join(base, tag)
+            R.write_run(d, data, T, P, W["numin"], W["numax"], W["dnu"], W["cut"], W["nbins"],
+                        W["nC"], store_k=0, resample=1, tuning=tune)
+            r = R.run(exe, d, timeout=900)
+            out[tag] = {"rc": r["rc"], "kx_s": r["info"].get("K(x)"), "lines_s": r["info"].get("Lines"),
+                        "input_s": r["info"].get("input"), "wall_s": r["wall_s"]}
+        ref = [out[t]["kx_s"] for t in ("reference_tuned", "reference_untuned")
+               if out[t]["rc"] == 0 and out[t]["kx_s"]]
+        if ref and out["dropin"]["rc"] == 0 and out["dropin"]["kx_s"]:
+            out["kx_speedup_vs_best_reference"] = min(ref) / out["dropin"]["kx_s"]
+    except Exception as e:  # a failed run is reported, not fatal
+        out["error"] = repr(e)[:300]
+    finally:
+        shutil.rmtree(base, ignore_errors=True)
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args)
         return
     ws, rank, lrank = dist_setup(args)
     import torch
@@ -428,6 +526,8 @@ def main():
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(W, L, float(T[0]), float(P[0]), args.cpu_seconds)
+    if rank == 0 and ws == 1 and ns == 1 and not args.no_reference_cuda:
+        out["reference_cuda"] = reference_cuda(W, L, float(T[0]), float(P[0]))
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
