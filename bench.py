@@ -190,7 +190,10 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(args):
+def dist_setup(args=None):
+    """One process per GPU (torchrun env); NCCL on GPUs, gloo without them
+    (HKB_DIST_BACKEND overrides).  States are independent, so the only
+    collective is the max of the per-rank times."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     lrank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -198,17 +201,22 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(lrank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = os.environ.get("HKB_DIST_BACKEND",
+                                 "nccl" if torch.cuda.is_available() else "gloo")
+        if backend == "nccl":
+            torch.cuda.set_device(lrank)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return ws, rank, lrank
 
 
 def barrier_max(ws, value):
+    """max over ranks of a per-rank time (the bench's only collective)."""
     if ws == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

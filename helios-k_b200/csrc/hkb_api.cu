@@ -72,6 +72,7 @@ struct hk_ctx {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   bool have_voigt_t = false, have_kdist_t = false;
   int64_t launches = 0;  // kernels launched since the last hk_opacity began
+  bool voigt_ms_acc_only = false;  // sectioned call: voigt_ms_acc is the whole time
   // T-P table recorded as one CUDA graph (hk_table_build / hk_table_run)
   cudaGraph_t table_graph = nullptr;
   cudaGraphExec_t table_exec = nullptr;
@@ -426,6 +427,89 @@ static hk_status check_ready(hk_ctx *c) {
   return HK_OK;
 }
 
+// States whose per-line records exceed the workspace (e.g. 5e8 ExoMol lines
+// at 112 B): a state pass over all lines fixes every state's cutoff bound and
+// FP32 scale, then each state's grid is cut into tile sections whose lines --
+// a contiguous range of the nu-sorted list -- fit the workspace, and each
+// section is prepared and summed on its own.  A tile sees the same lines in
+// the same order as in the batched path, so K is bit-identical to it.
+static hk_status opacity_sectioned(hk_ctx *c, int nstates, bool mixed, double *Kd, cudaStream_t s) {
+  const int64_t nx = c->g.nx, n = c->nlines;
+  const int G = voigt_tile_points();
+  const int tps = (int)((nx + G - 1) / G);
+  const size_t rec = line_prep_bytes(mixed);
+  const int64_t cap = (int64_t)(c->prep_budget / rec);
+  if (cap < 1) return fail(c, HK_ERR_NOMEM, "workspace budget below one line record");
+  CUDA_TRY(c, c->prep.ensure((size_t)std::min<int64_t>(cap, n) * rec));
+  StateDev *sd = c->states.as<StateDev>();
+  CUDA_TRY(c, launch_state_stats(c->L, c->g, sd, nstates, c->wbits.as<unsigned long long>(), s));
+  c->launches += 2;
+  std::vector<StateDev> hs(nstates);
+  CUDA_TRY(c, cudaMemcpyAsync(hs.data(), sd, nstates * sizeof(StateDev), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  CUDA_TRY(c, c->adjwork.ensure(4 * sizeof(double)));
+  double *q_d = c->adjwork.as<double>();
+  int64_t *lb_d = reinterpret_cast<int64_t *>(q_d + 2);
+  auto line_range = [&](int st, int t0, int t1, int64_t &L0, int64_t &L1) -> cudaError_t {
+    const double W = hs[st].wmax + hs[st].shift + 2.0 * c->g.dnu;
+    const double xlo = std::fma((double)t0 * G, c->g.dnu, c->g.numin) - W;
+    const double xhi = std::fma((double)(std::min<int64_t>((int64_t)t1 * G, nx) - 1), c->g.dnu, c->g.numin) + W;
+    const double pad = 1e-12 * (std::fabs(xlo) + std::fabs(xhi)) + 1e-300;
+    const double q[2] = {xlo - pad, xhi + pad};
+    int64_t lb[2];
+    cudaError_t e = cudaMemcpyAsync(q_d, q, sizeof q, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = launch_lower_bound(c->L.nu0, n, q_d, 2, lb_d, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(lb, lb_d, sizeof lb, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    L0 = lb[0];
+    L1 = lb[1];
+    return e;
+  };
+  for (int st = 0; st < nstates; ++st) {
+    struct Sec { int t0, t1; int64_t L0, L1; };
+    std::vector<Sec> secs;
+    std::vector<std::pair<int, int>> todo{{0, tps}};
+    while (!todo.empty()) {
+      const std::pair<int, int> tt = todo.back();
+      todo.pop_back();
+      int64_t L0 = 0, L1 = 0;
+      CUDA_TRY(c, line_range(st, tt.first, tt.second, L0, L1));
+      if (L1 - L0 <= cap) {
+        secs.push_back({tt.first, tt.second, L0, L1});
+      } else if (tt.second - tt.first == 1) {
+        return fail(c, HK_ERR_NOMEM, "one grid tile reaches %lld lines, above the workspace of %lld records",
+                    (long long)(L1 - L0), (long long)cap);
+      } else {
+        const int mid = (tt.first + tt.second) / 2;
+        todo.push_back({mid, tt.second});
+        todo.push_back({tt.first, mid});
+      }
+    }
+    for (const Sec &q : secs) {
+      const LinesDev Ls = lines_sub(c->L, q.L0, q.L1 - q.L0);
+      const VoigtPlan plan = plan_voigt_section(mixed, nx, q.t0, q.t1 - q.t0, 0);
+      if (plan.nsplit > 1) {
+        CUDA_TRY(c, c->vpart.ensure(plan.partial_doubles * sizeof(double)));
+        CUDA_TRY(c, c->vcnt.ensure(plan.counters * sizeof(unsigned)));
+      }
+      CUDA_TRY(c, launch_line_records(mixed, Ls, c->g, sd + st, c->prep.p, s));
+      CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
+      CUDA_TRY(c, launch_voigt_sum(mixed, plan, c->prep.p, Ls.nu0, Ls.n, c->g, sd + st,
+                                   c->ticket.as<unsigned>(), c->vpart.as<double>(),
+                                   c->vcnt.as<unsigned>(), Kd + (size_t)st * nx, nx, s));
+      CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
+      c->launches += 2;
+      float ms = 0.f;
+      CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
+      CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+      c->voigt_ms_acc += ms;
+    }
+  }
+  c->have_voigt_t = false;  // all Voigt time is in voigt_ms_acc
+  c->voigt_ms_acc_only = true;
+  return HK_OK;
+}
+
 hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, int precision,
                      double *K_out, int K_on_device, void *stream) {
   if (!c) return HK_ERR_ARG;
@@ -461,13 +545,19 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
     batch = std::min(batch, (int)std::max<size_t>(1, c->part_budget / part_per_state));
   }
   batch = std::min(batch, nstates);
-  CUDA_TRY(c, c->prep.ensure((size_t)batch * per_state));
-  StateDev *sd = c->states.as<StateDev>();
-  unsigned long long *wb = c->wbits.as<unsigned long long>();
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
+  c->voigt_ms_acc_only = false;
   c->launches = 0;
-  for (int b0 = 0; b0 < nstates; b0 += batch) {
+  if (per_state > c->prep_budget) {
+    if ((st = opacity_sectioned(c, nstates, mixed, Kd, s)) != HK_OK) return st;
+    batch = nstates;  // nothing left for the batched loop
+  } else {
+    CUDA_TRY(c, c->prep.ensure((size_t)batch * per_state));
+  }
+  StateDev *sd = c->states.as<StateDev>();
+  unsigned long long *wb = c->wbits.as<unsigned long long>();
+  for (int b0 = 0; per_state <= c->prep_budget && b0 < nstates; b0 += batch) {
     const int nb = std::min(batch, nstates - b0);
     const VoigtPlan plan = plan_voigt_sum(mixed, nx, nb, 0);
     c->launches += 3;  // line prep, state finalize, Voigt sum
@@ -635,6 +725,17 @@ hk_status hk_profile_eval(hk_ctx *c, int64_t n, const double *x, const double *y
 }
 
 // --------------------------------------------------------------- adjoint
+hk_status hk_set_workspace(hk_ctx *c, double prep_bytes, double part_bytes) {
+  if (!c) return HK_ERR_ARG;
+  if (!(prep_bytes >= 1.0) || !(part_bytes >= 1.0))
+    return fail(c, HK_ERR_ARG, "workspace budgets must be >= 1 byte");
+  c->prep_budget = (size_t)prep_bytes;
+  c->part_budget = (size_t)part_bytes;
+  table_release(c);
+  ok(c);
+  return HK_OK;
+}
+
 hk_status hk_set_line_scales(hk_ctx *c, const double *s_scale, const double *g_scale) {
   if (!c) return HK_ERR_ARG;
   if (c->nlines == 0 && (s_scale || g_scale)) return fail(c, HK_ERR_STATE, "no lines loaded");
@@ -683,6 +784,9 @@ hk_status hk_opacity_vjp(hk_ctx *c, double T, double P, int precision, const dou
   CUDA_TRY(c, c->states.ensure(sizeof(StateDev)));
   CUDA_TRY(c, c->wbits.ensure(2 * sizeof(unsigned long long)));
   CUDA_TRY(c, cudaMemcpyAsync(c->states.p, hs.data(), sizeof(StateDev), cudaMemcpyHostToDevice, s));
+  if ((size_t)n * sizeof(LinePrep) > c->prep_budget)
+    return fail(c, HK_ERR_RANGE, "the adjoint needs all %lld line records (%zu B) in the workspace (%zu B)",
+                (long long)n, (size_t)n * sizeof(LinePrep), c->prep_budget);
   CUDA_TRY(c, c->prep.ensure((size_t)std::max<int64_t>(n, 1) * sizeof(LinePrep)));
   // the plain per-line records (FP64 windows and constants) of this state
   CUDA_TRY(c, launch_line_prep(false, c->L, c->g, c->states.as<StateDev>(), 1, c->prep.p,
@@ -750,6 +854,9 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   const int64_t nx = c->g.nx;
   const bool mixed = precision == HK_PRECISION_MIXED;
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
+  if (per_state > c->prep_budget)
+    return fail(c, HK_ERR_UNSUPPORTED, "one state's line records (%zu B) exceed the workspace (%zu B): "
+                "tables of such lists run through hk_opacity's sectioned path", per_state, c->prep_budget);
   int batch = (int)std::max<size_t>(1, c->prep_budget / per_state);
   const int nsplit = voigt_nsplit(nx);
   if (nsplit > 1) {
@@ -832,13 +939,34 @@ int64_t hk_table_kernels(const hk_ctx *c) { return c ? c->table_kernels : 0; }
 
 int64_t hk_last_launches(const hk_ctx *c) { return c ? c->launches : 0; }
 
+hk_status hk_count_pairs(hk_ctx *c, double T, double P, int64_t *pairs3) {
+  if (!c || !pairs3) return HK_ERR_ARG;
+  hk_status st;
+  if ((st = check_ready(c)) != HK_OK) return st;
+  cudaSetDevice(c->device);
+  std::vector<StateDev> hs;
+  if ((st = build_states(c, 1, &T, &P, hs)) != HK_OK) return st;
+  CUDA_TRY(c, c->states.ensure(sizeof(StateDev)));
+  CUDA_TRY(c, c->adjwork.ensure(4 * sizeof(double)));
+  CUDA_TRY(c, cudaMemcpy(c->states.p, hs.data(), sizeof(StateDev), cudaMemcpyHostToDevice));
+  unsigned long long *d = reinterpret_cast<unsigned long long *>(c->adjwork.p);
+  CUDA_TRY(c, launch_count_pairs(c->L, c->g, c->states.as<StateDev>(), d, 0));
+  unsigned long long h[3];
+  CUDA_TRY(c, cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 3; ++k) pairs3[k] = (int64_t)h[k];
+  ok(c);
+  return HK_OK;
+}
+
 hk_status hk_last_timing(const hk_ctx *c, double *voigt_ms, double *kdist_ms) {
   if (!c) return HK_ERR_ARG;
   float ms = 0.f;
   if (voigt_ms) {
     *voigt_ms = -1.0;
-    if (c->have_voigt_t && cudaEventSynchronize(c->ev[1]) == cudaSuccess &&
-        cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]) == cudaSuccess)
+    if (c->voigt_ms_acc_only)
+      *voigt_ms = c->voigt_ms_acc;
+    else if (c->have_voigt_t && cudaEventSynchronize(c->ev[1]) == cudaSuccess &&
+             cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]) == cudaSuccess)
       *voigt_ms = c->voigt_ms_acc + ms;
   }
   if (kdist_ms) {

@@ -30,6 +30,35 @@ cudaError_t launch_opacity_vjp(bool mixed, const LinesDev &L, const GridDev &g,
 cudaError_t launch_line_prep(bool mixed, const LinesDev &L, const GridDev &g, StateDev *states_d,
                              int nstates, void *prep_d, unsigned long long *wbits_d,
                              cudaStream_t stream);
+// Sectioned states (a state's records larger than the workspace): the state
+// pass (cutoff bound, FP32 scale) over all lines, then one section's records
+// at a time; sections find their lines with launch_lower_bound on nu0.
+cudaError_t launch_state_stats(const LinesDev &L, const GridDev &g, StateDev *states_d,
+                               int nstates, unsigned long long *wbits_d, cudaStream_t stream);
+cudaError_t launch_line_records(bool mixed, const LinesDev &L, const GridDev &g,
+                                const StateDev *state_d, void *prep_d, cudaStream_t stream);
+cudaError_t launch_lower_bound(const double *a_d, int64_t n, const double *q_d, int m,
+                               int64_t *out_d, cudaStream_t stream);
+// lines [l0, l0 + n) of L as a list of their own
+inline LinesDev lines_sub(const LinesDev &L, int64_t l0, int64_t n) {
+  LinesDev s = L;
+  s.n = n;
+  auto off = [l0](const double *p) { return p ? p + l0 : p; };
+  s.nu0 = off(L.nu0);
+  s.Sfile = off(L.Sfile);
+  s.EL = off(L.EL);
+  s.gam = off(L.gam);
+  s.nexp = off(L.nexp);
+  s.delta = off(L.delta);
+  s.Aterm = off(L.Aterm);
+  s.sscale = off(L.sscale);
+  s.gscale = off(L.gscale);
+  s.iso = L.iso ? L.iso + l0 : nullptr;
+  return s;
+}
+
+cudaError_t launch_count_pairs(const LinesDev &L, const GridDev &g, const StateDev *state_d,
+                               unsigned long long *out_d, cudaStream_t stream);
 inline size_t line_prep_bytes(bool mixed) { return mixed ? sizeof(LinePrepF) : sizeof(LinePrep); }
 
 // Work plan of one Voigt launch: (state, tile) tickets, each tile's line
@@ -37,6 +66,7 @@ inline size_t line_prep_bytes(bool mixed) { return mixed ? sizeof(LinePrepF) : s
 // (parts are combined in part order through partial_doubles of scratch and
 // one counter per tile).
 struct VoigtPlan {
+  int tile0 = 0;  // first tile of the launch (a section of one state's grid)
   int tiles_per_state = 0;
   int64_t tiles = 0;
   int ctas = 0;
@@ -45,6 +75,8 @@ struct VoigtPlan {
   size_t counters = 0;
 };
 VoigtPlan plan_voigt_sum(bool mixed, int64_t nx, int nstates, int grid_ctas);
+// one state, tiles [tile0, tile0 + ntiles) of its grid
+VoigtPlan plan_voigt_section(bool mixed, int64_t nx, int tile0, int ntiles, int grid_ctas);
 int voigt_nsplit(int64_t nx);  // line-range parts per tile for a grid of nx points
 cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &plan, const void *prep_d,
                              const double *nu0_d, int64_t nlines, const GridDev &g,

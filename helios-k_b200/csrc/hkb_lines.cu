@@ -76,7 +76,12 @@ cudaError_t sort_lines_by_nu(int64_t n, double *nu_d, int64_t *order_d,
 // term, which sets the power-of-two scale of the mixed form's FP32 sums.
 // wbits holds two words per state: {half-width bits, term bits} (both
 // non-negative doubles, so their bit patterns order like the values).
-template <bool MIXED>
+// MODE: PREP_ALL writes the records and the per-state maxima; PREP_STATS only
+// the maxima (the state pass of a sectioned state); PREP_RECORDS only the
+// records (one section's lines, the state already finalised).
+enum { PREP_ALL = 0, PREP_STATS = 1, PREP_RECORDS = 2 };
+
+template <bool MIXED, int MODE>
 __global__ void __launch_bounds__(256)
 line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
                  void *__restrict__ out, unsigned long long *__restrict__ wbits) {
@@ -91,12 +96,13 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
     const double S1 = ls.S * ls.vy / CUDART_PI;
     const double Sc = ls.S * (1.0 / 1.7724538509055160273);
     const bool hasC = w[3] > w[2];
-    const double ey = hasC ? erfcx(ls.vy) : 1.0;
-    const float sig1 = hasC ? (float)c916_sig1(ls.vy) : 0.f;
     // largest region-A/B term of the line: S1 / r^2 with r^2 >= max(100, y^2)
     const double Y = ls.vy * ls.vy;
     const double term = S1 / fmax(100.0, Y);
-    if (MIXED) {
+    if (MODE == PREP_STATS) {
+    } else if (MIXED) {
+      const double ey = hasC ? erfcx(ls.vy) : 1.0;
+      const float sig1 = hasC ? (float)c916_sig1(ls.vy) : 0.f;
       LinePrepF r;
       r.nu = ls.nu;
       r.iad = ls.iad;
@@ -145,6 +151,8 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
       r.i1 = (int)w[5];
       reinterpret_cast<LinePrepF *>(out)[(int64_t)s * L.n + l] = r;
     } else {
+      const double ey = hasC ? erfcx(ls.vy) : 1.0;
+      const float sig1 = hasC ? (float)c916_sig1(ls.vy) : 0.f;
       LinePrep r;
       r.nu = ls.nu;
       r.iad = ls.iad;
@@ -168,6 +176,7 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
       else if (g.cutMode == 2) w_loc = fmax(w_loc, g.cut / ls.iad);
     }
   }
+  if (MODE == PREP_RECORDS) return;
   for (int o = 16; o > 0; o >>= 1) {
     w_loc = fmax(w_loc, __shfl_xor_sync(0xffffffffu, w_loc, o));
     s1_loc = fmax(s1_loc, __shfl_xor_sync(0xffffffffu, s1_loc, o));
@@ -200,6 +209,55 @@ __global__ void state_finalize_kernel(GridDev g, StateDev *__restrict__ states,
   states[s].s1exp = e;
 }
 
+// Exact (line, grid point) pair counts of one state by region, from the same
+// windows the sums use: A = (b0 - i0) + (i1 - b1), B = (c0 - b0) + (b1 - c1),
+// C = c1 - c0 (the algorithmic work of the Voigt sum).
+__global__ void __launch_bounds__(256)
+count_pairs_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ st,
+                   unsigned long long *__restrict__ out) {
+  __shared__ unsigned long long sa[8], sb[8], sc[8];
+  unsigned long long a = 0, b = 0, c = 0;
+  for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < L.n;
+       l += (int64_t)gridDim.x * blockDim.x) {
+    const LineState ls = prep_line(L, *st, l);
+    int64_t w[6];
+    line_windows(g, *st, ls, 0, g.nx, w);
+    a += (unsigned long long)((w[1] - w[0]) + (w[5] - w[4]));
+    b += (unsigned long long)((w[2] - w[1]) + (w[4] - w[3]));
+    c += (unsigned long long)(w[3] - w[2]);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sa[threadIdx.x >> 5] = a;
+    sb[threadIdx.x >> 5] = b;
+    sc[threadIdx.x >> 5] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < 8; ++w) {
+      a += sa[w];
+      b += sb[w];
+      c += sc[w];
+    }
+    atomicAdd(&out[0], a);
+    atomicAdd(&out[1], b);
+    atomicAdd(&out[2], c);
+  }
+}
+
+cudaError_t launch_count_pairs(const LinesDev &L, const GridDev &g, const StateDev *state_d,
+                               unsigned long long *out_d, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(out_d, 0, 3 * sizeof(unsigned long long), stream);
+  if (e != cudaSuccess || L.n == 0) return e;
+  const int64_t nb = (L.n + 255) / 256;
+  count_pairs_kernel<<<(unsigned)(nb < 4736 ? nb : 4736), 256, 0, stream>>>(L, g, state_d, out_d);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_line_prep(bool mixed, const LinesDev &L, const GridDev &g, StateDev *states_d,
                              int nstates, void *prep_d, unsigned long long *wbits_d,
                              cudaStream_t stream) {
@@ -210,13 +268,62 @@ cudaError_t launch_line_prep(bool mixed, const LinesDev &L, const GridDev &g, St
     const int bx = (int)(nb < 2368 ? nb : 2368);
     dim3 grid(bx, nstates);
     if (mixed)
-      line_prep_kernel<true><<<grid, 256, 0, stream>>>(L, g, states_d, prep_d, wbits_d);
+      line_prep_kernel<true, PREP_ALL><<<grid, 256, 0, stream>>>(L, g, states_d, prep_d, wbits_d);
     else
-      line_prep_kernel<false><<<grid, 256, 0, stream>>>(L, g, states_d, prep_d, wbits_d);
+      line_prep_kernel<false, PREP_ALL><<<grid, 256, 0, stream>>>(L, g, states_d, prep_d, wbits_d);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   state_finalize_kernel<<<(nstates + 127) / 128, 128, 0, stream>>>(g, states_d, nstates, wbits_d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_state_stats(const LinesDev &L, const GridDev &g, StateDev *states_d,
+                               int nstates, unsigned long long *wbits_d, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(wbits_d, 0, 2 * nstates * sizeof(unsigned long long), stream);
+  if (e != cudaSuccess) return e;
+  if (L.n > 0) {
+    const int64_t nb = (L.n + 255) / 256;
+    dim3 grid((unsigned)(nb < 2368 ? nb : 2368), nstates);
+    line_prep_kernel<true, PREP_STATS><<<grid, 256, 0, stream>>>(L, g, states_d, nullptr, wbits_d);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  state_finalize_kernel<<<(nstates + 127) / 128, 128, 0, stream>>>(g, states_d, nstates, wbits_d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_line_records(bool mixed, const LinesDev &L, const GridDev &g,
+                                const StateDev *state_d, void *prep_d, cudaStream_t stream) {
+  if (L.n == 0) return cudaSuccess;
+  const int64_t nb = (L.n + 255) / 256;
+  dim3 grid((unsigned)(nb < 2368 ? nb : 2368), 1);
+  if (mixed)
+    line_prep_kernel<true, PREP_RECORDS><<<grid, 256, 0, stream>>>(L, g, state_d, prep_d, nullptr);
+  else
+    line_prep_kernel<false, PREP_RECORDS><<<grid, 256, 0, stream>>>(L, g, state_d, prep_d, nullptr);
+  return cudaGetLastError();
+}
+
+// first index of each query value in the ascending array a (lower bound)
+__global__ void lower_bound_kernel(const double *__restrict__ a, int64_t n,
+                                   const double *__restrict__ q, int m, int64_t *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const double v = q[i];
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    if (a[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  out[i] = lo;
+}
+
+cudaError_t launch_lower_bound(const double *a_d, int64_t n, const double *q_d, int m,
+                               int64_t *out_d, cudaStream_t stream) {
+  if (m <= 0) return cudaSuccess;
+  lower_bound_kernel<<<(m + 127) / 128, 128, 0, stream>>>(a_d, n, q_d, m, out_d);
   return cudaGetLastError();
 }
 

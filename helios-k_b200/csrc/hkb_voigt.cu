@@ -524,7 +524,7 @@ template <bool MIXED>
 __global__ void __launch_bounds__(HK_THREADS, MIXED ? 4 : 2)
 voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
                  int64_t nlines, GridDev g, const StateDev *__restrict__ states,
-                 int tiles_per_state, int nsplit, int total_tickets,
+                 int tile0, int tiles_per_state, int nsplit, int total_tickets,
                  unsigned *__restrict__ ticket, double *__restrict__ partial,
                  unsigned *__restrict__ tile_cnt, double *__restrict__ K, int64_t k_stride) {
   using Rec = typename std::conditional<MIXED, RecF, RecD>::type;
@@ -554,7 +554,7 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
     const StateDev &st = states[s];
     const LinePrep *P = reinterpret_cast<const LinePrep *>(prep) + (int64_t)s * nlines;
     const LinePrepF *PF = reinterpret_cast<const LinePrepF *>(prep) + (int64_t)s * nlines;
-    const int64_t g0 = (int64_t)tile * HK_G;
+    const int64_t g0 = (int64_t)(tile0 + tile) * HK_G;
     const int64_t g1 = min(g0 + (int64_t)HK_G, g.nx);
     if (warp == 0) {
       const double W = st.wmax + st.shift + 2.0 * g.dnu;
@@ -845,6 +845,18 @@ int voigt_nsplit(int64_t nx) {
                                 std::max<int64_t>(1, (HK_TICKETS_PER_STATE + tps - 1) / tps));
 }
 
+VoigtPlan plan_voigt_section(bool mixed, int64_t nx, int tile0, int ntiles, int grid_ctas) {
+  VoigtPlan pl;
+  pl.tile0 = tile0;
+  pl.tiles_per_state = ntiles;
+  pl.tiles = ntiles;
+  pl.ctas = grid_ctas > 0 ? grid_ctas : voigt_ctas(mixed);
+  pl.nsplit = voigt_nsplit(nx);
+  pl.partial_doubles = pl.nsplit > 1 ? (size_t)pl.tiles * pl.nsplit * HK_G : 0;
+  pl.counters = pl.nsplit > 1 ? (size_t)pl.tiles : 0;
+  return pl;
+}
+
 VoigtPlan plan_voigt_sum(bool mixed, int64_t nx, int nstates, int grid_ctas) {
   VoigtPlan pl;
   pl.tiles_per_state = (int)((nx + HK_G - 1) / HK_G);
@@ -876,11 +888,11 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d
   const int ctas = (int)std::min<int64_t>(pl.ctas, total);
   if (mixed)
     voigt_sum_kernel<true><<<ctas, HK_THREADS, smem, stream>>>(
-        prep_d, nu0_d, nlines, g, states_d, pl.tiles_per_state, pl.nsplit, total, ticket_d,
+        prep_d, nu0_d, nlines, g, states_d, pl.tile0, pl.tiles_per_state, pl.nsplit, total, ticket_d,
         partial_d, tile_cnt_d, K_d, k_stride);
   else
     voigt_sum_kernel<false><<<ctas, HK_THREADS, smem, stream>>>(
-        prep_d, nu0_d, nlines, g, states_d, pl.tiles_per_state, pl.nsplit, total, ticket_d,
+        prep_d, nu0_d, nlines, g, states_d, pl.tile0, pl.tiles_per_state, pl.nsplit, total, ticket_d,
         partial_d, tile_cnt_d, K_d, k_stride);
   return cudaGetLastError();
 }

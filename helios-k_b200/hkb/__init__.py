@@ -74,12 +74,14 @@ def lib():
             "hk_kdist_noalloc": (_i, [_p, _i, _i64, _i, _i, _d, _d, _p, _p, _p, _p,
                                       C.c_char_p, _i]),
             "hk_set_line_scales": (_i, [_p, _p, _p]),
+            "hk_set_workspace": (_i, [_p, _d, _d]),
             "hk_opacity_vjp": (_i, [_p, _d, _d, _i, _p, _i, _p, _p, _p, _p, _i, _p]),
             "hk_table_build": (_i, [_p, _i, _p, _p, _i, _p, _i, _d, _p, _p]),
             "hk_table_run": (_i, [_p, _p]),
             "hk_table_free": (_i, [_p]),
             "hk_table_kernels": (_i64, [_p]),
             "hk_last_launches": (_i64, [_p]),
+            "hk_count_pairs": (_i, [_p, _d, _d, _p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -239,6 +241,10 @@ class Context:
                                  _ptr(res["recon"]), int(outputs_on_device), sh))
         return res
 
+    def set_workspace(self, prep_bytes=24 * 2**30, part_bytes=4 * 2**30):
+        """Workspace budgets; states above the first run in grid sections."""
+        self._chk(lib().hk_set_workspace(self._h, float(prep_bytes), float(part_bytes)))
+
     # --------------------------------------------------------- adjoint
     def set_line_scales(self, s_scale=None, g_scale=None):
         """Per-line multipliers of strength and Lorentz width (load order)."""
@@ -288,6 +294,12 @@ class Context:
     @property
     def table_kernels(self):
         return int(lib().hk_table_kernels(self._h))
+
+    def count_pairs(self, T, P):
+        """(A, B, C) pairs of one state inside the cutoff windows."""
+        out = np.zeros(3, np.int64)
+        self._chk(lib().hk_count_pairs(self._h, float(T), float(P), _ptr(out)))
+        return tuple(int(v) for v in out)
 
     @property
     def last_launches(self):

@@ -166,6 +166,11 @@ hk_status hk_kdist_noalloc(const double *K, int nstates, int64_t nx, int nbins, 
                            double kmin, double unitScale, double *coeff, int32_t *nxmin,
                            double *sortedK, void *stream, char *errbuf, int errbuf_len);
 
+/* Device workspace budgets (bytes): per-(state, line) records of one batch
+ * (default 24 GiB) and split-tile partial sums (default 4 GiB).  States whose
+ * records exceed the first run in grid sections (bit-identical K). */
+hk_status hk_set_workspace(hk_ctx *ctx, double prep_bytes, double part_bytes);
+
 /* ----------------------------------------------------------- adjoint */
 
 /* Optional per-line multipliers, in load order (host arrays of
@@ -217,6 +222,11 @@ int64_t hk_table_kernels(const hk_ctx *ctx);
 
 /* kernels launched by the last hk_opacity and the hk_kdist calls after it */
 int64_t hk_last_launches(const hk_ctx *ctx);
+
+/* (line, grid point) pairs of one state inside the cutoff windows, by
+ * region: pairs3 = {A, B, C} (the algorithmic work of the Voigt sum, from the
+ * same windows the sum uses). */
+hk_status hk_count_pairs(hk_ctx *ctx, double T, double P, int64_t *pairs3);
 
 
 /* Per-line state (nu, S, 1/alphaD, gammaL/alphaD) and the six window

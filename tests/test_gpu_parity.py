@@ -300,3 +300,25 @@ def test_table_graph_equals_opacity_and_kdist(small):
     assert np.array_equal(K1, Kr)
     assert np.array_equal(c1, fit["coeff"])
     assert np.array_equal(n1, fit["nxmin"])
+
+
+def test_sectioned_states_equal_batched(small):
+    """A workspace too small for one state's line records runs each state in
+    grid sections (the path of 5e8-line lists); K is bit-identical."""
+    ctx = small["ctx"]
+    ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+    Ts = np.array([1500.0, 300.0])
+    Ps = np.array([0.1, 10.0])
+    ref = {pr: ctx.opacity(Ts, Ps, pr) for pr in (hkb.MIXED, hkb.PLAIN_FP64)}
+    assert ctx.count_pairs(1500.0, 0.1) == tuple(
+        int(v) for v in (lambda w: ((w[:, 1] - w[:, 0]).sum() + (w[:, 5] - w[:, 4]).sum(),
+                                    (w[:, 2] - w[:, 1]).sum() + (w[:, 4] - w[:, 3]).sum(),
+                                    (w[:, 3] - w[:, 2]).sum()))(ctx.state_lines(1500.0, 0.1)[4]))
+    try:
+        ctx.set_workspace(prep_bytes=3000 * 112, part_bytes=4 * 2**30)
+        for pr in (hkb.MIXED, hkb.PLAIN_FP64):
+            K = ctx.opacity(Ts, Ps, pr)
+            assert np.array_equal(K, ref[pr])
+        assert ctx.last_launches > 6  # state pass + several sections per state
+    finally:
+        ctx.set_workspace()
