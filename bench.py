@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hitemp",
-                    choices=["hitemp", "small", "table", "hitemp_sparse", "adjoint"])
+                    choices=["hitemp", "small", "table", "hitemp_sparse", "adjoint", "exomol"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -65,6 +65,11 @@ def workload(name):
         T, P = synth.table_states()
         W["T"], W["P"] = list(T), list(P)
         W["label"] = "tp-table-1e7-lines-600-states"
+    elif name == "exomol":
+        W = dict(synth.WORKLOADS["exomol"])
+        T, P = synth.exomol_states()
+        W["T"], W["P"] = list(T), list(P)
+        W["label"] = "exomol-5e8-lines-4x4-states"
     else:
         W = dict(synth.WORKLOADS[name])
         W["label"] = {"hitemp": "hitemp-1e7-lines-single-state",
@@ -76,6 +81,9 @@ def workload(name):
 
 def make_lines(W):
     from hkb import synth
+    if W.get("database") == "exomol":
+        return synth.exomol_lines(W["n"], seed=W["seed"], logS=W["logS"], nu_max=W["nu_max"],
+                                  E_mean=W["E_mean"])
     return synth.hitran_lines(W["n"], seed=W["seed"], logS=W["logS"],
                               nu_min=W.get("nu_min", 0.0), nu_max=W.get("nu_max", 30000.0))
 
@@ -84,30 +92,31 @@ def open_ctx(W, L, device):
     import hkb
     from hkb import synth
     ctx = hkb.Context(device)
-    ctx.set_species(hkb.HITRAN, [synth.MASS], [1.0])
     Tq, Qq = synth.q_table()
-    ctx.set_partition(0, Tq, Qq)
-    ctx.set_options(qalphaL=1.0)
-    ctx.load_lines_hitran(L)
+    if W.get("database") == "exomol":
+        ctx.set_species(hkb.EXOMOL, [synth.MASS], [1.0], W["defaultL"], W["defaultn"])
+        ctx.set_partition(0, Tq, Qq)
+        ctx.load_lines_exomol(L)
+    else:
+        ctx.set_species(hkb.HITRAN, [synth.MASS], [1.0])
+        ctx.set_partition(0, Tq, Qq)
+        ctx.set_options(qalphaL=1.0)
+        ctx.load_lines_hitran(L)
     ctx.set_grid(W["numin"], W["numax"], W["dnu"], W["nbins"], 0, W["cut"])
     return ctx
 
 
 def count_pairs(ctx, T, P):
     """Exact (A, B, C) pair counts of one state from the device index windows."""
-    _, _, _, vy, win = ctx.state_lines(T, P)
-    i0, b0, c0, c1, b1, i1 = (win[:, k] for k in range(6))
-    pa = int(np.sum(b0 - i0) + np.sum(i1 - b1))
-    pb = int(np.sum(c0 - b0) + np.sum(b1 - c1))
-    pc = int(np.sum(c1 - c0))
-    return pa, pb, pc, win, vy
+    return ctx.count_pairs(T, P)
 
 
-def c_series_iterations(ctx, T, P, win, vy, sample=1000, seed=0):
-    """Mean Algorithm-916 series length of the FP32 form over region-C pairs,
-    replaying its stopping rule (|delta s| < TOLF for s1, s2, s3) in numpy."""
+def c_series_iterations(ctx, T, P, sample=1000, seed=0):
+    """Mean Algorithm-916 series length of the reference's FP32 form over
+    region-C pairs (the n_iter of the flop model), replaying its stopping rule
+    (|delta s| < TOLF for s1, s2, s3) in numpy on a sample of lines."""
     rng = np.random.default_rng(seed)
-    nu, S, iad, _, _ = ctx.state_lines(T, P)
+    nu, S, iad, vy, win = ctx.state_lines(T, P)
     has = np.nonzero(win[:, 3] > win[:, 2])[0]
     if len(has) == 0:
         return 0.0
@@ -229,7 +238,16 @@ def cpu_baseline(W, L, T, P, seconds, tile=2048, seed=0):
     from hkb import synth
     Tq, Qq = synth.q_table()
     Q = oracle.partition(Tq, Qq, T)
-    nu, S, iad, vy = oracle.prep_hitran(L, [synth.MASS], [1.0], [Q], T, P, qalphaL=1.0)
+    head = ""
+    if W["n"] > 20_000_000:
+        # per-line oracle arrays of a 5e8-line list do not fit the host: the
+        # rate is measured on a 2e7-line head of the list (same distributions)
+        L = {k: v[:20_000_000] for k, v in L.items()}
+        head = ", 2e7-line head of the list"
+    if W.get("database") == "exomol":
+        nu, S, iad, vy = oracle.prep_exomol(L, synth.MASS, 1.0, Q, W["defaultL"], W["defaultn"], T, P)
+    else:
+        nu, S, iad, vy = oracle.prep_hitran(L, [synth.MASS], [1.0], [Q], T, P, qalphaL=1.0)
     nx = oracle.grid_nx(W["numin"], W["numax"], W["dnu"])
     win = oracle.windows(nu, S, iad, vy, W["numin"], W["dnu"], nx, 0, W["cut"])
     rng = np.random.default_rng(seed)
@@ -248,7 +266,7 @@ def cpu_baseline(W, L, T, P, seconds, tile=2048, seed=0):
     cores = os.cpu_count() or 1
     return {"value": pairs / tsum, "unit": "Voigt evals/s", "cores": cores, "kind": "port",
             "sample": f"{used} random {tile}-point grid tiles of {ntiles} "
-                      f"({pairs:.3e} pairs, {tsum:.1f} s), FP64 oracle, OpenMP {cores} threads"}
+                      f"({pairs:.3e} pairs, {tsum:.1f} s){head}, FP64 oracle, OpenMP {cores} threads"}
 
 
 def run_reference(args):
@@ -295,7 +313,7 @@ def run_adjoint(args):
     T, P = W["T"][0], W["P"][0]
     prec = hkb.MIXED if args.precision == "mixed" else hkb.PLAIN_FP64
     nx, n = ctx.nx, ctx.num_lines
-    pa, pb, pc, _, _ = count_pairs(ctx, T, P)
+    pa, pb, pc = count_pairs(ctx, T, P)
     pairs = pa + pb + pc
     w = torch.as_tensor(np.random.default_rng(7).standard_normal(nx), device="cuda")
     K = torch.empty((1, nx), dtype=torch.float64, device="cuda")
@@ -395,14 +413,22 @@ def main():
     prec = hkb.MIXED if args.precision == "mixed" else hkb.PLAIN_FP64
 
     # exact algorithmic work (outside the timed region)
-    per_state = []
-    probe = range(ns) if ns <= 8 else np.linspace(0, ns - 1, 8).astype(int)
-    for s in probe:
-        pa, pb, pc, win, vy = count_pairs(ctx, float(T[s]), float(P[s]))
-        per_state.append((pa, pb, pc))
+    per_state = [count_pairs(ctx, float(T[s]), float(P[s])) for s in range(ns)]
     pa, pb, pc = (float(np.mean([p[k] for p in per_state])) for k in range(3))
-    pairs_step = (pa + pb + pc) * ns  # cutMode 0, no shift: same window per state
-    n_iter = c_series_iterations(ctx, float(T[0]), float(P[0]), win, vy) if pc > 0 else 0.0
+    pairs_step = (pa + pb + pc) * ns
+    # n_iter of the flop model, from the lines themselves or, for lists too
+    # large to download per line, from a 2e6-line head of the same list
+    if pc > 0 and ctx.num_lines <= 20_000_000:
+        n_iter = c_series_iterations(ctx, float(T[0]), float(P[0]))
+    elif pc > 0:
+        Wp = dict(W, n=2_000_000)
+        Lp = {k: v[:2_000_000] for k, v in L.items()}
+        pctx = open_ctx(Wp, Lp, lrank)
+        pctx._numin, pctx._dnu = W["numin"], W["dnu"]
+        n_iter = c_series_iterations(pctx, float(T[0]), float(P[0]))
+        pctx.close()
+    else:
+        n_iter = 0.0
     flops_step = ns * (pa * (F_A + F_ACC) + pb * (F_B + F_ACC) + pc * (F_C0 + F_C_ITER * n_iter + F_ACC))
 
     stream = torch.cuda.current_stream()
@@ -415,12 +441,28 @@ def main():
         ctx.kdist(K, nC=nC, stream=stream)
 
     # one step = the whole batch of states (line prep, Voigt sums, fits)
-    # replayed as one CUDA graph (hk_table_build / hk_table_run)
-    ctx.table_build(T, P, K, coeff, nxmin, nC=nC, precision=prec)
-    launches_per_step = ctx.table_kernels
+    # replayed as one CUDA graph (hk_table_build / hk_table_run); line lists
+    # whose per-state records exceed the workspace run the sectioned path of
+    # hk_opacity instead (not capturable: it sizes sections from the state
+    # pass)
+    try:
+        ctx.table_build(T, P, K, coeff, nxmin, nC=nC, precision=prec)
+        graph = True
+    except hkb.HkError as err:
+        if err.status != -8:  # HK_ERR_UNSUPPORTED
+            raise
+        graph = False
+
+    def timed_step():
+        if graph:
+            ctx.table_run(stream)
+        else:
+            step(prec)
+
     for _ in range(args.warmup):
-        ctx.table_run(stream)
+        timed_step()
     torch.cuda.synchronize()
+    launches_per_step = ctx.table_kernels if graph else ctx.last_launches
     if ws > 1:
         torch.distributed.barrier()
     clk = Clocks(lrank)
@@ -430,13 +472,14 @@ def main():
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.steps):
-        ctx.table_run(stream)
+        timed_step()
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     clocks = clk.stop()
     ms = barrier_max(ws, ms)
-    ctx.table_free()
+    if graph:
+        ctx.table_free()
 
     # dominant kernel: per-launch device time with CUDA events on the stream
     vms, kms = [], []
@@ -480,9 +523,11 @@ def main():
         plain = {"ms_per_step": pms, "value": pairs_step * ws / (pms * 1e-3),
                  "speedup_mixed_vs_plain": pms / ms}
     elif not args.no_plain and args.precision == "mixed":
-        # a table's plain FP64 run takes minutes: both forms on the same 20
-        # states spread over the table (opacity + fit), 1 untimed + 1 timed
-        sub = np.linspace(0, ns - 1, min(ns, 20)).astype(int)
+        # a table's plain FP64 run takes minutes: both forms on the same
+        # states spread over the table (20 of a T-P table, 1 of a 5e8-line
+        # list), opacity + fit, 1 untimed + 1 timed
+        nsub = 1 if W.get("database") == "exomol" else 20
+        sub = np.linspace(0, ns - 1, min(ns, nsub)).astype(int)
         Ks = K[:len(sub)]
 
         def sub_ms(pr):
@@ -509,11 +554,13 @@ def main():
         "dtype": "f32 profile, f64 offsets/strengths/sum/fit" if prec == hkb.MIXED else "f64",
         "data": "synthetic (seeded; BASELINE config distributions)",
         "config": {"workload": W["label"], "lines": W["n"], "grid_points": nx, "states": ns,
-                   "T": W["T"][0] if ns == 1 else "100-3000 K x 20",
-                   "P": W["P"][0] if ns == 1 else "1e-8-1e3 atm x 30",
+                   "T": W["T"][0] if ns == 1 else f"{min(W['T']):g}-{max(W['T']):g} K x {len(set(W['T']))}",
+                   "P": W["P"][0] if ns == 1 else f"{min(W['P']):.3g}-{max(W['P']):.3g} atm x {len(set(W['P']))}",
                    "cut_cm-1": W["cut"], "nbins": nb, "nC": nC,
                    "precision": args.precision, "parallelism": f"states x{ws} ranks",
-                   "l2": "inputs larger than L2 (line list ~480 MB resident), no flush"},
+                   "format": W.get("database", "hitran"),
+                   "execution": "one CUDA graph per step" if graph else "hk_opacity sections + hk_kdist",
+                   "l2": f"inputs larger than L2 (line columns ~{W['n'] * 48 / 1e9:.2g} GB resident), no flush"},
         "s_per_state": ms * 1e-3 / ns,
         "s_per_table": ms * 1e-3 if ns > 1 else None,
         "pairs_per_state": {"A": pa, "B": pb, "C": pc, "C_series_iters": n_iter},

@@ -55,13 +55,20 @@ def hitran_lines(n, seed=0, logS=(-30.0, -18.0), nu_max=30000.0, E_mean=3000.0,
 
 
 def exomol_lines(n, seed=4, logS=(-40.0, -18.0), nu_max=40000.0, E_mean=8000.0,
-                 chunk=None):
-    """ExoMol-format dict (nu, S_file, EL, A); widths come from the defaults."""
+                 chunk=1 << 24):
+    """ExoMol-format dict (nu, S_file, EL, A) drawn in chunks of `chunk` lines
+    (bounded host temporaries for 5e8-line lists); widths come from the
+    species defaults."""
     rng = np.random.default_rng(seed)
-    nu = rng.uniform(0.0, nu_max, n)
-    S296 = 10.0 ** rng.uniform(logS[0], logS[1], n)
-    EL = rng.exponential(E_mean, n)
-    S_file = S296 * float(q_of_T(296.0)) / (MASS / NA)
+    nu = np.empty(n)
+    S_file = np.empty(n)
+    EL = np.empty(n)
+    f = float(q_of_T(296.0)) / (MASS / NA)
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        nu[a:b] = rng.uniform(0.0, nu_max, b - a)
+        S_file[a:b] = 10.0 ** rng.uniform(logS[0], logS[1], b - a) * f
+        EL[a:b] = rng.exponential(E_mean, b - a)
     return dict(nu=nu, S=S_file, EL=EL, A=np.zeros(n))
 
 
@@ -75,6 +82,10 @@ WORKLOADS = {
     # the hitemp line distribution at 1/10 of the line density over the same
     # grid (used for profiler captures: same tiles and per-pair mix, 1/10 of
     # the work, ~150 MB on the device)
+    # 5e8 ExoMol-format lines (~12 GB of line columns in HBM), 4 x 4 states
+    "exomol": dict(n=500_000_000, seed=4, logS=(-40.0, -18.0), numin=0.0, numax=40000.0,
+                   dnu=0.01, cut=25.0, nbins=400, nC=20, database="exomol", defaultL=0.07,
+                   defaultn=0.5, nu_max=40000.0, E_mean=8000.0),
     "hitemp_sparse": dict(n=1_000_000, seed=1, logS=(-32.0, -18.0), T=[1500.0], P=[0.1],
                           numin=0.0, numax=30000.0, dnu=0.01, cut=25.0, nbins=300, nC=20),
 }
