@@ -356,12 +356,13 @@ def run_adjoint(args):
     ctx.close()
 
 
-def reference_cuda(W, L, T, P):
+def reference_cuda(W, L, T, P, tunings=(1, 0)):
     """The reference's own CUDA build (oracle/_ref/heliosk: the reference
     sources compiled for sm_100a by oracle/Makefile) beside this library's
     drop-in executable, on one run directory of this workload: K(x) seconds
     as each writes it to Info_<name>.dat (the reference's includes its kernel
-    self-tuning when doTuning = 1, so both settings are run)."""
+    self-tuning when doTuning = 1, so both settings are run).  P may be a list
+    (one process over a PFile of pressures, as the reference runs tables)."""
     import shutil
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_run as R
@@ -372,8 +373,8 @@ def reference_cuda(W, L, T, P):
     try:
         data = os.path.join(base, "data")
         R.write_data(data, L)
-        for tag, exe, tune in (("reference_tuned", R.REF_EXE, 1), ("reference_untuned", R.REF_EXE, 0),
-                               ("dropin", R.OUR_EXE, 1)):
+        runs = [("reference_tuned" if t else "reference_untuned", R.REF_EXE, t) for t in tunings]
+        for tag, exe, tune in runs + [("dropin", R.OUR_EXE, 1)]:
             d = os.path.join(base, tag)
             R.write_run(d, data, T, P, W["numin"], W["numax"], W["dnu"], W["cut"], W["nbins"],
                         W["nC"], store_k=0, resample=1, tuning=tune)
@@ -381,7 +382,7 @@ def reference_cuda(W, L, T, P):
             out[tag] = {"rc": r["rc"], "kx_s": r["info"].get("K(x)"), "lines_s": r["info"].get("Lines"),
                         "input_s": r["info"].get("input"), "wall_s": r["wall_s"]}
         ref = [out[t]["kx_s"] for t in ("reference_tuned", "reference_untuned")
-               if out[t]["rc"] == 0 and out[t]["kx_s"]]
+               if t in out and out[t]["rc"] == 0 and out[t]["kx_s"]]
         if ref and out["dropin"]["rc"] == 0 and out["dropin"]["kx_s"]:
             out["kx_speedup_vs_best_reference"] = min(ref) / out["dropin"]["kx_s"]
     except Exception as e:  # a failed run is reported, not fatal
@@ -583,6 +584,18 @@ def main():
         out["cpu_baseline"] = cpu_baseline(W, L, float(T[0]), float(P[0]), args.cpu_seconds)
     if rank == 0 and ws == 1 and ns == 1 and not args.no_reference_cuda:
         out["reference_cuda"] = reference_cuda(W, L, float(T[0]), float(P[0]))
+    elif rank == 0 and ws == 1 and args.workload == "table" and not args.no_reference_cuda:
+        # the reference runs a table as one process per T over a PFile of the
+        # 30 pressures: the middle temperature is run, x20 extrapolates
+        Tm = sorted(set(W["T"]))[len(set(W["T"])) // 2]
+        Pt = [p for t, p in zip(W["T"], W["P"]) if t == Tm]
+        rc = reference_cuda(W, L, Tm, Pt, tunings=(1,))
+        nT = len(set(W["T"]))
+        rc["table_extrapolation"] = f"one T ({Tm:.6g} K) x {len(Pt)} P run; x{nT} for the table"
+        for t in ("reference_tuned", "dropin"):
+            if t in rc and rc[t].get("kx_s"):
+                rc[t]["kx_s_table_est"] = rc[t]["kx_s"] * nT
+        out["reference_cuda"] = rc
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()

@@ -39,10 +39,17 @@ def write_data(data_dir, lines, species="syn"):
 
 def write_run(d, data_dir, T, P, numin, numax, dnu, cut, nbins, nC, name="syn", species="syn",
               store_k=2, resample=1, tuning=1):
-    """param.dat for one (T, P) in run directory d, reading data_dir."""
+    """param.dat for one T and one P (or, P a list, a PFile of pressures) in
+    run directory d, reading data_dir."""
     from hkb import synth
     os.makedirs(d, exist_ok=True)
-    synth.write_param(os.path.join(d, "param.dat"), name=name, T=T, P=P,
+    pfile = "-"
+    if np.ndim(P) > 0:
+        pfile = os.path.join(d, "P.dat")
+        with open(pfile, "w") as f:
+            f.write("\n".join("%.17g" % v for v in P) + "\n")
+        P = float(P[0])
+    synth.write_param(os.path.join(d, "param.dat"), name=name, T=T, P=P, PFile=pfile,
                       Species_Name=species, pathToData=data_dir.rstrip("/") + "/", numin=numin,
                       numax=numax, dnu=dnu, cut=cut, nbins=nbins, nC=nC,
                       doResampling=resample, doStoreFullK=store_k, doTuning=tuning)
