@@ -8,10 +8,13 @@
 // spacing, sub-Lorentzian, plinth removal, profiles 2-4, transmission and
 // means) are rejected with a message instead of being silently ignored.
 // Unlike the reference (heliosk.cu:365-367) a failed run exits with status 1.
+#include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -21,6 +24,31 @@
 #include "hkb_types.h"
 
 using namespace hkb;
+
+// Text lines [0, n) formatted by fmt(i, buf, cap) -> length, written to f
+// in order.  The formatting (printf %.20g of doubles, the bulk of a
+// multi-million-line K file) runs on all host threads in blocks; the bytes
+// are those a single fprintf loop writes.
+template <class Fmt>
+static void write_lines(FILE *f, int64_t n, Fmt fmt) {
+  const int64_t block = 1 << 16;
+  const int nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  std::vector<std::string> out(nt);
+  for (int64_t b0 = 0; b0 < n; b0 += block * nt) {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t) {
+      th.emplace_back([&, t] {
+        std::string &o = out[t];
+        o.clear();
+        const int64_t a = b0 + t * block, e = std::min(n, a + block);
+        char buf[256];
+        for (int64_t i = a; i < e; ++i) o.append(buf, (size_t)fmt(i, buf, sizeof buf));
+      });
+    }
+    for (auto &x : th) x.join();
+    for (int t = 0; t < nt; ++t) fwrite(out[t].data(), 1, out[t].size(), f);
+  }
+}
 
 static int die(const std::string &m) {
   printf("%s\n", m.c_str());
@@ -142,14 +170,16 @@ int main(int argc, char **argv) {
   }
 
   // full K output, heliosk.cu:1840-1935
+  const auto tw0 = std::chrono::steady_clock::now();
   if (p.doStoreFullK == 1) {
     FILE *f = fopen(("Out_" + p.name + ".dat").c_str(), mode);
     for (int iP = 0; iP < nP; ++iP) {
       const double *Kp = K.data() + (size_t)iP * nx;
-      for (int64_t j = 0; j < nx; ++j) {
-        if (nP == 1) fprintf(f, "%.20g %.20g\n", x[j], Kp[j] * unitScale);
-        else fprintf(f, "%.20g %.20g %.20g %.20g\n", x[j], Kp[j] * unitScale, p.T, p.Plist[iP]);
-      }
+      const double Pv = p.Plist[iP];
+      write_lines(f, nx, [&](int64_t j, char *buf, size_t cap) {
+        if (nP == 1) return snprintf(buf, cap, "%.20g %.20g\n", x[j], Kp[j] * unitScale);
+        return snprintf(buf, cap, "%.20g %.20g %.20g %.20g\n", x[j], Kp[j] * unitScale, p.T, Pv);
+      });
       fprintf(f, "\n\n");
     }
     fclose(f);
@@ -161,6 +191,8 @@ int main(int argc, char **argv) {
     }
     fclose(f);
   }
+
+  const double t_write = std::chrono::duration<double>(std::chrono::steady_clock::now() - tw0).count();
 
   // sort + resampling, heliosk.cu:2046-2193
   const int nxb = (int)(nx / p.nbins);
@@ -231,11 +263,12 @@ int main(int argc, char **argv) {
           f = fopen(fn, "a");
         }
         const double *Kp = Kb.data() + (size_t)iP * nx + (size_t)i * nxb;
-        for (int j = 0; j < nxb; ++j) {
+        const double Pv = p.Plist[iP];
+        write_lines(f, nxb, [&](int64_t j, char *buf, size_t cap) {
           const double y = j / ((double)(nxb - 1));
-          if (nP == 1) fprintf(f, "%g %.20g\n", y, Kp[j] * unitScale);
-          else fprintf(f, "%g %.20g %g %g %d\n", y, Kp[j] * unitScale, p.T, p.Plist[iP], j);
-        }
+          if (nP == 1) return snprintf(buf, cap, "%g %.20g\n", y, Kp[j] * unitScale);
+          return snprintf(buf, cap, "%g %.20g %g %g %d\n", y, Kp[j] * unitScale, p.T, Pv, (int)j);
+        });
         if (p.doStoreK == 1) fprintf(f, "\n\n");
         if (p.doStoreK == 2) {
           fclose(f);
@@ -250,6 +283,7 @@ int main(int argc, char **argv) {
     fprintf(f, "Time for input:        %g seconds\n", t_input);
     fprintf(f, "Time for Lines:        %g seconds\n", t_lines);
     fprintf(f, "Time for K(x):         %g seconds\n", t_K);
+    fprintf(f, "Time for write K(x):   %g seconds\n", t_write);
     fprintf(f, "Time for sort and Resampling:   %g seconds\n", t_fit);
   }
   fclose(info);

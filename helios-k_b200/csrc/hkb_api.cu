@@ -199,38 +199,47 @@ hk_status hk_set_options(hk_ctx *c, double qalphaL, double gammaF, int units, do
 }
 
 // --------------------------------------------------------------- lines
-static bool uniform(const double *a, int64_t n) {
-  for (int64_t i = 1; i < n; ++i)
-    if (a[i] != a[0]) return false;
-  return true;
-}
-
-// Upload one column; a uniform column becomes a scalar (null pointer).
-static hk_status upload_col(hk_ctx *c, DevBuf &buf, const std::vector<double> &h,
-                            bool allow_uniform, const double **dptr, double *cval) {
-  const int64_t n = (int64_t)h.size();
-  *cval = n ? h[0] : 0.0;
-  if (allow_uniform && uniform(h.data(), n)) {
-    buf.release();
-    *dptr = nullptr;
-    return HK_OK;
+// ------------------------------------------------------------ ingestion
+// Lines arrive as unsorted device columns in load order (from caller arrays
+// or from binary records unpacked on the GPU, hkb_ingest.cu); load_device
+// sorts them by centre once, gathers each column into sorted order, and keeps
+// a column whose values are all equal as a scalar (synthetic HITRAN: A = delta
+// = 0; ExoMol: gamma, n from the species defaults).
+struct IngestBuf {
+  DevBuf cols;  // 7 n doubles + n bytes, plus minmax scratch
+  LineCols lc{};
+  double *scratch = nullptr;
+  cudaError_t alloc(int64_t n) {
+    const size_t nd = (size_t)std::max<int64_t>(n, 1);
+    cudaError_t e = cols.ensure(7 * nd * sizeof(double) + nd + 2 * 592 * sizeof(double) + 64);
+    if (e != cudaSuccess) return e;
+    double *p = cols.as<double>();
+    lc.nu = p;
+    lc.S = p + nd;
+    lc.EL = p + 2 * nd;
+    lc.gam = p + 3 * nd;
+    lc.nexp = p + 4 * nd;
+    lc.delta = p + 5 * nd;
+    lc.Aterm = p + 6 * nd;
+    scratch = p + 7 * nd;
+    lc.iso = reinterpret_cast<uint8_t *>(scratch + 2 * 592);
+    return cudaSuccess;
   }
-  DevBuf tmp;
-  CUDA_TRY(c, tmp.ensure(n * sizeof(double)));
-  CUDA_TRY(c, cudaMemcpy(tmp.p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice));
-  CUDA_TRY(c, buf.ensure(n * sizeof(double)));
-  CUDA_TRY(c, launch_gather_lines(n, c->order.as<int64_t>(), tmp.as<double>(), buf.as<double>(), 0));
-  CUDA_TRY(c, cudaDeviceSynchronize());
-  tmp.release();
-  *dptr = buf.as<double>();
-  return HK_OK;
+};
+
+static IngestSpec ingest_spec(const hk_ctx *c, bool hitran) {
+  IngestSpec sp{};
+  sp.hitran = hitran ? 1 : 0;
+  sp.niso = (int)c->iso_mass.size();
+  sp.qalphaL = c->qalphaL;
+  sp.gammaF = c->gammaF;
+  sp.defaultL = c->defaultL;
+  sp.defaultn = c->defaultn;
+  sp.four_pi_c = 4.0 * M_PI * HK_C;  // voigt.h:349 divides A by this product
+  return sp;
 }
 
-static hk_status load_common(hk_ctx *c, int64_t n, const double *nu,
-                             const std::vector<double> &Sv, const std::vector<double> &ELv,
-                             const std::vector<double> &gamv, const std::vector<double> &nexpv,
-                             const std::vector<double> &deltav, const std::vector<double> &Atv,
-                             const std::vector<uint8_t> &isov) {
+static hk_status load_device(hk_ctx *c, int64_t n, IngestBuf &ib, int niso) {
   cudaSetDevice(c->device);
   c->nlines = 0;
   c->L = LinesDev{};
@@ -239,51 +248,44 @@ static hk_status load_common(hk_ctx *c, int64_t n, const double *nu,
     ok(c);
     return HK_OK;
   }
-  // sort by centre on the GPU (once per load)
   CUDA_TRY(c, c->nu0.ensure(n * sizeof(double)));
   CUDA_TRY(c, c->order.ensure(n * sizeof(int64_t)));
-  CUDA_TRY(c, cudaMemcpy(c->nu0.p, nu, n * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(c->nu0.p, ib.lc.nu, n * sizeof(double), cudaMemcpyDeviceToDevice));
   CUDA_TRY(c, sort_lines_by_nu(n, c->nu0.as<double>(), c->order.as<int64_t>(), 0));
   CUDA_TRY(c, cudaDeviceSynchronize());
-  hk_status st;
-  const double *p;
-  double cv;
-  if ((st = upload_col(c, c->Sfile, Sv, false, &p, &cv)) != HK_OK) return st;
-  c->L.Sfile = p;
-  if ((st = upload_col(c, c->EL, ELv, true, &p, &cv)) != HK_OK) return st;
-  c->L.EL = p;
-  c->L.EL_c = cv;
-  if ((st = upload_col(c, c->gam, gamv, true, &p, &cv)) != HK_OK) return st;
-  c->L.gam = p;
-  c->L.gam_c = cv;
-  if ((st = upload_col(c, c->nexp, nexpv, true, &p, &cv)) != HK_OK) return st;
-  c->L.nexp = p;
-  c->L.nexp_c = cv;
-  if ((st = upload_col(c, c->delta, deltav, true, &p, &cv)) != HK_OK) return st;
-  c->L.delta = p;
-  c->L.delta_c = cv;
-  if ((st = upload_col(c, c->Aterm, Atv, true, &p, &cv)) != HK_OK) return st;
-  c->L.Aterm = p;
-  c->L.Aterm_c = cv;
-  bool iso_uniform = true;
-  for (int64_t i = 1; i < n; ++i)
-    if (isov[i] != isov[0]) { iso_uniform = false; break; }
-  if (iso_uniform && isov[0] == 0) {
+  struct Col { DevBuf *buf; double *src; const double **dst; double *cval; bool uni; };
+  double dummy = 0.0;
+  const double *sfile = nullptr;
+  Col cols[6] = {{&c->Sfile, ib.lc.S, &sfile, &dummy, false},
+                 {&c->EL, ib.lc.EL, &c->L.EL, &c->L.EL_c, true},
+                 {&c->gam, ib.lc.gam, &c->L.gam, &c->L.gam_c, true},
+                 {&c->nexp, ib.lc.nexp, &c->L.nexp, &c->L.nexp_c, true},
+                 {&c->delta, ib.lc.delta, &c->L.delta, &c->L.delta_c, true},
+                 {&c->Aterm, ib.lc.Aterm, &c->L.Aterm, &c->L.Aterm_c, true}};
+  for (Col &q : cols) {
+    double lo = 0.0, hi = 0.0;
+    CUDA_TRY(c, column_minmax(n, q.src, ib.scratch, &lo, &hi, 0));
+    *q.cval = lo;
+    if (q.buf == &c->delta) c->max_abs_delta = std::max(std::fabs(lo), std::fabs(hi));
+    if (q.uni && lo == hi) {
+      q.buf->release();
+      *q.dst = nullptr;
+      continue;
+    }
+    CUDA_TRY(c, q.buf->ensure(n * sizeof(double)));
+    CUDA_TRY(c, launch_gather_lines(n, c->order.as<int64_t>(), q.src, q.buf->as<double>(), 0));
+    *q.dst = q.buf->as<double>();
+  }
+  c->L.Sfile = sfile;
+  if (niso <= 1) {
     c->iso.release();
     c->L.iso = nullptr;
   } else {
-    // gather on the host side of the permutation: pull the order back
-    std::vector<int64_t> ord(n);
-    CUDA_TRY(c, cudaMemcpy(ord.data(), c->order.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost));
-    std::vector<uint8_t> sorted(n);
-    for (int64_t k = 0; k < n; ++k) sorted[k] = isov[ord[k]];
     CUDA_TRY(c, c->iso.ensure(n));
-    CUDA_TRY(c, cudaMemcpy(c->iso.p, sorted.data(), n, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, launch_gather_u8(n, c->order.as<int64_t>(), ib.lc.iso, c->iso.as<uint8_t>(), 0));
     c->L.iso = c->iso.as<uint8_t>();
   }
-  double md = 0.0;
-  for (double d : deltav) md = std::max(md, std::fabs(d));
-  c->max_abs_delta = md;
+  CUDA_TRY(c, cudaDeviceSynchronize());
   c->L.nu0 = c->nu0.as<double>();
   c->L.n = n;
   c->nlines = n;
@@ -301,23 +303,34 @@ hk_status hk_load_lines_hitran(hk_ctx *c, int64_t n, const double *nu, const dou
   if (n < 0 || (n > 0 && (!nu || !S || !EL || !A || !delta || !gair || !gself || !nexp)))
     return fail(c, HK_ERR_ARG, "null line array");
   const int niso = (int)c->iso_mass.size();
-  std::vector<double> Sv(S, S + n), ELv(EL, EL + n), gamv(n), nexpv(nexp, nexp + n),
-      deltav(delta, delta + n), Atv(n);
-  std::vector<uint8_t> isov(n, 0);
-  for (int64_t i = 0; i < n; ++i) {
-    if (iso) {
+  if (iso)
+    for (int64_t i = 0; i < n; ++i)
       if (iso[i] < 0 || iso[i] >= niso)
         return fail(c, HK_ERR_FORMAT, "line %lld: isotopologue index %d not in the species table", (long long)i, iso[i]);
-      isov[i] = (uint8_t)iso[i];
-    }
-    // host.h:640-641
-    double vy = (1.0 - c->qalphaL) * gair[i] + c->qalphaL * gself[i];
-    vy *= c->gammaF;
-    gamv[i] = vy;
-    // voigt.h:349
-    Atv[i] = A[i] / (4.0 * M_PI * HK_C);
+  cudaSetDevice(c->device);
+  IngestBuf ib;
+  DevBuf tmp;  // gamma_air, gamma_self, A and the isotopologue indices as given
+  const size_t nd = (size_t)std::max<int64_t>(n, 1);
+  CUDA_TRY(c, ib.alloc(n));
+  CUDA_TRY(c, tmp.ensure(3 * nd * sizeof(double) + nd * sizeof(int32_t)));
+  double *ga = tmp.as<double>(), *gs = ga + nd, *Ad = ga + 2 * nd;
+  int32_t *iso32 = reinterpret_cast<int32_t *>(ga + 3 * nd);
+  const size_t B = (size_t)n * sizeof(double);
+  if (n) {
+    CUDA_TRY(c, cudaMemcpy(ib.lc.nu, nu, B, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(ib.lc.S, S, B, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(ib.lc.EL, EL, B, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(ib.lc.nexp, nexp, B, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(ib.lc.delta, delta, B, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(ga, gair, B, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(gs, gself, B, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(Ad, A, B, cudaMemcpyHostToDevice));
+    if (iso) CUDA_TRY(c, cudaMemcpy(iso32, iso, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CUDA_TRY(c, launch_finish_columns(n, ingest_spec(c, true), ga, gs, Ad, iso ? iso32 : nullptr,
+                                      ib.lc, 0));
   }
-  return load_common(c, n, nu, Sv, ELv, gamv, nexpv, deltav, Atv, isov);
+  tmp.release();
+  return load_device(c, n, ib, niso);
 }
 
 hk_status hk_load_lines_exomol(hk_ctx *c, int64_t n, const double *nu, const double *S,
@@ -326,14 +339,22 @@ hk_status hk_load_lines_exomol(hk_ctx *c, int64_t n, const double *nu, const dou
   if (c->iso_mass.empty()) return fail(c, HK_ERR_STATE, "hk_set_species must come before loading lines");
   if (c->database != HK_DB_EXOMOL) return fail(c, HK_ERR_STATE, "species database is not ExoMol");
   if (n < 0 || (n > 0 && (!nu || !S || !EL || !A))) return fail(c, HK_ERR_ARG, "null line array");
-  std::vector<double> Sv(S, S + n), ELv(EL, EL + n), gamv(n), nexpv(n, c->defaultn),
-      deltav(n, 0.0), Atv(n);
-  std::vector<uint8_t> isov(n, 0);
-  for (int64_t i = 0; i < n; ++i) {
-    gamv[i] = c->defaultL * c->gammaF;          // voigt.h:497
-    Atv[i] = A[i] / (4.0 * M_PI * HK_C);        // voigt.h:496
+  cudaSetDevice(c->device);
+  IngestBuf ib;
+  DevBuf tmp;  // A as given
+  CUDA_TRY(c, ib.alloc(n));
+  CUDA_TRY(c, tmp.ensure((size_t)std::max<int64_t>(n, 1) * sizeof(double)));
+  const size_t B = (size_t)n * sizeof(double);
+  if (n) {
+    CUDA_TRY(c, cudaMemcpy(ib.lc.nu, nu, B, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(ib.lc.S, S, B, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(ib.lc.EL, EL, B, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(tmp.p, A, B, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, launch_finish_columns(n, ingest_spec(c, false), nullptr, nullptr, tmp.as<double>(),
+                                      nullptr, ib.lc, 0));
   }
-  return load_common(c, n, nu, Sv, ELv, gamv, nexpv, deltav, Atv, isov);
+  tmp.release();
+  return load_device(c, n, ib, 1);
 }
 
 int64_t hk_num_lines(const hk_ctx *c) { return c ? c->nlines : 0; }
@@ -987,6 +1008,101 @@ hk_status hk_fp32_peak(hk_ctx *c, double *tflops) {
 }
 
 // ---------------------------------------------------------- file loader
+// The selected binary line files stream to the GPU in chunks of whole
+// records: fread fills one of two pinned buffers while the other's copy and
+// unpack run (heliosk.cu:1405-1423 overlaps reads and copies the same way for
+// ExoMol, 8192 lines at a time), and the records become columns on the device
+// (hkb_ingest.cu).  Nothing of a line list passes through pageable host
+// memory beyond the kernel's file cache.
+static constexpr int64_t kIngestChunk = 1 << 20;  // records per chunk
+
+static hk_status stream_line_files(hk_ctx *c, const SpeciesInfo &sp, int fi0, int fi1) {
+  const bool hitran = sp.database == HK_DB_HITRAN;
+  const size_t rec = hitran ? 68 : 32;
+  int64_t n = 0;
+  for (int fi = fi0; fi < fi1; ++fi) n += sp.NL[fi];
+  IngestSpec spec = ingest_spec(c, hitran);
+  for (size_t k = 0; k < sp.iso.size() && k < (size_t)HK_MAX_ISO; ++k)
+    strncpy(spec.cid[k], sp.iso[k].cid.c_str(), 4);  // zero-padded, as strncmp(.., 4) reads it
+  cudaSetDevice(c->device);
+  IngestBuf ib;
+  CUDA_TRY(c, ib.alloc(n));
+  struct Pipe {
+    unsigned char *host[2] = {nullptr, nullptr};
+    DevBuf dev[2], bad;
+    cudaStream_t st = nullptr;
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    FILE *f = nullptr;
+    ~Pipe() {
+      if (st) cudaStreamSynchronize(st);
+      for (int b = 0; b < 2; ++b) {
+        if (host[b]) cudaFreeHost(host[b]);
+        if (done[b]) cudaEventDestroy(done[b]);
+      }
+      if (st) cudaStreamDestroy(st);
+      if (f) fclose(f);
+    }
+  } pp;
+  const size_t chunk_bytes = (size_t)kIngestChunk * rec;
+  CUDA_TRY(c, cudaStreamCreateWithFlags(&pp.st, cudaStreamNonBlocking));
+  for (int b = 0; b < 2; ++b) {
+    CUDA_TRY(c, cudaHostAlloc((void **)&pp.host[b], chunk_bytes, cudaHostAllocDefault));
+    CUDA_TRY(c, pp.dev[b].ensure(chunk_bytes));
+    CUDA_TRY(c, cudaEventCreateWithFlags(&pp.done[b], cudaEventDisableTiming));
+  }
+  CUDA_TRY(c, pp.bad.ensure(sizeof(unsigned long long)));
+  const unsigned long long none = ~0ull;
+  CUDA_TRY(c, cudaMemcpy(pp.bad.p, &none, sizeof none, cudaMemcpyHostToDevice));
+  int64_t base = 0;
+  int b = 0;
+  bool used[2] = {false, false};
+  for (int fi = fi0; fi < fi1; ++fi) {
+    const std::string fname = sp.dataFilename[fi] + "bin";
+    pp.f = fopen(fname.c_str(), "rb");
+    if (!pp.f) return fail(c, HK_ERR_IO, "Error: line list file not found: %s", fname.c_str());
+    const int64_t nl = sp.NL[fi];
+    for (int64_t r0 = 0; r0 < nl; r0 += kIngestChunk) {
+      const int64_t cnt = std::min<int64_t>(kIngestChunk, nl - r0);
+      if (used[b]) CUDA_TRY(c, cudaEventSynchronize(pp.done[b]));  // buffer b is free again
+      const size_t got = fread(pp.host[b], rec, (size_t)cnt, pp.f);
+      if ((int64_t)got != cnt)
+        return fail(c, HK_ERR_FORMAT, "Error: line list file %s is truncated (%lld of %lld records)",
+                    fname.c_str(), (long long)(r0 + (int64_t)got), (long long)nl);
+      CUDA_TRY(c, cudaMemcpyAsync(pp.dev[b].p, pp.host[b], (size_t)cnt * rec,
+                                  cudaMemcpyHostToDevice, pp.st));
+      LineCols at = ib.lc;
+      for (double **q : {&at.nu, &at.S, &at.EL, &at.gam, &at.nexp, &at.delta, &at.Aterm}) *q += base + r0;
+      at.iso += base + r0;
+      CUDA_TRY(c, launch_unpack_records(pp.dev[b].as<unsigned char>(), cnt, base + r0, spec, at,
+                                        pp.bad.as<unsigned long long>(), pp.st));
+      CUDA_TRY(c, cudaEventRecord(pp.done[b], pp.st));
+      used[b] = true;
+      b ^= 1;
+    }
+    fclose(pp.f);
+    pp.f = nullptr;
+    base += nl;
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(pp.st));
+  unsigned long long bad = none;
+  CUDA_TRY(c, cudaMemcpy(&bad, pp.bad.p, sizeof bad, cudaMemcpyDeviceToHost));
+  if (bad != none) {
+    // host.h:624-639: a record whose isotopologue id is not in the species table
+    int64_t i = (int64_t)bad;
+    int fi = fi0;
+    while (fi + 1 < fi1 && i >= sp.NL[fi]) i -= sp.NL[fi++];
+    char cid[4] = {0, 0, 0, 0};
+    FILE *f = fopen((sp.dataFilename[fi] + "bin").c_str(), "rb");
+    if (f) {
+      if (fseek(f, (long)(i * (int64_t)rec), SEEK_SET) == 0 && fread(cid, 1, 4, f) != 4) cid[0] = 0;
+      fclose(f);
+    }
+    return fail(c, HK_ERR_FORMAT, "Error: partition function not found. %lld |%.3s|%s|", (long long)i,
+                cid, sp.iso[0].cid.c_str());
+  }
+  return load_device(c, n, ib, (int)sp.iso.size());
+}
+
 hk_status hk_load_species_file(hk_ctx *c, const char *path, const char *species, double numin,
                                double numax, int cutMode, double cut) {
   if (!c || !species) return HK_ERR_ARG;
@@ -1008,15 +1124,9 @@ hk_status hk_load_species_file(hk_ctx *c, const char *path, const char *species,
     if (rc != 0) return fail(c, rc, "%s", msg.c_str());
     if ((st = hk_set_partition(c, (int)j, (int)T.size(), T.data(), Q.data())) != HK_OK) return st;
   }
-  LineColumns cols;
-  rc = read_line_files(sp, numin, numax, cutMode, cut, cols, msg);
-  if (rc != 0) return fail(c, rc, "%s", msg.c_str());
-  const int64_t n = (int64_t)cols.nu.size();
-  if (sp.database == HK_DB_HITRAN)
-    return hk_load_lines_hitran(c, n, cols.nu.data(), cols.S.data(), cols.EL.data(), cols.A.data(),
-                                cols.delta.data(), cols.gair.data(), cols.gself.data(),
-                                cols.nexp.data(), cols.iso.data());
-  return hk_load_lines_exomol(c, n, cols.nu.data(), cols.S.data(), cols.EL.data(), cols.A.data());
+  int fi0, fi1;
+  line_file_range(sp, numin, numax, cutMode, cut, &fi0, &fi1);
+  return stream_line_files(c, sp, fi0, fi1);
 }
 
 }  // extern "C"

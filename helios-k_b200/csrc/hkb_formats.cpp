@@ -193,10 +193,10 @@ int read_species_param(const std::string &path, const std::string &species,
   return 0;
 }
 
-// heliosk.cu:943-956 file pruning, then the records of host.h:607-615
-// (HITRAN) or prepareExomol.cpp:222-225 (ExoMol).
-int read_line_files(const SpeciesInfo &sp, double numin, double numax, int cutMode,
-                    double cut, LineColumns &cols, std::string &msg) {
+// heliosk.cu:943-956: the files [fi0, fi1) whose wavenumber range, widened
+// by the cut, can reach [numin, numax] (all files for cutMode 1 and 2).
+void line_file_range(const SpeciesInfo &sp, double numin, double numax, int cutMode, double cut,
+                     int *fi0_out, int *fi1_out) {
   if (cut == 0.0) cut = 1.0e30;
   int fi0 = sp.nFiles, fi1 = 0;
   if (cutMode == 0) {
@@ -212,68 +212,8 @@ int read_line_files(const SpeciesInfo &sp, double numin, double numax, int cutMo
     fi0 = 0;
     fi1 = sp.nFiles;
   }
-  cols = LineColumns{};
-  for (int fi = fi0; fi < fi1; ++fi) {
-    const std::string fname = sp.dataFilename[fi] + "bin";
-    FILE *f = fopen(fname.c_str(), "rb");
-    if (!f) {
-      msg = "Error: line list file not found: " + fname;
-      return HK_ERR_IO;
-    }
-    const long long nl = sp.NL[fi];
-    const size_t rec = (sp.database == 0) ? 68 : 32;
-    std::vector<unsigned char> buf((size_t)nl * rec);
-    size_t got = nl ? fread(buf.data(), rec, (size_t)nl, f) : 0;
-    fclose(f);
-    if ((long long)got != nl) {
-      msg = "Error: line list file " + fname + " is truncated (" + std::to_string(got) +
-            " of " + std::to_string(nl) + " records)";
-      return HK_ERR_FORMAT;
-    }
-    const size_t base = cols.nu.size();
-    for (auto *v : {&cols.nu, &cols.S, &cols.EL, &cols.A, &cols.delta, &cols.gair, &cols.gself, &cols.nexp})
-      v->resize(base + nl);
-    cols.iso.resize(base + nl);
-    for (long long i = 0; i < nl; ++i) {
-      const unsigned char *r = buf.data() + (size_t)i * rec;
-      double v[8];
-      if (sp.database == 0) {
-        char cid[4];
-        memcpy(cid, r, 4);
-        memcpy(v, r + 4, 64);
-        int j = -1;
-        for (size_t k = 0; k < sp.iso.size(); ++k)
-          if (strncmp(cid, sp.iso[k].cid.c_str(), 4) == 0) j = (int)k;
-        if (j < 0) {
-          char b[160];
-          snprintf(b, sizeof b, "Error: partition function not found. %lld |%.3s|%s|", i, cid, sp.iso[0].cid.c_str());
-          msg = b;
-          return HK_ERR_FORMAT;
-        }
-        cols.nu[base + i] = v[0];
-        cols.S[base + i] = v[1];
-        cols.EL[base + i] = v[2];
-        cols.A[base + i] = v[3];
-        cols.delta[base + i] = v[4];
-        cols.gair[base + i] = v[5];
-        cols.gself[base + i] = v[6];
-        cols.nexp[base + i] = v[7];
-        cols.iso[base + i] = j;
-      } else {
-        memcpy(v, r, 32);
-        cols.nu[base + i] = v[0];
-        cols.S[base + i] = v[1];
-        cols.EL[base + i] = v[2];
-        cols.A[base + i] = v[3];
-        cols.delta[base + i] = 0.0;
-        cols.gair[base + i] = 0.0;
-        cols.gself[base + i] = 0.0;
-        cols.nexp[base + i] = sp.defaultn;
-        cols.iso[base + i] = 0;
-      }
-    }
-  }
-  return 0;
+  *fi0_out = fi0;
+  *fi1_out = fi1;
 }
 
 // host.h:75-525 (read_parameters): "key = value" lines, an unknown key is an

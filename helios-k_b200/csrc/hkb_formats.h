@@ -33,11 +33,6 @@ struct SpeciesInfo {
   double defaultL = 0.0, defaultn = 0.0;
 };
 
-struct LineColumns {
-  std::vector<double> nu, S, EL, A, delta, gair, gself, nexp;
-  std::vector<int32_t> iso;
-};
-
 // param.dat (define.h:113-161 Param, defaults of heliosk.cu:308-360)
 struct Params {
   std::string name;
@@ -63,8 +58,8 @@ int read_q_file(const std::string &fname, int ncol, std::vector<double> &T,
                 std::vector<double> &Q, std::string &msg);
 int read_species_param(const std::string &path, const std::string &species,
                        SpeciesInfo &sp, std::string &msg);
-int read_line_files(const SpeciesInfo &sp, double numin, double numax, int cutMode,
-                    double cut, LineColumns &cols, std::string &msg);
+void line_file_range(const SpeciesInfo &sp, double numin, double numax, int cutMode, double cut,
+                     int *fi0, int *fi1);
 int read_param_file(const std::string &fname, int argc, char **argv, Params &p,
                     std::string &msg);
 

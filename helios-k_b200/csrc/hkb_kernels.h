@@ -57,6 +57,30 @@ inline LinesDev lines_sub(const LinesDev &L, int64_t l0, int64_t n) {
   return s;
 }
 
+// Line ingestion (hkb_ingest.cu): binary records or caller columns to the
+// library's columns on the device, in load order.
+struct IngestSpec {
+  int hitran;           // 68-byte HITRAN records (else 32-byte ExoMol)
+  int niso;
+  char cid[HK_MAX_ISO][4];
+  double qalphaL, gammaF, defaultL, defaultn;
+  double four_pi_c;     // 4 pi c as the host forms it
+};
+struct LineCols {
+  double *nu, *S, *EL, *gam, *nexp, *delta, *Aterm;
+  uint8_t *iso;
+};
+cudaError_t launch_unpack_records(const unsigned char *raw_d, int64_t n, int64_t first,
+                                  const IngestSpec &sp, const LineCols &cols,
+                                  unsigned long long *bad_d, cudaStream_t stream);
+cudaError_t launch_finish_columns(int64_t n, const IngestSpec &sp, const double *gair_d,
+                                  const double *gself_d, const double *A_d, const int32_t *iso32_d,
+                                  const LineCols &cols, cudaStream_t stream);
+cudaError_t column_minmax(int64_t n, const double *v_d, double *scratch_d, double *lo, double *hi,
+                          cudaStream_t stream);
+cudaError_t launch_gather_u8(int64_t n, const int64_t *order_d, const uint8_t *src_d, uint8_t *dst_d,
+                             cudaStream_t stream);
+
 cudaError_t launch_count_pairs(const LinesDev &L, const GridDev &g, const StateDev *state_d,
                                unsigned long long *out_d, cudaStream_t stream);
 inline size_t line_prep_bytes(bool mixed) { return mixed ? sizeof(LinePrepF) : sizeof(LinePrep); }

@@ -109,18 +109,21 @@ def exomol_states():
 # ------------------------------------------------------------- file writers
 
 def write_species(dirname, name, database=0, nfiles=1, nl=None, limits=(0, 30000),
-                  defaultL=0.0, defaultn=0.0, qfile="q_synth.txt", npfcol=2):
-    """<name>.param in the layout ISO.h:16-219 parses."""
+                  defaultL=0.0, defaultn=0.0, qfile="q_synth.txt", npfcol=2, isos=None):
+    """<name>.param in the layout ISO.h:16-219 parses.  isos: rows
+    (cid, abundance, molar mass), all on the synthetic partition table;
+    default one isotopologue of mass MASS."""
     os.makedirs(dirname, exist_ok=True)
     nl = list(nl or [0])
-    cid = "11" if database in (0, 1) else "0"
+    if isos is None:
+        isos = [("11" if database in (0, 1) else "0", 1.0, MASS)]
     lines = [
         f"Database = {database}",
         "Molecule number = 1",
         f"Name = {name}",
-        "Number of Isotopologues = 1",
+        f"Number of Isotopologues = {len(isos)}",
         "#ID Abundance      Q(296K)   g     Molar Mass(g)  partition file :",
-        f"{cid} 1.0 {float(q_of_T(296.0)):.10g} 1 {MASS:.6f} {qfile}",
+        *[f"{cid} {ab:.10g} {float(q_of_T(296.0)):.10g} 1 {m:.6f} {qfile}" for cid, ab, m in isos],
         f"Number of columns in partition File = {npfcol}",
         f"Number of line/transition files = {nfiles}",
         "Number of lines per file :",
@@ -149,9 +152,11 @@ EXOMOL_DTYPE = np.dtype([("nu", "<f8"), ("S", "<f8"), ("EL", "<f8"), ("A", "<f8"
 assert HITRAN_DTYPE.itemsize == 68 and EXOMOL_DTYPE.itemsize == 32
 
 
-def write_hitran_bin(path, lines):
+def write_hitran_bin(path, lines, cids=None):
+    """68-byte records; cids: per-record 3-character isotopologue ids
+    (default " 11" for every line)."""
     rec = np.empty(len(lines["nu"]), HITRAN_DTYPE)
-    rec["cid"] = b" 11"
+    rec["cid"] = b" 11" if cids is None else cids
     for k in ("nu", "S", "EL", "A", "delta", "gair", "gself", "n"):
         rec[k] = lines[k]
     rec.tofile(path)
