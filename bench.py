@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference's own CUDA build beside ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--tuning", type=int, default=2, choices=[0, 1, 2],
+                    help="tile-shape tuner: 0 fixed default shape, 1 when it pays, 2 once "
+                         "before the timed steps")
     return ap.parse_args()
 
 
@@ -446,6 +449,9 @@ def main():
     # whose per-state records exceed the workspace run the sectioned path of
     # hk_opacity instead (not capturable: it sizes sections from the state
     # pass)
+    # the tile shape is tuned once, before the graph is recorded (outside
+    # the timed steps, like the workspace allocations)
+    ctx.set_tuning(args.tuning)
     try:
         ctx.table_build(T, P, K, coeff, nxmin, nC=nC, precision=prec)
         graph = True
@@ -464,6 +470,7 @@ def main():
         timed_step()
     torch.cuda.synchronize()
     launches_per_step = ctx.table_kernels if graph else ctx.last_launches
+    shape_used, shape_tuned, probe_ms = ctx.tuning_result()
     if ws > 1:
         torch.distributed.barrier()
     clk = Clocks(lrank)
@@ -561,6 +568,11 @@ def main():
                    "precision": args.precision, "parallelism": f"states x{ws} ranks",
                    "format": W.get("database", "hitran"),
                    "execution": "one CUDA graph per step" if graph else "hk_opacity sections + hk_kdist",
+                   "tile_shape": {"lines_per_chunk": hkb.tile_shape(shape_used)[0],
+                                  "points_per_tile": hkb.tile_shape(shape_used)[1],
+                                  "shape": shape_used, "tuned": shape_tuned >= 0,
+                                  "probe_ms": [round(float(v), 3) for v in probe_ms]
+                                  if shape_tuned >= 0 else None},
                    "l2": f"inputs larger than L2 (line columns ~{W['n'] * 48 / 1e9:.2g} GB resident), no flush"},
         "s_per_state": ms * 1e-3 / ns,
         "s_per_table": ms * 1e-3 if ns > 1 else None,

@@ -126,6 +126,8 @@ int main(int argc, char **argv) {
   cudaEventRecord(t1);
   const double t_input = compute ? seconds() : 0.0;
   chk(hk_set_grid(c, p.numin, p.numax, p.dnu, p.nbins, p.cutMode, p.cut, kmin));
+  // doTuning = 1: the tile-shape tuner, where its probes pay off (PFile tables)
+  chk(hk_set_tuning(c, p.doTuning == 1 ? 1 : 0));
   const int64_t nx = hk_grid_points(c);
   const int nP = p.nP;
   std::vector<double> K((size_t)nP * nx), x(nx);
@@ -147,6 +149,10 @@ int main(int argc, char **argv) {
     hk_last_timing(c, &voigt_ms, nullptr);
     t_K = voigt_ms >= 0.0 ? voigt_ms * 1e-3 : t_call;
     t_lines = t_call - t_K;
+    int shape = 0, tuned = -1, ch = 0, gp = 0;
+    hk_tuning_result(c, &shape, &tuned, nullptr);
+    hk_tile_shape_info(shape, &ch, &gp);
+    fprintf(info, "Tile shape: %d lines x %d points (%s)\n", ch, gp, tuned >= 0 ? "tuned" : "fixed");
   } else {
     // doStoreFullK = -1 / -2: read K back (heliosk.cu:1860-1935)
     const std::string fn = p.pathK + "Out_" + p.name + (p.doStoreFullK == -1 ? ".dat" : ".bin");

@@ -73,6 +73,16 @@ struct hk_ctx {
   bool have_voigt_t = false, have_kdist_t = false;
   int64_t launches = 0;  // kernels launched since the last hk_opacity began
   bool voigt_ms_acc_only = false;  // sectioned call: voigt_ms_acc is the whole time
+  // tile shape of the mixed Voigt kernel: fixed (tuning 0) or chosen by
+  // timed probes (tuning 1 when the probes cost at most a tenth of the
+  // call's sweep, tuning 2 always) once per loaded lines, grid and options
+  int tuning = 0;
+  int shape_fixed = 0;
+  bool tuned = false;
+  int tuned_shape = 0;
+  int last_shape = 0;
+  std::vector<double> tune_ms;  // probe time per shape at the last tuning
+  DevBuf tunework;              // probe states and their max-term words
   // T-P table recorded as one CUDA graph (hk_table_build / hk_table_run)
   cudaGraph_t table_graph = nullptr;
   cudaGraphExec_t table_exec = nullptr;
@@ -145,7 +155,8 @@ void hk_destroy(hk_ctx *c) {
   for (DevBuf *b : {&c->nu0, &c->Sfile, &c->EL, &c->gam, &c->nexp, &c->delta,
                     &c->Aterm, &c->iso, &c->order, &c->states, &c->ticket,
                     &c->prep, &c->wbits, &c->Kwork, &c->outwork, &c->scratch,
-                    &c->qrV, &c->qrC, &c->qrD, &c->vpart, &c->vcnt, &c->sscale, &c->gscale, &c->adjwork})
+                    &c->qrV, &c->qrC, &c->qrD, &c->vpart, &c->vcnt, &c->sscale, &c->gscale, &c->adjwork,
+                    &c->tunework})
     b->release();
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -154,7 +165,7 @@ void hk_destroy(hk_ctx *c) {
 
 const char *hk_last_error(const hk_ctx *c) { return c ? c->err.c_str() : "null context"; }
 
-int hk_tile_points(void) { return voigt_tile_points(); }
+int hk_tile_points(void) { return voigt_tile_points(0); }
 
 // ------------------------------------------------------------- species
 hk_status hk_set_species(hk_ctx *c, int database, int niso, const double *mass,
@@ -194,6 +205,7 @@ hk_status hk_set_options(hk_ctx *c, double qalphaL, double gammaF, int units, do
   c->gammaF = gammaF;
   c->units = units;
   c->Sscale = Sscale;
+  c->tuned = false;
   ok(c);
   return HK_OK;
 }
@@ -241,6 +253,7 @@ static IngestSpec ingest_spec(const hk_ctx *c, bool hitran) {
 
 static hk_status load_device(hk_ctx *c, int64_t n, IngestBuf &ib, int niso) {
   cudaSetDevice(c->device);
+  c->tuned = false;
   c->nlines = 0;
   c->L = LinesDev{};
   c->L.database = c->database;
@@ -392,6 +405,7 @@ hk_status hk_set_grid(hk_ctx *c, double numin, double numax, double dnu, int nbi
   c->nxb = nx / nbins;
   c->kmin = kmin;
   c->grid_set = true;
+  c->tuned = false;
   ok(c);
   return HK_OK;
 }
@@ -454,9 +468,10 @@ static hk_status check_ready(hk_ctx *c) {
 // a contiguous range of the nu-sorted list -- fit the workspace, and each
 // section is prepared and summed on its own.  A tile sees the same lines in
 // the same order as in the batched path, so K is bit-identical to it.
-static hk_status opacity_sectioned(hk_ctx *c, int nstates, bool mixed, double *Kd, cudaStream_t s) {
+static hk_status opacity_sectioned(hk_ctx *c, int nstates, bool mixed, int shape, double *Kd,
+                                   cudaStream_t s) {
   const int64_t nx = c->g.nx, n = c->nlines;
-  const int G = voigt_tile_points();
+  const int G = voigt_tile_points(shape);
   const int tps = (int)((nx + G - 1) / G);
   const size_t rec = line_prep_bytes(mixed);
   const int64_t cap = (int64_t)(c->prep_budget / rec);
@@ -508,7 +523,7 @@ static hk_status opacity_sectioned(hk_ctx *c, int nstates, bool mixed, double *K
     }
     for (const Sec &q : secs) {
       const LinesDev Ls = lines_sub(c->L, q.L0, q.L1 - q.L0);
-      const VoigtPlan plan = plan_voigt_section(mixed, nx, q.t0, q.t1 - q.t0, 0);
+      const VoigtPlan plan = plan_voigt_section(mixed, shape, nx, q.t0, q.t1 - q.t0, 0);
       if (plan.nsplit > 1) {
         CUDA_TRY(c, c->vpart.ensure(plan.partial_doubles * sizeof(double)));
         CUDA_TRY(c, c->vcnt.ensure(plan.counters * sizeof(unsigned)));
@@ -528,6 +543,85 @@ static hk_status opacity_sectioned(hk_ctx *c, int nstates, bool mixed, double *K
   }
   c->have_voigt_t = false;  // all Voigt time is in voigt_ms_acc
   c->voigt_ms_acc_only = true;
+  return HK_OK;
+}
+
+// ------------------------------------------------------------ autotuner
+// The mixed kernel's tile shape (lines per staged chunk x grid points per
+// tile; voigt_num_shapes() of them) changes only the order of the FP64
+// additions, so every shape meets the same accuracy; the fastest depends on
+// the line density, the window widths and the grid.  Like the reference's
+// self-tuning of its kernels' tile widths (heliosk.cu:1363-1705, timed trial
+// launches), the tuner times each shape on probes of the workload: up to 4 of
+// the call's states spread over it, each prepared on its own, on a section of
+// the grid in the middle (a quarter of it at least, and two waves of
+// tickets), after one warm-up tile per shape.  The choice holds until lines,
+// grid or options change.  Its probe outputs land in K rows the call then
+// overwrites.
+static int shape_for(const hk_ctx *c, bool mixed) {
+  if (!mixed) return 0;
+  return (c->tuning != 0 && c->tuned) ? c->tuned_shape : c->shape_fixed;
+}
+
+static hk_status tune_shape(hk_ctx *c, int nstates, const std::vector<StateDev> &hs, double *Kd,
+                            cudaStream_t s) {
+  const int64_t nx = c->g.nx, n = c->nlines;
+  const int nsh = voigt_num_shapes();
+  const size_t per_state = (size_t)std::max<int64_t>(n, 1) * line_prep_bytes(true);
+  int np = std::max(1, std::min({4, nstates / 12, (int)std::min<size_t>(4, c->prep_budget / per_state)}));
+  const int G0 = voigt_tile_points(0);  // the widest tile; every shape's tile divides it
+  const int tps0 = (int)((nx + G0 - 1) / G0);
+  const VoigtPlan p0 = plan_voigt_sum(true, 0, nx, 1, 0);
+  const int sec = std::min(tps0, std::max((tps0 + 3) / 4, (2 * p0.ctas + p0.nsplit - 1) / p0.nsplit));
+  const int first = (tps0 - sec) / 2;
+  const int64_t x0 = (int64_t)first * G0, x1 = std::min<int64_t>((int64_t)(first + sec) * G0, nx);
+  if (c->tuning == 1) {
+    // probe sweeps in state-equivalents against the call's sweep
+    const double cost = (double)nsh * np * (double)(x1 - x0) / (double)nx;
+    if (cost > 0.1 * nstates) return HK_OK;
+  }
+  std::vector<StateDev> ps(np);
+  for (int k = 0; k < np; ++k) ps[k] = hs[np == 1 ? 0 : (int)((int64_t)k * (nstates - 1) / (np - 1))];
+  CUDA_TRY(c, c->tunework.ensure(np * (sizeof(StateDev) + 2 * sizeof(unsigned long long))));
+  StateDev *tsd = c->tunework.as<StateDev>();
+  unsigned long long *twb = reinterpret_cast<unsigned long long *>(tsd + np);
+  CUDA_TRY(c, cudaMemcpyAsync(tsd, ps.data(), np * sizeof(StateDev), cudaMemcpyHostToDevice, s));
+  CUDA_TRY(c, c->prep.ensure((size_t)np * per_state));
+  CUDA_TRY(c, launch_line_prep(true, c->L, c->g, tsd, np, c->prep.p, twb, s));
+  c->launches += 2;
+  c->tune_ms.assign(nsh, -1.0);
+  int best = 0;
+  for (int v = 0; v < nsh; ++v) {
+    const int G = voigt_tile_points(v);
+    const int t0 = (int)(x0 / G), nt = (int)((x1 - x0 + G - 1) / G);
+    const VoigtPlan pw = plan_voigt_section(true, v, nx, t0, 1, 0);
+    const VoigtPlan pl = plan_voigt_section(true, v, nx, t0, nt, pw.ctas);
+    if (pl.nsplit > 1) {
+      CUDA_TRY(c, c->vpart.ensure(pl.partial_doubles * sizeof(double)));
+      CUDA_TRY(c, c->vcnt.ensure(pl.counters * sizeof(unsigned)));
+    }
+    CUDA_TRY(c, launch_voigt_sum(true, pw, c->prep.p, c->L.nu0, n, c->g, tsd, c->ticket.as<unsigned>(),
+                                 c->vpart.as<double>(), c->vcnt.as<unsigned>(), Kd, nx, s));
+    double ms_v = 0.0;
+    for (int k = 0; k < np; ++k) {
+      const char *pk = static_cast<const char *>(c->prep.p) + (size_t)k * per_state;
+      CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
+      CUDA_TRY(c, launch_voigt_sum(true, pl, pk, c->L.nu0, n, c->g, tsd + k, c->ticket.as<unsigned>(),
+                                   c->vpart.as<double>(), c->vcnt.as<unsigned>(), Kd + (size_t)k * nx,
+                                   nx, s));
+      CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
+      CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
+      float ms = 0.f;
+      CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+      ms_v += ms;
+    }
+    c->launches += 1 + np;
+    c->tune_ms[v] = ms_v;
+    c->voigt_ms_acc += ms_v;  // probe sweeps count as line-sum time
+    if (v == 0 || ms_v < c->tune_ms[best]) best = v;  // ties keep the lower shape
+  }
+  c->tuned_shape = best;
+  c->tuned = true;
   return HK_OK;
 }
 
@@ -557,21 +651,25 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   // budget; each batch is one prep launch and one persistent Voigt launch.
   const bool mixed = precision == HK_PRECISION_MIXED;
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
-  int batch = (int)std::max<size_t>(1, c->prep_budget / per_state);
-  const int nsplit = voigt_nsplit(nx);
-  if (nsplit > 1) {
-    // split tiles keep one partial row per part: bound that scratch too
-    const size_t part_per_state = (size_t)((nx + voigt_tile_points() - 1) / voigt_tile_points()) *
-                                  nsplit * voigt_tile_points() * sizeof(double);
-    batch = std::min(batch, (int)std::max<size_t>(1, c->part_budget / part_per_state));
-  }
-  batch = std::min(batch, nstates);
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
   c->voigt_ms_acc_only = false;
   c->launches = 0;
+  if (mixed && c->tuning != 0 && !c->tuned && per_state <= c->prep_budget && c->nlines > 0)
+    if ((st = tune_shape(c, nstates, hs, Kd, s)) != HK_OK) return st;
+  const int shape = shape_for(c, mixed);
+  c->last_shape = shape;
+  int batch = (int)std::max<size_t>(1, c->prep_budget / per_state);
+  const int nsplit = voigt_nsplit(nx, shape);
+  if (nsplit > 1) {
+    // split tiles keep one partial row per part: bound that scratch too
+    const int G = voigt_tile_points(shape);
+    const size_t part_per_state = (size_t)((nx + G - 1) / G) * nsplit * G * sizeof(double);
+    batch = std::min(batch, (int)std::max<size_t>(1, c->part_budget / part_per_state));
+  }
+  batch = std::min(batch, nstates);
   if (per_state > c->prep_budget) {
-    if ((st = opacity_sectioned(c, nstates, mixed, Kd, s)) != HK_OK) return st;
+    if ((st = opacity_sectioned(c, nstates, mixed, shape, Kd, s)) != HK_OK) return st;
     batch = nstates;  // nothing left for the batched loop
   } else {
     CUDA_TRY(c, c->prep.ensure((size_t)batch * per_state));
@@ -580,7 +678,7 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   unsigned long long *wb = c->wbits.as<unsigned long long>();
   for (int b0 = 0; per_state <= c->prep_budget && b0 < nstates; b0 += batch) {
     const int nb = std::min(batch, nstates - b0);
-    const VoigtPlan plan = plan_voigt_sum(mixed, nx, nb, 0);
+    const VoigtPlan plan = plan_voigt_sum(mixed, shape, nx, nb, 0);
     c->launches += 3;  // line prep, state finalize, Voigt sum
     if (plan.nsplit > 1) {
       CUDA_TRY(c, c->vpart.ensure(plan.partial_doubles * sizeof(double)));
@@ -757,6 +855,43 @@ hk_status hk_set_workspace(hk_ctx *c, double prep_bytes, double part_bytes) {
   return HK_OK;
 }
 
+int hk_num_tile_shapes(void) { return voigt_num_shapes(); }
+
+hk_status hk_tile_shape_info(int shape, int *lines_per_chunk, int *points_per_tile) {
+  if (shape < 0 || shape >= voigt_num_shapes()) return HK_ERR_ARG;
+  if (lines_per_chunk) *lines_per_chunk = voigt_chunk_lines(shape);
+  if (points_per_tile) *points_per_tile = voigt_tile_points(shape);
+  return HK_OK;
+}
+
+hk_status hk_set_tuning(hk_ctx *c, int mode) {
+  if (!c) return HK_ERR_ARG;
+  if (mode < 0 || mode > 2) return fail(c, HK_ERR_ARG, "tuning mode must be 0, 1 or 2");
+  c->tuning = mode;
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_set_tile_shape(hk_ctx *c, int shape) {
+  if (!c) return HK_ERR_ARG;
+  if (shape < 0 || shape >= voigt_num_shapes())
+    return fail(c, HK_ERR_ARG, "tile shape must be 0..%d", voigt_num_shapes() - 1);
+  c->shape_fixed = shape;
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_tuning_result(hk_ctx *c, int *last_shape, int *tuned_shape, double *probe_ms) {
+  if (!c) return HK_ERR_ARG;
+  if (last_shape) *last_shape = c->last_shape;
+  if (tuned_shape) *tuned_shape = c->tuned ? c->tuned_shape : -1;
+  if (probe_ms)
+    for (int v = 0; v < voigt_num_shapes(); ++v)
+      probe_ms[v] = (c->tuned && v < (int)c->tune_ms.size()) ? c->tune_ms[v] : -1.0;
+  ok(c);
+  return HK_OK;
+}
+
 hk_status hk_set_line_scales(hk_ctx *c, const double *s_scale, const double *g_scale) {
   if (!c) return HK_ERR_ARG;
   if (c->nlines == 0 && (s_scale || g_scale)) return fail(c, HK_ERR_STATE, "no lines loaded");
@@ -878,16 +1013,23 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   if (per_state > c->prep_budget)
     return fail(c, HK_ERR_UNSUPPORTED, "one state's line records (%zu B) exceed the workspace (%zu B): "
                 "tables of such lists run through hk_opacity's sectioned path", per_state, c->prep_budget);
+  c->launches = 0;
+  if (mixed && c->tuning != 0 && !c->tuned && c->nlines > 0) {
+    if ((st = tune_shape(c, nstates, hs, K, 0)) != HK_OK) return st;
+    CUDA_TRY(c, cudaDeviceSynchronize());
+  }
+  const int shape = shape_for(c, mixed);
+  c->last_shape = shape;
   int batch = (int)std::max<size_t>(1, c->prep_budget / per_state);
-  const int nsplit = voigt_nsplit(nx);
+  const int nsplit = voigt_nsplit(nx, shape);
   if (nsplit > 1) {
-    const size_t part_per_state = (size_t)((nx + voigt_tile_points() - 1) / voigt_tile_points()) *
-                                  nsplit * voigt_tile_points() * sizeof(double);
+    const int G = voigt_tile_points(shape);
+    const size_t part_per_state = (size_t)((nx + G - 1) / G) * nsplit * G * sizeof(double);
     batch = std::min(batch, (int)std::max<size_t>(1, c->part_budget / part_per_state));
   }
   batch = std::min(batch, nstates);
   CUDA_TRY(c, c->prep.ensure((size_t)batch * per_state));
-  const VoigtPlan plan0 = plan_voigt_sum(mixed, nx, batch, 0);
+  const VoigtPlan plan0 = plan_voigt_sum(mixed, shape, nx, batch, 0);
   if (plan0.nsplit > 1) {
     CUDA_TRY(c, c->vpart.ensure(plan0.partial_doubles * sizeof(double)));
     CUDA_TRY(c, c->vcnt.ensure(plan0.counters * sizeof(unsigned)));
@@ -905,7 +1047,7 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   int64_t kernels = 0;
   for (int b0 = 0; e == cudaSuccess && b0 < nstates; b0 += batch) {
     const int nb = std::min(batch, nstates - b0);
-    const VoigtPlan plan = plan_voigt_sum(mixed, nx, nb, plan0.ctas);
+    const VoigtPlan plan = plan_voigt_sum(mixed, shape, nx, nb, plan0.ctas);
     e = launch_line_prep(mixed, c->L, c->g, sd + b0, nb, c->prep.p, wb + 2 * b0, cs);
     if (e == cudaSuccess)
       e = launch_voigt_sum(mixed, plan, c->prep.p, c->L.nu0, c->nlines, c->g, sd + b0,

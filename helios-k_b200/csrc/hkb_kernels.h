@@ -14,7 +14,11 @@ namespace hkb {
 // minus the kernel's static shared arrays)
 constexpr int KD_SMEM_LIMIT = 225 * 1024;
 
-int voigt_tile_points();
+// Tile shapes of the mixed Voigt kernel: lines per staged chunk x grid points
+// per tile; shape 0 is the default and the plain FP64 form's only shape.
+int voigt_num_shapes();
+int voigt_tile_points(int shape);
+int voigt_chunk_lines(int shape);
 cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream);
 
 // Vector-Jacobian product of one state's opacity (hkb_adjoint.cu): G_d holds
@@ -90,6 +94,8 @@ inline size_t line_prep_bytes(bool mixed) { return mixed ? sizeof(LinePrepF) : s
 // (parts are combined in part order through partial_doubles of scratch and
 // one counter per tile).
 struct VoigtPlan {
+  int shape = 0;  // tile shape (mixed form)
+  int G = 0;      // grid points per tile of that shape
   int tile0 = 0;  // first tile of the launch (a section of one state's grid)
   int tiles_per_state = 0;
   int64_t tiles = 0;
@@ -98,10 +104,11 @@ struct VoigtPlan {
   size_t partial_doubles = 0;
   size_t counters = 0;
 };
-VoigtPlan plan_voigt_sum(bool mixed, int64_t nx, int nstates, int grid_ctas);
-// one state, tiles [tile0, tile0 + ntiles) of its grid
-VoigtPlan plan_voigt_section(bool mixed, int64_t nx, int tile0, int ntiles, int grid_ctas);
-int voigt_nsplit(int64_t nx);  // line-range parts per tile for a grid of nx points
+VoigtPlan plan_voigt_sum(bool mixed, int shape, int64_t nx, int nstates, int grid_ctas);
+// tiles [tile0, tile0 + ntiles) of each state's grid
+VoigtPlan plan_voigt_section(bool mixed, int shape, int64_t nx, int tile0, int ntiles, int grid_ctas);
+// line-range parts per tile for a grid of nx points in tiles of the shape
+int voigt_nsplit(int64_t nx, int shape);
 cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &plan, const void *prep_d,
                              const double *nu0_d, int64_t nlines, const GridDev &g,
                              const StateDev *states_d, unsigned *ticket_d, double *partial_d,

@@ -33,11 +33,33 @@ namespace hkb {
 
 constexpr int HK_WARPS = 8;
 constexpr int HK_THREADS = HK_WARPS * 32;
-constexpr int HK_PPL = 8;                    // points per lane
-constexpr int HK_SLICE = 32 * HK_PPL;        // points per warp
-constexpr int HK_G = HK_WARPS * HK_SLICE;    // points per tile (2048)
-constexpr int HK_CH = 128;                   // lines per staged chunk
-static_assert(HK_G <= 2048, "k * vb_hi must stay exact in FP32 (11 bits)");
+
+// Tile shapes: CH lines per staged chunk x G = 8 warps * 32 lanes * PPL grid
+// points per tile.  The autotuner (hk_set_tuning) picks one per workload;
+// shape 0 is the default.  MINB is the CTAs per SM the register budget is
+// set for (64 registers at 4; 80 at 3, where shared memory allows 3 only).
+template <int CH_, int PPL_, int MINB_>
+struct TileShape {
+  static constexpr int CH = CH_, PPL = PPL_, MINB = MINB_;
+  static constexpr int SLICE = 32 * PPL_;        // points per warp
+  static constexpr int G = HK_WARPS * SLICE;     // points per tile
+  static_assert(G <= 2048, "k * vb_hi must stay exact in FP32 (11 bits)");
+  static_assert(CH % 32 == 0 && CH <= HK_THREADS, "one staging thread per line");
+  static_assert(PPL % 2 == 0, "points are processed in pairs");
+};
+using Shape0 = TileShape<128, 8, 4>;  // default
+using Shape1 = TileShape<256, 8, 3>;
+using Shape2 = TileShape<64, 8, 4>;
+using Shape3 = TileShape<128, 4, 4>;
+using Shape4 = TileShape<256, 4, 4>;
+constexpr int HK_NSHAPES = 5;
+constexpr int HK_SHAPE_CH[HK_NSHAPES] = {Shape0::CH, Shape1::CH, Shape2::CH, Shape3::CH, Shape4::CH};
+constexpr int HK_SHAPE_G[HK_NSHAPES] = {Shape0::G, Shape1::G, Shape2::G, Shape3::G, Shape4::G};
+// the plain FP64 form keeps the default shape
+constexpr int HK_CH = Shape0::CH;
+constexpr int HK_PPL = Shape0::PPL;
+constexpr int HK_SLICE = Shape0::SLICE;
+constexpr int HK_G = Shape0::G;
 
 // Staged line record of the mixed form.  Regions A and B are summed in FP32
 // (flushed into the FP64 per-point sums at least once per chunk of lines)
@@ -88,9 +110,11 @@ constexpr int HK_MAX_LEVEL = 7;
 // region-C denominator tables (8 leading pad floats keep R[m-1-k] of the
 // first line in bounds for predicated reads), and the per-point FP64 sums.
 constexpr int HK_RPAD = 8;
-constexpr size_t HK_SMEM_MIXED = sizeof(RecF) * HK_CH +
-                                 sizeof(float) * (HK_RPAD + HK_CH * HK_C916_MR) +
-                                 sizeof(double) * HK_G;
+template <class SH>
+constexpr size_t smem_mixed() {
+  return sizeof(RecF) * SH::CH + sizeof(float) * (HK_RPAD + SH::CH * HK_C916_MR) +
+         sizeof(double) * SH::G;
+}
 
 struct __align__(16) RecD {
   double nu, iad, y2, y, S1, Sc, ey, pad;
@@ -254,8 +278,9 @@ __device__ __forceinline__ void stage_plain(const LinePrep *__restrict__ P, int6
 // are summed in FP64 into the per-point shared sums cacc.
 enum { HK_CLS_SKIP = 0, HK_CLS_B, HK_CLS_A, HK_CLS_BM, HK_CLS_AM, HK_CLS_G, HK_CLS_W };
 
+template <int SLICE>
 __device__ __forceinline__ int classify(const RecF &r, int wb) {
-  const int we = wb + HK_SLICE;
+  const int we = wb + SLICE;
   const int lo = max(r.i0, wb), hi = min(r.i1, we);
   if (hi <= lo) return HK_CLS_SKIP;
   if (r.flags & HK_F_WEAK) return HK_CLS_W;
@@ -315,11 +340,12 @@ __device__ __forceinline__ bool in_run(int k, int lo, int hi, int c0, int c1) {
 }
 
 // region B only, whole slice
-__device__ __forceinline__ void sweep_B(const RecF &rr, const float2 (&kf)[HK_PPL / 2],
-                                        float2 (&a32)[HK_PPL / 2]) {
+template <int PPL>
+__device__ __forceinline__ void sweep_B(const RecF &rr, const float2 (&kf)[PPL / 2],
+                                        float2 (&a32)[PPL / 2]) {
   const CoefB c = load_coef(rr);
 #pragma unroll
-  for (int q = 0; q < HK_PPL / 2; ++q) {
+  for (int q = 0; q < PPL / 2; ++q) {
     const float2 x = x_pair(c, kf[q]);
     float2 num, inv;
     gh2_pair(c, __fmul2_rn(x, x), num, inv);
@@ -328,14 +354,15 @@ __device__ __forceinline__ void sweep_B(const RecF &rr, const float2 (&kf)[HK_PP
 }
 
 // region B points of [lo, hi) minus region C, by 64-point blocks
+template <int PPL>
 __device__ __forceinline__ void sweep_BM(const RecF &rr, int wb, int lane,
-                                         const float2 (&kf)[HK_PPL / 2],
-                                         float2 (&a32)[HK_PPL / 2]) {
+                                         const float2 (&kf)[PPL / 2],
+                                         float2 (&a32)[PPL / 2]) {
   const CoefB c = load_coef(rr);
-  const int lo = max(rr.i0, wb), hi = min(rr.i1, wb + HK_SLICE);
+  const int lo = max(rr.i0, wb), hi = min(rr.i1, wb + 32 * PPL);
   const int c0 = rr.c0, c1 = rr.c1;
 #pragma unroll
-  for (int q = 0; q < HK_PPL / 2; ++q) {
+  for (int q = 0; q < PPL / 2; ++q) {
     const int blo = wb + 64 * q, bhi = blo + 64;
     const int l2 = max(lo, blo), h2 = min(hi, bhi);
     if (l2 >= h2 || (c0 <= l2 && c1 >= h2)) continue;  // no region-B point
@@ -359,17 +386,17 @@ __device__ __forceinline__ void sweep_BM(const RecF &rr, int wb, int lane,
 }
 
 // region A, whole slice (AM = false) or the points of [lo, hi) (AM = true)
-template <bool AM>
+template <bool AM, int PPL>
 __device__ __forceinline__ void sweep_A(const RecF &rr, int wb, int lane,
-                                        const float2 (&kf)[HK_PPL / 2],
-                                        float2 (&a32)[HK_PPL / 2]) {
+                                        const float2 (&kf)[PPL / 2],
+                                        float2 (&a32)[PPL / 2]) {
   const CoefB c = load_coef(rr);
   const float Yf = rr.y * rr.y;
   const float2 Y = make_float2(Yf, Yf);
   const bool wide = rr.flags & HK_F_WIDE;
-  const int lo = max(rr.i0, wb), hi = min(rr.i1, wb + HK_SLICE);
+  const int lo = max(rr.i0, wb), hi = min(rr.i1, wb + 32 * PPL);
 #pragma unroll
-  for (int q = 0; q < HK_PPL / 2; ++q) {
+  for (int q = 0; q < PPL / 2; ++q) {
     const int blo = wb + 64 * q, bhi = blo + 64;
     bool m0 = true, m1 = true;
     if (AM) {
@@ -400,9 +427,10 @@ __device__ __forceinline__ void sweep_A(const RecF &rr, int wb, int lane,
 // within rounding of r = 6 may take either evaluator (both hold there).
 // Points leave their owning lane here, so the warp syncs before cacc is
 // touched again.
+template <int SLICE>
 __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__ Rj,
                                         double *__restrict__ cacc, int wb, int lane) {
-  const int lo = max(r.c0, wb), hi = min(r.c1, wb + HK_SLICE);
+  const int lo = max(r.c0, wb), hi = min(r.c1, wb + SLICE);
   if (lo >= hi) return;
   const float dh = r.dh, dl = r.dl, vbh = r.vbh, vbl = r.vbl;
   const float y = r.y, iy = r.iy, ey = r.ey, sig1 = r.sig1;
@@ -427,23 +455,23 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
 // A/B boundaries in the slice, and weak lines: per-point window/region
 // tests.  WEAK lines (S1f = 1) add S1 t in FP64 to cacc; the others add
 // S1f t to the FP32 sums.
-template <bool WEAK>
+template <bool WEAK, int PPL>
 __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
-                                        const float2 (&kf)[HK_PPL / 2],
-                                        float2 (&a32)[HK_PPL / 2],
+                                        const float2 (&kf)[PPL / 2],
+                                        float2 (&a32)[PPL / 2],
                                         double *__restrict__ cacc) {
   // the record lives in shared memory like cacc: read it once into registers
   const int i0 = r.i0, i1 = r.i1, b0 = r.b0, b1 = r.b1, c0 = r.c0, c1 = r.c1;
   const float nkc = r.nkc, vb = r.vb, fr = r.fr;
   const float y = r.y;
   const float Yf = y * y;
-  const int we = wb + HK_SLICE;
+  const int we = wb + 32 * PPL;
   if (c0 <= max(i0, wb) && c1 >= min(i1, we)) return;  // region C only
   const float S1f = r.S1f, C1 = r.C1, C0 = r.C0;
   const float D2 = r.D2, D1 = r.D1, D0 = r.D0;
   const double S1w = WEAK ? r.Sc * (double)y * 0.56418958354775628 : 0.0;  // S y / pi
 #pragma unroll
-  for (int p = 0; p < HK_PPL; ++p) {
+  for (int p = 0; p < PPL; ++p) {
     const int k = wb + lane + 32 * p;
     if (k >= i0 && k < i1 && !(k >= c0 && k < c1)) {
       const float kk = (p & 1) ? kf[p >> 1].y : kf[p >> 1].x;
@@ -469,27 +497,28 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
 }
 
 // ------------------------------------------------------------ FP64 sweep
+template <int PPL>
 __device__ __forceinline__ void sweep_plain(const RecD &r, int wb, int lane,
-                                            const double (&xg)[HK_PPL],
-                                            double (&acc)[HK_PPL]) {
-  const int we = wb + HK_SLICE;
+                                            const double (&xg)[PPL],
+                                            double (&acc)[PPL]) {
+  const int we = wb + 32 * PPL;
   if (r.i1 <= wb || r.i0 >= we) return;
   const bool full = r.i0 <= wb && r.i1 >= we;
   if (full && ((r.b0 <= wb && r.c0 >= we) || (r.c1 <= wb && r.b1 >= we))) {
 #pragma unroll
-    for (int p = 0; p < HK_PPL; ++p) {
+    for (int p = 0; p < PPL; ++p) {
       const double x = (xg[p] - r.nu) * r.iad;
       acc[p] += r.S1 * gh2_d(x, r.y2);
     }
   } else if (full && (r.b0 >= we || r.b1 <= wb)) {
 #pragma unroll
-    for (int p = 0; p < HK_PPL; ++p) {
+    for (int p = 0; p < PPL; ++p) {
       const double x = (xg[p] - r.nu) * r.iad;
       acc[p] += r.S1 / (x * x + r.y2);
     }
   } else {
 #pragma unroll
-    for (int p = 0; p < HK_PPL; ++p) {
+    for (int p = 0; p < PPL; ++p) {
       const int k = wb + lane + 32 * p;
       if (k >= r.i0 && k < r.i1) {
         const double x = (xg[p] - r.nu) * r.iad;
@@ -505,41 +534,43 @@ __device__ __forceinline__ void sweep_plain(const RecD &r, int wb, int lane,
 
 // add the FP32 sums of level lev into the FP64 sums (exact unscale) and
 // clear them
-__device__ __forceinline__ void flush_sums(float2 (&a32)[HK_PPL / 2], double *__restrict__ cacc,
+template <int PPL>
+__device__ __forceinline__ void flush_sums(float2 (&a32)[PPL / 2], double *__restrict__ cacc,
                                            int wb, int lane, int s1exp, int lev) {
   const double u = ldexp(1.0, -(s1exp + HK_LEVEL_BITS * lev));
 #pragma unroll
-  for (int p = 0; p < HK_PPL; ++p) {
+  for (int p = 0; p < PPL; ++p) {
     const int k = wb + lane + 32 * p;
     const float v = (p & 1) ? a32[p >> 1].y : a32[p >> 1].x;
     cacc[k] = fma((double)v, u, cacc[k]);
   }
 #pragma unroll
-  for (int q = 0; q < HK_PPL / 2; ++q) a32[q] = make_float2(0.f, 0.f);
+  for (int q = 0; q < PPL / 2; ++q) a32[q] = make_float2(0.f, 0.f);
 }
 
 // ------------------------------------------------------- persistent kernel
-// mixed form: 4 CTAs (32 warps) per SM, 64 registers
-template <bool MIXED>
-__global__ void __launch_bounds__(HK_THREADS, MIXED ? 4 : 2)
+// mixed form: SH::MINB CTAs per SM (4: 32 warps, 64 registers)
+template <bool MIXED, class SH>
+__global__ void __launch_bounds__(HK_THREADS, MIXED ? SH::MINB : 2)
 voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
                  int64_t nlines, GridDev g, const StateDev *__restrict__ states,
                  int tile0, int tiles_per_state, int nsplit, int total_tickets,
                  unsigned *__restrict__ ticket, double *__restrict__ partial,
                  unsigned *__restrict__ tile_cnt, double *__restrict__ K, int64_t k_stride) {
   using Rec = typename std::conditional<MIXED, RecF, RecD>::type;
+  constexpr int CH = SH::CH, PPL = SH::PPL, SLICE = SH::SLICE, G = SH::G;
   extern __shared__ __align__(16) unsigned char smem_dyn[];
   Rec *rec = reinterpret_cast<Rec *>(smem_dyn);
-  float *Rtab = reinterpret_cast<float *>(smem_dyn + sizeof(Rec) * HK_CH) + HK_RPAD;
-  double *cacc = reinterpret_cast<double *>(smem_dyn + sizeof(Rec) * HK_CH +
-                                            sizeof(float) * (HK_RPAD + HK_CH * HK_C916_MR));
+  float *Rtab = reinterpret_cast<float *>(smem_dyn + sizeof(Rec) * CH) + HK_RPAD;
+  double *cacc = reinterpret_cast<double *>(smem_dyn + sizeof(Rec) * CH +
+                                            sizeof(float) * (HK_RPAD + CH * HK_C916_MR));
   __shared__ int s_ticket, s_last;
-  __shared__ int s_kcnt[HK_CH / 32][HK_NKEY];  // staged lines per (staging warp, key)
+  __shared__ int s_kcnt[CH / 32][HK_NKEY];  // staged lines per (staging warp, key)
   __shared__ long long s_L0, s_L1;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  const int wb = warp * HK_SLICE;
+  const int wb = warp * SLICE;
 
   for (;;) {
     if (tid == 0) s_ticket = (int)atomicAdd(ticket, 1u);
@@ -554,8 +585,8 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
     const StateDev &st = states[s];
     const LinePrep *P = reinterpret_cast<const LinePrep *>(prep) + (int64_t)s * nlines;
     const LinePrepF *PF = reinterpret_cast<const LinePrepF *>(prep) + (int64_t)s * nlines;
-    const int64_t g0 = (int64_t)(tile0 + tile) * HK_G;
-    const int64_t g1 = min(g0 + (int64_t)HK_G, g.nx);
+    const int64_t g0 = (int64_t)(tile0 + tile) * G;
+    const int64_t g1 = min(g0 + (int64_t)G, g.nx);
     if (warp == 0) {
       const double W = st.wmax + st.shift + 2.0 * g.dnu;
       const double xlo = grid_x(g, g0) - W;
@@ -571,11 +602,11 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
     __syncthreads();
     const int64_t L0 = s_L0, L1 = s_L1;
 
-    float2 kf[HK_PPL / 2];   // lane-local point indices, paired {p, p+1}
-    float2 a32[HK_PPL / 2];  // mixed: FP32 sums of the current chunk (scaled)
-    double acc[HK_PPL], xg[HK_PPL];
+    float2 kf[PPL / 2];   // lane-local point indices, paired {p, p+1}
+    float2 a32[PPL / 2];  // mixed: FP32 sums of the current chunk (scaled)
+    double acc[PPL], xg[PPL];
 #pragma unroll
-    for (int p = 0; p < HK_PPL; ++p) {
+    for (int p = 0; p < PPL; ++p) {
       const int k = wb + lane + 32 * p;
       acc[p] = 0.0;
       if (MIXED) {
@@ -592,27 +623,27 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
       }
     }
 
-    // Chunk c holds the lines L0 + c + q*nch (q < HK_CH): every chunk spans
+    // Chunk c holds the lines L0 + c + q*nch (q < CH): every chunk spans
     // the tile's whole line range, so the costly region-C points of its
     // lines fall into all warp slices instead of one or two (consecutive
     // nu-sorted lines would put a chunk's line cores into a single slice
     // and leave the other warps idle at the barrier).
     const int64_t nL = L1 - L0;
-    const int64_t nch = (nL + HK_CH - 1) / HK_CH;
+    const int64_t nch = (nL + CH - 1) / CH;
     const int64_t c_begin = nch * part / nsplit, c_end = nch * (part + 1) / nsplit;
     int lcur = 0;  // strength level held in a32 (warp-uniform)
     for (int64_t c = c_begin; c < c_end; ++c) {
       const int cnt = (int)((nL - c + nch - 1) / nch);
       if (MIXED) {
         // build the records, then place them sorted by key (stable counting
-        // sort over the HK_CH / 32 staging warps), so a warp's 32-line
+        // sort over the CH / 32 staging warps), so a warp's 32-line
         // groups mostly hold one strength level
         // (the key pass keeps no record: the record is rebuilt after the
         // scan rather than held in registers across the barrier)
         int key = HK_NKEY, rank = 0;
         const int64_t l = L0 + c + (int64_t)tid * nch;
         if (tid < cnt) key = line_key(PF, l, g0, g1, st.s1exp);
-        if (tid < HK_CH) {
+        if (tid < CH) {
           const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
           for (int v = 0; v < HK_NKEY; ++v) {
@@ -626,7 +657,7 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
           int pos = rank;
           for (int v = 0; v < key; ++v)
 #pragma unroll
-            for (int w = 0; w < HK_CH / 32; ++w) pos += s_kcnt[w][v];
+            for (int w = 0; w < CH / 32; ++w) pos += s_kcnt[w][v];
           for (int w = 0; w < warp; ++w) pos += s_kcnt[w][key];
           RecF r;
           stage_mixed(PF, g, l, g0, g1, st.s1exp, key, r);
@@ -641,7 +672,7 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
         const RecF *rf = reinterpret_cast<const RecF *>(rec);
         for (int g32 = 0; g32 < cnt; g32 += 32) {
           const int j = g32 + lane;
-          const int cls = (j < cnt) ? classify(rf[j], wb) : HK_CLS_SKIP;
+          const int cls = (j < cnt) ? classify<SLICE>(rf[j], wb) : HK_CLS_SKIP;
           const int lev = (j < cnt) ? (rf[j].flags >> 8) : 0;
           const unsigned bB = __ballot_sync(0xffffffffu, cls == HK_CLS_B);
           const unsigned bA = __ballot_sync(0xffffffffu, cls == HK_CLS_A);
@@ -655,7 +686,7 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
             // the FP32 sums) only when none of them is left
             unsigned m = __ballot_sync(0xffffffffu, lev == lcur) & live;
             if (m == 0u) {
-              flush_sums(a32, cacc, wb, lane, st.s1exp, lcur);
+              flush_sums<PPL>(a32, cacc, wb, lane, st.s1exp, lcur);
               lcur = __shfl_sync(0xffffffffu, lev, __ffs(live) - 1);
               m = __ballot_sync(0xffffffffu, lev == lcur) & live;
             }
@@ -664,43 +695,43 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
             while (mB) {
               const int b = __ffs(mB) - 1;
               mB &= mB - 1;
-              sweep_B(rf[g32 + b], kf, a32);
+              sweep_B<PPL>(rf[g32 + b], kf, a32);
             }
             while (mA) {
               const int b = __ffs(mA) - 1;
               mA &= mA - 1;
-              sweep_A<false>(rf[g32 + b], wb, lane, kf, a32);
+              sweep_A<false, PPL>(rf[g32 + b], wb, lane, kf, a32);
             }
             while (mBM) {
               const int b = __ffs(mBM) - 1;
               mBM &= mBM - 1;
-              sweep_BM(rf[g32 + b], wb, lane, kf, a32);
-              sweep_C(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
+              sweep_BM<PPL>(rf[g32 + b], wb, lane, kf, a32);
+              sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
             }
             while (mAM) {
               const int b = __ffs(mAM) - 1;
               mAM &= mAM - 1;
-              sweep_A<true>(rf[g32 + b], wb, lane, kf, a32);
+              sweep_A<true, PPL>(rf[g32 + b], wb, lane, kf, a32);
             }
             while (mG) {
               const int b = __ffs(mG) - 1;
               mG &= mG - 1;
-              sweep_G<false>(rf[g32 + b], wb, lane, kf, a32, cacc);
-              sweep_C(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
+              sweep_G<false, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc);
+              sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
             }
           }
           while (mW) {
             const int b = __ffs(mW) - 1;
             mW &= mW - 1;
-            sweep_G<true>(rf[g32 + b], wb, lane, kf, a32, cacc);
-            sweep_C(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
+            sweep_G<true, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc);
+            sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
           }
         }
         // at most one chunk of lines per FP32 sum
-        flush_sums(a32, cacc, wb, lane, st.s1exp, lcur);
+        flush_sums<PPL>(a32, cacc, wb, lane, st.s1exp, lcur);
       } else {
         for (int j = 0; j < cnt; ++j)
-          sweep_plain(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc);
+          sweep_plain<PPL>(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc);
       }
       __syncthreads();
     }
@@ -708,7 +739,7 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
     double *Ks = K + (int64_t)s * k_stride;
     if (nsplit == 1) {
 #pragma unroll
-      for (int p = 0; p < HK_PPL; ++p) {
+      for (int p = 0; p < PPL; ++p) {
         const int k = wb + lane + 32 * p;
         const int64_t gi = g0 + k;
         if (MIXED) acc[p] = cacc[k];
@@ -718,9 +749,9 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
       // Split tile: publish this part's sums; the CTA that completes the
       // tile's count adds the parts in part order (the result does not
       // depend on which CTA ran which part or when).
-      double *pt = partial + ((int64_t)tt * nsplit + part) * HK_G;
+      double *pt = partial + ((int64_t)tt * nsplit + part) * G;
 #pragma unroll
-      for (int p = 0; p < HK_PPL; ++p) {
+      for (int p = 0; p < PPL; ++p) {
         const int k = wb + lane + 32 * p;
         if (MIXED) acc[p] = cacc[k];
         pt[k] = acc[p];
@@ -731,12 +762,12 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
       __syncthreads();
       if (s_last) {
         __threadfence();
-        const double *p0 = partial + (int64_t)tt * nsplit * HK_G;
+        const double *p0 = partial + (int64_t)tt * nsplit * G;
 #pragma unroll
-        for (int p = 0; p < HK_PPL; ++p) {
+        for (int p = 0; p < PPL; ++p) {
           const int k = wb + lane + 32 * p;
           double sum = 0.0;
-          for (int j = 0; j < nsplit; ++j) sum += __ldcg(p0 + (int64_t)j * HK_G + k);
+          for (int j = 0; j < nsplit; ++j) sum += __ldcg(p0 + (int64_t)j * G + k);
           const int64_t gi = g0 + k;
           if (gi < g1) Ks[gi] = st.kmin + sum;
         }
@@ -813,57 +844,76 @@ cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream) {
 }
 
 // ------------------------------------------------------------- launchers
-int voigt_tile_points() { return HK_G; }
+int voigt_num_shapes() { return HK_NSHAPES; }
+int voigt_tile_points(int shape) { return HK_SHAPE_G[shape < 0 || shape >= HK_NSHAPES ? 0 : shape]; }
+int voigt_chunk_lines(int shape) { return HK_SHAPE_CH[shape < 0 || shape >= HK_NSHAPES ? 0 : shape]; }
 
-static int voigt_ctas(bool mixed) {
+// Calls f(kernel, dynamic shared memory) for the kernel of (precision,
+// shape); the plain FP64 form has the default shape only.
+template <class F>
+static cudaError_t with_kernel(bool mixed, int shape, F &&f) {
+  using KFn = void (*)(const void *, const double *, int64_t, GridDev, const StateDev *, int, int,
+                       int, int, unsigned *, double *, unsigned *, double *, int64_t);
+  if (!mixed) return f((KFn)voigt_sum_kernel<false, Shape0>, sizeof(RecD) * Shape0::CH);
+  switch (shape) {
+    case 0: return f((KFn)voigt_sum_kernel<true, Shape0>, smem_mixed<Shape0>());
+    case 1: return f((KFn)voigt_sum_kernel<true, Shape1>, smem_mixed<Shape1>());
+    case 2: return f((KFn)voigt_sum_kernel<true, Shape2>, smem_mixed<Shape2>());
+    case 3: return f((KFn)voigt_sum_kernel<true, Shape3>, smem_mixed<Shape3>());
+    case 4: return f((KFn)voigt_sum_kernel<true, Shape4>, smem_mixed<Shape4>());
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static int voigt_ctas(bool mixed, int shape) {
   int dev = 0, nsm = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const size_t smem = mixed ? HK_SMEM_MIXED : sizeof(RecD) * HK_CH;
-  if (mixed) {
-    cudaFuncSetAttribute(voigt_sum_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, voigt_sum_kernel<true>, HK_THREADS, smem);
-  } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, voigt_sum_kernel<false>, HK_THREADS, smem);
-  }
+  with_kernel(mixed, shape, [&](auto kfn, size_t smem) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, HK_THREADS, smem);
+  });
   return nsm * (per_sm < 1 ? 1 : per_sm);
 }
 
 // Tiles are split along their line range when a state has few tiles: one
 // tile's sweep lasts ~1/3 of a 1e7-line state, so an unsplit 1465-tile grid
 // ends in a last wave that leaves most of the GPU idle for that long.  The
-// split depends on the grid only (HK_TICKETS_PER_STATE, about 8 tickets per
-// resident CTA of a 148-SM B200 at 4 CTAs/SM), never on the batch or the
-// device, so one state's K is bit-identical however it is batched.
+// split depends on the grid and the tile shape only (HK_TICKETS_PER_STATE,
+// about 8 tickets per resident CTA of a 148-SM B200 at 4 CTAs/SM), never on
+// the batch or the device, so one state's K is bit-identical however it is
+// batched.
 constexpr int HK_TICKETS_PER_STATE = 4736;
 constexpr int HK_MAX_SPLIT = 8;
 
-int voigt_nsplit(int64_t nx) {
-  const int64_t tps = (nx + HK_G - 1) / HK_G;
+int voigt_nsplit(int64_t nx, int shape) {
+  const int G = voigt_tile_points(shape);
+  const int64_t tps = (nx + G - 1) / G;
   if (tps <= 0) return 1;
   return (int)std::min<int64_t>(HK_MAX_SPLIT,
                                 std::max<int64_t>(1, (HK_TICKETS_PER_STATE + tps - 1) / tps));
 }
 
-VoigtPlan plan_voigt_section(bool mixed, int64_t nx, int tile0, int ntiles, int grid_ctas) {
+VoigtPlan plan_voigt_section(bool mixed, int shape, int64_t nx, int tile0, int ntiles, int grid_ctas) {
   VoigtPlan pl;
+  pl.shape = mixed ? shape : 0;
+  pl.G = voigt_tile_points(pl.shape);
   pl.tile0 = tile0;
   pl.tiles_per_state = ntiles;
   pl.tiles = ntiles;
-  pl.ctas = grid_ctas > 0 ? grid_ctas : voigt_ctas(mixed);
-  pl.nsplit = voigt_nsplit(nx);
-  pl.partial_doubles = pl.nsplit > 1 ? (size_t)pl.tiles * pl.nsplit * HK_G : 0;
+  pl.ctas = grid_ctas > 0 ? grid_ctas : voigt_ctas(mixed, pl.shape);
+  pl.nsplit = voigt_nsplit(nx, pl.shape);
+  pl.partial_doubles = pl.nsplit > 1 ? (size_t)pl.tiles * pl.nsplit * pl.G : 0;
   pl.counters = pl.nsplit > 1 ? (size_t)pl.tiles : 0;
   return pl;
 }
 
-VoigtPlan plan_voigt_sum(bool mixed, int64_t nx, int nstates, int grid_ctas) {
-  VoigtPlan pl;
-  pl.tiles_per_state = (int)((nx + HK_G - 1) / HK_G);
+VoigtPlan plan_voigt_sum(bool mixed, int shape, int64_t nx, int nstates, int grid_ctas) {
+  const int G = voigt_tile_points(mixed ? shape : 0);
+  VoigtPlan pl = plan_voigt_section(mixed, shape, nx, 0, (int)((nx + G - 1) / G), grid_ctas);
   pl.tiles = (int64_t)pl.tiles_per_state * nstates;
-  pl.ctas = grid_ctas > 0 ? grid_ctas : voigt_ctas(mixed);
-  pl.nsplit = voigt_nsplit(nx);
-  pl.partial_doubles = pl.nsplit > 1 ? (size_t)pl.tiles * pl.nsplit * HK_G : 0;
+  pl.partial_doubles = pl.nsplit > 1 ? (size_t)pl.tiles * pl.nsplit * pl.G : 0;
   pl.counters = pl.nsplit > 1 ? (size_t)pl.tiles : 0;
   return pl;
 }
@@ -875,6 +925,7 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d
                              cudaStream_t stream) {
   const int64_t total64 = pl.tiles * pl.nsplit;
   if (total64 > 0x7fffffff) return cudaErrorInvalidValue;
+  if (pl.G != voigt_tile_points(pl.shape)) return cudaErrorInvalidValue;
   const int total = (int)total64;
   cudaError_t e = cudaMemsetAsync(ticket_d, 0, sizeof(unsigned), stream);
   if (e != cudaSuccess) return e;
@@ -884,17 +935,18 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d
     e = cudaMemsetAsync(tile_cnt_d, 0, sizeof(unsigned) * pl.counters, stream);
     if (e != cudaSuccess) return e;
   }
-  const size_t smem = mixed ? HK_SMEM_MIXED : sizeof(RecD) * HK_CH;
   const int ctas = (int)std::min<int64_t>(pl.ctas, total);
-  if (mixed)
-    voigt_sum_kernel<true><<<ctas, HK_THREADS, smem, stream>>>(
-        prep_d, nu0_d, nlines, g, states_d, pl.tile0, pl.tiles_per_state, pl.nsplit, total, ticket_d,
-        partial_d, tile_cnt_d, K_d, k_stride);
-  else
-    voigt_sum_kernel<false><<<ctas, HK_THREADS, smem, stream>>>(
-        prep_d, nu0_d, nlines, g, states_d, pl.tile0, pl.tiles_per_state, pl.nsplit, total, ticket_d,
-        partial_d, tile_cnt_d, K_d, k_stride);
-  return cudaGetLastError();
+  e = with_kernel(mixed, pl.shape, [&](auto kfn, size_t smem) {
+    if (smem > 48 * 1024) {
+      const cudaError_t ea = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (ea != cudaSuccess) return ea;
+    }
+    kfn<<<ctas, HK_THREADS, smem, stream>>>(prep_d, nu0_d, nlines, g, states_d, pl.tile0,
+                                            pl.tiles_per_state, pl.nsplit, total, ticket_d,
+                                            partial_d, tile_cnt_d, K_d, k_stride);
+    return cudaGetLastError();
+  });
+  return e;
 }
 
 cudaError_t launch_profile_eval(int64_t n, const double *x_d, const double *y_d,

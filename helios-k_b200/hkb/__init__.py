@@ -82,6 +82,11 @@ def lib():
             "hk_table_kernels": (_i64, [_p]),
             "hk_last_launches": (_i64, [_p]),
             "hk_count_pairs": (_i, [_p, _d, _d, _p]),
+            "hk_num_tile_shapes": (_i, []),
+            "hk_tile_shape_info": (_i, [_i, _p, _p]),
+            "hk_set_tuning": (_i, [_p, _i]),
+            "hk_set_tile_shape": (_i, [_p, _i]),
+            "hk_tuning_result": (_i, [_p, _p, _p, _p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -241,6 +246,23 @@ class Context:
                                  _ptr(res["recon"]), int(outputs_on_device), sh))
         return res
 
+    # ----------------------------------------------------- tile shapes
+    def set_tuning(self, mode):
+        """0: fixed tile shape; 1: tune when it pays (tables, batches);
+        2: tune on the first mixed call of a workload."""
+        self._chk(lib().hk_set_tuning(self._h, int(mode)))
+
+    def set_tile_shape(self, shape):
+        self._chk(lib().hk_set_tile_shape(self._h, int(shape)))
+
+    def tuning_result(self):
+        """(shape of the last mixed call, tuned shape or -1, probe ms per shape)."""
+        a = np.zeros(1, np.int32)
+        b = np.zeros(1, np.int32)
+        ms = np.zeros(num_tile_shapes(), np.float64)
+        self._chk(lib().hk_tuning_result(self._h, _ptr(a), _ptr(b), _ptr(ms)))
+        return int(a[0]), int(b[0]), ms
+
     def set_workspace(self, prep_bytes=24 * 2**30, part_bytes=4 * 2**30):
         """Workspace budgets; states above the first run in grid sections."""
         self._chk(lib().hk_set_workspace(self._h, float(prep_bytes), float(part_bytes)))
@@ -349,5 +371,20 @@ def _stream_handle(stream, device_io):
 
 
 def tile_points() -> int:
+    """Grid points per tile of the default shape."""
     return int(lib().hk_tile_points())
+
+
+def num_tile_shapes() -> int:
+    return int(lib().hk_num_tile_shapes())
+
+
+def tile_shape(shape):
+    """(lines per staged chunk, grid points per tile) of a tile shape."""
+    a = np.zeros(1, np.int32)
+    b = np.zeros(1, np.int32)
+    st = lib().hk_tile_shape_info(int(shape), _ptr(a), _ptr(b))
+    if st != HK_OK:
+        raise HkError(st, "tile shape %d out of range" % shape)
+    return int(a[0]), int(b[0])
 

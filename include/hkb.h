@@ -171,6 +171,31 @@ hk_status hk_kdist_noalloc(const double *K, int nstates, int64_t nx, int nbins, 
  * records exceed the first run in grid sections (bit-identical K). */
 hk_status hk_set_workspace(hk_ctx *ctx, double prep_bytes, double part_bytes);
 
+/* ------------------------------------------------------ tile shapes */
+
+/* The mixed Voigt kernel runs in one of hk_num_tile_shapes() tile shapes:
+ * lines per staged chunk x grid points per tile (shape 0, the default: 128 x
+ * 2048).  The shape changes only the order of the FP64 additions (results
+ * differ in the last bits, within the same error bound); the plain FP64 form
+ * always uses shape 0.  Replaces the reference's kernel self-tuning
+ * (doTuning, heliosk.cu:1363-1705; tile widths nkA..nkC, heliosk.cu:968-982). */
+int hk_num_tile_shapes(void);
+hk_status hk_tile_shape_info(int shape, int *lines_per_chunk, int *points_per_tile);
+
+/* mode 0: the fixed shape (hk_set_tile_shape, default 0).
+ * mode 1: tune when the probes cost at most a tenth of the call's sweep
+ *         (tables and large batches; single states keep the fixed shape).
+ * mode 2: tune on the first mixed call after lines, grid or options change.
+ * Tuning times each shape on up to 4 probe states of the call over a
+ * section of the grid and keeps the fastest until lines, grid or options
+ * change.  hk_table_build tunes before recording its graph. */
+hk_status hk_set_tuning(hk_ctx *ctx, int mode);
+hk_status hk_set_tile_shape(hk_ctx *ctx, int shape);
+/* last_shape: the shape of the last mixed call; tuned_shape: the tuner's
+ * choice (-1 if not tuned); probe_ms[hk_num_tile_shapes()] (optional): the
+ * probe time per shape (-1 if not tuned). */
+hk_status hk_tuning_result(hk_ctx *ctx, int *last_shape, int *tuned_shape, double *probe_ms);
+
 /* ----------------------------------------------------------- adjoint */
 
 /* Optional per-line multipliers, in load order (host arrays of
