@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hitemp",
-                    choices=["hitemp", "small", "table", "hitemp_sparse", "adjoint", "exomol"])
+                    choices=["hitemp", "small", "table", "table_sparse", "hitemp_sparse", "adjoint",
+                             "exomol"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -68,6 +69,15 @@ def workload(name):
         T, P = synth.table_states()
         W["T"], W["P"] = list(T), list(P)
         W["label"] = "tp-table-1e7-lines-600-states"
+    elif name == "table_sparse":
+        # 20 states spread over the T-P table on a 1e6-line list: K (20 x 3e6
+        # FP64, 480 MB) is larger than L2, the line records 2.2 GB -- the
+        # profiling case of the line prep and the per-bin sort/fit
+        W = dict(synth.WORKLOADS["hitemp_sparse"])
+        T, P = synth.table_states()
+        sub = np.linspace(0, len(T) - 1, 20).astype(int)
+        W["T"], W["P"] = list(np.asarray(T)[sub]), list(np.asarray(P)[sub])
+        W["label"] = "tp-subtable-1e6-lines-20-states"
     elif name == "exomol":
         W = dict(synth.WORKLOADS["exomol"])
         T, P = synth.exomol_states()

@@ -2,7 +2,7 @@
 //
 // One CTA per (state, bin) does the whole post-processing chain of
 // heliosk.cu:2046-2193 on the bin's values while they sit in shared memory:
-//   sort (bitonic, total order on the FP64 bit patterns)  heliosk.cu:2046-2051
+//   sort (total order on the FP64 bit patterns)          heliosk.cu:2046-2051
 //   findCut                                              resample.h:362-388
 //   rescale(+1), copyK2                                  resample.h:397-461
 //   lnK                                                  resample.h:472-481
@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cub/block/block_merge_sort.cuh>
 
 #include "hkb_kernels.h"
 #include "hkb_types.h"
@@ -55,6 +56,21 @@ __device__ double block_max(double v, double *red) {
   const int nw = blockDim.x >> 5;
   double t = (lane < nw) ? red[lane] : 0.0;
   for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+  return t;
+}
+
+// block-wide sum with one barrier: red2 holds two 32-entry buffers used in
+// turn by consecutive calls (a thread may start the next call's write while
+// others still read this call's buffer, never the same buffer)
+__device__ __forceinline__ double block_sum1(double v, double *red2, int parity) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  double *red = red2 + 32 * parity;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  double t = (lane < nw) ? red[lane] : 0.0;
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
   return t;
 }
 
@@ -126,12 +142,25 @@ struct KdistArgs {
   int use_smem;
 };
 
+struct KeyLess {
+  __device__ __forceinline__ bool operator()(uint64_t x, uint64_t y) const { return x < y; }
+};
+
+// IPT > 0: the bin is sorted in registers, IPT keys per thread, by a block
+// merge sort (CUB's BlockMergeSort: per-thread sort, then log2(1024) rounds of
+// merge-path merges through shared memory) -- O(n log n) comparisons where
+// the bitonic network needs O(n log^2 n); its tile (1024 IPT + 1 keys) uses
+// the key array.  IPT = 0: bitonic network, one shared-memory or global pass
+// per stage (bins the merge sort does not hold).  The sorted keys are the
+// same either way: the total order of the FP64 bit patterns has no ties
+// between distinct values.
+template <int IPT>
 __global__ void __launch_bounds__(KD_THREADS)
 kdist_kernel(KdistArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double red[32];
+  __shared__ double red[64];
   __shared__ int s_trans;
-  __shared__ double s_c[KD_MAX_NC];
+  __shared__ double s_c[KD_MAX_NC], s_cv[KD_MAX_NC], s_d[KD_MAX_NC];
   const int b = blockIdx.x, s = blockIdx.y;
   const int nxb = a.nxb, P2 = a.pow2;
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -146,27 +175,54 @@ kdist_kernel(KdistArgs a) {
     work = a.scratch + slot + P2;
   }
   const double *src = a.K + (int64_t)s * a.k_stride + (int64_t)b * nxb;
-  for (int i = tid; i < P2; i += nt)
-    keys[i] = (i < nxb) ? f2key(src[i]) : 0xffffffffffffffffull;
+  constexpr uint64_t KEY_END = 0xffffffffffffffffull;  // after every key of a value
+  if (IPT > 0) {
+    // coalesced into shared memory, then blocked into registers
+    for (int i = tid; i < nxb; i += nt) keys[i] = f2key(src[i]);
+  } else {
+    for (int i = tid; i < P2; i += nt) keys[i] = (i < nxb) ? f2key(src[i]) : KEY_END;
+  }
+  for (int i = tid; i < a.nc; i += nt) {
+    s_cv[i] = a.Cv[i];
+    s_d[i] = a.D[i];
+  }
   __syncthreads();
 
-  // bitonic sort, ascending
-  for (int size = 2; size <= P2; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int i = tid; i < (P2 >> 1); i += nt) {
-        const int pos = 2 * i - (i & (stride - 1));
-        const int q = pos + stride;
-        const uint64_t x = keys[pos], y = keys[q];
-        const bool up = (pos & size) == 0;
-        if ((x > y) == up) {
-          keys[pos] = y;
-          keys[q] = x;
-        }
-      }
-      __syncthreads();
+  // sort, ascending
+  if (IPT > 0) {
+    constexpr int NI = IPT > 0 ? IPT : 1;
+    using Sorter = cub::BlockMergeSort<uint64_t, KD_THREADS, NI>;
+    uint64_t v[NI];
+#pragma unroll
+    for (int i = 0; i < NI; ++i) {
+      const int k = tid * NI + i;
+      v[i] = k < nxb ? keys[k] : KEY_END;
     }
+    __syncthreads();  // the tile storage below overlays keys[]
+    Sorter(*reinterpret_cast<typename Sorter::TempStorage *>(keys)).Sort(v, KeyLess(), nxb, KEY_END);
+#pragma unroll
+    for (int i = 0; i < NI; ++i) {
+      const int k = tid * NI + i;
+      if (k < nxb) work[k] = key2f(v[i]);
+    }
+  } else {
+    for (int size = 2; size <= P2; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int i = tid; i < (P2 >> 1); i += nt) {
+          const int pos = 2 * i - (i & (stride - 1));
+          const int q = pos + stride;
+          const uint64_t x = keys[pos], y = keys[q];
+          const bool up = (pos & size) == 0;
+          if ((x > y) == up) {
+            keys[pos] = y;
+            keys[q] = x;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int i = tid; i < nxb; i += nt) work[i] = key2f(keys[i]);
   }
-  for (int i = tid; i < nxb; i += nt) work[i] = key2f(keys[i]);
   __syncthreads();
   if (a.sorted) {
     double *dst = a.sorted + (int64_t)s * a.k_stride + (int64_t)b * nxb;
@@ -215,26 +271,37 @@ kdist_kernel(KdistArgs a) {
   for (int j = tid; j < nxb; j += nt) work[j] = log(work[j] * a.unitScale);
   __syncthreads();
 
-  // leastSquare_kernel: Q^T b with the first nc-1 reflections
+  // leastSquare_kernel: Q^T b with the first nc-1 reflections.  Thread tid
+  // owns the bin elements k = tid + n nt (k >= j) in every reflection, so a
+  // reflection needs only its block sum's barrier.
   const int nc = a.nc;
   for (int j = 0; j < nc - 1; ++j) {
     const double *vj = a.V + (int64_t)nxb * j;
     double dot = 0.0;
-    for (int k = j + tid; k < nxb; k += nt) dot = __fma_rn(vj[k], work[k], dot);
-    dot = block_sum(dot, red);
-    const double t = dot / a.Cv[j];
-    for (int k = j + tid; k < nxb; k += nt) work[k] = __fma_rn(-t, vj[k], work[k]);
-    __syncthreads();
+    for (int k = tid; k < nxb; k += nt)
+      if (k >= j) dot = __fma_rn(vj[k], work[k], dot);
+    dot = block_sum1(dot, red, j & 1);
+    const double t = dot / s_cv[j];
+    for (int k = tid; k < nxb; k += nt)
+      if (k >= j) work[k] = __fma_rn(-t, vj[k], work[k]);
   }
+  // the R factor's rows used by the back-substitution, copied in parallel
+  // into the (now free) key array when it fits
+  const int lim = nc < 64 ? nc : 64;
+  double *Rb = reinterpret_cast<double *>(keys);
+  const bool rb = nc * lim <= P2;
+  if (rb)
+    for (int q = tid; q < nc * lim; q += nt) Rb[q] = a.V[q / lim + (int64_t)nxb * (q % lim)];
+  __syncthreads();
   if (tid == 0) {
     // back-substitution; the reference's reduction keeps 64 partial sums
-    const int lim = nc < 64 ? nc : 64;
     double *bb = work;
-    bb[nc - 1] /= a.D[nc - 1];
+    bb[nc - 1] /= s_d[nc - 1];
     for (int i = nc - 2; i >= 0; --i) {
       double sum = 0.0;
-      for (int j = i + 1; j < lim; ++j) sum = __fma_rn(a.V[i + (int64_t)nxb * j], bb[j], sum);
-      bb[i] = (bb[i] - sum) / a.D[i];
+      for (int j = i + 1; j < lim; ++j)
+        sum = __fma_rn(rb ? Rb[i * lim + j] : a.V[i + (int64_t)nxb * j], bb[j], sum);
+      bb[i] = (bb[i] - sum) / s_d[i];
     }
     double *co = a.coeff + ((int64_t)s * a.nbins + b) * nc;
     for (int i = 0; i < nc; ++i) {
@@ -324,15 +391,35 @@ cudaError_t launch_kdist(const double *K_d, int64_t k_stride, int nstates,
   const size_t smem = kdist_smem_bytes(nxb);
   a.use_smem = smem <= (size_t)KD_SMEM_LIMIT;
   size_t dyn = a.use_smem ? smem : 0;
+  if (!a.use_smem && scratch_d == nullptr) return cudaErrorInvalidValue;
+  // the merge sort when its tile (1024 IPT + 1 keys) fits the key array
+  int ipt = 0;
   if (a.use_smem) {
-    cudaError_t e = cudaFuncSetAttribute(kdist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-    if (e != cudaSuccess) return e;
-  } else if (scratch_d == nullptr) {
-    return cudaErrorInvalidValue;
+    static const int kIpt[] = {2, 4, 6, 8, 10, 12};
+    for (int q : kIpt)
+      if (q * KD_THREADS >= nxb && (size_t)(q * KD_THREADS + 1) <= (size_t)a.pow2) {
+        ipt = q;
+        break;
+      }
   }
-  dim3 grid(nbins, nstates);
-  kdist_kernel<<<grid, KD_THREADS, dyn, stream>>>(a);
-  return cudaGetLastError();
+  auto run = [&](auto kfn) -> cudaError_t {
+    if (a.use_smem) {
+      cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+      if (e != cudaSuccess) return e;
+    }
+    dim3 grid(nbins, nstates);
+    kfn<<<grid, KD_THREADS, dyn, stream>>>(a);
+    return cudaGetLastError();
+  };
+  switch (ipt) {
+    case 2: return run(kdist_kernel<2>);
+    case 4: return run(kdist_kernel<4>);
+    case 6: return run(kdist_kernel<6>);
+    case 8: return run(kdist_kernel<8>);
+    case 10: return run(kdist_kernel<10>);
+    case 12: return run(kdist_kernel<12>);
+    default: return run(kdist_kernel<0>);
+  }
 }
 
 }  // namespace hkb

@@ -12,7 +12,7 @@ namespace hkb {
 
 // dynamic shared memory budget of one kdist CTA (sm_100: 227 KB per block,
 // minus the kernel's static shared arrays)
-constexpr int KD_SMEM_LIMIT = 225 * 1024;
+constexpr int KD_SMEM_LIMIT = 224 * 1024;
 
 // Tile shapes of the mixed Voigt kernel: lines per staged chunk x grid points
 // per tile; shape 0 is the default and the plain FP64 form's only shape.

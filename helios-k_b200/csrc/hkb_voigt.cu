@@ -1,17 +1,17 @@
 // hkb_voigt.cu -- the Voigt line sum onto the wavenumber grid (sm_100a).
 //
 // One persistent kernel walks (state, grid tile) tickets.  A CTA owns a tile
-// of HK_G consecutive grid points, so every output point has exactly one
+// of G consecutive grid points, so every output point has exactly one
 // writer: there are no atomics on K and no partial-row reduction (the
 // reference's 32 KS_d rows + AddKStreams_kernel, voigt.h:728-742, are gone).
 // For its tile the CTA
 //   1. finds the nu-sorted line range whose cutoff windows can reach the tile
 //      (warp-parallel lower_bound),
-//   2. stages the lines in chunks of HK_CH through shared memory: each thread
+//   2. stages the lines in chunks of CH through shared memory: each thread
 //      loads one line's state record (FP64 parameters and global index
 //      windows, written by line_prep_kernel), clips the windows to the tile
 //      and forms the line-centre offset at the tile start,
-//   3. lets each warp sweep its 256-point slice against every staged line:
+//   3. lets each warp sweep its slice (32 lanes x PPL points) against every staged line:
 //      lane-interleaved points (coalesced stores), register accumulators.
 // Two precisions share the structure:
 //   MIXED: FP32 profile (the offset x from a double-float split of the FP64
@@ -55,11 +55,6 @@ using Shape4 = TileShape<256, 4, 4>;
 constexpr int HK_NSHAPES = 5;
 constexpr int HK_SHAPE_CH[HK_NSHAPES] = {Shape0::CH, Shape1::CH, Shape2::CH, Shape3::CH, Shape4::CH};
 constexpr int HK_SHAPE_G[HK_NSHAPES] = {Shape0::G, Shape1::G, Shape2::G, Shape3::G, Shape4::G};
-// the plain FP64 form keeps the default shape
-constexpr int HK_CH = Shape0::CH;
-constexpr int HK_PPL = Shape0::PPL;
-constexpr int HK_SLICE = Shape0::SLICE;
-constexpr int HK_G = Shape0::G;
 
 // Staged line record of the mixed form.  Regions A and B are summed in FP32
 // (flushed into the FP64 per-point sums at least once per chunk of lines)
