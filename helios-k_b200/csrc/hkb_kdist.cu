@@ -275,15 +275,65 @@ kdist_kernel(KdistArgs a) {
   // owns the bin elements k = tid + n nt (k >= j) in every reflection, so a
   // reflection needs only its block sum's barrier.
   const int nc = a.nc;
-  for (int j = 0; j < nc - 1; ++j) {
-    const double *vj = a.V + (int64_t)nxb * j;
-    double dot = 0.0;
-    for (int k = tid; k < nxb; k += nt)
-      if (k >= j) dot = __fma_rn(vj[k], work[k], dot);
-    dot = block_sum1(dot, red, j & 1);
-    const double t = dot / s_cv[j];
-    for (int k = tid; k < nxb; k += nt)
-      if (k >= j) work[k] = __fma_rn(-t, vj[k], work[k]);
+  if (IPT > 0) {
+    // (nxb <= 1024 IPT) the thread's entries of V's column in registers, the
+    // next column copied asynchronously into the free key array while this
+    // one is used; a thread copies and reads only its own entries
+    constexpr int NI = IPT > 0 ? IPT : 1;
+    double vv[NI];
+    double *pbuf = reinterpret_cast<double *>(keys);
+#pragma unroll
+    for (int n = 0; n < NI; ++n) {
+      const int k = tid + n * KD_THREADS;
+      vv[n] = (k < nxb && nc > 1) ? a.V[k] : 0.0;
+    }
+    for (int j = 0; j < nc - 1; ++j) {
+      const bool more = j + 1 < nc - 1;
+      if (more) {
+        const double *vnext = a.V + (int64_t)nxb * (j + 1);
+#pragma unroll
+        for (int n = 0; n < NI; ++n) {
+          const int k = tid + n * KD_THREADS;
+          if (k < nxb) {
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(pbuf + k);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(vnext + k));
+          }
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+      }
+      double dot = 0.0;
+#pragma unroll
+      for (int n = 0; n < NI; ++n) {
+        const int k = tid + n * KD_THREADS;
+        if (k < nxb && k >= j) dot = __fma_rn(vv[n], work[k], dot);
+      }
+      dot = block_sum1(dot, red, j & 1);
+      const double t = dot / s_cv[j];
+#pragma unroll
+      for (int n = 0; n < NI; ++n) {
+        const int k = tid + n * KD_THREADS;
+        if (k < nxb && k >= j) work[k] = __fma_rn(-t, vv[n], work[k]);
+      }
+      if (more) {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+#pragma unroll
+        for (int n = 0; n < NI; ++n) {
+          const int k = tid + n * KD_THREADS;
+          vv[n] = k < nxb ? pbuf[k] : 0.0;
+        }
+      }
+    }
+  } else {
+    for (int j = 0; j < nc - 1; ++j) {
+      const double *vj = a.V + (int64_t)nxb * j;
+      double dot = 0.0;
+      for (int k = tid; k < nxb; k += nt)
+        if (k >= j) dot = __fma_rn(vj[k], work[k], dot);
+      dot = block_sum1(dot, red, j & 1);
+      const double t = dot / s_cv[j];
+      for (int k = tid; k < nxb; k += nt)
+        if (k >= j) work[k] = __fma_rn(-t, vj[k], work[k]);
+    }
   }
   // the R factor's rows used by the back-substitution, copied in parallel
   // into the (now free) key array when it fits
