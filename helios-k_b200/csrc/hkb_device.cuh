@@ -299,15 +299,27 @@ __device__ __forceinline__ float rcp_fast(float v) {
 }
 
 // per-line constant Sig1(y), FP64 at staging
-__device__ __forceinline__ double c916_sig1(double y) {
+constexpr int HK_SIG1_M = 12;
+__device__ __forceinline__ double c916_e(int m) {
+  const double a = (double)HK_A916_F;
+  return exp(-(a * a * m * m));
+}
+// e[m-1] = c916_e(m) (a line-independent table, e.g. in shared memory)
+__device__ __forceinline__ double c916_sig1_tab(double y, const double *__restrict__ e) {
   const double a = (double)HK_A916_F;
   const double y2 = y * y;
   double s = 0.0;
-  for (int m = 1; m <= 12; ++m) {
+#pragma unroll 1
+  for (int m = 1; m <= HK_SIG1_M; ++m) {
     const double am2 = a * a * m * m;
-    s += exp(-am2) / (am2 + y2);
+    s += e[m - 1] / (am2 + y2);
   }
   return s;
+}
+__device__ __forceinline__ double c916_sig1(double y) {
+  double e[HK_SIG1_M];
+  for (int m = 1; m <= HK_SIG1_M; ++m) e[m - 1] = c916_e(m);
+  return c916_sig1_tab(y, e);
 }
 
 // R[m-1] = 1 / (a^2 m^2 + y^2), m = 1..HK_C916_MR, is a per-line table built

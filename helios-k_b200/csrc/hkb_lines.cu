@@ -87,6 +87,9 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
                  void *__restrict__ out, unsigned long long *__restrict__ wbits) {
   const int s = blockIdx.y;
   const StateDev &st = states[s];
+  __shared__ double s_e916[HK_SIG1_M];  // the line-independent terms of Sig1
+  if (MODE != PREP_STATS && threadIdx.x < HK_SIG1_M) s_e916[threadIdx.x] = c916_e(threadIdx.x + 1);
+  __syncthreads();
   double w_loc = 0.0, s1_loc = 0.0;
   for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < L.n;
        l += (int64_t)gridDim.x * blockDim.x) {
@@ -102,7 +105,7 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
     if (MODE == PREP_STATS) {
     } else if (MIXED) {
       const double ey = hasC ? erfcx(ls.vy) : 1.0;
-      const float sig1 = hasC ? (float)c916_sig1(ls.vy) : 0.f;
+      const float sig1 = hasC ? (float)c916_sig1_tab(ls.vy, s_e916) : 0.f;
       LinePrepF r;
       r.nu = ls.nu;
       r.iad = ls.iad;
@@ -152,7 +155,7 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
       reinterpret_cast<LinePrepF *>(out)[(int64_t)s * L.n + l] = r;
     } else {
       const double ey = hasC ? erfcx(ls.vy) : 1.0;
-      const float sig1 = hasC ? (float)c916_sig1(ls.vy) : 0.f;
+      const float sig1 = hasC ? (float)c916_sig1_tab(ls.vy, s_e916) : 0.f;
       LinePrep r;
       r.nu = ls.nu;
       r.iad = ls.iad;
