@@ -66,8 +66,8 @@ int main(int argc, char **argv) {
   if (p.subLorentzian != "-") return die("Error: sub-Lorentzian profiles are outside this build's path");
   if (p.removePlinth != 0) return die("Error: removePlinth is outside this build's path");
   if (p.profile != 1) return die("Error: only profile = 1 (Voigt) is on this build's path");
-  if (p.doTransmission != 0 || p.doMean != 0)
-    return die("Error: transmission / Planck-Rosseland means are outside this build's path");
+  if (p.doTransmission < 0 || p.doTransmission > 2) return die("Error: doTransmission must be 0, 1 or 2");
+  if (p.doTransmission > 0 && p.nTr < 1) return die("Error: nTr must be >= 1 for the transmission function");
   if (p.nbins < 1) return die("Error: nbins must be >= 1");
 
   const char *mode = p.replaceFiles == 0 ? "a" : "w";
@@ -200,22 +200,52 @@ int main(int argc, char **argv) {
 
   const double t_write = std::chrono::duration<double>(std::chrono::steady_clock::now() - tw0).count();
 
+  // Planck and Rosseland means, heliosk.cu:1953-2020 (on K in internal units)
+  double t_mean = 0.0;
+  if (p.doMean > 0) {
+    std::vector<double> sums((size_t)nP * 4);
+    cudaEventRecord(t0);
+    chk(hk_means(c, nP, Ts.data(), K.data(), 0, sums.data(), 0, nullptr));
+    cudaEventRecord(t1);
+    t_mean = seconds();
+    // sigma T^4 / pi and pi / (4 sigma T^3), the reference's analytic integrals
+    const double sigma = 2.0 * HK_KB * HK_KB * HK_KB * HK_KB /
+                         (HK_H * HK_H * HK_H * HK_C * HK_C * 15.0) * M_PI * M_PI * M_PI * M_PI * M_PI;
+    const double integral1 = sigma * p.T * p.T * p.T * p.T / M_PI;
+    const double integral2 = M_PI / (4.0 * sigma * p.T * p.T * p.T);
+    FILE *f = fopen(("Out_" + p.name + "_mean.dat").c_str(), mode);
+    for (int iP = 0; iP < nP; ++iP) {
+      const double *m = sums.data() + (size_t)iP * 4;
+      if (nP == 1) {
+        fprintf(f, "%.20g\n%.20g\n%.20g\n%.20g\n%.20g\n%.20g\n", m[0] / m[2], m[3] / m[1],
+                m[2] * p.dnu, integral1, m[3] * p.dnu, 1.0 / integral2);
+      } else {
+        // the reference prints the last two sums without dnu here
+        const double v[6] = {m[0] / m[2], m[3] / m[1], m[2], integral1, m[3], 1.0 / integral2};
+        for (double x : v) fprintf(f, "%.20g %.20g %.20g\n", x, p.T, p.Plist[iP]);
+      }
+    }
+    fclose(f);
+  }
+
   // sort + resampling, heliosk.cu:2046-2193
   const int nxb = (int)(nx / p.nbins);
   const bool fit = p.doResampling > 0;
   std::vector<double> coeff, sorted, recon;
   std::vector<int32_t> nxmin;
   double t_fit = 0.0;
-  if (fit || p.doStoreK > 0) {
+  // the transmission function reads the reconstructed (fit) or sorted K
+  const bool want_k = p.doStoreK > 0 || p.doTransmission > 0;
+  if (fit || want_k) {
     if (fit) {
       coeff.resize((size_t)nP * p.nbins * p.nC);
       nxmin.resize((size_t)nP * p.nbins);
     }
-    if (p.doStoreK > 0) (fit ? recon : sorted).resize((size_t)nP * nx);
+    if (want_k) (fit ? recon : sorted).resize((size_t)nP * nx);
     cudaEventRecord(t0);
     chk(hk_kdist(c, nP, K.data(), 0, p.nC, unitScale, fit ? coeff.data() : nullptr,
-                 fit ? nxmin.data() : nullptr, (!fit && p.doStoreK > 0) ? sorted.data() : nullptr,
-                 (fit && p.doStoreK > 0) ? recon.data() : nullptr, 0, nullptr));
+                 fit ? nxmin.data() : nullptr, (!fit && want_k) ? sorted.data() : nullptr,
+                 (fit && want_k) ? recon.data() : nullptr, 0, nullptr));
     cudaEventRecord(t1);
     t_fit = seconds();
   }
@@ -285,12 +315,55 @@ int main(int argc, char **argv) {
     if (f) fclose(f);
   }
 
+  // transmission function, heliosk.cu:2377-2430
+  double t_tr = 0.0;
+  if (p.doTransmission > 0) {
+    const std::vector<double> &Kb = fit ? recon : sorted;
+    std::vector<double> Tr((size_t)nP * p.nbins * p.nTr);
+    cudaEventRecord(t0);
+    chk(hk_transmission(c, nP, Kb.data(), fit ? nxmin.data() : nullptr, 0, p.nTr, p.dTr, Tr.data(), 0,
+                        nullptr));
+    cudaEventRecord(t1);
+    t_tr = seconds();
+    char fn[512];
+    FILE *f = nullptr;
+    if (p.doTransmission == 1) f = fopen(("Out_" + p.name + "_tr.dat").c_str(), mode);
+    if (p.doTransmission == 2 && p.replaceFiles == 1)
+      for (int i = 0; i < p.nbins; ++i) {
+        snprintf(fn, sizeof fn, "Out_%s_tr%.4d.dat", p.name.c_str(), i);
+        fclose(fopen(fn, "w"));
+      }
+    for (int iP = 0; iP < nP; ++iP) {
+      for (int i = 0; i < p.nbins; ++i) {
+        if (p.doTransmission == 2) {
+          snprintf(fn, sizeof fn, "Out_%s_tr%.4d.dat", p.name.c_str(), i);
+          f = fopen(fn, "a");
+        }
+        const double *Tb = Tr.data() + ((size_t)iP * p.nbins + i) * p.nTr;
+        const double Pv = p.Plist[iP];
+        write_lines(f, p.nTr, [&](int64_t j, char *buf, size_t cap) {
+          const double m = exp((double)((int)j - p.nTr / 2) * p.dTr);
+          if (nP == 1) return snprintf(buf, cap, "%.20g %.20g\n", m, Tb[j]);
+          return snprintf(buf, cap, "%.20g %.20g %.20g %.20g %d\n", m, Tb[j], p.T, Pv, (int)j);
+        });
+        if (p.doTransmission == 1) fprintf(f, "\n\n");
+        if (p.doTransmission == 2) {
+          fclose(f);
+          f = nullptr;
+        }
+      }
+    }
+    if (f) fclose(f);
+  }
+
   for (FILE *f : {info, stdout}) {
     fprintf(f, "Time for input:        %g seconds\n", t_input);
     fprintf(f, "Time for Lines:        %g seconds\n", t_lines);
     fprintf(f, "Time for K(x):         %g seconds\n", t_K);
     fprintf(f, "Time for write K(x):   %g seconds\n", t_write);
     fprintf(f, "Time for sort and Resampling:   %g seconds\n", t_fit);
+    if (p.doMean > 0) fprintf(f, "Time for mean K(x):    %g seconds\n", t_mean);
+    if (p.doTransmission > 0) fprintf(f, "Time for Transmission:   %g seconds\n", t_tr);
   }
   fclose(info);
   hk_destroy(c);

@@ -83,6 +83,7 @@ struct hk_ctx {
   int last_shape = 0;
   std::vector<double> tune_ms;  // probe time per shape at the last tuning
   DevBuf tunework;              // probe states and their max-term words
+  DevBuf meanwork;              // means / transmission inputs, partial sums and outputs
   // T-P table recorded as one CUDA graph (hk_table_build / hk_table_run)
   cudaGraph_t table_graph = nullptr;
   cudaGraphExec_t table_exec = nullptr;
@@ -156,7 +157,7 @@ void hk_destroy(hk_ctx *c) {
                     &c->Aterm, &c->iso, &c->order, &c->states, &c->ticket,
                     &c->prep, &c->wbits, &c->Kwork, &c->outwork, &c->scratch,
                     &c->qrV, &c->qrC, &c->qrD, &c->vpart, &c->vcnt, &c->sscale, &c->gscale, &c->adjwork,
-                    &c->tunework})
+                    &c->tunework, &c->meanwork})
     b->release();
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -1101,6 +1102,84 @@ hk_status hk_table_free(hk_ctx *c) {
 int64_t hk_table_kernels(const hk_ctx *c) { return c ? c->table_kernels : 0; }
 
 int64_t hk_last_launches(const hk_ctx *c) { return c ? c->launches : 0; }
+
+// ------------------------------------------- mean opacities, transmission
+hk_status hk_means(hk_ctx *c, int nstates, const double *T, const double *K, int K_on_device,
+                   double *sums, int sums_on_device, void *stream) {
+  if (!c) return HK_ERR_ARG;
+  if (!c->grid_set) return fail(c, HK_ERR_STATE, "hk_set_grid must come first");
+  if (nstates < 1 || !T || !K || !sums) return fail(c, HK_ERR_ARG, "need nstates >= 1, T, K and sums");
+  if (nstates > 65535) return fail(c, HK_ERR_RANGE, "at most 65535 states per call");
+  for (int s = 0; s < nstates; ++s)
+    if (!(T[s] > 0.0) || !std::isfinite(T[s])) return fail(c, HK_ERR_RANGE, "state %d: T must be finite and > 0", s);
+  cudaSetDevice(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t nx = c->g.nx;
+  const size_t nK = (size_t)nstates * nx;
+  const double *Kd = K;
+  if (!K_on_device) {
+    CUDA_TRY(c, c->Kwork.ensure(nK * sizeof(double)));
+    CUDA_TRY(c, cudaMemcpyAsync(c->Kwork.p, K, nK * sizeof(double), cudaMemcpyHostToDevice, st));
+    Kd = c->Kwork.as<double>();
+  }
+  const size_t nscr = means_scratch_doubles(nstates, nx);
+  CUDA_TRY(c, c->meanwork.ensure((nscr + 5 * (size_t)nstates) * sizeof(double)));
+  double *Td = c->meanwork.as<double>(), *outd = Td + nstates, *scr = outd + 4 * (size_t)nstates;
+  CUDA_TRY(c, cudaMemcpyAsync(Td, T, nstates * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(c, launch_means(Kd, nx, c->g, Td, nstates, scr, sums_on_device ? sums : outd, st));
+  if (!sums_on_device) {
+    CUDA_TRY(c, cudaMemcpyAsync(sums, outd, 4 * (size_t)nstates * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(c, cudaStreamSynchronize(st));
+  } else if (!K_on_device) {
+    CUDA_TRY(c, cudaStreamSynchronize(st));  // T's pageable copy
+  }
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_transmission(hk_ctx *c, int nstates, const double *K, const int32_t *nxmin,
+                          int inputs_on_device, int nTr, double dTr, double *Tr,
+                          int Tr_on_device, void *stream) {
+  if (!c) return HK_ERR_ARG;
+  if (!c->grid_set) return fail(c, HK_ERR_STATE, "hk_set_grid must come first");
+  if (nstates < 1 || !K || !Tr) return fail(c, HK_ERR_ARG, "need nstates >= 1, K and Tr");
+  if (nstates > 65535) return fail(c, HK_ERR_RANGE, "at most 65535 states per call");
+  if (nTr < 1) return fail(c, HK_ERR_RANGE, "nTr must be >= 1");
+  if (!std::isfinite(dTr)) return fail(c, HK_ERR_RANGE, "dTr must be finite");
+  if (c->nxb < 3) return fail(c, HK_ERR_RANGE, "the transmission function needs >= 3 points per bin");
+  cudaSetDevice(c->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t nx = c->g.nx;
+  const size_t nK = (size_t)nstates * nx, nN = (size_t)nstates * c->nbins;
+  const size_t nT = nN * (size_t)nTr;
+  const double *Kd = K;
+  const int *nmd = reinterpret_cast<const int *>(nxmin);
+  double *Trd = Tr;
+  size_t need = (inputs_on_device ? 0 : nK) + (Tr_on_device ? 0 : nT) +
+                ((!inputs_on_device && nxmin) ? (nN + 1) / 2 : 0);
+  CUDA_TRY(c, c->meanwork.ensure(std::max<size_t>(need, 1) * sizeof(double)));
+  double *w = c->meanwork.as<double>();
+  if (!inputs_on_device) {
+    CUDA_TRY(c, cudaMemcpyAsync(w, K, nK * sizeof(double), cudaMemcpyHostToDevice, st));
+    Kd = w;
+    w += nK;
+    if (nxmin) {
+      CUDA_TRY(c, cudaMemcpyAsync(w, nxmin, nN * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+      nmd = reinterpret_cast<const int *>(w);
+      w += (nN + 1) / 2;
+    }
+  }
+  if (!Tr_on_device) Trd = w;
+  CUDA_TRY(c, launch_transmission(Kd, nx, nstates, c->nxb, c->nbins, nmd, c->kmin, nTr, dTr, Trd, st));
+  if (!Tr_on_device) {
+    CUDA_TRY(c, cudaMemcpyAsync(Tr, Trd, nT * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(c, cudaStreamSynchronize(st));
+  } else if (!inputs_on_device) {
+    CUDA_TRY(c, cudaStreamSynchronize(st));
+  }
+  ok(c);
+  return HK_OK;
+}
 
 hk_status hk_count_pairs(hk_ctx *c, double T, double P, int64_t *pairs3) {
   if (!c || !pairs3) return HK_ERR_ARG;

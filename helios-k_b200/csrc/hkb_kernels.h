@@ -85,6 +85,14 @@ cudaError_t column_minmax(int64_t n, const double *v_d, double *scratch_d, doubl
 cudaError_t launch_gather_u8(int64_t n, const int64_t *order_d, const uint8_t *src_d, uint8_t *dst_d,
                              cudaStream_t stream);
 
+// Mean opacities and transmission function (hkb_means.cu)
+size_t means_scratch_doubles(int nstates, int64_t nx);
+cudaError_t launch_means(const double *K_d, int64_t k_stride, const GridDev &g, const double *T_d,
+                         int nstates, double *scratch_d, double *out_d, cudaStream_t stream);
+cudaError_t launch_transmission(const double *K_d, int64_t k_stride, int nstates, int nxb,
+                                int nbins, const int *nxmin_d, double kmin, int nTr, double dTr,
+                                double *Tr_d, cudaStream_t stream);
+
 cudaError_t launch_count_pairs(const LinesDev &L, const GridDev &g, const StateDev *state_d,
                                unsigned long long *out_d, cudaStream_t stream);
 inline size_t line_prep_bytes(bool mixed) { return mixed ? sizeof(LinePrepF) : sizeof(LinePrep); }

@@ -87,6 +87,8 @@ def lib():
             "hk_set_tuning": (_i, [_p, _i]),
             "hk_set_tile_shape": (_i, [_p, _i]),
             "hk_tuning_result": (_i, [_p, _p, _p, _p]),
+            "hk_means": (_i, [_p, _i, _p, _p, _i, _p, _i, _p]),
+            "hk_transmission": (_i, [_p, _i, _p, _p, _i, _i, _d, _p, _i, _p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -245,6 +247,36 @@ class Context:
                                  _ptr(res["coeff"]), _ptr(res["nxmin"]), _ptr(res["sorted"]),
                                  _ptr(res["recon"]), int(outputs_on_device), sh))
         return res
+
+    # ------------------------------------ mean opacities, transmission
+    def means(self, T, K, stream=None):
+        """(nstates, 4) sums [B K, (dB/dT)/K, B, dB/dT] over the grid with the
+        reference's end weights; Planck mean = [:, 0] / [:, 2], Rosseland
+        mean = [:, 3] / [:, 1].  K: (nstates, Nx) numpy or CUDA tensor."""
+        T = _f64(np.atleast_1d(T))
+        dev = _is_dev(K)
+        if not dev:
+            K = _f64(K)
+        ns = len(T)
+        out = np.empty((ns, 4), np.float64)
+        sh = _stream_handle(stream, dev)
+        self._chk(lib().hk_means(self._h, ns, _ptr(T), _ptr(K), int(dev), _ptr(out), 0, sh))
+        return out
+
+    def transmission(self, K, nxmin=None, nTr=1000, dTr=0.05, stream=None):
+        """(nstates, nbins, nTr) transmission function of per-bin K (sorted,
+        or reconstructed by the fit, with its nxmin)."""
+        dev = _is_dev(K)
+        if not dev:
+            K = _f64(K)
+            if nxmin is not None:
+                nxmin = np.ascontiguousarray(nxmin, dtype=np.int32)
+        ns = K.shape[0] if K.ndim == 2 else 1
+        out = np.empty((ns, self._nbins, nTr), np.float64)
+        sh = _stream_handle(stream, dev)
+        self._chk(lib().hk_transmission(self._h, ns, _ptr(K), _ptr(nxmin), int(dev), int(nTr),
+                                        float(dTr), _ptr(out), 0, sh))
+        return out
 
     # ----------------------------------------------------- tile shapes
     def set_tuning(self, mode):

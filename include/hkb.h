@@ -171,6 +171,31 @@ hk_status hk_kdist_noalloc(const double *K, int nstates, int64_t nx, int nbins, 
  * records exceed the first run in grid sections (bit-identical K). */
 hk_status hk_set_workspace(hk_ctx *ctx, double prep_bytes, double part_bytes);
 
+/* --------------------------------------- mean opacities, transmission */
+
+/* Planck and Rosseland mean ingredients of nstates opacities K (nstates x
+ * Nx, the states' temperatures T[s]), replacing Mean_kernel +
+ * IntegrateMean_kernel (resample.h:635-773; driver heliosk.cu:1953-2020):
+ * sums[4 s + q] = sum over the grid of B K (q = 0), of (dB/dT) / K where
+ * K != 0 (1), of B (2), of dB/dT (3), each with the reference's end weights.
+ * Planck mean = sums[0] / sums[2]; Rosseland mean = sums[3] / sums[1];
+ * sums[2] dnu and sums[3] dnu approximate sigma T^4 / pi and 4 sigma T^3 / pi.
+ * K is in the library's internal units (hk_opacity's output). */
+hk_status hk_means(hk_ctx *ctx, int nstates, const double *T, const double *K, int K_on_device,
+                   double *sums, int sums_on_device, void *stream);
+
+/* Transmission function per bin, replacing Integrate_kernel (resample.h:
+ * 541-608; driver heliosk.cu:2377-2430): K is nstates x Nx of per-bin values
+ * (hk_kdist's sorted K, or its reconstruction when the fit ran), nxmin the
+ * fit's Nxmin (nstates x nbins; NULL = 0, as without resampling), kmin the
+ * grid's.  Tr[(s nbins + b) nTr + j] for m_j = exp((j - nTr/2) dTr):
+ *   (sum_k exp(-K_k m_j) + end weights) / (Nxb - 1) (Nxb - Nxmin) / Nxb
+ *   + exp(-kmin m_j) Nxmin / Nxb.
+ * K and nxmin are both on the device or both on the host. */
+hk_status hk_transmission(hk_ctx *ctx, int nstates, const double *K, const int32_t *nxmin,
+                          int inputs_on_device, int nTr, double dTr, double *Tr,
+                          int Tr_on_device, void *stream);
+
 /* ------------------------------------------------------ tile shapes */
 
 /* The mixed Voigt kernel runs in one of hk_num_tile_shapes() tile shapes:

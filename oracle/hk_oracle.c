@@ -842,3 +842,73 @@ void hko_vjp_sums(int64_t n, const double *nu, const double *S, const double *ia
     G[3 * n + l] = gn;
   }
 }
+
+/* ------------------------------------------------ means, transmission */
+/* end weights of resample.h:611-619: index idy gets w[idy], index n-1-idy
+ * gets w[2-idy] (the reference's mirrored order, kept as it is) */
+static const double hko_wS[3] = {-5.0 / 8.0, 1.0 / 6.0, -1.0 / 24.0};
+
+/* resample.h:635-663 */
+void hko_planck(double nu, double T, double *B, double *dBdT) {
+  if (nu == 0.0) {
+    *B = 0.0;
+    *dBdT = 0.0;
+    return;
+  }
+  const double nu3 = nu * nu * nu;
+  const double t1 = 2.0 * HKO_H * nu3 * HKO_C * HKO_C;
+  const double t2 = HKO_H * nu * HKO_C / (HKO_KB * T);
+  const double e = exp(t2);
+  const double e1 = e - 1.0;
+  *B = t1 / e1;
+  *dBdT = t1 * t2 / (T * (e - 2.0 + 1.0 / e));
+}
+
+/* resample.h:670-773 with useIndividualX = 0 */
+void hko_means(const double *x, const double *K, int64_t nx, double T, double *out) {
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t k = 0; k < nx; ++k) {
+    double B, R;
+    hko_planck(x[k], T, &B, &R);
+    s[0] += B * K[k];
+    if (K[k] != 0.0) s[1] += R / K[k];
+    s[2] += B;
+    s[3] += R;
+  }
+  for (int idy = 0; idy < 3 && nx >= 3; ++idy) {
+    const int64_t a = idy, b = nx - 1 - idy;
+    double Ba, Ra, Bb, Rb;
+    hko_planck(x[a], T, &Ba, &Ra);
+    hko_planck(x[b], T, &Bb, &Rb);
+    s[0] += hko_wS[idy] * (Ba * K[a]);
+    s[0] += hko_wS[2 - idy] * (Bb * K[b]);
+    if (K[a] != 0.0) s[1] += hko_wS[idy] * (Ra / K[a]);
+    if (K[b] != 0.0) s[1] += hko_wS[2 - idy] * (Rb / K[b]);
+    s[2] += hko_wS[idy] * Ba;
+    s[2] += hko_wS[2 - idy] * Bb;
+    s[3] += hko_wS[idy] * Ra;
+    s[3] += hko_wS[2 - idy] * Rb;
+  }
+  for (int q = 0; q < 4; ++q) out[q] = s[q];
+}
+
+/* resample.h:541-608 */
+void hko_transmission(const double *K, int nxb, int nbins, const int32_t *nxmin,
+                      double kmin, int nTr, double dTr, double *Tr) {
+#pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < nbins; ++b) {
+    const double *Kb = K + (int64_t)b * nxb;
+    const int nm = nxmin ? nxmin[b] : 0;
+    for (int j = 0; j < nTr; ++j) {
+      const double m = exp((j - nTr / 2) * dTr);
+      double a = 0.0;
+      for (int k = 0; k < nxb; ++k) a += exp(-Kb[k] * m);
+      for (int idy = 0; idy < 3 && nxb >= 3; ++idy) {
+        a += hko_wS[idy] * exp(-Kb[idy] * m);
+        a += hko_wS[2 - idy] * exp(-Kb[nxb - 1 - idy] * m);
+      }
+      Tr[(int64_t)b * nTr + j] = a / ((double)(nxb - 1)) * (nxb - nm) / ((double)nxb) +
+                                 exp(-kmin * m) * nm / ((double)nxb);
+    }
+  }
+}

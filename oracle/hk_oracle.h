@@ -103,6 +103,20 @@ void hko_kdist(double *K, int64_t nx, int nxb, int nbins, int nc, double kmin,
                const double *D, int32_t *nxmin, double *coeff /* nbins*nc */,
                double *recon /* nx or NULL */);
 
+/* Planck / Rosseland mean ingredients, resample.h:635-773 (Mean_kernel,
+ * IntegrateMean_kernel, equal spacing) on the grid x (nx points, state
+ * temperature T): out[0] = sum B K, out[1] = sum over K != 0 of (dB/dT) / K,
+ * out[2] = sum B, out[3] = sum dB/dT, each with the reference's end weights
+ * (SimpsonCoefficient resample.h:611-619, applied as resample.h:730-747). */
+void hko_planck(double nu, double T, double *B, double *dBdT);
+void hko_means(const double *x, const double *K, int64_t nx, double T, double *out);
+/* Transmission function, resample.h:541-608 (Integrate_kernel): for every
+ * bin of nxb points of K (sorted or reconstructed) and m_j = exp((j - nTr/2)
+ * dTr), Tr[b nTr + j] = (sum_k exp(-K_k m_j) + end weights) / (nxb - 1)
+ * (nxb - Nxmin_b) / nxb + exp(-kmin m_j) Nxmin_b / nxb; nxmin NULL = 0. */
+void hko_transmission(const double *K, int nxb, int nbins, const int32_t *nxmin,
+                      double kmin, int nTr, double dTr, double *Tr);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,9 @@ def lib():
         L.hko_find_cut.argtypes = [_p, _i64, _i, _d, _i, _p]
         L.hko_kdist.argtypes = [_p, _i64, _i, _i, _i, _d, _d, _p, _p, _p, _p,
                                 _p, _p]
+        L.hko_planck.argtypes = [_d, _d, _p, _p]
+        L.hko_means.argtypes = [_p, _p, _i64, _d, _p]
+        L.hko_transmission.argtypes = [_p, _i, _i, _p, _d, _i, _d, _p]
         _lib = L
     return _lib
 
@@ -233,6 +236,34 @@ def kdist(K_sorted, nxb, nbins, nc, kmin=0.0, unitScale=1.0, recon=False,
     lib().hko_kdist(_ptr(K), nx, nxb, nbins, nc, kmin, unitScale, _ptr(V),
                     _ptr(Cv), _ptr(D), _ptr(nxmin), _ptr(coeff), _ptr(rec))
     return coeff.reshape(nbins, nc), nxmin, rec
+
+
+def planck(nu, T):
+    """(B, dB/dT) of resample.h:635-663 at wavenumber nu (cm^-1)."""
+    b = np.zeros(1)
+    r = np.zeros(1)
+    lib().hko_planck(float(nu), float(T), _ptr(b), _ptr(r))
+    return float(b[0]), float(r[0])
+
+
+def means(x, K, T):
+    """[sum B K, sum (dB/dT)/K, sum B, sum dB/dT] with the reference's end
+    weights (resample.h:635-773); Planck mean = [0]/[2], Rosseland = [3]/[1]."""
+    x = _f64(x)
+    K = _f64(K)
+    out = np.zeros(4)
+    lib().hko_means(_ptr(x), _ptr(K), len(K), float(T), _ptr(out))
+    return out
+
+
+def transmission(K, nxb, nbins, nxmin=None, kmin=0.0, nTr=1000, dTr=0.05):
+    """Tr[nbins, nTr] of resample.h:541-608 from per-bin K (sorted or
+    reconstructed); m_j = exp((j - nTr // 2) dTr)."""
+    K = _f64(K)
+    nm = None if nxmin is None else np.ascontiguousarray(nxmin, dtype=np.int32)
+    Tr = np.empty(nbins * nTr)
+    lib().hko_transmission(_ptr(K), nxb, nbins, _ptr(nm), float(kmin), nTr, float(dTr), _ptr(Tr))
+    return Tr.reshape(nbins, nTr)
 
 
 def state_opacity(lines, iso_mass, iso_ab, iso_Q, T, P, numin, numax, dnu,

@@ -38,9 +38,10 @@ def write_data(data_dir, lines, species="syn"):
 
 
 def write_run(d, data_dir, T, P, numin, numax, dnu, cut, nbins, nC, name="syn", species="syn",
-              store_k=2, resample=1, tuning=1):
+              store_k=2, resample=1, tuning=1, **extra):
     """param.dat for one T and one P (or, P a list, a PFile of pressures) in
-    run directory d, reading data_dir."""
+    run directory d, reading data_dir; extra: more param.dat keys (spaces
+    as underscores), e.g. doMean=1, doTransmission=1, nTr=100, dTr=0.05."""
     from hkb import synth
     os.makedirs(d, exist_ok=True)
     pfile = "-"
@@ -52,15 +53,15 @@ def write_run(d, data_dir, T, P, numin, numax, dnu, cut, nbins, nC, name="syn", 
     synth.write_param(os.path.join(d, "param.dat"), name=name, T=T, P=P, PFile=pfile,
                       Species_Name=species, pathToData=data_dir.rstrip("/") + "/", numin=numin,
                       numax=numax, dnu=dnu, cut=cut, nbins=nbins, nC=nC,
-                      doResampling=resample, doStoreFullK=store_k, doTuning=tuning)
+                      doResampling=resample, doStoreFullK=store_k, doTuning=tuning, **extra)
 
 
 def make_run_dir(d, lines, T, P, numin, numax, dnu, cut, nbins, nC, name="syn",
-                 species="syn", store_k=2, resample=1, tuning=1):
+                 species="syn", store_k=2, resample=1, tuning=1, **extra):
     """Species data and param.dat together in directory d."""
     write_data(d, lines, species)
     write_run(d, d, T, P, numin, numax, dnu, cut, nbins, nC, name, species, store_k, resample,
-              tuning)
+              tuning, **extra)
 
 
 _TIME_RE = {

@@ -55,3 +55,60 @@ def test_dropin_outputs_match_oracle(tmp_path):
     ce = np.max(np.abs(cb[:, 2:] - co.reshape(NBINS, NC)))
     print(f"drop-in Chebyshev max abs err {ce:.2e}")
     assert ce < 1e-6
+
+
+def test_dropin_means_and_transmission(tmp_path):
+    """doMean = 1 and doTransmission = 1 (heliosk.cu:1953-2020, 2377-2430):
+    Out_<name>_mean.dat and Out_<name>_tr.dat against the oracle chain
+    (opacity, per-bin sort, fit and reconstruction, means, transmission).
+    Tolerance 1e-5 relative (the mixed-form K's error bound)."""
+    assert os.path.exists(ref_run.OUR_EXE), "build helios-k_b200/bin/heliosk first"
+    L = synth.hitran_lines(3000, seed=17, nu_min=NUMIN - 40.0, nu_max=NUMAX + 40.0)
+    T, P = 900.0, 0.5
+    # K here (internal units) spans 2e11 .. 1e30: m = e^-75 .. e^73.5 takes
+    # Tr from 1 down to 0 (10 % of the values lie in (0.01, 0.99))
+    nTr, dTr = 100, 1.5
+    d = str(tmp_path / "run")
+    ref_run.make_run_dir(d, L, T, P, NUMIN, NUMAX, DNU, CUT, NBINS, NC, store_k=0, resample=1,
+                         doMean=1, doTransmission=1, nTr=nTr, dTr=dTr)
+    r = ref_run.run(ref_run.OUR_EXE, d, timeout=300)
+    assert r["rc"] == 0, r["tail"]
+    assert "mean K(x)" in r["info"] and "Transmission" in r["info"]
+    nx = oracle.grid_nx(NUMIN, NUMAX, DNU)
+    x = oracle.grid_x(NUMIN, DNU, nx)
+    Lr = synth.read_hitran_bin(os.path.join(d, "syn.bin"))
+    Tq, Qq = synth.q_table()
+    Q = oracle.partition(Tq, Qq, T)
+    nu, S, iad, vy = oracle.prep_hitran(Lr, [synth.MASS], [1.0], [Q], T, P, qalphaL=1.0)
+    win = oracle.windows(nu, S, iad, vy, NUMIN, DNU, nx, 0, CUT)
+    Kref, _ = oracle.opacity(nu, S, iad, vy, win, NUMIN, DNU, nx)
+    # means: Planck, Rosseland, sum B dnu, analytic, sum dB/dT dnu, analytic
+    mean = np.loadtxt(os.path.join(d, "Out_syn_mean.dat"))
+    m = oracle.means(x, Kref, T)
+    want = [m[0] / m[2], m[3] / m[1], m[2] * DNU, None, m[3] * DNU, None]
+    for k, w in enumerate(want):
+        if w is not None:
+            assert mean[k] == pytest.approx(w, rel=1e-5), k
+    # the analytic integrals (the grid covers part of the spectrum, so the
+    # numeric ones are smaller)
+    kb, h, c = 1.3806489e-16, 6.62606957e-27, 2.99792458e10
+    sigma = 2.0 * kb**4 / (h**3 * c**2 * 15.0) * np.pi**5
+    assert mean[3] == pytest.approx(sigma * T**4 / np.pi, rel=1e-12)
+    assert mean[5] == pytest.approx(4.0 * sigma * T**3 / np.pi, rel=1e-12)
+    assert mean[2] < mean[3] and mean[4] < mean[5]
+    # transmission of the reconstructed bins
+    nxb = nx // NBINS
+    key, idx = oracle.bin_keys(NUMIN, NUMAX, DNU, nx, NBINS)
+    Ks = oracle.sort_bins(Kref, idx, NBINS)
+    co, nxmin, rec = oracle.kdist(Ks, nxb, NBINS, NC, recon=True)
+    Tr_ref = oracle.transmission(rec, nxb, NBINS, nxmin, 0.0, nTr, dTr)
+    tr = np.loadtxt(os.path.join(d, "Out_syn_tr.dat"))
+    assert tr.shape == (NBINS * nTr, 2)
+    mm = np.exp((np.arange(nTr) - nTr // 2) * dTr)
+    np.testing.assert_allclose(tr[:, 0], np.tile(mm, NBINS), rtol=1e-15)
+    # Tr lies in [0, 1]; where exp(-K m) underflows both are ~0 (atol)
+    big = Tr_ref.ravel() > 1e-12
+    assert big.sum() > NBINS * nTr // 5 and Tr_ref.max() > 0.9
+    err = np.max(np.abs(tr[big, 1] - Tr_ref.ravel()[big]) / Tr_ref.ravel()[big])
+    print(f"drop-in means {mean[:2]}, transmission max rel err {err:.2e} (Tr > 1e-12)")
+    np.testing.assert_allclose(tr[:, 1], Tr_ref.ravel(), rtol=1e-5, atol=1e-12)
