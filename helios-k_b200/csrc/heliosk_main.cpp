@@ -64,8 +64,8 @@ int main(int argc, char **argv) {
   if (p.bins != "-" || p.edges != "-") return die("Error: binsFile / OutputEdgesFile are outside this build's path");
   if (p.Nxb != 0) return die("Error: 'Nnu per bin' (unequal spacing) is outside this build's path");
   if (p.subLorentzian != "-") return die("Error: sub-Lorentzian profiles are outside this build's path");
-  if (p.removePlinth != 0) return die("Error: removePlinth is outside this build's path");
-  if (p.profile != 1) return die("Error: only profile = 1 (Voigt) is on this build's path");
+  if (p.removePlinth != 0 && p.removePlinth != 1) return die("Error: removePlinth must be 0 or 1");
+  if (p.profile < 1 || p.profile > 4) return die("Error: profile must be 1, 2, 3 or 4");
   if (p.doTransmission < 0 || p.doTransmission > 2) return die("Error: doTransmission must be 0, 1 or 2");
   if (p.doTransmission > 0 && p.nTr < 1) return die("Error: nTr must be >= 1 for the transmission function");
   if (p.nbins < 1) return die("Error: nbins must be >= 1");
@@ -126,6 +126,7 @@ int main(int argc, char **argv) {
   cudaEventRecord(t1);
   const double t_input = compute ? seconds() : 0.0;
   chk(hk_set_grid(c, p.numin, p.numax, p.dnu, p.nbins, p.cutMode, p.cut, kmin));
+  chk(hk_set_profile(c, p.profile, p.removePlinth));
   // doTuning = 1: the tile-shape tuner, where its probes pay off (PFile tables)
   chk(hk_set_tuning(c, p.doTuning == 1 ? 1 : 0));
   const int64_t nx = hk_grid_points(c);

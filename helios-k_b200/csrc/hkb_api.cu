@@ -650,7 +650,9 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   }
   // States run in batches whose per-(state, line) records fit the prep
   // budget; each batch is one prep launch and one persistent Voigt launch.
-  const bool mixed = precision == HK_PRECISION_MIXED;
+  // profiles 2-4 and plinth removal run the FP64 form (the mixed form's
+  // FP32 region sums are built for the Voigt profile's regions)
+  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile == 1 && !c->g.plinth;
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
@@ -856,6 +858,19 @@ hk_status hk_set_workspace(hk_ctx *c, double prep_bytes, double part_bytes) {
   return HK_OK;
 }
 
+hk_status hk_set_profile(hk_ctx *c, int profile, int remove_plinth) {
+  if (!c) return HK_ERR_ARG;
+  if (profile < 1 || profile > 4)
+    return fail(c, HK_ERR_ARG, "profile must be 1 (Voigt), 2 (Lorentz), 3 (Doppler) or 4 (binned Gaussian)");
+  if (remove_plinth != 0 && remove_plinth != 1) return fail(c, HK_ERR_ARG, "remove_plinth must be 0 or 1");
+  c->g.profile = profile;
+  c->g.plinth = remove_plinth;
+  c->tuned = false;
+  table_release(c);
+  ok(c);
+  return HK_OK;
+}
+
 int hk_num_tile_shapes(void) { return voigt_num_shapes(); }
 
 hk_status hk_tile_shape_info(int shape, int *lines_per_chunk, int *points_per_tile) {
@@ -933,6 +948,8 @@ hk_status hk_opacity_vjp(hk_ctx *c, double T, double P, int precision, const dou
   if (!u) return fail(c, HK_ERR_ARG, "need the seed u (Nx values)");
   if (precision != HK_PRECISION_PLAIN_FP64 && precision != HK_PRECISION_MIXED)
     return fail(c, HK_ERR_ARG, "precision must be 0 (plain FP64) or 1 (mixed)");
+  if (c->g.profile != 1 || c->g.plinth)
+    return fail(c, HK_ERR_UNSUPPORTED, "the adjoint is for the Voigt profile without plinth removal");
   cudaSetDevice(c->device);
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<StateDev> hs;
@@ -1009,7 +1026,9 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   CUDA_TRY(c, c->wbits.ensure(2 * nstates * sizeof(unsigned long long)));
   CUDA_TRY(c, cudaMemcpy(c->states.p, hs.data(), nstates * sizeof(StateDev), cudaMemcpyHostToDevice));
   const int64_t nx = c->g.nx;
-  const bool mixed = precision == HK_PRECISION_MIXED;
+  // profiles 2-4 and plinth removal run the FP64 form (the mixed form's
+  // FP32 region sums are built for the Voigt profile's regions)
+  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile == 1 && !c->g.plinth;
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
   if (per_state > c->prep_budget)
     return fail(c, HK_ERR_UNSUPPORTED, "one state's line records (%zu B) exceed the workspace (%zu B): "

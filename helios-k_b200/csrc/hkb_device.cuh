@@ -161,6 +161,8 @@ __device__ __forceinline__ int64_t est_index(double edge, const GridDev &g,
   return (int64_t)e;
 }
 
+// Profiles 2-4 have no regions B and C: the whole cut window is region A
+// (nuLimits_kernel voigt.h:2250, "profile != 1"; only Line6A runs for them).
 // Window boundaries of one line restricted to grid indices [g0, g1):
 // out[0..5] = i0, b0, c0, c1, b1, i1 (absolute indices, each clipped to
 // [g0, g1]).  Equals clip(oracle window) because every predicate is
@@ -196,7 +198,7 @@ __device__ __forceinline__ void line_windows(const GridDev &g, const StateDev &s
   for (int r = 0; r < 2; ++r) {
     const double R = Rs[r];
     const double h2 = R - c.vy2;
-    if (h2 > 0.0) {
+    if (g.profile == 1 && h2 > 0.0) {  // regions B and C are the Voigt profile's
       const double h = sqrt(h2) / c.iad;
       lohi[r][0] = first_true(c, HK_P_LEFT_R, R, i0, ic, est_index(ls.nu - h, g, g1));
       lohi[r][1] = first_true(c, HK_P_RIGHT_R, R, ic, i1, est_index(ls.nu + h, g, g1));
@@ -270,6 +272,45 @@ static __device__ __noinline__ double voigt916_d(double x, double y, double ey) 
   if (ax == 0.0) t1 = ey;
   if (y == 0.0) t1 = ex2;
   return t1;
+}
+
+// Profiles 2-4 at x (Doppler units) for a line with S1 as line_prep_kernel
+// forms it per profile: Lorentz S1 / (x^2 + y^2) (S1 = S y / pi), Doppler
+// S1 exp(-x^2) (S1 = S / sqrt(pi)), binned Gaussian S1 (erf(x + vb/2) -
+// erf(x - vb/2)) / (2 vb) with vb the grid step in Doppler units (S1 = S):
+// Line6fA_kernel voigt.h:1235-1262, in FP64.
+// erf(a) - erf(b) for a > b without cancellation in the wings: as
+// erfc(b) - erfc(a) when both are positive, erfc(-a) - erfc(-b) when both
+// are negative (the same value; the reference subtracts FP32 erff).
+__device__ __forceinline__ double erf_diff(double a, double b) {
+  if (b >= 0.0) return erfc(b) - erfc(a);
+  if (a <= 0.0) return erfc(-a) - erfc(-b);
+  return erf(a) - erf(b);
+}
+
+__device__ __forceinline__ double profile_a_d(int profile, double x, double y2, double S1,
+                                              double vb) {
+  if (profile == 3) return S1 * exp(-(x * x));
+  if (profile == 4) return S1 * (1.0 / vb) * 0.5 * erf_diff(x + 0.5 * vb, x - 0.5 * vb);
+  return S1 / (x * x + y2);  // profile 1 region A, profile 2
+}
+
+// The profile's value at the line's cut edge, x_c = cut iad (cutMode 0),
+// cut y (1) or cut (2): Plinth_kernel (voigt.h:1091-1164) in FP64, the Voigt
+// profile by the region of r^2 = x_c^2 + y^2; 0 for the binned Gaussian (the
+// reference defines none).
+__device__ __forceinline__ double plinth_d(const GridDev &g, double S1, double Sc, double iad,
+                                           double vy) {
+  const double xc = (g.cutMode == 1) ? g.cut * vy : (g.cutMode == 2 ? g.cut : g.cut * iad);
+  const double y2 = vy * vy;
+  if (g.profile == 1) {
+    const double r2 = xc * xc + y2;
+    if (r2 >= 1.0e6) return S1 / r2;
+    if (r2 >= 100.0) return S1 * gh2_d(xc, y2);
+    return Sc * voigt916_d(xc, vy, erfcx(vy));
+  }
+  if (g.profile == 4) return 0.0;
+  return profile_a_d(g.profile, xc, y2, S1, 0.0);
 }
 
 // ------------------------------------------- region C, recurrence form

@@ -96,8 +96,10 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
     const LineState ls = prep_line(L, st, l);
     int64_t w[6];
     line_windows(g, st, ls, 0, g.nx, w);
-    const double S1 = ls.S * ls.vy / CUDART_PI;
+    // S1 per profile (S3_kernel voigt.h:452-463); the mixed form is Voigt only
     const double Sc = ls.S * (1.0 / 1.7724538509055160273);
+    const double S1 = (MIXED || g.profile <= 2) ? ls.S * ls.vy / CUDART_PI
+                                                : (g.profile == 3 ? Sc : ls.S);
     const bool hasC = w[3] > w[2];
     // largest region-A/B term of the line: S1 / r^2 with r^2 >= max(100, y^2)
     const double Y = ls.vy * ls.vy;
@@ -171,6 +173,7 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
       r.b1 = (int)w[4];
       r.i1 = (int)w[5];
       r.pad = 0;
+      r.plinth = (g.plinth && w[5] > w[0]) ? plinth_d(g, S1, Sc, ls.iad, ls.vy) : 0.0;
       reinterpret_cast<LinePrep *>(out)[(int64_t)s * L.n + l] = r;
     }
     if (w[5] > w[0]) s1_loc = fmax(s1_loc, term);

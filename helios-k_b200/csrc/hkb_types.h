@@ -50,21 +50,28 @@ struct GridDev {
   int64_t nx;
   int cutMode;
   double cut;  // 1e30 when the parameter file says 0 (heliosk.cu:947)
+  // line profile (define.h:69): 1 Voigt, 2 Lorentz, 3 Doppler, 4 binned
+  // Gaussian cross section; plinth 1: every line's profile value at its cut
+  // edge is subtracted inside its cut window (removePlinth)
+  int profile = 1;
+  int plinth = 0;
 };
 
 // One line scaled to one state, as written by line_prep_kernel and read by
-// the Voigt sum (80 bytes; FP64 parameters, global index windows).
+// the Voigt sum (96 bytes; FP64 parameters, global index windows).
 struct __align__(16) LinePrep {
   double nu;    // centre after the pressure shift
   double iad;   // 1 / alphaD
   double vy;    // gammaL / alphaD
-  double S1;    // S * vy / pi      (regions A, B)
+  double S1;    // S * vy / pi (regions A, B; Lorentz), S / sqrt(pi) (Doppler), S (binned Gaussian)
   double Sc;    // S / sqrt(pi)     (region C)
   double ey;    // erfcx(vy)        (lines with a region-C window)
   int i0, b0, c0, c1, b1, i1;  // [i0,b0) A [b0,c0) B [c0,c1) C [c1,b1) B [b1,i1) A
   float sig1;   // region-C series constant Sig1(vy)
   int pad;
+  double plinth;  // profile value at the cut edge (removePlinth), else 0
 };
+static_assert(sizeof(LinePrep) == 96, "LinePrep layout");
 
 // The same line and state for the mixed form (112 bytes): everything that
 // depends on the line and the state only, so staging a line into a tile adds

@@ -112,7 +112,7 @@ constexpr size_t smem_mixed() {
 }
 
 struct __align__(16) RecD {
-  double nu, iad, y2, y, S1, Sc, ey, pad;
+  double nu, iad, y2, y, S1, Sc, ey, pl;  // pl: plinth (removePlinth), else 0
   int i0, b0, c0, c1, b1, i1, p0, p1;
 };
 
@@ -244,7 +244,7 @@ __device__ __forceinline__ void stage_plain(const LinePrep *__restrict__ P, int6
   r.S1 = lp.S1;
   r.Sc = lp.Sc;
   r.ey = lp.ey;
-  r.pad = 0.0;
+  r.pl = nonempty ? lp.plinth : 0.0;
   r.i0 = nonempty ? li[0] : 0;
   r.b0 = li[1];
   r.c0 = li[2];
@@ -495,9 +495,28 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
 template <int PPL>
 __device__ __forceinline__ void sweep_plain(const RecD &r, int wb, int lane,
                                             const double (&xg)[PPL],
-                                            double (&acc)[PPL]) {
+                                            double (&acc)[PPL], const GridDev &g) {
   const int we = wb + 32 * PPL;
   if (r.i1 <= wb || r.i0 >= we) return;
+  if (g.profile != 1 || g.plinth) {
+    // profiles 2-4 (region A only) and plinth removal: Line6fA/B/C add the
+    // profile, then subtract the line's plinth, at every window point
+    const double vb = g.dnu * r.iad;
+#pragma unroll
+    for (int p = 0; p < PPL; ++p) {
+      const int k = wb + lane + 32 * p;
+      if (k >= r.i0 && k < r.i1) {
+        const double x = (xg[p] - r.nu) * r.iad;
+        double v;
+        if (k >= r.c0 && k < r.c1) v = r.Sc * voigt916_d(x, r.y, r.ey);
+        else if (k >= r.b0 && k < r.b1) v = r.S1 * gh2_d(x, r.y2);
+        else v = profile_a_d(g.profile, x, r.y2, r.S1, vb);
+        acc[p] += v;
+        acc[p] -= r.pl;
+      }
+    }
+    return;
+  }
   const bool full = r.i0 <= wb && r.i1 >= we;
   if (full && ((r.b0 <= wb && r.c0 >= we) || (r.c1 <= wb && r.b1 >= we))) {
 #pragma unroll
@@ -726,7 +745,7 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
         flush_sums<PPL>(a32, cacc, wb, lane, st.s1exp, lcur);
       } else {
         for (int j = 0; j < cnt; ++j)
-          sweep_plain<PPL>(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc);
+          sweep_plain<PPL>(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc, g);
       }
       __syncthreads();
     }

@@ -88,6 +88,7 @@ def lib():
             "hk_set_tile_shape": (_i, [_p, _i]),
             "hk_tuning_result": (_i, [_p, _p, _p, _p]),
             "hk_means": (_i, [_p, _i, _p, _p, _i, _p, _i, _p]),
+            "hk_set_profile": (_i, [_p, _i, _i]),
             "hk_transmission": (_i, [_p, _i, _p, _p, _i, _i, _d, _p, _i, _p]),
         }
         for name, (res, args) in sig.items():
@@ -247,6 +248,12 @@ class Context:
                                  _ptr(res["coeff"]), _ptr(res["nxmin"]), _ptr(res["sorted"]),
                                  _ptr(res["recon"]), int(outputs_on_device), sh))
         return res
+
+    def set_profile(self, profile=1, remove_plinth=0):
+        """1 Voigt, 2 Lorentz, 3 Doppler, 4 binned Gaussian; remove_plinth 1
+        subtracts each line's value at its cut edge (FP64 form for 2-4 and
+        plinth removal)."""
+        self._chk(lib().hk_set_profile(self._h, int(profile), int(remove_plinth)))
 
     # ------------------------------------ mean opacities, transmission
     def means(self, T, K, stream=None):

@@ -171,6 +171,15 @@ hk_status hk_kdist_noalloc(const double *K, int nstates, int64_t nx, int nbins, 
  * records exceed the first run in grid sections (bit-identical K). */
 hk_status hk_set_workspace(hk_ctx *ctx, double prep_bytes, double part_bytes);
 
+/* Line profile (param.dat `profile`, define.h:69): 1 Voigt (default),
+ * 2 Lorentz, 3 Doppler, 4 binned Gaussian cross section (Hill et al. 2012),
+ * as Line6fA_kernel (voigt.h:1235-1262) evaluates them over the whole cut
+ * window; remove_plinth 1 (param.dat `removePlinth`) subtracts each line's
+ * profile value at its cut edge (Plinth_kernel voigt.h:1091-1164) from every
+ * point of its window.  Profiles 2-4 and plinth removal run the FP64 form
+ * whatever precision hk_opacity is given; the adjoint refuses them. */
+hk_status hk_set_profile(hk_ctx *ctx, int profile, int remove_plinth);
+
 /* --------------------------------------- mean opacities, transmission */
 
 /* Planck and Rosseland mean ingredients of nstates opacities K (nstates x

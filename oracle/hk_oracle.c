@@ -272,6 +272,13 @@ static int64_t est_index(double nu_edge, double numin, double dnu, int64_t nx) {
 void hko_windows(int64_t n, const double *nu, const double *S,
                  const double *iad, const double *vy, double numin, double dnu,
                  int64_t nx, int cutMode, double cut, int64_t *win) {
+  hko_windows_p(n, nu, S, iad, vy, numin, dnu, nx, cutMode, cut, 1, win);
+}
+
+/* profiles 2-4 have no regions B and C (nuLimits_kernel voigt.h:2250) */
+void hko_windows_p(int64_t n, const double *nu, const double *S,
+                   const double *iad, const double *vy, double numin, double dnu,
+                   int64_t nx, int cutMode, double cut, int profile, int64_t *win) {
   if (cut == 0.0) cut = 1.0e30; /* heliosk.cu:947 */
 #pragma omp parallel for schedule(static)
   for (int64_t l = 0; l < n; ++l) {
@@ -307,7 +314,7 @@ void hko_windows(int64_t n, const double *nu, const double *S,
       double R = Rs[r];
       double h2 = R - c.vy2;
       int64_t lo, hi;
-      if (h2 > 0.0) {
+      if (profile == 1 && h2 > 0.0) {
         double h = sqrt(h2) / c.iad;
         lo = first_true(&c, P_LEFT_R, R, i0, ic,
                         est_index(c.nu - h, numin, dnu, nx));
@@ -455,6 +462,59 @@ void hko_opacity(int64_t n, const double *nu, const double *S,
                  const double *iad, const double *vy, const int64_t *win,
                  double numin, double dnu, int64_t ib, int64_t ie, double kmin,
                  double *K, int nthreads, int64_t pairs_out[3]) {
+  hko_opacity_p(n, nu, S, iad, vy, win, numin, dnu, ib, ie, kmin, 1, NULL, K, nthreads,
+                pairs_out);
+}
+
+/* profiles 2-4 at x (Doppler units): Line6fA_kernel voigt.h:1235-1262 with
+ * S1 of S3_kernel voigt.h:452-463 (S y / pi, S / sqrt(pi), S) */
+/* erf(a) - erf(b), a > b, through erfc on the same side of zero (no
+ * cancellation in the wings) */
+static double erf_diff(double a, double b) {
+  if (b >= 0.0) return erfc(b) - erfc(a);
+  if (a <= 0.0) return erfc(-a) - erfc(-b);
+  return erf(a) - erf(b);
+}
+
+static double profile_a(int profile, double x, double S, double y, double vb) {
+  if (profile == 3) return S / sqrt(M_PI) * exp(-(x * x));
+  if (profile == 4) return S * (1.0 / vb) * 0.5 * erf_diff(x + 0.5 * vb, x - 0.5 * vb);
+  return S * y / M_PI / (x * x + y * y);
+}
+
+/* Plinth_kernel (voigt.h:1091-1164) in FP64: the profile at the cut edge
+ * x_c = cut iad (cutMode 0), cut y (1), cut (2); 0 for profile 4 and for
+ * lines without a window. */
+void hko_plinth(int64_t n, const double *S, const double *iad, const double *vy,
+                const int64_t *win, int cutMode, double cut, int profile, double *out) {
+  if (cut == 0.0) cut = 1.0e30;
+  for (int64_t l = 0; l < n; ++l) {
+    const int64_t *o = win + 6 * l;
+    out[l] = 0.0;
+    if (!(o[5] > o[0]) || profile == 4) continue;
+    const double y = vy[l];
+    const double xc = (cutMode == 1) ? cut * y : (cutMode == 2 ? cut : cut * iad[l]);
+    if (profile != 1) {
+      out[l] = profile_a(profile, xc, S[l], y, 0.0);
+      continue;
+    }
+    const double r2 = xc * xc + y * y;
+    const double S1 = S[l] * y / M_PI;
+    if (r2 >= 1.0e6) {
+      out[l] = S1 / r2;
+    } else if (r2 >= 100.0) {
+      out[l] = S1 * hko_gh2(xc, y);
+    } else {
+      out[l] = S[l] / sqrt(M_PI) * hko_voigt916(xc, y);
+    }
+  }
+}
+
+void hko_opacity_p(int64_t n, const double *nu, const double *S,
+                   const double *iad, const double *vy, const int64_t *win,
+                   double numin, double dnu, int64_t ib, int64_t ie, double kmin,
+                   int profile, const double *plinth, double *K, int nthreads,
+                   int64_t pairs_out[3]) {
   lkey *ord = (lkey *)malloc((size_t)(n > 0 ? n : 1) * sizeof(lkey));
   double *ey = (double *)malloc((size_t)(n > 0 ? n : 1) * sizeof(double));
   int64_t m = 0, wmax = 0;
@@ -520,12 +580,16 @@ void hko_opacity(int64_t n, const double *nu, const double *S,
               (t3 * (2.0 * t2 + r2) - 2.0 * t1x) / (3.0 * r2 * (t3 * t2 - t1x));
           v = S1 * t4;
           ++pb;
+        } else if (profile != 1) {
+          v = profile_a(profile, x, Sl, y, dnu * il);
+          ++pa;
         } else {
           double r2 = x * x + y2;
           v = S1 / r2;
           ++pa;
         }
         acc[i - t0] += v;
+        if (plinth) acc[i - t0] -= plinth[l];
       }
     }
     for (int64_t i = t0; i < t1; ++i) K[i - ib] = kmin + acc[i - t0];

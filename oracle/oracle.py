@@ -67,6 +67,10 @@ def lib():
         L.hko_kdist.argtypes = [_p, _i64, _i, _i, _i, _d, _d, _p, _p, _p, _p,
                                 _p, _p]
         L.hko_planck.argtypes = [_d, _d, _p, _p]
+        L.hko_windows_p.argtypes = [_i64, _p, _p, _p, _p, _d, _d, _i64, _i, _d, _i, _p]
+        L.hko_plinth.argtypes = [_i64, _p, _p, _p, _p, _i, _d, _i, _p]
+        L.hko_opacity_p.argtypes = [_i64, _p, _p, _p, _p, _p, _d, _d, _i64, _i64, _d, _i, _p,
+                                    _p, _i, _p]
         L.hko_means.argtypes = [_p, _p, _i64, _d, _p]
         L.hko_transmission.argtypes = [_p, _i, _i, _p, _d, _i, _d, _p]
         _lib = L
@@ -155,18 +159,29 @@ def prep_exomol(lines: dict, mass, ab, Q, defaultL, defaultn, T, P,
     return tuple(outs)
 
 
-def windows(nu, S, iad, vy, numin, dnu, nx, cutMode, cut) -> np.ndarray:
+def windows(nu, S, iad, vy, numin, dnu, nx, cutMode, cut, profile=1) -> np.ndarray:
     """Per-line index windows (n, 6): i0, b0, c0, c1, b1, i1.
 
     Restates the region classes of voigt.h:2205-2341 and the per-pair
-    predicates of voigt.h:1223, 1481, 1662 as exact FP64 index ranges.
+    predicates of voigt.h:1223, 1481, 1662 as exact FP64 index ranges;
+    profiles 2-4 have no regions B and C.
     """
     nu, S, iad, vy = map(_f64, (nu, S, iad, vy))
     n = len(nu)
     win = np.empty((n, 6), np.int64)
-    lib().hko_windows(n, _ptr(nu), _ptr(S), _ptr(iad), _ptr(vy), numin, dnu,
-                      nx, cutMode, cut, _ptr(win))
+    lib().hko_windows_p(n, _ptr(nu), _ptr(S), _ptr(iad), _ptr(vy), numin, dnu,
+                        nx, cutMode, cut, int(profile), _ptr(win))
     return win
+
+
+def plinth(S, iad, vy, win, cutMode, cut, profile=1):
+    """Per-line profile value at the cut edge (Plinth_kernel voigt.h:1091-1164)."""
+    S, iad, vy = map(_f64, (S, iad, vy))
+    win = np.ascontiguousarray(win, dtype=np.int64)
+    out = np.empty(len(S), np.float64)
+    lib().hko_plinth(len(S), _ptr(S), _ptr(iad), _ptr(vy), _ptr(win), cutMode, cut, int(profile),
+                     _ptr(out))
+    return out
 
 
 def erfcx(y: float) -> float:
@@ -184,7 +199,7 @@ def gh2(x: float, y: float) -> float:
 
 
 def opacity(nu, S, iad, vy, win, numin, dnu, nx, kmin=0.0, nthreads=0,
-            irange=None):
+            irange=None, profile=1, plinth=None):
     """Line6fA/B/C + AddKStreams restated: K = kmin + sum of contributions.
 
     irange=(ib, ie) evaluates only grid indices ib <= i < ie of the nx-point
@@ -195,9 +210,10 @@ def opacity(nu, S, iad, vy, win, numin, dnu, nx, kmin=0.0, nthreads=0,
     ib, ie = irange if irange is not None else (0, nx)
     K = np.empty(ie - ib, np.float64)
     pairs = np.zeros(3, np.int64)
-    lib().hko_opacity(len(nu), _ptr(nu), _ptr(S), _ptr(iad), _ptr(vy),
-                      _ptr(win), numin, dnu, ib, ie, kmin, _ptr(K), nthreads,
-                      _ptr(pairs))
+    pl = None if plinth is None else _f64(plinth)
+    lib().hko_opacity_p(len(nu), _ptr(nu), _ptr(S), _ptr(iad), _ptr(vy),
+                        _ptr(win), numin, dnu, ib, ie, kmin, int(profile), _ptr(pl),
+                        _ptr(K), nthreads, _ptr(pairs))
     return K, tuple(int(p) for p in pairs)
 
 

@@ -1,0 +1,78 @@
+"""GPU: profiles 2-4 and plinth removal (hk_set_profile) against the FP64
+oracle (voigt.h:1091-1262 restated).
+
+Both precisions run the FP64 form for these, so the bound is the FP64 one:
+1e-12 relative where K > 1e-6 of its bin maximum; with plinth removal, where
+each point is a difference of profile values and plinths, 1e-9.  Index
+windows (no regions B and C for profiles 2-4) are bit-exact.
+"""
+import numpy as np
+import pytest
+
+import hkb
+import oracle
+from hkb import synth
+from test_gpu_parity import NBINS, DNU, NUMAX, NUMIN, masked_relerr
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small():
+    L = synth.hitran_lines(20000, seed=11, nu_max=3000.0)
+    Tq, Qq = synth.q_table()
+    ctx = hkb.Context(0)
+    ctx.set_species(hkb.HITRAN, [synth.MASS], [1.0])
+    ctx.set_partition(0, Tq, Qq)
+    ctx.set_options(qalphaL=1.0)
+    ctx.load_lines_hitran(L)
+    yield dict(ctx=ctx, L=L, Tq=Tq, Qq=Qq)
+    ctx.set_profile(1, 0)
+    ctx.close()
+
+
+def oracle_k(d, T, P, profile, plinth, cutMode, cut):
+    Q = oracle.partition(d["Tq"], d["Qq"], T)
+    nu, S, iad, vy = oracle.prep_hitran(d["L"], [synth.MASS], [1.0], [Q], T, P, qalphaL=1.0)
+    nx = oracle.grid_nx(NUMIN, NUMAX, DNU)
+    win = oracle.windows(nu, S, iad, vy, NUMIN, DNU, nx, cutMode, cut, profile=profile)
+    pl = oracle.plinth(S, iad, vy, win, cutMode, cut, profile) if plinth else None
+    K, _ = oracle.opacity(nu, S, iad, vy, win, NUMIN, DNU, nx, profile=profile, plinth=pl)
+    return K, win
+
+
+CASES = [(2, 0, 0, 25.0), (3, 0, 0, 25.0), (4, 0, 0, 25.0), (2, 0, 1, 500.0), (3, 0, 2, 40.0),
+         (1, 1, 0, 25.0), (2, 1, 0, 10.0), (3, 1, 0, 0.05), (1, 1, 1, 300.0)]
+
+
+@pytest.mark.parametrize("profile,plinth,cutMode,cut", CASES)
+def test_profile_matches_oracle(small, profile, plinth, cutMode, cut):
+    ctx = small["ctx"]
+    ctx.set_profile(profile, plinth)
+    ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, cutMode, cut)
+    for T, P in ((1500.0, 0.1), (500.0, 10.0)):
+        Kref, win = oracle_k(small, T, P, profile, plinth, cutMode, cut)
+        # the index rule on the device's own FP64 line parameters, bit-exact
+        gnu, gS, giad, gvy, gwin = ctx.state_lines(T, P)
+        nx = oracle.grid_nx(NUMIN, NUMAX, DNU)
+        assert np.array_equal(gwin, oracle.windows(gnu, gS, giad, gvy, NUMIN, DNU, nx, cutMode, cut,
+                                                   profile=profile))
+        if profile != 1:
+            assert np.all(gwin[:, 1] == gwin[:, 2]) and np.all(gwin[:, 3] == gwin[:, 4])
+        for prec in (hkb.MIXED, hkb.PLAIN_FP64):
+            K = ctx.opacity([T], [P], prec)[0]
+            err, n = masked_relerr(K, Kref, NBINS)
+            print(f"profile {profile} plinth {plinth} cut {cutMode}/{cut} T={T} P={P} err {err:.2e}")
+            assert err < (1e-9 if plinth else 1e-12)
+    with pytest.raises(hkb.HkError) as e:
+        ctx.opacity_vjp(1500.0, 0.1, np.ones(ctx.nx))
+    assert e.value.status == -8
+    ctx.set_profile(1, 0)
+
+
+def test_profile_arguments(small):
+    ctx = small["ctx"]
+    for bad in ((0, 0), (5, 0), (1, 2)):
+        with pytest.raises(hkb.HkError) as e:
+            ctx.set_profile(*bad)
+        assert e.value.status == -1
