@@ -60,7 +60,21 @@ int main(int argc, char **argv) {
   std::string msg;
   if (read_param_file("param.dat", argc, argv, p, msg) != 0) return die(msg);
   if (p.ciaSystem != "-") return die("Error: ciaSystem is outside this build's opacity path");
-  if (p.SpeciesFilename != "-") return die("Error: species mixtures (SpeciesFile) are outside this build's path");
+  // SpeciesFile: "<species> <abundance>" pairs (host.h:463-487, 579-590)
+  std::vector<std::string> mixNames;
+  std::vector<double> mixAb;
+  if (p.SpeciesFilename != "-") {
+    FILE *sf = fopen(p.SpeciesFilename.c_str(), "r");
+    if (!sf) return die("Error: Species file not found: " + p.SpeciesFilename);
+    char b[160];
+    double a;
+    while (fscanf(sf, "%159s %lf", b, &a) == 2) {
+      mixNames.push_back(b);
+      mixAb.push_back(a);
+    }
+    fclose(sf);
+    if (mixNames.empty()) return die("Error: no species in file " + p.SpeciesFilename);
+  }
   if (p.bins != "-" || p.edges != "-") return die("Error: binsFile / OutputEdgesFile are outside this build's path");
   if (p.Nxb != 0) return die("Error: 'Nnu per bin' (unequal spacing) is outside this build's path");
   if (p.subLorentzian != "-") return die("Error: sub-Lorentzian profiles are outside this build's path");
@@ -104,6 +118,8 @@ int main(int argc, char **argv) {
             p.cutMode, p.cut, p.doResampling, p.nC, p.doStoreFullK, p.doStoreK);
     fprintf(f, "nbins = %d\nkmin = %g\nqalphaL = %g\ngammaF = %g\nUnits = %d\nReplace files = %d\nprofile = %d\n",
             p.nbins, p.kmin, p.qalphaL, p.gammaF, p.units, p.replaceFiles, p.profile);
+    if (!mixNames.empty())
+      fprintf(f, "Species in file: %s\nNumber of Species: %d\n", p.SpeciesFilename.c_str(), (int)mixNames.size());
     fprintf(f, "Species Name = %s\nengine = %s\n\n", p.speciesName.c_str(), hk_version());
   }
 
@@ -122,7 +138,14 @@ int main(int argc, char **argv) {
 
   const bool compute = p.doStoreFullK >= 0;
   cudaEventRecord(t0);
-  if (compute) chk(hk_load_species_file(c, p.path.c_str(), p.speciesName.c_str(), p.numin, p.numax, p.cutMode, p.cut));
+  if (compute && mixNames.empty())
+    chk(hk_load_species_file(c, p.path.c_str(), p.speciesName.c_str(), p.numin, p.numax, p.cutMode, p.cut));
+  if (compute && !mixNames.empty()) {
+    std::vector<const char *> names;
+    for (auto &n : mixNames) names.push_back(n.c_str());
+    chk(hk_load_mixture(c, p.path.c_str(), (int)names.size(), names.data(), mixAb.data(), p.numin, p.numax,
+                        p.cutMode, p.cut));
+  }
   cudaEventRecord(t1);
   const double t_input = compute ? seconds() : 0.0;
   chk(hk_set_grid(c, p.numin, p.numax, p.dnu, p.nbins, p.cutMode, p.cut, kmin));

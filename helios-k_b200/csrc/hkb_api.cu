@@ -47,6 +47,7 @@ struct hk_ctx {
   std::vector<double> iso_mass, iso_ab;
   double defaultL = 0.0, defaultn = 0.0;
   std::vector<std::vector<double>> qT, qQ;
+  std::vector<double> iso_ss;  // per-isotopologue species scale (mixtures), empty = 1
   double qalphaL = 0.5, gammaF = 1.0, Sscale = 1.0;
   int units = 0;
   // lines (device, nu-sorted)
@@ -185,6 +186,7 @@ hk_status hk_set_species(hk_ctx *c, int database, int niso, const double *mass,
   c->defaultn = defaultn;
   c->qT.assign(niso, {});
   c->qQ.assign(niso, {});
+  c->iso_ss.clear();
   ok(c);
   return HK_OK;
 }
@@ -417,8 +419,11 @@ int64_t hk_grid_points(const hk_ctx *c) { return (c && c->grid_set) ? c->g.nx : 
 static hk_status build_states(hk_ctx *c, int nstates, const double *T, const double *P,
                               std::vector<StateDev> &out) {
   const int niso = (int)c->iso_mass.size();
-  double meanMass = 0.0;  // heliosk.cu:672-686
-  for (int i = 0; i < niso; ++i) meanMass += c->iso_ab[i] * c->iso_mass[i] * c->Sscale;
+  // species scale of each isotopologue: Sscale, times the species' abundance
+  // in a mixture; mean molar mass over all of them (heliosk.cu:672-686)
+  auto sscale = [&](int i) { return c->iso_ss.empty() ? c->Sscale : c->Sscale * c->iso_ss[i]; };
+  double meanMass = 0.0;
+  for (int i = 0; i < niso; ++i) meanMass += c->iso_ab[i] * c->iso_mass[i] * sscale(i);
   out.assign(nstates, StateDev{});
   for (int s = 0; s < nstates; ++s) {
     StateDev &st = out[s];
@@ -445,7 +450,7 @@ static hk_status build_states(hk_ctx *c, int nstates, const double *T, const dou
       partition_dlnq(c->qT[j].data(), c->qQ[j].data(), (int)c->qT[j].size(), Ts, &dl);
       st.dlnQ[j] = dl;
       double Abundance = c->iso_ab[j];
-      double Ss = c->Sscale;
+      double Ss = sscale(j);
       if (c->units == 0) {
         Abundance *= c->iso_mass[j] / meanMass;
         Ss *= c->iso_mass[j] / meanMass;
@@ -1256,17 +1261,12 @@ hk_status hk_fp32_peak(hk_ctx *c, double *tflops) {
 // memory beyond the kernel's file cache.
 static constexpr int64_t kIngestChunk = 1 << 20;  // records per chunk
 
-static hk_status stream_line_files(hk_ctx *c, const SpeciesInfo &sp, int fi0, int fi1) {
+// One species' selected files into ib's columns from line base0 on; the
+// species' isotopologues are spec.iso_base + (0 .. niso-1).
+static hk_status stream_species(hk_ctx *c, const SpeciesInfo &sp, int fi0, int fi1,
+                                const IngestSpec &spec, IngestBuf &ib, int64_t base0) {
   const bool hitran = sp.database == HK_DB_HITRAN;
   const size_t rec = hitran ? 68 : 32;
-  int64_t n = 0;
-  for (int fi = fi0; fi < fi1; ++fi) n += sp.NL[fi];
-  IngestSpec spec = ingest_spec(c, hitran);
-  for (size_t k = 0; k < sp.iso.size() && k < (size_t)HK_MAX_ISO; ++k)
-    strncpy(spec.cid[k], sp.iso[k].cid.c_str(), 4);  // zero-padded, as strncmp(.., 4) reads it
-  cudaSetDevice(c->device);
-  IngestBuf ib;
-  CUDA_TRY(c, ib.alloc(n));
   struct Pipe {
     unsigned char *host[2] = {nullptr, nullptr};
     DevBuf dev[2], bad;
@@ -1293,7 +1293,7 @@ static hk_status stream_line_files(hk_ctx *c, const SpeciesInfo &sp, int fi0, in
   CUDA_TRY(c, pp.bad.ensure(sizeof(unsigned long long)));
   const unsigned long long none = ~0ull;
   CUDA_TRY(c, cudaMemcpy(pp.bad.p, &none, sizeof none, cudaMemcpyHostToDevice));
-  int64_t base = 0;
+  int64_t base = base0;
   int b = 0;
   bool used[2] = {false, false};
   for (int fi = fi0; fi < fi1; ++fi) {
@@ -1328,7 +1328,7 @@ static hk_status stream_line_files(hk_ctx *c, const SpeciesInfo &sp, int fi0, in
   CUDA_TRY(c, cudaMemcpy(&bad, pp.bad.p, sizeof bad, cudaMemcpyDeviceToHost));
   if (bad != none) {
     // host.h:624-639: a record whose isotopologue id is not in the species table
-    int64_t i = (int64_t)bad;
+    int64_t i = (int64_t)bad - base0;
     int fi = fi0;
     while (fi + 1 < fi1 && i >= sp.NL[fi]) i -= sp.NL[fi++];
     char cid[4] = {0, 0, 0, 0};
@@ -1340,6 +1340,27 @@ static hk_status stream_line_files(hk_ctx *c, const SpeciesInfo &sp, int fi0, in
     return fail(c, HK_ERR_FORMAT, "Error: partition function not found. %lld |%.3s|%s|", (long long)i,
                 cid, sp.iso[0].cid.c_str());
   }
+  return HK_OK;
+}
+
+static IngestSpec species_spec(const hk_ctx *c, const SpeciesInfo &sp, int iso_base) {
+  IngestSpec spec = ingest_spec(c, sp.database == HK_DB_HITRAN);
+  spec.defaultL = sp.defaultL;
+  spec.defaultn = sp.defaultn;
+  spec.iso_base = iso_base;
+  for (size_t k = 0; k < sp.iso.size() && k < (size_t)HK_MAX_ISO; ++k)
+    strncpy(spec.cid[k], sp.iso[k].cid.c_str(), 4);  // zero-padded, as strncmp(.., 4) reads it
+  return spec;
+}
+
+static hk_status stream_line_files(hk_ctx *c, const SpeciesInfo &sp, int fi0, int fi1) {
+  int64_t n = 0;
+  for (int fi = fi0; fi < fi1; ++fi) n += sp.NL[fi];
+  cudaSetDevice(c->device);
+  IngestBuf ib;
+  CUDA_TRY(c, ib.alloc(n));
+  hk_status st = stream_species(c, sp, fi0, fi1, species_spec(c, sp, 0), ib, 0);
+  if (st != HK_OK) return st;
   return load_device(c, n, ib, (int)sp.iso.size());
 }
 
@@ -1367,6 +1388,73 @@ hk_status hk_load_species_file(hk_ctx *c, const char *path, const char *species,
   int fi0, fi1;
   line_file_range(sp, numin, numax, cutMode, cut, &fi0, &fi1);
   return stream_line_files(c, sp, fi0, fi1);
+}
+
+// Species mixtures (param.dat SpeciesFile, heliosk.cu:660-700 and 784-800):
+// the reference runs its whole line pipeline once per species, scaling that
+// species' strengths by its abundance, and sums into one K; the mean molar
+// mass (units 0 scaling) is the mixture's.  Here every species' lines go
+// into one line list -- isotopologue indices offset per species, the
+// abundance as the isotopologues' strength scale -- and one opacity call
+// sums them all.
+hk_status hk_load_mixture(hk_ctx *c, const char *path, int nspecies, const char *const *species,
+                          const double *abundance, double numin, double numax, int cutMode,
+                          double cut) {
+  if (!c) return HK_ERR_ARG;
+  if (nspecies < 1 || !species || (nspecies > 1 && !abundance))
+    return fail(c, HK_ERR_ARG, "need nspecies >= 1, species names and (for several) abundances");
+  std::vector<SpeciesInfo> sps(nspecies);
+  std::string msg;
+  int niso = 0;
+  for (int s = 0; s < nspecies; ++s) {
+    if (!species[s]) return fail(c, HK_ERR_ARG, "species %d: null name", s);
+    if (nspecies > 1 && !(abundance[s] >= 0.0 && std::isfinite(abundance[s])))
+      return fail(c, HK_ERR_ARG, "species %d: abundance must be finite and >= 0", s);
+    int rc = read_species_param(path ? path : "", species[s], sps[s], msg);
+    if (rc != 0) return fail(c, rc, "%s", msg.c_str());
+    if (sps[s].database != sps[0].database)
+      return fail(c, HK_ERR_UNSUPPORTED, "species %s: mixtures of HITRAN- and ExoMol-format species are not supported",
+                  species[s]);
+    niso += (int)sps[s].iso.size();
+  }
+  if (niso > HK_MAX_ISO) return fail(c, HK_ERR_RANGE, "the mixture has %d isotopologues, at most %d", niso, HK_MAX_ISO);
+  std::vector<double> mass, ab, ss;
+  for (int s = 0; s < nspecies; ++s)
+    for (auto &iso : sps[s].iso) {
+      mass.push_back(iso.mass);
+      ab.push_back(iso.ab);
+      ss.push_back(nspecies > 1 ? abundance[s] : 1.0);  // heliosk.cu:786-789
+    }
+  hk_status st = hk_set_species(c, sps[0].database, niso, mass.data(), ab.data(), sps[0].defaultL,
+                                sps[0].defaultn);
+  if (st != HK_OK) return st;
+  int j = 0;
+  for (int s = 0; s < nspecies; ++s)
+    for (auto &iso : sps[s].iso) {
+      std::vector<double> T, Q;
+      int rc = read_q_file(iso.qfile, sps[s].npfcol, T, Q, msg);
+      if (rc != 0) return fail(c, rc, "%s", msg.c_str());
+      if ((st = hk_set_partition(c, j++, (int)T.size(), T.data(), Q.data())) != HK_OK) return st;
+    }
+  c->iso_ss = ss;
+  std::vector<int> f0(nspecies), f1(nspecies);
+  int64_t n = 0;
+  for (int s = 0; s < nspecies; ++s) {
+    line_file_range(sps[s], numin, numax, cutMode, cut, &f0[s], &f1[s]);
+    for (int fi = f0[s]; fi < f1[s]; ++fi) n += sps[s].NL[fi];
+  }
+  cudaSetDevice(c->device);
+  IngestBuf ib;
+  CUDA_TRY(c, ib.alloc(n));
+  int64_t base = 0;
+  int iso_base = 0;
+  for (int s = 0; s < nspecies; ++s) {
+    if ((st = stream_species(c, sps[s], f0[s], f1[s], species_spec(c, sps[s], iso_base), ib, base)) != HK_OK)
+      return st;
+    for (int fi = f0[s]; fi < f1[s]; ++fi) base += sps[s].NL[fi];
+    iso_base += (int)sps[s].iso.size();
+  }
+  return load_device(c, n, ib, niso);
 }
 
 }  // extern "C"

@@ -85,7 +85,7 @@ __global__ void unpack_records_kernel(const unsigned char *__restrict__ raw, int
     cols.nexp[i] = ne;
     cols.delta[i] = de;
     cols.Aterm[i] = __ddiv_rn(A, sp.four_pi_c);
-    cols.iso[i] = (uint8_t)j;
+    cols.iso[i] = (uint8_t)(sp.iso_base + j);
   }
 }
 

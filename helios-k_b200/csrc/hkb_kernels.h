@@ -69,6 +69,7 @@ struct IngestSpec {
   char cid[HK_MAX_ISO][4];
   double qalphaL, gammaF, defaultL, defaultn;
   double four_pi_c;     // 4 pi c as the host forms it
+  int iso_base;         // the species' first isotopologue index (mixtures)
 };
 struct LineCols {
   double *nu, *S, *EL, *gam, *nexp, *delta, *Aterm;

@@ -24,7 +24,7 @@ constexpr float HK_C916_F = 0.38196948170661926f;
 
 constexpr int HK_DB_HITRAN = 0;
 constexpr int HK_DB_EXOMOL = 2;
-constexpr int HK_MAX_ISO = 16;
+constexpr int HK_MAX_ISO = 64;  // isotopologues of all species of a mixture
 
 // Sorted line list resident in HBM (SoA, FP64).  A null array means the
 // column is uniform and its *_c scalar is used instead.
@@ -116,6 +116,6 @@ struct StateDev {
   double ss[HK_MAX_ISO];    // species scale * (m / meanMass) when units == 0
   double dlnQ[HK_MAX_ISO];  // d ln Q / dT of the interpolated partition function
 };
-static_assert(sizeof(StateDev) == 728, "StateDev layout (the host copies it per state)");
+static_assert(sizeof(StateDev) == 2648, "StateDev layout (the host copies it per state)");
 
 }  // namespace hkb

@@ -89,6 +89,7 @@ def lib():
             "hk_tuning_result": (_i, [_p, _p, _p, _p]),
             "hk_means": (_i, [_p, _i, _p, _p, _i, _p, _i, _p]),
             "hk_set_profile": (_i, [_p, _i, _i]),
+            "hk_load_mixture": (_i, [_p, C.c_char_p, _i, _p, _p, _d, _d, _i, _d]),
             "hk_transmission": (_i, [_p, _i, _p, _p, _i, _i, _d, _p, _i, _p]),
         }
         for name, (res, args) in sig.items():
@@ -184,6 +185,14 @@ class Context:
     def load_species_file(self, path, species, numin, numax, cutMode, cut):
         self._chk(lib().hk_load_species_file(self._h, path.encode(), species.encode(),
                                              numin, numax, cutMode, cut))
+
+    def load_mixture(self, path, species, abundances, numin, numax, cutMode, cut):
+        """Several species' line files as one line list (SpeciesFile)."""
+        names = (C.c_char_p * len(species))(*[x.encode() for x in species])
+        ab = _f64(abundances)
+        self._chk(lib().hk_load_mixture(self._h, path.encode(), len(species),
+                                        C.cast(names, C.c_void_p), _ptr(ab), numin, numax,
+                                        cutMode, cut))
 
     @property
     def num_lines(self):

@@ -106,6 +106,18 @@ hk_status hk_load_species_file(hk_ctx *ctx, const char *path,
                                const char *species, double numin, double numax,
                                int cutMode, double cut);
 
+/* Species mixture (param.dat SpeciesFile: "<species> <abundance>" per line),
+ * replacing the per-species loop of heliosk.cu:660-700, 784-800: every
+ * species' selected line files are loaded into one line list (its
+ * isotopologues after the previous species'), each species' strengths scaled
+ * by its abundance (1 when nspecies == 1, as the reference), the mean molar
+ * mass taken over the mixture; one hk_opacity then sums all species.  All
+ * species must share the record format (HITRAN or ExoMol); at most 64
+ * isotopologues in all. */
+hk_status hk_load_mixture(hk_ctx *ctx, const char *path, int nspecies, const char *const *species,
+                          const double *abundance, double numin, double numax, int cutMode,
+                          double cut);
+
 int64_t hk_num_lines(const hk_ctx *ctx);
 
 /* --------------------------------------------------------------- grid */
