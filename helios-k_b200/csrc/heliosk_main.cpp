@@ -77,7 +77,8 @@ int main(int argc, char **argv) {
   }
   if (p.bins != "-" || p.edges != "-") return die("Error: binsFile / OutputEdgesFile are outside this build's path");
   if (p.Nxb != 0) return die("Error: 'Nnu per bin' (unequal spacing) is outside this build's path");
-  if (p.subLorentzian != "-") return die("Error: sub-Lorentzian profiles are outside this build's path");
+  double subL[14];
+  if (p.subLorentzian != "-" && read_sublorentz_file(p.subLorentzian, subL, msg) != 0) return die(msg);
   if (p.removePlinth != 0 && p.removePlinth != 1) return die("Error: removePlinth must be 0 or 1");
   if (p.profile < 1 || p.profile > 4) return die("Error: profile must be 1, 2, 3 or 4");
   if (p.doTransmission < 0 || p.doTransmission > 2) return die("Error: doTransmission must be 0, 1 or 2");
@@ -120,15 +121,22 @@ int main(int argc, char **argv) {
             p.nbins, p.kmin, p.qalphaL, p.gammaF, p.units, p.replaceFiles, p.profile);
     if (!mixNames.empty())
       fprintf(f, "Species in file: %s\nNumber of Species: %d\n", p.SpeciesFilename.c_str(), (int)mixNames.size());
+    if (p.subLorentzian != "-") fprintf(f, "sub-Lorentzian file: %s\n", p.subLorentzian.c_str());
     fprintf(f, "Species Name = %s\nengine = %s\n\n", p.speciesName.c_str(), hk_version());
   }
 
   chk(hk_set_options(c, p.qalphaL, p.gammaF, p.units, 1.0));
-  SpeciesInfo sp;
-  int rc = read_species_param(p.path, p.speciesName, sp, msg);
-  if (rc != 0) return die(msg);
-  double meanMass = 0.0;  // heliosk.cu:665-686
-  for (auto &iso : sp.iso) meanMass += iso.ab * iso.mass * 1.0;
+  // mean molar mass over the species (of the mixture), heliosk.cu:665-686
+  double meanMass = 0.0;
+  {
+    const std::vector<std::string> names = mixNames.empty() ? std::vector<std::string>{p.speciesName} : mixNames;
+    for (size_t k = 0; k < names.size(); ++k) {
+      SpeciesInfo sp;
+      if (read_species_param(p.path, names[k], sp, msg) != 0) return die(msg);
+      const double Sscale = names.size() > 1 ? mixAb[k] : 1.0;
+      for (auto &iso : sp.iso) meanMass += iso.ab * iso.mass * Sscale;
+    }
+  }
   double unitScale = 1.0;
   double kmin = p.kmin;
   if (p.units == 1) {  // heliosk.cu:692-701
@@ -150,6 +158,7 @@ int main(int argc, char **argv) {
   const double t_input = compute ? seconds() : 0.0;
   chk(hk_set_grid(c, p.numin, p.numax, p.dnu, p.nbins, p.cutMode, p.cut, kmin));
   chk(hk_set_profile(c, p.profile, p.removePlinth));
+  if (p.subLorentzian != "-") chk(hk_set_sublorentzian(c, subL));
   // doTuning = 1: the tile-shape tuner, where its probes pay off (PFile tables)
   chk(hk_set_tuning(c, p.doTuning == 1 ? 1 : 0));
   const int64_t nx = hk_grid_points(c);

@@ -48,6 +48,7 @@ struct hk_ctx {
   double defaultL = 0.0, defaultn = 0.0;
   std::vector<std::vector<double>> qT, qQ;
   std::vector<double> iso_ss;  // per-isotopologue species scale (mixtures), empty = 1
+  double sl_abe[9] = {};       // sub-Lorentzian alpha, beta, epsilon of B1, B2, B3
   double qalphaL = 0.5, gammaF = 1.0, Sscale = 1.0;
   int units = 0;
   // lines (device, nu-sorted)
@@ -438,6 +439,9 @@ static hk_status build_states(hk_ctx *c, int nstates, const double *T, const dou
     st.wmax = c->g.cut;
     st.shift = c->max_abs_delta * Ps;
     st.kmin = c->kmin;
+    // subLorentzianB (voigt.h:12-35): B_k = alpha_k + beta_k exp(-epsilon_k T)
+    for (int k = 0; k < 3; ++k)
+      st.sl_B[k] = c->sl_abe[3 * k] + c->sl_abe[3 * k + 1] * std::exp(-c->sl_abe[3 * k + 2] * Ts);
     for (int j = 0; j < niso; ++j) {
       double Q;
       if (c->qT[j].empty()) return fail(c, HK_ERR_STATE, "no partition table for isotopologue %d", j);
@@ -655,9 +659,9 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   }
   // States run in batches whose per-(state, line) records fit the prep
   // budget; each batch is one prep launch and one persistent Voigt launch.
-  // profiles 2-4 and plinth removal run the FP64 form (the mixed form's
-  // FP32 region sums are built for the Voigt profile's regions)
-  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile == 1 && !c->g.plinth;
+  // profiles 2-4, plinth removal and sub-Lorentzian wings run the FP64 form
+  // (the mixed form's FP32 region sums are built for the plain Voigt regions)
+  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile == 1 && !c->g.plinth && !c->g.subL;
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
@@ -868,8 +872,30 @@ hk_status hk_set_profile(hk_ctx *c, int profile, int remove_plinth) {
   if (profile < 1 || profile > 4)
     return fail(c, HK_ERR_ARG, "profile must be 1 (Voigt), 2 (Lorentz), 3 (Doppler) or 4 (binned Gaussian)");
   if (remove_plinth != 0 && remove_plinth != 1) return fail(c, HK_ERR_ARG, "remove_plinth must be 0 or 1");
+  if (remove_plinth && profile == 4)  // heliosk.cu:410-413
+    return fail(c, HK_ERR_UNSUPPORTED, "Error, remove plinth is not supported for profile 4");
   c->g.profile = profile;
   c->g.plinth = remove_plinth;
+  c->tuned = false;
+  table_release(c);
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_set_sublorentzian(hk_ctx *c, const double *p) {
+  if (!c) return HK_ERR_ARG;
+  if (!p) {
+    c->g.subL = 0;
+  } else {
+    for (int k = 0; k < 14; ++k)
+      if (!std::isfinite(p[k])) return fail(c, HK_ERR_ARG, "sub-Lorentzian parameter %d is not finite", k);
+    if (!(p[0] <= p[1] && p[1] <= p[2])) return fail(c, HK_ERR_ARG, "need sigma1 <= sigma2 <= sigma3");
+    c->g.subL = 1;
+    for (int k = 0; k < 3; ++k) c->g.sl_sigma[k] = p[k];
+    for (int k = 0; k < 9; ++k) c->sl_abe[k] = p[3 + k];
+    c->g.sl_lo = p[12];
+    c->g.sl_hi = p[13];
+  }
   c->tuned = false;
   table_release(c);
   ok(c);
@@ -953,8 +979,9 @@ hk_status hk_opacity_vjp(hk_ctx *c, double T, double P, int precision, const dou
   if (!u) return fail(c, HK_ERR_ARG, "need the seed u (Nx values)");
   if (precision != HK_PRECISION_PLAIN_FP64 && precision != HK_PRECISION_MIXED)
     return fail(c, HK_ERR_ARG, "precision must be 0 (plain FP64) or 1 (mixed)");
-  if (c->g.profile != 1 || c->g.plinth)
-    return fail(c, HK_ERR_UNSUPPORTED, "the adjoint is for the Voigt profile without plinth removal");
+  if (c->g.profile != 1 || c->g.plinth || c->g.subL)
+    return fail(c, HK_ERR_UNSUPPORTED,
+                "the adjoint is for the Voigt profile without plinth removal or sub-Lorentzian wings");
   cudaSetDevice(c->device);
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<StateDev> hs;
@@ -1031,9 +1058,9 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   CUDA_TRY(c, c->wbits.ensure(2 * nstates * sizeof(unsigned long long)));
   CUDA_TRY(c, cudaMemcpy(c->states.p, hs.data(), nstates * sizeof(StateDev), cudaMemcpyHostToDevice));
   const int64_t nx = c->g.nx;
-  // profiles 2-4 and plinth removal run the FP64 form (the mixed form's
-  // FP32 region sums are built for the Voigt profile's regions)
-  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile == 1 && !c->g.plinth;
+  // profiles 2-4, plinth removal and sub-Lorentzian wings run the FP64 form
+  // (the mixed form's FP32 region sums are built for the plain Voigt regions)
+  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile == 1 && !c->g.plinth && !c->g.subL;
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
   if (per_state > c->prep_budget)
     return fail(c, HK_ERR_UNSUPPORTED, "one state's line records (%zu B) exceed the workspace (%zu B): "

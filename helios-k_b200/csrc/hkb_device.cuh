@@ -295,6 +295,23 @@ __device__ __forceinline__ double profile_a_d(int profile, double x, double y2, 
   return S1 / (x * x + y2);  // profile 1 region A, profile 2
 }
 
+// Sub-Lorentzian factor chi(|x - nu|) x / nu for a grid point x of a line
+// at nu (sLChi voigt.h:47-72 and its use in Line6fAX/BX/CX, voigt.h:1345-
+// 1790), in FP64: 1 outside (sl_lo, sl_hi); chi piecewise exponential with
+// breakpoints sigma1 < sigma2 < sigma3 and the state's slopes B1, B2, B3.
+__device__ __forceinline__ double sublorentz_d(const GridDev &g, const StateDev &st, double x,
+                                               double nu) {
+  if (!(x > g.sl_lo && x < g.sl_hi)) return 1.0;
+  const double d = fabs(x - nu);
+  const double s1 = g.sl_sigma[0], s2 = g.sl_sigma[1], s3 = g.sl_sigma[2];
+  double chi;
+  if (d < s1) chi = 1.0;
+  else if (d < s2) chi = exp(-st.sl_B[0] * (d - s1));
+  else if (d < s3) chi = exp(-st.sl_B[0] * (s2 - s1) - st.sl_B[1] * (d - s2));
+  else chi = exp(-st.sl_B[0] * (s2 - s1) - st.sl_B[1] * (s3 - s2) - st.sl_B[2] * (d - s3));
+  return chi * x / nu;
+}
+
 // The profile's value at the line's cut edge, x_c = cut iad (cutMode 0),
 // cut y (1) or cut (2): Plinth_kernel (voigt.h:1091-1164) in FP64, the Voigt
 // profile by the region of r^2 = x_c^2 + y^2; 0 for the binned Gaussian (the

@@ -216,6 +216,31 @@ void line_file_range(const SpeciesInfo &sp, double numin, double numax, int cutM
   *fi1_out = fi1;
 }
 
+// host.h:489-515: the sub-Lorentzian file, "name value" for sigma1..3, a
+// 4-word header, "name alpha beta epsilon" for B1..B3, a 3-word header and
+// the range "lo hi" -> p[14] = {sigma1..3, alpha1, beta1, eps1, ..., lo, hi}
+int read_sublorentz_file(const std::string &fname, double p[14], std::string &msg) {
+  FILE *f = fopen(fname.c_str(), "r");
+  if (!f) {
+    msg = "Error: sub-Lorentzian file not found: " + fname;
+    return HK_ERR_IO;
+  }
+  char b[4][160];
+  bool good = true;
+  for (int k = 0; k < 3 && good; ++k) good = fscanf(f, "%159s %lf", b[0], &p[k]) == 2;
+  good = good && fscanf(f, "%159s %159s %159s %159s", b[0], b[1], b[2], b[3]) == 4;
+  for (int k = 0; k < 3 && good; ++k)
+    good = fscanf(f, "%159s %lf %lf %lf", b[0], &p[3 + 3 * k], &p[4 + 3 * k], &p[5 + 3 * k]) == 4;
+  good = good && fscanf(f, "%159s %159s %159s", b[0], b[1], b[2]) == 3;
+  good = good && fscanf(f, "%lf %lf", &p[12], &p[13]) == 2;
+  fclose(f);
+  if (!good) {
+    msg = "Error in sub-Lorentzian file read " + fname;
+    return HK_ERR_FORMAT;
+  }
+  return 0;
+}
+
 // host.h:75-525 (read_parameters): "key = value" lines, an unknown key is an
 // error; then "-flag value" command-line overrides.
 int read_param_file(const std::string &fname, int argc, char **argv, Params &p,

@@ -60,6 +60,7 @@ int read_species_param(const std::string &path, const std::string &species,
                        SpeciesInfo &sp, std::string &msg);
 void line_file_range(const SpeciesInfo &sp, double numin, double numax, int cutMode, double cut,
                      int *fi0, int *fi1);
+int read_sublorentz_file(const std::string &fname, double p[14], std::string &msg);
 int read_param_file(const std::string &fname, int argc, char **argv, Params &p,
                     std::string &msg);
 

@@ -55,6 +55,13 @@ struct GridDev {
   // edge is subtracted inside its cut window (removePlinth)
   int profile = 1;
   int plinth = 0;
+  // sub-Lorentzian wings (Perrin & Hartmann 1989 chi, voigt.h:1-72): on when
+  // subL = 1, for grid points with sl_lo < x < sl_hi; chi's breakpoints
+  // sl_sigma (cm^-1); the per-state slopes are StateDev.sl_B
+  int subL = 0;
+  int pad_g = 0;
+  double sl_sigma[3] = {0.0, 0.0, 0.0};
+  double sl_lo = 0.0, sl_hi = 0.0;
 };
 
 // One line scaled to one state, as written by line_prep_kernel and read by
@@ -115,7 +122,8 @@ struct StateDev {
   double ab[HK_MAX_ISO];    // abundance * (m / meanMass) when units == 0
   double ss[HK_MAX_ISO];    // species scale * (m / meanMass) when units == 0
   double dlnQ[HK_MAX_ISO];  // d ln Q / dT of the interpolated partition function
+  double sl_B[3];           // sub-Lorentzian slopes alpha + beta exp(-epsilon T)
 };
-static_assert(sizeof(StateDev) == 2648, "StateDev layout (the host copies it per state)");
+static_assert(sizeof(StateDev) == 2672, "StateDev layout (the host copies it per state)");
 
 }  // namespace hkb

@@ -495,12 +495,14 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
 template <int PPL>
 __device__ __forceinline__ void sweep_plain(const RecD &r, int wb, int lane,
                                             const double (&xg)[PPL],
-                                            double (&acc)[PPL], const GridDev &g) {
+                                            double (&acc)[PPL], const GridDev &g,
+                                            const StateDev &st) {
   const int we = wb + 32 * PPL;
   if (r.i1 <= wb || r.i0 >= we) return;
-  if (g.profile != 1 || g.plinth) {
-    // profiles 2-4 (region A only) and plinth removal: Line6fA/B/C add the
-    // profile, then subtract the line's plinth, at every window point
+  if (g.profile != 1 || g.plinth || g.subL) {
+    // profiles 2-4 (region A only), sub-Lorentzian wings and plinth removal:
+    // Line6fA/B/C(X) add the profile (times chi x/nu), then subtract the
+    // line's plinth, at every window point
     const double vb = g.dnu * r.iad;
 #pragma unroll
     for (int p = 0; p < PPL; ++p) {
@@ -511,6 +513,7 @@ __device__ __forceinline__ void sweep_plain(const RecD &r, int wb, int lane,
         if (k >= r.c0 && k < r.c1) v = r.Sc * voigt916_d(x, r.y, r.ey);
         else if (k >= r.b0 && k < r.b1) v = r.S1 * gh2_d(x, r.y2);
         else v = profile_a_d(g.profile, x, r.y2, r.S1, vb);
+        if (g.subL) v *= sublorentz_d(g, st, xg[p], r.nu);
         acc[p] += v;
         acc[p] -= r.pl;
       }
@@ -745,7 +748,7 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
         flush_sums<PPL>(a32, cacc, wb, lane, st.s1exp, lcur);
       } else {
         for (int j = 0; j < cnt; ++j)
-          sweep_plain<PPL>(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc, g);
+          sweep_plain<PPL>(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc, g, st);
       }
       __syncthreads();
     }

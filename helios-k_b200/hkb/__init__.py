@@ -89,6 +89,7 @@ def lib():
             "hk_tuning_result": (_i, [_p, _p, _p, _p]),
             "hk_means": (_i, [_p, _i, _p, _p, _i, _p, _i, _p]),
             "hk_set_profile": (_i, [_p, _i, _i]),
+            "hk_set_sublorentzian": (_i, [_p, _p]),
             "hk_load_mixture": (_i, [_p, C.c_char_p, _i, _p, _p, _d, _d, _i, _d]),
             "hk_transmission": (_i, [_p, _i, _p, _p, _i, _i, _d, _p, _i, _p]),
         }
@@ -263,6 +264,14 @@ class Context:
         subtracts each line's value at its cut edge (FP64 form for 2-4 and
         plinth removal)."""
         self._chk(lib().hk_set_profile(self._h, int(profile), int(remove_plinth)))
+
+    def set_sublorentzian(self, params=None):
+        """14 values (sigma1..3, alpha/beta/epsilon of B1..B3, x_lo, x_hi) or
+        None to turn the sub-Lorentzian chi factor off."""
+        p = None if params is None else _f64(params)
+        if p is not None and len(p) != 14:
+            raise ValueError("need 14 sub-Lorentzian parameters")
+        self._chk(lib().hk_set_sublorentzian(self._h, _ptr(p)))
 
     # ------------------------------------ mean opacities, transmission
     def means(self, T, K, stream=None):

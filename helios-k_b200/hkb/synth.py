@@ -186,7 +186,12 @@ def write_param(path, **kv):
             ("binsFile", "-"), ("OutputEdgesFile", "-"), ("kmin", 0.0), ("qalphaL", 1.0),
             ("gammaF", 1.0), ("doMean", 0), ("Units", 0), ("ReplaceFiles", 1),
             ("profile", 1), ("doTuning", 1)]
+    # optional keys (host.h:95-299), written only when given
+    optional = ["removePlinth", "subLorentzianfile"]
     with open(path, "w") as f:
         for k, default in keys:
             v = kv.get(k.replace(" ", "_"), kv.get(k, default))
             f.write(f"{k} = {v}\n")
+        for k in optional:
+            if k in kv:
+                f.write(f"{k} = {kv[k]}\n")

@@ -192,6 +192,15 @@ hk_status hk_set_workspace(hk_ctx *ctx, double prep_bytes, double part_bytes);
  * whatever precision hk_opacity is given; the adjoint refuses them. */
 hk_status hk_set_profile(hk_ctx *ctx, int profile, int remove_plinth);
 
+/* Sub-Lorentzian line wings (param.dat subLorentzianfile; Perrin & Hartmann
+ * 1989 chi factors, voigt.h:1-72, host.h:489-515): p = {sigma1, sigma2,
+ * sigma3, alpha1, beta1, epsilon1, alpha2, beta2, epsilon2, alpha3, beta3,
+ * epsilon3, x_lo, x_hi}; every term at a grid point lo < x < hi is multiplied
+ * by chi(|x - nu|) x / nu, chi = 1 below sigma1 and exp(-B1 (d - sigma1)
+ * ...) beyond, B_k = alpha_k + beta_k exp(-epsilon_k T).  NULL turns it off.
+ * Runs the FP64 form; the adjoint refuses it. */
+hk_status hk_set_sublorentzian(hk_ctx *ctx, const double *p);
+
 /* --------------------------------------- mean opacities, transmission */
 
 /* Planck and Rosseland mean ingredients of nstates opacities K (nstates x

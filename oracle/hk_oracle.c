@@ -462,8 +462,21 @@ void hko_opacity(int64_t n, const double *nu, const double *S,
                  const double *iad, const double *vy, const int64_t *win,
                  double numin, double dnu, int64_t ib, int64_t ie, double kmin,
                  double *K, int nthreads, int64_t pairs_out[3]) {
-  hko_opacity_p(n, nu, S, iad, vy, win, numin, dnu, ib, ie, kmin, 1, NULL, K, nthreads,
+  hko_opacity_p(n, nu, S, iad, vy, win, numin, dnu, ib, ie, kmin, 1, NULL, NULL, K, nthreads,
                 pairs_out);
+}
+
+/* sLChi (voigt.h:47-72) times x / nu inside (lo, hi), as Line6fAX/BX/CX
+ * apply it; sl = {sigma1, sigma2, sigma3, B1, B2, B3, lo, hi} */
+static double sublorentz(const double *sl, double x, double nu) {
+  if (!(x > sl[6] && x < sl[7])) return 1.0;
+  const double d = fabs(x - nu);
+  double chi;
+  if (d < sl[0]) chi = 1.0;
+  else if (d < sl[1]) chi = exp(-sl[3] * (d - sl[0]));
+  else if (d < sl[2]) chi = exp(-sl[3] * (sl[1] - sl[0]) - sl[4] * (d - sl[1]));
+  else chi = exp(-sl[3] * (sl[1] - sl[0]) - sl[4] * (sl[2] - sl[1]) - sl[5] * (d - sl[2]));
+  return chi * x / nu;
 }
 
 /* profiles 2-4 at x (Doppler units): Line6fA_kernel voigt.h:1235-1262 with
@@ -513,8 +526,8 @@ void hko_plinth(int64_t n, const double *S, const double *iad, const double *vy,
 void hko_opacity_p(int64_t n, const double *nu, const double *S,
                    const double *iad, const double *vy, const int64_t *win,
                    double numin, double dnu, int64_t ib, int64_t ie, double kmin,
-                   int profile, const double *plinth, double *K, int nthreads,
-                   int64_t pairs_out[3]) {
+                   int profile, const double *plinth, const double *sl, double *K,
+                   int nthreads, int64_t pairs_out[3]) {
   lkey *ord = (lkey *)malloc((size_t)(n > 0 ? n : 1) * sizeof(lkey));
   double *ey = (double *)malloc((size_t)(n > 0 ? n : 1) * sizeof(double));
   int64_t m = 0, wmax = 0;
@@ -588,6 +601,7 @@ void hko_opacity_p(int64_t n, const double *nu, const double *S,
           v = S1 / r2;
           ++pa;
         }
+        if (sl) v *= sublorentz(sl, hko_grid_x(numin, dnu, i), nul);
         acc[i - t0] += v;
         if (plinth) acc[i - t0] -= plinth[l];
       }

@@ -82,7 +82,8 @@ double hko_gh2(double x, double y);
 
 /* K[i - ib] = kmin + sum over lines (profile 1, Voigt), ib <= i < ie */
 /* profile 1..4 (define.h:69); plinth: per-line values subtracted inside
- * each line's window (removePlinth), or NULL */
+ * each line's window (removePlinth), or NULL; sl: sub-Lorentzian {sigma1,
+ * sigma2, sigma3, B1, B2, B3, x_lo, x_hi} (voigt.h:1-72), or NULL */
 void hko_windows_p(int64_t n, const double *nu, const double *S,
                    const double *iad, const double *vy, double numin, double dnu,
                    int64_t nx, int cutMode, double cut, int profile, int64_t *win);
@@ -91,8 +92,8 @@ void hko_plinth(int64_t n, const double *S, const double *iad, const double *vy,
 void hko_opacity_p(int64_t n, const double *nu, const double *S,
                    const double *iad, const double *vy, const int64_t *win,
                    double numin, double dnu, int64_t ib, int64_t ie, double kmin,
-                   int profile, const double *plinth, double *K, int nthreads,
-                   int64_t pairs_out[3]);
+                   int profile, const double *plinth, const double *sl, double *K,
+                   int nthreads, int64_t pairs_out[3]);
 void hko_opacity(int64_t n, const double *nu, const double *S,
                  const double *iad, const double *vy, const int64_t *win,
                  double numin, double dnu, int64_t ib, int64_t ie, double kmin,

@@ -70,7 +70,7 @@ def lib():
         L.hko_windows_p.argtypes = [_i64, _p, _p, _p, _p, _d, _d, _i64, _i, _d, _i, _p]
         L.hko_plinth.argtypes = [_i64, _p, _p, _p, _p, _i, _d, _i, _p]
         L.hko_opacity_p.argtypes = [_i64, _p, _p, _p, _p, _p, _d, _d, _i64, _i64, _d, _i, _p,
-                                    _p, _i, _p]
+                                    _p, _p, _i, _p]
         L.hko_means.argtypes = [_p, _p, _i64, _d, _p]
         L.hko_transmission.argtypes = [_p, _i, _i, _p, _d, _i, _d, _p]
         _lib = L
@@ -198,8 +198,16 @@ def gh2(x: float, y: float) -> float:
     return float(lib().hko_gh2(x, y))
 
 
+def sublorentz_params(p14, T):
+    """{sigma1..3, B1..B3, lo, hi} from the 14 file values (sigma1..3, alpha,
+    beta, epsilon of B1..B3, lo, hi) at temperature T (voigt.h:12-35)."""
+    p = [float(v) for v in p14]
+    B = [p[3 + 3 * k] + p[4 + 3 * k] * np.exp(-p[5 + 3 * k] * T) for k in range(3)]
+    return np.array(p[0:3] + B + p[12:14], np.float64)
+
+
 def opacity(nu, S, iad, vy, win, numin, dnu, nx, kmin=0.0, nthreads=0,
-            irange=None, profile=1, plinth=None):
+            irange=None, profile=1, plinth=None, sublorentz=None):
     """Line6fA/B/C + AddKStreams restated: K = kmin + sum of contributions.
 
     irange=(ib, ie) evaluates only grid indices ib <= i < ie of the nx-point
@@ -211,9 +219,10 @@ def opacity(nu, S, iad, vy, win, numin, dnu, nx, kmin=0.0, nthreads=0,
     K = np.empty(ie - ib, np.float64)
     pairs = np.zeros(3, np.int64)
     pl = None if plinth is None else _f64(plinth)
+    sl = None if sublorentz is None else _f64(sublorentz)
     lib().hko_opacity_p(len(nu), _ptr(nu), _ptr(S), _ptr(iad), _ptr(vy),
                         _ptr(win), numin, dnu, ib, ie, kmin, int(profile), _ptr(pl),
-                        _ptr(K), nthreads, _ptr(pairs))
+                        _ptr(sl), _ptr(K), nthreads, _ptr(pairs))
     return K, tuple(int(p) for p in pairs)
 
 

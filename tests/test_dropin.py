@@ -112,3 +112,54 @@ def test_dropin_means_and_transmission(tmp_path):
     err = np.max(np.abs(tr[big, 1] - Tr_ref.ravel()[big]) / Tr_ref.ravel()[big])
     print(f"drop-in means {mean[:2]}, transmission max rel err {err:.2e} (Tr > 1e-12)")
     np.testing.assert_allclose(tr[:, 1], Tr_ref.ravel(), rtol=1e-5, atol=1e-12)
+
+
+def test_dropin_mixture_profile_sublorentzian(tmp_path):
+    """SpeciesFile (two species), profile = 2 with removePlinth = 1 and a
+    subLorentzianfile in the reference's layouts (host.h:463-515): the
+    drop-in's K against the oracle chain, 1e-9 relative (FP64 form)."""
+    assert os.path.exists(ref_run.OUR_EXE), "build helios-k_b200/bin/heliosk first"
+    d = str(tmp_path / "run")
+    os.makedirs(d)
+    T, P = 900.0, 0.5
+    specs = {"spa": ("11", 18.0106, 41), "spb": ("26", 28.0101, 42)}
+    ab = {"spa": 2e-3, "spb": 5e-4}
+    lines = {}
+    for name, (cid, m, seed) in specs.items():
+        L = synth.hitran_lines(4000, seed=seed, nu_min=NUMIN - 40.0, nu_max=NUMAX + 40.0)
+        synth.write_species(d, name, database=0, nfiles=1, nl=[4000],
+                            limits=(int(NUMIN - 50), int(NUMAX + 50)), isos=[(cid, 1.0, m)])
+        synth.write_hitran_bin(os.path.join(d, name + ".bin"), L, cids=np.array([(" " + cid).encode()] * 4000))
+        lines[name] = L
+    with open(os.path.join(d, "species.dat"), "w") as f:
+        for name in specs:
+            f.write(f"{name} {ab[name]}\n")
+    sl14 = [3.0, 10.0, 20.0, 0.09, -0.05, 0.004, 0.05, 0.02, 0.003, 0.02, 0.0, 0.0, 1050.0, 1250.0]
+    with open(os.path.join(d, "sl.dat"), "w") as f:
+        f.write(f"sigma1 {sl14[0]}\nsigma2 {sl14[1]}\nsigma3 {sl14[2]}\nB alpha beta epsilon\n")
+        for k in range(3):
+            f.write(f"B{k + 1} {sl14[3 + 3 * k]} {sl14[4 + 3 * k]} {sl14[5 + 3 * k]}\n")
+        f.write(f"range lo hi\n{sl14[12]} {sl14[13]}\n")
+    ref_run.write_run(d, d, T, P, NUMIN, NUMAX, DNU, CUT, NBINS, NC, store_k=1, resample=0,
+                      SpeciesFile=os.path.join(d, "species.dat"), profile=2, removePlinth=1,
+                      subLorentzianfile=os.path.join(d, "sl.dat"))
+    r = ref_run.run(ref_run.OUR_EXE, d, timeout=300)
+    assert r["rc"] == 0, r["tail"]
+    K = np.loadtxt(os.path.join(d, "Out_syn.dat"))[:, 1]
+    Tq, Qq = synth.q_table()
+    Q = oracle.partition(Tq, Qq, T)
+    mean_mass = sum(ab[n] * specs[n][1] for n in specs)
+    cols = [oracle.prep_hitran(lines[n], [specs[n][1]], [1.0], [Q], T, P, qalphaL=1.0, units=0,
+                               meanMass=mean_mass, Sscale=ab[n]) for n in specs]
+    nu, S, iad, vy = (np.concatenate([c[k] for c in cols]) for k in range(4))
+    nx = oracle.grid_nx(NUMIN, NUMAX, DNU)
+    win = oracle.windows(nu, S, iad, vy, NUMIN, DNU, nx, 0, CUT, profile=2)
+    pl = oracle.plinth(S, iad, vy, win, 0, CUT, 2)
+    Kref, _ = oracle.opacity(nu, S, iad, vy, win, NUMIN, DNU, nx, profile=2, plinth=pl,
+                             sublorentz=oracle.sublorentz_params(sl14, T))
+    # the drop-in writes K * unitScale (units 0: 1) as %.20g
+    Rb, Kb = Kref.reshape(NBINS, -1), K.reshape(NBINS, -1)
+    m = Rb > 1e-6 * Rb.max(axis=1, keepdims=True)
+    err = np.max(np.abs(Kb - Rb)[m] / Rb[m])
+    print(f"drop-in mixture + Lorentz + plinth + sub-Lorentzian: max rel err {err:.2e}")
+    assert err < 1e-9

@@ -89,3 +89,32 @@ def test_plinth_is_the_cut_edge_value(profile, cutMode, cut):
         dc = xc * ALPHA
         assert pl[0] == pytest.approx(STRUE * GAMMA / (math.pi * (dc * dc + GAMMA * GAMMA)), rel=1e-2)
     assert oracle.plinth(np.array([1.0]), np.array([1.0]), np.array([1.0]), w[None, :], 0, 5.0, 4)[0] == 0.0
+
+
+SL14 = [3.0, 10.0, 20.0, 0.09, -0.05, 0.004, 0.05, 0.02, 0.003, 0.02, 0.0, 0.0, 95.0, 130.0]
+
+
+@pytest.mark.parametrize("profile", [1, 2])
+def test_sublorentz_factor(profile):
+    """chi(|x - nu|) x / nu inside (x_lo, x_hi), 1 outside; chi = 1 within
+    sigma1 of the centre, continuous at the breakpoints (voigt.h:47-72)."""
+    T = 700.0
+    nu = np.array([NU0])
+    iad = np.array([1.0 / ALPHA])
+    vy = np.array([GAMMA / ALPHA])
+    S = np.array([STRUE / ALPHA])
+    win = oracle.windows(nu, S, iad, vy, NUMIN, DNU, NX, 0, CUT, profile=profile)
+    K, _ = oracle.opacity(nu, S, iad, vy, win, NUMIN, DNU, NX, profile=profile)
+    sl = oracle.sublorentz_params(SL14, T)
+    Ks, _ = oracle.opacity(nu, S, iad, vy, win, NUMIN, DNU, NX, profile=profile, sublorentz=sl)
+    x = NUMIN + DNU * np.arange(NX)
+    d = np.abs(x - NU0)
+    B = sl[3:6]
+    chi = np.where(d < 3.0, 1.0, np.where(d < 10.0, np.exp(-B[0] * (d - 3.0)), np.where(
+        d < 20.0, np.exp(-B[0] * 7.0 - B[1] * (d - 10.0)),
+        np.exp(-B[0] * 7.0 - B[1] * 10.0 - B[2] * (d - 20.0)))))
+    f = np.where((x > 95.0) & (x < 130.0), chi * x / NU0, 1.0)
+    m = K > 0
+    np.testing.assert_allclose(Ks[m], K[m] * f[m], rtol=1e-13)
+    assert np.array_equal(Ks[~m], K[~m])
+    assert sl[3] == pytest.approx(0.09 - 0.05 * math.exp(-0.004 * T), rel=1e-15)

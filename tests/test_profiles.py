@@ -76,3 +76,34 @@ def test_profile_arguments(small):
         with pytest.raises(hkb.HkError) as e:
             ctx.set_profile(*bad)
         assert e.value.status == -1
+
+
+SL14 = [3.0, 10.0, 20.0, 0.09, -0.05, 0.004, 0.05, 0.02, 0.003, 0.02, 0.0, 0.0, 1100.0, 2900.0]
+
+
+@pytest.mark.parametrize("profile,plinth", [(1, 0), (2, 0), (1, 1)])
+def test_sublorentzian_matches_oracle(small, profile, plinth):
+    ctx = small["ctx"]
+    ctx.set_profile(profile, plinth)
+    ctx.set_sublorentzian(SL14)
+    try:
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+        for T, P in ((1500.0, 0.1), (500.0, 10.0)):
+            Q = oracle.partition(small["Tq"], small["Qq"], T)
+            nu, S, iad, vy = oracle.prep_hitran(small["L"], [synth.MASS], [1.0], [Q], T, P, qalphaL=1.0)
+            nx = oracle.grid_nx(NUMIN, NUMAX, DNU)
+            win = oracle.windows(nu, S, iad, vy, NUMIN, DNU, nx, 0, 25.0, profile=profile)
+            pl = oracle.plinth(S, iad, vy, win, 0, 25.0, profile) if plinth else None
+            Kref, _ = oracle.opacity(nu, S, iad, vy, win, NUMIN, DNU, nx, profile=profile, plinth=pl,
+                                     sublorentz=oracle.sublorentz_params(SL14, T))
+            for prec in (hkb.MIXED, hkb.PLAIN_FP64):
+                K = ctx.opacity([T], [P], prec)[0]
+                err, _ = masked_relerr(K, Kref, NBINS)
+                print(f"sub-Lorentzian profile {profile} plinth {plinth} T={T} err {err:.2e}")
+                assert err < (1e-9 if plinth else 1e-12)
+    finally:
+        ctx.set_sublorentzian(None)
+        ctx.set_profile(1, 0)
+    with pytest.raises(hkb.HkError) as e:
+        ctx.set_profile(4, 1)  # heliosk.cu:410-413
+    assert e.value.status == -8
