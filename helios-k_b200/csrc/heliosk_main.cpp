@@ -59,7 +59,8 @@ int main(int argc, char **argv) {
   Params p;
   std::string msg;
   if (read_param_file("param.dat", argc, argv, p, msg) != 0) return die(msg);
-  if (p.ciaSystem != "-") return die("Error: ciaSystem is outside this build's opacity path");
+  const bool useCia = p.ciaSystem != "-";
+  if (useCia && p.SpeciesFilename != "-") return die("Error, not allowed to use a cia system with a molecule");
   // SpeciesFile: "<species> <abundance>" pairs (host.h:463-487, 579-590)
   std::vector<std::string> mixNames;
   std::vector<double> mixAb;
@@ -122,13 +123,17 @@ int main(int argc, char **argv) {
     if (!mixNames.empty())
       fprintf(f, "Species in file: %s\nNumber of Species: %d\n", p.SpeciesFilename.c_str(), (int)mixNames.size());
     if (p.subLorentzian != "-") fprintf(f, "sub-Lorentzian file: %s\n", p.subLorentzian.c_str());
+    if (useCia) fprintf(f, "cia System = %s\n", p.ciaSystem.c_str());
     fprintf(f, "Species Name = %s\nengine = %s\n\n", p.speciesName.c_str(), hk_version());
   }
 
   chk(hk_set_options(c, p.qalphaL, p.gammaF, p.units, 1.0));
-  // mean molar mass over the species (of the mixture), heliosk.cu:665-686
+  // mean molar mass over the species (of the mixture), heliosk.cu:665-686;
+  // a CIA system's collider mass (heliosk.cu:700-702)
   double meanMass = 0.0;
-  {
+  if (useCia) {
+    chk(hk_load_cia(c, p.path.c_str(), p.ciaSystem.c_str(), &meanMass));
+  } else {
     const std::vector<std::string> names = mixNames.empty() ? std::vector<std::string>{p.speciesName} : mixNames;
     for (size_t k = 0; k < names.size(); ++k) {
       SpeciesInfo sp;
@@ -146,7 +151,7 @@ int main(int argc, char **argv) {
 
   const bool compute = p.doStoreFullK >= 0;
   cudaEventRecord(t0);
-  if (compute && mixNames.empty())
+  if (compute && mixNames.empty() && !useCia)
     chk(hk_load_species_file(c, p.path.c_str(), p.speciesName.c_str(), p.numin, p.numax, p.cutMode, p.cut));
   if (compute && !mixNames.empty()) {
     std::vector<const char *> names;

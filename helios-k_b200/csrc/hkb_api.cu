@@ -86,6 +86,11 @@ struct hk_ctx {
   std::vector<double> tune_ms;  // probe time per shape at the last tuning
   DevBuf tunework;              // probe states and their max-term words
   DevBuf meanwork;              // means / transmission inputs, partial sums and outputs
+  // collision-induced absorption in place of lines (hk_load_cia)
+  bool cia = false;
+  std::vector<CiaSet> cia_sets;
+  double cia_mass1 = 1.0;
+  DevBuf cia_nu, cia_val, cia_tab;
   // T-P table recorded as one CUDA graph (hk_table_build / hk_table_run)
   cudaGraph_t table_graph = nullptr;
   cudaGraphExec_t table_exec = nullptr;
@@ -159,7 +164,7 @@ void hk_destroy(hk_ctx *c) {
                     &c->Aterm, &c->iso, &c->order, &c->states, &c->ticket,
                     &c->prep, &c->wbits, &c->Kwork, &c->outwork, &c->scratch,
                     &c->qrV, &c->qrC, &c->qrD, &c->vpart, &c->vcnt, &c->sscale, &c->gscale, &c->adjwork,
-                    &c->tunework, &c->meanwork})
+                    &c->tunework, &c->meanwork, &c->cia_nu, &c->cia_val, &c->cia_tab})
     b->release();
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -188,6 +193,7 @@ hk_status hk_set_species(hk_ctx *c, int database, int niso, const double *mass,
   c->qT.assign(niso, {});
   c->qQ.assign(niso, {});
   c->iso_ss.clear();
+  c->cia = false;
   ok(c);
   return HK_OK;
 }
@@ -468,7 +474,7 @@ static hk_status build_states(hk_ctx *c, int nstates, const double *T, const dou
 
 static hk_status check_ready(hk_ctx *c) {
   if (!c->grid_set) return fail(c, HK_ERR_STATE, "hk_set_grid must come first");
-  if (c->iso_mass.empty()) return fail(c, HK_ERR_STATE, "hk_set_species must come first");
+  if (c->iso_mass.empty() && !c->cia) return fail(c, HK_ERR_STATE, "hk_set_species must come first");
   return HK_OK;
 }
 
@@ -635,6 +641,65 @@ static hk_status tune_shape(hk_ctx *c, int nstates, const std::vector<StateDev> 
   return HK_OK;
 }
 
+// ------------------------------------------------------------------ CIA
+// hk_opacity of a CIA context: per state the sets the reference reads for
+// its T (up to the first with T <= T_set; above all of them K = kmin), each
+// with the last grid index its scan reaches.
+static hk_status opacity_cia(hk_ctx *c, int nstates, const double *T, const double *P, double *K_out,
+                             int K_on_device, cudaStream_t s) {
+  const int64_t nx = c->g.nx;
+  double *Kd = K_out;
+  if (!K_on_device) {
+    CUDA_TRY(c, c->Kwork.ensure((size_t)nstates * nx * sizeof(double)));
+    Kd = c->Kwork.as<double>();
+  }
+  const int ns = (int)c->cia_sets.size();
+  std::vector<CiaSetDev> tab((size_t)nstates * ns);
+  std::vector<int> used(nstates), beyond(nstates);
+  for (int q = 0; q < nstates; ++q) {
+    if (!(T[q] > 0.0) || !(P[q] >= 0.0)) return fail(c, HK_ERR_ARG, "state %d: need T > 0 and P >= 0", q);
+    int k = 0;
+    int64_t off = 0;
+    for (; k < ns; ++k) {
+      const CiaSet &cs = c->cia_sets[k];
+      const int n = (int)cs.nu.size();
+      int64_t istop = nx - 1;
+      if (n == 2) {
+        istop = 0;
+      } else {
+        // first grid point at or past nu[n-2] (x_i = numin + i dnu, one FMA)
+        int64_t lo = 0, hi = nx;
+        while (lo < hi) {
+          const int64_t m = lo + (hi - lo) / 2;
+          if (std::fma((double)m, c->g.dnu, c->g.numin) >= cs.nu[n - 2]) hi = m;
+          else lo = m + 1;
+        }
+        if (lo < nx) istop = lo;
+      }
+      tab[(size_t)q * ns + k] = CiaSetDev{cs.T, off, n, 0, istop};
+      off += n;
+      if (T[q] <= cs.T) break;
+    }
+    used[q] = std::min(k + 1, ns);
+    beyond[q] = (k == ns);  // T above every set: host.h:773-775
+  }
+  CUDA_TRY(c, c->cia_tab.ensure(std::max<size_t>(tab.size(), 1) * sizeof(CiaSetDev)));
+  CUDA_TRY(c, cudaMemcpyAsync(c->cia_tab.p, tab.data(), tab.size() * sizeof(CiaSetDev), cudaMemcpyHostToDevice, s));
+  for (int q = 0; q < nstates; ++q)
+    CUDA_TRY(c, launch_cia(c->g, c->cia_tab.as<CiaSetDev>() + (size_t)q * ns, used[q], c->cia_nu.as<double>(),
+                           c->cia_val.as<double>(), T[q], P[q], c->cia_mass1, c->kmin, beyond[q],
+                           Kd + (size_t)q * nx, s));
+  c->launches = nstates;
+  c->have_voigt_t = false;
+  c->voigt_ms_acc = 0.0;
+  if (!K_on_device) {
+    CUDA_TRY(c, cudaMemcpyAsync(K_out, Kd, (size_t)nstates * nx * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(s));  // the set table is pageable host memory
+  ok(c);
+  return HK_OK;
+}
+
 hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, int precision,
                      double *K_out, int K_on_device, void *stream) {
   if (!c) return HK_ERR_ARG;
@@ -646,6 +711,7 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   if (nstates > 65535) return fail(c, HK_ERR_RANGE, "at most 65535 states per call");
   cudaSetDevice(c->device);
   cudaStream_t s = (cudaStream_t)stream;
+  if (c->cia) return opacity_cia(c, nstates, T, P, K_out, K_on_device, s);
   std::vector<StateDev> hs;
   if ((st = build_states(c, nstates, T, P, hs)) != HK_OK) return st;
   CUDA_TRY(c, c->states.ensure(nstates * sizeof(StateDev)));
@@ -1389,6 +1455,40 @@ static hk_status stream_line_files(hk_ctx *c, const SpeciesInfo &sp, int fi0, in
   hk_status st = stream_species(c, sp, fi0, fi1, species_spec(c, sp, 0), ib, 0);
   if (st != HK_OK) return st;
   return load_device(c, n, ib, (int)sp.iso.size());
+}
+
+hk_status hk_load_cia(hk_ctx *c, const char *path, const char *system, double *mass1) {
+  if (!c || !system) return HK_ERR_ARG;
+  std::string file;
+  int nsets = 0;
+  double m1 = 1.0;
+  if (!cia_system(system, file, &nsets, &m1))
+    return fail(c, HK_ERR_ARG, "unknown cia system %s", system);
+  std::vector<CiaSet> sets;
+  std::string msg;
+  const int rc = read_cia_file(std::string(path ? path : "") + file, nsets, sets, msg);
+  if (rc != 0) return fail(c, rc, "%s", msg.c_str());
+  std::vector<double> nu, val;
+  for (const CiaSet &cs : sets) {
+    nu.insert(nu.end(), cs.nu.begin(), cs.nu.end());
+    val.insert(val.end(), cs.cia.begin(), cs.cia.end());
+  }
+  cudaSetDevice(c->device);
+  CUDA_TRY(c, c->cia_nu.ensure(nu.size() * sizeof(double)));
+  CUDA_TRY(c, c->cia_val.ensure(val.size() * sizeof(double)));
+  CUDA_TRY(c, cudaMemcpy(c->cia_nu.p, nu.data(), nu.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(c->cia_val.p, val.data(), val.size() * sizeof(double), cudaMemcpyHostToDevice));
+  // a CIA system has no lines (heliosk.cu:842-845)
+  c->nlines = 0;
+  c->L = LinesDev{};
+  c->iso_mass.clear();
+  c->cia_sets = std::move(sets);
+  c->cia_mass1 = m1;
+  c->cia = true;
+  table_release(c);
+  if (mass1) *mass1 = m1;
+  ok(c);
+  return HK_OK;
 }
 
 hk_status hk_load_species_file(hk_ctx *c, const char *path, const char *species, double numin,

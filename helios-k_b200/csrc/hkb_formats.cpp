@@ -216,6 +216,77 @@ void line_file_range(const SpeciesInfo &sp, double numin, double numax, int cutM
   *fi1_out = fi1;
 }
 
+bool cia_system(const std::string &system, std::string &file, int *nsets, double *mass1) {
+  struct Sys { const char *name; int nsets; double mass1; };
+  // the systems the reference knows, with their set counts and the mass
+  // (g/mol) its cm^2/g conversion divides by (ISO.h:226-276)
+  static const Sys table[] = {
+      {"H2-H2", 113, 2.0 * 1.00794},     {"H2-H2_eq", 10, 2.0 * 1.00794},
+      {"H2-H2_norm", 10, 2.0 * 1.00794}, {"H2-He", 339, 4.002602},
+      {"H2-He_eq", 10, 4.002602},        {"H2-He_norm", 10, 4.002602},
+      {"H2-CH4_eq", 10, 16.04246},       {"H2-CH4_norm", 10, 16.04246},
+      {"H2-H", 4, 1.00794}};
+  for (const Sys &t : table)
+    if (system == t.name) {
+      file = system + "_2011.cia";
+      *nsets = t.nsets;
+      *mass1 = t.mass1;
+      return true;
+    }
+  return false;
+}
+
+int read_cia_file(const std::string &fname, int nsets, std::vector<CiaSet> &sets, std::string &msg) {
+  FILE *f = fopen(fname.c_str(), "r");
+  if (!f) {
+    msg = "Error: cia file is not available: " + fname;
+    return HK_ERR_IO;
+  }
+  sets.clear();
+  char skip[160], c2[12], c3[9], c4[9];
+  for (int it = 0; it < nsets; ++it) {
+    CiaSet cs;
+    bool good = fgets(skip, 21, f) && fgets(skip, 11, f) && fgets(c2, 11, f) && fgets(c3, 8, f) &&
+                fgets(c4, 8, f) && fgets(skip, 11, f) && fgets(skip, 37, f);
+    const int n = good ? atoi(c3) : 0;
+    if (!good || n < 2) {
+      fclose(f);
+      msg = "Error: cia file " + fname + ": set " + std::to_string(it) + " is missing or malformed";
+      return HK_ERR_FORMAT;
+    }
+    cs.T = strtod(c4, nullptr);
+    cs.numax = strtod(c2, nullptr);
+    cs.nu.resize(n);
+    cs.cia.resize(n);
+    for (int k = 0; k < n; ++k)
+      if (fscanf(f, "%lf %lf", &cs.nu[k], &cs.cia[k]) != 2) {
+        fclose(f);
+        msg = "Error: cia file " + fname + ": set " + std::to_string(it) + " is truncated";
+        return HK_ERR_FORMAT;
+      }
+    if (cs.nu[n - 1] != cs.numax) {
+      // host.h:749 ends a set's scan where nu reaches the header's numax
+      fclose(f);
+      msg = "Error: cia file " + fname + ": set " + std::to_string(it) + " does not end at its numax";
+      return HK_ERR_FORMAT;
+    }
+    for (int k = 1; k < n; ++k)
+      if (!(cs.nu[k] > cs.nu[k - 1])) {
+        fclose(f);
+        msg = "Error: cia file " + fname + ": set " + std::to_string(it) + " is not increasing in nu";
+        return HK_ERR_FORMAT;
+      }
+    if (!fgets(skip, 3, f) && it + 1 < nsets) {
+      fclose(f);
+      msg = "Error: cia file " + fname + " ends after set " + std::to_string(it);
+      return HK_ERR_FORMAT;
+    }
+    sets.push_back(std::move(cs));
+  }
+  fclose(f);
+  return 0;
+}
+
 // host.h:489-515: the sub-Lorentzian file, "name value" for sigma1..3, a
 // 4-word header, "name alpha beta epsilon" for B1..B3, a 3-word header and
 // the range "lo hi" -> p[14] = {sigma1..3, alpha1, beta1, eps1, ..., lo, hi}

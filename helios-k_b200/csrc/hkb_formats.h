@@ -60,6 +60,16 @@ int read_species_param(const std::string &path, const std::string &species,
                        SpeciesInfo &sp, std::string &msg);
 void line_file_range(const SpeciesInfo &sp, double numin, double numax, int cutMode, double cut,
                      int *fi0, int *fi1);
+// One temperature set of a HITRAN-format CIA file (Richard et al. 2012).
+struct CiaSet {
+  double T = 0.0, numax = 0.0;
+  std::vector<double> nu, cia;
+};
+// The first nsets sets of a CIA file, read as host.h:698-762 reads them
+// (fixed-width header fields, then N "nu cia" pairs).
+int read_cia_file(const std::string &fname, int nsets, std::vector<CiaSet> &sets, std::string &msg);
+// ISO.h:222-277: file name, number of sets and collider mass of a system
+bool cia_system(const std::string &system, std::string &file, int *nsets, double *mass1);
 int read_sublorentz_file(const std::string &fname, double p[14], std::string &msg);
 int read_param_file(const std::string &fname, int argc, char **argv, Params &p,
                     std::string &msg);

@@ -86,6 +86,18 @@ cudaError_t column_minmax(int64_t n, const double *v_d, double *scratch_d, doubl
 cudaError_t launch_gather_u8(int64_t n, const int64_t *order_d, const uint8_t *src_d, uint8_t *dst_d,
                              cudaStream_t stream);
 
+// Collision-induced absorption (hkb_cia.cu): one table set on the device
+struct CiaSetDev {
+  double T;
+  int64_t off;    // first row in the packed nu / cia arrays
+  int n;          // rows
+  int pad;
+  int64_t istop;  // last grid index the set's scan reaches
+};
+cudaError_t launch_cia(const GridDev &g, const CiaSetDev *sets_d, int nsets, const double *nu_d,
+                       const double *cia_d, double T, double P, double mass1, double kmin, int beyond,
+                       double *K_d, cudaStream_t stream);
+
 // Mean opacities and transmission function (hkb_means.cu)
 size_t means_scratch_doubles(int nstates, int64_t nx);
 cudaError_t launch_means(const double *K_d, int64_t k_stride, const GridDev &g, const double *T_d,

@@ -91,6 +91,7 @@ def lib():
             "hk_set_profile": (_i, [_p, _i, _i]),
             "hk_set_sublorentzian": (_i, [_p, _p]),
             "hk_load_mixture": (_i, [_p, C.c_char_p, _i, _p, _p, _d, _d, _i, _d]),
+            "hk_load_cia": (_i, [_p, C.c_char_p, C.c_char_p, _p]),
             "hk_transmission": (_i, [_p, _i, _p, _p, _i, _i, _d, _p, _i, _p]),
         }
         for name, (res, args) in sig.items():
@@ -194,6 +195,13 @@ class Context:
         self._chk(lib().hk_load_mixture(self._h, path.encode(), len(species),
                                         C.cast(names, C.c_void_p), _ptr(ab), numin, numax,
                                         cutMode, cut))
+
+    def load_cia(self, path, system):
+        """A HITRAN CIA table (<path><system>_2011.cia) in place of lines;
+        returns the collider mass of the units = 1 scaling."""
+        m = C.c_double(0.0)
+        self._chk(lib().hk_load_cia(self._h, path.encode(), system.encode(), C.byref(m)))
+        return m.value
 
     @property
     def num_lines(self):

@@ -195,3 +195,24 @@ def write_param(path, **kv):
         for k in optional:
             if k in kv:
                 f.write(f"{k} = {kv[k]}\n")
+
+
+# ------------------------------------------------------------ CIA files
+
+def write_cia(path, sets, formula="H2-H2"):
+    """A HITRAN-format CIA file (Richard et al. 2012): per temperature set a
+    100-character header -- formula (20), numin (10), numax (10), number of
+    points (7), T (7), max cross section (10), resolution (6), comment (27),
+    reference (3) -- then "nu cia" rows.  sets: [(T, nu array, cia array)]."""
+    with open(path, "w") as f:
+        for T, nu, cia in sets:
+            nu = np.asarray(nu, np.float64)
+            cia = np.asarray(cia, np.float64)
+            # readers stop a set where the last nu equals the header's numax
+            # (host.h:749): both must print to the same value
+            if float(f"{nu[-1]:10.3f}") != float(f"{nu[-1]:10.4f}"):
+                raise ValueError("the last nu of a set must have at most 3 decimals")
+            f.write(f"{formula:>20s}{nu[0]:10.3f}{nu[-1]:10.3f}{len(nu):7d}{T:7.1f}"
+                    f"{cia.max():10.3e}{0.0:6.3f}{'synthetic':>27s}{1:3d}\n")
+            for a, b in zip(nu, cia):
+                f.write(f"{a:10.4f} {b:10.3e}\n")

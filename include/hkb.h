@@ -118,6 +118,16 @@ hk_status hk_load_mixture(hk_ctx *ctx, const char *path, int nspecies, const cha
                           const double *abundance, double numin, double numax, int cutMode,
                           double cut);
 
+/* Collision-induced absorption in place of lines (param.dat ciaSystem;
+ * InitCia ISO.h:222-277, readCiaFile host.h:670-785): reads
+ * <path><system>_2011.cia (HITRAN CIA format) for the systems H2-H2,
+ * H2-H2_eq, H2-H2_norm, H2-He, H2-He_eq, H2-He_norm, H2-CH4_eq, H2-CH4_norm,
+ * H2-H; hk_opacity then interpolates it onto the grid for each state (the
+ * reference's T and P rules, K in cm^2/g plus kmin).  mass1 (optional) gets
+ * the collider mass the reference's units = 1 scaling uses.  Loading lines
+ * or species ends CIA mode. */
+hk_status hk_load_cia(hk_ctx *ctx, const char *path, const char *system, double *mass1);
+
 int64_t hk_num_lines(const hk_ctx *ctx);
 
 /* --------------------------------------------------------------- grid */

@@ -374,3 +374,90 @@ def vjp_hitran(lines, mass, Tq, Qq, T, P, u, numin, dnu, nx, cut=25.0, qalphaL=1
     dT = float(np.sum(np.where(ok, gS * dlS_dT + gy * dy_dT + gI * diad_dT, 0.0)))
     dP = float(np.sum(np.where(ok, gS * dlS_dnu * delta + gy * dy_dP + gI * diad_dP + gN * delta, 0.0)))
     return dT, dP, gS, gy * iad
+
+
+# ------------------------------------------------------------------ CIA
+AMAGAT = 2.6867774e19  # define.h:43
+NA = 6.0221412927e23
+
+
+def cia_opacity(path, nsets, mass1, x, T, P, kmin=0.0):
+    """readCiaFile (host.h:670-785) restated as it reads the file: per set a
+    fixed-width header (20, 10, 10, 7, 7, 10 characters, then 36 skipped),
+    linear interpolation in nu inside [nu0, nu1), the last set with
+    T_set <= T taken as is and the first set above T interpolated linearly
+    in T from the value left by the sets before; stop after that set; K =
+    cia * rho (P 273.15 / T amagat) * NA / mass1 + kmin, or kmin everywhere
+    when T is above the last set read.  x: the grid (FP64 array)."""
+    x = np.asarray(x, np.float64)
+    K = np.zeros(len(x))
+    with open(path, "r") as f:
+        data = f.read()
+    pos = 0
+
+    def fgets(n):  # C fgets(buf, n): up to n-1 characters, stops after a newline
+        nonlocal pos
+        end = data.find("\n", pos, pos + n - 1)
+        end = pos + n - 1 if end < 0 else end + 1
+        out = data[pos:end]
+        pos = end
+        return out
+
+    def scan_double():
+        nonlocal pos
+        while pos < len(data) and data[pos].isspace():
+            pos += 1
+        start = pos
+        while pos < len(data) and not data[pos].isspace():
+            pos += 1
+        return float(data[start:pos])
+
+    Tcia1 = 0.0
+    for _ in range(nsets):
+        Tcia0 = Tcia1
+        fgets(21)
+        fgets(11)
+        c2 = fgets(11)
+        c3 = fgets(8)
+        c4 = fgets(8)
+        fgets(11)
+        fgets(37)
+        ncia = int(c3)
+        Tcia1 = float(c4)
+        numax = float(c2)
+        nu0 = scan_double()
+        cia0 = scan_double()
+        nu1 = scan_double()
+        cia1 = scan_double()
+        nc = 2
+        for i in range(len(x)):
+            while x[i] >= nu1:
+                nu0, cia0 = nu1, cia1
+                nu1 = scan_double()
+                cia1 = scan_double()
+                nc += 1
+                if nc == ncia:
+                    break
+            if nu0 <= x[i] < nu1:
+                if Tcia1 <= T:
+                    K[i] = cia0 + (cia1 - cia0) * (x[i] - nu0) / (nu1 - nu0)
+                if T < Tcia1 and Tcia0 > 0.0:
+                    K0 = K[i]
+                    K1 = cia0 + (cia1 - cia0) * (x[i] - nu0) / (nu1 - nu0)
+                    K[i] = K0 + (K1 - K0) * (T - Tcia0) / (Tcia1 - Tcia0)
+            if nu1 == numax:
+                break
+            if i == len(x) - 1:
+                while nc < ncia:
+                    nu1 = scan_double()
+                    cia1 = scan_double()
+                    nc += 1
+        fgets(3)
+        if T <= Tcia1:
+            break
+    rho1 = P * 273.15 / T * AMAGAT
+    if Tcia1 < T:
+        return np.full(len(x), kmin)
+    K = K * rho1
+    K = K * (NA / mass1)  # host.h:779: K *= def_NA / cia.mass1
+    return K + kmin
