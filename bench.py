@@ -580,6 +580,7 @@ def main():
                    "execution": "one CUDA graph per step" if graph else "hk_opacity sections + hk_kdist",
                    "tile_shape": {"lines_per_chunk": hkb.tile_shape(shape_used)[0],
                                   "points_per_tile": hkb.tile_shape(shape_used)[1],
+                                  "warps": hkb.tile_shape(shape_used, warps=True)[2],
                                   "shape": shape_used, "tuned": shape_tuned >= 0,
                                   "probe_ms": [round(float(v), 3) for v in probe_ms]
                                   if shape_tuned >= 0 else None},

@@ -189,7 +189,7 @@ int main(int argc, char **argv) {
     t_lines = t_call - t_K;
     int shape = 0, tuned = -1, ch = 0, gp = 0;
     hk_tuning_result(c, &shape, &tuned, nullptr);
-    hk_tile_shape_info(shape, &ch, &gp);
+    hk_tile_shape_info(shape, &ch, &gp, nullptr);
     fprintf(info, "Tile shape: %d lines x %d points (%s)\n", ch, gp, tuned >= 0 ? "tuned" : "fixed");
   } else {
     // doStoreFullK = -1 / -2: read K back (heliosk.cu:1860-1935)

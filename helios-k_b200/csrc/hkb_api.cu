@@ -970,10 +970,11 @@ hk_status hk_set_sublorentzian(hk_ctx *c, const double *p) {
 
 int hk_num_tile_shapes(void) { return voigt_num_shapes(); }
 
-hk_status hk_tile_shape_info(int shape, int *lines_per_chunk, int *points_per_tile) {
+hk_status hk_tile_shape_info(int shape, int *lines_per_chunk, int *points_per_tile, int *warps) {
   if (shape < 0 || shape >= voigt_num_shapes()) return HK_ERR_ARG;
   if (lines_per_chunk) *lines_per_chunk = voigt_chunk_lines(shape);
   if (points_per_tile) *points_per_tile = voigt_tile_points(shape);
+  if (warps) *warps = voigt_tile_warps(shape);
   return HK_OK;
 }
 

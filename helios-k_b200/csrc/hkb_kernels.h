@@ -15,10 +15,12 @@ namespace hkb {
 constexpr int KD_SMEM_LIMIT = 224 * 1024;
 
 // Tile shapes of the mixed Voigt kernel: lines per staged chunk x grid points
-// per tile; shape 0 is the default and the plain FP64 form's only shape.
+// per tile (warps per CTA); shape 0 is the default and the plain FP64 form's
+// only shape.
 int voigt_num_shapes();
 int voigt_tile_points(int shape);
 int voigt_chunk_lines(int shape);
+int voigt_tile_warps(int shape);
 cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream);
 
 // Vector-Jacobian product of one state's opacity (hkb_adjoint.cu): G_d holds

@@ -31,20 +31,22 @@
 
 namespace hkb {
 
-constexpr int HK_WARPS = 8;
-constexpr int HK_THREADS = HK_WARPS * 32;
-
-// Tile shapes: CH lines per staged chunk x G = 8 warps * 32 lanes * PPL grid
-// points per tile.  The autotuner (hk_set_tuning) picks one per workload;
-// shape 0 is the default.  MINB is the CTAs per SM the register budget is
-// set for (64 registers at 4; 80 at 3, where shared memory allows 3 only).
-template <int CH_, int PPL_, int MINB_>
+// Tile shapes: CH lines per staged chunk x G = WARPS warps * 32 lanes * PPL
+// grid points per tile.  The autotuner (hk_set_tuning) picks one per
+// workload; shape 0 is the default.  MINB is the CTAs per SM the register
+// budget is set for (8 warps: 64 registers at 4, 80 at 3, where shared
+// memory allows 3 only; 4 warps of 16 points per lane: 102 registers at 5,
+// 64 at 8).  Four warps of 16 points keep the 2048-point tile and spread a
+// staged line's per-warp costs (coefficient loads, class ballots) over twice
+// the points.
+template <int CH_, int PPL_, int MINB_, int WARPS_ = 8>
 struct TileShape {
-  static constexpr int CH = CH_, PPL = PPL_, MINB = MINB_;
+  static constexpr int CH = CH_, PPL = PPL_, MINB = MINB_, WARPS = WARPS_;
+  static constexpr int THREADS = 32 * WARPS_;
   static constexpr int SLICE = 32 * PPL_;        // points per warp
-  static constexpr int G = HK_WARPS * SLICE;     // points per tile
+  static constexpr int G = WARPS_ * SLICE;       // points per tile
   static_assert(G <= 2048, "k * vb_hi must stay exact in FP32 (11 bits)");
-  static_assert(CH % 32 == 0 && CH <= HK_THREADS, "one staging thread per line");
+  static_assert(CH % 32 == 0 && CH <= THREADS, "one staging thread per line");
   static_assert(PPL % 2 == 0, "points are processed in pairs");
 };
 using Shape0 = TileShape<128, 8, 4>;  // default
@@ -52,9 +54,15 @@ using Shape1 = TileShape<256, 8, 3>;
 using Shape2 = TileShape<64, 8, 4>;
 using Shape3 = TileShape<128, 4, 4>;
 using Shape4 = TileShape<256, 4, 4>;
-constexpr int HK_NSHAPES = 5;
-constexpr int HK_SHAPE_CH[HK_NSHAPES] = {Shape0::CH, Shape1::CH, Shape2::CH, Shape3::CH, Shape4::CH};
-constexpr int HK_SHAPE_G[HK_NSHAPES] = {Shape0::G, Shape1::G, Shape2::G, Shape3::G, Shape4::G};
+using Shape5 = TileShape<128, 16, 5, 4>;
+using Shape6 = TileShape<64, 16, 8, 4>;
+constexpr int HK_NSHAPES = 7;
+constexpr int HK_SHAPE_CH[HK_NSHAPES] = {Shape0::CH, Shape1::CH, Shape2::CH, Shape3::CH,
+                                         Shape4::CH, Shape5::CH, Shape6::CH};
+constexpr int HK_SHAPE_G[HK_NSHAPES] = {Shape0::G, Shape1::G, Shape2::G, Shape3::G,
+                                        Shape4::G, Shape5::G, Shape6::G};
+constexpr int HK_SHAPE_WARPS[HK_NSHAPES] = {Shape0::WARPS, Shape1::WARPS, Shape2::WARPS, Shape3::WARPS,
+                                            Shape4::WARPS, Shape5::WARPS, Shape6::WARPS};
 
 // Staged line record of the mixed form.  Regions A and B are summed in FP32
 // (flushed into the FP64 per-point sums at least once per chunk of lines)
@@ -568,7 +576,7 @@ __device__ __forceinline__ void flush_sums(float2 (&a32)[PPL / 2], double *__res
 // ------------------------------------------------------- persistent kernel
 // mixed form: SH::MINB CTAs per SM (4: 32 warps, 64 registers)
 template <bool MIXED, class SH>
-__global__ void __launch_bounds__(HK_THREADS, MIXED ? SH::MINB : 2)
+__global__ void __launch_bounds__(SH::THREADS, MIXED ? SH::MINB : 2)
 voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
                  int64_t nlines, GridDev g, const StateDev *__restrict__ states,
                  int tile0, int tiles_per_state, int nsplit, int total_tickets,
@@ -864,6 +872,7 @@ cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream) {
 int voigt_num_shapes() { return HK_NSHAPES; }
 int voigt_tile_points(int shape) { return HK_SHAPE_G[shape < 0 || shape >= HK_NSHAPES ? 0 : shape]; }
 int voigt_chunk_lines(int shape) { return HK_SHAPE_CH[shape < 0 || shape >= HK_NSHAPES ? 0 : shape]; }
+int voigt_tile_warps(int shape) { return HK_SHAPE_WARPS[shape < 0 || shape >= HK_NSHAPES ? 0 : shape]; }
 
 // Calls f(kernel, dynamic shared memory) for the kernel of (precision,
 // shape); the plain FP64 form has the default shape only.
@@ -871,13 +880,18 @@ template <class F>
 static cudaError_t with_kernel(bool mixed, int shape, F &&f) {
   using KFn = void (*)(const void *, const double *, int64_t, GridDev, const StateDev *, int, int,
                        int, int, unsigned *, double *, unsigned *, double *, int64_t);
-  if (!mixed) return f((KFn)voigt_sum_kernel<false, Shape0>, sizeof(RecD) * Shape0::CH);
+  if (!mixed) return f((KFn)voigt_sum_kernel<false, Shape0>, sizeof(RecD) * Shape0::CH, Shape0::THREADS);
   switch (shape) {
-    case 0: return f((KFn)voigt_sum_kernel<true, Shape0>, smem_mixed<Shape0>());
-    case 1: return f((KFn)voigt_sum_kernel<true, Shape1>, smem_mixed<Shape1>());
-    case 2: return f((KFn)voigt_sum_kernel<true, Shape2>, smem_mixed<Shape2>());
-    case 3: return f((KFn)voigt_sum_kernel<true, Shape3>, smem_mixed<Shape3>());
-    case 4: return f((KFn)voigt_sum_kernel<true, Shape4>, smem_mixed<Shape4>());
+#define HK_SHAPE_CASE(n) \
+  case n: return f((KFn)voigt_sum_kernel<true, Shape##n>, smem_mixed<Shape##n>(), Shape##n::THREADS);
+    HK_SHAPE_CASE(0)
+    HK_SHAPE_CASE(1)
+    HK_SHAPE_CASE(2)
+    HK_SHAPE_CASE(3)
+    HK_SHAPE_CASE(4)
+    HK_SHAPE_CASE(5)
+    HK_SHAPE_CASE(6)
+#undef HK_SHAPE_CASE
     default: return cudaErrorInvalidValue;
   }
 }
@@ -886,10 +900,10 @@ static int voigt_ctas(bool mixed, int shape) {
   int dev = 0, nsm = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  with_kernel(mixed, shape, [&](auto kfn, size_t smem) {
+  with_kernel(mixed, shape, [&](auto kfn, size_t smem, int threads) {
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, HK_THREADS, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
   });
   return nsm * (per_sm < 1 ? 1 : per_sm);
 }
@@ -953,12 +967,12 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d
     if (e != cudaSuccess) return e;
   }
   const int ctas = (int)std::min<int64_t>(pl.ctas, total);
-  e = with_kernel(mixed, pl.shape, [&](auto kfn, size_t smem) {
+  e = with_kernel(mixed, pl.shape, [&](auto kfn, size_t smem, int threads) {
     if (smem > 48 * 1024) {
       const cudaError_t ea = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (ea != cudaSuccess) return ea;
     }
-    kfn<<<ctas, HK_THREADS, smem, stream>>>(prep_d, nu0_d, nlines, g, states_d, pl.tile0,
+    kfn<<<ctas, threads, smem, stream>>>(prep_d, nu0_d, nlines, g, states_d, pl.tile0,
                                             pl.tiles_per_state, pl.nsplit, total, ticket_d,
                                             partial_d, tile_cnt_d, K_d, k_stride);
     return cudaGetLastError();

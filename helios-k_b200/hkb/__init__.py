@@ -83,7 +83,7 @@ def lib():
             "hk_last_launches": (_i64, [_p]),
             "hk_count_pairs": (_i, [_p, _d, _d, _p]),
             "hk_num_tile_shapes": (_i, []),
-            "hk_tile_shape_info": (_i, [_i, _p, _p]),
+            "hk_tile_shape_info": (_i, [_i, _p, _p, _p]),
             "hk_set_tuning": (_i, [_p, _i]),
             "hk_set_tile_shape": (_i, [_p, _i]),
             "hk_tuning_result": (_i, [_p, _p, _p, _p]),
@@ -444,12 +444,14 @@ def num_tile_shapes() -> int:
     return int(lib().hk_num_tile_shapes())
 
 
-def tile_shape(shape):
-    """(lines per staged chunk, grid points per tile) of a tile shape."""
+def tile_shape(shape, warps=False):
+    """(lines per staged chunk, grid points per tile[, warps per CTA]) of a
+    tile shape."""
     a = np.zeros(1, np.int32)
     b = np.zeros(1, np.int32)
-    st = lib().hk_tile_shape_info(int(shape), _ptr(a), _ptr(b))
+    w = np.zeros(1, np.int32)
+    st = lib().hk_tile_shape_info(int(shape), _ptr(a), _ptr(b), _ptr(w))
     if st != HK_OK:
         raise HkError(st, "tile shape %d out of range" % shape)
-    return int(a[0]), int(b[0])
+    return (int(a[0]), int(b[0]), int(w[0])) if warps else (int(a[0]), int(b[0]))
 

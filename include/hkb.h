@@ -239,13 +239,13 @@ hk_status hk_transmission(hk_ctx *ctx, int nstates, const double *K, const int32
 /* ------------------------------------------------------ tile shapes */
 
 /* The mixed Voigt kernel runs in one of hk_num_tile_shapes() tile shapes:
- * lines per staged chunk x grid points per tile (shape 0, the default: 128 x
- * 2048).  The shape changes only the order of the FP64 additions (results
+ * lines per staged chunk x grid points per tile, run by a number of warps
+ * per CTA (shape 0, the default: 128 x 2048, 8 warps).  The shape changes only the order of the FP64 additions (results
  * differ in the last bits, within the same error bound); the plain FP64 form
  * always uses shape 0.  Replaces the reference's kernel self-tuning
  * (doTuning, heliosk.cu:1363-1705; tile widths nkA..nkC, heliosk.cu:968-982). */
 int hk_num_tile_shapes(void);
-hk_status hk_tile_shape_info(int shape, int *lines_per_chunk, int *points_per_tile);
+hk_status hk_tile_shape_info(int shape, int *lines_per_chunk, int *points_per_tile, int *warps);
 
 /* mode 0: the fixed shape (hk_set_tile_shape, default 0).
  * mode 1: tune when the probes cost at most a tenth of the call's sweep

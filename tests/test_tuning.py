@@ -16,7 +16,7 @@ from test_gpu_parity import NBINS, DNU, NUMAX, NUMIN, STATES, masked_relerr, ora
 
 pytestmark = pytest.mark.gpu
 
-NSHAPES = 5
+NSHAPES = 7
 
 
 @pytest.fixture(scope="module")
@@ -34,11 +34,11 @@ def small():
 
 def test_shape_table():
     assert hkb.num_tile_shapes() == NSHAPES
-    shapes = [hkb.tile_shape(v) for v in range(NSHAPES)]
-    assert shapes[0] == (128, 2048) and hkb.tile_points() == 2048
+    shapes = [hkb.tile_shape(v, warps=True) for v in range(NSHAPES)]
+    assert shapes[0] == (128, 2048, 8) and hkb.tile_points() == 2048
     assert len(set(shapes)) == NSHAPES
-    for ch, g in shapes:
-        assert ch % 32 == 0 and 2048 % g == 0
+    for ch, g, w in shapes:
+        assert ch % 32 == 0 and 2048 % g == 0 and ch <= 32 * w
     with pytest.raises(hkb.HkError):
         hkb.tile_shape(NSHAPES)
 
@@ -114,7 +114,7 @@ def test_tuning_mode1_pays_off_only_for_batches(small):
         ctx.set_tuning(1)
         ctx.opacity([1500.0], [0.1], hkb.MIXED)
         assert ctx.tuning_result()[1] == -1  # probes would cost more than the call
-        ns = 200
+        ns = 40 * NSHAPES + 20  # probes: shapes x 4 states x the whole grid <= 10 % of the call
         T = np.linspace(200.0, 3000.0, ns)
         P = 10.0 ** np.linspace(-6.0, 2.0, ns)
         K = torch.empty((ns, ctx.nx), dtype=torch.float64, device="cuda")
