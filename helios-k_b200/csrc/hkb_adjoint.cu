@@ -22,6 +22,8 @@
 // FP64 (the differentiated Algorithm-916 series); the sums are FP64.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "hkb_device.cuh"
 #include "hkb_kernels.h"
 
@@ -74,26 +76,65 @@ __device__ __forceinline__ void ab_terms(bool regionB, F x, F y, double Sp, doub
   cy = Sp * (double)(t + F(2) * Y * tY);
 }
 
+// Regions A and B of the mixed form in FP32: t, dt/ds, dt/dY of the shape
+// with one reciprocal (gh2_grad divides three times).
+__device__ __forceinline__ void ab_grad_f(bool regionB, float s, float Y, float &t, float &ts,
+                                          float &tY) {
+  const float u = s + Y;
+  if (!regionB) {
+    t = rcp_fast(u);
+    ts = -t * t;
+    tY = ts;
+    return;
+  }
+  const float a1 = u + 1.5f;
+  const float c4 = (float)(4.0 / CUDART_PI), c6 = (float)(6.0 / CUDART_PI);
+  const float num = fmaf(a1, u + 1.0f, -c4 * s);
+  const float q = fmaf(a1, a1, -c6 * s);
+  const float rden = rcp_fast(u * q);
+  t = num * rden;
+  const float num_s = (u + 1.0f) + a1 - c4, num_Y = (u + 1.0f) + a1;
+  const float den_s = fmaf(u, 2.0f * a1 - c6, q), den_Y = fmaf(u, 2.0f * a1, q);
+  ts = fmaf(-t, den_s, num_s) * rden;
+  tY = fmaf(-t, den_Y, num_Y) * rden;
+}
+
+// Tickets are (tile, part): a tile's line range is cut into nsplit parts so
+// that a grid of a few hundred tiles still fills the GPU; the per-line sums
+// go to G through FP64 atomics either way.
+// Mixed form: per line, the offset at the tile's first point of the window
+// is formed in FP64 once, x_k = (k - kc) vb + fr in FP32 as in the forward
+// (k - kc exact, |fr| <= vb/2); regions A and B accumulate per lane in FP32
+// with the line strength factored out, region C in FP64, and the lane sums
+// are reduced in FP64.
 template <bool MIXED>
-__global__ void __launch_bounds__(AD_THREADS)
+__global__ void __launch_bounds__(AD_THREADS, MIXED ? 4 : 2)
 adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ nu0, int64_t nlines,
-                    GridDev g, const StateDev *__restrict__ states, int ntiles,
+                    GridDev g, const StateDev *__restrict__ states, int ntiles, int nsplit,
                     unsigned *__restrict__ ticket, const double *__restrict__ u,
                     double *__restrict__ G) {
   __shared__ double su[AD_G];
+  __shared__ float suf[AD_G];
   __shared__ int s_t;
   __shared__ long long s_L0, s_L1;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const StateDev &st = states[0];
   const double isp = 0.56418958354775628695;  // 1/sqrt(pi)
+  const double idnu = 1.0 / g.dnu;
+  const int ntickets = ntiles * nsplit;
   for (;;) {
     if (tid == 0) s_t = (int)atomicAdd(ticket, 1u);
     __syncthreads();
     const int t = s_t;
-    if (t >= ntiles) break;
-    const int64_t g0 = (int64_t)t * AD_G;
+    if (t >= ntickets) break;
+    const int tile = t / nsplit, part = t - tile * nsplit;
+    const int64_t g0 = (int64_t)tile * AD_G;
     const int64_t g1 = min(g0 + (int64_t)AD_G, g.nx);
-    for (int k = tid; k < AD_G; k += AD_THREADS) su[k] = (g0 + k < g1) ? u[g0 + k] : 0.0;
+    for (int k = tid; k < AD_G; k += AD_THREADS) {
+      const double v = (g0 + k < g1) ? u[g0 + k] : 0.0;
+      su[k] = v;
+      suf[k] = (float)v;
+    }
     if (warp == 0) {
       const double W = st.wmax + st.shift + 2.0 * g.dnu;
       const double xlo = grid_x(g, g0) - W, xhi = grid_x(g, g1 - 1) + W;
@@ -101,8 +142,8 @@ adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ n
       const int64_t L0 = ad_lower_bound_warp(nu0, nlines, xlo - pad);
       const int64_t L1 = ad_lower_bound_warp(nu0, nlines, xhi + pad);
       if (lane == 0) {
-        s_L0 = L0;
-        s_L1 = L1;
+        s_L0 = L0 + (L1 - L0) * part / nsplit;
+        s_L1 = L0 + (L1 - L0) * (part + 1) / nsplit;
       }
     }
     __syncthreads();
@@ -113,24 +154,72 @@ adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ n
       if (lo >= hi || lp.Sc == 0.0) continue;
       const double Sp = lp.Sc * isp;  // S^/pi
       double gS = 0.0, gy = 0.0, gx = 0.0, gn = 0.0;
-      for (int64_t k = lo + lane; k < hi; k += 32) {
-        const double uk = su[k - g0];
-        const double xd = __dmul_rn(__dsub_rn(grid_x(g, k), lp.nu), lp.iad);
-        double c, cx, cy;
-        if (k >= lp.c0 && k < lp.c1) {
+      if (MIXED) {
+        // tile-relative int32 bounds: the A/B points [a0, c0) and [c1, a1),
+        // region B within [rb0, rb1), region C [c0, c1)
+        const int a0 = (int)(lo - g0), a1 = (int)(hi - g0);
+        const int rc0 = (int)min(max((int64_t)lp.c0, lo), hi) - (int)g0;
+        const int rc1 = (int)min(max((int64_t)lp.c1, lo), hi) - (int)g0;
+        const int rb0 = (int)min(max((int64_t)lp.b0, lo), hi) - (int)g0;
+        const int rb1 = (int)min(max((int64_t)lp.b1, lo), hi) - (int)g0;
+        const double D0 = __dmul_rn(__dsub_rn(grid_x(g, g0), lp.nu), lp.iad);
+        const double vb = __dmul_rn(g.dnu, lp.iad);
+        const double kc = fmin(fmax(rint((lp.nu - grid_x(g, g0)) * idnu), -8388608.0), 8388608.0);
+        const float vbf = (float)vb, frf = (float)(D0 + kc * vb), nkc = (float)(-kc);
+        const float Y = (float)(lp.vy * lp.vy);
+        // per lane: fS = sum u t, fY = sum u dt/dY, fn = sum u dt/ds x,
+        // fx = sum u dt/ds x^2 (s = x^2)
+        float fS = 0.f, fY = 0.f, fn = 0.f, fx = 0.f;
+        auto ab_seg = [&](int k0, int k1) {
+          float kf = (float)(k0 + lane) + nkc;
+          for (int k = k0 + lane; k < k1; k += 32, kf += 32.0f) {
+            const float uk = suf[k];
+            const float x = fmaf(kf, vbf, frf);
+            float tt, ts, tY;
+            ab_grad_f(k >= rb0 && k < rb1, x * x, Y, tt, ts, tY);
+            const float bs = uk * ts, bsx = bs * x;
+            fS = fmaf(uk, tt, fS);
+            fY = fmaf(uk, tY, fY);
+            fn += bsx;
+            fx = fmaf(bsx, x, fx);
+          }
+        };
+        ab_seg(a0, rc0);
+        ab_seg(rc1, a1);
+        for (int k = rc0 + lane; k < rc1; k += 32) {
+          const double xd = __dmul_rn(__dsub_rn(grid_x(g, g0 + k), lp.nu), lp.iad);
+          const double uk = su[k];
           const VDer d = voigt916_dd(xd, lp.vy, lp.ey);
-          c = lp.Sc * d.v;
-          cx = lp.Sc * d.vx;
-          cy = lp.Sc * d.vy;
-        } else if (MIXED) {
-          ab_terms<float>(k >= lp.b0 && k < lp.b1, (float)xd, (float)lp.vy, Sp, c, cx, cy);
-        } else {
-          ab_terms<double>(k >= lp.b0 && k < lp.b1, xd, lp.vy, Sp, c, cx, cy);
+          const double cx = lp.Sc * d.vx;
+          gS = fma(uk, lp.Sc * d.v, gS);
+          gy = fma(uk, lp.Sc * d.vy, gy);
+          gx = fma(uk * cx, xd, gx);
+          gn = fma(uk, cx, gn);
         }
-        gS = fma(uk, c, gS);
-        gy = fma(uk, cy, gy);
-        gx = fma(uk * cx, xd, gx);
-        gn = fma(uk, cx, gn);
+        // S^/pi y t, S^/pi (t + 2Y dt/dY), S^/pi 2y x dt/ds (times x for gx)
+        const double Spy = Sp * lp.vy;
+        gS = fma(Spy, (double)fS, gS);
+        gy = fma(Sp, fma(2.0 * lp.vy * lp.vy, (double)fY, (double)fS), gy);
+        gx = fma(2.0 * Spy, (double)fx, gx);
+        gn = fma(2.0 * Spy, (double)fn, gn);
+      } else {
+        for (int64_t k = lo + lane; k < hi; k += 32) {
+          const double uk = su[k - g0];
+          const double xd = __dmul_rn(__dsub_rn(grid_x(g, k), lp.nu), lp.iad);
+          double c, cx, cy;
+          if (k >= lp.c0 && k < lp.c1) {
+            const VDer d = voigt916_dd(xd, lp.vy, lp.ey);
+            c = lp.Sc * d.v;
+            cx = lp.Sc * d.vx;
+            cy = lp.Sc * d.vy;
+          } else {
+            ab_terms<double>(k >= lp.b0 && k < lp.b1, xd, lp.vy, Sp, c, cx, cy);
+          }
+          gS = fma(uk, c, gS);
+          gy = fma(uk, cy, gy);
+          gx = fma(uk * cx, xd, gx);
+          gn = fma(uk, cx, gn);
+        }
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
@@ -237,16 +326,23 @@ cudaError_t launch_opacity_vjp(bool mixed, const LinesDev &L, const GridDev &g,
   if (e != cudaSuccess) return e;
   if (L.n == 0 || g.nx == 0) return cudaSuccess;
   const int ntiles = (int)((g.nx + AD_G - 1) / AD_G);
-  int dev = 0, nsm = 0;
+  int dev = 0, nsm = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int ctas = min(ntiles, nsm * 4);
+  if (mixed)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_tile_kernel<true>, AD_THREADS, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_tile_kernel<false>, AD_THREADS, 0);
+  const int resident = nsm * (per_sm < 1 ? 1 : per_sm);
+  // about 8 tickets per resident CTA, at most 32 parts of a tile's lines
+  const int nsplit = (int)std::min<int64_t>(32, std::max<int64_t>(1, (8LL * resident + ntiles - 1) / ntiles));
+  const int ctas = (int)std::min<int64_t>((int64_t)ntiles * nsplit, resident);
   if (mixed)
     adjoint_tile_kernel<true><<<ctas, AD_THREADS, 0, stream>>>(prep_d, L.nu0, L.n, g, state_d, ntiles,
-                                                               ticket_d, u_d, G_d);
+                                                               nsplit, ticket_d, u_d, G_d);
   else
     adjoint_tile_kernel<false><<<ctas, AD_THREADS, 0, stream>>>(prep_d, L.nu0, L.n, g, state_d, ntiles,
-                                                                ticket_d, u_d, G_d);
+                                                                nsplit, ticket_d, u_d, G_d);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   adjoint_line_kernel<<<(unsigned)((L.n + 255) / 256), 256, 0, stream>>>(L, state_h, G_d, order_d,
