@@ -343,12 +343,13 @@ def run_adjoint(args):
     clk = Clocks(0)
     clk.start()
     t0 = time.perf_counter()
-    fwd = []
+    fwd, vjp = [], []
     for _ in range(args.steps):
         ctx.opacity([T], [P], prec, out=K, stream=stream)
         torch.cuda.synchronize()
         fwd.append(ctx.last_timing()[0])
         ctx.opacity_vjp(T, P, w / K[0], prec)
+        vjp.append(ctx.last_timing()[0])
     torch.cuda.synchronize()
     ms = (time.perf_counter() - t0) * 1e3 / args.steps
     clocks = clk.stop()
@@ -363,8 +364,10 @@ def run_adjoint(args):
                       "loss": "sum_i w_i log K_i, w ~ N(0,1)",
                       "timing": "wall clock around synchronous steps"},
            "pairs": {"A": pa, "B": pb, "C": pc}, "forward_voigt_ms": fwd_ms,
-           "adjoint_ms": ms - fwd_ms, "clocks": clocks,
-           "gpu_launches": args.steps * 7}  # prep 2 + voigt, then prep 2 + 2 adjoint
+           "adjoint_ms": ms - fwd_ms, "adjoint_kernels_ms": float(np.mean(vjp)),
+           "adjoint_pairs_per_s": pairs / (float(np.mean(vjp)) * 1e-3), "clocks": clocks,
+           # prep 2 + voigt, then prep 2 + the adjoint tile (+ mixed region C) and line kernels
+           "gpu_launches": args.steps * (8 if prec == hkb.MIXED else 7)}
     print(json.dumps(out), flush=True)
     ctx.close()
 

@@ -18,8 +18,9 @@
 // so that dLoss/dlog S^ = G_S, dLoss/dy = G_y, dLoss/d(1/alphaD) at fixed y
 // = G_x alphaD and dLoss/dnu_l = -G_n / alphaD.  Pass 2 (adjoint_line_kernel)
 // applies the chain rule of the line scaling (prep_line) to T and P.
-// Mixed form: regions A and B in FP32 (x from the FP64 offset), region C in
-// FP64 (the differentiated Algorithm-916 series); the sums are FP64.
+// Mixed form: regions A and B in FP32 (x from the FP64 offset) in pass 1,
+// region C in FP64 (the differentiated Algorithm-916 series) in its own
+// per-line pass (adjoint_c_kernel) between the two; the sums are FP64.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -105,16 +106,16 @@ __device__ __forceinline__ void ab_grad_f(bool regionB, float s, float Y, float 
 // Mixed form: per line, the offset at the tile's first point of the window
 // is formed in FP64 once, x_k = (k - kc) vb + fr in FP32 as in the forward
 // (k - kc exact, |fr| <= vb/2); regions A and B accumulate per lane in FP32
-// with the line strength factored out, region C in FP64, and the lane sums
-// are reduced in FP64.
+// with the line strength factored out and the lane sums are reduced in FP64;
+// region C is left to adjoint_c_kernel.
 template <bool MIXED>
 __global__ void __launch_bounds__(AD_THREADS, MIXED ? 4 : 2)
 adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ nu0, int64_t nlines,
                     GridDev g, const StateDev *__restrict__ states, int ntiles, int nsplit,
                     unsigned *__restrict__ ticket, const double *__restrict__ u,
                     double *__restrict__ G) {
-  __shared__ double su[AD_G];
-  __shared__ float suf[AD_G];
+  __shared__ double su[AD_G];  // u of the tile (FP32 in the first half for MIXED)
+  float *suf = reinterpret_cast<float *>(su);
   __shared__ int s_t;
   __shared__ long long s_L0, s_L1;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -132,8 +133,10 @@ adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ n
     const int64_t g1 = min(g0 + (int64_t)AD_G, g.nx);
     for (int k = tid; k < AD_G; k += AD_THREADS) {
       const double v = (g0 + k < g1) ? u[g0 + k] : 0.0;
-      su[k] = v;
-      suf[k] = (float)v;
+      if (MIXED)
+        suf[k] = (float)v;
+      else
+        su[k] = v;
     }
     if (warp == 0) {
       const double W = st.wmax + st.shift + 2.0 * g.dnu;
@@ -186,16 +189,6 @@ adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ n
         };
         ab_seg(a0, rc0);
         ab_seg(rc1, a1);
-        for (int k = rc0 + lane; k < rc1; k += 32) {
-          const double xd = __dmul_rn(__dsub_rn(grid_x(g, g0 + k), lp.nu), lp.iad);
-          const double uk = su[k];
-          const VDer d = voigt916_dd(xd, lp.vy, lp.ey);
-          const double cx = lp.Sc * d.vx;
-          gS = fma(uk, lp.Sc * d.v, gS);
-          gy = fma(uk, lp.Sc * d.vy, gy);
-          gx = fma(uk * cx, xd, gx);
-          gn = fma(uk, cx, gn);
-        }
         // S^/pi y t, S^/pi (t + 2Y dt/dY), S^/pi 2y x dt/ds (times x for gx)
         const double Spy = Sp * lp.vy;
         gS = fma(Spy, (double)fS, gS);
@@ -236,6 +229,48 @@ adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ n
       }
     }
     __syncthreads();
+  }
+}
+
+// Region C of the mixed form: one warp per line over its whole [c0, c1)
+// window in FP64 (Algorithm 916 with derivatives), added to the line's sums
+// after the tile pass.  Kept out of the tile kernel, whose FP32 loop would
+// otherwise carry the FP64 call's registers.  One warp owns each line, and
+// the tile pass has finished on the stream, so the adds need no atomics.
+__global__ void __launch_bounds__(AD_THREADS)
+adjoint_c_kernel(const LinePrep *__restrict__ P, int64_t nlines, GridDev g,
+                 const double *__restrict__ u, double *__restrict__ G) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = ((int64_t)blockIdx.x * AD_THREADS + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * AD_THREADS) >> 5;
+  for (int64_t l = w0; l < nlines; l += nw) {
+    const LinePrep &lp = P[l];
+    if (lp.c0 >= lp.c1 || lp.Sc == 0.0) continue;
+    const double Sc = lp.Sc, nu = lp.nu, iad = lp.iad, vy = lp.vy, ey = lp.ey;
+    double gS = 0.0, gy = 0.0, gx = 0.0, gn = 0.0;
+    for (int64_t k = lp.c0 + lane; k < lp.c1; k += 32) {
+      const double xd = __dmul_rn(__dsub_rn(grid_x(g, k), nu), iad);
+      const double uk = u[k];
+      const VDer d = voigt916_dd(xd, vy, ey);
+      const double cx = Sc * d.vx;
+      gS = fma(uk, Sc * d.v, gS);
+      gy = fma(uk, Sc * d.vy, gy);
+      gx = fma(uk * cx, xd, gx);
+      gn = fma(uk, cx, gn);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      gS += __shfl_xor_sync(0xffffffffu, gS, o);
+      gy += __shfl_xor_sync(0xffffffffu, gy, o);
+      gx += __shfl_xor_sync(0xffffffffu, gx, o);
+      gn += __shfl_xor_sync(0xffffffffu, gn, o);
+    }
+    if (lane == 0) {
+      G[l] += gS;
+      G[nlines + l] += gy;
+      G[2 * nlines + l] += gx;
+      G[3 * nlines + l] += gn;
+    }
   }
 }
 
@@ -345,6 +380,11 @@ cudaError_t launch_opacity_vjp(bool mixed, const LinesDev &L, const GridDev &g,
                                                                 nsplit, ticket_d, u_d, G_d);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (mixed) {
+    adjoint_c_kernel<<<nsm * 8, AD_THREADS, 0, stream>>>(prep_d, L.n, g, u_d, G_d);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   adjoint_line_kernel<<<(unsigned)((L.n + 255) / 256), 256, 0, stream>>>(L, state_h, G_d, order_d,
                                                                          dlogS_d, dgam_d, dTP_d);
   return cudaGetLastError();

@@ -1085,9 +1085,14 @@ hk_status hk_opacity_vjp(hk_ctx *c, double T, double P, int precision, const dou
     dlS = dlogS ? next : nullptr;
     dgm = dgammaL ? next + n : nullptr;
   }
+  CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
   CUDA_TRY(c, launch_opacity_vjp(precision == HK_PRECISION_MIXED, c->L, c->g, c->states.as<StateDev>(),
                                  hs[0], c->prep.as<LinePrep>(), ud, c->ticket.as<unsigned>(), G,
                                  c->order.as<int64_t>(), dlS, dgm, dTP, s));
+  CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
+  c->voigt_ms_acc = 0.0;
+  c->voigt_ms_acc_only = false;
+  c->have_voigt_t = true;
   double tp[2] = {0.0, 0.0};
   CUDA_TRY(c, cudaMemcpyAsync(tp, dTP, sizeof tp, cudaMemcpyDeviceToHost, s));
   if (!outputs_on_device) {

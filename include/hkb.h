@@ -336,7 +336,8 @@ hk_status hk_profile_eval(hk_ctx *ctx, int64_t n, const double *x,
                           const double *y, int precision, double *out);
 
 /* Device time of the last hk_opacity / hk_kdist kernels (CUDA events on
- * the launching stream), in milliseconds; and the grid tile size. */
+ * the launching stream), in milliseconds; and the grid tile size.  After
+ * hk_opacity_vjp, voigt_ms is the time of its two adjoint kernels. */
 hk_status hk_last_timing(const hk_ctx *ctx, double *voigt_ms, double *kdist_ms);
 int hk_tile_points(void);
 
