@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 
 #include "hkb_device.cuh"
 #include "hkb_kernels.h"
@@ -100,28 +101,20 @@ __device__ __forceinline__ void ab_grad_f(bool regionB, float s, float Y, float 
   tY = fmaf(-t, den_Y, num_Y) * rden;
 }
 
-// Tickets are (tile, part): a tile's line range is cut into nsplit parts so
-// that a grid of a few hundred tiles still fills the GPU; the per-line sums
-// go to G through FP64 atomics either way.
-// Mixed form: per line, the offset at the tile's first point of the window
-// is formed in FP64 once, x_k = (k - kc) vb + fr in FP32 as in the forward
-// (k - kc exact, |fr| <= vb/2); regions A and B accumulate per lane in FP32
-// with the line strength factored out and the lane sums are reduced in FP64;
-// region C is left to adjoint_c_kernel.
-template <bool MIXED>
-__global__ void __launch_bounds__(AD_THREADS, MIXED ? 4 : 2)
+// Plain form, FP64 throughout.  Tickets are (tile, part): a tile's line
+// range is cut into nsplit parts so that a grid of a few hundred tiles
+// still fills the GPU; the per-line sums go to G through FP64 atomics.
+__global__ void __launch_bounds__(AD_THREADS, 2)
 adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ nu0, int64_t nlines,
                     GridDev g, const StateDev *__restrict__ states, int ntiles, int nsplit,
                     unsigned *__restrict__ ticket, const double *__restrict__ u,
                     double *__restrict__ G) {
-  __shared__ double su[AD_G];  // u of the tile (FP32 in the first half for MIXED)
-  float *suf = reinterpret_cast<float *>(su);
+  __shared__ double su[AD_G];
   __shared__ int s_t;
   __shared__ long long s_L0, s_L1;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const StateDev &st = states[0];
   const double isp = 0.56418958354775628695;  // 1/sqrt(pi)
-  const double idnu = 1.0 / g.dnu;
   const int ntickets = ntiles * nsplit;
   for (;;) {
     if (tid == 0) s_t = (int)atomicAdd(ticket, 1u);
@@ -131,13 +124,7 @@ adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ n
     const int tile = t / nsplit, part = t - tile * nsplit;
     const int64_t g0 = (int64_t)tile * AD_G;
     const int64_t g1 = min(g0 + (int64_t)AD_G, g.nx);
-    for (int k = tid; k < AD_G; k += AD_THREADS) {
-      const double v = (g0 + k < g1) ? u[g0 + k] : 0.0;
-      if (MIXED)
-        suf[k] = (float)v;
-      else
-        su[k] = v;
-    }
+    for (int k = tid; k < AD_G; k += AD_THREADS) su[k] = (g0 + k < g1) ? u[g0 + k] : 0.0;
     if (warp == 0) {
       const double W = st.wmax + st.shift + 2.0 * g.dnu;
       const double xlo = grid_x(g, g0) - W, xhi = grid_x(g, g1 - 1) + W;
@@ -157,62 +144,22 @@ adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ n
       if (lo >= hi || lp.Sc == 0.0) continue;
       const double Sp = lp.Sc * isp;  // S^/pi
       double gS = 0.0, gy = 0.0, gx = 0.0, gn = 0.0;
-      if (MIXED) {
-        // tile-relative int32 bounds: the A/B points [a0, c0) and [c1, a1),
-        // region B within [rb0, rb1), region C [c0, c1)
-        const int a0 = (int)(lo - g0), a1 = (int)(hi - g0);
-        const int rc0 = (int)min(max((int64_t)lp.c0, lo), hi) - (int)g0;
-        const int rc1 = (int)min(max((int64_t)lp.c1, lo), hi) - (int)g0;
-        const int rb0 = (int)min(max((int64_t)lp.b0, lo), hi) - (int)g0;
-        const int rb1 = (int)min(max((int64_t)lp.b1, lo), hi) - (int)g0;
-        const double D0 = __dmul_rn(__dsub_rn(grid_x(g, g0), lp.nu), lp.iad);
-        const double vb = __dmul_rn(g.dnu, lp.iad);
-        const double kc = fmin(fmax(rint((lp.nu - grid_x(g, g0)) * idnu), -8388608.0), 8388608.0);
-        const float vbf = (float)vb, frf = (float)(D0 + kc * vb), nkc = (float)(-kc);
-        const float Y = (float)(lp.vy * lp.vy);
-        // per lane: fS = sum u t, fY = sum u dt/dY, fn = sum u dt/ds x,
-        // fx = sum u dt/ds x^2 (s = x^2)
-        float fS = 0.f, fY = 0.f, fn = 0.f, fx = 0.f;
-        auto ab_seg = [&](int k0, int k1) {
-          float kf = (float)(k0 + lane) + nkc;
-          for (int k = k0 + lane; k < k1; k += 32, kf += 32.0f) {
-            const float uk = suf[k];
-            const float x = fmaf(kf, vbf, frf);
-            float tt, ts, tY;
-            ab_grad_f(k >= rb0 && k < rb1, x * x, Y, tt, ts, tY);
-            const float bs = uk * ts, bsx = bs * x;
-            fS = fmaf(uk, tt, fS);
-            fY = fmaf(uk, tY, fY);
-            fn += bsx;
-            fx = fmaf(bsx, x, fx);
-          }
-        };
-        ab_seg(a0, rc0);
-        ab_seg(rc1, a1);
-        // S^/pi y t, S^/pi (t + 2Y dt/dY), S^/pi 2y x dt/ds (times x for gx)
-        const double Spy = Sp * lp.vy;
-        gS = fma(Spy, (double)fS, gS);
-        gy = fma(Sp, fma(2.0 * lp.vy * lp.vy, (double)fY, (double)fS), gy);
-        gx = fma(2.0 * Spy, (double)fx, gx);
-        gn = fma(2.0 * Spy, (double)fn, gn);
-      } else {
-        for (int64_t k = lo + lane; k < hi; k += 32) {
-          const double uk = su[k - g0];
-          const double xd = __dmul_rn(__dsub_rn(grid_x(g, k), lp.nu), lp.iad);
-          double c, cx, cy;
-          if (k >= lp.c0 && k < lp.c1) {
-            const VDer d = voigt916_dd(xd, lp.vy, lp.ey);
-            c = lp.Sc * d.v;
-            cx = lp.Sc * d.vx;
-            cy = lp.Sc * d.vy;
-          } else {
-            ab_terms<double>(k >= lp.b0 && k < lp.b1, xd, lp.vy, Sp, c, cx, cy);
-          }
-          gS = fma(uk, c, gS);
-          gy = fma(uk, cy, gy);
-          gx = fma(uk * cx, xd, gx);
-          gn = fma(uk, cx, gn);
+      for (int64_t k = lo + lane; k < hi; k += 32) {
+        const double uk = su[k - g0];
+        const double xd = __dmul_rn(__dsub_rn(grid_x(g, k), lp.nu), lp.iad);
+        double c, cx, cy;
+        if (k >= lp.c0 && k < lp.c1) {
+          const VDer d = voigt916_dd(xd, lp.vy, lp.ey);
+          c = lp.Sc * d.v;
+          cx = lp.Sc * d.vx;
+          cy = lp.Sc * d.vy;
+        } else {
+          ab_terms<double>(k >= lp.b0 && k < lp.b1, xd, lp.vy, Sp, c, cx, cy);
         }
+        gS = fma(uk, c, gS);
+        gy = fma(uk, cy, gy);
+        gx = fma(uk * cx, xd, gx);
+        gn = fma(uk, cx, gn);
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
@@ -232,44 +179,276 @@ adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ n
   }
 }
 
-// Region C of the mixed form: one warp per line over its whole [c0, c1)
-// window in FP64 (Algorithm 916 with derivatives), added to the line's sums
-// after the tile pass.  Kept out of the tile kernel, whose FP32 loop would
-// otherwise carry the FP64 call's registers.  One warp owns each line, and
-// the tile pass has finished on the stream, so the adds need no atomics.
+// ------------------------------------------------------------ mixed form
+constexpr int AB_G = 8192;  // grid points per tile of the mixed A/B pass
+
+// Warp sum of four values per lane with six shuffles: the first two levels
+// halve the values each lane carries, so value q's total ends in lanes
+// 8q .. 8q+7.
+template <class F>
+__device__ __forceinline__ F warp_sum4(F v0, F v1, F v2, F v3, int lane) {
+  const bool h4 = lane & 16, h3 = lane & 8;
+  const F w0 = (h4 ? v2 : v0) + __shfl_xor_sync(0xffffffffu, h4 ? v0 : v2, 16);
+  const F w1 = (h4 ? v3 : v1) + __shfl_xor_sync(0xffffffffu, h4 ? v1 : v3, 16);
+  F z = (h3 ? w1 : w0) + __shfl_xor_sync(0xffffffffu, h3 ? w0 : w1, 8);
+  z += __shfl_xor_sync(0xffffffffu, z, 4);
+  z += __shfl_xor_sync(0xffffffffu, z, 2);
+  z += __shfl_xor_sync(0xffffffffu, z, 1);
+  return z;
+}
+
+// The four per-lane sums of one line over tile points [k0, k1) of one
+// region (B or A), x_k = (k + kf0) vb + fr in FP32 with k + kf0 exact:
+//   fS = sum u t,  fY = sum u dt/dY,  fn = sum u dt/ds x,  fx = sum u dt/ds x^2
+// (s = x^2; region A: t = 1/(s+Y), dt/ds = dt/dY = -t^2).  U and A are the
+// types of u and of the sums: FP32 for tiles staged in FP32, FP64 for the
+// others.
+template <bool REGION_B, class U, class A>
+__device__ __forceinline__ void ab_seg(const U *__restrict__ us, int k0, int k1, int lane, float kf0,
+                                       float vbf, float frf, float Y, A &fS, A &fY, A &fn, A &fx) {
+  float kf = (float)(k0 + lane) + kf0;
+  for (int k = k0 + lane; k < k1; k += 32, kf += 32.0f) {
+    const A uk = (A)us[k];
+    const float x = fmaf(kf, vbf, frf);
+    if (REGION_B) {
+      float t, ts, tY;
+      ab_grad_f(true, x * x, Y, t, ts, tY);
+      const A bsx = uk * (A)(ts * x);
+      fS = fma(uk, (A)t, fS);
+      fY = fma(uk, (A)tY, fY);
+      fn += bsx;
+      fx = fma(bsx, (A)x, fx);
+    } else {
+      const float t = rcp_fast(fmaf(x, x, Y));
+      const A a = uk * (A)t;
+      const A p = a * (A)t, px = p * (A)x;
+      fS += a;
+      fY -= p;
+      fn -= px;
+      fx = fma(-px, (A)x, fx);
+    }
+  }
+}
+
+template <class U, class A>
+__device__ __forceinline__ void ab_line(const U *__restrict__ us, int a0, int rb0, int rc0, int rc1,
+                                        int rb1, int a1, int lane, float kf0, float vbf, float frf,
+                                        float Y, A &fS, A &fY, A &fn, A &fx) {
+  ab_seg<false>(us, a0, rb0, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+  ab_seg<true>(us, rb0, rc0, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+  ab_seg<true>(us, rc1, rb1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+  ab_seg<false>(us, rb1, a1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+}
+
+// Regions A and B of the mixed form.  Per line, the offset at the tile's
+// first point is formed in FP64 once and x_k = (k - kc) vb + fr follows in
+// FP32 as in the forward (k - kc exact, |fr| <= vb/2); the shape terms are
+// FP32 with one reciprocal.  u is staged in shared memory as FP32 scaled by
+// 2^-e (e from the tile's largest |u|), so the per-lane products and sums
+// are FP32 with the line strength and 2^e factored out; lane sums are
+// reduced in FP32 and added to G in FP64.  A tile whose nonzero |u| span
+// more than 2^64, or that holds a non-finite u, keeps u and the sums in
+// FP64 (u read from global memory).  Region C is left to adjoint_c_kernel.
+__global__ void __launch_bounds__(AD_THREADS, 4)
+adjoint_ab_kernel(const LinePrep *__restrict__ P, const double *__restrict__ nu0, int64_t nlines,
+                  GridDev g, const StateDev *__restrict__ states, int ntiles, int nsplit,
+                  unsigned *__restrict__ ticket, const double *__restrict__ u,
+                  double *__restrict__ G) {
+  __shared__ float suf[AB_G];
+  __shared__ double s_max[AD_WARPS], s_min[AD_WARPS];
+  __shared__ int s_bad[AD_WARPS];
+  __shared__ int s_t;
+  __shared__ long long s_L0, s_L1;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const StateDev &st = states[0];
+  const double isp = 0.56418958354775628695;  // 1/sqrt(pi)
+  const double idnu = 1.0 / g.dnu;
+  const int ntickets = ntiles * nsplit;
+  for (;;) {
+    if (tid == 0) s_t = (int)atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int t = s_t;
+    if (t >= ntickets) break;
+    const int tile = t / nsplit, part = t - tile * nsplit;
+    const int64_t g0 = (int64_t)tile * AB_G;
+    const int64_t g1 = min(g0 + (int64_t)AB_G, g.nx);
+    const int gi0 = (int)g0, gn = (int)(g1 - g0);
+    // the tile's range of |u|
+    {
+      double amax = 0.0, amin = CUDART_INF;
+      int bad = 0;
+      for (int k = tid; k < gn; k += AD_THREADS) {
+        const double v = fabs(u[g0 + k]);
+        bad |= !(v <= DBL_MAX);
+        amax = fmax(amax, v);
+        if (v > 0.0) amin = fmin(amin, v);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+        amin = fmin(amin, __shfl_xor_sync(0xffffffffu, amin, o));
+      }
+      bad = __any_sync(0xffffffffu, bad);
+      if (lane == 0) {
+        s_max[warp] = amax;
+        s_min[warp] = amin;
+        s_bad[warp] = bad;
+      }
+    }
+    if (warp == 0) {
+      const double W = st.wmax + st.shift + 2.0 * g.dnu;
+      const double xlo = grid_x(g, g0) - W, xhi = grid_x(g, g1 - 1) + W;
+      const double pad = 1e-12 * (fabs(xlo) + fabs(xhi)) + 1e-300;
+      const int64_t L0 = ad_lower_bound_warp(nu0, nlines, xlo - pad);
+      const int64_t L1 = ad_lower_bound_warp(nu0, nlines, xhi + pad);
+      if (lane == 0) {
+        s_L0 = L0 + (L1 - L0) * part / nsplit;
+        s_L1 = L0 + (L1 - L0) * (part + 1) / nsplit;
+      }
+    }
+    __syncthreads();
+    double amax = 0.0, amin = CUDART_INF;
+    int bad = 0;
+#pragma unroll
+    for (int w = 0; w < AD_WARPS; ++w) {
+      amax = fmax(amax, s_max[w]);
+      amin = fmin(amin, s_min[w]);
+      bad |= s_bad[w];
+    }
+    const int e = amax > 0.0 ? ilogb(amax) + 1 : 0;
+    const bool f32 = !bad && e > -1000 && e < 1000 && (amax == 0.0 || amin >= ldexp(amax, -64));
+    const double su_scale = f32 ? ldexp(1.0, e) : 1.0;  // u = su_scale * staged value
+    if (f32) {
+      const double inv = ldexp(1.0, -e);
+      for (int k = tid; k < AB_G; k += AD_THREADS) suf[k] = k < gn ? (float)(u[g0 + k] * inv) : 0.f;
+    }
+    __syncthreads();
+    const int64_t L0 = s_L0, L1 = s_L1;
+    const double xg0 = grid_x(g, g0);
+    for (int64_t l = L0 + warp; l < L1; l += AD_WARPS) {
+      const LinePrep &lp = P[l];
+      const int a0 = max(lp.i0 - gi0, 0), a1 = min(lp.i1 - gi0, gn);
+      const double Sc = lp.Sc;
+      if (a0 >= a1 || Sc == 0.0) continue;
+      // tile-relative bounds: A [a0, rb0), B [rb0, rc0), C [rc0, rc1),
+      // B [rc1, rb1), A [rb1, a1)
+      const int rb0 = min(max(lp.b0 - gi0, a0), a1), rc0 = min(max(lp.c0 - gi0, a0), a1);
+      const int rc1 = min(max(lp.c1 - gi0, a0), a1), rb1 = min(max(lp.b1 - gi0, a0), a1);
+      const double nu = lp.nu, iad = lp.iad, vy = lp.vy;
+      const double D0 = __dmul_rn(__dsub_rn(xg0, nu), iad);
+      const double vb = __dmul_rn(g.dnu, iad);
+      const double kc = fmin(fmax(rint((nu - xg0) * idnu), -8388608.0), 8388608.0);
+      const float vbf = (float)vb, frf = (float)(D0 + kc * vb), kf0 = (float)(-kc);
+      const double Yd = vy * vy;
+      const float Y = (float)Yd;
+      double z, zS;
+      if (f32) {
+        float fS = 0.f, fY = 0.f, fn = 0.f, fx = 0.f;
+        ab_line(suf, a0, rb0, rc0, rc1, rb1, a1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+        const float zf = warp_sum4(fS, fY, fn, fx, lane);
+        z = (double)zf;
+        zS = (double)__shfl_sync(0xffffffffu, zf, 0);
+      } else {
+        double fS = 0.0, fY = 0.0, fn = 0.0, fx = 0.0;
+        ab_line(u + g0, a0, rb0, rc0, rc1, rb1, a1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+        z = warp_sum4(fS, fY, fn, fx, lane);
+        zS = __shfl_sync(0xffffffffu, z, 0);
+      }
+      // value q = lane / 8: 0 fS, 1 fY, 2 fn, 3 fx.
+      //   G_S = S^/pi y fS, G_y = S^/pi (fS + 2Y fY), G_x = 2 S^/pi y fx,
+      //   G_n = 2 S^/pi y fn  (times the staging scale)
+      if ((lane & 7) == 0) {
+        const int q = lane >> 3;
+        const double Sp = Sc * isp * su_scale, Spy = Sp * vy;
+        const double v = q == 0 ? Spy * zS : q == 1 ? Sp * fma(2.0 * Yd, z, zS) : 2.0 * Spy * z;
+        const int64_t dst = q == 0 ? 0 : q == 1 ? 1 : q == 2 ? 3 : 2;
+        atomicAdd(&G[dst * nlines + l], v);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Region C of the mixed form in FP64 (Algorithm 916 with derivatives),
+// after the A/B pass.  Each warp takes 32 consecutive lines and walks the
+// concatenation of their [c0, c1) windows, one (line, point) pair per lane,
+// so lanes stay busy whatever the windows' widths (a few points per line);
+// the owner of pair j is found by a binary search over the warp's prefix
+// sums of the widths.  Pair terms are summed per line by a segmented
+// shuffle scan, and the last lane of each line's run adds to G.
 __global__ void __launch_bounds__(AD_THREADS)
 adjoint_c_kernel(const LinePrep *__restrict__ P, int64_t nlines, GridDev g,
                  const double *__restrict__ u, double *__restrict__ G) {
+  const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int64_t w0 = ((int64_t)blockIdx.x * AD_THREADS + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * AD_THREADS) >> 5;
-  for (int64_t l = w0; l < nlines; l += nw) {
-    const LinePrep &lp = P[l];
-    if (lp.c0 >= lp.c1 || lp.Sc == 0.0) continue;
-    const double Sc = lp.Sc, nu = lp.nu, iad = lp.iad, vy = lp.vy, ey = lp.ey;
-    double gS = 0.0, gy = 0.0, gx = 0.0, gn = 0.0;
-    for (int64_t k = lp.c0 + lane; k < lp.c1; k += 32) {
-      const double xd = __dmul_rn(__dsub_rn(grid_x(g, k), nu), iad);
-      const double uk = u[k];
-      const VDer d = voigt916_dd(xd, vy, ey);
-      const double cx = Sc * d.vx;
-      gS = fma(uk, Sc * d.v, gS);
-      gy = fma(uk, Sc * d.vy, gy);
-      gx = fma(uk * cx, xd, gx);
-      gn = fma(uk, cx, gn);
+  for (int64_t base = w0 * 32; base < nlines; base += nw * 32) {
+    const int64_t lme = base + lane;
+    int c0 = 0, wd = 0;
+    if (lme < nlines) {
+      const LinePrep &lp = P[lme];
+      if (lp.Sc != 0.0 && lp.c1 > lp.c0) {
+        c0 = lp.c0;
+        wd = lp.c1 - lp.c0;
+      }
     }
+    int incl = wd;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      gS += __shfl_xor_sync(0xffffffffu, gS, o);
-      gy += __shfl_xor_sync(0xffffffffu, gy, o);
-      gx += __shfl_xor_sync(0xffffffffu, gx, o);
-      gn += __shfl_xor_sync(0xffffffffu, gn, o);
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += v;
     }
-    if (lane == 0) {
-      G[l] += gS;
-      G[nlines + l] += gy;
-      G[2 * nlines + l] += gx;
-      G[3 * nlines + l] += gn;
+    const int total = __shfl_sync(FULL, incl, 31);
+    for (int j0 = 0; j0 < total; j0 += 32) {
+      const int j = j0 + lane;
+      // q = number of lanes whose inclusive sum is <= j: the owner of pair j
+      int q = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int v = __shfl_sync(FULL, incl, q + step - 1);
+        if (v <= j) q += step;
+      }
+      const bool act = j < total;
+      if (!act) q = 31;
+      const int qc0 = __shfl_sync(FULL, c0, q);
+      const int qincl = __shfl_sync(FULL, incl, q), qwd = __shfl_sync(FULL, wd, q);
+      double gS = 0.0, gy = 0.0, gx = 0.0, gn = 0.0;
+      if (act) {
+        const LinePrep &lp = P[base + q];
+        const int64_t k = (int64_t)qc0 + (j - (qincl - qwd));
+        const double xd = __dmul_rn(__dsub_rn(grid_x(g, k), lp.nu), lp.iad);
+        const double uk = u[k];
+        const double Sc = lp.Sc;
+        const VDer d = voigt916_dd(xd, lp.vy, lp.ey);
+        const double cx = Sc * d.vx;
+        gS = uk * (Sc * d.v);
+        gy = uk * (Sc * d.vy);
+        gx = uk * cx * xd;
+        gn = uk * cx;
+      }
+      // segmented inclusive scan over lanes of equal q (q ascends with lane)
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int qo = __shfl_up_sync(FULL, q, o);
+        const double a = __shfl_up_sync(FULL, gS, o), b = __shfl_up_sync(FULL, gy, o);
+        const double c = __shfl_up_sync(FULL, gx, o), d = __shfl_up_sync(FULL, gn, o);
+        if (lane >= o && qo == q) {
+          gS += a;
+          gy += b;
+          gx += c;
+          gn += d;
+        }
+      }
+      const int qn = __shfl_down_sync(FULL, q, 1);
+      const bool actn = __shfl_down_sync(FULL, (int)act, 1);
+      if (act && (lane == 31 || qn != q || !actn)) {
+        const int64_t l = base + q;
+        atomicAdd(&G[l], gS);
+        atomicAdd(&G[nlines + l], gy);
+        atomicAdd(&G[2 * nlines + l], gx);
+        atomicAdd(&G[3 * nlines + l], gn);
+      }
     }
   }
 }
@@ -360,31 +539,31 @@ cudaError_t launch_opacity_vjp(bool mixed, const LinesDev &L, const GridDev &g,
   if (e == cudaSuccess) e = cudaMemsetAsync(ticket_d, 0, sizeof(unsigned), stream);
   if (e != cudaSuccess) return e;
   if (L.n == 0 || g.nx == 0) return cudaSuccess;
-  const int ntiles = (int)((g.nx + AD_G - 1) / AD_G);
+  const int tpts = mixed ? AB_G : AD_G;
+  const int ntiles = (int)((g.nx + tpts - 1) / tpts);
   int dev = 0, nsm = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (mixed)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_tile_kernel<true>, AD_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_ab_kernel, AD_THREADS, 0);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_tile_kernel<false>, AD_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_tile_kernel, AD_THREADS, 0);
   const int resident = nsm * (per_sm < 1 ? 1 : per_sm);
-  // about 8 tickets per resident CTA, at most 32 parts of a tile's lines
-  const int nsplit = (int)std::min<int64_t>(32, std::max<int64_t>(1, (8LL * resident + ntiles - 1) / ntiles));
+  // about 8 tickets per resident CTA, at most 64 parts of a tile's lines
+  const int nsplit = (int)std::min<int64_t>(64, std::max<int64_t>(1, (8LL * resident + ntiles - 1) / ntiles));
   const int ctas = (int)std::min<int64_t>((int64_t)ntiles * nsplit, resident);
-  if (mixed)
-    adjoint_tile_kernel<true><<<ctas, AD_THREADS, 0, stream>>>(prep_d, L.nu0, L.n, g, state_d, ntiles,
-                                                               nsplit, ticket_d, u_d, G_d);
-  else
-    adjoint_tile_kernel<false><<<ctas, AD_THREADS, 0, stream>>>(prep_d, L.nu0, L.n, g, state_d, ntiles,
-                                                                nsplit, ticket_d, u_d, G_d);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
   if (mixed) {
-    adjoint_c_kernel<<<nsm * 8, AD_THREADS, 0, stream>>>(prep_d, L.n, g, u_d, G_d);
+    adjoint_ab_kernel<<<ctas, AD_THREADS, 0, stream>>>(prep_d, L.nu0, L.n, g, state_d, ntiles, nsplit,
+                                                       ticket_d, u_d, G_d);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    adjoint_c_kernel<<<nsm * 8, AD_THREADS, 0, stream>>>(prep_d, L.n, g, u_d, G_d);
+  } else {
+    adjoint_tile_kernel<<<ctas, AD_THREADS, 0, stream>>>(prep_d, L.nu0, L.n, g, state_d, ntiles, nsplit,
+                                                         ticket_d, u_d, G_d);
   }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   adjoint_line_kernel<<<(unsigned)((L.n + 255) / 256), 256, 0, stream>>>(L, state_h, G_d, order_d,
                                                                          dlogS_d, dgam_d, dTP_d);
   return cudaGetLastError();

@@ -61,6 +61,37 @@ def test_vjp_plain_and_mixed_vs_oracle(adj):
         assert eS < tol_line and eG < tol_line
 
 
+@pytest.mark.parametrize("case", ["beyond_fp32", "wide_tile"])
+def test_vjp_mixed_seed_range(adj, case):
+    """The mixed form stages u per 8192-point tile as FP32 scaled by a power
+    of two; a seed beyond the FP32 range takes the scale, and a tile whose
+    nonzero |u| span more than 2^64 keeps u and its sums in FP64."""
+    ctx = adj["ctx"]
+    _, K = loss(adj, T0, P0)
+    u = adj["w"] / K
+    if case == "beyond_fp32":
+        u = u * 1e45
+    else:
+        u = u.copy()
+        u[:5000] *= 1e30   # first tile only
+        u[20000:20010] = 0.0
+    rT, rP, rS, rG = reference(adj, u=u)
+    dT, dP, dS, dG = ctx.opacity_vjp(T0, P0, u, hkb.MIXED)
+    eT, eP = abs(dT - rT) / abs(rT), abs(dP - rP) / abs(rP)
+    eS = np.max(np.abs(dS - rS)) / np.max(np.abs(rS))
+    eG = np.max(np.abs(dG - rG)) / np.max(np.abs(rG))
+    print(f"{case}: dT {eT:.2e} dP {eP:.2e} dlogS {eS:.2e} dgammaL {eG:.2e}")
+    assert np.all(np.isfinite(dS)) and np.all(np.isfinite(dG))
+    assert eT < 1e-4 and eP < 1e-4
+    assert eS < 1e-5 and eG < 1e-5
+    if case == "wide_tile":
+        # lines of the other tiles, on their own scale
+        far = np.zeros(ctx.num_lines, bool)
+        far[ctx.line_order()] = ctx.state_lines(T0, P0)[0] > NUMIN + 5000 * DNU + 60.0
+        m = np.max(np.abs(rS[far]))
+        assert np.max(np.abs(dS[far] - rS[far])) < 1e-5 * m
+
+
 def test_vjp_vs_central_differences(adj):
     ctx = adj["ctx"]
     rT, rP, rS, rG = reference(adj)
