@@ -521,11 +521,29 @@ struct VDer {
 };
 
 // Algorithm 916 in FP64 with forward-mode derivatives: the series of
-// voigt916_d (same terms, same stopping rule, so v equals voigt916_d) with
-// each term differentiated.  With k = 2a/pi, q = sin(xy)^2 / y:
+// voigt916_d (same terms, same stopping rule) with each term differentiated.
+// With k = 2a/pi, q = sin(xy)^2 / y:
 //   V  = e^{-x^2} erfcx(y) cos 2xy + k e^{-x^2} q + k y (-cos 2xy s1 + (s2 + s3)/2)
 // and d erfcx/dy = 2y erfcx(y) - 2/sqrt(pi).  V is even in x.
-static __device__ __noinline__ VDer voigt916_dd(double x, double y, double ey) {
+// The Gaussian factors of the terms follow from recurrences instead of one
+// exp per term: with E_n = exp(-a^2 n^2) (E_n = E_{n-1} exp(-a^2) exp(-2a^2)^{n-1}),
+//   exp(-(a^2 n^2 + x^2)) = e^{-x^2} E_n,   exp(-(an + x)^2) = e^{-x^2} E_n R^n,
+//   exp(-(d + an)^2) = e^{-d^2} E_n P^n,    exp(-(d' - an)^2) = e^{-d'^2} E_n M^n,
+// R = exp(-2a|x|), d = a(n0 - 1) - |x|, P = exp(-2ad), d' = a n0 - |x|,
+// M = exp(2ad'): four exps per call in place of four per term (a few ulp
+// apart from the direct exps over the 10-15 terms the tolerance needs).
+constexpr double HK_E916_A2 = 0.778805723222652;   // exp(-a^2), a = HK_A916_D
+constexpr double HK_E916_2A2 = 0.606538354524358;  // exp(-2 a^2)
+
+__host__ __device__ inline double hk_rcp_d(double v) {
+#ifdef __CUDA_ARCH__
+  return __drcp_rn(v);
+#else
+  return 1.0 / v;
+#endif
+}
+
+__host__ __device__ __noinline__ inline VDer voigt916_dd(double x, double y, double ey) {
   const double a = HK_A916_D;
   const double ax = fabs(x), sx = x < 0.0 ? -1.0 : 1.0;
   const double ex2 = exp(-ax * ax);
@@ -537,34 +555,46 @@ static __device__ __noinline__ VDer voigt916_dd(double x, double y, double ey) {
     o.vy = 2.0 * y * ey - 2.0 * isp;
     return o;
   }
-  double s1 = 0.0, s2 = 0.0, s3 = 0.0, s1y = 0.0, s2x = 0.0, s2y = 0.0, s3x = 0.0, s3y = 0.0;
+  // s1, s2, s3 and, per sum, the weighted sums its derivatives need:
+  //   s1f = sum f^2 e1,  s2w = sum (an + x) f e2,  s2f = sum f^2 e2,
+  //   s3w = sum (a n3 - x) f3 e3,  s3f = sum f3^2 e3
+  double s1 = 0.0, s2 = 0.0, s3 = 0.0, s1f = 0.0, s2w = 0.0, s2f = 0.0, s3w = 0.0, s3f = 0.0;
   {
     double o1 = 0.0, o2 = 0.0, o3 = 0.0;
     const double yy = y * y;
     const int n0 = (int)ceil(ax / a);
+    const double d = a * (n0 - 1) - ax, d2 = a * n0 - ax;
+    const double R = exp(-2.0 * a * ax), P = exp(-2.0 * a * d), M = exp(2.0 * a * d2);
+    const double ex2p = exp(-d * d), ex2n = exp(-d2 * d2);
+    double E = 1.0, gE = HK_E916_A2, Rn = 1.0, Pn = 1.0, Mn = 1.0;
     bool st1 = false, st2 = false, st3 = false;
     for (int n = 1; n < 100; ++n) {
       const int n3p = n0 + n - 1, n3n = n0 - n;
-      const double an = a * n, an3p = a * n3p, an3n = a * n3n;
-      const double f = 1.0 / (an * an + yy);
-      const double f3p = 1.0 / (an3p * an3p + yy);
-      const double f3n = 1.0 / (an3n * an3n + yy);
-      const double e1 = exp(-(an * an + ax * ax));
-      const double e2 = exp(-(an + ax) * (an + ax));
-      const double e3p = exp(-(an3p - ax) * (an3p - ax));
-      s1 += f * e1;
-      s1y += -2.0 * y * f * f * e1;
-      s2 += f * e2;
-      s2x += -2.0 * (an + ax) * f * e2;
-      s2y += -2.0 * y * f * f * e2;
-      s3 += f3p * e3p;
-      s3x += 2.0 * (an3p - ax) * f3p * e3p;
-      s3y += -2.0 * y * f3p * f3p * e3p;
+      E *= gE;
+      gE *= HK_E916_2A2;
+      Rn *= R;
+      Pn *= P;
+      Mn *= M;
+      const double an = a * n, an3p = a * n3p;
+      const double f = hk_rcp_d(an * an + yy);
+      const double f3p = hk_rcp_d(an3p * an3p + yy);
+      const double e1 = ex2 * E;
+      const double fe1 = f * e1, fe2 = fe1 * Rn, fe3 = f3p * (ex2p * E * Pn);
+      s1 += fe1;
+      s1f += f * fe1;
+      s2 += fe2;
+      s2w += (an + ax) * fe2;
+      s2f += f * fe2;
+      s3 += fe3;
+      s3w += (d + an) * fe3;
+      s3f += f3p * fe3;
       if (n3n >= 1) {
-        const double e3n = exp(-(an3n - ax) * (an3n - ax));
-        s3 += f3n * e3n;
-        s3x += 2.0 * (an3n - ax) * f3n * e3n;
-        s3y += -2.0 * y * f3n * f3n * e3n;
+        const double an3n = a * n3n;
+        const double f3n = hk_rcp_d(an3n * an3n + yy);
+        const double fe = f3n * (ex2n * E * Mn);
+        s3 += fe;
+        s3w += (d2 - an) * fe;
+        s3f += f3n * fe;
       }
       if (fabs(s1 - o1) < HK_TOL) st1 = true;
       if (fabs(s2 - o2) < HK_TOL) st2 = true;
@@ -575,9 +605,18 @@ static __device__ __noinline__ VDer voigt916_dd(double x, double y, double ey) {
       o3 = s3;
     }
   }
-  const double s1x = -2.0 * ax * s1;
+  const double s1x = -2.0 * ax * s1, s1y = -2.0 * y * s1f;
+  const double s2x = -2.0 * s2w, s2y = -2.0 * y * s2f;
+  const double s3x = 2.0 * s3w, s3y = -2.0 * y * s3f;
   const double xy = ax * y;
-  const double c2 = cos(2.0 * xy), sn2 = sin(2.0 * xy), sn = sin(xy);
+  double c2, sn2;
+#ifdef __CUDA_ARCH__
+  sincos(2.0 * xy, &sn2, &c2);
+#else
+  sn2 = sin(2.0 * xy);
+  c2 = cos(2.0 * xy);
+#endif
+  const double sn = sin(xy);
   const double k = 2.0 * a / CUDART_PI;
   double q, qy;
   if (y != 0.0) {
