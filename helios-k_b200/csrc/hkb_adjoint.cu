@@ -207,6 +207,7 @@ template <bool REGION_B, class U, class A>
 __device__ __forceinline__ void ab_seg(const U *__restrict__ us, int k0, int k1, int lane, float kf0,
                                        float vbf, float frf, float Y, A &fS, A &fY, A &fn, A &fx) {
   float kf = (float)(k0 + lane) + kf0;
+#pragma unroll 4
   for (int k = k0 + lane; k < k1; k += 32, kf += 32.0f) {
     const A uk = (A)us[k];
     const float x = fmaf(kf, vbf, frf);
