@@ -725,9 +725,10 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   }
   // States run in batches whose per-(state, line) records fit the prep
   // budget; each batch is one prep launch and one persistent Voigt launch.
-  // profiles 2-4, plinth removal and sub-Lorentzian wings run the FP64 form
-  // (the mixed form's FP32 region sums are built for the plain Voigt regions)
-  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile == 1 && !c->g.plinth && !c->g.subL;
+  // profiles 3-4, plinth removal and sub-Lorentzian wings run the FP64 form
+  // (the mixed form's FP32 sums hold the Voigt regions; the Lorentz profile
+  // is its region A over the whole window)
+  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile <= 2 && !c->g.plinth && !c->g.subL;
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
@@ -1130,9 +1131,10 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   CUDA_TRY(c, c->wbits.ensure(2 * nstates * sizeof(unsigned long long)));
   CUDA_TRY(c, cudaMemcpy(c->states.p, hs.data(), nstates * sizeof(StateDev), cudaMemcpyHostToDevice));
   const int64_t nx = c->g.nx;
-  // profiles 2-4, plinth removal and sub-Lorentzian wings run the FP64 form
-  // (the mixed form's FP32 region sums are built for the plain Voigt regions)
-  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile == 1 && !c->g.plinth && !c->g.subL;
+  // profiles 3-4, plinth removal and sub-Lorentzian wings run the FP64 form
+  // (the mixed form's FP32 sums hold the Voigt regions; the Lorentz profile
+  // is its region A over the whole window)
+  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile <= 2 && !c->g.plinth && !c->g.subL;
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
   if (per_state > c->prep_budget)
     return fail(c, HK_ERR_UNSUPPORTED, "one state's line records (%zu B) exceed the workspace (%zu B): "

@@ -96,14 +96,16 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
     const LineState ls = prep_line(L, st, l);
     int64_t w[6];
     line_windows(g, st, ls, 0, g.nx, w);
-    // S1 per profile (S3_kernel voigt.h:452-463); the mixed form is Voigt only
+    // S1 per profile (S3_kernel voigt.h:452-463); the mixed form runs profiles 1-2
     const double Sc = ls.S * (1.0 / 1.7724538509055160273);
     const double S1 = (MIXED || g.profile <= 2) ? ls.S * ls.vy / CUDART_PI
                                                 : (g.profile == 3 ? Sc : ls.S);
     const bool hasC = w[3] > w[2];
     // largest region-A/B term of the line: S1 / r^2 with r^2 >= max(100, y^2)
+    // (Voigt: region C covers r < 10), r^2 >= y^2 for the Lorentz profile
     const double Y = ls.vy * ls.vy;
-    const double term = S1 / fmax(100.0, Y);
+    const double rmin = g.profile == 2 ? Y : fmax(100.0, Y);
+    const double term = rmin > 0.0 ? S1 / rmin : 0.0;
     if (MODE == PREP_STATS) {
     } else if (MIXED) {
       const double ey = hasC ? erfcx(ls.vy) : 1.0;
@@ -132,7 +134,9 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
         const double xb = fabs((grid_x(g, w[5] - 1) - ls.nu) * ls.iad);
         const double umax = fmax(xa, xb) * fmax(xa, xb) + Y;
         if (umax >= 1e18) flags |= HK_PF_WIDE;
-        if (fmax(100.0, Y) < 0x1p-64 * umax || Y > 0x1p60) flags |= HK_PF_RANGE;
+        // (Lorentz: Y >= 2^-60 also keeps the product of two denominators,
+        // >= Y^2, a normal float)
+        if (rmin < 0x1p-64 * umax || Y > 0x1p60 || (g.profile == 2 && Y < 0x1p-60)) flags |= HK_PF_RANGE;
       }
       r.flags = flags;
       // region C's Algorithm-916 part: |x| < sqrt(36 - y^2), from the FP64

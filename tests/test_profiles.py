@@ -1,10 +1,13 @@
 """GPU: profiles 2-4 and plinth removal (hk_set_profile) against the FP64
 oracle (voigt.h:1091-1262 restated).
 
-Both precisions run the FP64 form for these, so the bound is the FP64 one:
-1e-12 relative where K > 1e-6 of its bin maximum; with plinth removal, where
-each point is a difference of profile values and plinths, 1e-9.  Index
-windows (no regions B and C for profiles 2-4) are bit-exact.
+The Lorentz profile (2) without plinth removal runs the mixed form's region
+A over the whole window when the mixed precision is asked for: 1e-5
+relative where K > 1e-6 of its bin maximum (the mixed bound).  Everything
+else runs the FP64 form in both precisions, so the bound is the FP64 one:
+1e-12; with plinth removal, where each point is a difference of profile
+values and plinths, 1e-9.  Index windows (no regions B and C for profiles
+2-4) are bit-exact.
 """
 import numpy as np
 import pytest
@@ -63,7 +66,10 @@ def test_profile_matches_oracle(small, profile, plinth, cutMode, cut):
             K = ctx.opacity([T], [P], prec)[0]
             err, n = masked_relerr(K, Kref, NBINS)
             print(f"profile {profile} plinth {plinth} cut {cutMode}/{cut} T={T} P={P} err {err:.2e}")
-            assert err < (1e-9 if plinth else 1e-12)
+            if prec == hkb.MIXED and profile == 2 and not plinth:
+                assert err < 1e-5
+            else:
+                assert err < (1e-9 if plinth else 1e-12)
     with pytest.raises(hkb.HkError) as e:
         ctx.opacity_vjp(1500.0, 0.1, np.ones(ctx.nx))
     assert e.value.status == -8
