@@ -186,14 +186,15 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
       else if (g.cutMode == 2) w_loc = fmax(w_loc, g.cut / ls.iad);
     }
   }
-  if (MODE == PREP_RECORDS) return;
-  for (int o = 16; o > 0; o >>= 1) {
-    w_loc = fmax(w_loc, __shfl_xor_sync(0xffffffffu, w_loc, o));
-    s1_loc = fmax(s1_loc, __shfl_xor_sync(0xffffffffu, s1_loc, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    if (g.cutMode != 0) atomicMax(&wbits[2 * s], (unsigned long long)__double_as_longlong(w_loc));
-    atomicMax(&wbits[2 * s + 1], (unsigned long long)__double_as_longlong(s1_loc));
+  if constexpr (MODE != PREP_RECORDS) {
+    for (int o = 16; o > 0; o >>= 1) {
+      w_loc = fmax(w_loc, __shfl_xor_sync(0xffffffffu, w_loc, o));
+      s1_loc = fmax(s1_loc, __shfl_xor_sync(0xffffffffu, s1_loc, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      if (g.cutMode != 0) atomicMax(&wbits[2 * s], (unsigned long long)__double_as_longlong(w_loc));
+      atomicMax(&wbits[2 * s + 1], (unsigned long long)__double_as_longlong(s1_loc));
+    }
   }
 }
 
