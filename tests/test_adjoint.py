@@ -151,3 +151,66 @@ def test_autograd_function(adj):
     assert np.max(np.abs(log_s.grad.numpy() - rS)) < 1e-9 * np.max(np.abs(rS))
     assert np.max(np.abs(log_g.grad.numpy() - rG * aL)) < 1e-9 * np.max(np.abs(rG * aL))
     ctx.set_line_scales(None, None)
+
+
+def _fd_vs_vjp(ctx, w, T0, P0, h=2.5e-4):
+    """dLoss/dT, dLoss/dP of Loss = sum w log K from the VJP (plain FP64)
+    against central differences of the forward at h and h/2 relative,
+    Richardson-extrapolated (error O(h^4): the net derivative can be a small
+    difference of large per-line terms).  T0 +- h T0 must stay inside one
+    segment of the partition table (1 K nodes): Q(T) is piecewise linear and
+    the VJP takes the slope of the segment holding T0."""
+    def lossf(T, P):
+        return float(np.sum(w * np.log(ctx.opacity([T], [P], hkb.PLAIN_FP64)[0])))
+
+    def central(dT_, dP_):
+        if dT_:
+            return (lossf(T0 + dT_, P0) - lossf(T0 - dT_, P0)) / (2 * dT_)
+        return (lossf(T0, P0 + dP_) - lossf(T0, P0 - dP_)) / (2 * dP_)
+    K = ctx.opacity([T0], [P0], hkb.PLAIN_FP64)[0]
+    assert np.all(K > 0.0)
+    dT, dP, _, _ = ctx.opacity_vjp(T0, P0, w / K, hkb.PLAIN_FP64)
+    hT, hP = h * T0, h * P0
+    fT = (4.0 * central(hT / 2, 0) - central(hT, 0)) / 3.0
+    fP = (4.0 * central(0, hP / 2) - central(0, hP)) / 3.0
+    return dT, fT, dP, fP
+
+
+def test_vjp_exomol_vs_central_differences():
+    """ExoMol lists: S scaling by exp(-c2 E''/T) without the HITRAN
+    reference-temperature ratio, widths from the species defaults with P0 =
+    1 bar; the chain rule of adjoint_line_kernel's ExoMol branch."""
+    L = synth.exomol_lines(3000, seed=8, nu_max=NUMAX)
+    L["nu"] = NUMIN - 30.0 + (NUMAX - NUMIN + 60.0) * (L["nu"] / NUMAX)
+    Tq, Qq = synth.q_table()
+    with hkb.Context(0) as ctx:
+        ctx.set_species(hkb.EXOMOL, [synth.MASS], [1.0], defaultL=0.07, defaultn=0.5)
+        ctx.set_partition(0, Tq, Qq)
+        ctx.load_lines_exomol(L)
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+        w = np.random.default_rng(3).standard_normal(ctx.nx)
+        dT, fT, dP, fP = _fd_vs_vjp(ctx, w, 800.5, P0)
+    print(f"exomol: dT {dT:.6g} fd {fT:.6g}; dP {dP:.6g} fd {fP:.6g}")
+    assert abs(fT - dT) < 1e-4 * abs(dT)
+    assert abs(fP - dP) < 1e-4 * abs(dP)
+
+
+def test_vjp_two_isotopologues_vs_central_differences():
+    """Two isotopologues with their own masses, abundances and partition
+    tables: d ln Q / dT per isotopologue in the chain rule."""
+    L = synth.hitran_lines(1500, seed=9, nu_max=NUMAX + 30.0, nu_min=NUMIN - 30.0)
+    L["iso"] = (np.arange(1500) % 3 == 0).astype(np.int32)
+    L["delta"] = np.random.default_rng(4).uniform(-0.01, 0.01, 1500)
+    Tq, Qq = synth.q_table()
+    with hkb.Context(0) as ctx:
+        ctx.set_species(hkb.HITRAN, [synth.MASS, synth.MASS + 2.0], [0.9, 0.1])
+        ctx.set_partition(0, Tq, Qq)
+        ctx.set_partition(1, Tq, Qq * (1.0 + Tq / 3000.0))
+        ctx.set_options(qalphaL=0.6)
+        ctx.load_lines_hitran(L)
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+        w = np.random.default_rng(5).standard_normal(ctx.nx)
+        dT, fT, dP, fP = _fd_vs_vjp(ctx, w, 800.5, P0)
+    print(f"two isotopologues: dT {dT:.6g} fd {fT:.6g}; dP {dP:.6g} fd {fP:.6g}")
+    assert abs(fT - dT) < 1e-4 * abs(dT)
+    assert abs(fP - dP) < 1e-4 * abs(dP)
