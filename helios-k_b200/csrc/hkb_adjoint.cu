@@ -342,8 +342,11 @@ adjoint_ab_kernel(const LinePrep *__restrict__ P, const double *__restrict__ nu0
       const float vbf = (float)vb, frf = (float)(D0 + kc * vb), kf0 = (float)(-kc);
       const double Yd = vy * vy;
       const float Y = (float)Yd;
+      // Lorentz lines with y^2 < 2^-40 would square t = 1/(x^2 + y^2) past
+      // the FP32 range at the centre: their sums stay in FP64
+      const bool f32l = f32 && !(g.profile == 2 && Yd < 0x1p-40);
       double z, zS;
-      if (f32) {
+      if (f32l) {
         float fS = 0.f, fY = 0.f, fn = 0.f, fx = 0.f;
         ab_line(suf, a0, rb0, rc0, rc1, rb1, a1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
         const float zf = warp_sum4(fS, fY, fn, fx, lane);
@@ -360,7 +363,7 @@ adjoint_ab_kernel(const LinePrep *__restrict__ P, const double *__restrict__ nu0
       //   G_n = 2 S^/pi y fn  (times the staging scale)
       if ((lane & 7) == 0) {
         const int q = lane >> 3;
-        const double Sp = Sc * isp * su_scale, Spy = Sp * vy;
+        const double Sp = Sc * isp * (f32l ? su_scale : 1.0), Spy = Sp * vy;
         const double v = q == 0 ? Spy * zS : q == 1 ? Sp * fma(2.0 * Yd, z, zS) : 2.0 * Spy * z;
         const int64_t dst = q == 0 ? 0 : q == 1 ? 1 : q == 2 ? 3 : 2;
         atomicAdd(&G[dst * nlines + l], v);

@@ -280,6 +280,8 @@ hk_status hk_set_line_scales(hk_ctx *ctx, const double *s_scale, const double *g
  * the FP64 offset), region C through the FP64 Algorithm-916 series, and the
  * per-line sums are FP64 (accumulated with atomics: the last bits may vary
  * between runs).  Any of dT, dP, dlogS, dgammaL may be NULL.  Synchronous.
+ * Voigt and Lorentz profiles without plinth removal or sub-Lorentzian
+ * wings; HK_ERR_UNSUPPORTED otherwise.
  * No counterpart in the reference (it computes no derivatives). */
 hk_status hk_opacity_vjp(hk_ctx *ctx, double T, double P, int precision, const double *u,
                          int u_on_device, double *dT, double *dP, double *dlogS,
@@ -337,7 +339,7 @@ hk_status hk_profile_eval(hk_ctx *ctx, int64_t n, const double *x,
 
 /* Device time of the last hk_opacity / hk_kdist kernels (CUDA events on
  * the launching stream), in milliseconds; and the grid tile size.  After
- * hk_opacity_vjp, voigt_ms is the time of its two adjoint kernels. */
+ * hk_opacity_vjp, voigt_ms is the time of its adjoint kernels. */
 hk_status hk_last_timing(const hk_ctx *ctx, double *voigt_ms, double *kdist_ms);
 int hk_tile_points(void);
 

@@ -334,19 +334,21 @@ def partition_dlnq(Tq, q, T):
 
 
 def vjp_hitran(lines, mass, Tq, Qq, T, P, u, numin, dnu, nx, cut=25.0, qalphaL=1.0,
-               s_scale=None, g_scale=None):
+               s_scale=None, g_scale=None, profile=1):
     """FP64 reference gradient of a loss with seed u = dLoss/dK (one HITRAN
     isotopologue, cutMode 0): returns (dT, dP, dlogS per line, dgammaL per
     line), by the chain rule of the line scaling of prep_hitran applied to
     the per-line sums of vjp_sums.  Optional per-line multipliers of the
-    strength and of the Lorentz width, as the library's hk_set_line_scales."""
+    strength and of the Lorentz width, as the library's hk_set_line_scales.
+    profile 2 (Lorentz): windows without regions B and C, so every point
+    takes the region-A term, which is the Lorentzian."""
     Q = partition(Tq, Qq, T)
     nu, S, iad, vy = prep_hitran(lines, [mass], [1.0], [Q], T, P, qalphaL=qalphaL)
     if s_scale is not None:
         S = S * s_scale
     if g_scale is not None:
         vy = vy * g_scale
-    win = windows(nu, S, iad, vy, numin, dnu, nx, 0, cut)
+    win = windows(nu, S, iad, vy, numin, dnu, nx, 0, cut, profile=profile)
     gS, gy, gx, gn = vjp_sums(nu, S, iad, vy, win, numin, dnu, nx, u)
     c = _H * _C / _KB
     el = _f64(lines["EL"])

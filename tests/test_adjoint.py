@@ -92,6 +92,34 @@ def test_vjp_mixed_seed_range(adj, case):
         assert np.max(np.abs(dS[far] - rS[far])) < 1e-5 * m
 
 
+def test_vjp_lorentz_profile(adj):
+    """Profile 2 (Lorentz): windows hold region A only, whose term is the
+    Lorentzian; both forms against the oracle gradient with profile-2
+    windows, and the plain one against central differences."""
+    ctx = adj["ctx"]
+    ctx.set_profile(2, 0)
+    try:
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+        K = ctx.opacity([T0], [P0], hkb.PLAIN_FP64)[0]
+        u = adj["w"] / K
+        rT, rP, rS, rG = oracle.vjp_hitran(adj["L"], synth.MASS, adj["Tq"], adj["Qq"], T0, P0, u,
+                                           NUMIN, DNU, ctx.nx, profile=2)
+        for prec, tol, tol_line in ((hkb.PLAIN_FP64, 1e-9, 1e-9), (hkb.MIXED, 1e-4, 1e-5)):
+            dT, dP, dS, dG = ctx.opacity_vjp(T0, P0, u, prec)
+            eT, eP = abs(dT - rT) / abs(rT), abs(dP - rP) / abs(rP)
+            eS = np.max(np.abs(dS - rS)) / np.max(np.abs(rS))
+            eG = np.max(np.abs(dG - rG)) / np.max(np.abs(rG))
+            print(f"lorentz precision {prec}: dT {eT:.2e} dP {eP:.2e} dlogS {eS:.2e} dgammaL {eG:.2e}")
+            assert eT < tol and eP < tol
+            assert eS < tol_line and eG < tol_line
+        dT, fT, dP, fP = _fd_vs_vjp(ctx, adj["w"], 800.5, P0)
+        print(f"lorentz: dT {dT:.6g} fd {fT:.6g}; dP {dP:.6g} fd {fP:.6g}")
+        assert abs(fT - dT) < 1e-5 * abs(dT) and abs(fP - dP) < 1e-5 * abs(dP)
+    finally:
+        ctx.set_profile(1, 0)
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+
+
 def test_vjp_vs_central_differences(adj):
     ctx = adj["ctx"]
     rT, rP, rS, rG = reference(adj)
