@@ -106,3 +106,20 @@ def test_single_lines_at_special_places(case):
             assert np.all(K[Kref == 0.0] == 0.0)
             print(f"{case} precision {prec}: {err:.2e} over {n} points")
             assert err < tol
+
+
+def test_empty_line_list():
+    """No lines at all: K = kmin everywhere in both forms, the fit runs on it,
+    and the adjoint returns zero gradients."""
+    L = _lines([])
+    kmin = 1e-30
+    with _ctx(L) as ctx:
+        assert ctx.num_lines == 0
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, CUT, kmin)
+        for prec in (hkb.MIXED, hkb.PLAIN_FP64):
+            K = ctx.opacity([T, 300.0], [P, 1e-3], prec)
+            assert np.all(K == kmin)
+        r = ctx.kdist(K[:1], nC=20)
+        assert r["coeff"].shape == (1, NBINS, 20)
+        dT, dP, dS, dG = ctx.opacity_vjp(T, P, np.ones(ctx.nx), hkb.MIXED)
+        assert dT == 0.0 and dP == 0.0 and len(dS) == 0 and len(dG) == 0
