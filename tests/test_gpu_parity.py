@@ -47,8 +47,8 @@ def masked_relerr(K, Kref, nbins):
     Kr = Kref.reshape(nbins, -1)
     Kg = K.reshape(nbins, -1)
     mask = Kr > 1e-6 * Kr.max(axis=1, keepdims=True)
-    err = np.abs(Kg - Kr) / np.abs(Kr)
-    return float(err[mask].max()), int(mask.sum())
+    err = np.abs(Kg[mask] - Kr[mask]) / np.abs(Kr[mask])
+    return float(err.max()), int(mask.sum())
 
 
 def test_profile_fp64_and_fp32(small):
