@@ -78,17 +78,11 @@ __device__ __forceinline__ void ab_terms(bool regionB, F x, F y, double Sp, doub
   cy = Sp * (double)(t + F(2) * Y * tY);
 }
 
-// Regions A and B of the mixed form in FP32: t, dt/ds, dt/dY of the shape
-// with one reciprocal (gh2_grad divides three times).
-__device__ __forceinline__ void ab_grad_f(bool regionB, float s, float Y, float &t, float &ts,
-                                          float &tY) {
+// Region B of the mixed form in FP32: the GH2 shape t and dt/ds, dt/dY with
+// one reciprocal (gh2_grad divides three times).  Region A needs no helper:
+// t = 1/(s + Y), dt/ds = dt/dY = -t^2.
+__device__ __forceinline__ void gh2_grad_f(float s, float Y, float &t, float &ts, float &tY) {
   const float u = s + Y;
-  if (!regionB) {
-    t = rcp_fast(u);
-    ts = -t * t;
-    tY = ts;
-    return;
-  }
   const float a1 = u + 1.5f;
   const float c4 = (float)(4.0 / CUDART_PI), c6 = (float)(6.0 / CUDART_PI);
   const float num = fmaf(a1, u + 1.0f, -c4 * s);
@@ -213,7 +207,7 @@ __device__ __forceinline__ void ab_seg(const U *__restrict__ us, int k0, int k1,
     const float x = fmaf(kf, vbf, frf);
     if (REGION_B) {
       float t, ts, tY;
-      ab_grad_f(true, x * x, Y, t, ts, tY);
+      gh2_grad_f(x * x, Y, t, ts, tY);
       const A bsx = uk * (A)(ts * x);
       fS = fma(uk, (A)t, fS);
       fY = fma(uk, (A)tY, fY);
