@@ -10,17 +10,19 @@
 // A line contributes c_li = (S^/sqrt(pi)) V^(x_li, y_l) to K_i, with
 // S^ = S(T) / alphaD (LineState.S), x = (nu_i - nu_l) / alphaD,
 // y = gammaL / alphaD and V^ the region's shape (region C: Algorithm 916;
-// B: y/sqrt(pi) GH2; A: y/sqrt(pi) / (x^2 + y^2)).  Pass 1 (adjoint_tile_kernel)
-// recomputes the forward per (grid tile, line) -- nothing of the forward is
-// stored -- and reduces four sums per line:
+// B: y/sqrt(pi) GH2; A: y/sqrt(pi) / (x^2 + y^2); the Lorentz profile is
+// region A over the whole window).  Pass 1 recomputes the forward per (grid
+// tile, line) -- nothing of the forward is stored -- and reduces four sums
+// per line:
 //   G_S = sum_i u_i c_li,         G_y = sum_i u_i dc/dy,
 //   G_x = sum_i u_i dc/dx x_li,   G_n = sum_i u_i dc/dx,
 // so that dLoss/dlog S^ = G_S, dLoss/dy = G_y, dLoss/d(1/alphaD) at fixed y
 // = G_x alphaD and dLoss/dnu_l = -G_n / alphaD.  Pass 2 (adjoint_line_kernel)
 // applies the chain rule of the line scaling (prep_line) to T and P.
-// Mixed form: regions A and B in FP32 (x from the FP64 offset) in pass 1,
-// region C in FP64 (the differentiated Algorithm-916 series) in its own
-// per-line pass (adjoint_c_kernel) between the two; the sums are FP64.
+// Plain form: pass 1 is adjoint_tile_kernel, FP64 for all regions.  Mixed
+// form: pass 1 is adjoint_ab_kernel (regions A and B in FP32, x from the
+// FP64 offset), then adjoint_c_kernel takes region C in FP64 (the
+// differentiated Algorithm-916 series) before pass 2; the sums are FP64.
 #include <cuda_runtime.h>
 
 #include <algorithm>
