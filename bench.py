@@ -169,18 +169,65 @@ def c_series_iterations(ctx, T, P, sample=1000, seed=0):
 
 
 class Clocks:
-    """nvidia-smi sampler running during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region:
+    NVML read every 10 ms from a thread (read-only queries), else
+    nvidia-smi at 200 ms.  The NVML device is the CUDA device's (matched by
+    UUID, else by index)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, device):
         self.device = device
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.p = None
+        self.f = None
+        self.thread = None
+        self.nv = None
+        self.handle = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.handle = self._nvml_handle(device)
+        except Exception:
+            self.nv = None
+
+    def _nvml_handle(self, device):
+        nv = self.nv
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(device).uuid)
+            return nv.nvmlDeviceGetHandleByUUID("GPU-" + uuid)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(device)
+
+    def _poll(self):
+        nv, h = self.nv, self.handle
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append(float(sm))
+                for k, b in enumerate(bits):
+                    if r & b:
+                        self.reasons.add(self.NAMES[k])
+            except Exception:
+                pass
+            self.stop_flag.wait(0.01)
 
     def start(self):
+        if self.nv is not None:
+            import threading
+            self.samples, self.reasons = [], set()
+            self.stop_flag = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
@@ -189,7 +236,21 @@ class Clocks:
             self.p = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join()
+            self.thread = None
+            smax = None
+            try:
+                smax = float(self.nv.nvmlDeviceGetMaxClockInfo(self.handle, self.nv.NVML_CLOCK_SM))
+            except Exception:
+                pass
+            sm = self.samples
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                    "reasons": sorted(self.reasons), "samples": len(sm), "source": "nvml 10 ms"}
         if self.p is None:
+            if self.f is not None:
+                os.unlink(self.f.name)
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
         self.p.wait()
@@ -198,18 +259,17 @@ class Clocks:
         rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
         os.unlink(self.f.name)
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             try:
                 sm.append(float(r[1]))
                 smax = float(r[2])
-                for k, nm in enumerate(names):
+                for k, nm in enumerate(self.NAMES):
                     if r[5 + k].strip() == "Active":
                         reasons.add(nm)
             except (ValueError, IndexError):
                 pass
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi 200 ms"}
 
 
 def dist_setup(args=None):
