@@ -352,18 +352,22 @@ def run_reference(args):
     W = workload(args.workload)
     L = make_lines(W)
     T, P = W["T"][0], W["P"][0]
-    per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
-    vals = []
+    # each step a bounded sample: the whole run stays near a minute
+    per_step = max(0.5, min(args.cpu_seconds, 60.0 / max(1, args.steps + args.warmup)))
+    vals, secs = [], []
     cb = None
     for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         cb = cpu_baseline(W, L, T, P, per_step, seed=k)
         if k >= args.warmup:
             vals.append(cb["value"])
+            secs.append(time.perf_counter() - t0)
     v = float(np.mean(vals))
     cb["value"] = v
     out = {"impl": "reference", "metric": "Voigt evals/s", "value": v, "unit": "Voigt evals/s",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "ms_per_step": 1e3 * float(np.mean(secs)), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None,
            "dtype": "f64", "data": "synthetic (seeded; BASELINE config distributions)",
            "config": {"workload": W["label"], "lines": W["n"], "states": 1, "T": T, "P": P,
                       "cut": W["cut"], "sample": "bounded grid-tile sample per step"},
