@@ -10,8 +10,9 @@
 // A line contributes c_li = (S^/sqrt(pi)) V^(x_li, y_l) to K_i, with
 // S^ = S(T) / alphaD (LineState.S), x = (nu_i - nu_l) / alphaD,
 // y = gammaL / alphaD and V^ the region's shape (region C: Algorithm 916;
-// B: y/sqrt(pi) GH2; A: y/sqrt(pi) / (x^2 + y^2); the Lorentz profile is
-// region A over the whole window).  Pass 1 recomputes the forward per (grid
+// B: y/sqrt(pi) GH2; A: y/sqrt(pi) / (x^2 + y^2); profiles 2-4 are their
+// region-A shape over the whole window: Lorentz, Doppler, binned Gaussian,
+// the last two in the FP64 form whatever the precision asked for).  Pass 1 recomputes the forward per (grid
 // tile, line) -- nothing of the forward is stored -- and reduces four sums
 // per line:
 //   G_S = sum_i u_i c_li,         G_y = sum_i u_i dc/dy,
@@ -80,6 +81,31 @@ __device__ __forceinline__ void ab_terms(bool regionB, F x, F y, double Sp, doub
   cy = Sp * (double)(t + F(2) * Y * tY);
 }
 
+// Profiles 3-4 (region A only, FP64): the shape with its S1 and dc/dx,
+// dc/dvb (vb = dnu iad, the grid step in Doppler units).  Doppler: S1
+// e^{-x^2}.  Binned Gaussian: S1 (erf(x+h) - erf(x-h)) / (2 vb), h = vb/2; its
+// two exponentials come from the larger one, e^{-(|x|-h)^2}, so neither their
+// difference nor their sum cancels or overflows.
+__device__ __forceinline__ void profile34_grad_d(int profile, double x, double S1, double vb,
+                                                 double &c, double &cx, double &cvb) {
+  if (profile == 3) {
+    c = S1 * exp(-(x * x));
+    cx = -2.0 * x * c;
+    cvb = 0.0;
+    return;
+  }
+  const double isp = 0.56418958354775628695;  // 1/sqrt(pi)
+  const double h = 0.5 * vb, ax = fabs(x), sx = x < 0.0 ? -1.0 : 1.0;
+  const double D = erf_diff(x + h, x - h);
+  const double Eb = exp(-(ax - h) * (ax - h));
+  const double dE = sx * Eb * expm1(-4.0 * ax * h);    // e^{-(x+h)^2} - e^{-(x-h)^2}
+  const double sE = Eb * (1.0 + exp(-4.0 * ax * h));   // e^{-(x+h)^2} + e^{-(x-h)^2}
+  const double k = S1 / (2.0 * vb);
+  c = k * D;
+  cx = k * (2.0 * isp) * dE;
+  cvb = k * (sE * isp - D / vb);
+}
+
 // Region B of the mixed form in FP32: the GH2 shape t and dt/ds, dt/dY with
 // one reciprocal (gh2_grad divides three times).  Region A needs no helper:
 // t = 1/(s + Y), dt/ds = dt/dY = -t^2.
@@ -140,9 +166,19 @@ adjoint_tile_kernel(const LinePrep *__restrict__ P, const double *__restrict__ n
       if (lo >= hi || lp.Sc == 0.0) continue;
       const double Sp = lp.Sc * isp;  // S^/pi
       double gS = 0.0, gy = 0.0, gx = 0.0, gn = 0.0;
+      const double vbl = g.dnu * lp.iad;
       for (int64_t k = lo + lane; k < hi; k += 32) {
         const double uk = su[k - g0];
         const double xd = __dmul_rn(__dsub_rn(grid_x(g, k), lp.nu), lp.iad);
+        if (g.profile >= 3) {
+          // no y dependence; the shape depends on iad through x and vb
+          double c, cx, cvb;
+          profile34_grad_d(g.profile, xd, lp.S1, vbl, c, cx, cvb);
+          gS = fma(uk, c, gS);
+          gx = fma(uk, fma(cx, xd, cvb * vbl), gx);
+          gn = fma(uk, cx, gn);
+          continue;
+        }
         double c, cx, cy;
         if (k >= lp.c0 && k < lp.c1) {
           const VDer d = voigt916_dd(xd, lp.vy, lp.ey);
@@ -534,6 +570,7 @@ cudaError_t launch_opacity_vjp(bool mixed, const LinesDev &L, const GridDev &g,
                                const LinePrep *prep_d, const double *u_d, unsigned *ticket_d,
                                double *G_d, const int64_t *order_d, double *dlogS_d,
                                double *dgam_d, double *dTP_d, cudaStream_t stream) {
+  mixed = mixed && g.profile <= 2;  // Doppler and binned Gaussian: the FP64 form
   cudaError_t e = cudaMemsetAsync(G_d, 0, 4 * sizeof(double) * (size_t)L.n, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(dTP_d, 0, 2 * sizeof(double), stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(ticket_d, 0, sizeof(unsigned), stream);

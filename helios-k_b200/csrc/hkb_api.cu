@@ -1047,10 +1047,9 @@ hk_status hk_opacity_vjp(hk_ctx *c, double T, double P, int precision, const dou
   if (!u) return fail(c, HK_ERR_ARG, "need the seed u (Nx values)");
   if (precision != HK_PRECISION_PLAIN_FP64 && precision != HK_PRECISION_MIXED)
     return fail(c, HK_ERR_ARG, "precision must be 0 (plain FP64) or 1 (mixed)");
-  if (c->g.profile > 2 || c->g.plinth || c->g.subL)
+  if (c->g.plinth || c->g.subL)
     return fail(c, HK_ERR_UNSUPPORTED,
-                "the adjoint is for the Voigt and Lorentz profiles without plinth removal or "
-                "sub-Lorentzian wings");
+                "the adjoint is for the line profiles without plinth removal or sub-Lorentzian wings");
   cudaSetDevice(c->device);
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<StateDev> hs;

@@ -280,8 +280,9 @@ hk_status hk_set_line_scales(hk_ctx *ctx, const double *s_scale, const double *g
  * the FP64 offset), region C through the FP64 Algorithm-916 series, and the
  * per-line sums are FP64 (accumulated with atomics: the last bits may vary
  * between runs).  Any of dT, dP, dlogS, dgammaL may be NULL.  Synchronous.
- * Voigt and Lorentz profiles without plinth removal or sub-Lorentzian
- * wings; HK_ERR_UNSUPPORTED otherwise.
+ * The four line profiles (Doppler and binned Gaussian in FP64 in either
+ * precision) without plinth removal or sub-Lorentzian wings;
+ * HK_ERR_UNSUPPORTED with either option.
  * No counterpart in the reference (it computes no derivatives). */
 hk_status hk_opacity_vjp(hk_ctx *ctx, double T, double P, int precision, const double *u,
                          int u_on_device, double *dT, double *dP, double *dlogS,

@@ -871,9 +871,34 @@ static void gh2_grad(double s, double Y, double *t, double *ts, double *tY) {
  * regions), G[l] = sum_i u_i c_li, G[n+l] = sum_i u_i dc/dy,
  * G[2n+l] = sum_i u_i dc/dx x_li, G[3n+l] = sum_i u_i dc/dx, i over the line's
  * window inside [0, nx).  OpenMP over lines. */
+/* profiles 3-4 (region A only): the shape c with its S1 and dc/dx, dc/dvb
+ * (vb = dnu iad, the grid step in Doppler units): Doppler S/sqrt(pi)
+ * e^{-x^2}; binned Gaussian S (erf(x+h) - erf(x-h)) / (2 vb), h = vb/2, whose
+ * exponentials are taken from the larger one, e^{-(|x|-h)^2}, so neither the
+ * difference nor the sum cancels or overflows. */
+static void profile34_grad(int profile, double x, double S, double vb, double *c, double *cx,
+                           double *cvb) {
+  if (profile == 3) {
+    const double v = S / sqrt(M_PI) * exp(-(x * x));
+    *c = v;
+    *cx = -2.0 * x * v;
+    *cvb = 0.0;
+    return;
+  }
+  const double h = 0.5 * vb, ax = fabs(x), sx = x < 0.0 ? -1.0 : 1.0;
+  const double D = erf_diff(x + h, x - h);
+  const double Eb = exp(-(ax - h) * (ax - h));
+  const double dE = sx * Eb * expm1(-4.0 * ax * h); /* e^{-(x+h)^2} - e^{-(x-h)^2} */
+  const double sE = Eb * (1.0 + exp(-4.0 * ax * h)); /* e^{-(x+h)^2} + e^{-(x-h)^2} */
+  const double k = S / (2.0 * vb);
+  *c = k * D;
+  *cx = k * (2.0 / sqrt(M_PI)) * dE;
+  *cvb = k * (sE / sqrt(M_PI) - D / vb);
+}
+
 void hko_vjp_sums(int64_t n, const double *nu, const double *S, const double *iad,
                   const double *vy, const int64_t *win, double numin, double dnu, int64_t nx,
-                  const double *u, double *G, int nthreads) {
+                  const double *u, double *G, int profile, int nthreads) {
   const double isp = 1.0 / sqrt(M_PI);
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -890,6 +915,16 @@ void hko_vjp_sums(int64_t n, const double *nu, const double *S, const double *ia
     for (int64_t i = a0; i < a1 && Sl != 0.0; ++i) {
       const double x = (hko_grid_x(numin, dnu, i) - nu[l]) * iad[l];
       double c, cx, cy;
+      if (profile >= 3) {
+        /* the shape depends on iad through x and vb: G_x takes both */
+        double cvb;
+        const double vb = dnu * iad[l];
+        profile34_grad(profile, x, Sl, vb, &c, &cx, &cvb);
+        gS += u[i] * c;
+        gx += u[i] * (cx * x + cvb * vb);
+        gn += u[i] * cx;
+        continue;
+      }
       if (i >= o[2] && i < o[3]) {
         double v, vx, vyy;
         voigt916_grad(x, y, ey, &v, &vx, &vyy);

@@ -103,7 +103,7 @@ void hko_opacity(int64_t n, const double *nu, const double *S,
  * oracle of the adjoint */
 void hko_vjp_sums(int64_t n, const double *nu, const double *S, const double *iad,
                   const double *vy, const int64_t *win, double numin, double dnu, int64_t nx,
-                  const double *u, double *G, int nthreads);
+                  const double *u, double *G, int profile, int nthreads);
 
 /* k-distribution fit, resample.h */
 void hko_vandermonde(int nxb, int nc, double *V);

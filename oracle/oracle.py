@@ -59,7 +59,7 @@ def lib():
         L.hko_gh2.argtypes = [_d, _d]
         L.hko_opacity.argtypes = [_i64, _p, _p, _p, _p, _p, _d, _d, _i64, _i64,
                                   _d, _p, _i, _p]
-        L.hko_vjp_sums.argtypes = [_i64, _p, _p, _p, _p, _p, _d, _d, _i64, _p, _p, _i]
+        L.hko_vjp_sums.argtypes = [_i64, _p, _p, _p, _p, _p, _d, _d, _i64, _p, _p, _i, _i]
         L.hko_vandermonde.argtypes = [_i, _i, _p]
         L.hko_qr.argtypes = [_i, _i, _p, _p, _p]
         L.hko_sort_bins.argtypes = [_i64, _p, _i, _p]
@@ -308,15 +308,17 @@ def state_opacity(lines, iso_mass, iso_ab, iso_Q, T, P, numin, numax, dnu,
 _H, _C, _KB, _T0 = 6.62606957e-27, 2.99792458e10, 1.3806489e-16, 296.0
 
 
-def vjp_sums(nu, S, iad, vy, win, numin, dnu, nx, u, nthreads=0):
+def vjp_sums(nu, S, iad, vy, win, numin, dnu, nx, u, nthreads=0, profile=1):
     """hko_vjp_sums: (4, n) per-line sums of the vector-Jacobian product of
-    K (G_S, G_y, G_x, G_n), FP64."""
+    K (G_S, G_y, G_x, G_n), FP64.  Profiles 3-4 have no y dependence
+    (G_y = 0) and their G_x includes the dependence on iad through the grid
+    step vb = dnu iad (binned Gaussian)."""
     n = len(nu)
     nu, S, iad, vy, u = map(_f64, (nu, S, iad, vy, u))
     win = np.ascontiguousarray(win, dtype=np.int64)
     G = np.zeros(4 * n, np.float64)
     lib().hko_vjp_sums(n, _ptr(nu), _ptr(S), _ptr(iad), _ptr(vy), _ptr(win), numin, dnu, nx,
-                       _ptr(u), _ptr(G), nthreads)
+                       _ptr(u), _ptr(G), int(profile), nthreads)
     return G.reshape(4, n)
 
 
@@ -340,8 +342,8 @@ def vjp_hitran(lines, mass, Tq, Qq, T, P, u, numin, dnu, nx, cut=25.0, qalphaL=1
     line), by the chain rule of the line scaling of prep_hitran applied to
     the per-line sums of vjp_sums.  Optional per-line multipliers of the
     strength and of the Lorentz width, as the library's hk_set_line_scales.
-    profile 2 (Lorentz): windows without regions B and C, so every point
-    takes the region-A term, which is the Lorentzian."""
+    profiles 2-4: windows without regions B and C; every point takes the
+    profile's region-A term (Lorentz, Doppler, binned Gaussian)."""
     Q = partition(Tq, Qq, T)
     nu, S, iad, vy = prep_hitran(lines, [mass], [1.0], [Q], T, P, qalphaL=qalphaL)
     if s_scale is not None:
@@ -349,7 +351,7 @@ def vjp_hitran(lines, mass, Tq, Qq, T, P, u, numin, dnu, nx, cut=25.0, qalphaL=1
     if g_scale is not None:
         vy = vy * g_scale
     win = windows(nu, S, iad, vy, numin, dnu, nx, 0, cut, profile=profile)
-    gS, gy, gx, gn = vjp_sums(nu, S, iad, vy, win, numin, dnu, nx, u)
+    gS, gy, gx, gn = vjp_sums(nu, S, iad, vy, win, numin, dnu, nx, u, profile=profile)
     c = _H * _C / _KB
     el = _f64(lines["EL"])
     delta = _f64(lines["delta"])

@@ -92,29 +92,44 @@ def test_vjp_mixed_seed_range(adj, case):
         assert np.max(np.abs(dS[far] - rS[far])) < 1e-5 * m
 
 
-def test_vjp_lorentz_profile(adj):
-    """Profile 2 (Lorentz): windows hold region A only, whose term is the
-    Lorentzian; both forms against the oracle gradient with profile-2
-    windows, and the plain one against central differences."""
+@pytest.mark.parametrize("profile", [2, 3, 4])
+def test_vjp_profiles_2_to_4(adj, profile):
+    """Profiles 2-4: windows hold region A only, whose term is the profile's
+    shape (Lorentz; Doppler and binned Gaussian in the FP64 form in both
+    precisions, without y dependence and, for the binned Gaussian, with the
+    grid step vb = dnu iad in the iad derivative).  Both precisions against
+    the oracle gradient with the profile's windows, the plain one against
+    central differences.  The Doppler and binned-Gaussian cores leave most
+    grid points empty, so K carries a floor kmin (constant in every
+    parameter) there."""
     ctx = adj["ctx"]
-    ctx.set_profile(2, 0)
+    ctx.set_profile(profile, 0)
     try:
         ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+        kmin = 1e-12 * ctx.opacity([T0], [P0], hkb.PLAIN_FP64)[0].max()
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0, kmin)
         K = ctx.opacity([T0], [P0], hkb.PLAIN_FP64)[0]
         u = adj["w"] / K
         rT, rP, rS, rG = oracle.vjp_hitran(adj["L"], synth.MASS, adj["Tq"], adj["Qq"], T0, P0, u,
-                                           NUMIN, DNU, ctx.nx, profile=2)
+                                           NUMIN, DNU, ctx.nx, profile=profile)
         for prec, tol, tol_line in ((hkb.PLAIN_FP64, 1e-9, 1e-9), (hkb.MIXED, 1e-4, 1e-5)):
             dT, dP, dS, dG = ctx.opacity_vjp(T0, P0, u, prec)
-            eT, eP = abs(dT - rT) / abs(rT), abs(dP - rP) / abs(rP)
+            eT = abs(dT - rT) / abs(rT)
+            eP = abs(dP - rP) / abs(rP) if rP != 0.0 else abs(dP)
             eS = np.max(np.abs(dS - rS)) / np.max(np.abs(rS))
-            eG = np.max(np.abs(dG - rG)) / np.max(np.abs(rG))
-            print(f"lorentz precision {prec}: dT {eT:.2e} dP {eP:.2e} dlogS {eS:.2e} dgammaL {eG:.2e}")
+            if profile == 2:
+                eG = np.max(np.abs(dG - rG)) / np.max(np.abs(rG))
+            else:
+                assert np.all(rG == 0.0)
+                eG = float(np.max(np.abs(dG)))
+            print(f"profile {profile} precision {prec}: dT {eT:.2e} dP {eP:.2e} dlogS {eS:.2e} "
+                  f"dgammaL {eG:.2e}")
             assert eT < tol and eP < tol
             assert eS < tol_line and eG < tol_line
         dT, fT, dP, fP = _fd_vs_vjp(ctx, adj["w"], 800.5, P0)
-        print(f"lorentz: dT {dT:.6g} fd {fT:.6g}; dP {dP:.6g} fd {fP:.6g}")
-        assert abs(fT - dT) < 1e-5 * abs(dT) and abs(fP - dP) < 1e-5 * abs(dP)
+        print(f"profile {profile}: dT {dT:.6g} fd {fT:.6g}; dP {dP:.6g} fd {fP:.6g}")
+        assert abs(fT - dT) < 1e-5 * abs(dT)
+        assert abs(fP - dP) <= 1e-5 * abs(dP)
     finally:
         ctx.set_profile(1, 0)
         ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
