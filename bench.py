@@ -1,19 +1,26 @@
 #!/usr/bin/env python
 """Benchmark of the HELIOS-K opacity hot path on B200.
 
-One step = one pass of the path over one batch: the Voigt line sum of every
-state onto the grid (hk_opacity, persistent kernel) followed by the per-bin
-sort + Chebyshev k-distribution fit (hk_kdist).  Inputs are resident in HBM
-(line list >> L2, so no L2 flush is needed between steps).
+One step = one pass of the path over one batch: the line scaling and Voigt
+line sum of every state onto the grid followed by the per-bin sort +
+Chebyshev k-distribution fit, replayed as one CUDA graph (hk_table_run).
+Inputs are resident in HBM (line list >> L2, so no L2 flush is needed
+between steps).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload hitemp|small|table] [--precision mixed|plain]
+                  [--workload hitemp|small|table|...] [--precision mixed|plain]
 
 Metric: Voigt evaluations per second (algorithmic (line, grid point) pairs
 inside the cutoff windows, counted exactly from the index windows), plus the
-seconds per state/table.  Multi-GPU: every rank computes its own copy of the
-workload's states (states are independent; no collective on the data path),
-time = max over ranks, value = pairs of all ranks / that time.
+seconds per state and per T-P table.  The default run (hitemp: one state of
+a 1e7-line list) adds a table leg: the 600-state T-P table of the same list
+as one graph replay (s_per_table), its plain-FP64 subset, its error against
+the FP64 oracle and the reference's own CUDA build on one temperature row.
+
+Multi-GPU (one process per GPU): every rank computes its own copy of the
+single-state workload (weak scaling; time = max over ranks, value = pairs of
+all ranks / that time); the table leg splits the table's states across the
+ranks (rank r takes states r, r + N, ...; no collective on the data path).
 """
 import argparse
 import json
@@ -56,6 +63,10 @@ def parse():
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference's own CUDA build beside ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-table", action="store_true",
+                    help="skip the T-P table leg of the default (hitemp) run")
+    ap.add_argument("--table-steps", type=int, default=1,
+                    help="timed replays of the 600-state table (each ~17 s), after 1 untimed")
     ap.add_argument("--tuning", type=int, default=2, choices=[0, 1, 2],
                     help="tile-shape tuner: 0 fixed default shape, 1 when it pays, 2 once "
                          "before the timed steps")
@@ -303,49 +314,138 @@ def barrier_max(ws, value):
     return float(t.item())
 
 
-def cpu_baseline(W, L, T, P, seconds, tile=2048, seed=0):
-    """The FP64 oracle (OpenMP, all host threads) on a bounded sample of grid
-    tiles of the same workload; returns pairs/s and what was sampled."""
+def rank_states(n, ws, rank):
+    """The states of a table that rank `rank` of `ws` computes: r, r + ws,
+    ... (disjoint; every state exactly once over the ranks; counts differ by
+    at most one)."""
+    return np.arange(rank, n, ws)
+
+
+def workload_config(W):
+    """The workload part of the JSON line: the same dict in both arms."""
+    ns = len(W["T"])
+    return {"workload": W["label"], "lines": W["n"],
+            "grid_points": int(round((W["numax"] - W["numin"]) / W["dnu"])),
+            "states": ns,
+            "T": W["T"][0] if ns == 1 else f"{min(W['T']):g}-{max(W['T']):g} K x {len(set(W['T']))}",
+            "P": W["P"][0] if ns == 1 else f"{min(W['P']):.3g}-{max(W['P']):.3g} atm x {len(set(W['P']))}",
+            "cut_cm-1": W["cut"], "nbins": W["nbins"], "nC": W["nC"],
+            "format": W.get("database", "hitran"),
+            "l2": f"inputs larger than L2 (line columns ~{W['n'] * 48 / 1e9:.2g} GB resident), no flush"}
+
+
+TILE = 2048  # points per sampled grid tile (oracle samples and parity)
+
+
+def tile_order(nx, seed):
+    """Seeded order in which the oracle samples grid tiles."""
+    return [int(t) for t in np.random.default_rng(seed).permutation((nx + TILE - 1) // TILE)]
+
+
+def oracle_state(W, L, T, P):
+    """FP64 oracle line state and windows of one state (prep + index rule)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from hkb import synth
     Tq, Qq = synth.q_table()
     Q = oracle.partition(Tq, Qq, T)
-    head = ""
-    if W["n"] > 20_000_000:
-        # per-line oracle arrays of a 5e8-line list do not fit the host: the
-        # rate is measured on a 2e7-line head of the list (same distributions)
-        L = {k: v[:20_000_000] for k, v in L.items()}
-        head = ", 2e7-line head of the list"
     if W.get("database") == "exomol":
         nu, S, iad, vy = oracle.prep_exomol(L, synth.MASS, 1.0, Q, W["defaultL"], W["defaultn"], T, P)
     else:
         nu, S, iad, vy = oracle.prep_hitran(L, [synth.MASS], [1.0], [Q], T, P, qalphaL=1.0)
     nx = oracle.grid_nx(W["numin"], W["numax"], W["dnu"])
     win = oracle.windows(nu, S, iad, vy, W["numin"], W["dnu"], nx, 0, W["cut"])
-    rng = np.random.default_rng(seed)
-    ntiles = (nx + tile - 1) // tile
-    order = rng.permutation(ntiles)
-    pairs, tsum, used = 0, 0.0, 0
+    return nu, S, iad, vy, win, nx
+
+
+def barrier_sum(ws, value):
+    """sum over ranks of a per-rank count (outside the timed regions)."""
+    if ws == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cpu_baseline(W, L, T, P, seconds, seed=0, max_tiles=None):
+    """The FP64 oracle (OpenMP, all host threads) on a bounded sample of grid
+    tiles of the same workload.  Returns (summary, {tile: oracle K}): pairs/s,
+    what was sampled, and the state's total pairs with the full step time
+    they extrapolate to at that rate."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    head = ""
+    if W["n"] > 20_000_000:
+        # per-line oracle arrays of a 5e8-line list do not fit the host: the
+        # rate is measured on a 2e7-line head of the list (same distributions)
+        L = {k: v[:20_000_000] for k, v in L.items()}
+        head = ", 2e7-line head of the list"
+    nu, S, iad, vy, win, nx = oracle_state(W, L, T, P)
+    total = int(np.sum(win[:, 5] - win[:, 0]))
+    order = tile_order(nx, seed)
+    pairs, tsum, used, Ktiles = 0, 0.0, 0, {}
     for t in order:
-        ib, ie = int(t * tile), int(min(nx, (t + 1) * tile))
+        ib, ie = int(t * TILE), int(min(nx, (t + 1) * TILE))
         t0 = time.perf_counter()
-        _, pr = oracle.opacity(nu, S, iad, vy, win, W["numin"], W["dnu"], nx, irange=(ib, ie))
+        Kt, pr = oracle.opacity(nu, S, iad, vy, win, W["numin"], W["dnu"], nx, irange=(ib, ie))
         tsum += time.perf_counter() - t0
         pairs += sum(pr)
+        Ktiles[t] = Kt
         used += 1
-        if tsum >= seconds:
+        if tsum >= seconds or (max_tiles and used >= max_tiles):
             break
     cores = os.cpu_count() or 1
-    return {"value": pairs / tsum, "unit": "Voigt evals/s", "cores": cores, "kind": "port",
-            "sample": f"{used} random {tile}-point grid tiles of {ntiles} "
-                      f"({pairs:.3e} pairs, {tsum:.1f} s){head}, FP64 oracle, OpenMP {cores} threads"}
+    rate = pairs / tsum
+    return ({"value": rate, "unit": "Voigt evals/s", "cores": cores, "kind": "port",
+             "sample": f"{used} random {TILE}-point grid tiles of {len(order)} "
+                       f"({pairs:.3e} pairs, {tsum:.1f} s){head}, FP64 oracle, OpenMP {cores} threads",
+             "state_pairs": total, "state_s_extrapolated": total / rate},
+            Ktiles)
+
+
+def parity_figure(Kg_tiles, binmax_tiles, Ko_tiles, tol=1e-5):
+    """Max relative error of the GPU's K against the oracle's on sampled
+    tiles, where K > 1e-6 of its bin maximum (the bin maximum of the GPU's K:
+    the oracle sums only the sampled tiles)."""
+    worst, pts, used = 0.0, 0, 0
+    for t, Ko in Ko_tiles.items():
+        if t not in Kg_tiles:
+            continue
+        Kg, bm = Kg_tiles[t], binmax_tiles[t]
+        m = Kg > 1e-6 * bm
+        if m.any():
+            worst = max(worst, float(np.max(np.abs(Kg[m] - Ko[m]) / np.abs(Ko[m]))))
+        pts += int(m.sum())
+        used += 1
+    return {"max_rel_err": worst, "points": pts, "tiles": used, "tolerance": tol,
+            "pass": bool(worst < tol), "oracle": "FP64 CPU restatement",
+            "mask": "K > 1e-6 of its bin maximum"}
+
+
+def gpu_tiles(Krow, tiles, nxb):
+    """{tile: (K of the tile, per-point bin maximum)} from one state's K row
+    (a torch tensor on the device)."""
+    import torch
+    nx = Krow.shape[0]
+    bmax = Krow[: (nx // nxb) * nxb].view(-1, nxb).max(dim=1).values
+    out_k, out_b = {}, {}
+    for t in tiles:
+        ib, ie = t * TILE, min(nx, (t + 1) * TILE)
+        out_k[t] = Krow[ib:ie].double().cpu().numpy()
+        bins = torch.arange(ib, ie, device=Krow.device) // nxb
+        out_b[t] = bmax[bins].cpu().numpy()
+    return out_k, out_b
 
 
 def run_reference(args):
     """--impl reference: the reference has no CPU path of its own, so the
     reference arm is the FP64 CPU restatement (oracle) on the box's host
-    cores, each step a bounded sample of the same workload."""
+    cores, each step a bounded sample of the same workload.  ms_per_step is
+    the time of one whole step at the measured rate (the state's pairs /
+    pairs per second); sample_s is the wall time of the sample itself."""
     ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
         return
@@ -354,23 +454,24 @@ def run_reference(args):
     T, P = W["T"][0], W["P"][0]
     # each step a bounded sample: the whole run stays near a minute
     per_step = max(0.5, min(args.cpu_seconds, 60.0 / max(1, args.steps + args.warmup)))
-    vals, secs = [], []
-    cb = None
+    vals, secs, cb = [], [], None
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        cb = cpu_baseline(W, L, T, P, per_step, seed=k)
+        cb, _ = cpu_baseline(W, L, T, P, per_step, seed=k)
         if k >= args.warmup:
             vals.append(cb["value"])
             secs.append(time.perf_counter() - t0)
     v = float(np.mean(vals))
     cb["value"] = v
+    cb["state_s_extrapolated"] = cb["state_pairs"] / v
     out = {"impl": "reference", "metric": "Voigt evals/s", "value": v, "unit": "Voigt evals/s",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": 1e3 * float(np.mean(secs)), "higher_is_better": True, "scaling": "weak",
+           "ms_per_step": 1e3 * cb["state_pairs"] / v, "ms_per_step_kind":
+               "extrapolated: the state's pairs / the sampled pairs per second",
+           "sample_s": float(np.mean(secs)), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None,
            "dtype": "f64", "data": "synthetic (seeded; BASELINE config distributions)",
-           "config": {"workload": W["label"], "lines": W["n"], "states": 1, "T": T, "P": P,
-                      "cut": W["cut"], "sample": "bounded grid-tile sample per step"},
+           "config": workload_config(W),
            "cpu_baseline": cb,
            "e2e": {"value": v, "unit": "Voigt evals/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
@@ -472,6 +573,143 @@ def reference_cuda(W, L, T, P, tunings=(1, 0)):
     return out
 
 
+def flop_model(pa, pb, pc, n_iter):
+    """Algorithmic FP32 flops of one state from its pairs by region."""
+    return pa * (F_A + F_ACC) + pb * (F_B + F_ACC) + pc * (F_C0 + F_C_ITER * n_iter + F_ACC)
+
+
+def n_iter_of(ctx, W, L, T, P, lrank):
+    """n_iter of the flop model, from the lines themselves or, for lists too
+    large to download per line, from a 2e6-line head of the same list."""
+    if ctx.num_lines <= 20_000_000:
+        return c_series_iterations(ctx, float(T), float(P))
+    Wp = dict(W, n=2_000_000)
+    Lp = {k: v[:2_000_000] for k, v in L.items()}
+    pctx = open_ctx(Wp, Lp, lrank)
+    pctx._numin, pctx._dnu = W["numin"], W["dnu"]
+    n = c_series_iterations(pctx, float(T), float(P))
+    pctx.close()
+    return n
+
+
+def table_leg(ctx, W, L, args, ws, rank, lrank, stream, fp32_peak):
+    """The 600-state T-P table of the same line list (20 T x 30 P): the line
+    scaling, Voigt sums and k-distribution fits of every state recorded as
+    one CUDA graph (hk_table_build) and replayed (hk_table_run), 1 untimed +
+    args.table_steps timed replays.  N ranks split the states (rank r takes
+    r, r + N, ...).  Adds the plain-FP64 form on 20 states spread over the
+    table, the error against the FP64 oracle on sampled tiles of two states,
+    and (rank 0, 1 GPU) the reference's own CUDA build on one temperature
+    row of 30 pressures."""
+    import torch
+    import hkb
+    from hkb import synth
+    Ta, Pa = synth.table_states()
+    mine = rank_states(len(Ta), ws, rank)
+    T, P = Ta[mine], Pa[mine]
+    ns, nx, nb, nC = len(T), ctx.nx, W["nbins"], W["nC"]
+    K = torch.empty((ns, nx), dtype=torch.float64, device="cuda")
+    coeff = torch.empty((ns, nb, nC), dtype=torch.float64, device="cuda")
+    nxmin = torch.empty((ns, nb), dtype=torch.int32, device="cuda")
+    t0 = time.perf_counter()
+    ctx.table_build(T, P, K, coeff, nxmin, nC=nC, precision=hkb.MIXED)
+    build_s = time.perf_counter() - t0
+    kernels = ctx.table_kernels
+    shape_used, shape_tuned, probe_ms = ctx.tuning_result()
+    ctx.table_run(stream)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    clk = Clocks(lrank)
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.table_steps):
+        ctx.table_run(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    s_table = barrier_max(ws, e0.elapsed_time(e1) / args.table_steps * 1e-3)
+    ctx.table_free()
+    # the timed output of two states on the tiles the oracle samples (before
+    # the plain-form leg below overwrites the first rows of K)
+    par_states = sorted({0, ns // 2})
+    par_tiles = {s: tile_order(nx, 100 + s)[:1] for s in par_states}
+    par_gpu = {s: gpu_tiles(K[s], par_tiles[s], nx // nb) for s in par_states}
+    # exact pairs of every state (outside the timed region)
+    pairs = np.array([ctx.count_pairs(float(T[s]), float(P[s])) for s in range(ns)], np.float64)
+    pairs_all = barrier_sum(ws, float(pairs.sum()))
+    # flop model: n_iter from four states spread over the table
+    probe = np.linspace(0, ns - 1, min(ns, 4)).astype(int)
+    n_iter = float(np.mean([n_iter_of(ctx, W, L, T[s], P[s], lrank) if pairs[s, 2] > 0 else 0.0
+                            for s in probe]))
+    flops = barrier_sum(ws, float(sum(flop_model(*pairs[s], n_iter) for s in range(ns))))
+    out = {"workload": "tp-table-1e7-lines-600-states", "states": int(len(Ta)),
+           "states_this_rank": int(ns), "T": f"{Ta.min():g}-{Ta.max():g} K x 20",
+           "P": f"{Pa.min():.3g}-{Pa.max():.3g} atm x 30 (log)",
+           "s_per_table": s_table, "replays_timed": args.table_steps,
+           "value": pairs_all / s_table, "unit": "Voigt evals/s",
+           "pairs": pairs_all, "build_s": build_s, "graph_kernels": kernels,
+           "tile_shape": {"shape": shape_used, "tuned": shape_tuned >= 0,
+                          "probe_ms": [round(float(v), 3) for v in probe_ms]
+                          if shape_tuned >= 0 else None},
+           "roofline": {"bound": "fp32", "kernel": "whole replay (line prep, Voigt sums, fits)",
+                        "achieved": flops / s_table / 1e12 / ws, "peak": fp32_peak,
+                        "unit": "TFLOP/s", "frac": flops / s_table / 1e12 / ws / fp32_peak,
+                        "C_series_iters": n_iter},
+           "clocks": clocks}
+    # error against the FP64 oracle: one sampled tile of two states
+    if rank == 0 and not args.no_cpu_baseline:
+        par = []
+        for s in par_states:
+            kg, bm = par_gpu[s]
+            _, ko = cpu_baseline(W, L, float(T[s]), float(P[s]), 1e9, seed=100 + s, max_tiles=1)
+            par.append(parity_figure(kg, bm, ko))
+        out["parity"] = {"max_rel_err": max(p["max_rel_err"] for p in par),
+                         "points": sum(p["points"] for p in par),
+                         "tiles": sum(p["tiles"] for p in par),
+                         "states": [int(mine[s]) for s in par_states],
+                         "tolerance": 1e-5, "pass": all(p["pass"] for p in par),
+                         "oracle": "FP64 CPU restatement", "mask": par[0]["mask"]}
+    # plain FP64 form against the mixed form on 20 states spread over the table
+    if not args.no_plain:
+        sub = np.linspace(0, ns - 1, min(ns, 20)).astype(int)
+        Ks = K[: len(sub)]
+
+        def sub_ms(pr):
+            ctx.opacity(T[sub], P[sub], pr, out=Ks, stream=stream)
+            ctx.kdist(Ks, nC=nC, stream=stream)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            ctx.opacity(T[sub], P[sub], pr, out=Ks, stream=stream)
+            ctx.kdist(Ks, nC=nC, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return barrier_max(ws, e0.elapsed_time(e1))
+        mms, pms = sub_ms(hkb.MIXED), sub_ms(hkb.PLAIN_FP64)
+        out["plain_fp64"] = {"subset_states": len(sub), "mixed_ms": mms, "plain_ms": pms,
+                             "speedup_mixed_vs_plain": pms / mms,
+                             "plain_s_per_table_est": pms * 1e-3 * len(Ta) / len(sub) / ws}
+    if rank == 0 and ws == 1 and not args.no_reference_cuda:
+        # the reference runs a table as one process per T over a PFile of the
+        # 30 pressures: the middle temperature is run, x20 extrapolates
+        Tm = float(np.unique(Ta)[len(np.unique(Ta)) // 2])
+        Pt = [float(p) for t, p in zip(Ta, Pa) if t == Tm]
+        rc = reference_cuda(W, L, Tm, Pt, tunings=(1,))
+        nT = len(np.unique(Ta))
+        rc["table_extrapolation"] = f"one T ({Tm:.6g} K) x {len(Pt)} P run; x{nT} for the table"
+        for t in ("reference_tuned", "dropin"):
+            if t in rc and rc[t].get("kx_s"):
+                rc[t]["kx_s_table_est"] = rc[t]["kx_s"] * nT
+        if rc.get("reference_tuned", {}).get("kx_s"):
+            rc["table_speedup_vs_reference_kx"] = rc["reference_tuned"]["kx_s"] * nT / s_table
+        out["reference_cuda"] = rc
+    del K, coeff, nxmin
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -490,6 +728,10 @@ def main():
     ctx._numin, ctx._dnu = W["numin"], W["dnu"]
     T = np.array(W["T"], np.float64)
     P = np.array(W["P"], np.float64)
+    if args.workload == "table" and ws > 1:
+        # the table workload on N ranks: disjoint states per rank
+        mine = rank_states(len(T), ws, rank)
+        T, P = T[mine], P[mine]
     ns, nx, nb, nC = len(T), ctx.nx, W["nbins"], W["nC"]
     prec = hkb.MIXED if args.precision == "mixed" else hkb.PLAIN_FP64
 
@@ -497,20 +739,8 @@ def main():
     per_state = [count_pairs(ctx, float(T[s]), float(P[s])) for s in range(ns)]
     pa, pb, pc = (float(np.mean([p[k] for p in per_state])) for k in range(3))
     pairs_step = (pa + pb + pc) * ns
-    # n_iter of the flop model, from the lines themselves or, for lists too
-    # large to download per line, from a 2e6-line head of the same list
-    if pc > 0 and ctx.num_lines <= 20_000_000:
-        n_iter = c_series_iterations(ctx, float(T[0]), float(P[0]))
-    elif pc > 0:
-        Wp = dict(W, n=2_000_000)
-        Lp = {k: v[:2_000_000] for k, v in L.items()}
-        pctx = open_ctx(Wp, Lp, lrank)
-        pctx._numin, pctx._dnu = W["numin"], W["dnu"]
-        n_iter = c_series_iterations(pctx, float(T[0]), float(P[0]))
-        pctx.close()
-    else:
-        n_iter = 0.0
-    flops_step = ns * (pa * (F_A + F_ACC) + pb * (F_B + F_ACC) + pc * (F_C0 + F_C_ITER * n_iter + F_ACC))
+    n_iter = n_iter_of(ctx, W, L, T[0], P[0], lrank) if pc > 0 else 0.0
+    flops_step = ns * flop_model(pa, pb, pc, n_iter)
 
     stream = torch.cuda.current_stream()
     K = torch.empty((ns, nx), dtype=torch.float64, device="cuda")
@@ -563,6 +793,11 @@ def main():
     ms = e0.elapsed_time(e1) / args.steps
     clocks = clk.stop()
     ms = barrier_max(ws, ms)
+    # the timed output on the tiles the oracle samples (before anything else
+    # overwrites K)
+    nxb = nx // nb
+    sample = tile_order(nx, 0)[:32]
+    Kg_tiles, bmax_tiles = gpu_tiles(K[0], sample, nxb)
     if graph:
         ctx.table_free()
 
@@ -638,20 +873,17 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 profile, f64 offsets/strengths/sum/fit" if prec == hkb.MIXED else "f64",
         "data": "synthetic (seeded; BASELINE config distributions)",
-        "config": {"workload": W["label"], "lines": W["n"], "grid_points": nx, "states": ns,
-                   "T": W["T"][0] if ns == 1 else f"{min(W['T']):g}-{max(W['T']):g} K x {len(set(W['T']))}",
-                   "P": W["P"][0] if ns == 1 else f"{min(W['P']):.3g}-{max(W['P']):.3g} atm x {len(set(W['P']))}",
-                   "cut_cm-1": W["cut"], "nbins": nb, "nC": nC,
-                   "precision": args.precision, "parallelism": f"states x{ws} ranks",
-                   "format": W.get("database", "hitran"),
-                   "execution": "one CUDA graph per step" if graph else "hk_opacity sections + hk_kdist",
-                   "tile_shape": {"lines_per_chunk": hkb.tile_shape(shape_used)[0],
-                                  "points_per_tile": hkb.tile_shape(shape_used)[1],
-                                  "warps": hkb.tile_shape(shape_used, warps=True)[2],
-                                  "shape": shape_used, "tuned": shape_tuned >= 0,
-                                  "probe_ms": [round(float(v), 3) for v in probe_ms]
-                                  if shape_tuned >= 0 else None},
-                   "l2": f"inputs larger than L2 (line columns ~{W['n'] * 48 / 1e9:.2g} GB resident), no flush"},
+        "config": workload_config(W),
+        "precision": args.precision,
+        "parallelism": f"{'states split' if args.workload == 'table' and ws > 1 else 'replicas'} "
+                       f"x{ws} ranks",
+        "execution": {"mode": "one CUDA graph per step" if graph else "hk_opacity sections + hk_kdist",
+                      "tile_shape": {"lines_per_chunk": hkb.tile_shape(shape_used)[0],
+                                     "points_per_tile": hkb.tile_shape(shape_used)[1],
+                                     "warps": hkb.tile_shape(shape_used, warps=True)[2],
+                                     "shape": shape_used, "tuned": shape_tuned >= 0,
+                                     "probe_ms": [round(float(v), 3) for v in probe_ms]
+                                     if shape_tuned >= 0 else None}},
         "s_per_state": ms * 1e-3 / ns,
         "s_per_table": ms * 1e-3 if ns > 1 else None,
         "pairs_per_state": {"A": pa, "B": pb, "C": pc, "C_series_iters": n_iter},
@@ -671,7 +903,11 @@ def main():
         "plain_fp64": plain,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(W, L, float(T[0]), float(P[0]), args.cpu_seconds)
+        cb, Ko = cpu_baseline(W, L, float(T[0]), float(P[0]), args.cpu_seconds,
+                              max_tiles=len(sample))
+        out["cpu_baseline"] = cb
+        out["parity"] = parity_figure(Kg_tiles, bmax_tiles, Ko,
+                                      tol=1e-5 if prec == hkb.MIXED else 1e-12)
     if rank == 0 and ws == 1 and ns == 1 and not args.no_reference_cuda:
         out["reference_cuda"] = reference_cuda(W, L, float(T[0]), float(P[0]))
     elif rank == 0 and ws == 1 and args.workload == "table" and not args.no_reference_cuda:
@@ -686,6 +922,12 @@ def main():
             if t in rc and rc[t].get("kx_s"):
                 rc[t]["kx_s_table_est"] = rc[t]["kx_s"] * nT
         out["reference_cuda"] = rc
+    if args.workload == "hitemp" and prec == hkb.MIXED and not args.no_table:
+        del K, coeff, nxmin
+        torch.cuda.empty_cache()
+        tab = table_leg(ctx, W, L, args, ws, rank, lrank, stream, fp32_peak)
+        out["table"] = tab
+        out["s_per_table"] = tab["s_per_table"]
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()

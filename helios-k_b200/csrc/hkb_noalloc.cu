@@ -70,12 +70,22 @@ extern "C" hk_status hk_kdist_noalloc(const double *K, int nstates, int64_t nx, 
     return s;
   };
   if (errbuf && errbuf_len > 0) errbuf[0] = '\0';
+  // an error left by one of the caller's earlier launches is reported as
+  // such (and left pending), not mistaken for a failure of this call
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess) {
+    if (errbuf && errbuf_len > 0)
+      snprintf(errbuf, errbuf_len, "a CUDA error was already pending before this call: %s",
+               cudaGetErrorString(pending));
+    return HK_ERR_CUDA;
+  }
   if (!K || !coeff || !nxmin) return bad(HK_ERR_ARG, "K, coeff and nxmin must be device pointers");
   if (nstates < 1 || nstates > 65535) return bad(HK_ERR_RANGE, "nstates must be 1..65535");
   if (nbins < 1 || nx < 1 || nx % nbins != 0)
     return bad(HK_ERR_RANGE, "nx must be a positive multiple of nbins");
   const long long nxb = nx / nbins;
-  if (nxb < 4 || nxb > (1LL << 30)) return bad(HK_ERR_RANGE, "points per bin must be >= 4");
+  if (nxb < 4) return bad(HK_ERR_RANGE, "points per bin must be >= 4");
+  if (nxb > (1LL << 30)) return bad(HK_ERR_RANGE, "points per bin must be <= 2^30");
   if (nC < 1 || nC > 100 || nC > nxb) return bad(HK_ERR_RANGE, "nC must be 1..100 and <= points per bin");
   if (nxb * nC + 2LL * nC > HK_NOALLOC_DOUBLES) {
     char m[200];

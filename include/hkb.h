@@ -183,7 +183,9 @@ hk_status hk_kdist(hk_ctx *ctx, int nstates, const double *K, int K_on_device,
  *    that first call before any stream capture.
  *  - All calls share the array: calls that overlap on the GPU (different
  *    streams, or different host threads) race.  Serialise them.
- *  - Asynchronous on `stream`; on failure a message is written to errbuf. */
+ *  - Asynchronous on `stream`; on failure a message is written to errbuf.
+ *    A CUDA error already pending from an earlier launch of the caller's is
+ *    reported as such (HK_ERR_CUDA, left pending) before anything runs. */
 hk_status hk_kdist_noalloc(const double *K, int nstates, int64_t nx, int nbins, int nC,
                            double kmin, double unitScale, double *coeff, int32_t *nxmin,
                            double *sortedK, void *stream, char *errbuf, int errbuf_len);

@@ -336,9 +336,10 @@ def partition_dlnq(Tq, q, T):
 
 
 def vjp_hitran(lines, mass, Tq, Qq, T, P, u, numin, dnu, nx, cut=25.0, qalphaL=1.0,
-               s_scale=None, g_scale=None, profile=1):
+               s_scale=None, g_scale=None, profile=1, cutMode=0):
     """FP64 reference gradient of a loss with seed u = dLoss/dK (one HITRAN
-    isotopologue, cutMode 0): returns (dT, dP, dlogS per line, dgammaL per
+    isotopologue; the windows of cutMode at the state, held fixed: a window
+    edge that moves with T or P is not differentiated): returns (dT, dP, dlogS per line, dgammaL per
     line), by the chain rule of the line scaling of prep_hitran applied to
     the per-line sums of vjp_sums.  Optional per-line multipliers of the
     strength and of the Lorentz width, as the library's hk_set_line_scales.
@@ -350,7 +351,7 @@ def vjp_hitran(lines, mass, Tq, Qq, T, P, u, numin, dnu, nx, cut=25.0, qalphaL=1
         S = S * s_scale
     if g_scale is not None:
         vy = vy * g_scale
-    win = windows(nu, S, iad, vy, numin, dnu, nx, 0, cut, profile=profile)
+    win = windows(nu, S, iad, vy, numin, dnu, nx, cutMode, cut, profile=profile)
     gS, gy, gx, gn = vjp_sums(nu, S, iad, vy, win, numin, dnu, nx, u, profile=profile)
     c = _H * _C / _KB
     el = _f64(lines["EL"])

@@ -9,9 +9,17 @@ plots/p004, 30000 grid points, one bin, nC = 20):
   Out_r_bin.dat  reconstruction from the fit     -> Krecon_r
 The text values are printed with %.20g, so parsing them as float64 is exact.
 
-Usage (needs the reference source tree; the fixture itself is committed):
+p004_files.json records the files the reference's own run wrote, to pin the
+drop-in's output files to them: the SHA-256, size and line count of
+Out_i_bin.dat and Out_r_bin.dat, the SHA-256 of Out_r_bin.dat's first column
+(the "%g" bin coordinates), and the whole text of Out_r_cbin.dat.
+
+Usage (needs the reference source tree; the fixtures themselves are committed):
   python tests/golden/make_p004.py /path/to/HELIOS-K
+  (or HK_REFERENCE_DIR=/path/to/HELIOS-K python tests/golden/make_p004.py)
 """
+import hashlib
+import json
 import os
 import sys
 
@@ -37,7 +45,21 @@ def main(ref_root):
                         Krecon_r=Kr_r, cbin_r=cb,
                         params=np.array([0.0, 30000.0, 1.0, 1, 20, 0.0]))
     print("wrote", out, len(K_i), len(cb))
+    files = {}
+    for name in ("Out_i_bin.dat", "Out_r_bin.dat"):
+        raw = open(os.path.join(d, name), "rb").read()
+        col0 = b"\n".join(ln.split(b" ")[0] for ln in raw.split(b"\n") if ln.strip())
+        files[name] = {"sha256": hashlib.sha256(raw).hexdigest(), "bytes": len(raw),
+                       "lines": raw.count(b"\n"), "col0_sha256": hashlib.sha256(col0).hexdigest()}
+    files["Out_r_cbin.dat"] = {"text": open(os.path.join(d, "Out_r_cbin.dat")).read()}
+    jout = os.path.join(os.path.dirname(os.path.abspath(__file__)), "p004_files.json")
+    with open(jout, "w") as f:
+        json.dump(files, f, indent=1)
+    print("wrote", jout)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HK_REFERENCE_DIR")
+    if not root:
+        sys.exit("usage: make_p004.py <reference source tree> (or set HK_REFERENCE_DIR)")
+    main(root)

@@ -112,8 +112,9 @@ def test_vjp_profiles_2_to_4(adj, profile):
         u = adj["w"] / K
         rT, rP, rS, rG = oracle.vjp_hitran(adj["L"], synth.MASS, adj["Tq"], adj["Qq"], T0, P0, u,
                                            NUMIN, DNU, ctx.nx, profile=profile)
+        got = {}
         for prec, tol, tol_line in ((hkb.PLAIN_FP64, 1e-9, 1e-9), (hkb.MIXED, 1e-4, 1e-5)):
-            dT, dP, dS, dG = ctx.opacity_vjp(T0, P0, u, prec)
+            dT, dP, dS, dG = got[prec] = ctx.opacity_vjp(T0, P0, u, prec)
             eT = abs(dT - rT) / abs(rT)
             eP = abs(dP - rP) / abs(rP) if rP != 0.0 else abs(dP)
             eS = np.max(np.abs(dS - rS)) / np.max(np.abs(rS))
@@ -126,10 +127,78 @@ def test_vjp_profiles_2_to_4(adj, profile):
                   f"dgammaL {eG:.2e}")
             assert eT < tol and eP < tol
             assert eS < tol_line and eG < tol_line
+        if profile >= 3:
+            # the Doppler and binned-Gaussian adjoint runs its FP64 kernels in
+            # either precision: the mixed request must give the plain result,
+            # up to the order of the FP64 atomic additions
+            _same_up_to_atomics(got[hkb.MIXED], got[hkb.PLAIN_FP64])
         dT, fT, dP, fP = _fd_vs_vjp(ctx, adj["w"], 800.5, P0)
         print(f"profile {profile}: dT {dT:.6g} fd {fT:.6g}; dP {dP:.6g} fd {fP:.6g}")
         assert abs(fT - dT) < 1e-5 * abs(dT)
         assert abs(fP - dP) <= 1e-5 * abs(dP)
+    finally:
+        ctx.set_profile(1, 0)
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+
+
+def _same_up_to_atomics(a, b, rtol=1e-12):
+    """Two VJP results of the same FP64 kernels: per-line sums are added with
+    atomics, so only their order (the last bits) may differ."""
+    for x, y in zip(a[:2], b[:2]):
+        assert abs(x - y) <= rtol * abs(y) + 1e-300
+    for x, y in zip(a[2:], b[2:]):
+        m = np.max(np.abs(y))
+        assert np.max(np.abs(x - y)) <= rtol * m + 1e-300
+
+
+def test_vjp_doppler_cut_mode_1(adj):
+    """Profile 3 with cutMode 1: the window half-width cut * gammaL moves with
+    T and P, so the gradient holds the windows fixed (their edges are not
+    differentiated).  Against the oracle gradient on the same windows, and
+    against central differences taken with steps small enough that no window
+    index changes (checked)."""
+    ctx = adj["ctx"]
+    cut = 500.0
+    ctx.set_profile(3, 0)
+    try:
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 1, cut)
+        kmin = 1e-12 * ctx.opacity([T0], [P0], hkb.PLAIN_FP64)[0].max()
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 1, cut, kmin)
+        K = ctx.opacity([T0], [P0], hkb.PLAIN_FP64)[0]
+        u = adj["w"] / K
+        rT, rP, rS, _ = oracle.vjp_hitran(adj["L"], synth.MASS, adj["Tq"], adj["Qq"], T0, P0, u,
+                                          NUMIN, DNU, ctx.nx, cut=cut, profile=3, cutMode=1)
+        got = {}
+        for prec in (hkb.PLAIN_FP64, hkb.MIXED):
+            dT, dP, dS, _ = got[prec] = ctx.opacity_vjp(T0, P0, u, prec)
+            print(f"Doppler cutMode 1 precision {prec}: dT {dT:.6g} ref {rT:.6g}; dP {dP:.6g} "
+                  f"ref {rP:.6g}")
+            assert abs(dT - rT) < 1e-9 * abs(rT)
+            assert (abs(dP - rP) / abs(rP) if rP != 0.0 else abs(dP)) < 1e-9
+            assert np.max(np.abs(dS - rS)) < 1e-9 * np.max(np.abs(rS))
+        _same_up_to_atomics(got[hkb.MIXED], got[hkb.PLAIN_FP64])
+        win0 = ctx.state_lines(T0, P0)[4]
+
+        def fixed_windows(T, P):
+            return np.array_equal(ctx.state_lines(T, P)[4], win0)
+
+        def lossf(T, P):
+            return float(np.sum(adj["w"] * np.log(ctx.opacity([T], [P], hkb.PLAIN_FP64)[0])))
+        # the largest relative step at which no window index moves
+        for h in (1e-6, 1e-7, 1e-8, 1e-9):
+            if all(fixed_windows(T0 * (1 + s), P0) and fixed_windows(T0, P0 * (1 + s))
+                   for s in (h, -h)):
+                break
+        else:
+            pytest.fail("every step moved a window index")
+        hT, hP = h * T0, h * P0
+        fT = (lossf(T0 + hT, P0) - lossf(T0 - hT, P0)) / (2 * hT)
+        fP = (lossf(T0, P0 + hP) - lossf(T0, P0 - hP)) / (2 * hP)
+        print(f"Doppler cutMode 1: step {h:g}, fd dT {fT:.6g}, fd dP {fP:.6g}")
+        assert abs(fT - rT) < 1e-4 * abs(rT)
+        # no pressure dependence inside fixed windows (delta = 0 here): the
+        # difference quotient is rounding only
+        assert abs(fP) <= 1e-4 * abs(fT) + 1e-12 * abs(lossf(T0, P0)) / hP
     finally:
         ctx.set_profile(1, 0)
         ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)

@@ -21,6 +21,15 @@ def test_reference_arm_json_line():
     assert d["value"] > 0 and d["ms_per_step"] > 0 and d["higher_is_better"] is True
     cb = d["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"]
+    # ms_per_step is one whole step (the state's pairs) at the sampled rate;
+    # the sample's own wall time is reported apart
+    assert cb["state_pairs"] > 1e10
+    assert abs(d["ms_per_step"] - 1e3 * cb["state_pairs"] / d["value"]) < 1e-9 * d["ms_per_step"]
+    assert 0 < d["sample_s"] < d["ms_per_step"] * 1e-3
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
     assert d["config"]["workload"].startswith("hitemp")
+    # the same workload dict as our arm prints
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["config"] == json.loads(json.dumps(bench.workload_config(bench.workload("hitemp"))))
