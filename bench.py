@@ -630,6 +630,7 @@ def table_leg(ctx, W, L, args, ws, rank, lrank, stream, fp32_peak):
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = clk.stop()
+    ctx.table_status(stream)  # raises if a bounded wait inside the run ran out
     s_table = barrier_max(ws, e0.elapsed_time(e1) / args.table_steps * 1e-3)
     ctx.table_free()
     # the timed output of two states on the tiles the oracle samples (before
@@ -792,6 +793,8 @@ def main():
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     clocks = clk.stop()
+    if graph:
+        ctx.table_status(stream)  # raises if a bounded wait inside a run ran out
     ms = barrier_max(ws, ms)
     # the timed output on the tiles the oracle samples (before anything else
     # overwrites K)

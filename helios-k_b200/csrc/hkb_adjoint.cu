@@ -499,7 +499,7 @@ adjoint_c_kernel(const LinePrep *__restrict__ P, int64_t nlines, GridDev g,
 __global__ void __launch_bounds__(256)
 adjoint_line_kernel(LinesDev L, StateDev st, const double *__restrict__ G,
                     const int64_t *__restrict__ order, double *__restrict__ dlogS,
-                    double *__restrict__ dgam, double *__restrict__ dTP) {
+                    double *__restrict__ dgam, int log_gamma, double *__restrict__ dTP) {
   __shared__ double sT[8], sP[8];
   const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double vT = 0.0, vP = 0.0;
@@ -543,7 +543,8 @@ adjoint_line_kernel(LinesDev L, StateDev st, const double *__restrict__ G,
     }
     const int64_t o = order ? order[l] : l;
     if (dlogS) dlogS[o] = gS;
-    if (dgam) dgam[o] = gy * iad;
+    // dLoss/dgammaL = G_y / alphaD; per log gammaL: times gammaL
+    if (dgam) dgam[o] = log_gamma ? gy * iad * aL : gy * iad;
   }
   for (int off = 16; off > 0; off >>= 1) {
     vT += __shfl_xor_sync(0xffffffffu, vT, off);
@@ -569,7 +570,7 @@ cudaError_t launch_opacity_vjp(bool mixed, const LinesDev &L, const GridDev &g,
                                const StateDev *state_d, const StateDev &state_h,
                                const LinePrep *prep_d, const double *u_d, unsigned *ticket_d,
                                double *G_d, const int64_t *order_d, double *dlogS_d,
-                               double *dgam_d, double *dTP_d, cudaStream_t stream) {
+                               double *dgam_d, int log_gamma, double *dTP_d, cudaStream_t stream) {
   mixed = mixed && g.profile <= 2;  // Doppler and binned Gaussian: the FP64 form
   cudaError_t e = cudaMemsetAsync(G_d, 0, 4 * sizeof(double) * (size_t)L.n, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(dTP_d, 0, 2 * sizeof(double), stream);
@@ -602,7 +603,8 @@ cudaError_t launch_opacity_vjp(bool mixed, const LinesDev &L, const GridDev &g,
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   adjoint_line_kernel<<<(unsigned)((L.n + 255) / 256), 256, 0, stream>>>(L, state_h, G_d, order_d,
-                                                                         dlogS_d, dgam_d, dTP_d);
+                                                                         dlogS_d, dgam_d, log_gamma,
+                                                                         dTP_d);
   return cudaGetLastError();
 }
 

@@ -95,6 +95,8 @@ struct hk_ctx {
   cudaGraph_t table_graph = nullptr;
   cudaGraphExec_t table_exec = nullptr;
   int64_t table_kernels = 0;
+  int table_states = 0;
+  DevBuf tsync;  // the table kernel's counters, flags and per-state scales
 };
 
 static hk_status fail(hk_ctx *c, hk_status s, const char *fmt, ...) {
@@ -1038,9 +1040,9 @@ hk_status hk_set_line_scales(hk_ctx *c, const double *s_scale, const double *g_s
   return HK_OK;
 }
 
-hk_status hk_opacity_vjp(hk_ctx *c, double T, double P, int precision, const double *u,
-                         int u_on_device, double *dT, double *dP, double *dlogS, double *dgammaL,
-                         int outputs_on_device, void *stream) {
+static hk_status opacity_vjp(hk_ctx *c, double T, double P, int precision, const double *u,
+                             int u_on_device, double *dT, double *dP, double *dlogS, double *dgammaL,
+                             int log_gamma, int outputs_on_device, void *stream) {
   if (!c) return HK_ERR_ARG;
   hk_status st;
   if ((st = check_ready(c)) != HK_OK) return st;
@@ -1089,7 +1091,7 @@ hk_status hk_opacity_vjp(hk_ctx *c, double T, double P, int precision, const dou
   CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
   CUDA_TRY(c, launch_opacity_vjp(precision == HK_PRECISION_MIXED, c->L, c->g, c->states.as<StateDev>(),
                                  hs[0], c->prep.as<LinePrep>(), ud, c->ticket.as<unsigned>(), G,
-                                 c->order.as<int64_t>(), dlS, dgm, dTP, s));
+                                 c->order.as<int64_t>(), dlS, dgm, log_gamma, dTP, s));
   CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
   c->voigt_ms_acc = 0.0;
   c->voigt_ms_acc_only = false;
@@ -1107,6 +1109,20 @@ hk_status hk_opacity_vjp(hk_ctx *c, double T, double P, int precision, const dou
   return HK_OK;
 }
 
+hk_status hk_opacity_vjp(hk_ctx *c, double T, double P, int precision, const double *u,
+                         int u_on_device, double *dT, double *dP, double *dlogS, double *dgammaL,
+                         int outputs_on_device, void *stream) {
+  return opacity_vjp(c, T, P, precision, u, u_on_device, dT, dP, dlogS, dgammaL, 0,
+                     outputs_on_device, stream);
+}
+
+hk_status hk_opacity_vjp_log(hk_ctx *c, double T, double P, int precision, const double *u,
+                             int u_on_device, double *dT, double *dP, double *dlogS,
+                             double *dlogGammaL, int outputs_on_device, void *stream) {
+  return opacity_vjp(c, T, P, precision, u, u_on_device, dT, dP, dlogS, dlogGammaL, 1,
+                     outputs_on_device, stream);
+}
+
 // ---------------------------------------------------------------- tables
 hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *P,
                          int precision, double *K, int nC, double unitScale, double *coeff,
@@ -1121,10 +1137,11 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   if (nstates > 65535) return fail(c, HK_ERR_RANGE, "at most 65535 states per table");
   if (nC < 1 || nC > 100) return fail(c, HK_ERR_RANGE, "nC must be 1..100 (def_NmaxSample)");
   if (c->nxb < 4 || nC > c->nxb) return fail(c, HK_ERR_RANGE, "need Nxb >= 4 and nC <= Nxb for the fit");
+  if (c->cia) return fail(c, HK_ERR_UNSUPPORTED, "CIA contexts have no line table: use hk_opacity");
   cudaSetDevice(c->device);
   table_release(c);
   // everything the graph touches is allocated and uploaded first: capture
-  // records only asynchronous copies, memsets and kernels
+  // records only asynchronous memsets and kernels
   std::vector<StateDev> hs;
   if ((st = build_states(c, nstates, T, P, hs)) != HK_OK) return st;
   CUDA_TRY(c, c->states.ensure(nstates * sizeof(StateDev)));
@@ -1135,58 +1152,44 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   // (the mixed form's FP32 sums hold the Voigt regions; the Lorentz profile
   // is its region A over the whole window)
   const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile <= 2 && !c->g.plinth && !c->g.subL;
-  const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
-  if (per_state > c->prep_budget)
-    return fail(c, HK_ERR_UNSUPPORTED, "one state's line records (%zu B) exceed the workspace (%zu B): "
-                "tables of such lists run through hk_opacity's sectioned path", per_state, c->prep_budget);
   c->launches = 0;
-  if (mixed && c->tuning != 0 && !c->tuned && c->nlines > 0) {
+  if (mixed && c->tuning != 0 && !c->tuned && c->nlines > 0 &&
+      (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(true) <= c->prep_budget) {
     if ((st = tune_shape(c, nstates, hs, K, 0)) != HK_OK) return st;
     CUDA_TRY(c, cudaDeviceSynchronize());
   }
   const int shape = shape_for(c, mixed);
   c->last_shape = shape;
-  int batch = (int)std::max<size_t>(1, c->prep_budget / per_state);
-  const int nsplit = voigt_nsplit(nx, shape);
-  if (nsplit > 1) {
-    const int G = voigt_tile_points(shape);
-    const size_t part_per_state = (size_t)((nx + G - 1) / G) * nsplit * G * sizeof(double);
-    batch = std::min(batch, (int)std::max<size_t>(1, c->part_budget / part_per_state));
-  }
-  batch = std::min(batch, nstates);
-  CUDA_TRY(c, c->prep.ensure((size_t)batch * per_state));
-  const VoigtPlan plan0 = plan_voigt_sum(mixed, shape, nx, batch, 0);
-  if (plan0.nsplit > 1) {
-    CUDA_TRY(c, c->vpart.ensure(plan0.partial_doubles * sizeof(double)));
-    CUDA_TRY(c, c->vcnt.ensure(plan0.counters * sizeof(unsigned)));
-  }
+  // one persistent launch for the whole table: line prep into a ring of
+  // per-state record slots and every state's Voigt sums (hkb_voigt.cu)
+  const TablePlan tp = plan_table(mixed, shape, c->nlines, nx, nstates);
+  if (tp.ring_bytes > c->prep_budget)
+    return fail(c, HK_ERR_UNSUPPORTED, "%d states' line records (%zu B) exceed the workspace (%zu B): "
+                "tables of such lists run through hk_opacity's sectioned path", tp.slots, tp.ring_bytes,
+                c->prep_budget);
+  CUDA_TRY(c, c->prep.ensure(tp.ring_bytes));
+  if (tp.partial_doubles) CUDA_TRY(c, c->vpart.ensure(tp.partial_doubles * sizeof(double)));
+  CUDA_TRY(c, c->vcnt.ensure(std::max<size_t>(tp.counters, 1) * sizeof(unsigned)));
+  CUDA_TRY(c, c->tsync.ensure(table_sync_bytes(nstates)));
   if ((st = ensure_qr(c, nC, 0)) != HK_OK) return st;
   const size_t nscr = kdist_scratch_doubles(c->nxb, c->nbins, nstates);
   if (nscr) CUDA_TRY(c, c->scratch.ensure(nscr * sizeof(double)));
   CUDA_TRY(c, cudaDeviceSynchronize());
 
+  TableBufs tb;
+  tb.ring = c->prep.p;
+  tb.partial = tp.partial_doubles ? c->vpart.as<double>() : nullptr;
+  tb.tile_cnt = c->vcnt.as<unsigned>();
+  tb.sync = c->tsync.p;
   cudaStream_t cs = nullptr;
   CUDA_TRY(c, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
-  StateDev *sd = c->states.as<StateDev>();
-  unsigned long long *wb = c->wbits.as<unsigned long long>();
-  int64_t kernels = 0;
-  for (int b0 = 0; e == cudaSuccess && b0 < nstates; b0 += batch) {
-    const int nb = std::min(batch, nstates - b0);
-    const VoigtPlan plan = plan_voigt_sum(mixed, shape, nx, nb, plan0.ctas);
-    e = launch_line_prep(mixed, c->L, c->g, sd + b0, nb, c->prep.p, wb + 2 * b0, cs);
-    if (e == cudaSuccess)
-      e = launch_voigt_sum(mixed, plan, c->prep.p, c->L.nu0, c->nlines, c->g, sd + b0,
-                           c->ticket.as<unsigned>(), c->vpart.as<double>(), c->vcnt.as<unsigned>(),
-                           K + (size_t)b0 * nx, nx, cs);
-    kernels += 3;
-  }
-  if (e == cudaSuccess) {
+  if (e == cudaSuccess)
+    e = launch_voigt_table(mixed, tp, c->L, c->g, c->states.as<StateDev>(), tb, K, nx, cs);
+  if (e == cudaSuccess)
     e = launch_kdist(K, nx, nstates, c->nxb, c->nbins, nC, c->kmin, unitScale, c->qrV.as<double>(),
                      c->qrC.as<double>(), c->qrD.as<double>(), coeff, nxmin, nullptr, nullptr,
                      nscr ? c->scratch.as<double>() : nullptr, cs);
-    kernels += 1;
-  }
   cudaGraph_t g = nullptr;
   const cudaError_t e2 = cudaStreamEndCapture(cs, &g);
   cudaStreamDestroy(cs);
@@ -1203,7 +1206,23 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   }
   c->table_graph = g;
   c->table_exec = x;
-  c->table_kernels = kernels;
+  c->table_kernels = 2;  // the table kernel and the k-distribution kernel
+  c->table_states = nstates;
+  ok(c);
+  return HK_OK;
+}
+
+hk_status hk_table_status(hk_ctx *c, void *stream) {
+  if (!c) return HK_ERR_ARG;
+  if (!c->table_exec) return fail(c, HK_ERR_STATE, "hk_table_build must come first");
+  cudaSetDevice(c->device);
+  CUDA_TRY(c, cudaStreamSynchronize((cudaStream_t)stream));
+  int err = 0;
+  CUDA_TRY(c, cudaMemcpy(&err, table_error_word(c->tsync.p, c->table_states), sizeof(int),
+                         cudaMemcpyDeviceToHost));
+  if (err != 0)
+    return fail(c, HK_ERR_TIMEOUT, "a wait inside the table kernel ran out: the last run's results "
+                "are incomplete");
   ok(c);
   return HK_OK;
 }

@@ -409,7 +409,7 @@ constexpr int HK_ASY_K = 8;
 __device__ __forceinline__ float voigt_asy(float x, float y) {
   x = fabsf(x);
   const float x2 = x * x, y2 = y * y;
-  const float r2 = x2 + y2;
+  const float r2 = fmaf(x, x, y2);
   const float ir2 = rcp_fast(r2);
   const float ir4 = ir2 * ir2;
   const float ur = (x2 - y2) * ir4;
@@ -501,7 +501,7 @@ __device__ __forceinline__ float voigt916_core(float x, float y, float iy, float
   const float sin2 = sin_sq(x * y);
   const float cos2xy = fmaf(-2.0f, sin2, 1.0f);
   const float t2 = sin2 * ex2 * iy;
-  const float t3 = y * (-cos2xy * s1 + 0.5f * (s2 + s3));
+  const float t3 = y * fmaf(-cos2xy, s1, 0.5f * (s2 + s3));
   return fmaf(ex2 * ey, cos2xy, HK_C916_F * (t2 + t3));
 }
 

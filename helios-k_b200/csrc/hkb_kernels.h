@@ -25,12 +25,13 @@ cudaError_t measure_fp32_peak(double *tflops, cudaStream_t stream);
 
 // Vector-Jacobian product of one state's opacity (hkb_adjoint.cu): G_d holds
 // 4 x nlines FP64 sums, dTP_d the two scalars; dlogS_d / dgam_d (load order
-// through order_d, may be null) the per-line results.
+// through order_d, may be null) the per-line results, dgam_d per gammaL or,
+// with log_gamma, per log gammaL.
 cudaError_t launch_opacity_vjp(bool mixed, const LinesDev &L, const GridDev &g,
                                const StateDev *state_d, const StateDev &state_h,
                                const LinePrep *prep_d, const double *u_d, unsigned *ticket_d,
                                double *G_d, const int64_t *order_d, double *dlogS_d,
-                               double *dgam_d, double *dTP_d, cudaStream_t stream);
+                               double *dgam_d, int log_gamma, double *dTP_d, cudaStream_t stream);
 
 // per-(line, state) records: LinePrepF (mixed) or LinePrep (plain FP64)
 cudaError_t launch_line_prep(bool mixed, const LinesDev &L, const GridDev &g, StateDev *states_d,
@@ -137,6 +138,45 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &plan, const void *prep
                              const StateDev *states_d, unsigned *ticket_d, double *partial_d,
                              unsigned *tile_cnt_d, double *K_d, int64_t k_stride,
                              cudaStream_t stream);
+
+// A whole T-P table as one persistent launch (hkb_voigt.cu): line prep into
+// a ring of per-state record slots and the Voigt sums of every state, as
+// tickets of one counter (the prep tickets of state s interleaved with the
+// sum tickets of state s - 1; a slot is reused once its previous state's
+// sums are done).
+struct TableFin {  // per state, written by the kernel's last prep ticket of the state
+  double wmax;
+  int s1exp, pad;
+};
+static_assert(sizeof(TableFin) == 16, "TableFin layout");
+struct TablePlan {
+  int shape = 0, G = 0;
+  int S = 0, R = 3, slots = 1;  // states, ring slots of the schedule, slots allocated
+  int lpt = 0, npb = 0;         // lines per prep ticket, prep tickets per state
+  int tps = 0, nsplit = 1;
+  long long nsum = 0, total = 0;
+  int ctas = 0;
+  size_t ring_bytes = 0, partial_doubles = 0, counters = 0;
+};
+// device buffers of a table launch: the record ring, split-tile partial rows
+// and counters (slots x tiles), and the sync block of table_sync_bytes(S)
+struct TableBufs {
+  void *ring = nullptr;
+  double *partial = nullptr;
+  unsigned *tile_cnt = nullptr;
+  void *sync = nullptr;
+};
+inline size_t table_sync_bytes(int nstates) {
+  // ticket (8) + pad (8), wbits 16 S, fin 16 S, prep/sum counts and ready flags 12 S, error word
+  return 16 + 16 * (size_t)nstates + sizeof(TableFin) * (size_t)nstates + 12 * (size_t)nstates + 16;
+}
+TablePlan plan_table(bool mixed, int shape, int64_t nlines, int64_t nx, int nstates);
+cudaError_t launch_voigt_table(bool mixed, const TablePlan &plan, const LinesDev &L, const GridDev &g,
+                               const StateDev *states_d, const TableBufs &bufs, double *K_d,
+                               int64_t k_stride, cudaStream_t stream);
+// the launch's error word in its sync block (0: every wait ended; 1: a wait
+// for another ticket ran out and the results are incomplete)
+int *table_error_word(void *sync_d, int nstates);
 
 cudaError_t launch_prep_dump(const LinesDev &L, const GridDev &g,
                              const StateDev &st, double *out4_d,

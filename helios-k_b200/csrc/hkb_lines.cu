@@ -15,6 +15,7 @@
 
 #include "hkb_device.cuh"
 #include "hkb_kernels.h"
+#include "hkb_prep.cuh"
 
 namespace hkb {
 
@@ -68,19 +69,13 @@ cudaError_t sort_lines_by_nu(int64_t n, double *nu_d, int64_t *order_d,
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
-// One thread per (line, state): FP64 scaling (prep_line), the global index
-// windows (line_windows over [0, Nx)), and the region-C per-line constants
-// erfcx(y) and Sig1(y) for lines that have a region-C window.  For cutMode
-// 1/2 it also bounds the state's largest cutoff half-width (cm^-1), which
-// sizes each tile's line search; and it takes the state's largest region-A/B
-// term, which sets the power-of-two scale of the mixed form's FP32 sums.
-// wbits holds two words per state: {half-width bits, term bits} (both
-// non-negative doubles, so their bit patterns order like the values).
-// MODE: PREP_ALL writes the records and the per-state maxima; PREP_STATS only
-// the maxima (the state pass of a sectioned state); PREP_RECORDS only the
-// records (one section's lines, the state already finalised).
-enum { PREP_ALL = 0, PREP_STATS = 1, PREP_RECORDS = 2 };
-
+// One thread per (line, state): the record of prep_record (hkb_prep.cuh) for
+// every line of every state of a batch.  For cutMode 1/2 it also bounds the
+// state's largest cutoff half-width (cm^-1), which sizes each tile's line
+// search; and it takes the state's largest region-A/B term, which sets the
+// power-of-two scale of the mixed form's FP32 sums.  wbits holds two words
+// per state: {half-width bits, term bits} (both non-negative doubles, so
+// their bit patterns order like the values).
 template <bool MIXED, int MODE>
 __global__ void __launch_bounds__(256)
 line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
@@ -91,101 +86,11 @@ line_prep_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states,
   if (MODE != PREP_STATS && threadIdx.x < HK_SIG1_M) s_e916[threadIdx.x] = c916_e(threadIdx.x + 1);
   __syncthreads();
   double w_loc = 0.0, s1_loc = 0.0;
+  void *out_s = MODE == PREP_STATS ? nullptr
+                                   : static_cast<char *>(out) + (size_t)s * L.n * (MIXED ? sizeof(LinePrepF) : sizeof(LinePrep));
   for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < L.n;
-       l += (int64_t)gridDim.x * blockDim.x) {
-    const LineState ls = prep_line(L, st, l);
-    int64_t w[6];
-    line_windows(g, st, ls, 0, g.nx, w);
-    // S1 per profile (S3_kernel voigt.h:452-463); the mixed form runs profiles 1-2
-    const double Sc = ls.S * (1.0 / 1.7724538509055160273);
-    const double S1 = (MIXED || g.profile <= 2) ? ls.S * ls.vy / CUDART_PI
-                                                : (g.profile == 3 ? Sc : ls.S);
-    const bool hasC = w[3] > w[2];
-    // largest region-A/B term of the line: S1 / r^2 with r^2 >= max(100, y^2)
-    // (Voigt: region C covers r < 10), r^2 >= y^2 for the Lorentz profile
-    const double Y = ls.vy * ls.vy;
-    const double rmin = g.profile == 2 ? Y : fmax(100.0, Y);
-    const double term = rmin > 0.0 ? S1 / rmin : 0.0;
-    if (MODE == PREP_STATS) {
-    } else if (MIXED) {
-      const double ey = hasC ? erfcx(ls.vy) : 1.0;
-      const float sig1 = hasC ? (float)c916_sig1_tab(ls.vy, s_e916) : 0.f;
-      LinePrepF r;
-      r.nu = ls.nu;
-      r.iad = ls.iad;
-      r.S1 = S1;
-      r.Sc = Sc;
-      r.y = (float)ls.vy;
-      r.ey = (float)ey;
-      r.sig1 = sig1;
-      const double A2 = 2.0 * Y + 3.0 - 6.0 / CUDART_PI, B2 = (Y + 1.5) * (Y + 1.5);
-      r.A1 = (float)(2.0 * Y + 2.5 - 4.0 / CUDART_PI);
-      r.B1 = (float)((Y + 1.5) * (Y + 1.0));
-      r.D2 = (float)(A2 + Y);
-      r.D1 = (float)(B2 + A2 * Y);
-      r.D0 = (float)(B2 * Y);
-      int ex = -100000;
-      if (term > 0.0) frexp(term, &ex);
-      r.ex = ex;
-      int flags = 0;
-      if (w[5] > w[0]) {
-        // the largest |x| inside the cut window (at its first or last point)
-        const double xa = fabs((grid_x(g, w[0]) - ls.nu) * ls.iad);
-        const double xb = fabs((grid_x(g, w[5] - 1) - ls.nu) * ls.iad);
-        const double umax = fmax(xa, xb) * fmax(xa, xb) + Y;
-        if (umax >= 1e18) flags |= HK_PF_WIDE;
-        // (Lorentz: Y >= 2^-60 also keeps the product of two denominators,
-        // >= Y^2, a normal float)
-        if (rmin < 0x1p-64 * umax || Y > 0x1p60 || (g.profile == 2 && Y < 0x1p-60)) flags |= HK_PF_RANGE;
-      }
-      r.flags = flags;
-      // region C's Algorithm-916 part: |x| < sqrt(36 - y^2), from the FP64
-      // offsets (a point within rounding of r = 6 may fall on either side;
-      // both evaluators hold there)
-      int64_t t0 = w[3], t1 = w[3];
-      if (w[3] > w[2] && Y < 36.0) {
-        const double xt = sqrt(36.0 - Y);
-        const double x0 = (g.numin - ls.nu) * ls.iad, vb = g.dnu * ls.iad;
-        const double k0 = floor((-xt - x0) / vb) + 1.0, k1 = floor((xt - x0) / vb) + 1.0;
-        t0 = (int64_t)fmin(fmax(k0, (double)w[2]), (double)w[3]);
-        t1 = (int64_t)fmin(fmax(k1, (double)t0), (double)w[3]);
-      }
-      r.t0 = (int)t0;
-      r.t1 = (int)t1;
-      r.i0 = (int)w[0];
-      r.b0 = (int)w[1];
-      r.c0 = (int)w[2];
-      r.c1 = (int)w[3];
-      r.b1 = (int)w[4];
-      r.i1 = (int)w[5];
-      reinterpret_cast<LinePrepF *>(out)[(int64_t)s * L.n + l] = r;
-    } else {
-      const double ey = hasC ? erfcx(ls.vy) : 1.0;
-      const float sig1 = hasC ? (float)c916_sig1_tab(ls.vy, s_e916) : 0.f;
-      LinePrep r;
-      r.nu = ls.nu;
-      r.iad = ls.iad;
-      r.vy = ls.vy;
-      r.S1 = S1;
-      r.Sc = Sc;
-      r.ey = ey;
-      r.sig1 = sig1;
-      r.i0 = (int)w[0];
-      r.b0 = (int)w[1];
-      r.c0 = (int)w[2];
-      r.c1 = (int)w[3];
-      r.b1 = (int)w[4];
-      r.i1 = (int)w[5];
-      r.pad = 0;
-      r.plinth = (g.plinth && w[5] > w[0]) ? plinth_d(g, S1, Sc, ls.iad, ls.vy) : 0.0;
-      reinterpret_cast<LinePrep *>(out)[(int64_t)s * L.n + l] = r;
-    }
-    if (w[5] > w[0]) s1_loc = fmax(s1_loc, term);
-    if (ls.S != 0.0 && ls.iad > 0.0) {
-      if (g.cutMode == 1) w_loc = fmax(w_loc, g.cut * ls.vy / ls.iad);
-      else if (g.cutMode == 2) w_loc = fmax(w_loc, g.cut / ls.iad);
-    }
-  }
+       l += (int64_t)gridDim.x * blockDim.x)
+    prep_record<MIXED, MODE>(L, g, st, l, s_e916, out_s, w_loc, s1_loc);
   if constexpr (MODE != PREP_RECORDS) {
     for (int o = 16; o > 0; o >>= 1) {
       w_loc = fmax(w_loc, __shfl_xor_sync(0xffffffffu, w_loc, o));
@@ -203,18 +108,10 @@ __global__ void state_finalize_kernel(GridDev g, StateDev *__restrict__ states,
                                       const unsigned long long *__restrict__ wbits) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nstates) return;
-  if (g.cutMode == 0) {
-    states[s].wmax = g.cut;
-  } else {
-    const double w = __longlong_as_double((long long)wbits[2 * s]);
-    states[s].wmax = w * (1.0 + 1e-9) + 1e-300;
-  }
-  const double tmax = __longlong_as_double((long long)wbits[2 * s + 1]);
-  int e = 0;
-  if (tmax > 0.0 && isfinite(tmax)) {
-    frexp(tmax, &e);  // tmax in [2^(e-1), 2^e)
-    e = 40 - e;
-  }
+  double wmax;
+  int e;
+  state_scale(g, wbits[2 * s], wbits[2 * s + 1], wmax, e);
+  states[s].wmax = wmax;
   states[s].s1scale = ldexp(1.0, e);
   states[s].s1unscale = ldexp(1.0, -e);
   states[s].s1exp = e;

@@ -28,6 +28,7 @@
 
 #include "hkb_device.cuh"
 #include "hkb_kernels.h"
+#include "hkb_prep.cuh"
 
 namespace hkb {
 
@@ -169,24 +170,48 @@ __device__ __forceinline__ float2 f2(double v) {
 // chunk -- its strength level (0..HK_MAX_LEVEL), HK_MAX_LEVEL + 1 for lines
 // summed in FP64 (weak), HK_MAX_LEVEL + 2 for lines without points in the
 // tile -- and stage_mixed builds the record for that key.
+// Record loads: the Voigt launch reads records another kernel wrote (the
+// read-only path is fine); the fused table kernel reads records its own CTAs
+// wrote into reused ring slots, so its loads go to L2 (.cg), never through
+// a stale L1 or the non-coherent path.
+template <bool CG>
+__device__ __forceinline__ int4 rec_words(const void *p, int word16) {
+  const int4 *q = reinterpret_cast<const int4 *>(p) + word16;
+  if constexpr (CG) return __ldcg(q);
+  else return *q;
+}
+
+template <bool CG, class R>
+__device__ __forceinline__ R load_record(const R *p) {
+  static_assert(sizeof(R) % 16 == 0, "records are read in 16-byte words");
+  R r;
+  int4 *d = reinterpret_cast<int4 *>(&r);
+#pragma unroll
+  for (int k = 0; k < (int)(sizeof(R) / 16); ++k) d[k] = rec_words<CG>(p, k);
+  return r;
+}
+
 constexpr int HK_NKEY = HK_MAX_LEVEL + 3;
 constexpr int HK_KEY_WEAK = HK_MAX_LEVEL + 1, HK_KEY_EMPTY = HK_MAX_LEVEL + 2;
 
+template <bool CG>
 __device__ __forceinline__ int line_key(const LinePrepF *__restrict__ P, int64_t l,
                                         int64_t g0, int64_t g1, int s1exp) {
-  const LinePrepF &lp = P[l];
-  const int i0 = clip_local(lp.i0, g0, g1), i1 = clip_local(lp.i1, g0, g1);
+  // words 4 and 5 of the record: {ex, flags, i0, b0}, {c0, c1, b1, i1}
+  const int4 w4 = rec_words<CG>(P + l, 4), w5 = rec_words<CG>(P + l, 5);
+  const int i0 = clip_local(w4.z, g0, g1), i1 = clip_local(w5.w, g0, g1);
   if (i1 <= i0) return HK_KEY_EMPTY;
   // the state's largest term has exponent 40 - s1exp, so 40 - (ex + s1exp) >= 0
-  const int lev = (40 - (lp.ex + s1exp)) / HK_LEVEL_BITS;
-  if ((lp.flags & HK_PF_RANGE) || lev > HK_MAX_LEVEL) return HK_KEY_WEAK;
+  const int lev = (40 - (w4.x + s1exp)) / HK_LEVEL_BITS;
+  if ((w4.y & HK_PF_RANGE) || lev > HK_MAX_LEVEL) return HK_KEY_WEAK;
   return lev;
 }
 
+template <bool CG>
 __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, const GridDev &g,
                                             int64_t l, int64_t g0, int64_t g1, int s1exp,
                                             int key, RecF &r) {
-  const LinePrepF lp = P[l];
+  const LinePrepF lp = load_record<CG>(P + l);
   const bool nonempty = key != HK_KEY_EMPTY;
   const bool weak = key == HK_KEY_WEAK;
   const int lev = (weak || !nonempty) ? 0 : key;
@@ -208,7 +233,7 @@ __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, con
   r.D0 = lp.D0;
   r.nkc = (float)(-kc);
   r.vb = (float)vb;
-  r.fr = (float)(D0 + kc * vb);
+  r.fr = (float)__fma_rn(kc, vb, D0);
   r.dh = dh;
   r.dl = dl;
   r.vbh = vbh;
@@ -237,9 +262,10 @@ __device__ __forceinline__ void stage_rtab(float y, float *__restrict__ Rtab) {
   for (int m = 1; m <= HK_C916_MR; ++m) Rtab[m - 1] = rcp_fast(fmaf(a2 * m, (float)m, Yf));
 }
 
+template <bool CG>
 __device__ __forceinline__ void stage_plain(const LinePrep *__restrict__ P, int64_t l,
                                             int64_t g0, int64_t g1, RecD *recp) {
-  const LinePrep lp = P[l];
+  const LinePrep lp = load_record<CG>(P + l);
   int li[6] = {clip_local(lp.i0, g0, g1), clip_local(lp.b0, g0, g1),
                clip_local(lp.c0, g0, g1), clip_local(lp.c1, g0, g1),
                clip_local(lp.b1, g0, g1), clip_local(lp.i1, g0, g1)};
@@ -480,20 +506,21 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
       const float kk = (p & 1) ? kf[p >> 1].y : kf[p >> 1].x;
       const float x = fmaf(kk + nkc, vb, fr);
       const float s = x * x;
-      float t;
+      // the term as (factor, reciprocal), added with one FMA like the packed sweeps
+      float f, inv;
       if (k >= b0 && k < b1) {
-        const float num = fmaf(s, fmaf(S1f, s, C1), C0);
-        const float den = fmaf(fmaf(s + D2, s, D1), s, D0);
-        t = num * rcp_fast(den);
+        f = fmaf(s, fmaf(S1f, s, C1), C0);
+        inv = rcp_fast(fmaf(fmaf(s + D2, s, D1), s, D0));
       } else {
-        t = S1f * rcp_fast(s + Yf);
+        f = S1f;
+        inv = rcp_fast(fmaf(x, x, Yf));
       }
       if (WEAK) {
-        cacc[k] = fma(S1w, (double)t, cacc[k]);
+        cacc[k] = fma(S1w, (double)(f * inv), cacc[k]);
       } else if (p & 1) {
-        a32[p >> 1].y += t;
+        a32[p >> 1].y = fmaf(f, inv, a32[p >> 1].y);
       } else {
-        a32[p >> 1].x += t;
+        a32[p >> 1].x = fmaf(f, inv, a32[p >> 1].x);
       }
     }
   }
@@ -573,6 +600,221 @@ __device__ __forceinline__ void flush_sums(float2 (&a32)[PPL / 2], double *__res
   for (int q = 0; q < PPL / 2; ++q) a32[q] = make_float2(0.f, 0.f);
 }
 
+// ------------------------------------------------------- one tile's sum
+// Everything one ticket of the Voigt sum does: the sum of the lines whose
+// windows reach the tile [g0, g1) (the part-th of nsplit parts of its line
+// range) into the tile's points, written to Ks (one state's K row) or, for a
+// split tile, published to pt (this tile's nsplit partial rows of G points)
+// and combined in part order by the CTA that completes the count *cnt.
+// wmax and s1exp are the state's search half-width and FP32 scale exponent.
+template <bool MIXED, class SH, bool CG>
+__device__ __forceinline__ void sum_tile(const void *prep_s, const double *__restrict__ nu0,
+                                         int64_t nlines, const GridDev &g, const StateDev &st,
+                                         double wmax, int s1exp, int64_t g0, int64_t g1, int part,
+                                         int nsplit, double *pt, unsigned *cnt, double *Ks,
+                                         unsigned char *smem_dyn) {
+  using Rec = typename std::conditional<MIXED, RecF, RecD>::type;
+  constexpr int CH = SH::CH, PPL = SH::PPL, SLICE = SH::SLICE, G = SH::G;
+  Rec *rec = reinterpret_cast<Rec *>(smem_dyn);
+  float *Rtab = reinterpret_cast<float *>(smem_dyn + sizeof(Rec) * CH) + HK_RPAD;
+  double *cacc = reinterpret_cast<double *>(smem_dyn + sizeof(Rec) * CH +
+                                            sizeof(float) * (HK_RPAD + CH * HK_C916_MR));
+  __shared__ int s_last;
+  __shared__ int s_kcnt[CH / 32][HK_NKEY];  // staged lines per (staging warp, key)
+  __shared__ long long s_L0, s_L1;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int wb = warp * SLICE;
+  const LinePrep *P = reinterpret_cast<const LinePrep *>(prep_s);
+  const LinePrepF *PF = reinterpret_cast<const LinePrepF *>(prep_s);
+  if (warp == 0) {
+    const double W = wmax + st.shift + 2.0 * g.dnu;
+    const double xlo = grid_x(g, g0) - W;
+    const double xhi = grid_x(g, g1 - 1) + W;
+    const double pad = 1e-12 * (fabs(xlo) + fabs(xhi)) + 1e-300;
+    const int64_t L0 = lower_bound_warp(nu0, nlines, xlo - pad);
+    const int64_t L1 = lower_bound_warp(nu0, nlines, xhi + pad);
+    if (lane == 0) {
+      s_L0 = L0;
+      s_L1 = L1;
+    }
+  }
+  __syncthreads();
+  const int64_t L0 = s_L0, L1 = s_L1;
+
+  float2 kf[PPL / 2];   // lane-local point indices, paired {p, p+1}
+  float2 a32[PPL / 2];  // mixed: FP32 sums of the current chunk (scaled)
+  double acc[PPL], xg[PPL];
+#pragma unroll
+  for (int p = 0; p < PPL; ++p) {
+    const int k = wb + lane + 32 * p;
+    acc[p] = 0.0;
+    if (MIXED) {
+      if (p & 1) {
+        kf[p >> 1].y = (float)k;
+        a32[p >> 1].y = 0.f;
+      } else {
+        kf[p >> 1].x = (float)k;
+        a32[p >> 1].x = 0.f;
+      }
+      cacc[k] = 0.0;  // owned by this lane only: no barrier needed
+    } else {
+      xg[p] = grid_x(g, g0 + k);
+    }
+  }
+
+  // Chunk c holds the lines L0 + c + q*nch (q < CH): every chunk spans
+  // the tile's whole line range, so the costly region-C points of its
+  // lines fall into all warp slices instead of one or two (consecutive
+  // nu-sorted lines would put a chunk's line cores into a single slice
+  // and leave the other warps idle at the barrier).
+  const int64_t nL = L1 - L0;
+  const int64_t nch = (nL + CH - 1) / CH;
+  const int64_t c_begin = nch * part / nsplit, c_end = nch * (part + 1) / nsplit;
+  int lcur = 0;  // strength level held in a32 (warp-uniform)
+  for (int64_t c = c_begin; c < c_end; ++c) {
+    const int cnt_c = (int)((nL - c + nch - 1) / nch);
+    if (MIXED) {
+      // build the records, then place them sorted by key (stable counting
+      // sort over the CH / 32 staging warps), so a warp's 32-line
+      // groups mostly hold one strength level
+      // (the key pass keeps no record: the record is rebuilt after the
+      // scan rather than held in registers across the barrier)
+      int key = HK_NKEY, rank = 0;
+      const int64_t l = L0 + c + (int64_t)tid * nch;
+      if (tid < cnt_c) key = line_key<CG>(PF, l, g0, g1, s1exp);
+      if (tid < CH) {
+        const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+        for (int v = 0; v < HK_NKEY; ++v) {
+          const unsigned m = __ballot_sync(0xffffffffu, key == v);
+          if (key == v) rank = __popc(m & lt);
+          if (lane == 0) s_kcnt[warp][v] = __popc(m);
+        }
+      }
+      __syncthreads();
+      if (tid < cnt_c) {
+        int pos = rank;
+        for (int v = 0; v < key; ++v)
+#pragma unroll
+          for (int w = 0; w < CH / 32; ++w) pos += s_kcnt[w][v];
+        for (int w = 0; w < warp; ++w) pos += s_kcnt[w][key];
+        RecF r;
+        stage_mixed<CG>(PF, g, l, g0, g1, s1exp, key, r);
+        reinterpret_cast<RecF *>(rec)[pos] = r;
+        if (r.c1 > r.c0 && r.i1 > r.i0) stage_rtab(r.y, Rtab + pos * HK_C916_MR);
+      }
+    } else if (tid < cnt_c) {
+      stage_plain<CG>(P, L0 + c + (int64_t)tid * nch, g0, g1, reinterpret_cast<RecD *>(rec) + tid);
+    }
+    __syncthreads();
+    if (MIXED) {
+      const RecF *rf = reinterpret_cast<const RecF *>(rec);
+      for (int g32 = 0; g32 < cnt_c; g32 += 32) {
+        const int j = g32 + lane;
+        const int cls = (j < cnt_c) ? classify<SLICE>(rf[j], wb) : HK_CLS_SKIP;
+        const int lev = (j < cnt_c) ? (rf[j].flags >> 8) : 0;
+        const unsigned bB = __ballot_sync(0xffffffffu, cls == HK_CLS_B);
+        const unsigned bA = __ballot_sync(0xffffffffu, cls == HK_CLS_A);
+        const unsigned bBM = __ballot_sync(0xffffffffu, cls == HK_CLS_BM);
+        const unsigned bAM = __ballot_sync(0xffffffffu, cls == HK_CLS_AM);
+        const unsigned bG = __ballot_sync(0xffffffffu, cls == HK_CLS_G);
+        unsigned mW = __ballot_sync(0xffffffffu, cls == HK_CLS_W);
+        unsigned live = bB | bA | bBM | bAM | bG;
+        while (live) {
+          // the lines of the current level first; switch level (flushing
+          // the FP32 sums) only when none of them is left
+          unsigned m = __ballot_sync(0xffffffffu, lev == lcur) & live;
+          if (m == 0u) {
+            flush_sums<PPL>(a32, cacc, wb, lane, s1exp, lcur);
+            lcur = __shfl_sync(0xffffffffu, lev, __ffs(live) - 1);
+            m = __ballot_sync(0xffffffffu, lev == lcur) & live;
+          }
+          live &= ~m;
+          unsigned mB = m & bB, mA = m & bA, mBM = m & bBM, mAM = m & bAM, mG = m & bG;
+          while (mB) {
+            const int b = __ffs(mB) - 1;
+            mB &= mB - 1;
+            sweep_B<PPL>(rf[g32 + b], kf, a32);
+          }
+          while (mA) {
+            const int b = __ffs(mA) - 1;
+            mA &= mA - 1;
+            sweep_A<false, PPL>(rf[g32 + b], wb, lane, kf, a32);
+          }
+          while (mBM) {
+            const int b = __ffs(mBM) - 1;
+            mBM &= mBM - 1;
+            sweep_BM<PPL>(rf[g32 + b], wb, lane, kf, a32);
+            sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
+          }
+          while (mAM) {
+            const int b = __ffs(mAM) - 1;
+            mAM &= mAM - 1;
+            sweep_A<true, PPL>(rf[g32 + b], wb, lane, kf, a32);
+          }
+          while (mG) {
+            const int b = __ffs(mG) - 1;
+            mG &= mG - 1;
+            sweep_G<false, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc);
+            sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
+          }
+        }
+        while (mW) {
+          const int b = __ffs(mW) - 1;
+          mW &= mW - 1;
+          sweep_G<true, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc);
+          sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
+        }
+      }
+      // at most one chunk of lines per FP32 sum
+      flush_sums<PPL>(a32, cacc, wb, lane, s1exp, lcur);
+    } else {
+      for (int j = 0; j < cnt_c; ++j)
+        sweep_plain<PPL>(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc, g, st);
+    }
+    __syncthreads();
+  }
+
+  if (nsplit == 1) {
+#pragma unroll
+    for (int p = 0; p < PPL; ++p) {
+      const int k = wb + lane + 32 * p;
+      const int64_t gi = g0 + k;
+      if (MIXED) acc[p] = cacc[k];
+      if (gi < g1) Ks[gi] = st.kmin + acc[p];
+    }
+  } else {
+    // Split tile: publish this part's sums; the CTA that completes the
+    // tile's count adds the parts in part order (the result does not
+    // depend on which CTA ran which part or when).  The last arriver resets
+    // the count, so the counter is ready for the next use of its slot.
+#pragma unroll
+    for (int p = 0; p < PPL; ++p) {
+      const int k = wb + lane + 32 * p;
+      if (MIXED) acc[p] = cacc[k];
+      pt[(int64_t)part * G + k] = acc[p];
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = (atomicAdd(cnt, 1u) == (unsigned)(nsplit - 1));
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+#pragma unroll
+      for (int p = 0; p < PPL; ++p) {
+        const int k = wb + lane + 32 * p;
+        double sum = 0.0;
+        for (int j = 0; j < nsplit; ++j) sum += __ldcg(pt + (int64_t)j * G + k);
+        const int64_t gi = g0 + k;
+        if (gi < g1) Ks[gi] = st.kmin + sum;
+      }
+      if (tid == 0) atomicExch(cnt, 0u);
+    }
+  }
+}
+
 // ------------------------------------------------------- persistent kernel
 // mixed form: SH::MINB CTAs per SM (4: 32 warps, 64 registers)
 template <bool MIXED, class SH>
@@ -582,21 +824,11 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
                  int tile0, int tiles_per_state, int nsplit, int total_tickets,
                  unsigned *__restrict__ ticket, double *__restrict__ partial,
                  unsigned *__restrict__ tile_cnt, double *__restrict__ K, int64_t k_stride) {
-  using Rec = typename std::conditional<MIXED, RecF, RecD>::type;
-  constexpr int CH = SH::CH, PPL = SH::PPL, SLICE = SH::SLICE, G = SH::G;
+  constexpr int G = SH::G;
   extern __shared__ __align__(16) unsigned char smem_dyn[];
-  Rec *rec = reinterpret_cast<Rec *>(smem_dyn);
-  float *Rtab = reinterpret_cast<float *>(smem_dyn + sizeof(Rec) * CH) + HK_RPAD;
-  double *cacc = reinterpret_cast<double *>(smem_dyn + sizeof(Rec) * CH +
-                                            sizeof(float) * (HK_RPAD + CH * HK_C916_MR));
-  __shared__ int s_ticket, s_last;
-  __shared__ int s_kcnt[CH / 32][HK_NKEY];  // staged lines per (staging warp, key)
-  __shared__ long long s_L0, s_L1;
+  __shared__ int s_ticket;
   const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  const int warp = tid >> 5;
-  const int wb = warp * SLICE;
-
+  const size_t rec_bytes = MIXED ? sizeof(LinePrepF) : sizeof(LinePrep);
   for (;;) {
     if (tid == 0) s_ticket = (int)atomicAdd(ticket, 1u);
     __syncthreads();
@@ -608,195 +840,184 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
     const int s = tt / tiles_per_state;
     const int tile = tt - s * tiles_per_state;
     const StateDev &st = states[s];
-    const LinePrep *P = reinterpret_cast<const LinePrep *>(prep) + (int64_t)s * nlines;
-    const LinePrepF *PF = reinterpret_cast<const LinePrepF *>(prep) + (int64_t)s * nlines;
+    const void *prep_s = static_cast<const char *>(prep) + (size_t)s * nlines * rec_bytes;
     const int64_t g0 = (int64_t)(tile0 + tile) * G;
     const int64_t g1 = min(g0 + (int64_t)G, g.nx);
-    if (warp == 0) {
-      const double W = st.wmax + st.shift + 2.0 * g.dnu;
-      const double xlo = grid_x(g, g0) - W;
-      const double xhi = grid_x(g, g1 - 1) + W;
-      const double pad = 1e-12 * (fabs(xlo) + fabs(xhi)) + 1e-300;
-      const int64_t L0 = lower_bound_warp(nu0, nlines, xlo - pad);
-      const int64_t L1 = lower_bound_warp(nu0, nlines, xhi + pad);
-      if (lane == 0) {
-        s_L0 = L0;
-        s_L1 = L1;
-      }
+    sum_tile<MIXED, SH, false>(prep_s, nu0, nlines, g, st, st.wmax, st.s1exp, g0, g1, part, nsplit,
+                               partial + (int64_t)tt * nsplit * G, tile_cnt + tt,
+                               K + (int64_t)s * k_stride, smem_dyn);
+  }
+}
+
+// ----------------------------------------------------- T-P table kernel
+// A whole T-P table in one persistent launch.  Tickets of two kinds come
+// from one 64-bit counter:
+//   prep (s, b): lines [b LPT, (b + 1) LPT) of state s scaled into ring slot
+//                s mod R (prep_record, the records line_prep_kernel writes);
+//                the ticket that completes state s's count turns the state's
+//                maxima into its search half-width and FP32 scale and marks
+//                the state ready;
+//   sum (s, i):  tile i / nsplit, part i mod nsplit of state s (sum_tile).
+// Phase p (p = 0 .. S) holds the preps of state p and the sums of state
+// p - 1, interleaved one for one from the phase's start (the rest of the
+// larger kind follows), so the line prep (FP64 and memory) runs beside the
+// Voigt sums (FP32) on the same SMs.  A sum ticket waits until its state is
+// ready (its preps were handed out in the previous phase, most of a phase
+// earlier); a prep ticket of state s >= R waits until every sum ticket of
+// state s - R (its slot's previous user, two phases earlier for R = 3) is
+// done.  Every ticket waits only for tickets handed out before it, whose
+// CTAs are resident and running, so the waits end (no cycle); each is
+// bounded anyway and, once one runs out, every later wait gives up at once
+// and the error word tells the host.
+struct TableSched {
+  int S, R;        // states, ring slots (R >= 2)
+  int npb, lpt;    // prep tickets per state, lines per prep ticket
+  int tps, nsplit; // tiles per state, parts per tile
+  long long nsum;  // sum tickets per state (tps * nsplit)
+  long long total; // S * (npb + nsum)
+};
+
+// ticket -> (kind, state, index) of the phase order above
+__host__ __device__ inline void table_ticket(const TableSched &sc, long long t, bool &prep, int &s,
+                                             long long &idx) {
+  const long long npb = sc.npb, nsum = sc.nsum, per = npb + nsum;
+  const long long k = npb < nsum ? npb : nsum;
+  if (t < npb) {  // phase 0: the first state's preps
+    prep = true;
+    s = 0;
+    idx = t;
+    return;
+  }
+  const long long u = t - npb;
+  const long long q = u / per;
+  if (q >= sc.S - 1) {  // phase S: the last state's sums
+    prep = false;
+    s = sc.S - 1;
+    idx = u - (long long)(sc.S - 1) * per;
+    return;
+  }
+  const int p = 1 + (int)q;
+  const long long r = u - q * per;
+  if (r < 2 * k) {
+    prep = (r & 1) != 0;
+    idx = r >> 1;
+  } else {
+    prep = nsum < npb;
+    idx = r - k;
+  }
+  s = prep ? p : p - 1;
+}
+
+constexpr int HK_TABLE_WAIT_POLLS = 1 << 22;  // x >= 256 ns: 1-4 s per wait
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// one thread: wait until *p >= v; false if the wait (or an earlier one) ran out
+__device__ bool wait_at_least(const unsigned *p, unsigned v, int *err) {
+  for (int it = 0; it < HK_TABLE_WAIT_POLLS; ++it) {
+    if (ld_acquire(p) >= v) return true;
+    if (*(volatile int *)err != 0) return false;
+    __nanosleep(256);
+  }
+  atomicExch(err, 1);
+  return false;
+}
+
+// The prep ticket's lines, out of line: the FP64 scaling and window searches
+// want more registers than the sum loop's budget, and keeping them in their
+// own function keeps their spills out of the sum loop.
+template <bool MIXED>
+__device__ __noinline__ void prep_lines(const LinesDev &L, const GridDev &g, const StateDev &st,
+                                        int64_t l, int64_t l1, int step, const double *e916,
+                                        void *out, double &w_loc, double &s1_loc) {
+  for (; l < l1; l += step) prep_record<MIXED, PREP_ALL>(L, g, st, l, e916, out, w_loc, s1_loc);
+}
+
+template <bool MIXED, class SH>
+__global__ void __launch_bounds__(SH::THREADS, MIXED ? SH::MINB : 2)
+voigt_table_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states, TableSched sc,
+                   void *ring, double *partial, unsigned *tile_cnt, unsigned long long *ticket,
+                   unsigned long long *wbits, unsigned *prep_cnt, unsigned *sum_cnt,
+                   unsigned *ready, TableFin *fin, int *err, double *__restrict__ K,
+                   int64_t k_stride) {
+  constexpr int G = SH::G, THREADS = SH::THREADS;
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  __shared__ long long s_ticket;
+  __shared__ int s_go;
+  __shared__ double s_e916[HK_SIG1_M];
+  const int tid = threadIdx.x;
+  const size_t rec_bytes = MIXED ? sizeof(LinePrepF) : sizeof(LinePrep);
+  const int64_t n = L.n;
+  if (tid < HK_SIG1_M) s_e916[tid] = c916_e(tid + 1);
+  for (;;) {
+    if (tid == 0) s_ticket = (long long)atomicAdd(ticket, 1ull);
+    __syncthreads();
+    const long long t = s_ticket;
+    if (t >= sc.total) break;
+    bool prep;
+    int s;
+    long long idx;
+    table_ticket(sc, t, prep, s, idx);
+    const int slot = s % sc.R;
+    if (tid == 0) {
+      bool go;
+      if (prep) go = s < sc.R || wait_at_least(sum_cnt + (s - sc.R), (unsigned)sc.nsum, err);
+      else go = wait_at_least(ready + s, 1u, err);
+      s_go = go;
     }
     __syncthreads();
-    const int64_t L0 = s_L0, L1 = s_L1;
-
-    float2 kf[PPL / 2];   // lane-local point indices, paired {p, p+1}
-    float2 a32[PPL / 2];  // mixed: FP32 sums of the current chunk (scaled)
-    double acc[PPL], xg[PPL];
-#pragma unroll
-    for (int p = 0; p < PPL; ++p) {
-      const int k = wb + lane + 32 * p;
-      acc[p] = 0.0;
-      if (MIXED) {
-        if (p & 1) {
-          kf[p >> 1].y = (float)k;
-          a32[p >> 1].y = 0.f;
-        } else {
-          kf[p >> 1].x = (float)k;
-          a32[p >> 1].x = 0.f;
-        }
-        cacc[k] = 0.0;  // owned by this lane only: no barrier needed
-      } else {
-        xg[p] = grid_x(g, g0 + k);
+    const bool go = s_go;
+    const StateDev &st = states[s];
+    void *ring_s = static_cast<char *>(ring) + (size_t)slot * n * rec_bytes;
+    if (prep) {
+      double w_loc = 0.0, s1_loc = 0.0;
+      if (go) {
+        const int64_t l0 = idx * sc.lpt, l1 = min(l0 + (int64_t)sc.lpt, n);
+        prep_lines<MIXED>(L, g, st, l0 + tid, l1, THREADS, s_e916, ring_s, w_loc, s1_loc);
       }
-    }
-
-    // Chunk c holds the lines L0 + c + q*nch (q < CH): every chunk spans
-    // the tile's whole line range, so the costly region-C points of its
-    // lines fall into all warp slices instead of one or two (consecutive
-    // nu-sorted lines would put a chunk's line cores into a single slice
-    // and leave the other warps idle at the barrier).
-    const int64_t nL = L1 - L0;
-    const int64_t nch = (nL + CH - 1) / CH;
-    const int64_t c_begin = nch * part / nsplit, c_end = nch * (part + 1) / nsplit;
-    int lcur = 0;  // strength level held in a32 (warp-uniform)
-    for (int64_t c = c_begin; c < c_end; ++c) {
-      const int cnt = (int)((nL - c + nch - 1) / nch);
-      if (MIXED) {
-        // build the records, then place them sorted by key (stable counting
-        // sort over the CH / 32 staging warps), so a warp's 32-line
-        // groups mostly hold one strength level
-        // (the key pass keeps no record: the record is rebuilt after the
-        // scan rather than held in registers across the barrier)
-        int key = HK_NKEY, rank = 0;
-        const int64_t l = L0 + c + (int64_t)tid * nch;
-        if (tid < cnt) key = line_key(PF, l, g0, g1, st.s1exp);
-        if (tid < CH) {
-          const unsigned lt = (1u << lane) - 1u;
-#pragma unroll
-          for (int v = 0; v < HK_NKEY; ++v) {
-            const unsigned m = __ballot_sync(0xffffffffu, key == v);
-            if (key == v) rank = __popc(m & lt);
-            if (lane == 0) s_kcnt[warp][v] = __popc(m);
-          }
-        }
-        __syncthreads();
-        if (tid < cnt) {
-          int pos = rank;
-          for (int v = 0; v < key; ++v)
-#pragma unroll
-            for (int w = 0; w < CH / 32; ++w) pos += s_kcnt[w][v];
-          for (int w = 0; w < warp; ++w) pos += s_kcnt[w][key];
-          RecF r;
-          stage_mixed(PF, g, l, g0, g1, st.s1exp, key, r);
-          reinterpret_cast<RecF *>(rec)[pos] = r;
-          if (r.c1 > r.c0 && r.i1 > r.i0) stage_rtab(r.y, Rtab + pos * HK_C916_MR);
-        }
-      } else if (tid < cnt) {
-        stage_plain(P, L0 + c + (int64_t)tid * nch, g0, g1, reinterpret_cast<RecD *>(rec) + tid);
+      for (int o = 16; o > 0; o >>= 1) {
+        w_loc = fmax(w_loc, __shfl_xor_sync(0xffffffffu, w_loc, o));
+        s1_loc = fmax(s1_loc, __shfl_xor_sync(0xffffffffu, s1_loc, o));
       }
-      __syncthreads();
-      if (MIXED) {
-        const RecF *rf = reinterpret_cast<const RecF *>(rec);
-        for (int g32 = 0; g32 < cnt; g32 += 32) {
-          const int j = g32 + lane;
-          const int cls = (j < cnt) ? classify<SLICE>(rf[j], wb) : HK_CLS_SKIP;
-          const int lev = (j < cnt) ? (rf[j].flags >> 8) : 0;
-          const unsigned bB = __ballot_sync(0xffffffffu, cls == HK_CLS_B);
-          const unsigned bA = __ballot_sync(0xffffffffu, cls == HK_CLS_A);
-          const unsigned bBM = __ballot_sync(0xffffffffu, cls == HK_CLS_BM);
-          const unsigned bAM = __ballot_sync(0xffffffffu, cls == HK_CLS_AM);
-          const unsigned bG = __ballot_sync(0xffffffffu, cls == HK_CLS_G);
-          unsigned mW = __ballot_sync(0xffffffffu, cls == HK_CLS_W);
-          unsigned live = bB | bA | bBM | bAM | bG;
-          while (live) {
-            // the lines of the current level first; switch level (flushing
-            // the FP32 sums) only when none of them is left
-            unsigned m = __ballot_sync(0xffffffffu, lev == lcur) & live;
-            if (m == 0u) {
-              flush_sums<PPL>(a32, cacc, wb, lane, st.s1exp, lcur);
-              lcur = __shfl_sync(0xffffffffu, lev, __ffs(live) - 1);
-              m = __ballot_sync(0xffffffffu, lev == lcur) & live;
-            }
-            live &= ~m;
-            unsigned mB = m & bB, mA = m & bA, mBM = m & bBM, mAM = m & bAM, mG = m & bG;
-            while (mB) {
-              const int b = __ffs(mB) - 1;
-              mB &= mB - 1;
-              sweep_B<PPL>(rf[g32 + b], kf, a32);
-            }
-            while (mA) {
-              const int b = __ffs(mA) - 1;
-              mA &= mA - 1;
-              sweep_A<false, PPL>(rf[g32 + b], wb, lane, kf, a32);
-            }
-            while (mBM) {
-              const int b = __ffs(mBM) - 1;
-              mBM &= mBM - 1;
-              sweep_BM<PPL>(rf[g32 + b], wb, lane, kf, a32);
-              sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
-            }
-            while (mAM) {
-              const int b = __ffs(mAM) - 1;
-              mAM &= mAM - 1;
-              sweep_A<true, PPL>(rf[g32 + b], wb, lane, kf, a32);
-            }
-            while (mG) {
-              const int b = __ffs(mG) - 1;
-              mG &= mG - 1;
-              sweep_G<false, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc);
-              sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
-            }
-          }
-          while (mW) {
-            const int b = __ffs(mW) - 1;
-            mW &= mW - 1;
-            sweep_G<true, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc);
-            sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
-          }
-        }
-        // at most one chunk of lines per FP32 sum
-        flush_sums<PPL>(a32, cacc, wb, lane, st.s1exp, lcur);
-      } else {
-        for (int j = 0; j < cnt; ++j)
-          sweep_plain<PPL>(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc, g, st);
-      }
-      __syncthreads();
-    }
-
-    double *Ks = K + (int64_t)s * k_stride;
-    if (nsplit == 1) {
-#pragma unroll
-      for (int p = 0; p < PPL; ++p) {
-        const int k = wb + lane + 32 * p;
-        const int64_t gi = g0 + k;
-        if (MIXED) acc[p] = cacc[k];
-        if (gi < g1) Ks[gi] = st.kmin + acc[p];
-      }
-    } else {
-      // Split tile: publish this part's sums; the CTA that completes the
-      // tile's count adds the parts in part order (the result does not
-      // depend on which CTA ran which part or when).
-      double *pt = partial + ((int64_t)tt * nsplit + part) * G;
-#pragma unroll
-      for (int p = 0; p < PPL; ++p) {
-        const int k = wb + lane + 32 * p;
-        if (MIXED) acc[p] = cacc[k];
-        pt[k] = acc[p];
+      if ((tid & 31) == 0) {
+        if (g.cutMode != 0) atomicMax(&wbits[2 * s], (unsigned long long)__double_as_longlong(w_loc));
+        atomicMax(&wbits[2 * s + 1], (unsigned long long)__double_as_longlong(s1_loc));
       }
       __threadfence();
       __syncthreads();
-      if (tid == 0) s_last = (atomicAdd(&tile_cnt[tt], 1u) == (unsigned)(nsplit - 1));
-      __syncthreads();
-      if (s_last) {
+      if (tid == 0 && atomicAdd(prep_cnt + s, 1u) == (unsigned)(sc.npb - 1)) {
+        // the last prep ticket of the state: every other one has published
         __threadfence();
-        const double *p0 = partial + (int64_t)tt * nsplit * G;
-#pragma unroll
-        for (int p = 0; p < PPL; ++p) {
-          const int k = wb + lane + 32 * p;
-          double sum = 0.0;
-          for (int j = 0; j < nsplit; ++j) sum += __ldcg(p0 + (int64_t)j * G + k);
-          const int64_t gi = g0 + k;
-          if (gi < g1) Ks[gi] = st.kmin + sum;
-        }
+        TableFin f;
+        state_scale(g, atomicAdd(&wbits[2 * s], 0ull), atomicAdd(&wbits[2 * s + 1], 0ull), f.wmax,
+                    f.s1exp);
+        f.pad = 0;
+        fin[s] = f;
+        __threadfence();
+        st_release(ready + s, 1u);
       }
+    } else {
+      if (go) {
+        const TableFin f = {__ldcg(&fin[s].wmax), __ldcg(&fin[s].s1exp), 0};
+        const int tile = (int)(idx / sc.nsplit), part = (int)(idx - (long long)tile * sc.nsplit);
+        const int64_t g0 = (int64_t)tile * G;
+        const int64_t g1 = min(g0 + (int64_t)G, g.nx);
+        const size_t tslot = (size_t)slot * sc.tps + tile;
+        sum_tile<MIXED, SH, true>(ring_s, L.nu0, n, g, st, f.wmax, f.s1exp, g0, g1, part, sc.nsplit,
+                                  partial + tslot * sc.nsplit * G, tile_cnt + tslot,
+                                  K + (int64_t)s * k_stride, smem_dyn);
+      }
+      // every record read of this ticket has completed: count it
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) atomicAdd(sum_cnt + s, 1u);
     }
   }
 }
@@ -978,6 +1199,104 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d
     return cudaGetLastError();
   });
   return e;
+}
+
+// The fused table kernel of (precision, shape) and its dynamic shared memory.
+template <class F>
+static cudaError_t with_table_kernel(bool mixed, int shape, F &&f) {
+  using KFn = void (*)(LinesDev, GridDev, const StateDev *, TableSched, void *, double *, unsigned *,
+                       unsigned long long *, unsigned long long *, unsigned *, unsigned *, unsigned *,
+                       TableFin *, int *, double *, int64_t);
+  if (!mixed) return f((KFn)voigt_table_kernel<false, Shape0>, sizeof(RecD) * Shape0::CH, Shape0::THREADS);
+  switch (shape) {
+#define HK_SHAPE_CASE(n) \
+  case n: return f((KFn)voigt_table_kernel<true, Shape##n>, smem_mixed<Shape##n>(), Shape##n::THREADS);
+    HK_SHAPE_CASE(0)
+    HK_SHAPE_CASE(1)
+    HK_SHAPE_CASE(2)
+    HK_SHAPE_CASE(3)
+    HK_SHAPE_CASE(4)
+    HK_SHAPE_CASE(5)
+    HK_SHAPE_CASE(6)
+#undef HK_SHAPE_CASE
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+TablePlan plan_table(bool mixed, int shape, int64_t nlines, int64_t nx, int nstates) {
+  TablePlan tp;
+  tp.shape = mixed ? shape : 0;
+  tp.G = voigt_tile_points(tp.shape);
+  tp.S = nstates;
+  // the preps of state s run beside the sums of state s - 1; a third slot
+  // gives the sums of state s - 3 a phase of slack before their slot is reused
+  tp.R = 3;
+  tp.slots = std::min(tp.R, nstates);
+  tp.lpt = 4096;
+  tp.npb = (int)std::max<int64_t>(1, (nlines + tp.lpt - 1) / tp.lpt);
+  tp.tps = (int)((nx + tp.G - 1) / tp.G);
+  tp.nsplit = voigt_nsplit(nx, tp.shape);
+  tp.nsum = (long long)tp.tps * tp.nsplit;
+  tp.total = (long long)nstates * (tp.npb + tp.nsum);
+  tp.ring_bytes = (size_t)tp.slots * (size_t)std::max<int64_t>(nlines, 1) * (mixed ? sizeof(LinePrepF) : sizeof(LinePrep));
+  tp.partial_doubles = tp.nsplit > 1 ? (size_t)tp.slots * tp.tps * tp.nsplit * tp.G : 0;
+  tp.counters = (size_t)tp.slots * tp.tps;
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  with_table_kernel(mixed, tp.shape, [&](auto kfn, size_t smem, int threads) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem);
+  });
+  tp.ctas = nsm * (per_sm < 1 ? 1 : per_sm);
+  return tp;
+}
+
+cudaError_t launch_voigt_table(bool mixed, const TablePlan &tp, const LinesDev &L, const GridDev &g,
+                               const StateDev *states_d, const TableBufs &b, double *K_d,
+                               int64_t k_stride, cudaStream_t stream) {
+  if (tp.S < 1 || tp.R < 2 || tp.slots != std::min(tp.R, tp.S)) return cudaErrorInvalidValue;
+  if (tp.G != voigt_tile_points(tp.shape)) return cudaErrorInvalidValue;
+  if (tp.nsplit > 1 && !b.partial) return cudaErrorInvalidValue;
+  // the counters, maxima and flags start from zero on every launch (replay)
+  cudaError_t e = cudaMemsetAsync(b.sync, 0, table_sync_bytes(tp.S), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b.tile_cnt, 0, sizeof(unsigned) * tp.counters, stream);
+  if (e != cudaSuccess) return e;
+  TableSched sc;
+  sc.S = tp.S;
+  sc.R = tp.R;
+  sc.npb = tp.npb;
+  sc.lpt = tp.lpt;
+  sc.tps = tp.tps;
+  sc.nsplit = tp.nsplit;
+  sc.nsum = tp.nsum;
+  sc.total = tp.total;
+  // the sync block: ticket, wbits[2S], fin[S], prep_cnt[S], sum_cnt[S], ready[S], err
+  char *q = static_cast<char *>(b.sync);
+  unsigned long long *ticket = reinterpret_cast<unsigned long long *>(q);
+  unsigned long long *wbits = ticket + 2;
+  TableFin *fin = reinterpret_cast<TableFin *>(wbits + 2 * (size_t)tp.S);
+  unsigned *prep_cnt = reinterpret_cast<unsigned *>(fin + tp.S);
+  unsigned *sum_cnt = prep_cnt + tp.S;
+  unsigned *ready = sum_cnt + tp.S;
+  int *err = reinterpret_cast<int *>(ready + tp.S);
+  const int ctas = (int)std::min<long long>(tp.ctas, tp.total);
+  return with_table_kernel(mixed, tp.shape, [&](auto kfn, size_t smem, int threads) {
+    if (smem > 48 * 1024) {
+      const cudaError_t ea = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (ea != cudaSuccess) return ea;
+    }
+    kfn<<<ctas, threads, smem, stream>>>(L, g, states_d, sc, b.ring, b.partial, b.tile_cnt, ticket, wbits,
+                                         prep_cnt, sum_cnt, ready, fin, err, K_d, k_stride);
+    return cudaGetLastError();
+  });
+}
+
+int *table_error_word(void *sync_d, int nstates) {
+  char *q = static_cast<char *>(sync_d);
+  return reinterpret_cast<int *>(q + 16 + 16 * (size_t)nstates + sizeof(TableFin) * (size_t)nstates +
+                                 12 * (size_t)nstates);
 }
 
 cudaError_t launch_profile_eval(int64_t n, const double *x_d, const double *y_d,

@@ -23,7 +23,7 @@ HEADER_PATH = os.path.join(os.path.dirname(os.path.dirname(_PKG)), "include", "h
 HK_OK = 0
 STATUS_NAMES = {0: "HK_OK", -1: "HK_ERR_ARG", -2: "HK_ERR_IO", -3: "HK_ERR_FORMAT",
                 -4: "HK_ERR_RANGE", -5: "HK_ERR_CUDA", -6: "HK_ERR_STATE",
-                -7: "HK_ERR_NOMEM", -8: "HK_ERR_UNSUPPORTED"}
+                -7: "HK_ERR_NOMEM", -8: "HK_ERR_UNSUPPORTED", -9: "HK_ERR_TIMEOUT"}
 PLAIN_FP64 = 0
 MIXED = 1
 HITRAN = 0
@@ -76,8 +76,10 @@ def lib():
             "hk_set_line_scales": (_i, [_p, _p, _p]),
             "hk_set_workspace": (_i, [_p, _d, _d]),
             "hk_opacity_vjp": (_i, [_p, _d, _d, _i, _p, _i, _p, _p, _p, _p, _i, _p]),
+            "hk_opacity_vjp_log": (_i, [_p, _d, _d, _i, _p, _i, _p, _p, _p, _p, _i, _p]),
             "hk_table_build": (_i, [_p, _i, _p, _p, _i, _p, _i, _d, _p, _p]),
             "hk_table_run": (_i, [_p, _p]),
+            "hk_table_status": (_i, [_p, _p]),
             "hk_table_free": (_i, [_p]),
             "hk_table_kernels": (_i64, [_p]),
             "hk_last_launches": (_i64, [_p]),
@@ -339,19 +341,28 @@ class Context:
         g = None if g_scale is None else _f64(g_scale)
         self._chk(lib().hk_set_line_scales(self._h, _ptr(s), _ptr(g)))
 
-    def opacity_vjp(self, T, P, u, precision=MIXED, per_line=True, stream=None):
+    def opacity_vjp(self, T, P, u, precision=MIXED, per_line=True, stream=None, log_gamma=False,
+                    device_out=False):
         """dLoss/dT, dLoss/dP and (per_line) dLoss/dlog S, dLoss/dgammaL for
-        the seed u = dLoss/dK (Nx values; numpy or CUDA tensor)."""
+        the seed u = dLoss/dK (Nx values; numpy or CUDA tensor).  log_gamma:
+        the width gradient per log gammaL instead (hk_opacity_vjp_log);
+        device_out: the per-line results as CUDA tensors (no host copy)."""
         dev = _is_dev(u)
         if not dev:
             u = _f64(u)
         n = self.num_lines
         dT, dP = C.c_double(0), C.c_double(0)
-        dS = np.empty(n, np.float64) if per_line else None
-        dG = np.empty(n, np.float64) if per_line else None
-        sh = _stream_handle(stream, dev)
-        self._chk(lib().hk_opacity_vjp(self._h, float(T), float(P), precision, _ptr(u), int(dev),
-                                       C.byref(dT), C.byref(dP), _ptr(dS), _ptr(dG), 0, sh))
+        if device_out:
+            import torch
+            mk = lambda: torch.empty(n, dtype=torch.float64, device=torch.device("cuda", self.device))
+        else:
+            mk = lambda: np.empty(n, np.float64)
+        dS = mk() if per_line else None
+        dG = mk() if per_line else None
+        sh = _stream_handle(stream, dev or device_out)
+        fn = lib().hk_opacity_vjp_log if log_gamma else lib().hk_opacity_vjp
+        self._chk(fn(self._h, float(T), float(P), precision, _ptr(u), int(dev), C.byref(dT),
+                     C.byref(dP), _ptr(dS), _ptr(dG), int(device_out), sh))
         return dT.value, dP.value, dS, dG
 
     # ---------------------------------------------------------- tables
@@ -373,6 +384,11 @@ class Context:
     def table_run(self, stream=None):
         """Replay the recorded table (one graph launch, asynchronous)."""
         self._chk(lib().hk_table_run(self._h, _stream_handle(stream, True)))
+
+    def table_status(self, stream=None):
+        """Synchronise the stream; raises HkError (status -9) if a bounded
+        wait inside the last table run ran out (its results incomplete)."""
+        self._chk(lib().hk_table_status(self._h, _stream_handle(stream, True)))
 
     def table_free(self):
         self._chk(lib().hk_table_free(self._h))

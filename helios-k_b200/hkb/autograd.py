@@ -11,7 +11,6 @@ comes from libhkb's kernels.
 """
 from __future__ import annotations
 
-import numpy as np
 import torch
 
 import hkb
@@ -44,20 +43,18 @@ class Opacity(torch.autograd.Function):
         Tf, Pf, prec = ctx.state
         s, g = ctx.scales
         hk.set_line_scales(s, g)  # the context may have served other calls since
-        dT, dP, dS, dG = hk.opacity_vjp(Tf, Pf, gK.detach().to(torch.float64).contiguous(), prec)
-        # d/dlog g = gammaL * dLoss/dgammaL, gammaL = vy / iad of this state
-        _, _, iad, vy, _ = hk.state_lines(Tf, Pf)
-        aL_sorted = np.where(iad > 0, vy / np.where(iad > 0, iad, 1.0), 0.0)
-        aL = np.empty_like(aL_sorted)
-        aL[hk.line_order()] = aL_sorted
+        # per-line gradients per log S and per log gammaL, left on the GPU
+        dT, dP, dS, dG = hk.opacity_vjp(Tf, Pf, gK.detach().to(torch.float64).contiguous(), prec,
+                                        log_gamma=True, device_out=True)
+
         def like(v, meta):
             dt, dev = meta
-            return torch.as_tensor(np.asarray(v), dtype=dt).to(dev)
+            return torch.as_tensor(v, dtype=dt, device=dev)
 
         need = ctx.needs_input_grad
         m = ctx.meta
         gT = like(dT, m[0]) if need[1] else None
         gP = like(dP, m[1]) if need[2] else None
-        gS = like(dS, m[2]) if need[3] else None
-        gG = like(dG * aL, m[3]) if need[4] else None
+        gS = dS.to(dtype=m[2][0], device=m[2][1]) if need[3] else None
+        gG = dG.to(dtype=m[3][0], device=m[3][1]) if need[4] else None
         return None, gT, gP, gS, gG, None

@@ -42,7 +42,8 @@ enum {
   HK_ERR_CUDA = -5,        /* CUDA runtime error                        */
   HK_ERR_STATE = -6,       /* call order (e.g. no grid set)             */
   HK_ERR_NOMEM = -7,       /* device or host allocation failed          */
-  HK_ERR_UNSUPPORTED = -8  /* option outside this build's scope        */
+  HK_ERR_UNSUPPORTED = -8, /* option outside this build's scope        */
+  HK_ERR_TIMEOUT = -9      /* a bounded wait on the GPU ran out         */
 };
 
 enum { HK_PRECISION_PLAIN_FP64 = 0, HK_PRECISION_MIXED = 1 };
@@ -290,25 +291,40 @@ hk_status hk_opacity_vjp(hk_ctx *ctx, double T, double P, int precision, const d
                          int u_on_device, double *dT, double *dP, double *dlogS,
                          double *dgammaL, int outputs_on_device, void *stream);
 
+/* The same vector-Jacobian product with the per-line width gradient taken
+ * per log gammaL (dLoss/dlog gammaL = gammaL dLoss/dgammaL, gammaL of this
+ * state with its line scale): the natural parameters of a fit of per-line
+ * multipliers exp(log g).  With outputs_on_device the per-line results stay
+ * on the GPU (no host round trip).  No counterpart in the reference. */
+hk_status hk_opacity_vjp_log(hk_ctx *ctx, double T, double P, int precision, const double *u,
+                             int u_on_device, double *dT, double *dP, double *dlogS,
+                             double *dlogGammaL, int outputs_on_device, void *stream);
+
 /* ------------------------------------------------------------ tables */
 
-/* A whole T-P table as one CUDA graph: the line scaling, Voigt sums and
- * k-distribution fits of all nstates states (in batches sized to the
- * context's workspace budget, each batch one persistent Voigt launch),
- * recorded once by hk_table_build and replayed by hk_table_run as a single
- * graph launch.  K (nstates x Nx), coeff (nstates x nbins x nC) and nxmin
+/* A whole T-P table as one CUDA graph of two kernels: one persistent launch
+ * scales the lines to every state (records in a ring of per-state slots)
+ * and sums every state's Voigt profiles, as tickets of one counter (the
+ * line prep of a state before its sums, a slot reused once the sums of its
+ * previous state are done); one k-distribution launch then fits all states.
+ * hk_table_build records it once; hk_table_run replays it with one graph
+ * launch.  K (nstates x Nx), coeff (nstates x nbins x nC) and nxmin
  * (nstates x nbins) are DEVICE buffers owned by the caller that must stay
  * valid while the table exists; hk_table_build allocates all workspace and
  * synchronises the device; hk_table_run is asynchronous on `stream`.  The
  * results equal those of hk_opacity + hk_kdist on the same states.  A new
- * hk_table_build, hk_table_free or hk_destroy drops the graph; other calls on
- * the same context between runs reuse its workspace, so rebuild after them.
+ * hk_table_build, hk_table_free or hk_destroy drops the graph; other calls
+ * on the same context between runs reuse its workspace, so rebuild after
+ * them.  The kernel's waits for other tickets are bounded: hk_table_status
+ * synchronises `stream` and returns HK_ERR_TIMEOUT if one of the last run's
+ * ran out (its results are then incomplete), else HK_OK.
  * Replaces the reference's one-state-per-run loop (heliosk.cu:1051-2193 run
  * once per pressure of the PFile). */
 hk_status hk_table_build(hk_ctx *ctx, int nstates, const double *T, const double *P,
                          int precision, double *K, int nC, double unitScale,
                          double *coeff, int32_t *nxmin);
 hk_status hk_table_run(hk_ctx *ctx, void *stream);
+hk_status hk_table_status(hk_ctx *ctx, void *stream);
 hk_status hk_table_free(hk_ctx *ctx);
 /* kernels recorded in the table graph */
 int64_t hk_table_kernels(const hk_ctx *ctx);

@@ -283,14 +283,14 @@ def test_table_graph_equals_opacity_and_kdist(small):
     coeff = torch.empty((ns, NBINS, nC), dtype=torch.float64, device=dev)
     nxmin = torch.empty((ns, NBINS), dtype=torch.int32, device=dev)
     ctx.table_build(Ts, Ps, K, coeff, nxmin, nC=nC)
-    assert ctx.table_kernels >= 4
+    assert ctx.table_kernels == 2   # one persistent table launch + one fit launch
     ctx.table_run()
-    torch.cuda.synchronize()
+    ctx.table_status()
     K1, c1, n1 = K.cpu().numpy(), coeff.cpu().numpy(), nxmin.cpu().numpy()
     K.zero_()
     coeff.zero_()
     ctx.table_run()
-    torch.cuda.synchronize()
+    ctx.table_status()
     assert np.array_equal(K.cpu().numpy(), K1)
     assert np.array_equal(coeff.cpu().numpy(), c1)
     ctx.table_free()
