@@ -96,6 +96,7 @@ struct hk_ctx {
   cudaGraphExec_t table_exec = nullptr;
   int64_t table_kernels = 0;
   int table_states = 0;
+  int table_fused = 0;  // hk_set_table_mode: 1 = one persistent launch for the table's sums
   DevBuf tsync;  // the table kernel's counters, flags and per-state scales
 };
 
@@ -577,7 +578,7 @@ static hk_status opacity_sectioned(hk_ctx *c, int nstates, bool mixed, int shape
 // grid or options change.  Its probe outputs land in K rows the call then
 // overwrites.
 static int shape_for(const hk_ctx *c, bool mixed) {
-  if (!mixed) return 0;
+  if (!mixed || c->g.profile >= 3) return 0;  // the Gaussian profiles' kernels: shape 0
   return (c->tuning != 0 && c->tuned) ? c->tuned_shape : c->shape_fixed;
 }
 
@@ -727,16 +728,17 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   }
   // States run in batches whose per-(state, line) records fit the prep
   // budget; each batch is one prep launch and one persistent Voigt launch.
-  // profiles 3-4, plinth removal and sub-Lorentzian wings run the FP64 form
-  // (the mixed form's FP32 sums hold the Voigt regions; the Lorentz profile
-  // is its region A over the whole window)
-  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile <= 2 && !c->g.plinth && !c->g.subL;
+  // plinth removal and sub-Lorentzian wings run the FP64 form; the mixed
+  // form holds the Voigt regions, the Lorentz profile (its region A over the
+  // whole window) and the Doppler and binned-Gaussian profiles (region A, cut
+  // to where their FP32 terms are normal floats)
+  const bool mixed = precision == HK_PRECISION_MIXED && !c->g.plinth && !c->g.subL;
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
   c->voigt_ms_acc_only = false;
   c->launches = 0;
-  if (mixed && c->tuning != 0 && !c->tuned && per_state <= c->prep_budget && c->nlines > 0)
+  if (mixed && c->g.profile <= 2 && c->tuning != 0 && !c->tuned && per_state <= c->prep_budget && c->nlines > 0)
     if ((st = tune_shape(c, nstates, hs, Kd, s)) != HK_OK) return st;
   const int shape = shape_for(c, mixed);
   c->last_shape = shape;
@@ -1124,6 +1126,96 @@ hk_status hk_opacity_vjp_log(hk_ctx *c, double T, double P, int precision, const
 }
 
 // ---------------------------------------------------------------- tables
+// Two ways to record a table, with the same bits: the per-batch launches
+// (line prep, scale, Voigt sum per batch of states whose records fit the
+// workspace; the default, the faster one measured on the 1e7-line, 600-state
+// table: 28.6 ms per state against 30.1) and, with hk_set_table_mode(ctx, 1),
+// one persistent launch for every state's line prep and sums (two kernels in
+// the graph).  Tables of fewer states than this always take the per-batch
+// launches: the fused launch can only hide a state's line prep behind
+// another state's sums (one 1e7-line state: 31.1 ms per-batch, 32.8 fused).
+constexpr int HK_TABLE_FUSED_MIN = 4;
+
+hk_status hk_set_table_mode(hk_ctx *c, int fused) {
+  if (!c) return HK_ERR_ARG;
+  if (fused != 0 && fused != 1) return fail(c, HK_ERR_ARG, "table mode must be 0 (per batch) or 1 (fused)");
+  c->table_fused = fused;
+  ok(c);
+  return HK_OK;
+}
+
+static hk_status table_build_batched(hk_ctx *c, int nstates, bool mixed, int shape, double *K, int nC,
+                                     double unitScale, double *coeff, int32_t *nxmin) {
+  const int64_t nx = c->g.nx;
+  const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
+  if (per_state > c->prep_budget)
+    return fail(c, HK_ERR_UNSUPPORTED, "one state's line records (%zu B) exceed the workspace (%zu B): "
+                "tables of such lists run through hk_opacity's sectioned path", per_state, c->prep_budget);
+  int batch = (int)std::max<size_t>(1, c->prep_budget / per_state);
+  const int nsplit = voigt_nsplit(nx, shape);
+  if (nsplit > 1) {
+    const int G = voigt_tile_points(shape);
+    const size_t part_per_state = (size_t)((nx + G - 1) / G) * nsplit * G * sizeof(double);
+    batch = std::min(batch, (int)std::max<size_t>(1, c->part_budget / part_per_state));
+  }
+  batch = std::min(batch, nstates);
+  CUDA_TRY(c, c->prep.ensure((size_t)batch * per_state));
+  const VoigtPlan plan0 = plan_voigt_sum(mixed, shape, nx, batch, 0);
+  if (plan0.nsplit > 1) {
+    CUDA_TRY(c, c->vpart.ensure(plan0.partial_doubles * sizeof(double)));
+    CUDA_TRY(c, c->vcnt.ensure(plan0.counters * sizeof(unsigned)));
+  }
+  hk_status st;
+  if ((st = ensure_qr(c, nC, 0)) != HK_OK) return st;
+  const size_t nscr = kdist_scratch_doubles(c->nxb, c->nbins, nstates);
+  if (nscr) CUDA_TRY(c, c->scratch.ensure(nscr * sizeof(double)));
+  CUDA_TRY(c, c->tsync.ensure(table_sync_bytes(nstates)));
+  CUDA_TRY(c, cudaMemset(c->tsync.p, 0, table_sync_bytes(nstates)));  // no waits: status stays OK
+  CUDA_TRY(c, cudaDeviceSynchronize());
+  cudaStream_t cs = nullptr;
+  CUDA_TRY(c, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+  StateDev *sd = c->states.as<StateDev>();
+  unsigned long long *wb = c->wbits.as<unsigned long long>();
+  int64_t kernels = 0;
+  for (int b0 = 0; e == cudaSuccess && b0 < nstates; b0 += batch) {
+    const int nb = std::min(batch, nstates - b0);
+    const VoigtPlan plan = plan_voigt_sum(mixed, shape, nx, nb, plan0.ctas);
+    e = launch_line_prep(mixed, c->L, c->g, sd + b0, nb, c->prep.p, wb + 2 * b0, cs);
+    if (e == cudaSuccess)
+      e = launch_voigt_sum(mixed, plan, c->prep.p, c->L.nu0, c->nlines, c->g, sd + b0,
+                           c->ticket.as<unsigned>(), c->vpart.as<double>(), c->vcnt.as<unsigned>(),
+                           K + (size_t)b0 * nx, nx, cs);
+    kernels += 3;  // line prep, state scale, Voigt sum
+  }
+  if (e == cudaSuccess) {
+    e = launch_kdist(K, nx, nstates, c->nxb, c->nbins, nC, c->kmin, unitScale, c->qrV.as<double>(),
+                     c->qrC.as<double>(), c->qrD.as<double>(), coeff, nxmin, nullptr, nullptr,
+                     nscr ? c->scratch.as<double>() : nullptr, cs);
+    kernels += 1;
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+  cudaStreamDestroy(cs);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return fail(c, HK_ERR_CUDA, "recording the table graph: %s",
+                cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  cudaGraphExec_t x = nullptr;
+  e = cudaGraphInstantiate(&x, g, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(c, HK_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+  }
+  c->table_graph = g;
+  c->table_exec = x;
+  c->table_kernels = kernels;
+  c->table_states = nstates;
+  ok(c);
+  return HK_OK;
+}
+
 hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *P,
                          int precision, double *K, int nC, double unitScale, double *coeff,
                          int32_t *nxmin) {
@@ -1148,18 +1240,21 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   CUDA_TRY(c, c->wbits.ensure(2 * nstates * sizeof(unsigned long long)));
   CUDA_TRY(c, cudaMemcpy(c->states.p, hs.data(), nstates * sizeof(StateDev), cudaMemcpyHostToDevice));
   const int64_t nx = c->g.nx;
-  // profiles 3-4, plinth removal and sub-Lorentzian wings run the FP64 form
-  // (the mixed form's FP32 sums hold the Voigt regions; the Lorentz profile
-  // is its region A over the whole window)
-  const bool mixed = precision == HK_PRECISION_MIXED && c->g.profile <= 2 && !c->g.plinth && !c->g.subL;
+  // plinth removal and sub-Lorentzian wings run the FP64 form; the mixed
+  // form holds the Voigt regions, the Lorentz profile (its region A over the
+  // whole window) and the Doppler and binned-Gaussian profiles (region A, cut
+  // to where their FP32 terms are normal floats)
+  const bool mixed = precision == HK_PRECISION_MIXED && !c->g.plinth && !c->g.subL;
   c->launches = 0;
-  if (mixed && c->tuning != 0 && !c->tuned && c->nlines > 0 &&
+  if (mixed && c->g.profile <= 2 && c->tuning != 0 && !c->tuned && c->nlines > 0 &&
       (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(true) <= c->prep_budget) {
     if ((st = tune_shape(c, nstates, hs, K, 0)) != HK_OK) return st;
     CUDA_TRY(c, cudaDeviceSynchronize());
   }
   const int shape = shape_for(c, mixed);
   c->last_shape = shape;
+  if (!c->table_fused || nstates < HK_TABLE_FUSED_MIN)
+    return table_build_batched(c, nstates, mixed, shape, K, nC, unitScale, coeff, nxmin);
   // one persistent launch for the whole table: line prep into a ring of
   // per-state record slots and every state's Voigt sums (hkb_voigt.cu)
   const TablePlan tp = plan_table(mixed, shape, c->nlines, nx, nstates);

@@ -362,15 +362,18 @@ __device__ __forceinline__ double c916_e(int m) {
   const double a = (double)HK_A916_F;
   return exp(-(a * a * m * m));
 }
-// e[m-1] = c916_e(m) (a line-independent table, e.g. in shared memory)
+// e[m-1] = c916_e(m) (a line-independent table, e.g. in shared memory).
+// Each term takes the correctly rounded reciprocal of its denominator
+// (__drcp_rn, a few instructions) times e_m instead of an FP64 division;
+// the sum is rounded to FP32 for the region-C evaluator.
 __device__ __forceinline__ double c916_sig1_tab(double y, const double *__restrict__ e) {
   const double a = (double)HK_A916_F;
   const double y2 = y * y;
   double s = 0.0;
-#pragma unroll 1
+#pragma unroll 4
   for (int m = 1; m <= HK_SIG1_M; ++m) {
     const double am2 = a * a * m * m;
-    s += e[m - 1] / (am2 + y2);
+    s = __fma_rn(e[m - 1], __drcp_rn(am2 + y2), s);
   }
   return s;
 }

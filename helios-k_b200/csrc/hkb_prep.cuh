@@ -32,15 +32,16 @@ __device__ __forceinline__ void prep_record(const LinesDev &L, const GridDev &g,
   const LineState ls = prep_line(L, st, l);
   int64_t w[6];
   line_windows(g, st, ls, 0, g.nx, w);
-  // S1 per profile (S3_kernel voigt.h:452-463); the mixed form runs profiles 1-2
+  // S1 per profile (S3_kernel voigt.h:452-463)
   const double Sc = ls.S * (1.0 / 1.7724538509055160273);
-  const double S1 = (MIXED || g.profile <= 2) ? ls.S * ls.vy / CUDART_PI
-                                              : (g.profile == 3 ? Sc : ls.S);
+  const double S1 = g.profile <= 2 ? ls.S * ls.vy / CUDART_PI : (g.profile == 3 ? Sc : ls.S);
   const bool hasC = w[3] > w[2];
   // largest region-A/B term of the line: S1 / r^2 with r^2 >= max(100, y^2)
-  // (Voigt: region C covers r < 10), r^2 >= y^2 for the Lorentz profile
+  // (Voigt: region C covers r < 10), r^2 >= y^2 for the Lorentz profile;
+  // S1 for the Doppler profile, S1 / (2 vb) erf(vb / 2) < S1 / sqrt(pi) for
+  // the binned Gaussian
   const double Y = ls.vy * ls.vy;
-  const double rmin = g.profile == 2 ? Y : fmax(100.0, Y);
+  const double rmin = g.profile == 2 ? Y : (g.profile >= 3 ? 1.0 : fmax(100.0, Y));
   const double term = rmin > 0.0 ? S1 / rmin : 0.0;
   if (MODE == PREP_STATS) {
   } else if (MIXED) {
@@ -64,7 +65,7 @@ __device__ __forceinline__ void prep_record(const LinesDev &L, const GridDev &g,
     if (term > 0.0) frexp(term, &ex);
     r.ex = ex;
     int flags = 0;
-    if (w[5] > w[0]) {
+    if (w[5] > w[0] && g.profile <= 2) {
       // the largest |x| inside the cut window (at its first or last point)
       const double xa = fabs((grid_x(g, w[0]) - ls.nu) * ls.iad);
       const double xb = fabs((grid_x(g, w[5] - 1) - ls.nu) * ls.iad);

@@ -92,6 +92,19 @@ struct __align__(16) RecF {
 };
 static_assert(sizeof(RecF) == 112, "RecF layout");
 
+// Profiles 3 (Doppler) and 4 (binned Gaussian) have no regions B and C, so
+// their records reuse the GH2 slots: the FP64 offset D0 at the tile start
+// and the FP64 grid step vb (Doppler units) in C0..D2 and D1..D0, and, for
+// the binned Gaussian, the half step vb / 2 in C1.
+__device__ __forceinline__ void gauss_put(RecF &r, double D0, double vb, float h) {
+  double *d = reinterpret_cast<double *>(&r.C0);
+  d[0] = D0;
+  d[1] = vb;
+  r.C1 = h;
+}
+__device__ __forceinline__ double gauss_D0(const RecF &r) { return reinterpret_cast<const double *>(&r.C0)[0]; }
+__device__ __forceinline__ double gauss_vb(const RecF &r) { return reinterpret_cast<const double *>(&r.C0)[1]; }
+
 // Strength levels: with 2^(40 - s1exp) the state's largest region-A/B term
 // S1 / max(100, Y), a line of level lev = (40 - ex - s1exp) / 96 (ex: the
 // exponent of its own largest term) gets S1f = S1 * 2^(s1exp + 96 lev), which
@@ -207,7 +220,7 @@ __device__ __forceinline__ int line_key(const LinePrepF *__restrict__ P, int64_t
   return lev;
 }
 
-template <bool CG>
+template <bool CG, bool G34>
 __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, const GridDev &g,
                                             int64_t l, int64_t g0, int64_t g1, int s1exp,
                                             int key, RecF &r) {
@@ -252,6 +265,32 @@ __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, con
   r.t1 = clip_local(lp.t1, g0, g1);
   r.flags = ((lp.flags & HK_PF_WIDE) ? HK_F_WIDE : 0) | (weak ? HK_F_WEAK : 0) | (lev << 8);
   r.iy = lp.y > 0.f ? (float)(1.0 / (double)lp.y) : 0.f;
+  if (G34) {
+    // Doppler / binned Gaussian: S1f exp(-u^2) with u = |x| (- vb / 2) is a
+    // normal float only for u^2 <= (126 + e) ln 2 (S1f < 2^e): the points
+    // beyond add exactly 0 in FP32 (flush to zero), as in the reference's
+    // FP32 kernels, so the window is cut to the rest.  Weak lines (FP64
+    // sums) keep their whole window.
+    const double h = g.profile == 4 ? 0.5 * vb : 0.0;
+    if (g.profile == 4 && !weak) {
+      // (erf(x + h) - erf(x - h)) / (2 vb) folded into the strength
+      r.S1f = (float)(S1f / (2.0 * vb));
+    }
+    gauss_put(r, D0, vb, (float)h);
+    if (!weak && nonempty) {
+      int e = 0;
+      frexp((double)r.S1f, &e);
+      const double u2 = (double)max(0, 126 + e) * 0.69314718055994531;
+      const double xd = sqrt(u2) + h + 1e-6;
+      // tile points k with |D0 + k vb| <= xd
+      const double ka = ceil((-xd - D0) / vb), kb = floor((xd - D0) / vb) + 1.0;
+      const int k0 = (int)fmin(fmax(ka, 0.0), (double)(g1 - g0));
+      const int k1 = (int)fmin(fmax(kb, 0.0), (double)(g1 - g0));
+      r.i0 = max(r.i0, k0);
+      r.i1 = min(r.i1, k1);
+      r.b0 = r.c0 = r.c1 = r.b1 = r.i0;  // region A only
+    }
+  }
 }
 
 // region C inside the tile: denominators of the Algorithm-916 series
@@ -449,6 +488,54 @@ __device__ __forceinline__ void sweep_A(const RecF &rr, int wb, int lane,
   }
 }
 
+// Profiles 3 and 4 (Doppler, binned Gaussian), the points of [lo, hi) in
+// the slice: S1f exp(-x^2) and S1f (erf(x + h) - erf(x - h)) (S1f carrying
+// 1 / (2 vb)), FP32 but for the Gaussian's exponent: x^2 log2(e) = n + f is
+// formed in FP64 from the FP64 offset, so 2^-f (MUFU) and the exponent
+// 2^(e - n) of S1f 2^-n keep the term's FP32 accuracy at any |x|.  The
+// binned Gaussian takes, on the side of x away from zero, erfc(u) - erfc(v)
+// = e^-u^2 (erfcx(u) - erfcx(v) e^(u^2 - v^2)), u = |x| - h, v = |x| + h (no
+// cancellation in the wings), and erf(x + h) - erf(x - h) near the centre.
+__device__ __forceinline__ float gauss_scaled(double u, float mS, int eS) {
+  const double q = u * u * 1.4426950408889634;  // u^2 log2(e)
+  const double n = rint(q);
+  const float f = (float)(q - n);
+  const int et = eS - (int)n;
+  const float sc = et >= -126 ? __int_as_float((et + 127) << 23) : 0.f;
+  return mS * ex2_fast(-f) * sc;
+}
+
+template <bool AM, int PPL>
+__device__ __forceinline__ void sweep_G34(const RecF &rr, int profile, int wb, int lane,
+                                          const float2 (&kf)[PPL / 2], float2 (&a32)[PPL / 2]) {
+  const int lo = max(rr.i0, wb), hi = min(rr.i1, wb + 32 * PPL);
+  const double D0 = gauss_D0(rr), vb = gauss_vb(rr);
+  const float h = rr.C1;
+  int eS = 0;
+  const float mS = 2.0f * frexpf(rr.S1f, &eS);  // S1f = mS 2^(eS - 1), mS in [1, 2)
+  eS -= 1;
+#pragma unroll
+  for (int p = 0; p < PPL; ++p) {
+    const int k = wb + lane + 32 * p;
+    if (AM && !(k >= lo && k < hi)) continue;
+    const float kk = (p & 1) ? kf[p >> 1].y : kf[p >> 1].x;
+    const double x = fabs(fma((double)kk, vb, D0));
+    float t;
+    if (profile == 3) {
+      t = gauss_scaled(x, mS, eS);
+    } else if (x > (double)h) {
+      const float u = (float)(x - (double)h), v = (float)(x + (double)h);
+      const float w = fmaf(-erfcxf(v), ex2_fast(-4.0f * 1.4426950408889634f * (float)x * h), erfcxf(u));
+      t = gauss_scaled(x - (double)h, mS, eS) * w;
+    } else {
+      const float xf = (float)x;
+      t = rr.S1f * (erff(xf + h) - erff(xf - h));
+    }
+    if (p & 1) a32[p >> 1].y += t;
+    else a32[p >> 1].x += t;
+  }
+}
+
 // Region C points of the slice, summed in FP64 into cacc, lanes packed by
 // evaluator so a warp never runs both: [t0, t1) holds |x| < sqrt(36 - y^2)
 // (Algorithm 916), the rest of [lo, hi) has r >= 6 (asymptotic series).  The
@@ -484,11 +571,25 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
 // A/B boundaries in the slice, and weak lines: per-point window/region
 // tests.  WEAK lines (S1f = 1) add S1 t in FP64 to cacc; the others add
 // S1f t to the FP32 sums.
-template <bool WEAK, int PPL>
+template <bool WEAK, bool G34, int PPL>
 __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
                                         const float2 (&kf)[PPL / 2],
                                         float2 (&a32)[PPL / 2],
-                                        double *__restrict__ cacc) {
+                                        double *__restrict__ cacc, int profile) {
+  if (WEAK && G34) {
+    // Doppler / binned Gaussian lines summed in FP64: the FP64 form's term
+    const double D0 = gauss_D0(r), vb = gauss_vb(r);
+    const double S1 = profile == 3 ? r.Sc : r.Sc * 1.7724538509055160273;  // S / sqrt(pi), S
+#pragma unroll
+    for (int p = 0; p < PPL; ++p) {
+      const int k = wb + lane + 32 * p;
+      if (k >= r.i0 && k < r.i1) {
+        const float kk = (p & 1) ? kf[p >> 1].y : kf[p >> 1].x;
+        cacc[k] += profile_a_d(profile, fma((double)kk, vb, D0), 0.0, S1, vb);
+      }
+    }
+    return;
+  }
   // the record lives in shared memory like cacc: read it once into registers
   const int i0 = r.i0, i1 = r.i1, b0 = r.b0, b1 = r.b1, c0 = r.c0, c1 = r.c1;
   const float nkc = r.nkc, vb = r.vb, fr = r.fr;
@@ -607,7 +708,7 @@ __device__ __forceinline__ void flush_sums(float2 (&a32)[PPL / 2], double *__res
 // split tile, published to pt (this tile's nsplit partial rows of G points)
 // and combined in part order by the CTA that completes the count *cnt.
 // wmax and s1exp are the state's search half-width and FP32 scale exponent.
-template <bool MIXED, class SH, bool CG>
+template <bool MIXED, class SH, bool CG, bool G34 = false>
 __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__restrict__ nu0,
                                          int64_t nlines, const GridDev &g, const StateDev &st,
                                          double wmax, int s1exp, int64_t g0, int64_t g1, int part,
@@ -701,7 +802,7 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
           for (int w = 0; w < CH / 32; ++w) pos += s_kcnt[w][v];
         for (int w = 0; w < warp; ++w) pos += s_kcnt[w][key];
         RecF r;
-        stage_mixed<CG>(PF, g, l, g0, g1, s1exp, key, r);
+        stage_mixed<CG, G34>(PF, g, l, g0, g1, s1exp, key, r);
         reinterpret_cast<RecF *>(rec)[pos] = r;
         if (r.c1 > r.c0 && r.i1 > r.i0) stage_rtab(r.y, Rtab + pos * HK_C916_MR);
       }
@@ -741,7 +842,8 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
           while (mA) {
             const int b = __ffs(mA) - 1;
             mA &= mA - 1;
-            sweep_A<false, PPL>(rf[g32 + b], wb, lane, kf, a32);
+            if constexpr (G34) sweep_G34<false, PPL>(rf[g32 + b], g.profile, wb, lane, kf, a32);
+            else sweep_A<false, PPL>(rf[g32 + b], wb, lane, kf, a32);
           }
           while (mBM) {
             const int b = __ffs(mBM) - 1;
@@ -752,19 +854,20 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
           while (mAM) {
             const int b = __ffs(mAM) - 1;
             mAM &= mAM - 1;
-            sweep_A<true, PPL>(rf[g32 + b], wb, lane, kf, a32);
+            if constexpr (G34) sweep_G34<true, PPL>(rf[g32 + b], g.profile, wb, lane, kf, a32);
+            else sweep_A<true, PPL>(rf[g32 + b], wb, lane, kf, a32);
           }
           while (mG) {
             const int b = __ffs(mG) - 1;
             mG &= mG - 1;
-            sweep_G<false, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc);
+            sweep_G<false, G34, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile);
             sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
           }
         }
         while (mW) {
           const int b = __ffs(mW) - 1;
           mW &= mW - 1;
-          sweep_G<true, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc);
+          sweep_G<true, G34, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile);
           sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
         }
       }
@@ -817,7 +920,9 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
 
 // ------------------------------------------------------- persistent kernel
 // mixed form: SH::MINB CTAs per SM (4: 32 warps, 64 registers)
-template <bool MIXED, class SH>
+// G34: the Doppler / binned-Gaussian profiles of the mixed form (their own
+// instantiation, so the Voigt and Lorentz kernels carry none of their code)
+template <bool MIXED, class SH, bool G34 = false>
 __global__ void __launch_bounds__(SH::THREADS, MIXED ? SH::MINB : 2)
 voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
                  int64_t nlines, GridDev g, const StateDev *__restrict__ states,
@@ -843,7 +948,7 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
     const void *prep_s = static_cast<const char *>(prep) + (size_t)s * nlines * rec_bytes;
     const int64_t g0 = (int64_t)(tile0 + tile) * G;
     const int64_t g1 = min(g0 + (int64_t)G, g.nx);
-    sum_tile<MIXED, SH, false>(prep_s, nu0, nlines, g, st, st.wmax, st.s1exp, g0, g1, part, nsplit,
+    sum_tile<MIXED, SH, false, G34>(prep_s, nu0, nlines, g, st, st.wmax, st.s1exp, g0, g1, part, nsplit,
                                partial + (int64_t)tt * nsplit * G, tile_cnt + tt,
                                K + (int64_t)s * k_stride, smem_dyn);
   }
@@ -940,7 +1045,7 @@ __device__ __noinline__ void prep_lines(const LinesDev &L, const GridDev &g, con
   for (; l < l1; l += step) prep_record<MIXED, PREP_ALL>(L, g, st, l, e916, out, w_loc, s1_loc);
 }
 
-template <bool MIXED, class SH>
+template <bool MIXED, class SH, bool G34 = false>
 __global__ void __launch_bounds__(SH::THREADS, MIXED ? SH::MINB : 2)
 voigt_table_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states, TableSched sc,
                    void *ring, double *partial, unsigned *tile_cnt, unsigned long long *ticket,
@@ -1010,7 +1115,7 @@ voigt_table_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states, T
         const int64_t g0 = (int64_t)tile * G;
         const int64_t g1 = min(g0 + (int64_t)G, g.nx);
         const size_t tslot = (size_t)slot * sc.tps + tile;
-        sum_tile<MIXED, SH, true>(ring_s, L.nu0, n, g, st, f.wmax, f.s1exp, g0, g1, part, sc.nsplit,
+        sum_tile<MIXED, SH, true, G34>(ring_s, L.nu0, n, g, st, f.wmax, f.s1exp, g0, g1, part, sc.nsplit,
                                   partial + tslot * sc.nsplit * G, tile_cnt + tslot,
                                   K + (int64_t)s * k_stride, smem_dyn);
       }
@@ -1098,10 +1203,11 @@ int voigt_tile_warps(int shape) { return HK_SHAPE_WARPS[shape < 0 || shape >= HK
 // Calls f(kernel, dynamic shared memory) for the kernel of (precision,
 // shape); the plain FP64 form has the default shape only.
 template <class F>
-static cudaError_t with_kernel(bool mixed, int shape, F &&f) {
+static cudaError_t with_kernel(bool mixed, int shape, F &&f, bool g34 = false) {
   using KFn = void (*)(const void *, const double *, int64_t, GridDev, const StateDev *, int, int,
                        int, int, unsigned *, double *, unsigned *, double *, int64_t);
   if (!mixed) return f((KFn)voigt_sum_kernel<false, Shape0>, sizeof(RecD) * Shape0::CH, Shape0::THREADS);
+  if (g34) return f((KFn)voigt_sum_kernel<true, Shape0, true>, smem_mixed<Shape0>(), Shape0::THREADS);
   switch (shape) {
 #define HK_SHAPE_CASE(n) \
   case n: return f((KFn)voigt_sum_kernel<true, Shape##n>, smem_mixed<Shape##n>(), Shape##n::THREADS);
@@ -1178,6 +1284,7 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d
   const int64_t total64 = pl.tiles * pl.nsplit;
   if (total64 > 0x7fffffff) return cudaErrorInvalidValue;
   if (pl.G != voigt_tile_points(pl.shape)) return cudaErrorInvalidValue;
+  if (mixed && g.profile >= 3 && pl.shape != 0) return cudaErrorInvalidValue;  // shape 0 only
   const int total = (int)total64;
   cudaError_t e = cudaMemsetAsync(ticket_d, 0, sizeof(unsigned), stream);
   if (e != cudaSuccess) return e;
@@ -1197,17 +1304,18 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d
                                             pl.tiles_per_state, pl.nsplit, total, ticket_d,
                                             partial_d, tile_cnt_d, K_d, k_stride);
     return cudaGetLastError();
-  });
+  }, mixed && g.profile >= 3);
   return e;
 }
 
 // The fused table kernel of (precision, shape) and its dynamic shared memory.
 template <class F>
-static cudaError_t with_table_kernel(bool mixed, int shape, F &&f) {
+static cudaError_t with_table_kernel(bool mixed, int shape, F &&f, bool g34 = false) {
   using KFn = void (*)(LinesDev, GridDev, const StateDev *, TableSched, void *, double *, unsigned *,
                        unsigned long long *, unsigned long long *, unsigned *, unsigned *, unsigned *,
                        TableFin *, int *, double *, int64_t);
   if (!mixed) return f((KFn)voigt_table_kernel<false, Shape0>, sizeof(RecD) * Shape0::CH, Shape0::THREADS);
+  if (g34) return f((KFn)voigt_table_kernel<true, Shape0, true>, smem_mixed<Shape0>(), Shape0::THREADS);
   switch (shape) {
 #define HK_SHAPE_CASE(n) \
   case n: return f((KFn)voigt_table_kernel<true, Shape##n>, smem_mixed<Shape##n>(), Shape##n::THREADS);
@@ -1258,6 +1366,7 @@ cudaError_t launch_voigt_table(bool mixed, const TablePlan &tp, const LinesDev &
                                int64_t k_stride, cudaStream_t stream) {
   if (tp.S < 1 || tp.R < 2 || tp.slots != std::min(tp.R, tp.S)) return cudaErrorInvalidValue;
   if (tp.G != voigt_tile_points(tp.shape)) return cudaErrorInvalidValue;
+  if (mixed && g.profile >= 3 && tp.shape != 0) return cudaErrorInvalidValue;  // shape 0 only
   if (tp.nsplit > 1 && !b.partial) return cudaErrorInvalidValue;
   // the counters, maxima and flags start from zero on every launch (replay)
   cudaError_t e = cudaMemsetAsync(b.sync, 0, table_sync_bytes(tp.S), stream);
@@ -1290,7 +1399,7 @@ cudaError_t launch_voigt_table(bool mixed, const TablePlan &tp, const LinesDev &
     kfn<<<ctas, threads, smem, stream>>>(L, g, states_d, sc, b.ring, b.partial, b.tile_cnt, ticket, wbits,
                                          prep_cnt, sum_cnt, ready, fin, err, K_d, k_stride);
     return cudaGetLastError();
-  });
+  }, mixed && g.profile >= 3);
 }
 
 int *table_error_word(void *sync_d, int nstates) {

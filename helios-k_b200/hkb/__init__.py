@@ -80,6 +80,7 @@ def lib():
             "hk_table_build": (_i, [_p, _i, _p, _p, _i, _p, _i, _d, _p, _p]),
             "hk_table_run": (_i, [_p, _p]),
             "hk_table_status": (_i, [_p, _p]),
+            "hk_set_table_mode": (_i, [_p, _i]),
             "hk_table_free": (_i, [_p]),
             "hk_table_kernels": (_i64, [_p]),
             "hk_last_launches": (_i64, [_p]),
@@ -380,6 +381,11 @@ class Context:
         self._table_bufs = (K, coeff, nxmin)
         self._chk(lib().hk_table_build(self._h, len(T), _ptr(T), _ptr(P), precision, _ptr(K),
                                        nC, unitScale, _ptr(coeff), _ptr(nxmin)))
+
+    def set_table_mode(self, fused):
+        """0: per-batch launches (default); 1: one persistent launch for the
+        line prep and Voigt sums of every state (tables of >= 4 states)."""
+        self._chk(lib().hk_set_table_mode(self._h, int(fused)))
 
     def table_run(self, stream=None):
         """Replay the recorded table (one graph launch, asynchronous)."""

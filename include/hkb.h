@@ -302,13 +302,16 @@ hk_status hk_opacity_vjp_log(hk_ctx *ctx, double T, double P, int precision, con
 
 /* ------------------------------------------------------------ tables */
 
-/* A whole T-P table as one CUDA graph of two kernels: one persistent launch
- * scales the lines to every state (records in a ring of per-state slots)
- * and sums every state's Voigt profiles, as tickets of one counter (the
- * line prep of a state before its sums, a slot reused once the sums of its
- * previous state are done); one k-distribution launch then fits all states.
- * hk_table_build records it once; hk_table_run replays it with one graph
- * launch.  K (nstates x Nx), coeff (nstates x nbins x nC) and nxmin
+/* A whole T-P table as one CUDA graph, recorded once by hk_table_build and
+ * replayed by hk_table_run with one graph launch.  Table mode 0 (default):
+ * per batch of states whose line records fit the workspace, a line-prep and
+ * a persistent Voigt launch, then one k-distribution launch for all states.
+ * Table mode 1 (hk_set_table_mode, tables of 4 states or more): two kernels,
+ * one persistent launch that scales the lines to every state (records in a
+ * ring of per-state slots) and sums every state's Voigt profiles as tickets
+ * of one counter (the line prep of state s beside the sums of state s - 1, a
+ * slot reused once its previous state's sums are done), then one
+ * k-distribution launch.  Both modes give the same bits.  K (nstates x Nx), coeff (nstates x nbins x nC) and nxmin
  * (nstates x nbins) are DEVICE buffers owned by the caller that must stay
  * valid while the table exists; hk_table_build allocates all workspace and
  * synchronises the device; hk_table_run is asynchronous on `stream`.  The
@@ -323,6 +326,8 @@ hk_status hk_opacity_vjp_log(hk_ctx *ctx, double T, double P, int precision, con
 hk_status hk_table_build(hk_ctx *ctx, int nstates, const double *T, const double *P,
                          int precision, double *K, int nC, double unitScale,
                          double *coeff, int32_t *nxmin);
+/* 0: per-batch launches (default); 1: one persistent launch for the sums. */
+hk_status hk_set_table_mode(hk_ctx *ctx, int fused);
 hk_status hk_table_run(hk_ctx *ctx, void *stream);
 hk_status hk_table_status(hk_ctx *ctx, void *stream);
 hk_status hk_table_free(hk_ctx *ctx);

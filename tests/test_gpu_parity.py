@@ -269,9 +269,10 @@ def test_errors_are_reported(small):
 
 
 def test_table_graph_equals_opacity_and_kdist(small):
-    """hk_table_build/hk_table_run (one CUDA graph for the whole T-P table)
-    give the same bits as hk_opacity + hk_kdist on the same states, on every
-    replay."""
+    """hk_table_build/hk_table_run (one CUDA graph for the whole T-P table;
+    table mode 1: one persistent launch for the line prep and sums of every
+    state) give the same bits as hk_opacity + hk_kdist on the same states, on
+    every replay, and as the default per-batch graph."""
     import torch
     ctx = small["ctx"]
     ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
@@ -282,7 +283,9 @@ def test_table_graph_equals_opacity_and_kdist(small):
     K = torch.empty((ns, nx), dtype=torch.float64, device=dev)
     coeff = torch.empty((ns, NBINS, nC), dtype=torch.float64, device=dev)
     nxmin = torch.empty((ns, NBINS), dtype=torch.int32, device=dev)
+    ctx.set_table_mode(1)
     ctx.table_build(Ts, Ps, K, coeff, nxmin, nC=nC)
+    ctx.set_table_mode(0)
     assert ctx.table_kernels == 2   # one persistent table launch + one fit launch
     ctx.table_run()
     ctx.table_status()
@@ -300,6 +303,39 @@ def test_table_graph_equals_opacity_and_kdist(small):
     assert np.array_equal(K1, Kr)
     assert np.array_equal(c1, fit["coeff"])
     assert np.array_equal(n1, fit["nxmin"])
+    # the default per-batch table graph gives the same bits
+    ctx.table_build(Ts, Ps, K, coeff, nxmin, nC=nC)
+    assert ctx.table_kernels == 4   # line prep, state scale, Voigt sum (one batch), fit
+    ctx.table_run()
+    ctx.table_status()
+    assert np.array_equal(K.cpu().numpy(), K1)
+    assert np.array_equal(coeff.cpu().numpy(), c1)
+    ctx.table_free()
+
+
+def test_small_table_graph_equals_opacity(small):
+    """Tables of fewer than 4 states record the per-batch launches (line
+    prep, state scale, Voigt sum, then the fit): same bits as hk_opacity +
+    hk_kdist."""
+    import torch
+    ctx = small["ctx"]
+    ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+    Ts, Ps = np.array([1500.0, 300.0]), np.array([0.1, 1e-3])
+    ns, nx, nC = len(Ts), ctx.nx, 20
+    dev = torch.device("cuda")
+    K = torch.empty((ns, nx), dtype=torch.float64, device=dev)
+    coeff = torch.empty((ns, NBINS, nC), dtype=torch.float64, device=dev)
+    nxmin = torch.empty((ns, NBINS), dtype=torch.int32, device=dev)
+    ctx.table_build(Ts, Ps, K, coeff, nxmin, nC=nC)
+    assert ctx.table_kernels == 4
+    ctx.table_run()
+    ctx.table_status()
+    K1, c1 = K.cpu().numpy(), coeff.cpu().numpy()
+    ctx.table_free()
+    Kr = ctx.opacity(Ts, Ps, hkb.MIXED)
+    fit = ctx.kdist(Kr, nC=nC)
+    assert np.array_equal(K1, Kr)
+    assert np.array_equal(c1, fit["coeff"])
 
 
 def test_sectioned_states_equal_batched(small):
