@@ -578,7 +578,9 @@ static hk_status opacity_sectioned(hk_ctx *c, int nstates, bool mixed, int shape
 // grid or options change.  Its probe outputs land in K rows the call then
 // overwrites.
 static int shape_for(const hk_ctx *c, bool mixed) {
-  if (!mixed || c->g.profile >= 3) return 0;  // the Gaussian profiles' kernels: shape 0
+  // the kernels of the Gaussian profiles, plinth removal and sub-Lorentzian
+  // wings have the default shape only
+  if (!mixed || c->g.profile >= 3 || c->g.plinth || c->g.subL) return 0;
   return (c->tuning != 0 && c->tuned) ? c->tuned_shape : c->shape_fixed;
 }
 
@@ -728,17 +730,19 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   }
   // States run in batches whose per-(state, line) records fit the prep
   // budget; each batch is one prep launch and one persistent Voigt launch.
-  // plinth removal and sub-Lorentzian wings run the FP64 form; the mixed
-  // form holds the Voigt regions, the Lorentz profile (its region A over the
-  // whole window) and the Doppler and binned-Gaussian profiles (region A, cut
-  // to where their FP32 terms are normal floats)
-  const bool mixed = precision == HK_PRECISION_MIXED && !c->g.plinth && !c->g.subL;
+  // the mixed form holds the Voigt regions and the Lorentz profile (with
+  // plinth removal and sub-Lorentzian wings too) and the Doppler and
+  // binned-Gaussian profiles (region A, cut to where their FP32 terms are
+  // normal floats); the Gaussian profiles with plinth removal or
+  // sub-Lorentzian wings run the FP64 form
+  const bool mixed = precision == HK_PRECISION_MIXED &&
+                     !(c->g.profile >= 3 && (c->g.plinth || c->g.subL));
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
   c->voigt_ms_acc_only = false;
   c->launches = 0;
-  if (mixed && c->g.profile <= 2 && c->tuning != 0 && !c->tuned && per_state <= c->prep_budget && c->nlines > 0)
+  if (mixed && c->g.profile <= 2 && !c->g.plinth && !c->g.subL && c->tuning != 0 && !c->tuned && per_state <= c->prep_budget && c->nlines > 0)
     if ((st = tune_shape(c, nstates, hs, Kd, s)) != HK_OK) return st;
   const int shape = shape_for(c, mixed);
   c->last_shape = shape;
@@ -1240,13 +1244,15 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   CUDA_TRY(c, c->wbits.ensure(2 * nstates * sizeof(unsigned long long)));
   CUDA_TRY(c, cudaMemcpy(c->states.p, hs.data(), nstates * sizeof(StateDev), cudaMemcpyHostToDevice));
   const int64_t nx = c->g.nx;
-  // plinth removal and sub-Lorentzian wings run the FP64 form; the mixed
-  // form holds the Voigt regions, the Lorentz profile (its region A over the
-  // whole window) and the Doppler and binned-Gaussian profiles (region A, cut
-  // to where their FP32 terms are normal floats)
-  const bool mixed = precision == HK_PRECISION_MIXED && !c->g.plinth && !c->g.subL;
+  // the mixed form holds the Voigt regions and the Lorentz profile (with
+  // plinth removal and sub-Lorentzian wings too) and the Doppler and
+  // binned-Gaussian profiles (region A, cut to where their FP32 terms are
+  // normal floats); the Gaussian profiles with plinth removal or
+  // sub-Lorentzian wings run the FP64 form
+  const bool mixed = precision == HK_PRECISION_MIXED &&
+                     !(c->g.profile >= 3 && (c->g.plinth || c->g.subL));
   c->launches = 0;
-  if (mixed && c->g.profile <= 2 && c->tuning != 0 && !c->tuned && c->nlines > 0 &&
+  if (mixed && c->g.profile <= 2 && !c->g.plinth && !c->g.subL && c->tuning != 0 && !c->tuned && c->nlines > 0 &&
       (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(true) <= c->prep_budget) {
     if ((st = tune_shape(c, nstates, hs, K, 0)) != HK_OK) return st;
     CUDA_TRY(c, cudaDeviceSynchronize());

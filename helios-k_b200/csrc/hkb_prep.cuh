@@ -75,6 +75,15 @@ __device__ __forceinline__ void prep_record(const LinesDev &L, const GridDev &g,
       // >= Y^2, a normal float)
       if (rmin < 0x1p-64 * umax || Y > 0x1p60 || (g.profile == 2 && Y < 0x1p-60)) flags |= HK_PF_RANGE;
     }
+    r.plr = 0.f;
+    r.inu = g.subL ? (float)(1.0 / ls.nu) : 0.f;
+    if (g.plinth && w[5] > w[0] && S1 > 0.0) {
+      const double pl = plinth_d(g, S1, Sc, ls.iad, ls.vy);
+      r.plr = (float)(pl / S1);
+      // the line's peak: Sc V(0, y) = Sc erfcx(y) (Voigt), S1 / y^2 (Lorentz)
+      const double peak = g.profile == 2 ? S1 / Y : Sc * erfcx(ls.vy);
+      if (!(pl <= 0x1p-13 * peak)) flags |= HK_PF_RANGE;
+    }
     r.flags = flags;
     // region C's Algorithm-916 part: |x| < sqrt(36 - y^2), from the FP64
     // offsets (a point within rounding of r = 6 may fall on either side;

@@ -93,6 +93,9 @@ static_assert(sizeof(LinePrep) == 96, "LinePrep layout");
 constexpr int HK_PF_WIDE = 2, HK_PF_RANGE = 1;
 //   [t0, t1): the part of region C with |x| < sqrt(36 - y^2) (Algorithm 916
 //   in FP32; the rest of region C takes the asymptotic series)
+//   HK_PF_RANGE also marks a line whose plinth exceeds 2^-13 of its peak:
+//   the FP32 difference profile - plinth would cancel too far near its
+//   window edges, so it is summed in FP64.
 struct __align__(16) LinePrepF {
   double nu, iad;
   double S1, Sc;
@@ -102,6 +105,8 @@ struct __align__(16) LinePrepF {
   int ex, flags;
   int i0, b0, c0, c1, b1, i1;
   int t0, t1;
+  float plr;  // plinth / S1 (removePlinth), else 0
+  float inu;  // 1 / nu (sub-Lorentzian wings), else 0
 };
 static_assert(sizeof(LinePrepF) == 112, "LinePrepF layout");
 

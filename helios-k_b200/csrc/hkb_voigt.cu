@@ -127,10 +127,10 @@ constexpr int HK_MAX_LEVEL = 7;
 // region-C denominator tables (8 leading pad floats keep R[m-1-k] of the
 // first line in bounds for predicated reads), and the per-point FP64 sums.
 constexpr int HK_RPAD = 8;
-template <class SH>
+template <class SH, bool EXT = false>
 constexpr size_t smem_mixed() {
   return sizeof(RecF) * SH::CH + sizeof(float) * (HK_RPAD + SH::CH * HK_C916_MR) +
-         sizeof(double) * SH::G;
+         sizeof(double) * SH::G + (EXT ? sizeof(float2) * SH::CH : 0);
 }
 
 struct __align__(16) RecD {
@@ -220,10 +220,10 @@ __device__ __forceinline__ int line_key(const LinePrepF *__restrict__ P, int64_t
   return lev;
 }
 
-template <bool CG, bool G34>
+template <bool CG, bool G34, bool EXT = false>
 __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, const GridDev &g,
                                             int64_t l, int64_t g0, int64_t g1, int s1exp,
-                                            int key, RecF &r) {
+                                            int key, RecF &r, float2 *ext = nullptr) {
   const LinePrepF lp = load_record<CG>(P + l);
   const bool nonempty = key != HK_KEY_EMPTY;
   const bool weak = key == HK_KEY_WEAK;
@@ -265,6 +265,11 @@ __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, con
   r.t1 = clip_local(lp.t1, g0, g1);
   r.flags = ((lp.flags & HK_PF_WIDE) ? HK_F_WIDE : 0) | (weak ? HK_F_WEAK : 0) | (lev << 8);
   r.iy = lp.y > 0.f ? (float)(1.0 / (double)lp.y) : 0.f;
+  if (EXT) {
+    // plinth in the line's FP32 units (S1f = 1 for a weak line: then the
+    // plinth per S1, which its FP64 sweep scales), and 1 / nu
+    *ext = make_float2((float)((double)lp.plr * S1f), lp.inu);
+  }
   if (G34) {
     // Doppler / binned Gaussian: S1f exp(-u^2) with u = |x| (- vb / 2) is a
     // normal float only for u^2 <= (126 + e) ln 2 (S1f < 2^e): the points
@@ -357,6 +362,62 @@ __device__ __forceinline__ int classify(const RecF &r, int wb) {
   if (r.b0 <= lo && r.b1 >= hi) return (full && noC) ? HK_CLS_B : HK_CLS_BM;
   if (r.b0 >= r.b1 || r.b1 <= lo || r.b0 >= hi) return full ? HK_CLS_A : HK_CLS_AM;
   return HK_CLS_G;
+}
+
+// Plinth removal and sub-Lorentzian wings in the mixed form (their own
+// kernel instantiation): every term of a grid point lo < x < hi times
+// chi(|x - nu|) x / nu (sLChi voigt.h:47-72), chi = exp(-B1 clamp(d - s1, 0,
+// s2 - s1) - B2 clamp(d - s2, 0, s3 - s2) - B3 max(d - s3, 0)) -- the
+// reference's piecewise exponential written as one continuous expression --
+// and each line's plinth subtracted at every point of its window (after the
+// profile, without chi, as Plinth_kernel voigt.h:1091-1164).
+struct ExtF {
+  float s1, s2, s3, B1, B2, B3;  // chi breakpoints (cm^-1) and the state's slopes
+  int kl0, kl1;                  // tile points with sl_lo < x < sl_hi
+  float dnu;
+};
+
+__device__ __forceinline__ ExtF ext_consts(const GridDev &g, const StateDev &st, int64_t g0, int64_t g1) {
+  ExtF e;
+  e.s1 = (float)g.sl_sigma[0];
+  e.s2 = (float)g.sl_sigma[1];
+  e.s3 = (float)g.sl_sigma[2];
+  e.B1 = (float)st.sl_B[0];
+  e.B2 = (float)st.sl_B[1];
+  e.B3 = (float)st.sl_B[2];
+  e.dnu = (float)g.dnu;
+  if (g.subL) {
+    // first tile points with x > sl_lo and with x >= sl_hi (x = numin + i dnu)
+    int64_t a = g0, b = g1;
+    while (a < b) {
+      const int64_t m = a + (b - a) / 2;
+      if (grid_x(g, m) > g.sl_lo) b = m;
+      else a = m + 1;
+    }
+    int64_t c = a, d = g1;
+    while (c < d) {
+      const int64_t m = c + (d - c) / 2;
+      if (grid_x(g, m) >= g.sl_hi) d = m;
+      else c = m + 1;
+    }
+    e.kl0 = (int)(a - g0);
+    e.kl1 = (int)(c - g0);
+  } else {
+    e.kl0 = e.kl1 = 0;
+  }
+  return e;
+}
+
+// chi(|x - nu|) x / nu at a point x (Doppler units) of a line with grid step
+// vb (Doppler units) and 1 / nu = inu: |x - nu| = |x| dnu / vb (cm^-1)
+__device__ __forceinline__ float chi_factor(const ExtF &e, float x, float vb, float inu) {
+  const float xc = x * (e.dnu / vb);  // x - nu, cm^-1
+  const float d = fabsf(xc);
+  const float t1 = fminf(fmaxf(d - e.s1, 0.f), e.s2 - e.s1);
+  const float t2 = fminf(fmaxf(d - e.s2, 0.f), e.s3 - e.s2);
+  const float t3 = fmaxf(d - e.s3, 0.f);
+  const float arg = fmaf(-e.B1, t1, fmaf(-e.B2, t2, -e.B3 * t3));
+  return ex2_fast(1.4426950408889634f * arg) * fmaf(xc, inu, 1.0f);
 }
 
 // 1/d0 and 1/d1 from one reciprocal: R = 1/(d0 d1), then (d1 R, d0 R).
@@ -543,9 +604,10 @@ __device__ __forceinline__ void sweep_G34(const RecF &rr, int profile, int wb, i
 // within rounding of r = 6 may take either evaluator (both hold there).
 // Points leave their owning lane here, so the warp syncs before cacc is
 // touched again.
-template <int SLICE>
+template <int SLICE, bool EXT = false>
 __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__ Rj,
-                                        double *__restrict__ cacc, int wb, int lane) {
+                                        double *__restrict__ cacc, int wb, int lane,
+                                        const ExtF *ex = nullptr, float inu = 0.f, double pld = 0.0) {
   const int lo = max(r.c0, wb), hi = min(r.c1, wb + SLICE);
   if (lo >= hi) return;
   const float dh = r.dh, dl = r.dl, vbh = r.vbh, vbl = r.vbl;
@@ -556,14 +618,18 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
   for (int k = t0 + lane; k < t1; k += 32) {
     const float kk = (float)k;
     const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
-    cacc[k] = fma(Sc, (double)voigt916_core(x, y, iy, ey, sig1, Rj), cacc[k]);
+    float v = voigt916_core(x, y, iy, ey, sig1, Rj);
+    if (EXT && k >= ex->kl0 && k < ex->kl1) v *= chi_factor(*ex, x, r.vb, inu);
+    cacc[k] = fma(Sc, (double)v, cacc[k]) - pld;
   }
   const int n1 = t0 - lo, ns = n1 + (hi - t1);
   for (int i = lane; i < ns; i += 32) {
     const int k = i < n1 ? lo + i : t1 + (i - n1);
     const float kk = (float)k;
     const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
-    cacc[k] = fma(Sc, (double)voigt_asy(x, y), cacc[k]);
+    float v = voigt_asy(x, y);
+    if (EXT && k >= ex->kl0 && k < ex->kl1) v *= chi_factor(*ex, x, r.vb, inu);
+    cacc[k] = fma(Sc, (double)v, cacc[k]) - pld;
   }
   __syncwarp();
 }
@@ -571,11 +637,12 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
 // A/B boundaries in the slice, and weak lines: per-point window/region
 // tests.  WEAK lines (S1f = 1) add S1 t in FP64 to cacc; the others add
 // S1f t to the FP32 sums.
-template <bool WEAK, bool G34, int PPL>
+template <bool WEAK, bool G34, int PPL, bool EXT = false>
 __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
                                         const float2 (&kf)[PPL / 2],
                                         float2 (&a32)[PPL / 2],
-                                        double *__restrict__ cacc, int profile) {
+                                        double *__restrict__ cacc, int profile,
+                                        const ExtF *ex = nullptr, float2 xt = make_float2(0.f, 0.f)) {
   if (WEAK && G34) {
     // Doppler / binned Gaussian lines summed in FP64: the FP64 form's term
     const double D0 = gauss_D0(r), vb = gauss_vb(r);
@@ -600,6 +667,9 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
   const float S1f = r.S1f, C1 = r.C1, C0 = r.C0;
   const float D2 = r.D2, D1 = r.D1, D0 = r.D0;
   const double S1w = WEAK ? r.Sc * (double)y * 0.56418958354775628 : 0.0;  // S y / pi
+  // EXT: the plinth in FP32 units (a weak line's in FP64 from its plinth / S1)
+  const float plf = EXT ? xt.x : 0.f;
+  const double plw = (EXT && WEAK) ? (double)xt.x * S1w : 0.0;
 #pragma unroll
   for (int p = 0; p < PPL; ++p) {
     const int k = wb + lane + 32 * p;
@@ -616,7 +686,17 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
         f = S1f;
         inv = rcp_fast(fmaf(x, x, Yf));
       }
-      if (WEAK) {
+      if (EXT) {
+        float t = f * inv;
+        if (k >= ex->kl0 && k < ex->kl1) t *= chi_factor(*ex, x, vb, xt.y);
+        if (WEAK) {
+          cacc[k] = fma(S1w, (double)t, cacc[k]) - plw;
+        } else if (p & 1) {
+          a32[p >> 1].y += t - plf;
+        } else {
+          a32[p >> 1].x += t - plf;
+        }
+      } else if (WEAK) {
         cacc[k] = fma(S1w, (double)(f * inv), cacc[k]);
       } else if (p & 1) {
         a32[p >> 1].y = fmaf(f, inv, a32[p >> 1].y);
@@ -708,7 +788,7 @@ __device__ __forceinline__ void flush_sums(float2 (&a32)[PPL / 2], double *__res
 // split tile, published to pt (this tile's nsplit partial rows of G points)
 // and combined in part order by the CTA that completes the count *cnt.
 // wmax and s1exp are the state's search half-width and FP32 scale exponent.
-template <bool MIXED, class SH, bool CG, bool G34 = false>
+template <bool MIXED, class SH, bool CG, bool G34 = false, bool EXT = false>
 __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__restrict__ nu0,
                                          int64_t nlines, const GridDev &g, const StateDev &st,
                                          double wmax, int s1exp, int64_t g0, int64_t g1, int part,
@@ -743,6 +823,10 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
   }
   __syncthreads();
   const int64_t L0 = s_L0, L1 = s_L1;
+  // plinth and 1 / nu of the staged lines (EXT), after the per-point sums
+  float2 *ext = reinterpret_cast<float2 *>(cacc + G);
+  ExtF exc;
+  if (EXT) exc = ext_consts(g, st, g0, g1);
 
   float2 kf[PPL / 2];   // lane-local point indices, paired {p, p+1}
   float2 a32[PPL / 2];  // mixed: FP32 sums of the current chunk (scaled)
@@ -802,7 +886,7 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
           for (int w = 0; w < CH / 32; ++w) pos += s_kcnt[w][v];
         for (int w = 0; w < warp; ++w) pos += s_kcnt[w][key];
         RecF r;
-        stage_mixed<CG, G34>(PF, g, l, g0, g1, s1exp, key, r);
+        stage_mixed<CG, G34, EXT>(PF, g, l, g0, g1, s1exp, key, r, ext + pos);
         reinterpret_cast<RecF *>(rec)[pos] = r;
         if (r.c1 > r.c0 && r.i1 > r.i0) stage_rtab(r.y, Rtab + pos * HK_C916_MR);
       }
@@ -833,6 +917,20 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
             m = __ballot_sync(0xffffffffu, lev == lcur) & live;
           }
           live &= ~m;
+          if constexpr (EXT) {
+            // every class through the generic sweep with chi and plinth
+            const double u = ldexp(1.0, -(s1exp + HK_LEVEL_BITS * lcur));
+            unsigned mX = m;
+            while (mX) {
+              const int b = __ffs(mX) - 1;
+              mX &= mX - 1;
+              const float2 xt = ext[g32 + b];
+              sweep_G<false, false, PPL, true>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile, &exc, xt);
+              sweep_C<SLICE, true>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, &exc, xt.y,
+                                   (double)xt.x * u);
+            }
+            continue;
+          }
           unsigned mB = m & bB, mA = m & bA, mBM = m & bBM, mAM = m & bAM, mG = m & bG;
           while (mB) {
             const int b = __ffs(mB) - 1;
@@ -867,8 +965,17 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
         while (mW) {
           const int b = __ffs(mW) - 1;
           mW &= mW - 1;
-          sweep_G<true, G34, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile);
-          sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
+          if constexpr (EXT) {
+            // weak line: FP64 sums; its plinth from plinth / S1 (S1f = 1)
+            const float2 xt = ext[g32 + b];
+            const RecF &rw = rf[g32 + b];
+            sweep_G<true, false, PPL, true>(rw, wb, lane, kf, a32, cacc, g.profile, &exc, xt);
+            sweep_C<SLICE, true>(rw, Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, &exc, xt.y,
+                                 (double)xt.x * (rw.Sc * (double)rw.y * 0.56418958354775628));
+          } else {
+            sweep_G<true, G34, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile);
+            sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
+          }
         }
       }
       // at most one chunk of lines per FP32 sum
@@ -922,7 +1029,7 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
 // mixed form: SH::MINB CTAs per SM (4: 32 warps, 64 registers)
 // G34: the Doppler / binned-Gaussian profiles of the mixed form (their own
 // instantiation, so the Voigt and Lorentz kernels carry none of their code)
-template <bool MIXED, class SH, bool G34 = false>
+template <bool MIXED, class SH, bool G34 = false, bool EXT = false>
 __global__ void __launch_bounds__(SH::THREADS, MIXED ? SH::MINB : 2)
 voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
                  int64_t nlines, GridDev g, const StateDev *__restrict__ states,
@@ -948,7 +1055,7 @@ voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
     const void *prep_s = static_cast<const char *>(prep) + (size_t)s * nlines * rec_bytes;
     const int64_t g0 = (int64_t)(tile0 + tile) * G;
     const int64_t g1 = min(g0 + (int64_t)G, g.nx);
-    sum_tile<MIXED, SH, false, G34>(prep_s, nu0, nlines, g, st, st.wmax, st.s1exp, g0, g1, part, nsplit,
+    sum_tile<MIXED, SH, false, G34, EXT>(prep_s, nu0, nlines, g, st, st.wmax, st.s1exp, g0, g1, part, nsplit,
                                partial + (int64_t)tt * nsplit * G, tile_cnt + tt,
                                K + (int64_t)s * k_stride, smem_dyn);
   }
@@ -1045,7 +1152,7 @@ __device__ __noinline__ void prep_lines(const LinesDev &L, const GridDev &g, con
   for (; l < l1; l += step) prep_record<MIXED, PREP_ALL>(L, g, st, l, e916, out, w_loc, s1_loc);
 }
 
-template <bool MIXED, class SH, bool G34 = false>
+template <bool MIXED, class SH, bool G34 = false, bool EXT = false>
 __global__ void __launch_bounds__(SH::THREADS, MIXED ? SH::MINB : 2)
 voigt_table_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states, TableSched sc,
                    void *ring, double *partial, unsigned *tile_cnt, unsigned long long *ticket,
@@ -1115,7 +1222,7 @@ voigt_table_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states, T
         const int64_t g0 = (int64_t)tile * G;
         const int64_t g1 = min(g0 + (int64_t)G, g.nx);
         const size_t tslot = (size_t)slot * sc.tps + tile;
-        sum_tile<MIXED, SH, true, G34>(ring_s, L.nu0, n, g, st, f.wmax, f.s1exp, g0, g1, part, sc.nsplit,
+        sum_tile<MIXED, SH, true, G34, EXT>(ring_s, L.nu0, n, g, st, f.wmax, f.s1exp, g0, g1, part, sc.nsplit,
                                   partial + tslot * sc.nsplit * G, tile_cnt + tslot,
                                   K + (int64_t)s * k_stride, smem_dyn);
       }
@@ -1203,11 +1310,13 @@ int voigt_tile_warps(int shape) { return HK_SHAPE_WARPS[shape < 0 || shape >= HK
 // Calls f(kernel, dynamic shared memory) for the kernel of (precision,
 // shape); the plain FP64 form has the default shape only.
 template <class F>
-static cudaError_t with_kernel(bool mixed, int shape, F &&f, bool g34 = false) {
+static cudaError_t with_kernel(bool mixed, int shape, F &&f, bool g34 = false, bool ext = false) {
   using KFn = void (*)(const void *, const double *, int64_t, GridDev, const StateDev *, int, int,
                        int, int, unsigned *, double *, unsigned *, double *, int64_t);
   if (!mixed) return f((KFn)voigt_sum_kernel<false, Shape0>, sizeof(RecD) * Shape0::CH, Shape0::THREADS);
   if (g34) return f((KFn)voigt_sum_kernel<true, Shape0, true>, smem_mixed<Shape0>(), Shape0::THREADS);
+  if (ext)
+    return f((KFn)voigt_sum_kernel<true, Shape0, false, true>, smem_mixed<Shape0, true>(), Shape0::THREADS);
   switch (shape) {
 #define HK_SHAPE_CASE(n) \
   case n: return f((KFn)voigt_sum_kernel<true, Shape##n>, smem_mixed<Shape##n>(), Shape##n::THREADS);
@@ -1284,7 +1393,8 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d
   const int64_t total64 = pl.tiles * pl.nsplit;
   if (total64 > 0x7fffffff) return cudaErrorInvalidValue;
   if (pl.G != voigt_tile_points(pl.shape)) return cudaErrorInvalidValue;
-  if (mixed && g.profile >= 3 && pl.shape != 0) return cudaErrorInvalidValue;  // shape 0 only
+  if (mixed && (g.profile >= 3 || g.plinth || g.subL) && pl.shape != 0)
+    return cudaErrorInvalidValue;  // shape 0 only
   const int total = (int)total64;
   cudaError_t e = cudaMemsetAsync(ticket_d, 0, sizeof(unsigned), stream);
   if (e != cudaSuccess) return e;
@@ -1304,18 +1414,21 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d
                                             pl.tiles_per_state, pl.nsplit, total, ticket_d,
                                             partial_d, tile_cnt_d, K_d, k_stride);
     return cudaGetLastError();
-  }, mixed && g.profile >= 3);
+  }, mixed && g.profile >= 3, mixed && g.profile <= 2 && (g.plinth || g.subL));
   return e;
 }
 
 // The fused table kernel of (precision, shape) and its dynamic shared memory.
 template <class F>
-static cudaError_t with_table_kernel(bool mixed, int shape, F &&f, bool g34 = false) {
+static cudaError_t with_table_kernel(bool mixed, int shape, F &&f, bool g34 = false, bool ext = false) {
   using KFn = void (*)(LinesDev, GridDev, const StateDev *, TableSched, void *, double *, unsigned *,
                        unsigned long long *, unsigned long long *, unsigned *, unsigned *, unsigned *,
                        TableFin *, int *, double *, int64_t);
   if (!mixed) return f((KFn)voigt_table_kernel<false, Shape0>, sizeof(RecD) * Shape0::CH, Shape0::THREADS);
   if (g34) return f((KFn)voigt_table_kernel<true, Shape0, true>, smem_mixed<Shape0>(), Shape0::THREADS);
+  if (ext)
+    return f((KFn)voigt_table_kernel<true, Shape0, false, true>, smem_mixed<Shape0, true>(),
+             Shape0::THREADS);
   switch (shape) {
 #define HK_SHAPE_CASE(n) \
   case n: return f((KFn)voigt_table_kernel<true, Shape##n>, smem_mixed<Shape##n>(), Shape##n::THREADS);
@@ -1366,7 +1479,8 @@ cudaError_t launch_voigt_table(bool mixed, const TablePlan &tp, const LinesDev &
                                int64_t k_stride, cudaStream_t stream) {
   if (tp.S < 1 || tp.R < 2 || tp.slots != std::min(tp.R, tp.S)) return cudaErrorInvalidValue;
   if (tp.G != voigt_tile_points(tp.shape)) return cudaErrorInvalidValue;
-  if (mixed && g.profile >= 3 && tp.shape != 0) return cudaErrorInvalidValue;  // shape 0 only
+  if (mixed && (g.profile >= 3 || g.plinth || g.subL) && tp.shape != 0)
+    return cudaErrorInvalidValue;  // shape 0 only
   if (tp.nsplit > 1 && !b.partial) return cudaErrorInvalidValue;
   // the counters, maxima and flags start from zero on every launch (replay)
   cudaError_t e = cudaMemsetAsync(b.sync, 0, table_sync_bytes(tp.S), stream);
@@ -1399,7 +1513,7 @@ cudaError_t launch_voigt_table(bool mixed, const TablePlan &tp, const LinesDev &
     kfn<<<ctas, threads, smem, stream>>>(L, g, states_d, sc, b.ring, b.partial, b.tile_cnt, ticket, wbits,
                                          prep_cnt, sum_cnt, ready, fin, err, K_d, k_stride);
     return cudaGetLastError();
-  }, mixed && g.profile >= 3);
+  }, mixed && g.profile >= 3, mixed && g.profile <= 2 && (g.plinth || g.subL));
 }
 
 int *table_error_word(void *sync_d, int nstates) {
