@@ -731,12 +731,13 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   // States run in batches whose per-(state, line) records fit the prep
   // budget; each batch is one prep launch and one persistent Voigt launch.
   // the mixed form holds the Voigt regions and the Lorentz profile (with
-  // plinth removal and sub-Lorentzian wings too) and the Doppler and
-  // binned-Gaussian profiles (region A, cut to where their FP32 terms are
-  // normal floats); the Gaussian profiles with plinth removal or
-  // sub-Lorentzian wings run the FP64 form
-  const bool mixed = precision == HK_PRECISION_MIXED &&
-                     !(c->g.profile >= 3 && (c->g.plinth || c->g.subL));
+  // sub-Lorentzian wings too) and the Doppler and binned-Gaussian profiles
+  // (region A, cut to where their FP32 terms are normal floats).  Plinth
+  // removal runs the FP64 form: profile - plinth cancels near each window
+  // edge, and a strong line's edge can fall in a bin whose maximum is far
+  // below it, where the FP32 difference misses the 1e-5 bound
+  const bool mixed = precision == HK_PRECISION_MIXED && !c->g.plinth &&
+                     !(c->g.profile >= 3 && c->g.subL);
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
@@ -1245,12 +1246,13 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   CUDA_TRY(c, cudaMemcpy(c->states.p, hs.data(), nstates * sizeof(StateDev), cudaMemcpyHostToDevice));
   const int64_t nx = c->g.nx;
   // the mixed form holds the Voigt regions and the Lorentz profile (with
-  // plinth removal and sub-Lorentzian wings too) and the Doppler and
-  // binned-Gaussian profiles (region A, cut to where their FP32 terms are
-  // normal floats); the Gaussian profiles with plinth removal or
-  // sub-Lorentzian wings run the FP64 form
-  const bool mixed = precision == HK_PRECISION_MIXED &&
-                     !(c->g.profile >= 3 && (c->g.plinth || c->g.subL));
+  // sub-Lorentzian wings too) and the Doppler and binned-Gaussian profiles
+  // (region A, cut to where their FP32 terms are normal floats).  Plinth
+  // removal runs the FP64 form: profile - plinth cancels near each window
+  // edge, and a strong line's edge can fall in a bin whose maximum is far
+  // below it, where the FP32 difference misses the 1e-5 bound
+  const bool mixed = precision == HK_PRECISION_MIXED && !c->g.plinth &&
+                     !(c->g.profile >= 3 && c->g.subL);
   c->launches = 0;
   if (mixed && c->g.profile <= 2 && !c->g.plinth && !c->g.subL && c->tuning != 0 && !c->tuned && c->nlines > 0 &&
       (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(true) <= c->prep_budget) {

@@ -78,9 +78,11 @@ __device__ __forceinline__ void prep_record(const LinesDev &L, const GridDev &g,
     r.plr = 0.f;
     r.inu = g.subL ? (float)(1.0 / ls.nu) : 0.f;
     if (g.plinth && w[5] > w[0] && S1 > 0.0) {
+      // (the mixed form is not run with plinth removal; the plinth per S1
+      // would be subtracted per point, and lines whose plinth exceeds 2^-13
+      // of their peak summed in FP64)
       const double pl = plinth_d(g, S1, Sc, ls.iad, ls.vy);
       r.plr = (float)(pl / S1);
-      // the line's peak: Sc V(0, y) = Sc erfcx(y) (Voigt), S1 / y^2 (Lorentz)
       const double peak = g.profile == 2 ? S1 / Y : Sc * erfcx(ls.vy);
       if (!(pl <= 0x1p-13 * peak)) flags |= HK_PF_RANGE;
     }

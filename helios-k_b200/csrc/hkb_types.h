@@ -93,9 +93,8 @@ static_assert(sizeof(LinePrep) == 96, "LinePrep layout");
 constexpr int HK_PF_WIDE = 2, HK_PF_RANGE = 1;
 //   [t0, t1): the part of region C with |x| < sqrt(36 - y^2) (Algorithm 916
 //   in FP32; the rest of region C takes the asymptotic series)
-//   HK_PF_RANGE also marks a line whose plinth exceeds 2^-13 of its peak:
-//   the FP32 difference profile - plinth would cancel too far near its
-//   window edges, so it is summed in FP64.
+//   HK_PF_RANGE also marks a line whose plinth exceeds 2^-13 of its peak
+//   (with plinth removal, which the library runs in the FP64 form).
 struct __align__(16) LinePrepF {
   double nu, iad;
   double S1, Sc;

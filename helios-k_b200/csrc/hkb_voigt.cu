@@ -364,13 +364,14 @@ __device__ __forceinline__ int classify(const RecF &r, int wb) {
   return HK_CLS_G;
 }
 
-// Plinth removal and sub-Lorentzian wings in the mixed form (their own
-// kernel instantiation): every term of a grid point lo < x < hi times
-// chi(|x - nu|) x / nu (sLChi voigt.h:47-72), chi = exp(-B1 clamp(d - s1, 0,
-// s2 - s1) - B2 clamp(d - s2, 0, s3 - s2) - B3 max(d - s3, 0)) -- the
-// reference's piecewise exponential written as one continuous expression --
-// and each line's plinth subtracted at every point of its window (after the
-// profile, without chi, as Plinth_kernel voigt.h:1091-1164).
+// Sub-Lorentzian wings in the mixed form (their own kernel instantiation):
+// every term of a grid point lo < x < hi times chi(|x - nu|) x / nu (sLChi
+// voigt.h:47-72), chi = exp(-B1 clamp(d - s1, 0, s2 - s1) - B2 clamp(d - s2,
+// 0, s3 - s2) - B3 max(d - s3, 0)) -- the reference's piecewise exponential
+// written as one continuous expression.  The sweep also subtracts a plinth
+// per point when the staged plinth is nonzero; the library runs plinth
+// removal in the FP64 form (the FP32 difference profile - plinth cancels
+// near window edges), so in practice that plinth is 0.
 struct ExtF {
   float s1, s2, s3, B1, B2, B3;  // chi breakpoints (cm^-1) and the state's slopes
   int kl0, kl1;                  // tile points with sl_lo < x < sl_hi
@@ -1414,7 +1415,7 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d
                                             pl.tiles_per_state, pl.nsplit, total, ticket_d,
                                             partial_d, tile_cnt_d, K_d, k_stride);
     return cudaGetLastError();
-  }, mixed && g.profile >= 3, mixed && g.profile <= 2 && (g.plinth || g.subL));
+  }, mixed && g.profile >= 3, mixed && g.profile <= 2 && g.subL);
   return e;
 }
 
@@ -1513,7 +1514,7 @@ cudaError_t launch_voigt_table(bool mixed, const TablePlan &tp, const LinesDev &
     kfn<<<ctas, threads, smem, stream>>>(L, g, states_d, sc, b.ring, b.partial, b.tile_cnt, ticket, wbits,
                                          prep_cnt, sum_cnt, ready, fin, err, K_d, k_stride);
     return cudaGetLastError();
-  }, mixed && g.profile >= 3, mixed && g.profile <= 2 && (g.plinth || g.subL));
+  }, mixed && g.profile >= 3, mixed && g.profile <= 2 && g.subL);
 }
 
 int *table_error_word(void *sync_d, int nstates) {

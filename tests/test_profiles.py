@@ -2,14 +2,13 @@
 oracle (voigt.h:1091-1262 restated).
 
 The mixed form runs when the mixed precision is asked for -- the Voigt and
-Lorentz profiles with and without plinth removal and sub-Lorentzian wings,
-the Doppler and binned-Gaussian profiles (where their FP32 terms are normal
-floats) without them: 1e-5 relative where K > 1e-6 of its bin maximum (the
-mixed bound), and faster than the FP64 form.  The Doppler profile with
-plinth removal runs the FP64 form in both precisions, so its bound is the
-FP64 one for differences of profile values and plinths: 1e-9; the FP64 form
-itself: 1e-12, 1e-9 with plinth removal.  Index windows (no regions B and C
-for profiles 2-4) are bit-exact.
+Lorentz profiles with and without sub-Lorentzian wings, the Doppler and
+binned-Gaussian profiles (where their FP32 terms are normal floats): 1e-5
+relative where K > 1e-6 of its bin maximum (the mixed bound), and faster
+than the FP64 form.  Plinth removal runs the FP64 form in both precisions
+(profile - plinth cancels near window edges), so its bound is the FP64 one
+for differences of profile values and plinths: 1e-9; the FP64 form itself:
+1e-12.  Index windows (no regions B and C for profiles 2-4) are bit-exact.
 """
 import numpy as np
 import pytest
@@ -71,12 +70,11 @@ def test_profile_matches_oracle(small, profile, plinth, cutMode, cut):
             err, n = masked_relerr(K, Kref, NBINS)
             print(f"profile {profile} plinth {plinth} cut {cutMode}/{cut} T={T} P={P} "
                   f"precision {prec}: err {err:.2e}, line sum {ms[prec]:.3f} ms")
-            mixed_used = profile <= 2 or not plinth
-            if prec == hkb.MIXED and mixed_used:
+            if prec == hkb.MIXED and not plinth:
                 assert err < 1e-5
             else:
                 assert err < (1e-9 if plinth else 1e-12)
-        if profile <= 2 or not plinth:
+        if not plinth:
             assert ms[hkb.MIXED] < ms[hkb.PLAIN_FP64]
     if not plinth:
         ctx.opacity_vjp(1500.0, 0.1, np.ones(ctx.nx))  # every profile has an adjoint
@@ -120,14 +118,49 @@ def test_sublorentzian_matches_oracle(small, profile, plinth):
                 err, _ = masked_relerr(K, Kref, NBINS)
                 print(f"sub-Lorentzian profile {profile} plinth {plinth} T={T} precision {prec}: "
                       f"err {err:.2e}, line sum {ms[prec]:.3f} ms")
-                if prec == hkb.MIXED:
+                if prec == hkb.MIXED and not plinth:
                     assert err < 1e-5
                 else:
                     assert err < (1e-9 if plinth else 1e-12)
-            assert ms[hkb.MIXED] < ms[hkb.PLAIN_FP64]
+            if not plinth:
+                assert ms[hkb.MIXED] < ms[hkb.PLAIN_FP64]
     finally:
         ctx.set_sublorentzian(None)
         ctx.set_profile(1, 0)
     with pytest.raises(hkb.HkError) as e:
         ctx.set_profile(4, 1)  # heliosk.cu:410-413
     assert e.value.status == -8
+
+
+@pytest.mark.parametrize("profile,plinth,subl", [(3, 0, False), (4, 0, False), (1, 0, True),
+                                                 (2, 0, True)])
+def test_profile_tables_equal_opacity(small, profile, plinth, subl):
+    """The mixed kernels of the Gaussian profiles and of sub-Lorentzian wings
+    in both table modes (per-batch launches and one persistent launch) give
+    the same bits as hk_opacity."""
+    import torch
+    ctx = small["ctx"]
+    ctx.set_profile(profile, plinth)
+    if subl:
+        ctx.set_sublorentzian(SL14)
+    try:
+        ctx.set_grid(NUMIN, NUMAX, DNU, NBINS, 0, 25.0)
+        Ts = np.array([1500.0, 500.0, 900.0, 2200.0, 300.0])
+        Ps = np.array([0.1, 10.0, 1.0, 1e-3, 0.5])
+        ref = ctx.opacity(Ts, Ps, hkb.MIXED)
+        ns, nx = len(Ts), ctx.nx
+        K = torch.empty((ns, nx), dtype=torch.float64, device="cuda")
+        coeff = torch.empty((ns, NBINS, 20), dtype=torch.float64, device="cuda")
+        nxmin = torch.empty((ns, NBINS), dtype=torch.int32, device="cuda")
+        for mode in (0, 1):
+            ctx.set_table_mode(mode)
+            ctx.table_build(Ts, Ps, K, coeff, nxmin, nC=20)
+            assert ctx.table_kernels == (2 if mode else 4)
+            ctx.table_run()
+            ctx.table_status()
+            assert np.array_equal(K.cpu().numpy(), ref), f"table mode {mode}"
+            ctx.table_free()
+    finally:
+        ctx.set_table_mode(0)
+        ctx.set_sublorentzian(None)
+        ctx.set_profile(1, 0)
