@@ -201,8 +201,10 @@ hk_status hk_set_workspace(hk_ctx *ctx, double prep_bytes, double part_bytes);
  * as Line6fA_kernel (voigt.h:1235-1262) evaluates them over the whole cut
  * window; remove_plinth 1 (param.dat `removePlinth`) subtracts each line's
  * profile value at its cut edge (Plinth_kernel voigt.h:1091-1164) from every
- * point of its window.  Profiles 2-4 and plinth removal run the FP64 form
- * whatever precision hk_opacity is given; the adjoint refuses them. */
+ * point of its window.  All four profiles have a mixed (FP32) form -- the
+ * Doppler and binned-Gaussian terms evaluated where they are normal FP32
+ * floats -- and an adjoint; plinth removal runs the FP64 form whatever
+ * precision hk_opacity is given, and the adjoint refuses it. */
 hk_status hk_set_profile(hk_ctx *ctx, int profile, int remove_plinth);
 
 /* Sub-Lorentzian line wings (param.dat subLorentzianfile; Perrin & Hartmann
@@ -211,7 +213,9 @@ hk_status hk_set_profile(hk_ctx *ctx, int profile, int remove_plinth);
  * epsilon3, x_lo, x_hi}; every term at a grid point lo < x < hi is multiplied
  * by chi(|x - nu|) x / nu, chi = 1 below sigma1 and exp(-B1 (d - sigma1)
  * ...) beyond, B_k = alpha_k + beta_k exp(-epsilon_k T).  NULL turns it off.
- * Runs the FP64 form; the adjoint refuses it. */
+ * The mixed form applies it to the Voigt and Lorentz profiles (the Doppler
+ * and binned-Gaussian profiles with it run the FP64 form); the adjoint
+ * refuses it. */
 hk_status hk_set_sublorentzian(hk_ctx *ctx, const double *p);
 
 /* --------------------------------------- mean opacities, transmission */
