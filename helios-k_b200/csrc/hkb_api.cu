@@ -577,6 +577,17 @@ static hk_status opacity_sectioned(hk_ctx *c, int nstates, bool mixed, int shape
 // tickets), after one warm-up tile per shape.  The choice holds until lines,
 // grid or options change.  Its probe outputs land in K rows the call then
 // overwrites.
+// Whether a call of the given precision runs the mixed form.  It holds the
+// Voigt regions and the Lorentz profile (with sub-Lorentzian wings or plinth
+// removal), the Doppler profile (with plinth removal too) and the binned
+// Gaussian (region A; FP32 where their terms are normal floats, FP64 tails).
+// Sub-Lorentzian wings run the FP64 form with plinth removal (chi t - plinth
+// is no difference of one function, so no cancellation-free form exists)
+// and with the Gaussian profiles.
+static bool mixed_form(const hk_ctx *c, int precision) {
+  return precision == HK_PRECISION_MIXED && !(c->g.subL && (c->g.plinth || c->g.profile >= 3));
+}
+
 static int shape_for(const hk_ctx *c, bool mixed) {
   // the kernels of the Gaussian profiles, plinth removal and sub-Lorentzian
   // wings have the default shape only
@@ -730,14 +741,7 @@ hk_status hk_opacity(hk_ctx *c, int nstates, const double *T, const double *P, i
   }
   // States run in batches whose per-(state, line) records fit the prep
   // budget; each batch is one prep launch and one persistent Voigt launch.
-  // the mixed form holds the Voigt regions and the Lorentz profile (with
-  // sub-Lorentzian wings too) and the Doppler and binned-Gaussian profiles
-  // (region A, cut to where their FP32 terms are normal floats).  Plinth
-  // removal runs the FP64 form: profile - plinth cancels near each window
-  // edge, and a strong line's edge can fall in a bin whose maximum is far
-  // below it, where the FP32 difference misses the 1e-5 bound
-  const bool mixed = precision == HK_PRECISION_MIXED && !c->g.plinth &&
-                     !(c->g.profile >= 3 && c->g.subL);
+  const bool mixed = mixed_form(c, precision);
   const size_t per_state = (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(mixed);
   c->voigt_ms_acc = 0.0;
   c->have_voigt_t = false;
@@ -1245,14 +1249,7 @@ hk_status hk_table_build(hk_ctx *c, int nstates, const double *T, const double *
   CUDA_TRY(c, c->wbits.ensure(2 * nstates * sizeof(unsigned long long)));
   CUDA_TRY(c, cudaMemcpy(c->states.p, hs.data(), nstates * sizeof(StateDev), cudaMemcpyHostToDevice));
   const int64_t nx = c->g.nx;
-  // the mixed form holds the Voigt regions and the Lorentz profile (with
-  // sub-Lorentzian wings too) and the Doppler and binned-Gaussian profiles
-  // (region A, cut to where their FP32 terms are normal floats).  Plinth
-  // removal runs the FP64 form: profile - plinth cancels near each window
-  // edge, and a strong line's edge can fall in a bin whose maximum is far
-  // below it, where the FP32 difference misses the 1e-5 bound
-  const bool mixed = precision == HK_PRECISION_MIXED && !c->g.plinth &&
-                     !(c->g.profile >= 3 && c->g.subL);
+  const bool mixed = mixed_form(c, precision);
   c->launches = 0;
   if (mixed && c->g.profile <= 2 && !c->g.plinth && !c->g.subL && c->tuning != 0 && !c->tuned && c->nlines > 0 &&
       (size_t)std::max<int64_t>(c->nlines, 1) * line_prep_bytes(true) <= c->prep_budget) {

@@ -316,9 +316,14 @@ __device__ __forceinline__ double sublorentz_d(const GridDev &g, const StateDev 
 // cut y (1) or cut (2): Plinth_kernel (voigt.h:1091-1164) in FP64, the Voigt
 // profile by the region of r^2 = x_c^2 + y^2; 0 for the binned Gaussian (the
 // reference defines none).
+// the cut edge in Doppler units: cut iad (cutMode 0), cut y (1), cut (2)
+__device__ __forceinline__ double plinth_xc(const GridDev &g, double iad, double vy) {
+  return (g.cutMode == 1) ? g.cut * vy : (g.cutMode == 2 ? g.cut : g.cut * iad);
+}
+
 __device__ __forceinline__ double plinth_d(const GridDev &g, double S1, double Sc, double iad,
                                            double vy) {
-  const double xc = (g.cutMode == 1) ? g.cut * vy : (g.cutMode == 2 ? g.cut : g.cut * iad);
+  const double xc = plinth_xc(g, iad, vy);
   const double y2 = vy * vy;
   if (g.profile == 1) {
     const double r2 = xc * xc + y2;

@@ -75,16 +75,33 @@ __device__ __forceinline__ void prep_record(const LinesDev &L, const GridDev &g,
       // >= Y^2, a normal float)
       if (rmin < 0x1p-64 * umax || Y > 0x1p60 || (g.profile == 2 && Y < 0x1p-60)) flags |= HK_PF_RANGE;
     }
-    r.plr = 0.f;
+    r.ext0 = 0.f;
     r.inu = g.subL ? (float)(1.0 / ls.nu) : 0.f;
     if (g.plinth && w[5] > w[0] && S1 > 0.0) {
-      // (the mixed form is not run with plinth removal; the plinth per S1
-      // would be subtracted per point, and lines whose plinth exceeds 2^-13
-      // of their peak summed in FP64)
-      const double pl = plinth_d(g, S1, Sc, ls.iad, ls.vy);
-      r.plr = (float)(pl / S1);
-      const double peak = g.profile == 2 ? S1 / Y : Sc * erfcx(ls.vy);
-      if (!(pl <= 0x1p-13 * peak)) flags |= HK_PF_RANGE;
+      // The mixed form takes profile - plinth as t(x) - t(x_c) without
+      // cancellation where a point lies in the region of the cut edge x_c
+      // (the Lorentzian and GH2 differences factored by x_c - |x|, the
+      // Doppler one as t (1 - exp(-(x_c^2 - x^2))) with x_c - |x| from the
+      // FP64 offsets); elsewhere the term is at least 4 plinths, so the plain
+      // difference keeps FP32 accuracy.  A Voigt line whose cut edge lies in
+      // region C or within a factor 4 of a region boundary (r_c^2 < 400, or
+      // 0.999e6 <= r_c^2 < 4e6: a point and the edge in different regions
+      // with close values) and a line FP32 cannot hold are summed per point
+      // in FP64, from the record's FP64 vy, erfcx(vy) and plinth.
+      const double xc = plinth_xc(g, ls.iad, ls.vy);
+      rec_put_d(&r.ext0, xc);
+      bool pl64 = false;
+      if (g.profile <= 2) {
+        pl64 = (flags & (HK_PF_RANGE | HK_PF_WIDE)) != 0;
+        const double rc2 = xc * xc + Y;
+        if (g.profile == 1 && (rc2 < 400.0 || (rc2 >= 0.999e6 && rc2 < 4e6))) pl64 = true;
+      }
+      if (pl64) {
+        flags |= HK_PF_RANGE | HK_PF_PL64;
+        rec_put_d(&r.y, ls.vy);
+        rec_put_d(&r.sig1, ey);
+        rec_put_d(&r.B1, plinth_d(g, S1, Sc, ls.iad, ls.vy));
+      }
     }
     r.flags = flags;
     // region C's Algorithm-916 part: |x| < sqrt(36 - y^2), from the FP64

@@ -89,12 +89,17 @@ static_assert(sizeof(LinePrep) == 96, "LinePrep layout");
 //   ex: frexp exponent of the line's largest region-A/B term S1 / max(100, Y)
 //   flags: HK_PF_WIDE  -- some x^2 + Y in the cut window reaches 1e18;
 //          HK_PF_RANGE -- the window's terms span more than 2^64, or Y > 2^60:
-//                         FP32 sums cannot hold the line (FP64 instead).
-constexpr int HK_PF_WIDE = 2, HK_PF_RANGE = 1;
+//                         FP32 sums cannot hold the line (FP64 instead);
+//          HK_PF_PL64  -- plinth removal: the line is summed per point in
+//                         FP64 (set with HK_PF_RANGE; see below).
+constexpr int HK_PF_WIDE = 2, HK_PF_RANGE = 1, HK_PF_PL64 = 4;
 //   [t0, t1): the part of region C with |x| < sqrt(36 - y^2) (Algorithm 916
 //   in FP32; the rest of region C takes the asymptotic series)
-//   HK_PF_RANGE also marks a line whose plinth exceeds 2^-13 of its peak
-//   (with plinth removal, which the library runs in the FP64 form).
+//   ext0, inu: sub-Lorentzian wings: inu = 1 / nu.  Plinth removal (never
+//   together with sub-Lorentzian wings in the mixed form): the two words
+//   hold the cut edge x_c (double, Doppler units), and an HK_PF_PL64 line,
+//   whose FP32 profile fields are unused, holds vy (double) in {y, ey},
+//   erfcx(vy) in {sig1, A1} and its plinth in {B1, D2}.
 struct __align__(16) LinePrepF {
   double nu, iad;
   double S1, Sc;
@@ -104,10 +109,13 @@ struct __align__(16) LinePrepF {
   int ex, flags;
   int i0, b0, c0, c1, b1, i1;
   int t0, t1;
-  float plr;  // plinth / S1 (removePlinth), else 0
-  float inu;  // 1 / nu (sub-Lorentzian wings), else 0
+  float ext0, inu;
 };
 static_assert(sizeof(LinePrepF) == 112, "LinePrepF layout");
+
+// a double kept in two consecutive (8-byte aligned) float words of a record
+__host__ __device__ inline double rec_get_d(const float *w) { return *reinterpret_cast<const double *>(w); }
+__host__ __device__ inline void rec_put_d(float *w, double v) { *reinterpret_cast<double *>(w) = v; }
 
 // Per-(T, P) constants formed on the host.
 struct StateDev {

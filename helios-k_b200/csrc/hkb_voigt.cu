@@ -117,20 +117,42 @@ __device__ __forceinline__ double gauss_vb(const RecF &r) { return reinterpret_c
 // flags: HK_F_WEAK -- level above HK_MAX_LEVEL (2^768 below the strongest
 // line) or HK_PF_RANGE: the line is summed in FP64 with S1f = 1;
 // HK_F_WIDE -- some x^2 + Y in the window reaches 1e18, so two region-A
-// denominators may not be multiplied in FP32 (paired reciprocals are off).
+// denominators may not be multiplied in FP32 (paired reciprocals are off);
+// with plinth removal, HK_F_PLA / HK_F_PLB -- the cut edge x_c lies in
+// region A / B, whose points take the factored difference t(x) - t(x_c);
+// HK_F_PL64 -- the line is summed per point in FP64 (HK_PF_PL64).
 // The level sits in flags bits 8-11.
-constexpr int HK_F_WEAK = 1, HK_F_WIDE = 2;
+constexpr int HK_F_WEAK = 1, HK_F_WIDE = 2, HK_F_PLA = 4, HK_F_PLB = 8, HK_F_PL64 = 16;
 constexpr int HK_LEVEL_BITS = 96;
 constexpr int HK_MAX_LEVEL = 7;
 
+// Options of the mixed form with their own kernel instantiations: none,
+// sub-Lorentzian wings (chi factor), plinth removal.
+enum { HK_EXT_NONE = 0, HK_EXT_CHI = 1, HK_EXT_PL = 2 };
+
+// Per staged line with plinth removal (shared memory, beside its RecF):
+// x = D0 + k vb in FP64 (k the tile-local point), and
+//   factored lines: xd = x_c; plf the plinth in the line's FP32 units (the
+//     plain difference, where the term is at least 4 plinths); xcf = x_c;
+//     ic = 1 / (x_c^2 + Y) (edge in region A) or 1 / D(x_c^2) (region B);
+//     q0..q2 the GH2 difference polynomial (region B);
+//   FP64 lines: xd = the plinth, vy and ey = erfcx(vy) in FP64.
+struct __align__(16) ExtPL {
+  double D0, vb, xd, vy, ey;
+  float plf, xcf, ic, q0, q1, q2;
+};
+static_assert(sizeof(ExtPL) == 64, "ExtPL layout");
+
 // Shared memory of one mixed-form CTA: staged records, the per-line
 // region-C denominator tables (8 leading pad floats keep R[m-1-k] of the
-// first line in bounds for predicated reads), and the per-point FP64 sums.
+// first line in bounds for predicated reads), the per-point FP64 sums, and
+// the per-line option data (1 / nu for the chi factor, ExtPL).
 constexpr int HK_RPAD = 8;
-template <class SH, bool EXT = false>
+template <class SH, int EXT = HK_EXT_NONE>
 constexpr size_t smem_mixed() {
   return sizeof(RecF) * SH::CH + sizeof(float) * (HK_RPAD + SH::CH * HK_C916_MR) +
-         sizeof(double) * SH::G + (EXT ? sizeof(float2) * SH::CH : 0);
+         sizeof(double) * SH::G +
+         (EXT == HK_EXT_CHI ? sizeof(float) * SH::CH : EXT == HK_EXT_PL ? sizeof(ExtPL) * SH::CH : 0);
 }
 
 struct __align__(16) RecD {
@@ -220,10 +242,72 @@ __device__ __forceinline__ int line_key(const LinePrepF *__restrict__ P, int64_t
   return lev;
 }
 
-template <bool CG, bool G34, bool EXT = false>
+// The plinth data of a staged line (ExtPL) and its class flag.  S1f: the
+// line's FP32 scale (1 for a line summed in FP64); D0, vb: its FP64 offset at
+// the tile start and grid step.  GH2 in s = x^2 is S1 N(s) / D(s) with
+// N = s^2 + A1 s + B1, D = s^3 + D2 s^2 + D1 s + D0; its difference is
+//   t(s) - t(c) = S1 (c - s) Q(s) / (D(s) D(c)),  Q = q2 s^2 + q1 s + q0,
+// where (with Y = y^2 and p = 1/pi) every term of q0, q1, q2 is positive:
+//   q2 = c^2 + c (2Y + 5/2 - 4p) + Y^2 + 5Y/2 + 3/2,
+//   q1 = c^2 (2Y + 5/2 - 4p) + c (4Y^2 + 10Y - 18pY + 27/4 + 24p^2 - 27p)
+//        + 2Y^3 + (15/2 - 6p) Y^2 + (39/4 - 15p) Y + 9/2 - 9p,
+//   q0 = c^2 (Y^2 + 5Y/2 + 3/2) + c (2Y^3 + (15/2 - 6p) Y^2 + (39/4 - 15p) Y
+//        + 9/2 - 9p) + Y^4 + (5 - 2p) Y^3 + (39/4 - 3p) Y^2 + 9Y + 27/8,
+// so Q and the product hold FP32 accuracy at any distance from the edge.
+template <bool G34>
+__device__ __forceinline__ void stage_plinth(const LinePrepF &lp, const GridDev &g, double D0,
+                                             double vb, double S1f, RecF &r, ExtPL &e) {
+  e.D0 = D0;
+  e.vb = vb;
+  e.vy = e.ey = 0.0;
+  e.plf = e.xcf = e.ic = e.q0 = e.q1 = e.q2 = 0.f;
+  const double xc = rec_get_d(&lp.ext0);
+  e.xd = xc;
+  if (lp.flags & HK_PF_PL64) {
+    e.xd = rec_get_d(&lp.B1);
+    e.vy = rec_get_d(&lp.y);
+    e.ey = rec_get_d(&lp.sig1);
+    // the FP32 fields of the record hold FP64 words: give the staged line
+    // plain values (its sweep reads none of them)
+    r.y = (float)e.vy;
+    r.iy = 0.f;
+    r.ey = r.sig1 = 0.f;
+    r.t0 = r.t1 = r.c0;
+    r.flags |= HK_F_PL64;
+    return;
+  }
+  if (!(xc > 0.0)) return;  // no plinth (empty window)
+  e.xcf = (float)xc;
+  if (G34) return;          // Doppler: the factor 1 - exp(-(x_c^2 - x^2)) per point
+  const double c = xc * xc;
+  const double Y = (double)lp.y * (double)lp.y;
+  if (g.profile == 2 || c + Y >= 2e6) {
+    const double ic = 1.0 / (c + Y);
+    e.ic = (float)ic;
+    e.plf = (float)(S1f * ic);
+    r.flags |= HK_F_PLA;
+  } else {
+    const double D2 = lp.D2, D1 = lp.D1, D0c = lp.D0, A1 = lp.A1, B1 = lp.B1;
+    const double Dc = ((c + D2) * c + D1) * c + D0c;
+    const double Nc = (c + A1) * c + B1;
+    const double p = 0.31830988618379067;
+    const double Y2 = Y * Y, Y3 = Y2 * Y, Y4 = Y2 * Y2, c2 = c * c;
+    const double k1 = 2.0 * Y + 2.5 - 4.0 * p;
+    const double k0 = 2.0 * Y3 + (7.5 - 6.0 * p) * Y2 + (9.75 - 15.0 * p) * Y + 4.5 - 9.0 * p;
+    e.q2 = (float)(c2 + c * k1 + Y2 + 2.5 * Y + 1.5);
+    e.q1 = (float)(c2 * k1 + c * (4.0 * Y2 + (10.0 - 18.0 * p) * Y + 6.75 + 24.0 * p * p - 27.0 * p) + k0);
+    e.q0 = (float)(c2 * (Y2 + 2.5 * Y + 1.5) + c * k0 + Y4 + (5.0 - 2.0 * p) * Y3 +
+                   (9.75 - 3.0 * p) * Y2 + 9.0 * Y + 3.375);
+    e.ic = (float)(1.0 / Dc);
+    e.plf = (float)(S1f * Nc / Dc);
+    r.flags |= HK_F_PLB;
+  }
+}
+
+template <bool CG, bool G34, int EXT = HK_EXT_NONE>
 __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, const GridDev &g,
                                             int64_t l, int64_t g0, int64_t g1, int s1exp,
-                                            int key, RecF &r, float2 *ext = nullptr) {
+                                            int key, RecF &r, void *ext = nullptr) {
   const LinePrepF lp = load_record<CG>(P + l);
   const bool nonempty = key != HK_KEY_EMPTY;
   const bool weak = key == HK_KEY_WEAK;
@@ -265,17 +349,17 @@ __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, con
   r.t1 = clip_local(lp.t1, g0, g1);
   r.flags = ((lp.flags & HK_PF_WIDE) ? HK_F_WIDE : 0) | (weak ? HK_F_WEAK : 0) | (lev << 8);
   r.iy = lp.y > 0.f ? (float)(1.0 / (double)lp.y) : 0.f;
-  if (EXT) {
-    // plinth in the line's FP32 units (S1f = 1 for a weak line: then the
-    // plinth per S1, which its FP64 sweep scales), and 1 / nu
-    *ext = make_float2((float)((double)lp.plr * S1f), lp.inu);
-  }
+  if (EXT == HK_EXT_CHI) *static_cast<float *>(ext) = lp.inu;
+  if (EXT == HK_EXT_PL) stage_plinth<G34>(lp, g, D0, vb, S1f, r, *static_cast<ExtPL *>(ext));
   if (G34) {
     // Doppler / binned Gaussian: S1f exp(-u^2) with u = |x| (- vb / 2) is a
-    // normal float only for u^2 <= (126 + e) ln 2 (S1f < 2^e): the points
-    // beyond add exactly 0 in FP32 (flush to zero), as in the reference's
-    // FP32 kernels, so the window is cut to the rest.  Weak lines (FP64
-    // sums) keep their whole window.
+    // normal float only for u^2 <= (126 + e) ln 2 (S1f < 2^e), so the FP32
+    // sums take [t0, t1), where it is one with room to spare (e - 2 for
+    // the Doppler term; e - 30 for the binned Gaussian's erfcx factor), and
+    // the points beyond, out to where the FP64 term S1 exp(-u^2) (S1 / vb
+    // bounds the binned Gaussian's) falls below 2^-1075 and is exactly 0,
+    // are summed in FP64: [i0, t0) and [t1, i1).  Weak lines (FP64 sums)
+    // keep their whole window.
     const double h = g.profile == 4 ? 0.5 * vb : 0.0;
     if (g.profile == 4 && !weak) {
       // (erf(x + h) - erf(x - h)) / (2 vb) folded into the strength
@@ -285,14 +369,21 @@ __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, con
     if (!weak && nonempty) {
       int e = 0;
       frexp((double)r.S1f, &e);
-      const double u2 = (double)max(0, 126 + e) * 0.69314718055994531;
+      const double u2 = (double)max(0, (g.profile == 4 ? 96 : 124) + e) * 0.69314718055994531;
       const double xd = sqrt(u2) + h + 1e-6;
-      // tile points k with |D0 + k vb| <= xd
+      const double S1d = g.profile == 3 ? lp.Sc : lp.Sc * 1.7724538509055160273;
+      const double lt = log(fmax(S1d * fmax(1.0, 1.0 / vb), 1e-300));
+      const double xt = fmax(xd, sqrt(fmax(746.2 + lt, 0.0)) + h + 1e-6);
+      // tile points k with |D0 + k vb| <= xd (FP32) and <= xt (FP64)
+      const double n = (double)(g1 - g0);
       const double ka = ceil((-xd - D0) / vb), kb = floor((xd - D0) / vb) + 1.0;
-      const int k0 = (int)fmin(fmax(ka, 0.0), (double)(g1 - g0));
-      const int k1 = (int)fmin(fmax(kb, 0.0), (double)(g1 - g0));
-      r.i0 = max(r.i0, k0);
-      r.i1 = min(r.i1, k1);
+      const double ta = ceil((-xt - D0) / vb), tb = floor((xt - D0) / vb) + 1.0;
+      const int k0 = (int)fmin(fmax(ka, 0.0), n), k1 = (int)fmin(fmax(kb, 0.0), n);
+      const int u0 = (int)fmin(fmax(ta, 0.0), n), u1 = (int)fmin(fmax(tb, 0.0), n);
+      r.i0 = max(r.i0, u0);
+      r.i1 = max(r.i0, min(r.i1, u1));
+      r.t0 = min(max(r.i0, k0), r.i1);
+      r.t1 = max(r.t0, min(r.i1, k1));
       r.b0 = r.c0 = r.c1 = r.b1 = r.i0;  // region A only
     }
   }
@@ -368,10 +459,9 @@ __device__ __forceinline__ int classify(const RecF &r, int wb) {
 // every term of a grid point lo < x < hi times chi(|x - nu|) x / nu (sLChi
 // voigt.h:47-72), chi = exp(-B1 clamp(d - s1, 0, s2 - s1) - B2 clamp(d - s2,
 // 0, s3 - s2) - B3 max(d - s3, 0)) -- the reference's piecewise exponential
-// written as one continuous expression.  The sweep also subtracts a plinth
-// per point when the staged plinth is nonzero; the library runs plinth
-// removal in the FP64 form (the FP32 difference profile - plinth cancels
-// near window edges), so in practice that plinth is 0.
+// written as one continuous expression.  (With plinth removal too, chi t -
+// plinth is no difference of one function, so the library runs the pair in
+// the FP64 form.)
 struct ExtF {
   float s1, s2, s3, B1, B2, B3;  // chi breakpoints (cm^-1) and the state's slopes
   int kl0, kl1;                  // tile points with sl_lo < x < sl_hi
@@ -567,11 +657,35 @@ __device__ __forceinline__ float gauss_scaled(double u, float mS, int eS) {
   return mS * ex2_fast(-f) * sc;
 }
 
-template <bool AM, int PPL>
+// PL: plinth removal (Doppler): t (1 - exp(-(x_c^2 - x^2))) with
+// x_c^2 - x^2 = (x_c - x)(x_c + x) from the FP64 offset, no cancellation.
+// The FP32 part [t0, t1) adds to the FP32 sums; the FP64 tails [i0, t0)
+// and [t1, i1) add the FP64 form's term to cacc.
+template <int PPL, bool PL = false>
 __device__ __forceinline__ void sweep_G34(const RecF &rr, int profile, int wb, int lane,
-                                          const float2 (&kf)[PPL / 2], float2 (&a32)[PPL / 2]) {
-  const int lo = max(rr.i0, wb), hi = min(rr.i1, wb + 32 * PPL);
+                                          const float2 (&kf)[PPL / 2], float2 (&a32)[PPL / 2],
+                                          double *__restrict__ cacc, const ExtPL *pe = nullptr) {
+  const int we = wb + 32 * PPL;
+  const int lo = max(rr.t0, wb), hi = min(rr.t1, we);
   const double D0 = gauss_D0(rr), vb = gauss_vb(rr);
+  if (max(rr.i0, wb) < min(rr.t0, we) || max(rr.t1, wb) < min(rr.i1, we)) {
+    const double S1 = profile == 3 ? rr.Sc : rr.Sc * 1.7724538509055160273;  // S / sqrt(pi), S
+#pragma unroll 1
+    for (int p = 0; p < PPL; ++p) {
+      const int k = wb + lane + 32 * p;
+      if ((k >= rr.i0 && k < rr.t0) || (k >= rr.t1 && k < rr.i1)) {
+        const double x = fma((double)k, vb, D0);
+        double v = profile_a_d(profile, x, 0.0, S1, vb);
+        if (PL) {
+          const double ax = fabs(x);
+          v *= -expm1(-(pe->xd - ax) * (pe->xd + ax));
+        }
+        cacc[k] += v;
+      }
+    }
+  }
+  if (lo >= hi) return;
+  const bool full = lo == wb && hi == we;
   const float h = rr.C1;
   int eS = 0;
   const float mS = 2.0f * frexpf(rr.S1f, &eS);  // S1f = mS 2^(eS - 1), mS in [1, 2)
@@ -579,7 +693,7 @@ __device__ __forceinline__ void sweep_G34(const RecF &rr, int profile, int wb, i
 #pragma unroll
   for (int p = 0; p < PPL; ++p) {
     const int k = wb + lane + 32 * p;
-    if (AM && !(k >= lo && k < hi)) continue;
+    if (!full && !(k >= lo && k < hi)) continue;
     const float kk = (p & 1) ? kf[p >> 1].y : kf[p >> 1].x;
     const double x = fabs(fma((double)kk, vb, D0));
     float t;
@@ -593,6 +707,7 @@ __device__ __forceinline__ void sweep_G34(const RecF &rr, int profile, int wb, i
       const float xf = (float)x;
       t = rr.S1f * (erff(xf + h) - erff(xf - h));
     }
+    if (PL) t *= -expm1f(-(float)(pe->xd - x) * (pe->xcf + (float)x));
     if (p & 1) a32[p >> 1].y += t;
     else a32[p >> 1].x += t;
   }
@@ -605,7 +720,10 @@ __device__ __forceinline__ void sweep_G34(const RecF &rr, int profile, int wb, i
 // within rounding of r = 6 may take either evaluator (both hold there).
 // Points leave their owning lane here, so the warp syncs before cacc is
 // touched again.
-template <int SLICE, bool EXT = false>
+// EXT: HK_EXT_CHI multiplies the chi factor (ex, inu = 1 / nu); HK_EXT_PL
+// subtracts the plinth pld (FP64 units), which a point of region C exceeds
+// at least fourfold (the line's edge lies in region A or B, r_c^2 >= 400).
+template <int SLICE, int EXT = HK_EXT_NONE>
 __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__ Rj,
                                         double *__restrict__ cacc, int wb, int lane,
                                         const ExtF *ex = nullptr, float inu = 0.f, double pld = 0.0) {
@@ -620,7 +738,7 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
     const float kk = (float)k;
     const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
     float v = voigt916_core(x, y, iy, ey, sig1, Rj);
-    if (EXT && k >= ex->kl0 && k < ex->kl1) v *= chi_factor(*ex, x, r.vb, inu);
+    if (EXT == HK_EXT_CHI && k >= ex->kl0 && k < ex->kl1) v *= chi_factor(*ex, x, r.vb, inu);
     cacc[k] = fma(Sc, (double)v, cacc[k]) - pld;
   }
   const int n1 = t0 - lo, ns = n1 + (hi - t1);
@@ -629,7 +747,7 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
     const float kk = (float)k;
     const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
     float v = voigt_asy(x, y);
-    if (EXT && k >= ex->kl0 && k < ex->kl1) v *= chi_factor(*ex, x, r.vb, inu);
+    if (EXT == HK_EXT_CHI && k >= ex->kl0 && k < ex->kl1) v *= chi_factor(*ex, x, r.vb, inu);
     cacc[k] = fma(Sc, (double)v, cacc[k]) - pld;
   }
   __syncwarp();
@@ -637,15 +755,20 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
 
 // A/B boundaries in the slice, and weak lines: per-point window/region
 // tests.  WEAK lines (S1f = 1) add S1 t in FP64 to cacc; the others add
-// S1f t to the FP32 sums.
-template <bool WEAK, bool G34, int PPL, bool EXT = false>
+// S1f t to the FP32 sums.  EXT == HK_EXT_CHI: every term times the chi
+// factor (ex, inu = 1 / nu).  EXT == HK_EXT_PL: the term less the plinth
+// (pe): at a point of the edge's region (HK_F_PLA / HK_F_PLB) the factored
+// difference, with x_c - |x| from the FP64 offset, elsewhere t - plinth.
+template <bool WEAK, bool G34, int PPL, int EXT = HK_EXT_NONE>
 __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
                                         const float2 (&kf)[PPL / 2],
                                         float2 (&a32)[PPL / 2],
                                         double *__restrict__ cacc, int profile,
-                                        const ExtF *ex = nullptr, float2 xt = make_float2(0.f, 0.f)) {
+                                        const ExtF *ex = nullptr, float inu = 0.f,
+                                        const ExtPL *pe = nullptr) {
   if (WEAK && G34) {
     // Doppler / binned Gaussian lines summed in FP64: the FP64 form's term
+    // (with plinth removal: times 1 - exp(-(x_c^2 - x^2)), x_c - |x| exact)
     const double D0 = gauss_D0(r), vb = gauss_vb(r);
     const double S1 = profile == 3 ? r.Sc : r.Sc * 1.7724538509055160273;  // S / sqrt(pi), S
 #pragma unroll
@@ -653,7 +776,13 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
       const int k = wb + lane + 32 * p;
       if (k >= r.i0 && k < r.i1) {
         const float kk = (p & 1) ? kf[p >> 1].y : kf[p >> 1].x;
-        cacc[k] += profile_a_d(profile, fma((double)kk, vb, D0), 0.0, S1, vb);
+        const double x = fma((double)kk, vb, D0);
+        double v = profile_a_d(profile, x, 0.0, S1, vb);
+        if (EXT == HK_EXT_PL) {
+          const double ax = fabs(x);
+          v *= -expm1(-(pe->xd - ax) * (pe->xd + ax));
+        }
+        cacc[k] += v;
       }
     }
     return;
@@ -668,9 +797,8 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
   const float S1f = r.S1f, C1 = r.C1, C0 = r.C0;
   const float D2 = r.D2, D1 = r.D1, D0 = r.D0;
   const double S1w = WEAK ? r.Sc * (double)y * 0.56418958354775628 : 0.0;  // S y / pi
-  // EXT: the plinth in FP32 units (a weak line's in FP64 from its plinth / S1)
-  const float plf = EXT ? xt.x : 0.f;
-  const double plw = (EXT && WEAK) ? (double)xt.x * S1w : 0.0;
+  const int plc = EXT == HK_EXT_PL ? (r.flags & (HK_F_PLA | HK_F_PLB)) : 0;
+  const float plf = EXT == HK_EXT_PL ? pe->plf : 0.f;
 #pragma unroll
   for (int p = 0; p < PPL; ++p) {
     const int k = wb + lane + 32 * p;
@@ -680,22 +808,42 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
       const float s = x * x;
       // the term as (factor, reciprocal), added with one FMA like the packed sweeps
       float f, inv;
-      if (k >= b0 && k < b1) {
+      const bool inB = k >= b0 && k < b1;
+      if (inB) {
         f = fmaf(s, fmaf(S1f, s, C1), C0);
         inv = rcp_fast(fmaf(fmaf(s + D2, s, D1), s, D0));
       } else {
         f = S1f;
         inv = rcp_fast(fmaf(x, x, Yf));
       }
-      if (EXT) {
-        float t = f * inv;
-        if (k >= ex->kl0 && k < ex->kl1) t *= chi_factor(*ex, x, vb, xt.y);
-        if (WEAK) {
-          cacc[k] = fma(S1w, (double)t, cacc[k]) - plw;
-        } else if (p & 1) {
-          a32[p >> 1].y += t - plf;
+      if (EXT == HK_EXT_PL) {
+        float t;
+        if (plc == (inB ? HK_F_PLB : HK_F_PLA)) {
+          // (x_c - |x|)(x_c + |x|) = x_c^2 - s; times 1 / (x_c^2 + Y) in
+          // region A, times Q(s) / D(x_c^2) in region B
+          const float dx = (float)(pe->xd - fabs(fma((double)k, pe->vb, pe->D0)));
+          float w = dx * (pe->xcf + fabsf(x)) * pe->ic;
+          if (inB) w *= fmaf(fmaf(pe->q2, s, pe->q1), s, pe->q0);
+          t = (S1f * inv) * w;
         } else {
-          a32[p >> 1].x += t - plf;
+          t = fmaf(f, inv, -plf);
+        }
+        if (WEAK) {
+          cacc[k] = fma(S1w, (double)t, cacc[k]);
+        } else if (p & 1) {
+          a32[p >> 1].y += t;
+        } else {
+          a32[p >> 1].x += t;
+        }
+      } else if (EXT == HK_EXT_CHI) {
+        float t = f * inv;
+        if (k >= ex->kl0 && k < ex->kl1) t *= chi_factor(*ex, x, vb, inu);
+        if (WEAK) {
+          cacc[k] = fma(S1w, (double)t, cacc[k]);
+        } else if (p & 1) {
+          a32[p >> 1].y += t;
+        } else {
+          a32[p >> 1].x += t;
         }
       } else if (WEAK) {
         cacc[k] = fma(S1w, (double)(f * inv), cacc[k]);
@@ -704,6 +852,31 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
       } else {
         a32[p >> 1].x = fmaf(f, inv, a32[p >> 1].x);
       }
+    }
+  }
+}
+
+// Plinth removal, a line summed per point in FP64 (HK_F_PL64: its cut edge
+// lies in region C or close to a region boundary, or FP32 cannot hold it):
+// the FP64 form's terms (regions C, B, A) less the plinth, from the line's
+// FP64 vy, erfcx(vy) and plinth (pe) and x = D0 + k vb.
+template <int PPL>
+__device__ __forceinline__ void sweep_pl64(const RecF &r, const ExtPL &pe, int wb, int lane,
+                                           double *__restrict__ cacc, int profile) {
+  const int we = wb + 32 * PPL;
+  if (r.i1 <= wb || r.i0 >= we) return;
+  const double vy = pe.vy, Y = vy * vy;
+  const double S1 = r.Sc * vy * 0.56418958354775628;  // S vy / pi
+#pragma unroll 1
+  for (int p = 0; p < PPL; ++p) {
+    const int k = wb + lane + 32 * p;
+    if (k >= r.i0 && k < r.i1) {
+      const double x = fma((double)k, pe.vb, pe.D0);
+      double v;
+      if (k >= r.c0 && k < r.c1) v = r.Sc * voigt916_d(x, vy, pe.ey);
+      else if (k >= r.b0 && k < r.b1) v = S1 * gh2_d(x, Y);
+      else v = profile_a_d(profile, x, Y, S1, pe.vb);
+      cacc[k] += v - pe.xd;
     }
   }
 }
@@ -789,7 +962,7 @@ __device__ __forceinline__ void flush_sums(float2 (&a32)[PPL / 2], double *__res
 // split tile, published to pt (this tile's nsplit partial rows of G points)
 // and combined in part order by the CTA that completes the count *cnt.
 // wmax and s1exp are the state's search half-width and FP32 scale exponent.
-template <bool MIXED, class SH, bool CG, bool G34 = false, bool EXT = false>
+template <bool MIXED, class SH, bool CG, bool G34 = false, int EXT = HK_EXT_NONE>
 __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__restrict__ nu0,
                                          int64_t nlines, const GridDev &g, const StateDev &st,
                                          double wmax, int s1exp, int64_t g0, int64_t g1, int part,
@@ -824,10 +997,12 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
   }
   __syncthreads();
   const int64_t L0 = s_L0, L1 = s_L1;
-  // plinth and 1 / nu of the staged lines (EXT), after the per-point sums
-  float2 *ext = reinterpret_cast<float2 *>(cacc + G);
+  // per staged line: 1 / nu (chi factor) or ExtPL (plinth), after the
+  // per-point sums
+  float *ext_inu = reinterpret_cast<float *>(cacc + G);
+  ExtPL *ext_pl = reinterpret_cast<ExtPL *>(cacc + G);
   ExtF exc;
-  if (EXT) exc = ext_consts(g, st, g0, g1);
+  if (EXT == HK_EXT_CHI) exc = ext_consts(g, st, g0, g1);
 
   float2 kf[PPL / 2];   // lane-local point indices, paired {p, p+1}
   float2 a32[PPL / 2];  // mixed: FP32 sums of the current chunk (scaled)
@@ -887,7 +1062,8 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
           for (int w = 0; w < CH / 32; ++w) pos += s_kcnt[w][v];
         for (int w = 0; w < warp; ++w) pos += s_kcnt[w][key];
         RecF r;
-        stage_mixed<CG, G34, EXT>(PF, g, l, g0, g1, s1exp, key, r, ext + pos);
+        stage_mixed<CG, G34, EXT>(PF, g, l, g0, g1, s1exp, key, r,
+                                  EXT == HK_EXT_PL ? (void *)(ext_pl + pos) : (void *)(ext_inu + pos));
         reinterpret_cast<RecF *>(rec)[pos] = r;
         if (r.c1 > r.c0 && r.i1 > r.i0) stage_rtab(r.y, Rtab + pos * HK_C916_MR);
       }
@@ -918,20 +1094,34 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
             m = __ballot_sync(0xffffffffu, lev == lcur) & live;
           }
           live &= ~m;
-          if constexpr (EXT) {
-            // every class through the generic sweep with chi and plinth
+          if constexpr (EXT == HK_EXT_CHI) {
+            // every class through the generic sweep with the chi factor
+            unsigned mX = m;
+            while (mX) {
+              const int b = __ffs(mX) - 1;
+              mX &= mX - 1;
+              const float inu = ext_inu[g32 + b];
+              sweep_G<false, false, PPL, EXT>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile, &exc, inu);
+              sweep_C<SLICE, EXT>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, &exc, inu);
+            }
+            continue;
+          }
+          if constexpr (EXT == HK_EXT_PL && !G34) {
+            // every class through the generic sweep less the plinth
             const double u = ldexp(1.0, -(s1exp + HK_LEVEL_BITS * lcur));
             unsigned mX = m;
             while (mX) {
               const int b = __ffs(mX) - 1;
               mX &= mX - 1;
-              const float2 xt = ext[g32 + b];
-              sweep_G<false, false, PPL, true>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile, &exc, xt);
-              sweep_C<SLICE, true>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, &exc, xt.y,
-                                   (double)xt.x * u);
+              const ExtPL *pe = ext_pl + g32 + b;
+              sweep_G<false, false, PPL, EXT>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile, nullptr, 0.f,
+                                              pe);
+              sweep_C<SLICE, EXT>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, nullptr, 0.f,
+                                  (double)pe->plf * u);
             }
             continue;
           }
+          constexpr bool PLG = EXT == HK_EXT_PL && G34;  // Doppler with plinth removal
           unsigned mB = m & bB, mA = m & bA, mBM = m & bBM, mAM = m & bAM, mG = m & bG;
           while (mB) {
             const int b = __ffs(mB) - 1;
@@ -941,7 +1131,7 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
           while (mA) {
             const int b = __ffs(mA) - 1;
             mA &= mA - 1;
-            if constexpr (G34) sweep_G34<false, PPL>(rf[g32 + b], g.profile, wb, lane, kf, a32);
+            if constexpr (G34) sweep_G34<PPL, PLG>(rf[g32 + b], g.profile, wb, lane, kf, a32, cacc, ext_pl + g32 + b);
             else sweep_A<false, PPL>(rf[g32 + b], wb, lane, kf, a32);
           }
           while (mBM) {
@@ -953,7 +1143,7 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
           while (mAM) {
             const int b = __ffs(mAM) - 1;
             mAM &= mAM - 1;
-            if constexpr (G34) sweep_G34<true, PPL>(rf[g32 + b], g.profile, wb, lane, kf, a32);
+            if constexpr (G34) sweep_G34<PPL, PLG>(rf[g32 + b], g.profile, wb, lane, kf, a32, cacc, ext_pl + g32 + b);
             else sweep_A<true, PPL>(rf[g32 + b], wb, lane, kf, a32);
           }
           while (mG) {
@@ -966,13 +1156,24 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
         while (mW) {
           const int b = __ffs(mW) - 1;
           mW &= mW - 1;
-          if constexpr (EXT) {
-            // weak line: FP64 sums; its plinth from plinth / S1 (S1f = 1)
-            const float2 xt = ext[g32 + b];
+          if constexpr (EXT == HK_EXT_CHI) {
+            const float inu = ext_inu[g32 + b];
+            sweep_G<true, false, PPL, EXT>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile, &exc, inu);
+            sweep_C<SLICE, EXT>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, &exc, inu);
+          } else if constexpr (EXT == HK_EXT_PL) {
+            // FP64 sums (S1f = 1): the plinth per S1 scaled by S1, or the
+            // whole line per point in FP64
+            const ExtPL *pe = ext_pl + g32 + b;
             const RecF &rw = rf[g32 + b];
-            sweep_G<true, false, PPL, true>(rw, wb, lane, kf, a32, cacc, g.profile, &exc, xt);
-            sweep_C<SLICE, true>(rw, Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, &exc, xt.y,
-                                 (double)xt.x * (rw.Sc * (double)rw.y * 0.56418958354775628));
+            if constexpr (G34) {
+              sweep_G<true, true, PPL, EXT>(rw, wb, lane, kf, a32, cacc, g.profile, nullptr, 0.f, pe);
+            } else if (rw.flags & HK_F_PL64) {
+              sweep_pl64<PPL>(rw, *pe, wb, lane, cacc, g.profile);
+            } else {
+              sweep_G<true, false, PPL, EXT>(rw, wb, lane, kf, a32, cacc, g.profile, nullptr, 0.f, pe);
+              sweep_C<SLICE, EXT>(rw, Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, nullptr, 0.f,
+                                  (double)pe->plf * (rw.Sc * (double)rw.y * 0.56418958354775628));
+            }
           } else {
             sweep_G<true, G34, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile);
             sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
@@ -1030,7 +1231,7 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
 // mixed form: SH::MINB CTAs per SM (4: 32 warps, 64 registers)
 // G34: the Doppler / binned-Gaussian profiles of the mixed form (their own
 // instantiation, so the Voigt and Lorentz kernels carry none of their code)
-template <bool MIXED, class SH, bool G34 = false, bool EXT = false>
+template <bool MIXED, class SH, bool G34 = false, int EXT = HK_EXT_NONE>
 __global__ void __launch_bounds__(SH::THREADS, MIXED ? SH::MINB : 2)
 voigt_sum_kernel(const void *__restrict__ prep, const double *__restrict__ nu0,
                  int64_t nlines, GridDev g, const StateDev *__restrict__ states,
@@ -1153,7 +1354,7 @@ __device__ __noinline__ void prep_lines(const LinesDev &L, const GridDev &g, con
   for (; l < l1; l += step) prep_record<MIXED, PREP_ALL>(L, g, st, l, e916, out, w_loc, s1_loc);
 }
 
-template <bool MIXED, class SH, bool G34 = false, bool EXT = false>
+template <bool MIXED, class SH, bool G34 = false, int EXT = HK_EXT_NONE>
 __global__ void __launch_bounds__(SH::THREADS, MIXED ? SH::MINB : 2)
 voigt_table_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states, TableSched sc,
                    void *ring, double *partial, unsigned *tile_cnt, unsigned long long *ticket,
@@ -1308,16 +1509,32 @@ int voigt_tile_points(int shape) { return HK_SHAPE_G[shape < 0 || shape >= HK_NS
 int voigt_chunk_lines(int shape) { return HK_SHAPE_CH[shape < 0 || shape >= HK_NSHAPES ? 0 : shape]; }
 int voigt_tile_warps(int shape) { return HK_SHAPE_WARPS[shape < 0 || shape >= HK_NSHAPES ? 0 : shape]; }
 
+// The option instantiation of the mixed form for a grid's options (the
+// host runs sub-Lorentzian wings with plinth removal, and the Gaussian
+// profiles with sub-Lorentzian wings, in the FP64 form).
+static int ext_kind(const GridDev &g) {
+  if (g.subL) return HK_EXT_CHI;
+  if (g.plinth) return HK_EXT_PL;
+  return HK_EXT_NONE;
+}
+
 // Calls f(kernel, dynamic shared memory) for the kernel of (precision,
 // shape); the plain FP64 form has the default shape only.
 template <class F>
-static cudaError_t with_kernel(bool mixed, int shape, F &&f, bool g34 = false, bool ext = false) {
+static cudaError_t with_kernel(bool mixed, int shape, F &&f, bool g34 = false, int ext = HK_EXT_NONE) {
   using KFn = void (*)(const void *, const double *, int64_t, GridDev, const StateDev *, int, int,
                        int, int, unsigned *, double *, unsigned *, double *, int64_t);
   if (!mixed) return f((KFn)voigt_sum_kernel<false, Shape0>, sizeof(RecD) * Shape0::CH, Shape0::THREADS);
+  if (g34 && ext == HK_EXT_PL)
+    return f((KFn)voigt_sum_kernel<true, Shape0, true, HK_EXT_PL>, smem_mixed<Shape0, HK_EXT_PL>(),
+             Shape0::THREADS);
   if (g34) return f((KFn)voigt_sum_kernel<true, Shape0, true>, smem_mixed<Shape0>(), Shape0::THREADS);
-  if (ext)
-    return f((KFn)voigt_sum_kernel<true, Shape0, false, true>, smem_mixed<Shape0, true>(), Shape0::THREADS);
+  if (ext == HK_EXT_CHI)
+    return f((KFn)voigt_sum_kernel<true, Shape0, false, HK_EXT_CHI>, smem_mixed<Shape0, HK_EXT_CHI>(),
+             Shape0::THREADS);
+  if (ext == HK_EXT_PL)
+    return f((KFn)voigt_sum_kernel<true, Shape0, false, HK_EXT_PL>, smem_mixed<Shape0, HK_EXT_PL>(),
+             Shape0::THREADS);
   switch (shape) {
 #define HK_SHAPE_CASE(n) \
   case n: return f((KFn)voigt_sum_kernel<true, Shape##n>, smem_mixed<Shape##n>(), Shape##n::THREADS);
@@ -1415,20 +1632,26 @@ cudaError_t launch_voigt_sum(bool mixed, const VoigtPlan &pl, const void *prep_d
                                             pl.tiles_per_state, pl.nsplit, total, ticket_d,
                                             partial_d, tile_cnt_d, K_d, k_stride);
     return cudaGetLastError();
-  }, mixed && g.profile >= 3, mixed && g.profile <= 2 && g.subL);
+  }, mixed && g.profile >= 3, mixed ? ext_kind(g) : HK_EXT_NONE);
   return e;
 }
 
 // The fused table kernel of (precision, shape) and its dynamic shared memory.
 template <class F>
-static cudaError_t with_table_kernel(bool mixed, int shape, F &&f, bool g34 = false, bool ext = false) {
+static cudaError_t with_table_kernel(bool mixed, int shape, F &&f, bool g34 = false, int ext = HK_EXT_NONE) {
   using KFn = void (*)(LinesDev, GridDev, const StateDev *, TableSched, void *, double *, unsigned *,
                        unsigned long long *, unsigned long long *, unsigned *, unsigned *, unsigned *,
                        TableFin *, int *, double *, int64_t);
   if (!mixed) return f((KFn)voigt_table_kernel<false, Shape0>, sizeof(RecD) * Shape0::CH, Shape0::THREADS);
+  if (g34 && ext == HK_EXT_PL)
+    return f((KFn)voigt_table_kernel<true, Shape0, true, HK_EXT_PL>, smem_mixed<Shape0, HK_EXT_PL>(),
+             Shape0::THREADS);
   if (g34) return f((KFn)voigt_table_kernel<true, Shape0, true>, smem_mixed<Shape0>(), Shape0::THREADS);
-  if (ext)
-    return f((KFn)voigt_table_kernel<true, Shape0, false, true>, smem_mixed<Shape0, true>(),
+  if (ext == HK_EXT_CHI)
+    return f((KFn)voigt_table_kernel<true, Shape0, false, HK_EXT_CHI>, smem_mixed<Shape0, HK_EXT_CHI>(),
+             Shape0::THREADS);
+  if (ext == HK_EXT_PL)
+    return f((KFn)voigt_table_kernel<true, Shape0, false, HK_EXT_PL>, smem_mixed<Shape0, HK_EXT_PL>(),
              Shape0::THREADS);
   switch (shape) {
 #define HK_SHAPE_CASE(n) \
@@ -1514,7 +1737,7 @@ cudaError_t launch_voigt_table(bool mixed, const TablePlan &tp, const LinesDev &
     kfn<<<ctas, threads, smem, stream>>>(L, g, states_d, sc, b.ring, b.partial, b.tile_cnt, ticket, wbits,
                                          prep_cnt, sum_cnt, ready, fin, err, K_d, k_stride);
     return cudaGetLastError();
-  }, mixed && g.profile >= 3, mixed && g.profile <= 2 && g.subL);
+  }, mixed && g.profile >= 3, mixed ? ext_kind(g) : HK_EXT_NONE);
 }
 
 int *table_error_word(void *sync_d, int nstates) {

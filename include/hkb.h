@@ -202,9 +202,12 @@ hk_status hk_set_workspace(hk_ctx *ctx, double prep_bytes, double part_bytes);
  * window; remove_plinth 1 (param.dat `removePlinth`) subtracts each line's
  * profile value at its cut edge (Plinth_kernel voigt.h:1091-1164) from every
  * point of its window.  All four profiles have a mixed (FP32) form -- the
- * Doppler and binned-Gaussian terms evaluated where they are normal FP32
- * floats -- and an adjoint; plinth removal runs the FP64 form whatever
- * precision hk_opacity is given, and the adjoint refuses it. */
+ * Doppler and binned-Gaussian terms in FP32 where they are normal floats,
+ * in FP64 beyond -- and an adjoint.  Plinth removal has a mixed form too (profile -
+ * plinth formed without cancellation: factored differences in FP32, and FP64
+ * per point for a Voigt line whose cut edge lies in region C or near a
+ * region boundary), except with sub-Lorentzian wings (FP64 form); the
+ * adjoint refuses it. */
 hk_status hk_set_profile(hk_ctx *ctx, int profile, int remove_plinth);
 
 /* Sub-Lorentzian line wings (param.dat subLorentzianfile; Perrin & Hartmann
@@ -213,8 +216,9 @@ hk_status hk_set_profile(hk_ctx *ctx, int profile, int remove_plinth);
  * epsilon3, x_lo, x_hi}; every term at a grid point lo < x < hi is multiplied
  * by chi(|x - nu|) x / nu, chi = 1 below sigma1 and exp(-B1 (d - sigma1)
  * ...) beyond, B_k = alpha_k + beta_k exp(-epsilon_k T).  NULL turns it off.
- * The mixed form applies it to the Voigt and Lorentz profiles (the Doppler
- * and binned-Gaussian profiles with it run the FP64 form); the adjoint
+ * The mixed form applies it to the Voigt and Lorentz profiles without
+ * plinth removal (the Doppler and binned-Gaussian profiles with it, and
+ * either profile with plinth removal too, run the FP64 form); the adjoint
  * refuses it. */
 hk_status hk_set_sublorentzian(hk_ctx *ctx, const double *p);
 

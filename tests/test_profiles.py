@@ -2,13 +2,16 @@
 oracle (voigt.h:1091-1262 restated).
 
 The mixed form runs when the mixed precision is asked for -- the Voigt and
-Lorentz profiles with and without sub-Lorentzian wings, the Doppler and
-binned-Gaussian profiles (where their FP32 terms are normal floats): 1e-5
-relative where K > 1e-6 of its bin maximum (the mixed bound), and faster
-than the FP64 form.  Plinth removal runs the FP64 form in both precisions
-(profile - plinth cancels near window edges), so its bound is the FP64 one
-for differences of profile values and plinths: 1e-9; the FP64 form itself:
-1e-12.  Index windows (no regions B and C for profiles 2-4) are bit-exact.
+Lorentz profiles with sub-Lorentzian wings or plinth removal, the Doppler
+profile with plinth removal, the binned Gaussian (FP32 where their terms are
+normal floats, FP64 tails beyond): 1e-5 relative where K > 1e-6 of its bin maximum (the mixed
+bound), and faster than the FP64 form.  Plinth removal in the mixed form
+takes profile - plinth without cancellation (factored differences, or FP64
+per point for lines whose cut edge lies in region C or near a region
+boundary); sub-Lorentzian wings with plinth removal run the FP64 form, whose
+bound for differences of profile values and plinths is 1e-9; the FP64 form
+itself: 1e-12.  Index windows (no regions B and C for profiles 2-4) are
+bit-exact.
 """
 import numpy as np
 import pytest
@@ -70,11 +73,13 @@ def test_profile_matches_oracle(small, profile, plinth, cutMode, cut):
             err, n = masked_relerr(K, Kref, NBINS)
             print(f"profile {profile} plinth {plinth} cut {cutMode}/{cut} T={T} P={P} "
                   f"precision {prec}: err {err:.2e}, line sum {ms[prec]:.3f} ms")
-            if prec == hkb.MIXED and not plinth:
+            if prec == hkb.MIXED:
                 assert err < 1e-5
             else:
                 assert err < (1e-9 if plinth else 1e-12)
-        if not plinth:
+        # the mixed form saves per-pair work; with windows of a few points
+        # (the 0.05 cm^-1 Doppler cut) per-tile costs decide either form
+        if ms[hkb.PLAIN_FP64] > 0.2:
             assert ms[hkb.MIXED] < ms[hkb.PLAIN_FP64]
     if not plinth:
         ctx.opacity_vjp(1500.0, 0.1, np.ones(ctx.nx))  # every profile has an adjoint
@@ -133,10 +138,11 @@ def test_sublorentzian_matches_oracle(small, profile, plinth):
 
 
 @pytest.mark.parametrize("profile,plinth,subl", [(3, 0, False), (4, 0, False), (1, 0, True),
-                                                 (2, 0, True)])
+                                                 (2, 0, True), (1, 1, False), (2, 1, False),
+                                                 (3, 1, False)])
 def test_profile_tables_equal_opacity(small, profile, plinth, subl):
-    """The mixed kernels of the Gaussian profiles and of sub-Lorentzian wings
-    in both table modes (per-batch launches and one persistent launch) give
+    """The mixed kernels of the Gaussian profiles, of sub-Lorentzian wings and
+    of plinth removal in both table modes (per-batch launches and one persistent launch) give
     the same bits as hk_opacity."""
     import torch
     ctx = small["ctx"]
@@ -163,4 +169,56 @@ def test_profile_tables_equal_opacity(small, profile, plinth, subl):
     finally:
         ctx.set_table_mode(0)
         ctx.set_sublorentzian(None)
+        ctx.set_profile(1, 0)
+
+
+# Plinth removal with cut edges in bins of their own: 60 lines over 12
+# decades of strength, 10 cm^-1 bins, so most bins hold one or two windows
+# and K at a point beside a cut edge is that line's profile - plinth alone
+# (the plain FP32 difference misses 1e-5 there by orders of magnitude).  The
+# cut rules put the edges in every class: r_c^2 = x_c^2 + y^2 below 400 and
+# within a factor 4 of r^2 = 1e6 (FP64 per point), in region B and in
+# region A (factored differences).
+SPARSE_BINS = 300
+EDGE_CASES = [(1, 0, 25.0), (1, 1, 300.0), (1, 1, 3.0), (1, 2, 15.0), (1, 2, 100.0),
+              (1, 2, 1500.0), (1, 2, 5000.0), (2, 0, 25.0), (2, 1, 50.0), (3, 2, 4.0),
+              (3, 0, 0.03)]
+
+
+@pytest.fixture(scope="module")
+def sparse():
+    L = synth.hitran_lines(60, seed=5, nu_max=3000.0)
+    Tq, Qq = synth.q_table()
+    ctx = hkb.Context(0)
+    ctx.set_species(hkb.HITRAN, [synth.MASS], [1.0])
+    ctx.set_partition(0, Tq, Qq)
+    ctx.set_options(qalphaL=1.0)
+    ctx.load_lines_hitran(L)
+    yield dict(ctx=ctx, L=L, Tq=Tq, Qq=Qq)
+    ctx.set_profile(1, 0)
+    ctx.close()
+
+
+@pytest.mark.parametrize("profile,cutMode,cut", EDGE_CASES)
+def test_plinth_isolated_edges(sparse, profile, cutMode, cut):
+    ctx = sparse["ctx"]
+    ctx.set_profile(profile, 1)
+    ctx.set_grid(NUMIN, NUMAX, DNU, SPARSE_BINS, cutMode, cut)
+    try:
+        total = 0
+        for T, P in ((1500.0, 0.1), (500.0, 10.0), (2500.0, 1e-3)):
+            Kref, _ = oracle_k(sparse, T, P, profile, 1, cutMode, cut)
+            K = ctx.opacity([T], [P], hkb.MIXED)[0]
+            if not (Kref > 0).any():
+                # windows narrower than a grid step (a cut of a few Lorentz
+                # widths at low pressure): nothing to compare but zeros
+                assert np.abs(K - Kref).max() <= 1e-5 * max(np.abs(Kref).max(), 1e-300)
+                continue
+            err, n = masked_relerr(K, Kref, SPARSE_BINS)
+            total += n
+            print(f"isolated edges: profile {profile} cut {cutMode}/{cut} T={T} P={P}: "
+                  f"err {err:.2e} over {n} points")
+            assert err < 1e-5
+        assert total > 0
+    finally:
         ctx.set_profile(1, 0)
