@@ -1003,6 +1003,9 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
   ExtPL *ext_pl = reinterpret_cast<ExtPL *>(cacc + G);
   ExtF exc;
   if (EXT == HK_EXT_CHI) exc = ext_consts(g, st, g0, g1);
+  // chi x / nu is 1 at every point of a tile outside (x_lo, x_hi): such a
+  // tile takes the regular sweeps
+  const bool chi_tile = EXT == HK_EXT_CHI && exc.kl0 < exc.kl1;
 
   float2 kf[PPL / 2];   // lane-local point indices, paired {p, p+1}
   float2 a32[PPL / 2];  // mixed: FP32 sums of the current chunk (scaled)
@@ -1094,7 +1097,7 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
             m = __ballot_sync(0xffffffffu, lev == lcur) & live;
           }
           live &= ~m;
-          if constexpr (EXT == HK_EXT_CHI) {
+          if (EXT == HK_EXT_CHI && chi_tile) {
             // every class through the generic sweep with the chi factor
             unsigned mX = m;
             while (mX) {
@@ -1156,7 +1159,7 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
         while (mW) {
           const int b = __ffs(mW) - 1;
           mW &= mW - 1;
-          if constexpr (EXT == HK_EXT_CHI) {
+          if (EXT == HK_EXT_CHI && chi_tile) {
             const float inu = ext_inu[g32 + b];
             sweep_G<true, false, PPL, EXT>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile, &exc, inu);
             sweep_C<SLICE, EXT>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane, &exc, inu);
