@@ -148,11 +148,16 @@ static_assert(sizeof(ExtPL) == 64, "ExtPL layout");
 // first line in bounds for predicated reads), the per-point FP64 sums, and
 // the per-line option data (1 / nu for the chi factor, ExtPL).
 constexpr int HK_RPAD = 8;
+// Far field (the default option set): each warp's FP64 sums of the blocks'
+// Taylor coefficients, HK_FN per 64-point block.
+constexpr int HK_FB = 64, HK_FN = 8;
 template <class SH, int EXT = HK_EXT_NONE>
 constexpr size_t smem_mixed() {
   return sizeof(RecF) * SH::CH + sizeof(float) * (HK_RPAD + SH::CH * HK_C916_MR) +
          sizeof(double) * SH::G +
-         (EXT == HK_EXT_CHI ? sizeof(float) * SH::CH : EXT == HK_EXT_PL ? sizeof(ExtPL) * SH::CH : 0);
+         (EXT == HK_EXT_CHI ? sizeof(float) * SH::CH
+          : EXT == HK_EXT_PL ? sizeof(ExtPL) * SH::CH
+                             : sizeof(double) * SH::WARPS * HK_FN * (SH::G / HK_FB));
 }
 
 struct __align__(16) RecD {
@@ -442,13 +447,112 @@ __device__ __forceinline__ void stage_plain(const LinePrep *__restrict__ P, int6
 // are summed in FP64 into the per-point shared sums cacc.
 enum { HK_CLS_SKIP = 0, HK_CLS_B, HK_CLS_A, HK_CLS_BM, HK_CLS_AM, HK_CLS_G, HK_CLS_W };
 
+// ------------------------------------------------------------ far field
+// Over a 64-point block far from a line's centre the line's term is a smooth
+// function of the point, so the tile keeps, per block, the sum over such
+// lines of their Taylor expansions about the block centre in the grid offset
+// j = k - (blo + 31.5), |j| <= 31.5, and evaluates that one polynomial per
+// point at the end of the tile (far_terms, far_eval).  A block is far for a
+// line when it lies inside the line's cut window and inside one of regions
+// A and B (no region boundary, no region-C point) and its centre is at
+// least HK_FAR_DK grid steps from the line centre.  The term's nearest
+// singularity in the complex offset plane is r0 = |x0 + iy| >= |x0| away
+// (the zeros of x^2 + y^2 and of GH2's other denominator factor), so
+// |j vb| / r0 <= 31.5 / 315.5 < 0.1 and HK_FN = 8 terms leave 0.1^8 = 1e-8
+// of the term.  FP64 (weak) lines and lines with x^2 + y^2 >= 1e18 in
+// their window take the direct sweeps throughout.
+constexpr float HK_FAR_DK = 315.5f;
+
+__device__ __forceinline__ bool far_block(const RecF &r, int blo) {
+  if (r.flags & (HK_F_WEAK | HK_F_WIDE)) return false;
+  const int bhi = blo + HK_FB;
+  if (blo < r.i0 || bhi > r.i1) return false;
+  if (r.c0 < r.c1 && r.c0 < bhi && r.c1 > blo) return false;
+  if ((r.b0 > blo && r.b0 < bhi) || (r.b1 > blo && r.b1 < bhi)) return false;
+  const float m = (float)blo + 31.5f + r.nkc;  // block centre - kc, exact for |kc| < 2^21
+  return fabsf(m) >= HK_FAR_DK && fabsf(r.nkc) < 2097152.f;
+}
+
+// bit q: block q of the slice starting at wb is far for the line
 template <int SLICE>
-__device__ __forceinline__ int classify(const RecF &r, int wb) {
+__device__ __forceinline__ unsigned far_mask(const RecF &r, int wb) {
+  unsigned m = 0u;
+#pragma unroll
+  for (int q = 0; q < SLICE / HK_FB; ++q) m |= far_block(r, wb + HK_FB * q) ? (1u << q) : 0u;
+  return m;
+}
+
+// The line's Taylor coefficients about the centre of block blo (grid units),
+// scaled like its FP32 sums (S1f), added to fq.  Region B: GH2 = N(s)/D(s)
+// with s = s0 + b j + c j^2 (s0 = x0^2, b = 2 x0 vb, c = vb^2); N and D as
+// polynomials in j (every term of each coefficient has the same sign), then
+// the quotient series q_n = (N_n - sum_i D_i q_(n-i)) / D_0.  Region A:
+// S1f / (d0 + d1 j + d2 j^2), q_n = -(d1 q_(n-1) + d2 q_(n-2)) / d0.
+__device__ __forceinline__ void far_terms(const RecF &r, int blo, float (&fq)[HK_FN]) {
+  const float x0 = fmaf((float)blo + 31.5f + r.nkc, r.vb, r.fr);
+  const float vb = r.vb;
+  const float b = 2.0f * x0 * vb, c = vb * vb;
+  float q[HK_FN];
+  if (blo >= r.b0 && blo + HK_FB <= r.b1) {
+    const float S1f = r.S1f, C1 = r.C1, C0 = r.C0, E2 = r.D2, E1 = r.D1, E0 = r.D0;
+    const float s0 = x0 * x0;
+    // s^2 and s^3 as polynomials in j
+    const float t0 = s0 * s0, t1 = 2.0f * s0 * b, t2 = fmaf(b, b, 2.0f * s0 * c), t3 = 2.0f * b * c,
+                t4 = c * c;
+    const float u0 = t0 * s0, u1 = fmaf(t0, b, t1 * s0), u2 = fmaf(t0, c, fmaf(t1, b, t2 * s0)),
+                u3 = fmaf(t1, c, fmaf(t2, b, t3 * s0)), u4 = fmaf(t2, c, fmaf(t3, b, t4 * s0)),
+                u5 = fmaf(t3, c, t4 * b), u6 = t4 * c;
+    const float N0 = fmaf(S1f, t0, fmaf(C1, s0, C0)), N1 = fmaf(S1f, t1, C1 * b),
+                N2 = fmaf(S1f, t2, C1 * c), N3 = S1f * t3, N4 = S1f * t4;
+    const float D0 = u0 + fmaf(E2, t0, fmaf(E1, s0, E0)), D1 = u1 + fmaf(E2, t1, E1 * b),
+                D2 = u2 + fmaf(E2, t2, E1 * c), D3 = fmaf(E2, t3, u3), D4 = fmaf(E2, t4, u4), D5 = u5,
+                D6 = u6;
+    const float iD = 1.0f / D0;
+    q[0] = N0 * iD;
+    q[1] = fmaf(-D1, q[0], N1) * iD;
+    q[2] = fmaf(-D1, q[1], fmaf(-D2, q[0], N2)) * iD;
+    q[3] = fmaf(-D1, q[2], fmaf(-D2, q[1], fmaf(-D3, q[0], N3))) * iD;
+    q[4] = fmaf(-D1, q[3], fmaf(-D2, q[2], fmaf(-D3, q[1], fmaf(-D4, q[0], N4)))) * iD;
+    q[5] = -fmaf(D1, q[4], fmaf(D2, q[3], fmaf(D3, q[2], fmaf(D4, q[1], D5 * q[0])))) * iD;
+    q[6] = -fmaf(D1, q[5], fmaf(D2, q[4], fmaf(D3, q[3], fmaf(D4, q[2], fmaf(D5, q[1], D6 * q[0]))))) * iD;
+    q[7] = -fmaf(D1, q[6], fmaf(D2, q[5], fmaf(D3, q[4], fmaf(D4, q[3], fmaf(D5, q[2], D6 * q[1]))))) * iD;
+  } else {
+    const float d0 = fmaf(x0, x0, r.y * r.y);
+    const float iD = 1.0f / d0;
+    q[0] = r.S1f * iD;
+    q[1] = -(b * q[0]) * iD;
+#pragma unroll
+    for (int n = 2; n < HK_FN; ++n) q[n] = -fmaf(b, q[n - 1], c * q[n - 2]) * iD;
+  }
+#pragma unroll
+  for (int n = 0; n < HK_FN; ++n) fq[n] += q[n];
+}
+
+// fq (the FP32 sums of level lev) into the warp's FP64 coefficient sums
+__device__ __forceinline__ void far_flush(float (&fq)[HK_FN], double *__restrict__ fdw, int lane,
+                                          int nblk, int s1exp, int lev) {
+  if (lane < nblk) {
+    const double u = ldexp(1.0, -(s1exp + HK_LEVEL_BITS * lev));
+#pragma unroll
+    for (int n = 0; n < HK_FN; ++n) fdw[n * nblk + lane] = fma((double)fq[n], u, fdw[n * nblk + lane]);
+  }
+#pragma unroll
+  for (int n = 0; n < HK_FN; ++n) fq[n] = 0.f;
+}
+
+// fm: the slice's far blocks (FAR), which the direct sweeps skip
+template <int SLICE, bool FAR = false>
+__device__ __forceinline__ int classify(const RecF &r, int wb, unsigned &fm) {
+  fm = 0u;
   const int we = wb + SLICE;
   const int lo = max(r.i0, wb), hi = min(r.i1, we);
   if (hi <= lo) return HK_CLS_SKIP;
   if (r.flags & HK_F_WEAK) return HK_CLS_W;
-  const bool full = lo == wb && hi == we;
+  if (FAR) {
+    fm = far_mask<SLICE>(r, wb);
+    if (fm == (1u << (SLICE / HK_FB)) - 1u) return HK_CLS_SKIP;
+  }
+  const bool full = lo == wb && hi == we && fm == 0u;
   const bool noC = r.c0 >= r.c1 || r.c1 <= lo || r.c0 >= hi;
   if (r.b0 <= lo && r.b1 >= hi) return (full && noC) ? HK_CLS_B : HK_CLS_BM;
   if (r.b0 >= r.b1 || r.b1 <= lo || r.b0 >= hi) return full ? HK_CLS_A : HK_CLS_AM;
@@ -577,7 +681,7 @@ __device__ __forceinline__ void sweep_B(const RecF &rr, const float2 (&kf)[PPL /
 template <int PPL>
 __device__ __forceinline__ void sweep_BM(const RecF &rr, int wb, int lane,
                                          const float2 (&kf)[PPL / 2],
-                                         float2 (&a32)[PPL / 2]) {
+                                         float2 (&a32)[PPL / 2], unsigned fm = 0u) {
   const CoefB c = load_coef(rr);
   const int lo = max(rr.i0, wb), hi = min(rr.i1, wb + 32 * PPL);
   const int c0 = rr.c0, c1 = rr.c1;
@@ -585,7 +689,7 @@ __device__ __forceinline__ void sweep_BM(const RecF &rr, int wb, int lane,
   for (int q = 0; q < PPL / 2; ++q) {
     const int blo = wb + 64 * q, bhi = blo + 64;
     const int l2 = max(lo, blo), h2 = min(hi, bhi);
-    if (l2 >= h2 || (c0 <= l2 && c1 >= h2)) continue;  // no region-B point
+    if (l2 >= h2 || (c0 <= l2 && c1 >= h2) || ((fm >> q) & 1u)) continue;  // no region-B point, or far
     const float2 x = x_pair(c, kf[q]);
     float2 s = __fmul2_rn(x, x);
     float2 num, inv;
@@ -609,7 +713,7 @@ __device__ __forceinline__ void sweep_BM(const RecF &rr, int wb, int lane,
 template <bool AM, int PPL>
 __device__ __forceinline__ void sweep_A(const RecF &rr, int wb, int lane,
                                         const float2 (&kf)[PPL / 2],
-                                        float2 (&a32)[PPL / 2]) {
+                                        float2 (&a32)[PPL / 2], unsigned fm = 0u) {
   const CoefB c = load_coef(rr);
   const float Yf = rr.y * rr.y;
   const float2 Y = make_float2(Yf, Yf);
@@ -620,7 +724,7 @@ __device__ __forceinline__ void sweep_A(const RecF &rr, int wb, int lane,
     const int blo = wb + 64 * q, bhi = blo + 64;
     bool m0 = true, m1 = true;
     if (AM) {
-      if (max(lo, blo) >= min(hi, bhi)) continue;
+      if (max(lo, blo) >= min(hi, bhi) || ((fm >> q) & 1u)) continue;
       m0 = blo + lane >= lo && blo + lane < hi;
       m1 = blo + lane + 32 >= lo && blo + lane + 32 < hi;
     }
@@ -765,7 +869,7 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
                                         float2 (&a32)[PPL / 2],
                                         double *__restrict__ cacc, int profile,
                                         const ExtF *ex = nullptr, float inu = 0.f,
-                                        const ExtPL *pe = nullptr) {
+                                        const ExtPL *pe = nullptr, unsigned fm = 0u) {
   if (WEAK && G34) {
     // Doppler / binned Gaussian lines summed in FP64: the FP64 form's term
     // (with plinth removal: times 1 - exp(-(x_c^2 - x^2)), x_c - |x| exact)
@@ -802,7 +906,7 @@ __device__ __forceinline__ void sweep_G(const RecF &r, int wb, int lane,
 #pragma unroll
   for (int p = 0; p < PPL; ++p) {
     const int k = wb + lane + 32 * p;
-    if (k >= i0 && k < i1 && !(k >= c0 && k < c1)) {
+    if (k >= i0 && k < i1 && !(k >= c0 && k < c1) && !((fm >> ((32 * p + lane) >> 6)) & 1u)) {
       const float kk = (p & 1) ? kf[p >> 1].y : kf[p >> 1].x;
       const float x = fmaf(kk + nkc, vb, fr);
       const float s = x * x;
@@ -970,6 +1074,10 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
                                          unsigned char *smem_dyn) {
   using Rec = typename std::conditional<MIXED, RecF, RecD>::type;
   constexpr int CH = SH::CH, PPL = SH::PPL, SLICE = SH::SLICE, G = SH::G;
+  // the far field runs in the mixed form without options (Voigt, Lorentz)
+  constexpr bool FAR = MIXED && !G34 && EXT == HK_EXT_NONE;
+  constexpr int NBLK = G / HK_FB;  // 64-point blocks of the tile (<= 32)
+  static_assert(!FAR || (NBLK <= 32 && SLICE % HK_FB == 0), "far-field block layout");
   Rec *rec = reinterpret_cast<Rec *>(smem_dyn);
   float *Rtab = reinterpret_cast<float *>(smem_dyn + sizeof(Rec) * CH) + HK_RPAD;
   double *cacc = reinterpret_cast<double *>(smem_dyn + sizeof(Rec) * CH +
@@ -1001,6 +1109,10 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
   // per-point sums
   float *ext_inu = reinterpret_cast<float *>(cacc + G);
   ExtPL *ext_pl = reinterpret_cast<ExtPL *>(cacc + G);
+  // far field: warp w's coefficient sums fd[(w HK_FN + n) NBLK + block]
+  double *fd = cacc + G;
+  if (FAR)
+    for (int t = lane; t < HK_FN * NBLK; t += 32) fd[warp * HK_FN * NBLK + t] = 0.0;
   ExtF exc;
   if (EXT == HK_EXT_CHI) exc = ext_consts(g, st, g0, g1);
   // chi x / nu is 1 at every point of a tile outside (x_lo, x_hi): such a
@@ -1078,7 +1190,8 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
       const RecF *rf = reinterpret_cast<const RecF *>(rec);
       for (int g32 = 0; g32 < cnt_c; g32 += 32) {
         const int j = g32 + lane;
-        const int cls = (j < cnt_c) ? classify<SLICE>(rf[j], wb) : HK_CLS_SKIP;
+        unsigned fm = 0u;  // the line's far blocks in this slice
+        const int cls = (j < cnt_c) ? classify<SLICE, FAR>(rf[j], wb, fm) : HK_CLS_SKIP;
         const int lev = (j < cnt_c) ? (rf[j].flags >> 8) : 0;
         const unsigned bB = __ballot_sync(0xffffffffu, cls == HK_CLS_B);
         const unsigned bA = __ballot_sync(0xffffffffu, cls == HK_CLS_A);
@@ -1140,19 +1253,25 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
           while (mBM) {
             const int b = __ffs(mBM) - 1;
             mBM &= mBM - 1;
-            sweep_BM<PPL>(rf[g32 + b], wb, lane, kf, a32);
+            const unsigned fb = FAR ? __shfl_sync(0xffffffffu, fm, b) : 0u;
+            sweep_BM<PPL>(rf[g32 + b], wb, lane, kf, a32, fb);
             sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
           }
           while (mAM) {
             const int b = __ffs(mAM) - 1;
             mAM &= mAM - 1;
-            if constexpr (G34) sweep_G34<PPL, PLG>(rf[g32 + b], g.profile, wb, lane, kf, a32, cacc, ext_pl + g32 + b);
-            else sweep_A<true, PPL>(rf[g32 + b], wb, lane, kf, a32);
+            if constexpr (G34) {
+              sweep_G34<PPL, PLG>(rf[g32 + b], g.profile, wb, lane, kf, a32, cacc, ext_pl + g32 + b);
+            } else {
+              const unsigned fb = FAR ? __shfl_sync(0xffffffffu, fm, b) : 0u;
+              sweep_A<true, PPL>(rf[g32 + b], wb, lane, kf, a32, fb);
+            }
           }
           while (mG) {
             const int b = __ffs(mG) - 1;
             mG &= mG - 1;
-            sweep_G<false, G34, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile);
+            const unsigned fb = FAR ? __shfl_sync(0xffffffffu, fm, b) : 0u;
+            sweep_G<false, G34, PPL>(rf[g32 + b], wb, lane, kf, a32, cacc, g.profile, nullptr, 0.f, nullptr, fb);
             sweep_C<SLICE>(rf[g32 + b], Rtab + (g32 + b) * HK_C916_MR, cacc, wb, lane);
           }
         }
@@ -1185,6 +1304,28 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
       }
       // at most one chunk of lines per FP32 sum
       flush_sums<PPL>(a32, cacc, wb, lane, s1exp, lcur);
+      if constexpr (FAR) {
+        // far field: warp w takes lines w, w + WARPS, ... (strength-level
+        // order), lane = block of the tile
+        const int blo = lane * HK_FB;
+        double *fdw = fd + warp * HK_FN * NBLK;
+        float fq[HK_FN];
+#pragma unroll
+        for (int n = 0; n < HK_FN; ++n) fq[n] = 0.f;
+        int flev = -1;
+        for (int j = warp; j < cnt_c; j += SH::WARPS) {
+          const RecF &r = rf[j];
+          const bool far = lane < NBLK && far_block(r, blo);
+          if (!__any_sync(0xffffffffu, far)) continue;
+          const int lev = r.flags >> 8;
+          if (lev != flev) {
+            if (flev >= 0) far_flush(fq, fdw, lane, NBLK, s1exp, flev);
+            flev = lev;
+          }
+          if (far) far_terms(r, blo, fq);
+        }
+        if (flev >= 0) far_flush(fq, fdw, lane, NBLK, s1exp, flev);
+      }
     } else {
       for (int j = 0; j < cnt_c; ++j)
         sweep_plain<PPL>(reinterpret_cast<const RecD &>(rec[j]), wb, lane, xg, acc, g, st);
@@ -1192,6 +1333,27 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
     __syncthreads();
   }
 
+  if constexpr (FAR) {
+    // the blocks' coefficient sums over the warps (fixed order), then one
+    // polynomial per point into the FP64 sums
+    __syncthreads();
+    for (int t = threadIdx.x; t < HK_FN * NBLK; t += SH::THREADS) {
+      double v = fd[t];
+      for (int w = 1; w < SH::WARPS; ++w) v += fd[w * HK_FN * NBLK + t];
+      fd[t] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PPL; ++p) {
+      const int k = wb + lane + 32 * p;
+      const int bl = k / HK_FB;
+      const double jj = (double)(k - bl * HK_FB) - 31.5;
+      double v = fd[(HK_FN - 1) * NBLK + bl];
+#pragma unroll
+      for (int n = HK_FN - 2; n >= 0; --n) v = fma(v, jj, fd[n * NBLK + bl]);
+      cacc[k] += v;
+    }
+  }
   if (nsplit == 1) {
 #pragma unroll
     for (int p = 0; p < PPL; ++p) {
