@@ -87,7 +87,7 @@ struct __align__(16) RecF {
   double Sc;               // S/sqrt(pi) (region C, FP64 sum)
   int i0, b0, c0, c1;      // tile-local window boundaries
   int b1, i1, flags;
-  float iy;                // 1/y (region C)
+  unsigned fmask;          // far-field blocks of the tile (bit b: block b)
   int t0, t1;              // region C: the Algorithm-916 part (tile-local)
 };
 static_assert(sizeof(RecF) == 112, "RecF layout");
@@ -247,6 +247,50 @@ __device__ __forceinline__ int line_key(const LinePrepF *__restrict__ P, int64_t
   return lev;
 }
 
+// ------------------------------------------------------------ far field
+// Over a 64-point block far from a line's centre the line's term is a smooth
+// function of the point, so the tile keeps, per block, the sum over such
+// lines of their Taylor expansions about the block centre in the grid offset
+// j = k - (blo + 31.5), |j| <= 31.5, and evaluates that one polynomial per
+// point at the end of the tile (far_terms; the evaluation closes sum_tile).
+// A block is far for a line when it lies inside the line's cut window and
+// inside one of regions A and B (no region boundary, no region-C point) and
+// its centre is at least HK_FAR_DK grid steps from the line centre.  The
+// term's singularities in the complex offset plane are the zeros of
+// x^2 + y^2, r0 = |x0 + iy| >= |x0| >= 315 vb away (for small y nearly a
+// double pole, whose Taylor remainder after N terms is about (N + 1) rho^N),
+// and for GH2 those of its other denominator factor, close to +-i
+// sqrt(y^2 + 0.55).  With rho = |j vb| / r0 <= 0.1, HK_FN = 8 terms leave
+// 9 * 0.1^8 = 1e-7 of the term (measured in FP64 over region B next to
+// region C: 9.8e-8; in FP32 with rounding: 5.2e-7).  FP64 (weak) lines and
+// lines with x^2 + y^2 >= 1e18 in their window take the direct sweeps
+// throughout.
+constexpr float HK_FAR_DK = 315.5f;
+
+// bits [a, b) of a 32-bit mask (a, b clamped to [0, 32])
+__device__ __forceinline__ unsigned range_bits(int a, int b) {
+  a = max(a, 0);
+  b = min(b, 32);
+  if (b <= a) return 0u;
+  const unsigned hi = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
+  return hi & ~((1u << a) - 1u);
+}
+
+// The far blocks of a staged line (tile-local record r, line centre at the
+// tile point kc): blocks inside the cut window, minus those whose centre
+// 64 b + 31.5 lies within HK_FAR_DK of kc, those holding region-C points
+// and those a region boundary cuts.
+__device__ __forceinline__ unsigned far_blocks(const RecF &r, double kc) {
+  if (!(fabs(kc) < 2097152.0)) return 0u;  // block centre - kc exact in FP32
+  unsigned m = range_bits((r.i0 + HK_FB - 1) / HK_FB, r.i1 / HK_FB);
+  const double lo = (kc - (double)HK_FAR_DK - 31.5) / HK_FB, hi = (kc + (double)HK_FAR_DK - 31.5) / HK_FB;
+  m &= ~range_bits((int)floor(lo) + 1, (int)ceil(hi));
+  if (r.c0 < r.c1) m &= ~range_bits(r.c0 / HK_FB, (r.c1 + HK_FB - 1) / HK_FB);
+  if (r.b0 % HK_FB) m &= ~(1u << (r.b0 / HK_FB));
+  if (r.b1 % HK_FB) m &= ~(1u << (r.b1 / HK_FB));
+  return m;
+}
+
 // The plinth data of a staged line (ExtPL) and its class flag.  S1f: the
 // line's FP32 scale (1 for a line summed in FP64); D0, vb: its FP64 offset at
 // the tile start and grid step.  GH2 in s = x^2 is S1 N(s) / D(s) with
@@ -275,7 +319,6 @@ __device__ __forceinline__ void stage_plinth(const LinePrepF &lp, const GridDev 
     // the FP32 fields of the record hold FP64 words: give the staged line
     // plain values (its sweep reads none of them)
     r.y = (float)e.vy;
-    r.iy = 0.f;
     r.ey = r.sig1 = 0.f;
     r.t0 = r.t1 = r.c0;
     r.flags |= HK_F_PL64;
@@ -353,7 +396,9 @@ __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, con
   r.t0 = clip_local(lp.t0, g0, g1);
   r.t1 = clip_local(lp.t1, g0, g1);
   r.flags = ((lp.flags & HK_PF_WIDE) ? HK_F_WIDE : 0) | (weak ? HK_F_WEAK : 0) | (lev << 8);
-  r.iy = lp.y > 0.f ? (float)(1.0 / (double)lp.y) : 0.f;
+  r.fmask = (!G34 && EXT == HK_EXT_NONE && nonempty && !weak && !(lp.flags & HK_PF_WIDE))
+                ? far_blocks(r, kc)
+                : 0u;
   if (EXT == HK_EXT_CHI) *static_cast<float *>(ext) = lp.inu;
   if (EXT == HK_EXT_PL) stage_plinth<G34>(lp, g, D0, vb, S1f, r, *static_cast<ExtPL *>(ext));
   if (G34) {
@@ -440,46 +485,19 @@ __device__ __forceinline__ void stage_plain(const LinePrep *__restrict__ P, int6
 //   HK_CLS_AM  [lo, hi) lies in region A (window edge in the slice);
 //   HK_CLS_G   [lo, hi) holds an A/B region boundary;
 //   HK_CLS_W   an HK_F_WEAK line (FP64 sums);
+//   HK_CLS_BF, HK_CLS_AF  as B and A but for far-field blocks of the slice,
+//              which they skip;
 // non-intersecting lines cost nothing.  B and A run the packed f32x2 loop
 // with no tests; BM and AM run it per 64-point block of pairs, skipping
 // blocks without points of their region and masking only the blocks a
 // boundary cuts; G tests every point.  Region-C points go to sweep_C and
 // are summed in FP64 into the per-point shared sums cacc.
-enum { HK_CLS_SKIP = 0, HK_CLS_B, HK_CLS_A, HK_CLS_BM, HK_CLS_AM, HK_CLS_G, HK_CLS_W };
-
-// ------------------------------------------------------------ far field
-// Over a 64-point block far from a line's centre the line's term is a smooth
-// function of the point, so the tile keeps, per block, the sum over such
-// lines of their Taylor expansions about the block centre in the grid offset
-// j = k - (blo + 31.5), |j| <= 31.5, and evaluates that one polynomial per
-// point at the end of the tile (far_terms, far_eval).  A block is far for a
-// line when it lies inside the line's cut window and inside one of regions
-// A and B (no region boundary, no region-C point) and its centre is at
-// least HK_FAR_DK grid steps from the line centre.  The term's nearest
-// singularity in the complex offset plane is r0 = |x0 + iy| >= |x0| away
-// (the zeros of x^2 + y^2 and of GH2's other denominator factor), so
-// |j vb| / r0 <= 31.5 / 315.5 < 0.1 and HK_FN = 8 terms leave 0.1^8 = 1e-8
-// of the term.  FP64 (weak) lines and lines with x^2 + y^2 >= 1e18 in
-// their window take the direct sweeps throughout.
-constexpr float HK_FAR_DK = 315.5f;
-
-__device__ __forceinline__ bool far_block(const RecF &r, int blo) {
-  if (r.flags & (HK_F_WEAK | HK_F_WIDE)) return false;
-  const int bhi = blo + HK_FB;
-  if (blo < r.i0 || bhi > r.i1) return false;
-  if (r.c0 < r.c1 && r.c0 < bhi && r.c1 > blo) return false;
-  if ((r.b0 > blo && r.b0 < bhi) || (r.b1 > blo && r.b1 < bhi)) return false;
-  const float m = (float)blo + 31.5f + r.nkc;  // block centre - kc, exact for |kc| < 2^21
-  return fabsf(m) >= HK_FAR_DK && fabsf(r.nkc) < 2097152.f;
-}
+enum { HK_CLS_SKIP = 0, HK_CLS_B, HK_CLS_A, HK_CLS_BM, HK_CLS_AM, HK_CLS_G, HK_CLS_W, HK_CLS_BF, HK_CLS_AF };
 
 // bit q: block q of the slice starting at wb is far for the line
 template <int SLICE>
 __device__ __forceinline__ unsigned far_mask(const RecF &r, int wb) {
-  unsigned m = 0u;
-#pragma unroll
-  for (int q = 0; q < SLICE / HK_FB; ++q) m |= far_block(r, wb + HK_FB * q) ? (1u << q) : 0u;
-  return m;
+  return (r.fmask >> (wb / HK_FB)) & ((1u << (SLICE / HK_FB)) - 1u);
 }
 
 // The line's Taylor coefficients about the centre of block blo (grid units),
@@ -552,10 +570,10 @@ __device__ __forceinline__ int classify(const RecF &r, int wb, unsigned &fm) {
     fm = far_mask<SLICE>(r, wb);
     if (fm == (1u << (SLICE / HK_FB)) - 1u) return HK_CLS_SKIP;
   }
-  const bool full = lo == wb && hi == we && fm == 0u;
+  const bool full = lo == wb && hi == we;
   const bool noC = r.c0 >= r.c1 || r.c1 <= lo || r.c0 >= hi;
-  if (r.b0 <= lo && r.b1 >= hi) return (full && noC) ? HK_CLS_B : HK_CLS_BM;
-  if (r.b0 >= r.b1 || r.b1 <= lo || r.b0 >= hi) return full ? HK_CLS_A : HK_CLS_AM;
+  if (r.b0 <= lo && r.b1 >= hi) return (full && noC) ? (fm ? HK_CLS_BF : HK_CLS_B) : HK_CLS_BM;
+  if (r.b0 >= r.b1 || r.b1 <= lo || r.b0 >= hi) return full ? (fm ? HK_CLS_AF : HK_CLS_A) : HK_CLS_AM;
   return HK_CLS_G;
 }
 
@@ -663,13 +681,14 @@ __device__ __forceinline__ bool in_run(int k, int lo, int hi, int c0, int c1) {
   return k >= lo && k < hi && !(k >= c0 && k < c1);
 }
 
-// region B only, whole slice
-template <int PPL>
+// region B only, whole slice (SKIP: but the far-field blocks in fm)
+template <int PPL, bool SKIP = false>
 __device__ __forceinline__ void sweep_B(const RecF &rr, const float2 (&kf)[PPL / 2],
-                                        float2 (&a32)[PPL / 2]) {
+                                        float2 (&a32)[PPL / 2], unsigned fm = 0u) {
   const CoefB c = load_coef(rr);
 #pragma unroll
   for (int q = 0; q < PPL / 2; ++q) {
+    if (SKIP && ((fm >> q) & 1u)) continue;
     const float2 x = x_pair(c, kf[q]);
     float2 num, inv;
     gh2_pair(c, __fmul2_rn(x, x), num, inv);
@@ -709,7 +728,8 @@ __device__ __forceinline__ void sweep_BM(const RecF &rr, int wb, int lane,
   }
 }
 
-// region A, whole slice (AM = false) or the points of [lo, hi) (AM = true)
+// region A, whole slice (AM = false) or the points of [lo, hi) (AM = true);
+// both skip the far-field blocks in fm
 template <bool AM, int PPL>
 __device__ __forceinline__ void sweep_A(const RecF &rr, int wb, int lane,
                                         const float2 (&kf)[PPL / 2],
@@ -723,8 +743,9 @@ __device__ __forceinline__ void sweep_A(const RecF &rr, int wb, int lane,
   for (int q = 0; q < PPL / 2; ++q) {
     const int blo = wb + 64 * q, bhi = blo + 64;
     bool m0 = true, m1 = true;
+    if ((fm >> q) & 1u) continue;
     if (AM) {
-      if (max(lo, blo) >= min(hi, bhi) || ((fm >> q) & 1u)) continue;
+      if (max(lo, blo) >= min(hi, bhi)) continue;
       m0 = blo + lane >= lo && blo + lane < hi;
       m1 = blo + lane + 32 >= lo && blo + lane + 32 < hi;
     }
@@ -834,7 +855,8 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
   const int lo = max(r.c0, wb), hi = min(r.c1, wb + SLICE);
   if (lo >= hi) return;
   const float dh = r.dh, dl = r.dl, vbh = r.vbh, vbl = r.vbl;
-  const float y = r.y, iy = r.iy, ey = r.ey, sig1 = r.sig1;
+  const float y = r.y, ey = r.ey, sig1 = r.sig1;
+  const float iy = y > 0.f ? (float)(1.0 / (double)y) : 0.f;
   const double Sc = r.Sc;
   const int t0 = min(max(r.t0, lo), hi), t1 = min(max(r.t1, t0), hi);
   __syncwarp();
@@ -1198,8 +1220,10 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
         const unsigned bBM = __ballot_sync(0xffffffffu, cls == HK_CLS_BM);
         const unsigned bAM = __ballot_sync(0xffffffffu, cls == HK_CLS_AM);
         const unsigned bG = __ballot_sync(0xffffffffu, cls == HK_CLS_G);
+        const unsigned bBF = FAR ? __ballot_sync(0xffffffffu, cls == HK_CLS_BF) : 0u;
+        const unsigned bAF = FAR ? __ballot_sync(0xffffffffu, cls == HK_CLS_AF) : 0u;
         unsigned mW = __ballot_sync(0xffffffffu, cls == HK_CLS_W);
-        unsigned live = bB | bA | bBM | bAM | bG;
+        unsigned live = bB | bA | bBM | bAM | bG | bBF | bAF;
         while (live) {
           // the lines of the current level first; switch level (flushing
           // the FP32 sums) only when none of them is left
@@ -1239,6 +1263,19 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
           }
           constexpr bool PLG = EXT == HK_EXT_PL && G34;  // Doppler with plinth removal
           unsigned mB = m & bB, mA = m & bA, mBM = m & bBM, mAM = m & bAM, mG = m & bG;
+          if constexpr (FAR) {
+            unsigned mBF = m & bBF, mAF = m & bAF;
+            while (mBF) {
+              const int b = __ffs(mBF) - 1;
+              mBF &= mBF - 1;
+              sweep_B<PPL, true>(rf[g32 + b], kf, a32, __shfl_sync(0xffffffffu, fm, b));
+            }
+            while (mAF) {
+              const int b = __ffs(mAF) - 1;
+              mAF &= mAF - 1;
+              sweep_A<false, PPL>(rf[g32 + b], wb, lane, kf, a32, __shfl_sync(0xffffffffu, fm, b));
+            }
+          }
           while (mB) {
             const int b = __ffs(mB) - 1;
             mB &= mB - 1;
@@ -1315,8 +1352,9 @@ __device__ __forceinline__ void sum_tile(const void *prep_s, const double *__res
         int flev = -1;
         for (int j = warp; j < cnt_c; j += SH::WARPS) {
           const RecF &r = rf[j];
-          const bool far = lane < NBLK && far_block(r, blo);
-          if (!__any_sync(0xffffffffu, far)) continue;
+          const unsigned fmk = r.fmask;
+          if (fmk == 0u) continue;
+          const bool far = (fmk >> lane) & 1u;
           const int lev = r.flags >> 8;
           if (lev != flev) {
             if (flev >= 0) far_flush(fq, fdw, lane, NBLK, s1exp, flev);
