@@ -525,7 +525,7 @@ __device__ __forceinline__ void far_terms(const RecF &r, int blo, float (&fq)[HK
     const float D0 = u0 + fmaf(E2, t0, fmaf(E1, s0, E0)), D1 = u1 + fmaf(E2, t1, E1 * b),
                 D2 = u2 + fmaf(E2, t2, E1 * c), D3 = fmaf(E2, t3, u3), D4 = fmaf(E2, t4, u4), D5 = u5,
                 D6 = u6;
-    const float iD = 1.0f / D0;
+    const float iD = rcp_fast(D0);  // 1 ulp: one factor on every coefficient
     q[0] = N0 * iD;
     q[1] = fmaf(-D1, q[0], N1) * iD;
     q[2] = fmaf(-D1, q[1], fmaf(-D2, q[0], N2)) * iD;
@@ -536,7 +536,7 @@ __device__ __forceinline__ void far_terms(const RecF &r, int blo, float (&fq)[HK
     q[7] = -fmaf(D1, q[6], fmaf(D2, q[5], fmaf(D3, q[4], fmaf(D4, q[3], fmaf(D5, q[2], D6 * q[1]))))) * iD;
   } else {
     const float d0 = fmaf(x0, x0, r.y * r.y);
-    const float iD = 1.0f / d0;
+    const float iD = rcp_fast(d0);
     q[0] = r.S1f * iD;
     q[1] = -(b * q[0]) * iD;
 #pragma unroll
