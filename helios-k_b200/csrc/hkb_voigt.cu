@@ -1557,8 +1557,10 @@ __device__ __noinline__ void prep_lines(const LinesDev &L, const GridDev &g, con
   for (; l < l1; l += step) prep_record<MIXED, PREP_ALL>(L, g, st, l, e916, out, w_loc, s1_loc);
 }
 
+// (at most 3 CTAs per SM in the mixed form: the prep tickets' FP64 state
+// beside the sums' registers spills at 64 registers per thread)
 template <bool MIXED, class SH, bool G34 = false, int EXT = HK_EXT_NONE>
-__global__ void __launch_bounds__(SH::THREADS, MIXED ? SH::MINB : 2)
+__global__ void __launch_bounds__(SH::THREADS, MIXED ? (SH::MINB > 3 ? 3 : SH::MINB) : 2)
 voigt_table_kernel(LinesDev L, GridDev g, const StateDev *__restrict__ states, TableSched sc,
                    void *ring, double *partial, unsigned *tile_cnt, unsigned long long *ticket,
                    unsigned long long *wbits, unsigned *prep_cnt, unsigned *sum_cnt,
