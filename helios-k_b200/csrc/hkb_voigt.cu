@@ -75,22 +75,21 @@ constexpr int HK_SHAPE_WARPS[HK_NSHAPES] = {Shape0::WARPS, Shape1::WARPS, Shape2
 // D2 = A2 + Y, D1 = B2 + A2 Y, D0 = B2 Y, with A1 = 2Y + 2.5 - 4/pi,
 // B1 = (Y+1.5)(Y+1), A2 = 2Y + 3 - 6/pi, B2 = (Y+1.5)^2.  Every coefficient
 // is positive, so neither form cancels.
-// x at tile point k, regions A and B: x = (k - kc) vb + fr, kc the point
+// x at tile point k, every region: x = (k - kc) vb + fr, kc the point
 // nearest the line centre (|fr| <= vb/2): the subtraction is exact, so x
-// carries ~2 roundings relative to itself.  Region C, where x crosses zero,
-// uses the double-float split x = (dh + k vbh) + (dl + k vbl) instead.
+// carries ~2 roundings relative to itself (|k - kc| vb <= |x| + vb/2 and
+// |x| >= vb/2 off kc) whatever vb, also where x crosses zero.
 struct __align__(16) RecF {
   float S1f, C1, C0, D2;
   float D1, D0, nkc, vb;   // nkc = -kc
   float fr, y, ey, sig1;   // y, erfcx(y), region-C series constant
-  float dh, dl, vbh, vbl;  // region C: x at the tile start, step (hi, lo)
   double Sc;               // S/sqrt(pi) (region C, FP64 sum)
   int i0, b0, c0, c1;      // tile-local window boundaries
   int b1, i1, flags;
   unsigned fmask;          // far-field blocks of the tile (bit b: block b)
   int t0, t1;              // region C: the Algorithm-916 part (tile-local)
 };
-static_assert(sizeof(RecF) == 112, "RecF layout");
+static_assert(sizeof(RecF) == 96, "RecF layout");
 
 // Profiles 3 (Doppler) and 4 (binned Gaussian) have no regions B and C, so
 // their records reuse the GH2 slots: the FP64 offset D0 at the tile start
@@ -362,10 +361,6 @@ __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, con
   const int lev = (weak || !nonempty) ? 0 : key;
   const double D0 = __dmul_rn(__dsub_rn(grid_x(g, g0), lp.nu), lp.iad);
   const double vb = __dmul_rn(g.dnu, lp.iad);
-  const float dh = (float)D0;
-  const float dl = (float)(D0 - (double)dh);
-  const float vbh = __uint_as_float(__float_as_uint((float)vb) & 0xFFFFF800u);  // 13 bits
-  const float vbl = (float)(vb - (double)vbh);
   // the tile point nearest the centre (|kc| <= 2^23 keeps k - kc exact)
   const double kc = fmin(fmax(rint(-D0 / vb), -8388608.0), 8388608.0);
   // S1f = S1 * 2^(s1exp + 96 lev): the line's largest term near 2^40
@@ -379,10 +374,6 @@ __device__ __forceinline__ void stage_mixed(const LinePrepF *__restrict__ P, con
   r.nkc = (float)(-kc);
   r.vb = (float)vb;
   r.fr = (float)__fma_rn(kc, vb, D0);
-  r.dh = dh;
-  r.dl = dl;
-  r.vbh = vbh;
-  r.vbl = vbl;
   r.Sc = lp.Sc;
   r.y = lp.y;
   r.ey = lp.ey;
@@ -854,7 +845,7 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
                                         const ExtF *ex = nullptr, float inu = 0.f, double pld = 0.0) {
   const int lo = max(r.c0, wb), hi = min(r.c1, wb + SLICE);
   if (lo >= hi) return;
-  const float dh = r.dh, dl = r.dl, vbh = r.vbh, vbl = r.vbl;
+  const float nkc = r.nkc, vbf = r.vb, fr = r.fr;
   const float y = r.y, ey = r.ey, sig1 = r.sig1;
   const float iy = y > 0.f ? (float)(1.0 / (double)y) : 0.f;
   const double Sc = r.Sc;
@@ -862,7 +853,7 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
   __syncwarp();
   for (int k = t0 + lane; k < t1; k += 32) {
     const float kk = (float)k;
-    const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
+    const float x = fmaf(kk + nkc, vbf, fr);
     float v = voigt916_core(x, y, iy, ey, sig1, Rj);
     if (EXT == HK_EXT_CHI && k >= ex->kl0 && k < ex->kl1) v *= chi_factor(*ex, x, r.vb, inu);
     cacc[k] = fma(Sc, (double)v, cacc[k]) - pld;
@@ -871,7 +862,7 @@ __device__ __forceinline__ void sweep_C(const RecF &r, const float *__restrict__
   for (int i = lane; i < ns; i += 32) {
     const int k = i < n1 ? lo + i : t1 + (i - n1);
     const float kk = (float)k;
-    const float x = fmaf(kk, vbh, dh) + fmaf(kk, vbl, dl);
+    const float x = fmaf(kk + nkc, vbf, fr);
     float v = voigt_asy(x, y);
     if (EXT == HK_EXT_CHI && k >= ex->kl0 && k < ex->kl1) v *= chi_factor(*ex, x, r.vb, inu);
     cacc[k] = fma(Sc, (double)v, cacc[k]) - pld;

@@ -1,0 +1,68 @@
+"""GPU: the far field of the mixed Voigt sum against the FP64 oracle.
+
+Beyond 315.5 grid steps from a line's centre the mixed form sums the line's
+term over 64-point blocks as 8-term Taylor expansions (one polynomial per
+block for all such lines), truncated at about 1e-7 of the term.  These
+states put most pairs in far blocks and cover the cases that bound the
+truncation: small Lorentz widths (the poles +-iy nearly coincide), grid
+steps of 1e-3 to 0.1 cm^-1 (Doppler-unit steps vb from ~0.01 to ~10, region-B
+blocks next to region C), both profiles with regions A and B (Voigt) and
+region A only (Lorentz), and heavily overlapping windows.  The bound here,
+3e-6 where K > 1e-6 of its bin maximum, is tighter than the mixed form's
+1e-5 so that a far-field regression shows; the form measures ~5e-7.
+"""
+import numpy as np
+import pytest
+
+import hkb
+import oracle
+from hkb import synth
+from test_gpu_parity import masked_relerr
+
+pytestmark = pytest.mark.gpu
+
+FAR_BOUND = 3e-6
+# 3000 lines in a 200 cm^-1 band (windows of 25 cm^-1 overlap ~400-fold): at
+# 100-300 cm^-1 the Doppler widths are small (vb = 2 - 570 on these grids, far
+# blocks mostly in region A); at 20000-20200 cm^-1 they are large (vb = 0.01
+# - 3.4, windows wholly in region B, far blocks next to region C)
+BANDS = {"low": (100.0, 300.0), "high": (20000.0, 20200.0)}
+
+
+@pytest.fixture(scope="module", params=sorted(BANDS))
+def band(request):
+    lo, hi = BANDS[request.param]
+    L = synth.hitran_lines(3000, seed=21, nu_min=lo, nu_max=hi)
+    Tq, Qq = synth.q_table()
+    ctx = hkb.Context(0)
+    ctx.set_species(hkb.HITRAN, [synth.MASS], [1.0])
+    ctx.set_partition(0, Tq, Qq)
+    ctx.set_options(qalphaL=1.0)
+    ctx.load_lines_hitran(L)
+    yield dict(ctx=ctx, L=L, Tq=Tq, Qq=Qq, numin=lo - 10.0, numax=hi + 10.0)
+    ctx.set_profile(1, 0)
+    ctx.close()
+
+
+@pytest.mark.parametrize("profile", [1, 2])
+@pytest.mark.parametrize("dnu,nbins", [(0.001, 22), (0.01, 22), (0.1, 22)])
+def test_far_field_matches_oracle(band, profile, dnu, nbins):
+    ctx = band["ctx"]
+    NUMIN, NUMAX = band["numin"], band["numax"]
+    ctx.set_profile(profile, 0)
+    ctx.set_grid(NUMIN, NUMAX, dnu, nbins, 0, 25.0)
+    nx = oracle.grid_nx(NUMIN, NUMAX, dnu)
+    for T, P in ((300.0, 1e-4), (2000.0, 1.0), (800.0, 50.0)):
+        Q = oracle.partition(band["Tq"], band["Qq"], T)
+        nu, S, iad, vy = oracle.prep_hitran(band["L"], [synth.MASS], [1.0], [Q], T, P, qalphaL=1.0)
+        win = oracle.windows(nu, S, iad, vy, NUMIN, dnu, nx, 0, 25.0, profile=profile)
+        Kref, _ = oracle.opacity(nu, S, iad, vy, win, NUMIN, dnu, nx, profile=profile)
+        K = ctx.opacity([T], [P], hkb.MIXED)[0]
+        err, n = masked_relerr(K, Kref, nbins)
+        # far blocks: window points at least 315.5 - 32 grid steps from the centre
+        far_frac = float(np.mean([(w[5] - w[0] - 2 * 284) / max(w[5] - w[0], 1)
+                                  for w in win if w[5] - w[0] > 2 * 284] or [0.0]))
+        print(f"far field: profile {profile} dnu {dnu} T={T} P={P}: err {err:.2e} over {n} points, "
+              f"far share of long windows ~{far_frac:.2f}")
+        assert n > 0 and err < FAR_BOUND
+    ctx.set_profile(1, 0)
