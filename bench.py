@@ -45,7 +45,7 @@ F_A, F_B, F_C0, F_C_ITER = 6, 20, 30, 12
 # DRAM bytes (read + write) of one voigt_sum_kernel<1> launch, from one ncu
 # capture of this workload (profiles/dram_traffic_hitemp.txt); other
 # workloads have no capture and report null
-VOIGT_DRAM_BYTES = {"hitemp-1e7-lines-single-state": 2007121664 + 109830400}
+VOIGT_DRAM_BYTES = {"hitemp-1e7-lines-single-state": 2007904000 + 110621952}
 SIZEOF_STATE = 2672  # bytes of hkb::StateDev copied per state per call
 
 
