@@ -273,6 +273,160 @@ __device__ __forceinline__ void ab_line(const U *__restrict__ us, int a0, int rb
   ab_seg<false>(us, rb1, a1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
 }
 
+// ------------------------------------------------------- far field
+// As in the forward sum: over a 64-point block whose centre is at least
+// AF_DK grid steps from the line centre, inside one region segment (A or B,
+// which lie on one side of the centre), the shape t is a Taylor series in
+// j = k - (block centre), and so is dt/dY.  The block's four sums are then
+// the series' coefficients dotted with the block's moments M_n = sum_j u_j
+// j^n of the staged u, computed once per tile:
+//   fS = sum q_n M_n,  fY = sum dq_n M_n,  fn = sum c_n M_n,
+//   fx = sum (x0 c_n + vb c_(n-1)) M_n,  c_n = (n + 1) q_(n+1) / (2 vb)
+// ((dt/ds) x = (1/2) dt/dx and (dt/ds) x^2 = (x/2) dt/dx).  Region A:
+// t = 1/(s + Y), q_n = -(b q_(n-1) + c q_(n-2)) / d0, dt/dY = -t^2 (the
+// square of the series).  Region B: GH2 = N(s)/D(s) with N and D as
+// polynomials in j, the quotient series and its derivative in Y
+// (forward mode through the recursion, N and D's coefficients depend on Y).
+// The remainder is about 1e-7 of the term (ratio 31.5 / 315 and a near
+// double pole for small y); float32 prototypes of all four sums against
+// FP64 with random signed u: <= 3.8e-7 of sum |u f|.
+constexpr int AF_FB = 64, AF_NC = 8;
+constexpr int AF_NB = AB_G / AF_FB;
+constexpr float AF_DK = 315.5f;
+
+// far block range [fl, fh) of a one-sided segment [k0, k1) (tile-local
+// points, line centre at the tile point kc): blocks wholly inside it whose
+// centre is at least AF_DK from kc (empty if the segment holds the centre)
+__device__ __forceinline__ void af_range(int k0, int k1, float kc, int &fl, int &fh) {
+  const int bl = (k0 + AF_FB - 1) / AF_FB, bh = k1 / AF_FB;
+  const int nb0 = (int)floorf((kc - AF_DK - 31.5f) * (1.0f / AF_FB)) + 1;
+  const int nb1 = (int)ceilf((kc + AF_DK - 31.5f) * (1.0f / AF_FB));
+  fl = fh = 0;
+  if (bh <= nb0 || bl >= nb1) {
+    fl = bl;
+    fh = bh;
+  } else if (bl < nb0 && bh <= nb1) {
+    fl = bl;
+    fh = nb0;
+  } else if (bl >= nb0 && bh > nb1) {
+    fl = nb1;
+    fh = bh;
+  }
+  if (fh <= fl) fl = fh = 0;
+}
+
+template <bool REGION_B>
+__device__ __forceinline__ void af_seg(const float *__restrict__ mom, int fl, int fh, int lane, float kf0,
+                                       float vbf, float frf, float Y, float &fS, float &fY, float &fn,
+                                       float &fx) {
+  const float ih = 0.5f * rcp_fast(vbf);
+  for (int b = fl + lane; b < fh; b += 32) {
+    const float x0 = fmaf((float)(b * AF_FB) + 31.5f + kf0, vbf, frf);
+    const float bb = 2.0f * x0 * vbf, cc = vbf * vbf;
+    float q[AF_NC + 1], dq[AF_NC];
+    if (REGION_B) {
+      const float c4 = (float)(4.0 / CUDART_PI), c6 = (float)(6.0 / CUDART_PI);
+      const float A1 = fmaf(2.0f, Y, 2.5f - c4), B1 = (Y + 1.5f) * (Y + 1.0f);
+      const float A2 = fmaf(2.0f, Y, 3.0f - c6), B2 = (Y + 1.5f) * (Y + 1.5f);
+      const float E2 = A2 + Y, E1 = fmaf(A2, Y, B2), E0 = B2 * Y;
+      const float dB1 = fmaf(2.0f, Y, 2.5f), dE1 = fmaf(2.0f, Y + 1.5f, fmaf(2.0f, Y, A2));
+      const float dE0 = fmaf(2.0f * (Y + 1.5f), Y, B2);
+      const float s0 = x0 * x0;
+      // s, s^2, s^3 as polynomials in j
+      const float S1[3] = {s0, bb, cc};
+      const float S2[5] = {s0 * s0, 2.0f * s0 * bb, fmaf(bb, bb, 2.0f * s0 * cc), 2.0f * bb * cc, cc * cc};
+      float S3[7];
+#pragma unroll
+      for (int n = 0; n < 7; ++n) S3[n] = 0.f;
+#pragma unroll
+      for (int i = 0; i < 5; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) S3[i + k] = fmaf(S2[i], S1[k], S3[i + k]);
+      float N[5], D[7], dN[3], dD[5];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) N[n] = S2[n] + (n < 3 ? A1 * S1[n] : 0.f);
+      N[0] += B1;
+#pragma unroll
+      for (int n = 0; n < 3; ++n) dN[n] = 2.0f * S1[n];
+      dN[0] += dB1;
+#pragma unroll
+      for (int n = 0; n < 7; ++n) D[n] = S3[n] + (n < 5 ? E2 * S2[n] : 0.f) + (n < 3 ? E1 * S1[n] : 0.f);
+      D[0] += E0;
+#pragma unroll
+      for (int n = 0; n < 5; ++n) dD[n] = 3.0f * S2[n] + (n < 3 ? dE1 * S1[n] : 0.f);
+      dD[0] += dE0;
+      const float iD = rcp_fast(D[0]);
+#pragma unroll
+      for (int n = 0; n <= AF_NC; ++n) {
+        float a = n < 5 ? N[n] : 0.f;
+#pragma unroll
+        for (int i = 1; i <= 6; ++i)
+          if (i <= n) a = fmaf(-D[i], q[n - i], a);
+        q[n] = a * iD;
+      }
+#pragma unroll
+      for (int n = 0; n < AF_NC; ++n) {
+        float a = fmaf(-dD[0], q[n], n < 3 ? dN[n] : 0.f);
+#pragma unroll
+        for (int i = 1; i <= 6; ++i)
+          if (i <= n) a = fmaf(-D[i], dq[n - i], i < 5 ? fmaf(-dD[i], q[n - i], a) : a);
+        dq[n] = a * iD;
+      }
+    } else {
+      const float iD = rcp_fast(fmaf(x0, x0, Y));
+      q[0] = iD;
+      q[1] = -(bb * q[0]) * iD;
+#pragma unroll
+      for (int n = 2; n <= AF_NC; ++n) q[n] = -fmaf(bb, q[n - 1], cc * q[n - 2]) * iD;
+#pragma unroll
+      for (int n = 0; n < AF_NC; ++n) {
+        float a = 0.f;
+#pragma unroll
+        for (int i = 0; i <= n; ++i) a = fmaf(q[i], q[n - i], a);
+        dq[n] = -a;
+      }
+    }
+    float cprev = 0.f;
+#pragma unroll
+    for (int n = 0; n < AF_NC; ++n) {
+      const float m = mom[n * AF_NB + b];
+      const float cn = (float)(n + 1) * q[n + 1] * ih;
+      fS = fmaf(q[n], m, fS);
+      fY = fmaf(dq[n], m, fY);
+      fn = fmaf(cn, m, fn);
+      fx = fmaf(fmaf(x0, cn, vbf * cprev), m, fx);
+      cprev = cn;
+    }
+  }
+}
+
+// one region segment: the direct sweep outside its far blocks, the far
+// field inside them
+template <bool REGION_B>
+__device__ __forceinline__ void ab_seg_far(const float *__restrict__ us, const float *__restrict__ mom,
+                                           int k0, int k1, int lane, float kf0, float vbf, float frf,
+                                           float Y, float &fS, float &fY, float &fn, float &fx) {
+  int fl = 0, fh = 0;
+  if (k1 - k0 >= AF_FB && fabsf(kf0) < 2097152.0f) af_range(k0, k1, -kf0, fl, fh);
+  if (fl < fh) {
+    ab_seg<REGION_B>(us, k0, fl * AF_FB, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+    af_seg<REGION_B>(mom, fl, fh, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+    ab_seg<REGION_B>(us, fh * AF_FB, k1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+  } else {
+    ab_seg<REGION_B>(us, k0, k1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+  }
+}
+
+__device__ __forceinline__ void ab_line_far(const float *__restrict__ us, const float *__restrict__ mom,
+                                            int a0, int rb0, int rc0, int rc1, int rb1, int a1, int lane,
+                                            float kf0, float vbf, float frf, float Y, float &fS, float &fY,
+                                            float &fn, float &fx) {
+  ab_seg_far<false>(us, mom, a0, rb0, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+  ab_seg_far<true>(us, mom, rb0, rc0, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+  ab_seg_far<true>(us, mom, rc1, rb1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+  ab_seg_far<false>(us, mom, rb1, a1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+}
+
 // Regions A and B of the mixed form.  Per line, the offset at the tile's
 // first point is formed in FP64 once and x_k = (k - kc) vb + fr follows in
 // FP32 as in the forward (k - kc exact, |fr| <= vb/2); the shape terms are
@@ -288,6 +442,7 @@ adjoint_ab_kernel(const LinePrep *__restrict__ P, const double *__restrict__ nu0
                   unsigned *__restrict__ ticket, const double *__restrict__ u,
                   double *__restrict__ G) {
   __shared__ float suf[AB_G];
+  __shared__ float s_mom[AF_NC * AF_NB];  // far field: block moments of the staged u
   __shared__ double s_max[AD_WARPS], s_min[AD_WARPS];
   __shared__ int s_bad[AD_WARPS];
   __shared__ int s_t;
@@ -356,6 +511,26 @@ adjoint_ab_kernel(const LinePrep *__restrict__ P, const double *__restrict__ nu0
       for (int k = tid; k < AB_G; k += AD_THREADS) suf[k] = k < gn ? (float)(u[g0 + k] * inv) : 0.f;
     }
     __syncthreads();
+    if (f32) {
+      // moments M_n = sum_j u j^n of each 64-point block (j = -31.5 .. 31.5)
+      for (int b = tid; b < AF_NB; b += AD_THREADS) {
+        float m[AF_NC];
+#pragma unroll
+        for (int n = 0; n < AF_NC; ++n) m[n] = 0.f;
+        for (int i = 0; i < AF_FB; ++i) {
+          const float jj = (float)i - 31.5f;
+          float p = suf[b * AF_FB + i];
+#pragma unroll
+          for (int n = 0; n < AF_NC; ++n) {
+            m[n] += p;
+            p *= jj;
+          }
+        }
+#pragma unroll
+        for (int n = 0; n < AF_NC; ++n) s_mom[n * AF_NB + b] = m[n];
+      }
+      __syncthreads();
+    }
     const int64_t L0 = s_L0, L1 = s_L1;
     const double xg0 = grid_x(g, g0);
     for (int64_t l = L0 + warp; l < L1; l += AD_WARPS) {
@@ -380,7 +555,7 @@ adjoint_ab_kernel(const LinePrep *__restrict__ P, const double *__restrict__ nu0
       double z, zS;
       if (f32l) {
         float fS = 0.f, fY = 0.f, fn = 0.f, fx = 0.f;
-        ab_line(suf, a0, rb0, rc0, rc1, rb1, a1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
+        ab_line_far(suf, s_mom, a0, rb0, rc0, rc1, rb1, a1, lane, kf0, vbf, frf, Y, fS, fY, fn, fx);
         const float zf = warp_sum4(fS, fY, fn, fx, lane);
         z = (double)zf;
         zS = (double)__shfl_sync(0xffffffffu, zf, 0);
