@@ -499,7 +499,7 @@ def run_reference(args):
                "extrapolated: the state's pairs / the sampled pairs per second",
            "sample_s": float(np.mean(secs)), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None,
-           "dtype": "f64", "data": "synthetic (seeded; BASELINE config distributions)",
+           "dtype": "f64", "data": "synthetic (seeded; the benchmark configurations' line distributions)",
            "config": workload_config(W),
            "cpu_baseline": cb,
            "e2e": {"value": v, "unit": "Voigt evals/s", "h2d_bytes_per_step": 0,
@@ -552,7 +552,7 @@ def run_adjoint(args):
            "unit": "Voigt evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32 A/B (f64 offsets), f64 region C and sums" if prec == hkb.MIXED else "f64",
-           "data": "synthetic (seeded; BASELINE config distributions)",
+           "data": "synthetic (seeded; the benchmark configurations' line distributions)",
            "config": {"workload": W["label"], "lines": W["n"], "grid_points": nx, "T": T, "P": P,
                       "cut_cm-1": W["cut"], "precision": args.precision,
                       "loss": "sum_i w_i log K_i, w ~ N(0,1)",
@@ -933,7 +933,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 profile, f64 offsets/strengths/sum/fit" if prec == hkb.MIXED else "f64",
-        "data": "synthetic (seeded; BASELINE config distributions)",
+        "data": "synthetic (seeded; the benchmark configurations' line distributions)",
         "config": workload_config(W),
         "precision": args.precision,
         "parallelism": f"{'states split' if args.workload == 'table' and ws > 1 else 'replicas'} "
