@@ -631,7 +631,16 @@ adjoint_c_kernel(const LinePrep *__restrict__ P, int64_t nlines, GridDev g,
         const double xd = __dmul_rn(__dsub_rn(grid_x(g, k), lp.nu), lp.iad);
         const double uk = u[k];
         const double Sc = lp.Sc;
-        const VDer d = voigt916_dd(xd, lp.vy, lp.ey);
+        // FP32 values and derivatives (lines without Lorentz width: FP64)
+        VDer d;
+        if (lp.vy > 0.0) {
+          const VDerF f = voigt_c_grad_f((float)xd, (float)lp.vy, (float)lp.ey, lp.sig1, lp.dsig1);
+          d.v = f.v;
+          d.vx = f.vx;
+          d.vy = f.vy;
+        } else {
+          d = voigt916_dd(xd, lp.vy, lp.ey);
+        }
         const double cx = Sc * d.vx;
         gS = uk * (Sc * d.v);
         gy = uk * (Sc * d.vy);

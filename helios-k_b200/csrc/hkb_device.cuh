@@ -382,6 +382,18 @@ __device__ __forceinline__ double c916_sig1_tab(double y, const double *__restri
   }
   return s;
 }
+// dSig1/dy = sum_m e_m (-2 y) / (a^2 m^2 + y^2)^2 (the mixed adjoint's region C)
+__device__ __forceinline__ double c916_dsig1_tab(double y, const double *__restrict__ e) {
+  const double a = (double)HK_A916_F;
+  const double y2 = y * y;
+  double s = 0.0;
+#pragma unroll 4
+  for (int m = 1; m <= HK_SIG1_M; ++m) {
+    const double r = __drcp_rn(a * a * m * m + y2);
+    s = __fma_rn(e[m - 1] * r, r, s);
+  }
+  return -2.0 * y * s;
+}
 __device__ __forceinline__ double c916_sig1(double y) {
   double e[HK_SIG1_M];
   for (int m = 1; m <= HK_SIG1_M; ++m) e[m - 1] = c916_e(m);
@@ -519,6 +531,142 @@ __device__ __forceinline__ float voigt916_tab(float x, float y, float iy, float 
   x = fabsf(x);
   if (fmaf(x, x, y * y) >= HK_ASY_R2) return voigt_asy(x, y);
   return voigt916_core(x, y, iy, ey, sig1, R);
+}
+
+// Region C in FP32 with the partial derivatives in x and y (the mixed
+// adjoint), y > 0.  r >= 6: the asymptotic series of w and, by a second
+// Horner sum, of dw/dz = -(i/sqrt(pi)) u S'(u), S' = sum (2k+1) c_k u^k,
+// u = 1/z^2, so dV/dx = Im(u S')/sqrt(pi), dV/dy = Re(u S')/sqrt(pi) (no
+// cancellation, unlike -2 z w + 2i/sqrt(pi)), plus the Stokes term
+// exp(-z^2) and its derivative -2 z exp(-z^2) for y < 1.  r < 6: Algorithm
+// 916 as voigt916_core with every term differentiated: a Gaussian of s3
+// (s2) carries 2 (a m - x) (-2 (a m + x)) in x and each R_m = 1 / (a^2 m^2
+// + y^2) carries -2 y R_m in y; s1 = e^(-x^2) Sig1(y) with dsig1 = Sig1'(y).
+// Float32 emulation against FP64 wofz: V 1.3e-6 relative, the derivatives
+// 2e-6 of |w|.
+struct VDerF {
+  float v, vx, vy;
+};
+
+__device__ __forceinline__ VDerF voigt_c_grad_f(float x, float y, float ey, float sig1, float dsig1) {
+  const float isp = 0.56418958354775628f;  // 1/sqrt(pi)
+  const float L2E = 1.4426950408889634f;
+  const float sx = x < 0.f ? -1.f : 1.f;
+  x = fabsf(x);
+  VDerF o;
+  const float x2 = x * x, Y = y * y;
+  if (x2 + Y >= HK_ASY_R2) {
+    const float ir2 = rcp_fast(x2 + Y), ir4 = ir2 * ir2;
+    const float ur = (x2 - Y) * ir4, ui = -2.0f * x * y * ir4;
+    const float c[HK_ASY_K + 1] = {1.0f, 0.5f, 0.75f, 1.875f, 6.5625f, 29.53125f,
+                                   162.421875f, 1055.7421875f, 7918.06640625f};
+    float sr = c[HK_ASY_K], si = 0.f, pr = (2 * HK_ASY_K + 1) * c[HK_ASY_K], pi = 0.f;
+#pragma unroll
+    for (int k = HK_ASY_K - 1; k >= 0; --k) {
+      const float nr = fmaf(sr, ur, fmaf(-si, ui, c[k]));
+      si = fmaf(sr, ui, si * ur);
+      sr = nr;
+      const float qr = fmaf(pr, ur, fmaf(-pi, ui, (float)(2 * k + 1) * c[k]));
+      pi = fmaf(pr, ui, pi * ur);
+      pr = qr;
+    }
+    float v = fmaf(y, sr, -x * si) * (isp * ir2);
+    float vx = fmaf(ur, pi, ui * pr) * isp;
+    float vy = fmaf(ur, pr, -ui * pi) * isp;
+    if (y < 1.0f) {
+      const float E = ex2_fast(L2E * (Y - x2));
+      float s2, c2;
+      sincosf(2.0f * x * y, &s2, &c2);
+      v = fmaf(E, c2, v);
+      vx = fmaf(-2.0f * E, fmaf(x, c2, y * s2), vx);
+      vy = fmaf(2.0f * E, fmaf(y, c2, -x * s2), vy);
+    }
+    o.v = v;
+    o.vx = sx * vx;
+    o.vy = vy;
+    return o;
+  }
+  if (x == 0.f) {
+    o.v = ey;
+    o.vx = 0.f;
+    o.vy = fmaf(2.0f * y, ey, -2.0f * isp);
+    return o;
+  }
+  const float a = HK_A916_F, a2 = a * a;
+  const float G = 0.48675662279129028f;  // exp(-2 a^2)
+  const float ex2 = expf(-x2);
+  const int mc = min(HK_C916_MR - HK_C916_K, max(1, __float2int_rn(x * (1.0f / a))));
+  const float mcf = (float)mc;
+  const float d = fmaf(a, mcf, -x);
+  const float Tc = ex2_fast(-L2E * d * d);
+  const float up0 = ex2_fast(L2E * fmaf(-a2, fmaf(2.0f, mcf, 1.0f), 2.0f * a * x));
+  const float dn0 = ex2_fast(L2E * fmaf(a2, fmaf(2.0f, mcf, -1.0f), -2.0f * a * x));
+  // s3, sum (a m - x) R T, sum R^2 T
+  float Rm = rcp_fast(fmaf(a2 * mcf, mcf, Y));
+  float s3 = Tc * Rm, s3w = d * (Tc * Rm), s3f = Rm * (Tc * Rm);
+  float T = Tc, q = up0;
+#pragma unroll
+  for (int k = 1; k <= HK_C916_K; ++k) {
+    T *= q;
+    q *= G;
+    const float mf = mcf + (float)k;
+    Rm = rcp_fast(fmaf(a2 * mf, mf, Y));
+    const float tr = T * Rm;
+    s3 += tr;
+    s3w = fmaf(fmaf(a, mf, -x), tr, s3w);
+    s3f = fmaf(Rm, tr, s3f);
+  }
+  T = Tc;
+  q = dn0;
+#pragma unroll
+  for (int k = 1; k <= HK_C916_K; ++k) {
+    T *= q;
+    q *= G;
+    if (mc - k >= 1) {
+      const float mf = mcf - (float)k;
+      Rm = rcp_fast(fmaf(a2 * mf, mf, Y));
+      const float tr = T * Rm;
+      s3 += tr;
+      s3w = fmaf(fmaf(a, mf, -x), tr, s3w);
+      s3f = fmaf(Rm, tr, s3f);
+    }
+  }
+  float s2 = 0.f, s2w = 0.f, s2f = 0.f;
+  const int n2 = min(HK_C916_K, __float2int_ru((5.1f - x) * (1.0f / a)));
+  if (n2 > 0) {
+    float T2 = ex2 * ex2_fast(-L2E * fmaf(2.0f * a, x, a2));
+    float q2 = ex2_fast(L2E * fmaf(-3.0f, a2, -2.0f * a * x));
+    for (int k = 0; k < n2; ++k) {
+      const float mf = (float)(k + 1);
+      Rm = rcp_fast(fmaf(a2 * mf, mf, Y));
+      const float tr = T2 * Rm;
+      s2 += tr;
+      s2w = fmaf(fmaf(a, mf, x), tr, s2w);
+      s2f = fmaf(Rm, tr, s2f);
+      T2 *= q2;
+      q2 *= G;
+    }
+  }
+  const float s1 = ex2 * sig1;
+  const float s1x = -2.0f * x * s1, s1y = ex2 * dsig1;
+  const float s2x = -2.0f * s2w, s2y = -2.0f * y * s2f;
+  const float s3x = 2.0f * s3w, s3y = -2.0f * y * s3f;
+  const float sin2 = sin_sq(x * y);
+  const float cos2 = fmaf(-2.0f, sin2, 1.0f);
+  const float sn2 = sinf(2.0f * x * y);
+  const float iy = 1.0f / y;
+  const float qq = sin2 * iy;  // sin(xy)^2 / y
+  const float t2 = ex2 * qq;
+  const float B = fmaf(-cos2, s1, 0.5f * (s2 + s3));
+  o.v = fmaf(ex2 * ey, cos2, HK_C916_F * fmaf(y, B, t2));
+  const float dcx = -2.0f * y * sn2, dcy = -2.0f * x * sn2;
+  const float dt2x = ex2 * fmaf(-2.0f * x, qq, sn2), dt2y = ex2 * fmaf(x, sn2, -qq) * iy;
+  const float dBx = fmaf(-dcx, s1, fmaf(-cos2, s1x, 0.5f * (s2x + s3x)));
+  const float dBy = fmaf(-dcy, s1, fmaf(-cos2, s1y, 0.5f * (s2y + s3y)));
+  const float eyp = fmaf(2.0f * y, ey, -2.0f * isp);
+  o.vx = sx * fmaf(ey * ex2, fmaf(-2.0f * x, cos2, dcx), HK_C916_F * fmaf(y, dBx, dt2x));
+  o.vy = fmaf(ex2, fmaf(eyp, cos2, ey * dcy), HK_C916_F * (B + fmaf(y, dBy, dt2y)));
+  return o;
 }
 
 // ------------------------------------------------- derivatives (adjoint)

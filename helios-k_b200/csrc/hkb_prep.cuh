@@ -141,7 +141,7 @@ __device__ __forceinline__ void prep_record(const LinesDev &L, const GridDev &g,
     r.c1 = (int)w[3];
     r.b1 = (int)w[4];
     r.i1 = (int)w[5];
-    r.pad = 0;
+    r.dsig1 = hasC ? (float)c916_dsig1_tab(ls.vy, e916) : 0.f;
     r.plinth = (g.plinth && w[5] > w[0]) ? plinth_d(g, S1, Sc, ls.iad, ls.vy) : 0.0;
     reinterpret_cast<LinePrep *>(out)[l] = r;
   }

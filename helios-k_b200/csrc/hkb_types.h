@@ -75,7 +75,7 @@ struct __align__(16) LinePrep {
   double ey;    // erfcx(vy)        (lines with a region-C window)
   int i0, b0, c0, c1, b1, i1;  // [i0,b0) A [b0,c0) B [c0,c1) C [c1,b1) B [b1,i1) A
   float sig1;   // region-C series constant Sig1(vy)
-  int pad;
+  float dsig1;  // dSig1/dy (region C of the mixed adjoint)
   double plinth;  // profile value at the cut edge (removePlinth), else 0
 };
 static_assert(sizeof(LinePrep) == 96, "LinePrep layout");
