@@ -22,8 +22,10 @@
 // applies the chain rule of the line scaling (prep_line) to T and P.
 // Plain form: pass 1 is adjoint_tile_kernel, FP64 for all regions.  Mixed
 // form: pass 1 is adjoint_ab_kernel (regions A and B in FP32, x from the
-// FP64 offset), then adjoint_c_kernel takes region C in FP64 (the
-// differentiated Algorithm-916 series) before pass 2; the sums are FP64.
+// FP64 offset, the far field as per-block series), then adjoint_c_kernel
+// takes region C in FP32 (voigt_c_grad_f: the asymptotic series of w and
+// dw/dz, the differentiated Algorithm-916 series) before pass 2; the sums
+// are FP64.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -580,7 +582,7 @@ adjoint_ab_kernel(const LinePrep *__restrict__ P, const double *__restrict__ nu0
   }
 }
 
-// Region C of the mixed form in FP64 (Algorithm 916 with derivatives),
+// Region C of the mixed form in FP32 (voigt_c_grad_f; FP64 for y = 0),
 // after the A/B pass.  Each warp takes 32 consecutive lines and walks the
 // concatenation of their [c0, c1) windows, one (line, point) pair per lane,
 // so lanes stay busy whatever the windows' widths (a few points per line);
