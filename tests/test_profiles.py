@@ -69,6 +69,7 @@ def test_profile_matches_oracle(small, profile, plinth, cutMode, cut):
         ms = {}
         for prec in (hkb.MIXED, hkb.PLAIN_FP64):
             K = ctx.opacity([T], [P], prec)[0]
+            ctx.opacity([T], [P], prec)  # time a warm call: the first may load the kernel
             ms[prec] = ctx.last_timing()[0]
             err, n = masked_relerr(K, Kref, NBINS)
             print(f"profile {profile} plinth {plinth} cut {cutMode}/{cut} T={T} P={P} "
@@ -119,6 +120,7 @@ def test_sublorentzian_matches_oracle(small, profile, plinth):
             ms = {}
             for prec in (hkb.MIXED, hkb.PLAIN_FP64):
                 K = ctx.opacity([T], [P], prec)[0]
+                ctx.opacity([T], [P], prec)  # time a warm call
                 ms[prec] = ctx.last_timing()[0]
                 err, _ = masked_relerr(K, Kref, NBINS)
                 print(f"sub-Lorentzian profile {profile} plinth {plinth} T={T} precision {prec}: "
