@@ -66,3 +66,27 @@ def test_far_field_matches_oracle(band, profile, dnu, nbins):
               f"far share of long windows ~{far_frac:.2f}")
         assert n > 0 and err < FAR_BOUND
     ctx.set_profile(1, 0)
+
+
+def test_far_field_no_cutoff(band):
+    """The reference's 'no cutoff' (cut = 1e30, heliosk.cu:947): every window
+    spans the whole grid, so nearly every pair lies in a far block, with x
+    up to ~1e6 Doppler widths."""
+    ctx = band["ctx"]
+    NUMIN, NUMAX = band["numin"], band["numax"]
+    dnu, nbins = 0.01, 22
+    ctx.set_profile(1, 0)
+    ctx.set_grid(NUMIN, NUMAX, dnu, nbins, 0, 1e30)
+    nx = oracle.grid_nx(NUMIN, NUMAX, dnu)
+    try:
+        for T, P in ((300.0, 1e-4), (2000.0, 1.0)):
+            Q = oracle.partition(band["Tq"], band["Qq"], T)
+            nu, S, iad, vy = oracle.prep_hitran(band["L"], [synth.MASS], [1.0], [Q], T, P, qalphaL=1.0)
+            win = oracle.windows(nu, S, iad, vy, NUMIN, dnu, nx, 0, 1e30)
+            Kref, _ = oracle.opacity(nu, S, iad, vy, win, NUMIN, dnu, nx)
+            K = ctx.opacity([T], [P], hkb.MIXED)[0]
+            err, n = masked_relerr(K, Kref, nbins)
+            print(f"no cutoff: T={T} P={P}: err {err:.2e} over {n} points")
+            assert n > 0 and err < FAR_BOUND
+    finally:
+        ctx.set_grid(NUMIN, NUMAX, dnu, nbins, 0, 25.0)
