@@ -551,7 +551,7 @@ def run_adjoint(args):
     out = {"metric": "Voigt evals/s (forward + adjoint)", "value": 2 * pairs / (ms * 1e-3),
            "unit": "Voigt evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f32 A/B (f64 offsets), f64 region C and sums" if prec == hkb.MIXED else "f64",
+           "dtype": "f32 profile and derivatives, f64 offsets/strengths/sums" if prec == hkb.MIXED else "f64",
            "data": "synthetic (seeded; the benchmark configurations' line distributions)",
            "config": {"workload": W["label"], "lines": W["n"], "grid_points": nx, "T": T, "P": P,
                       "cut_cm-1": W["cut"], "precision": args.precision,

@@ -153,9 +153,11 @@ static __device__ __noinline__ int64_t first_true(const WinCtx &c, int kind, dou
   return a;
 }
 
+// A starting index for first_true (any value gives the same answer; a
+// close one saves steps): idnu = 1 / dnu.
 __device__ __forceinline__ int64_t est_index(double edge, const GridDev &g,
-                                             int64_t hi) {
-  const double e = ceil((edge - g.numin) / g.dnu);
+                                             int64_t hi, double idnu) {
+  const double e = ceil((edge - g.numin) * idnu);
   if (!(e > -1.0)) return 0;
   if (e > (double)hi) return hi;
   return (int64_t)e;
@@ -185,13 +187,16 @@ __device__ __forceinline__ void line_windows(const GridDev &g, const StateDev &s
   else if (g.cutMode == 2) w = __ddiv_rn(g.cut, ls.iad);
   else w = g.cut;
   c.w = w;
-  const int64_t i0 = first_true(c, HK_P_LEFT_CUT, 0.0, g0, g1, est_index(ls.nu - w, g, g1));
-  const int64_t i1 = first_true(c, HK_P_RIGHT_CUT, 0.0, i0, g1, est_index(ls.nu + w, g, g1));
+  // the searches' starting points need no exact arithmetic (FP64 division
+  // and square root are slow on this part)
+  const double idnu = 1.0 / g.dnu;
+  const int64_t i0 = first_true(c, HK_P_LEFT_CUT, 0.0, g0, g1, est_index(ls.nu - w, g, g1, idnu));
+  const int64_t i1 = first_true(c, HK_P_RIGHT_CUT, 0.0, i0, g1, est_index(ls.nu + w, g, g1, idnu));
   if (i1 <= i0) {
     for (int k = 0; k < 6; ++k) out[k] = i0;
     return;
   }
-  const int64_t ic = first_true(c, HK_P_CENTER, 0.0, i0, i1, est_index(ls.nu, g, g1));
+  const int64_t ic = first_true(c, HK_P_CENTER, 0.0, i0, i1, est_index(ls.nu, g, g1, idnu));
   const double Rs[2] = {1.0e6, 100.0};
   int64_t lohi[2][2];
 #pragma unroll
@@ -199,9 +204,9 @@ __device__ __forceinline__ void line_windows(const GridDev &g, const StateDev &s
     const double R = Rs[r];
     const double h2 = R - c.vy2;
     if (g.profile == 1 && h2 > 0.0) {  // regions B and C are the Voigt profile's
-      const double h = sqrt(h2) / c.iad;
-      lohi[r][0] = first_true(c, HK_P_LEFT_R, R, i0, ic, est_index(ls.nu - h, g, g1));
-      lohi[r][1] = first_true(c, HK_P_RIGHT_R, R, ic, i1, est_index(ls.nu + h, g, g1));
+      const double h = (double)(sqrtf((float)h2) / (float)c.iad);
+      lohi[r][0] = first_true(c, HK_P_LEFT_R, R, i0, ic, est_index(ls.nu - h, g, g1, idnu));
+      lohi[r][1] = first_true(c, HK_P_RIGHT_R, R, ic, i1, est_index(ls.nu + h, g, g1, idnu));
     } else {
       lohi[r][0] = ic;
       lohi[r][1] = ic;

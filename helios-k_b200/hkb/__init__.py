@@ -129,6 +129,21 @@ def _is_dev(t):
     return hasattr(t, "is_cuda") and t.is_cuda
 
 
+def _host_f64(n):
+    """A numpy float64 array of n values in page-locked memory when torch
+    can supply it (its caching host allocator reuses the block once the
+    array is dropped), so a device-to-host copy into it runs at full link
+    speed; plain numpy memory otherwise, and above 1 GiB (the allocator
+    rounds blocks up to powers of two)."""
+    try:
+        import torch
+        if 8 * n <= (1 << 30) and torch.cuda.is_available():
+            return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    except ImportError:
+        pass
+    return np.empty(n, np.float64)
+
+
 class Context:
     """One libhkb context bound to one GPU (hk_create / hk_destroy)."""
 
@@ -357,7 +372,7 @@ class Context:
             import torch
             mk = lambda: torch.empty(n, dtype=torch.float64, device=torch.device("cuda", self.device))
         else:
-            mk = lambda: np.empty(n, np.float64)
+            mk = lambda: _host_f64(n)
         dS = mk() if per_line else None
         dG = mk() if per_line else None
         sh = _stream_handle(stream, dev or device_out)
