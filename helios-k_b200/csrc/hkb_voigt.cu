@@ -149,7 +149,7 @@ static_assert(sizeof(ExtPL) == 64, "ExtPL layout");
 constexpr int HK_RPAD = 8;
 // Far field (the default option set): each warp's FP64 sums of the blocks'
 // Taylor coefficients, HK_FN per 64-point block.
-constexpr int HK_FB = 64, HK_FN = 8;
+constexpr int HK_FB = 64, HK_FN = 9;
 template <class SH, int EXT = HK_EXT_NONE>
 constexpr size_t smem_mixed() {
   return sizeof(RecF) * SH::CH + sizeof(float) * (HK_RPAD + SH::CH * HK_C916_MR) +
@@ -256,15 +256,17 @@ __device__ __forceinline__ int line_key(const LinePrepF *__restrict__ P, int64_t
 // inside one of regions A and B (no region boundary, no region-C point) and
 // its centre is at least HK_FAR_DK grid steps from the line centre.  The
 // term's singularities in the complex offset plane are the zeros of
-// x^2 + y^2, r0 = |x0 + iy| >= |x0| >= 315 vb away (for small y nearly a
+// x^2 + y^2, r0 = |x0 + iy| >= |x0| >= 250 vb away (for small y nearly a
 // double pole, whose Taylor remainder after N terms is about (N + 1) rho^N),
 // and for GH2 those of its other denominator factor, close to +-i
-// sqrt(y^2 + 0.55).  With rho = |j vb| / r0 <= 0.1, HK_FN = 8 terms leave
-// 9 * 0.1^8 = 1e-7 of the term (measured in FP64 over region B next to
-// region C: 9.8e-8; in FP32 with rounding: 5.2e-7).  FP64 (weak) lines and
+// sqrt(y^2 + 0.55).  With rho = |j vb| / r0 <= 31.5 / 250.5 = 0.126,
+// HK_FN = 9 terms leave 10 * 0.126^9 = 8e-8 of the term, below the FP32
+// rounding of the sums (9 terms is what the per-warp FP64 coefficient sums
+// leave room for at 4 CTAs per SM; 8 terms needed 315.5 steps for the same
+// bound, leaving a wider near zone to the direct sweeps).  FP64 (weak) lines and
 // lines with x^2 + y^2 >= 1e18 in their window take the direct sweeps
 // throughout.
-constexpr float HK_FAR_DK = 315.5f;
+constexpr float HK_FAR_DK = 250.5f;
 
 // bits [a, b) of a 32-bit mask (a, b clamped to [0, 32])
 __device__ __forceinline__ unsigned range_bits(int a, int b) {
@@ -525,6 +527,7 @@ __device__ __forceinline__ void far_terms(const RecF &r, int blo, float (&fq)[HK
     q[5] = -fmaf(D1, q[4], fmaf(D2, q[3], fmaf(D3, q[2], fmaf(D4, q[1], D5 * q[0])))) * iD;
     q[6] = -fmaf(D1, q[5], fmaf(D2, q[4], fmaf(D3, q[3], fmaf(D4, q[2], fmaf(D5, q[1], D6 * q[0]))))) * iD;
     q[7] = -fmaf(D1, q[6], fmaf(D2, q[5], fmaf(D3, q[4], fmaf(D4, q[3], fmaf(D5, q[2], D6 * q[1]))))) * iD;
+    q[8] = -fmaf(D1, q[7], fmaf(D2, q[6], fmaf(D3, q[5], fmaf(D4, q[4], fmaf(D5, q[3], D6 * q[2]))))) * iD;
   } else {
     const float d0 = fmaf(x0, x0, r.y * r.y);
     const float iD = rcp_fast(d0);
