@@ -46,7 +46,7 @@ struct TileShape {
   static constexpr int THREADS = 32 * WARPS_;
   static constexpr int SLICE = 32 * PPL_;        // points per warp
   static constexpr int G = WARPS_ * SLICE;       // points per tile
-  static_assert(G <= 2048, "k * vb_hi must stay exact in FP32 (11 bits)");
+  static_assert(G <= 2048, "a staged line's far-block mask holds 32 blocks of 64 points");
   static_assert(CH % 32 == 0 && CH <= THREADS, "one staging thread per line");
   static_assert(PPL % 2 == 0, "points are processed in pairs");
 };
