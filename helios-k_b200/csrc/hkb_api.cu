@@ -1051,6 +1051,56 @@ hk_status hk_set_line_scales(hk_ctx *c, const double *s_scale, const double *g_s
   return HK_OK;
 }
 
+// true when p is device (or managed) memory of this context's GPU
+static bool on_ctx_device(const hk_ctx *c, const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == c->device;
+}
+
+hk_status hk_set_line_scales_device(hk_ctx *c, const double *s_scale, const double *g_scale,
+                                    void *stream) {
+  if (!c) return HK_ERR_ARG;
+  if (c->nlines == 0 && (s_scale || g_scale)) return fail(c, HK_ERR_STATE, "no lines loaded");
+  cudaSetDevice(c->device);
+  const double *src[2] = {s_scale, g_scale};
+  for (int q = 0; q < 2; ++q)
+    if (src[q] && !on_ctx_device(c, src[q]))
+      return fail(c, HK_ERR_ARG, "%s is not device memory of GPU %d", q ? "g_scale" : "s_scale", c->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t n = c->nlines;
+  DevBuf *dst[2] = {&c->sscale, &c->gscale};
+  const double **field[2] = {&c->L.sscale, &c->L.gscale};
+  for (int q = 0; q < 2; ++q) {
+    if (!src[q]) {
+      dst[q]->release();
+      *field[q] = nullptr;
+      continue;
+    }
+    // the values, then the word of the first invalid load index
+    CUDA_TRY(c, dst[q]->ensure(n * sizeof(double) + sizeof(unsigned long long)));
+    unsigned long long *bad = reinterpret_cast<unsigned long long *>(dst[q]->as<double>() + n);
+    CUDA_TRY(c, launch_gather_scales(n, c->order.as<int64_t>(), src[q], dst[q]->as<double>(), bad, s));
+    unsigned long long first_bad = 0;
+    CUDA_TRY(c, cudaMemcpyAsync(&first_bad, bad, sizeof first_bad, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(c, cudaStreamSynchronize(s));
+    if (first_bad < (unsigned long long)n) {
+      // the buffer now holds the invalid values: no multiplier stays in force
+      for (int r = 0; r < 2; ++r) {
+        dst[r]->release();
+        *field[r] = nullptr;
+      }
+      return fail(c, HK_ERR_ARG, "line scale %lld must be finite and > 0", (long long)first_bad);
+    }
+    *field[q] = dst[q]->as<double>();
+  }
+  ok(c);
+  return HK_OK;
+}
+
 static hk_status opacity_vjp(hk_ctx *c, double T, double P, int precision, const double *u,
                              int u_on_device, double *dT, double *dP, double *dlogS, double *dgammaL,
                              int log_gamma, int outputs_on_device, void *stream) {

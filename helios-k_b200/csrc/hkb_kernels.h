@@ -201,6 +201,10 @@ cudaError_t launch_kdist(const double *K_d, int64_t k_stride, int nstates,
 cudaError_t launch_gather_lines(int64_t n, const int64_t *order_d,
                                 const double *src_d, double *dst_d,
                                 cudaStream_t stream);
+// per-line multipliers (device, load order) into the sorted order; *bad_d:
+// the smallest load index of a value that is not finite and > 0, else n
+cudaError_t launch_gather_scales(int64_t n, const int64_t *order_d, const double *src_d,
+                                 double *dst_d, unsigned long long *bad_d, cudaStream_t stream);
 
 cudaError_t sort_lines_by_nu(int64_t n, double *nu_d, int64_t *order_d,
                              cudaStream_t stream);

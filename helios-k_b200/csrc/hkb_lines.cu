@@ -41,6 +41,30 @@ cudaError_t launch_gather_lines(int64_t n, const int64_t *order_d,
   return cudaGetLastError();
 }
 
+// Per-line multipliers from load order into the nu-sorted order, dst[k] =
+// src[order[k]], each checked to be finite and > 0: *bad ends as the
+// smallest load index of a value that is not (n when all are).
+__global__ void bad_init_kernel(unsigned long long *bad, int64_t n) { *bad = (unsigned long long)n; }
+
+__global__ void gather_scales_kernel(int64_t n, const int64_t *__restrict__ order,
+                                     const double *__restrict__ src, double *__restrict__ dst,
+                                     unsigned long long *bad) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = order[k];
+    const double v = src[j];
+    dst[k] = v;
+    if (!(v > 0.0 && v <= 1.7976931348623157e308)) atomicMin(bad, (unsigned long long)j);
+  }
+}
+
+cudaError_t launch_gather_scales(int64_t n, const int64_t *order_d, const double *src_d,
+                                 double *dst_d, unsigned long long *bad_d, cudaStream_t stream) {
+  bad_init_kernel<<<1, 1, 0, stream>>>(bad_d, n);
+  if (n > 0) gather_scales_kernel<<<1184, 256, 0, stream>>>(n, order_d, src_d, dst_d, bad_d);
+  return cudaGetLastError();
+}
+
 // Sorts nu_d in place (ascending) and returns the permutation in order_d.
 cudaError_t sort_lines_by_nu(int64_t n, double *nu_d, int64_t *order_d,
                              cudaStream_t stream) {

@@ -74,6 +74,7 @@ def lib():
             "hk_kdist_noalloc": (_i, [_p, _i, _i64, _i, _i, _d, _d, _p, _p, _p, _p,
                                       C.c_char_p, _i]),
             "hk_set_line_scales": (_i, [_p, _p, _p]),
+            "hk_set_line_scales_device": (_i, [_p, _p, _p, _p]),
             "hk_set_workspace": (_i, [_p, _d, _d]),
             "hk_opacity_vjp": (_i, [_p, _d, _d, _i, _p, _i, _p, _p, _p, _p, _i, _p]),
             "hk_opacity_vjp_log": (_i, [_p, _d, _d, _i, _p, _i, _p, _p, _p, _p, _i, _p]),
@@ -351,8 +352,22 @@ class Context:
         self._chk(lib().hk_set_workspace(self._h, float(prep_bytes), float(part_bytes)))
 
     # --------------------------------------------------------- adjoint
-    def set_line_scales(self, s_scale=None, g_scale=None):
-        """Per-line multipliers of strength and Lorentz width (load order)."""
+    def set_line_scales(self, s_scale=None, g_scale=None, stream=None):
+        """Per-line multipliers of strength and Lorentz width (load order).
+
+        CUDA tensors (float64 on this context's GPU, or convertible to it)
+        are reordered and checked on the GPU, in order on `stream` (default:
+        torch's current stream), without passing through host memory
+        (hk_set_line_scales_device); anything else goes through the host
+        (hk_set_line_scales)."""
+        if _is_dev(s_scale) or _is_dev(g_scale):
+            import torch
+            dev = torch.device("cuda", self.device)
+            conv = lambda v: None if v is None else torch.as_tensor(v, dtype=torch.float64, device=dev).contiguous()
+            s, g = conv(s_scale), conv(g_scale)
+            self._chk(lib().hk_set_line_scales_device(self._h, _ptr(s), _ptr(g),
+                                                      _stream_handle(stream, True)))
+            return
         s = None if s_scale is None else _f64(s_scale)
         g = None if g_scale is None else _f64(g_scale)
         self._chk(lib().hk_set_line_scales(self._h, _ptr(s), _ptr(g)))

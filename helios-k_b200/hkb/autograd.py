@@ -17,9 +17,10 @@ import hkb
 
 
 def _scales(v):
+    # a CUDA tensor stays on the GPU (hk_set_line_scales_device)
     if v is None:
         return None
-    return torch.exp(v.detach().to(torch.float64)).cpu().numpy()
+    return torch.exp(v.detach().to(torch.float64)).contiguous()
 
 
 class Opacity(torch.autograd.Function):

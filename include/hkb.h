@@ -282,6 +282,21 @@ hk_status hk_tuning_result(hk_ctx *ctx, int *last_shape, int *tuned_shape, doubl
  * Loading a new line list clears them.  No counterpart in the reference. */
 hk_status hk_set_line_scales(hk_ctx *ctx, const double *s_scale, const double *g_scale);
 
+/* The same multipliers from DEVICE arrays (load order, hk_num_lines values
+ * each, on this context's GPU; NULL restores 1), reordered and checked on
+ * the GPU in stream order on `stream` (a cudaStream_t, NULL the legacy
+ * stream); the call returns once they are in place, having copied only the
+ * check's 8-byte result to the host.  For callers whose parameters live on
+ * the GPU (an optimiser's tensors): hk_set_line_scales would take them
+ * through host memory twice.  Pointers that are not device memory of this
+ * context's GPU are refused (HK_ERR_ARG) before any launch.  A value that is
+ * not finite and > 0 fails with HK_ERR_ARG naming its load index, and then
+ * both multipliers are restored to 1.  Work on other streams that still
+ * reads the previous multipliers must be complete.  No counterpart in the
+ * reference. */
+hk_status hk_set_line_scales_device(hk_ctx *ctx, const double *s_scale, const double *g_scale,
+                                    void *stream);
+
 /* Vector-Jacobian product of the opacity of one state: with the seed
  * u[i] = dLoss/dK_i (Nx values, e.g. w_i / K_i for Loss = sum_i w_i log K_i),
  * returns dLoss/dT (K), dLoss/dP (atm for HITRAN, bar for ExoMol), and per
